@@ -1,0 +1,358 @@
+"""Benchmark: Airfoil ms/iteration on the 2400x1200 (2.88M-cell) mesh, plain FP64.
+
+One step = one Airfoil outer iteration through the OP2 API on libop2b
+(save_soln + 2 x {adt_calc, res_calc, bres_calc, update}, rms read back after
+each update, as apps/c/airfoil/airfoil_plain/dp/airfoil.cpp:221-297 does).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl op2b|reference]
+
+N > 1 runs under torchrun: every rank solves its own replica (the single-mesh
+path does not shard; there is no collective on the data path), timing is the
+max over ranks.  Prints one JSON line on rank 0.
+
+* value      device-timed ms/iteration, inputs resident in HBM (CUDA events on
+             the library's stream, K iterations between a barrier and
+             synchronize on both sides).  The working set (~690 MB) is larger
+             than L2 (126 MB), so no flush is needed between iterations.
+* e2e        the same metric through the public API with host buffers:
+             op_decl_* uploads from pinned host memory, K iterations, and
+             op_fetch_data of q, all inside the timed region, per iteration.
+* roofline   the dominant loop's algorithmic bytes per call / its average
+             CUDA-event duration, against MEASURED_PEAKS.json hbm_gbs.
+* cpu_baseline  the reference's own OpenMP build (oracle/_ref, compiled from
+             the reference sources) on a bounded sample of the same mesh.
+* --impl reference   times that reference build alone (rank 0; others exit).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "op2-common_b200"))
+sys.path.insert(0, REPO)
+
+FALLBACK_HBM_GBS = 6650.0
+LOOPS = ("save_soln", "adt_calc", "res_calc", "bres_calc", "update")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="op2b", choices=["op2b", "reference"])
+    p.add_argument("--mesh", type=int, nargs=2, default=[2400, 1200])
+    p.add_argument("--seed", type=int, default=1)
+    p.add_argument("--inc-mode", type=int, default=None,
+                   help="0 atomics, 1 colouring, 2 staged+atomics (default: library default)")
+    p.add_argument("--precision", default="f64", choices=["f64", "mixed"])
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--cpu-iters", type=int, default=4)
+    return p.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", str(rank)))
+    return ws, rank, local
+
+
+def mesh_file(I, J, seed):
+    from op2b import mesh as M
+    path = os.path.join(tempfile.gettempdir(), f"op2b_mesh_{I}x{J}_s{seed}.bin")
+    if not os.path.exists(path):
+        m = M.channel_bump(I, J, seed=seed)
+        tmp = path + f".{os.getpid()}"
+        M.write_grid_bin(m, tmp)
+        os.replace(tmp, path)
+        return m, path
+    return M.read_grid_bin(path), path
+
+
+def peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
+
+
+def traffic_from_profiles(loop, workload_key):
+    """dram bytes per launch of `loop` from the committed ncu summary, if any."""
+    p = os.path.join(REPO, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    return d.get(workload_key, {}).get(loop)
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (start before, stop after)."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(tempfile.gettempdir(), f"op2b_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index),
+                                          f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for ln in f:
+                parts = [x.strip() for x in ln.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx = float(parts[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def run_reference(args, m_path, ncell, iters, skip, threads):
+    from oracle import oracle as O
+    binary = O.ref_binary("ref_airfoil_openmp")
+    kind = "reference"
+    if binary is None:
+        return None
+    env = {"OMP_NUM_THREADS": str(threads)}
+    summary, _ = O.run_reference_airfoil_timed(binary, m_path, iters, skip, env=env)
+    return dict(value=summary["ms_per_iter"], unit="ms/iter", cores=summary.get("threads", threads),
+                kind=kind, sample=f"{summary['timed_iters']} iterations of the {args.mesh[0]}x"
+                f"{args.mesh[1]} mesh ({ncell} cells) after {skip} untimed, OpenMP build of the "
+                "reference (v1 translator output), OMP_NUM_THREADS=" + str(threads))
+
+
+def impl_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    m, path = mesh_file(*args.mesh, args.seed)
+    threads = os.cpu_count() or 1
+    # one step = one iteration of the reference's OpenMP build on the same mesh;
+    # warm-up iterations (plan construction included) are run but not timed
+    res = run_reference(args, path, m.ncell, args.warmup + args.steps, args.warmup, threads)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/ref_airfoil_openmp not built (make -C oracle)"}))
+        return 0
+    v = res["value"]
+    line = {"metric": "Airfoil ms/iter (2400x1200 FP64)", "value": v, "unit": "ms/iter",
+            "impl": "reference", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": v, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"airfoil {args.mesh[0]}x{args.mesh[1]} plain FP64, "
+                       "random numbering", "cells": m.ncell, "edges": m.nedge},
+            "cpu_baseline": res,
+            "e2e": {"value": v, "unit": "ms/iter", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return impl_reference(args)
+    ws, rank, local = dist_env()
+    os.environ["OP2B_DEVICE"] = str(local)
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    from op2b import build, lib as L
+    from op2b.airfoil import Airfoil
+    build.build()
+    L.load()
+    m, m_path = mesh_file(*args.mesh, args.seed)
+    dtype = np.float64 if args.precision == "f64" else np.float32
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---------------------------------------------------------- device-resident timing
+    L.op_init()
+    if args.inc_mode is not None:
+        L.set_option("inc_mode", args.inc_mode)
+    app = Airfoil(m, dtype=dtype)
+    stream = torch.cuda.ExternalStream(L.load().op2b_get_stream())
+    app.iterate(args.warmup, history=False)
+    L.synchronize()
+    L.load().op2b_reset_stats()
+    clocks = Clocks(local)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    L.synchronize()
+    launches0 = L.load().op2b_kernel_launches()
+    clocks.start()
+    e0.record(stream)
+    hist = app.iterate(args.steps)
+    e1.record(stream)
+    L.synchronize()
+    barrier()
+    clk = clocks.stop()
+    launches = L.load().op2b_kernel_launches() - launches0
+    ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    ms = max_over_ranks(ms)
+    stats = {n: L.loop_stats(n) for n in LOOPS}
+    final_rms = hist[-1][0] if hist else float("nan")
+    L.op_exit()
+
+    # ---------------------------------------------------------- end to end through the API
+    e2e = None
+    if not args.no_e2e:
+        pinned = {}
+
+        def pin(a):
+            t = torch.empty(a.shape, dtype={np.float64: torch.float64, np.float32: torch.float32,
+                                            np.int32: torch.int32}[a.dtype.type],
+                            pin_memory=True)
+            arr = t.numpy()
+            arr[...] = a
+            pinned[id(arr)] = t
+            return arr
+
+        from op2b.mesh import Mesh
+        hm = Mesh(x=pin(m.x.astype(dtype)), cell=pin(m.cell), edge=pin(m.edge),
+                  ecell=pin(m.ecell), bedge=pin(m.bedge), becell=pin(m.becell),
+                  bound=pin(m.bound))
+        L.op_init()
+        if args.inc_mode is not None:
+            L.set_option("inc_mode", args.inc_mode)
+        warm = Airfoil(hm, dtype=dtype)      # warm the plan/alloc paths once
+        warm.iterate(1, history=False)
+        L.op_exit()
+        L.op_init()
+        if args.inc_mode is not None:
+            L.set_option("inc_mode", args.inc_mode)
+        barrier()
+        t0 = time.perf_counter()
+        app2 = Airfoil(hm, dtype=dtype)
+        h2 = app2.iterate(args.steps)
+        q = L.op_fetch_data(app2.p_q)
+        t1 = time.perf_counter()
+        barrier()
+        ms_e2e = max_over_ranks(1e3 * (t1 - t0) / max(args.steps, 1))
+        es = np.dtype(dtype).itemsize
+        h2d = (m.x.size * es + (m.cell.size + m.edge.size + m.ecell.size + m.bedge.size
+                                + m.becell.size + m.bound.size) * 4
+               + m.ncell * 4 * es * 3 + m.ncell * es)
+        d2h = q.nbytes + args.steps * 2 * 32
+        e2e = {"value": ms_e2e, "unit": "ms/iter",
+               "h2d_bytes_per_step": int(h2d / max(args.steps, 1)),
+               "d2h_bytes_per_step": int(d2h / max(args.steps, 1)),
+               "note": "op_decl_* uploads from pinned host memory + K iterations + "
+                       "op_fetch_data(q), per iteration"}
+        L.op_exit()
+
+    # ---------------------------------------------------------- CPU baseline (rank 0, N=1)
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        cpu = run_reference(args, m_path, m.ncell, 1 + args.cpu_iters, 1, threads)
+        if cpu is None:
+            from oracle import oracle as O
+            t0 = time.perf_counter()
+            O.airfoil_run(m, __import__("op2b.mesh", fromlist=["x"]).airfoil_constants(), 2)
+            cpu = dict(value=1e3 * (time.perf_counter() - t0) / 2, unit="ms/iter", cores=1,
+                       kind="port", sample="2 iterations of the C restatement (oracle)")
+
+    if rank == 0:
+        peak, peak_src = peaks()
+        work = f"{args.mesh[0]}x{args.mesh[1]}"
+        loops = {}
+        for n, s in stats.items():
+            if s and s["calls"]:
+                avg = s["total_ms"] / s["calls"]
+                loops[n] = {"calls": s["calls"], "avg_ms": avg,
+                            "alg_bytes": s["bytes_per_call"],
+                            "gbs": s["bytes_per_call"] / (avg * 1e-3) / 1e9 if avg > 0 else None}
+        dom = max(loops, key=lambda n: loops[n]["avg_ms"] * loops[n]["calls"])
+        d = loops[dom]
+        traffic = traffic_from_profiles(dom, f"{work}_{args.precision}_mode{args.inc_mode}")
+        line = {
+            "metric": "Airfoil ms/iter (2400x1200 FP64)", "value": ms, "unit": "ms/iter",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "f64" else "f32-storage/f64-update",
+            "data": "synthetic (seeded channel-with-bump mesh, random numbering)",
+            "config": {"workload": f"airfoil {work} plain {'FP64' if args.precision == 'f64' else 'mixed'}"
+                                   f", random numbering, inc_mode {args.inc_mode if args.inc_mode is not None else 'default'}",
+                       "cells": m.ncell, "edges": m.nedge, "nodes": m.nnode,
+                       "bedges": m.nbedge, "parallelism": "replicas" if ws > 1 else "single",
+                       "l2": "inputs larger than L2 (working set ~0.7 GB > 126 MB), no flush"},
+            "roofline": {"bound": "hbm", "loop": dom, "achieved": d["gbs"], "peak": peak,
+                         "unit": "GB/s", "frac": d["gbs"] / peak if d["gbs"] else None,
+                         "traffic": traffic, "peak_source": peak_src},
+            "loops": loops,
+            "rms_final": final_rms,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "clocks": clk,
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

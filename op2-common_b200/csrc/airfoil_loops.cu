@@ -1,0 +1,372 @@
+// Device loops for the five Airfoil kernels (save_soln, adt_calc, res_calc,
+// bres_calc, update) on sm_100a.
+//
+// Layout: every dat is AoS in HBM (element = dim contiguous values), maps
+// are AoS int32 [from][dim].  A cell's q is one aligned 32-byte (FP64) or
+// 16-byte (FP32) record, so a gathered q costs one DRAM sector, and direct
+// loops read it with 16-byte vector loads that coalesce across a warp.
+//
+// Direct loops (save_soln, update, adt_calc's cell-side streams) run a
+// persistent grid (a multiple of the SM count) with grid-stride loops.
+// update fuses the rms sum and the maxerr max/argmax (op_arg_gbl OP_INC,
+// OP_MAX and op_arg_info of update.h) into one pass: warp shuffles, one shared
+// memory round per block, and the last block to finish reduces the per-block
+// partials in a fixed order, so the result is deterministic run to run and
+// needs no second launch.
+//
+// Indirect increments (res_calc, bres_calc) have three variants, selected by
+// the runtime: plain FP64/FP32 atomics (this file), and the plan-driven
+// staged variants in airfoil_staged.cu.
+#include "airfoil_math.cuh"
+#include "loops.h"
+
+#include <stdint.h>
+
+namespace op2b {
+
+// ---------------------------------------------------------------- loads
+
+template <typename T> struct Vec;
+template <> struct Vec<double> {
+  static __device__ __forceinline__ void ld2(const double *p, double &a, double &b) {
+    double2 v = __ldg(reinterpret_cast<const double2 *>(p));
+    a = v.x;
+    b = v.y;
+  }
+  static __device__ __forceinline__ void ld4(const double *p, double *o) {
+    double2 v0 = __ldg(reinterpret_cast<const double2 *>(p));
+    double2 v1 = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+    o[0] = v0.x; o[1] = v0.y; o[2] = v1.x; o[3] = v1.y;
+  }
+  static __device__ __forceinline__ void ld4_rw(const double *p, double *o) {
+    double2 v0 = reinterpret_cast<const double2 *>(p)[0];
+    double2 v1 = reinterpret_cast<const double2 *>(p)[1];
+    o[0] = v0.x; o[1] = v0.y; o[2] = v1.x; o[3] = v1.y;
+  }
+  static __device__ __forceinline__ void st4(double *p, const double *v) {
+    reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+  }
+};
+template <> struct Vec<float> {
+  static __device__ __forceinline__ void ld2(const float *p, float &a, float &b) {
+    float2 v = __ldg(reinterpret_cast<const float2 *>(p));
+    a = v.x;
+    b = v.y;
+  }
+  static __device__ __forceinline__ void ld4(const float *p, float *o) {
+    float4 v = __ldg(reinterpret_cast<const float4 *>(p));
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+  }
+  static __device__ __forceinline__ void ld4_rw(const float *p, float *o) {
+    float4 v = *reinterpret_cast<const float4 *>(p);
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+  }
+  static __device__ __forceinline__ void st4(float *p, const float *v) {
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  }
+};
+
+static inline int grid_for(const LaunchCtx &c, long long n, int threads, int per_sm) {
+  long long want = (n + threads - 1) / threads;
+  long long cap = (long long)c.nsm * per_sm;
+  if (want < 1) want = 1;
+  return (int)(want < cap ? want : cap);
+}
+
+// ---------------------------------------------------------------- save_soln
+
+// save_soln.h:1-4 is a copy of q into qold: 16-byte vector copy, 4 loads in
+// flight per thread before the stores.
+__global__ void __launch_bounds__(256) k_copy16(const uint4 *__restrict__ src,
+                                                uint4 *__restrict__ dst, long long n16) {
+  long long stride = (long long)gridDim.x * blockDim.x;
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i + 3 * stride < n16; i += 4 * stride) {
+    uint4 a = __ldcs(src + i), b = __ldcs(src + i + stride);
+    uint4 c = __ldcs(src + i + 2 * stride), d = __ldcs(src + i + 3 * stride);
+    __stcs(dst + i, a);
+    __stcs(dst + i + stride, b);
+    __stcs(dst + i + 2 * stride, c);
+    __stcs(dst + i + 3 * stride, d);
+  }
+  for (; i < n16; i += stride)
+    __stcs(dst + i, __ldcs(src + i));
+}
+
+__global__ void k_copy_tail(const unsigned char *src, unsigned char *dst, long long n) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = src[i];
+}
+
+cudaError_t launch_copy(const LaunchCtx &c, const void *src, void *dst, size_t bytes) {
+  long long n16 = (long long)(bytes / 16);
+  if (n16 > 0) {
+    k_copy16<<<grid_for(c, n16, 256, 8), 256, 0, c.stream>>>(
+        static_cast<const uint4 *>(src), static_cast<uint4 *>(dst), n16);
+    c.count();
+  }
+  long long tail = (long long)(bytes - 16 * (size_t)n16);
+  if (tail > 0) {
+    k_copy_tail<<<1, 32, 0, c.stream>>>(static_cast<const unsigned char *>(src) + 16 * n16,
+                                        static_cast<unsigned char *>(dst) + 16 * n16, tail);
+    c.count();
+  }
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- adt_calc
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_adt_calc(int ncell, const int4 *__restrict__ pcell, const T *__restrict__ x,
+           const T *__restrict__ q, T *__restrict__ adt, AirConst<T> k) {
+  int stride = gridDim.x * blockDim.x;
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < ncell; n += stride) {
+    int4 c = __ldg(pcell + n);
+    T x1x, x1y, x2x, x2y, x3x, x3y, x4x, x4y, qq[4];
+    Vec<T>::ld2(x + 2 * (size_t)c.x, x1x, x1y);
+    Vec<T>::ld2(x + 2 * (size_t)c.y, x2x, x2y);
+    Vec<T>::ld2(x + 2 * (size_t)c.z, x3x, x3y);
+    Vec<T>::ld2(x + 2 * (size_t)c.w, x4x, x4y);
+    Vec<T>::ld4(q + 4 * (size_t)n, qq);
+    adt[n] = air_adt<T>(x1x, x1y, x2x, x2y, x3x, x3y, x4x, x4y, qq[0], qq[1],
+                        qq[2], qq[3], k);
+  }
+}
+
+template <typename T>
+cudaError_t launch_adt_calc(const LaunchCtx &c, int ncell, const int *pcell, const T *x,
+                            const T *q, T *adt, const AirConst<T> &k) {
+  if (ncell <= 0) return cudaSuccess;
+  k_adt_calc<T><<<grid_for(c, ncell, 256, 8), 256, 0, c.stream>>>(
+      ncell, reinterpret_cast<const int4 *>(pcell), x, q, adt, k);
+  c.count();
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- res_calc (atomics)
+
+template <typename T> __device__ __forceinline__ void red_add(T *p, T v) { atomicAdd(p, v); }
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_res_calc_atomic(int nedge, const int2 *__restrict__ pedge, const int2 *__restrict__ pecell,
+                  const T *__restrict__ x, const T *__restrict__ q,
+                  const T *__restrict__ adt, T *__restrict__ res, AirConst<T> k) {
+  int stride = gridDim.x * blockDim.x;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nedge; e += stride) {
+    int2 nn = __ldg(pedge + e);
+    int2 cc = __ldg(pecell + e);
+    T x1x, x1y, x2x, x2y, q1[4], q2[4], f[4];
+    Vec<T>::ld2(x + 2 * (size_t)nn.x, x1x, x1y);
+    Vec<T>::ld2(x + 2 * (size_t)nn.y, x2x, x2y);
+    Vec<T>::ld4(q + 4 * (size_t)cc.x, q1);
+    Vec<T>::ld4(q + 4 * (size_t)cc.y, q2);
+    T a1 = __ldg(adt + cc.x), a2 = __ldg(adt + cc.y);
+    air_flux<T>(x1x, x1y, x2x, x2y, q1, q2, a1, a2, k, f);
+    T *r1 = res + 4 * (size_t)cc.x, *r2 = res + 4 * (size_t)cc.y;
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+      red_add(r1 + m, f[m]);
+      red_add(r2 + m, -f[m]);
+    }
+  }
+}
+
+template <typename T>
+cudaError_t launch_res_calc_atomic(const LaunchCtx &c, int nedge, const int *pedge,
+                                   const int *pecell, const T *x, const T *q, const T *adt,
+                                   T *res, const AirConst<T> &k) {
+  if (nedge <= 0) return cudaSuccess;
+  k_res_calc_atomic<T><<<grid_for(c, nedge, 256, 8), 256, 0, c.stream>>>(
+      nedge, reinterpret_cast<const int2 *>(pedge), reinterpret_cast<const int2 *>(pecell), x,
+      q, adt, res, k);
+  c.count();
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- bres_calc (atomics)
+
+template <typename T>
+__global__ void __launch_bounds__(128)
+k_bres_calc_atomic(int nbedge, const int2 *__restrict__ pbedge, const int *__restrict__ pbecell,
+                   const int *__restrict__ bound, const T *__restrict__ x,
+                   const T *__restrict__ q, const T *__restrict__ adt, T *__restrict__ res,
+                   AirConst<T> k) {
+  int stride = gridDim.x * blockDim.x;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nbedge; e += stride) {
+    int2 nn = __ldg(pbedge + e);
+    int c1 = __ldg(pbecell + e);
+    int b = __ldg(bound + e);
+    T x1x, x1y, x2x, x2y, q1[4], r[4];
+    Vec<T>::ld2(x + 2 * (size_t)nn.x, x1x, x1y);
+    Vec<T>::ld2(x + 2 * (size_t)nn.y, x2x, x2y);
+    Vec<T>::ld4(q + 4 * (size_t)c1, q1);
+    air_bflux<T>(x1x, x1y, x2x, x2y, q1, __ldg(adt + c1), b, k, r);
+    T *r1 = res + 4 * (size_t)c1;
+    if (b == 1) {  // a wall edge leaves components 0 and 3 untouched
+      red_add(r1 + 1, r[1]);
+      red_add(r1 + 2, r[2]);
+    } else {
+#pragma unroll
+      for (int m = 0; m < 4; m++) red_add(r1 + m, r[m]);
+    }
+  }
+}
+
+template <typename T>
+cudaError_t launch_bres_calc_atomic(const LaunchCtx &c, int nbedge, const int *pbedge,
+                                    const int *pbecell, const int *bound, const T *x,
+                                    const T *q, const T *adt, T *res, const AirConst<T> &k) {
+  if (nbedge <= 0) return cudaSuccess;
+  k_bres_calc_atomic<T><<<grid_for(c, nbedge, 128, 8), 128, 0, c.stream>>>(
+      nbedge, reinterpret_cast<const int2 *>(pbedge), pbecell, bound, x, q, adt, res, k);
+  c.count();
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- update
+
+// (sum, max, argmax) triple; argmax keeps the lowest index among equal
+// maxima, which is the index op_seq.h's in-order "sqdel > maxerr" test
+// (update.h:13-16) ends with.
+struct RedTriple {
+  double sum, maxv;
+  long long idx;
+};
+
+__device__ __forceinline__ void red_merge(RedTriple &a, double s, double m, long long i) {
+  a.sum += s;
+  if (m > a.maxv || (m == a.maxv && i < a.idx)) {
+    a.maxv = m;
+    a.idx = i;
+  }
+}
+
+template <int THREADS>
+__device__ __forceinline__ RedTriple block_reduce(RedTriple t) {
+  __shared__ double s_sum[THREADS / 32], s_max[THREADS / 32];
+  __shared__ long long s_idx[THREADS / 32];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    double s = __shfl_down_sync(0xffffffffu, t.sum, off);
+    double m = __shfl_down_sync(0xffffffffu, t.maxv, off);
+    long long i = __shfl_down_sync(0xffffffffu, t.idx, off);
+    red_merge(t, s, m, i);
+  }
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+    s_sum[warp] = t.sum;
+    s_max[warp] = t.maxv;
+    s_idx[warp] = t.idx;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    RedTriple w{0.0, -INFINITY, LLONG_MAX};
+    if (lane < THREADS / 32) w = RedTriple{s_sum[lane], s_max[lane], s_idx[lane]};
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      double s = __shfl_down_sync(0xffffffffu, w.sum, off);
+      double m = __shfl_down_sync(0xffffffffu, w.maxv, off);
+      long long i = __shfl_down_sync(0xffffffffu, w.idx, off);
+      red_merge(w, s, m, i);
+    }
+    t = w;
+  }
+  return t;  // valid in thread 0
+}
+
+// One pass over the cells: q = qold - res/adt, res = 0, and the block's
+// partial (sum del^2, max del^2, first index of the max).  The last block to
+// arrive reduces all partials in block order and writes `out`.
+template <typename T, int THREADS>
+__global__ void __launch_bounds__(THREADS)
+k_update(int ncell, const T *__restrict__ qold, T *__restrict__ q, T *__restrict__ res,
+         const T *__restrict__ adt, RedSlot *__restrict__ parts, unsigned *__restrict__ counter,
+         RedSlot *__restrict__ out) {
+  RedTriple t{0.0, -INFINITY, LLONG_MAX};
+  int stride = gridDim.x * THREADS;
+  for (int n = blockIdx.x * THREADS + threadIdx.x; n < ncell; n += stride) {
+    T qo[4], r[4], qn[4];
+    Vec<T>::ld4(qold + 4 * (size_t)n, qo);
+    Vec<T>::ld4_rw(res + 4 * (size_t)n, r);
+    double adti = 1.0f / (double)__ldg(adt + n);
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+      double del = adti * (double)r[m];
+      qn[m] = (T)((double)qo[m] - del);
+      double sq = del * del;
+      t.sum += sq;
+      if (sq > t.maxv) {
+        t.maxv = sq;
+        t.idx = n;
+      }
+    }
+    Vec<T>::st4(q + 4 * (size_t)n, qn);
+    T z[4] = {(T)0, (T)0, (T)0, (T)0};
+    Vec<T>::st4(res + 4 * (size_t)n, z);
+  }
+  t = block_reduce<THREADS>(t);
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    parts[blockIdx.x] = RedSlot{t.sum, t.maxv, t.idx, 0};
+    __threadfence();
+    unsigned ticket = atomicAdd(counter, 1u);
+    last = (ticket == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  RedTriple a{0.0, -INFINITY, LLONG_MAX};
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += THREADS) {
+    const volatile RedSlot *p = parts + b;
+    red_merge(a, p->sum, p->maxv, p->idx);
+  }
+  a = block_reduce<THREADS>(a);
+  if (threadIdx.x == 0) {
+    *out = RedSlot{a.sum, a.maxv, a.idx, 0};
+    *counter = 0u;  // ready for the next launch (same stream, so ordered)
+  }
+}
+
+template <typename T>
+cudaError_t launch_update(const LaunchCtx &c, int ncell, const T *qold, T *q, T *res,
+                          const T *adt, const RedScratch &s) {
+  constexpr int TH = 256;
+  int grid = grid_for(c, ncell, TH, 4);
+  if (grid > s.capacity) grid = s.capacity;
+  k_update<T, TH><<<grid, TH, 0, c.stream>>>(ncell, qold, q, res, adt, s.parts, s.counter,
+                                             s.out);
+  c.count();
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- instantiations
+
+template cudaError_t launch_adt_calc<double>(const LaunchCtx &, int, const int *, const double *,
+                                             const double *, double *, const AirConst<double> &);
+template cudaError_t launch_adt_calc<float>(const LaunchCtx &, int, const int *, const float *,
+                                            const float *, float *, const AirConst<float> &);
+template cudaError_t launch_res_calc_atomic<double>(const LaunchCtx &, int, const int *,
+                                                    const int *, const double *, const double *,
+                                                    const double *, double *,
+                                                    const AirConst<double> &);
+template cudaError_t launch_res_calc_atomic<float>(const LaunchCtx &, int, const int *,
+                                                   const int *, const float *, const float *,
+                                                   const float *, float *,
+                                                   const AirConst<float> &);
+template cudaError_t launch_bres_calc_atomic<double>(const LaunchCtx &, int, const int *,
+                                                     const int *, const int *, const double *,
+                                                     const double *, const double *, double *,
+                                                     const AirConst<double> &);
+template cudaError_t launch_bres_calc_atomic<float>(const LaunchCtx &, int, const int *,
+                                                    const int *, const int *, const float *,
+                                                    const float *, const float *, float *,
+                                                    const AirConst<float> &);
+template cudaError_t launch_update<double>(const LaunchCtx &, int, const double *, double *,
+                                           double *, const double *, const RedScratch &);
+template cudaError_t launch_update<float>(const LaunchCtx &, int, const float *, float *,
+                                          float *, const float *, const RedScratch &);
+
+} // namespace op2b

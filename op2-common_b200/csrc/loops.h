@@ -1,0 +1,55 @@
+// Launch interface between the host runtime (op2b_core.cpp) and the device
+// loops (*.cu).  Internal to libop2b.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "airfoil_math.cuh"
+
+namespace op2b {
+
+// Where and how a launcher issues its kernels.
+struct LaunchCtx {
+  cudaStream_t stream;
+  int nsm;                 // SMs on the device (148 on B200)
+  long *launch_counter;    // incremented once per kernel launch
+  void count() const {
+    if (launch_counter) ++*launch_counter;
+  }
+};
+
+// One partial of the fused update reduction (32 bytes).
+struct RedSlot {
+  double sum;
+  double maxv;
+  long long idx;
+  long long pad;
+};
+
+// Device scratch of the update reduction: `capacity` partial slots, a ticket
+// counter (zero between launches) and the final slot.
+struct RedScratch {
+  RedSlot *parts;
+  unsigned *counter;
+  RedSlot *out;
+  int capacity;
+};
+
+cudaError_t launch_copy(const LaunchCtx &c, const void *src, void *dst, size_t bytes);
+
+template <typename T>
+cudaError_t launch_adt_calc(const LaunchCtx &c, int ncell, const int *pcell, const T *x,
+                            const T *q, T *adt, const AirConst<T> &k);
+template <typename T>
+cudaError_t launch_res_calc_atomic(const LaunchCtx &c, int nedge, const int *pedge,
+                                   const int *pecell, const T *x, const T *q, const T *adt,
+                                   T *res, const AirConst<T> &k);
+template <typename T>
+cudaError_t launch_bres_calc_atomic(const LaunchCtx &c, int nbedge, const int *pbedge,
+                                    const int *pbecell, const int *bound, const T *x,
+                                    const T *q, const T *adt, T *res, const AirConst<T> &k);
+template <typename T>
+cudaError_t launch_update(const LaunchCtx &c, int ncell, const T *qold, T *q, T *res,
+                          const T *adt, const RedScratch &s);
+
+}  // namespace op2b

@@ -1,0 +1,762 @@
+// Host runtime of libop2b: the OP2 C API (include/op2b.h) on one B200.
+//
+// Semantics follow the reference core (op2/src/core/op_lib_core.cpp):
+//  * op_decl_set/map/dat copy the caller's arrays (op_lib_core.cpp:420-576);
+//    the caller may free them afterwards.  Maps are range-checked on
+//    declaration (check_map, :146-164) and stored on the device AoS.
+//  * dats live only in device memory; op_fetch_data* copy them out.
+//  * op_par_loop runs the device loop registered under the loop's name after
+//    checking the argument list against that loop's signature (dats, dims,
+//    maps, indices, access modes); gbl reductions are written back into the
+//    caller's variables before the call returns, INC adding to the initial
+//    value and MAX keeping the larger (translator-v2/resources/templates/cpp/
+//    cuda/loop_host.hpp.jinja:405-415).
+//  * there is no host execution path: an unknown loop name, a signature
+//    mismatch or a CUDA error is reported through op2b_last_error() and, for
+//    the void-returning reference entry points, printed (and fatal when
+//    OP2B_ABORT_ON_ERROR / option "abort_on_error" is set).
+#include "op2b.h"
+#include "op2b_runtime.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace op2b {
+
+Runtime &rt() {
+  static Runtime r;
+  return r;
+}
+
+static thread_local std::string g_last_error;
+
+void set_error(const char *fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  if (rt().opt_diags > 0 || rt().opt_abort)
+    fprintf(stderr, "op2b error: %s\n", buf);
+  if (rt().opt_abort)
+    exit(1);
+}
+
+bool cuda_ok(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return true;
+  set_error("%s: CUDA error %d (%s)", what, (int)e, cudaGetErrorString(e));
+  return false;
+}
+
+static char *copy_str(const char *s) {
+  if (!s) s = "";
+  size_t n = strlen(s);
+  char *d = (char *)malloc(n + 1);
+  memcpy(d, s, n + 1);
+  return d;
+}
+
+int type_bytes(const char *type) {
+  if (!type) return 0;
+  std::string t(type);
+  size_t c = t.find(':');
+  if (c != std::string::npos) t = t.substr(0, c);
+  if (t == "double") return 8;
+  if (t == "float") return 4;
+  if (t == "int" || t == "uint") return 4;
+  if (t == "ll" || t == "ull" || t == "long") return 8;
+  if (t == "bool") return 1;
+  return 0;
+}
+
+bool is_real(const char *type, int bytes) {
+  if (!type) return false;
+  std::string t(type);
+  size_t c = t.find(':');
+  if (c != std::string::npos) t = t.substr(0, c);
+  return (bytes == 8 && t == "double") || (bytes == 4 && t == "float");
+}
+
+LaunchCtx Runtime::ctx() { return LaunchCtx{stream, nsm, &launches}; }
+
+bool Runtime::ready() {
+  if (!initialised) {
+    set_error("op_init has not been called");
+    return false;
+  }
+  return true;
+}
+
+// ------------------------------------------------------------------ timing
+
+void Runtime::begin_loop(const char *name) {
+  cur_loop = name;
+  if (!opt_timing) return;
+  if (ev_free.size() < 2) {
+    for (int i = 0; i < 64; i++) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) == cudaSuccess) ev_free.push_back(e);
+    }
+  }
+  cur_ev0 = ev_free.back();
+  ev_free.pop_back();
+  cur_ev1 = ev_free.back();
+  ev_free.pop_back();
+  cudaEventRecord(cur_ev0, stream);
+}
+
+void Runtime::end_loop(double bytes) {
+  LoopStat &s = stats[cur_loop];
+  s.calls++;
+  s.bytes_per_call = bytes;
+  if (!opt_timing) return;
+  cudaEventRecord(cur_ev1, stream);
+  pending.push_back(PendingTime{cur_loop, cur_ev0, cur_ev1});
+  if (pending.size() > 4096) resolve_timing();
+}
+
+void Runtime::resolve_timing() {
+  if (pending.empty()) return;
+  cudaStreamSynchronize(stream);
+  for (auto &p : pending) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, p.e0, p.e1) == cudaSuccess) {
+      LoopStat &s = stats[p.name];
+      s.total_ms += ms;
+      s.last_ms = ms;
+      s.timed++;
+    }
+    ev_free.push_back(p.e0);
+    ev_free.push_back(p.e1);
+  }
+  pending.clear();
+}
+
+const double *Runtime::const_ptr(const char *name, int dim) {
+  auto it = consts.find(name);
+  if (it == consts.end() || (int)it->second.size() < dim) {
+    set_error("constant '%s' (dim %d) was not declared with op_decl_const", name, dim);
+    return nullptr;
+  }
+  return it->second.data();
+}
+
+}  // namespace op2b
+
+using namespace op2b;
+
+// ====================================================================== C API
+
+extern "C" {
+
+const char *op2b_last_error(void) { return g_last_error.c_str(); }
+
+int op2b_status(void) { return rt().initialised ? 0 : -1; }
+
+static void parse_args(int argc, char **argv) {
+  Runtime &r = rt();
+  for (int i = 0; i < argc; i++) {
+    if (!argv || !argv[i]) continue;
+    const char *a = argv[i];
+    const char *p;
+    if ((p = strstr(a, "OP_BLOCK_SIZE="))) r.opt_block_size = atoi(p + 14);
+    if ((p = strstr(a, "OP_PART_SIZE="))) r.opt_part_size = atoi(p + 13);
+    if ((p = strstr(a, "OP_CACHE_LINE_SIZE="))) r.opt_cache_line = atoi(p + 19);
+    if ((p = strstr(a, "OP_MAPS_BASE_INDEX="))) {
+      int v = atoi(p + 19);
+      if (v == 0 || v == 1) r.opt_maps_base = v;
+    }
+  }
+}
+
+void op_init(int argc, char **argv, int diags) {
+  Runtime &r = rt();
+  if (r.initialised) return;
+  r.opt_diags = diags;
+  if (const char *e = getenv("OP2B_ABORT_ON_ERROR")) r.opt_abort = atoi(e) != 0;
+  if (const char *e = getenv("OP2B_INC_MODE")) r.opt_inc_mode = atoi(e);
+  parse_args(argc, argv);
+  int dev = 0;
+  if (const char *e = getenv("OP2B_DEVICE")) dev = atoi(e);
+  if (!cuda_ok(cudaSetDevice(dev), "op_init: cudaSetDevice")) return;
+  cudaDeviceProp prop;
+  if (!cuda_ok(cudaGetDeviceProperties(&prop, dev), "op_init: cudaGetDeviceProperties")) return;
+  r.device = dev;
+  r.nsm = prop.multiProcessorCount;
+  r.cc_major = prop.major;
+  r.cc_minor = prop.minor;
+  if (r.cc_major != 10) {
+    set_error("op_init: device %d is sm_%d%d; libop2b is built for sm_100a (B200) only", dev,
+              r.cc_major, r.cc_minor);
+    return;
+  }
+  if (!cuda_ok(cudaStreamCreateWithFlags(&r.own_stream, cudaStreamNonBlocking),
+               "op_init: stream"))
+    return;
+  r.stream = r.own_stream;
+  // update-reduction scratch: partial slots + ticket + final slot
+  r.red.capacity = 8192;
+  void *p = nullptr;
+  size_t bytes = sizeof(RedSlot) * (size_t)(r.red.capacity + 1) + 256;
+  if (!cuda_ok(cudaMalloc(&p, bytes), "op_init: reduction scratch")) return;
+  cudaMemset(p, 0, bytes);
+  r.red_base = p;
+  r.red.parts = reinterpret_cast<RedSlot *>(p);
+  r.red.out = r.red.parts + r.red.capacity;
+  r.red.counter = reinterpret_cast<unsigned *>(reinterpret_cast<char *>(r.red.out + 1));
+  if (!cuda_ok(cudaMallocHost(&r.pinned, 4096), "op_init: pinned buffer")) return;
+  r.initialised = true;
+  if (diags > 1)
+    printf(" op2b: device %d (%s, %d SMs), stream %p\n", dev, prop.name, r.nsm,
+           (void *)r.stream);
+}
+
+void op_exit(void) {
+  Runtime &r = rt();
+  if (!r.initialised) return;
+  cudaStreamSynchronize(r.stream);
+  release_plans();
+  for (auto &d : r.dats)
+    if (d) {
+      cudaFree(d->data_d);
+      free((void *)d->name);
+      free((void *)d->type);
+      free(d->data);
+    }
+  for (auto &m : r.maps)
+    if (m) {
+      cudaFree(m->map_d);
+      free(m->map);
+      free((void *)m->name);
+    }
+  for (auto &s : r.sets)
+    if (s) free((void *)s->name);
+  r.dats.clear();
+  r.maps.clear();
+  r.sets.clear();
+  r.consts.clear();
+  for (auto &p : r.pending) {
+    cudaEventDestroy(p.e0);
+    cudaEventDestroy(p.e1);
+  }
+  r.pending.clear();
+  for (auto e : r.ev_free) cudaEventDestroy(e);
+  r.ev_free.clear();
+  cudaFree(r.red_base);
+  cudaFreeHost(r.pinned);
+  cudaStreamDestroy(r.own_stream);
+  r.red_base = nullptr;
+  r.pinned = nullptr;
+  r.stream = r.own_stream = nullptr;
+  r.stats.clear();
+  r.launches = 0;
+  r.initialised = false;
+}
+
+op_set op_decl_set(int size, char const *name) {
+  if (!rt().ready()) return nullptr;
+  if (size < 0) {
+    set_error("op_decl_set: negative size for set %s", name ? name : "");
+    return nullptr;
+  }
+  auto s = std::make_unique<op_set_core>();
+  s->index = (int)rt().sets.size();
+  s->size = size;
+  s->name = copy_str(name);
+  s->core_size = size;
+  s->exec_size = 0;
+  s->nonexec_size = 0;
+  rt().sets.push_back(std::move(s));
+  return rt().sets.back().get();
+}
+
+op_map op_decl_map(op_set from, op_set to, int dim, int *imap, char const *name) {
+  Runtime &r = rt();
+  if (!r.ready()) return nullptr;
+  if (!from || !to) {
+    set_error("op_decl_map: invalid 'from'/'to' set for map %s", name ? name : "");
+    return nullptr;
+  }
+  if (dim <= 0) {
+    set_error("op_decl_map: non-positive dimension for map %s", name ? name : "");
+    return nullptr;
+  }
+  size_t n = (size_t)from->size * (size_t)dim;
+  if (n > 0 && !imap) {
+    set_error("op_decl_map: NULL data for map %s", name ? name : "");
+    return nullptr;
+  }
+  int *h = (int *)malloc(sizeof(int) * (n ? n : 1));
+  for (size_t i = 0; i < n; i++) {
+    int v = imap[i] - r.opt_maps_base;
+    if (v < 0 || v >= to->size) {
+      free(h);
+      set_error("op_decl_map: invalid data for map %s: element %zu, dimension %zu, value %d "
+                "outside [0, %d)",
+                name ? name : "", i / dim, i % dim, imap[i], to->size);
+      return nullptr;
+    }
+    h[i] = v;
+  }
+  auto m = std::make_unique<op_map_core>();
+  m->index = (int)r.maps.size();
+  m->from = from;
+  m->to = to;
+  m->dim = dim;
+  m->map = h;
+  m->map_d = nullptr;
+  m->name = copy_str(name);
+  if (n > 0) {
+    if (!cuda_ok(cudaMalloc((void **)&m->map_d, n * sizeof(int)), "op_decl_map: cudaMalloc") ||
+        !cuda_ok(cudaMemcpy(m->map_d, h, n * sizeof(int), cudaMemcpyHostToDevice),
+                 "op_decl_map: upload")) {
+      free(h);
+      cudaFree(m->map_d);
+      return nullptr;
+    }
+  }
+  r.maps.push_back(std::move(m));
+  return r.maps.back().get();
+}
+
+op_dat op_decl_dat_char(op_set set, int dim, char const *type, int type_size, char *data,
+                        char const *name) {
+  Runtime &r = rt();
+  if (!r.ready()) return nullptr;
+  if (!set) {
+    set_error("op_decl_dat: invalid set for data %s", name ? name : "");
+    return nullptr;
+  }
+  if (dim <= 0 || type_size <= 0) {
+    set_error("op_decl_dat: non-positive dimension or type size for data %s",
+              name ? name : "");
+    return nullptr;
+  }
+  int tb = type_bytes(type);
+  if (tb != 0 && tb != type_size) {
+    set_error("op_decl_dat: type '%s' does not have size %d (data %s)", type, type_size,
+              name ? name : "");
+    return nullptr;
+  }
+  auto d = std::make_unique<op_dat_core>();
+  d->index = (int)r.dats.size();
+  d->set = set;
+  d->dim = dim;
+  d->size = dim * type_size;
+  d->data = nullptr;
+  d->data_d = nullptr;
+  d->type = copy_str(type);
+  d->name = copy_str(name);
+  size_t bytes = (size_t)set->size * (size_t)d->size;
+  if (bytes > 0) {
+    // 256-byte aligned allocation rounded up to 32 bytes so every element
+    // record and 16/32-byte vector access stays in bounds
+    size_t alloc = (bytes + 255) & ~(size_t)255;
+    if (!cuda_ok(cudaMalloc((void **)&d->data_d, alloc), "op_decl_dat: cudaMalloc")) return nullptr;
+    cudaError_t e = data ? cudaMemcpyAsync(d->data_d, data, bytes, cudaMemcpyHostToDevice, r.stream)
+                         : cudaMemsetAsync(d->data_d, 0, alloc, r.stream);
+    if (!cuda_ok(e, "op_decl_dat: upload") ||
+        !cuda_ok(cudaStreamSynchronize(r.stream), "op_decl_dat: upload")) {
+      cudaFree(d->data_d);
+      return nullptr;
+    }
+  }
+  r.dats.push_back(std::move(d));
+  return r.dats.back().get();
+}
+
+op_dat op_decl_dat_temp_char(op_set set, int dim, char const *type, int type_size,
+                             char const *name) {
+  return op_decl_dat_char(set, dim, type, type_size, nullptr, name);
+}
+
+int op_free_dat_temp_char(op_dat dat) {
+  Runtime &r = rt();
+  for (auto &d : r.dats)
+    if (d.get() == dat) {
+      cudaStreamSynchronize(r.stream);
+      cudaFree(d->data_d);
+      free((void *)d->name);
+      free((void *)d->type);
+      free(d->data);
+      d.reset();
+      return 0;
+    }
+  set_error("op_free_dat_temp: unknown dat");
+  return -1;
+}
+
+void op_decl_const_char(int dim, char const *type, int type_size, char *dat, char const *name) {
+  Runtime &r = rt();
+  if (!name || !dat || dim <= 0) {
+    set_error("op_decl_const: needs a name, data and a positive dimension");
+    return;
+  }
+  std::vector<double> v((size_t)dim);
+  std::string t = type ? type : "";
+  for (int i = 0; i < dim; i++) {
+    if (t == "double" && type_size == 8)
+      v[i] = reinterpret_cast<double *>(dat)[i];
+    else if (t == "float" && type_size == 4)
+      v[i] = reinterpret_cast<float *>(dat)[i];
+    else if (t == "int" && type_size == 4)
+      v[i] = reinterpret_cast<int *>(dat)[i];
+    else {
+      set_error("op_decl_const: unsupported type '%s' for constant %s", type ? type : "", name);
+      return;
+    }
+  }
+  std::string n(name);
+  while (!n.empty() && (n[0] == '&' || n[0] == ' ')) n.erase(0, 1);
+  r.consts[n] = v;
+}
+
+// ------------------------------------------------------------------ op_arg
+
+static op_arg blank_arg() {
+  op_arg a;
+  memset(&a, 0, sizeof(a));
+  a.idx = -1;
+  a.opt = 1;
+  return a;
+}
+
+op_arg op_arg_dat(op_dat dat, int idx, op_map map, int dim, char const *type, op_access acc) {
+  op_arg a = blank_arg();
+  a.argtype = OP_ARG_DAT;
+  a.dat = dat;
+  a.map = map;
+  a.dim = dim;
+  a.idx = idx;
+  a.type = type;
+  a.acc = acc;
+  if (dat) {
+    a.size = dat->size;
+    a.data = dat->data;
+    a.data_d = dat->data_d;
+  }
+  if (map) {
+    a.map_data = map->map;
+    a.map_data_d = map->map_d;
+  }
+  return a;
+}
+
+op_arg op_opt_arg_dat(int opt, op_dat dat, int idx, op_map map, int dim, char const *type,
+                      op_access acc) {
+  op_arg a = op_arg_dat(dat, idx, map, dim, type, acc);
+  a.opt = opt;
+  return a;
+}
+
+op_arg op_arg_gbl_char(char *data, int dim, const char *type, int type_size, op_access acc) {
+  op_arg a = blank_arg();
+  a.argtype = OP_ARG_GBL;
+  a.data = data;
+  a.dim = dim;
+  a.size = dim * type_size;
+  a.type = type;
+  a.acc = acc;
+  return a;
+}
+
+op_arg op_opt_arg_gbl_char(int opt, char *data, int dim, const char *type, int type_size,
+                           op_access acc) {
+  op_arg a = op_arg_gbl_char(data, dim, type, type_size, acc);
+  a.opt = opt;
+  return a;
+}
+
+// op_arg_info_char (op_lib_core.cpp:973-1015): payload written at the
+// winning element of the MIN/MAX argument `ref`.
+op_arg op_arg_info_char(char *data, int dim, const char *type, int type_size, int ref) {
+  op_arg a = blank_arg();
+  a.argtype = OP_ARG_INFO;
+  a.data = data;
+  a.dim = dim;
+  a.size = dim * type_size;
+  a.type = type;
+  a.acc = ref;  // the reference keeps the referenced argument's position here too
+  a.idx = ref;
+  return a;
+}
+
+op_arg op_arg_idx(int idx, op_map map) {
+  op_arg a = blank_arg();
+  a.argtype = OP_ARG_IDX;
+  a.idx = idx;
+  a.map = map;
+  a.acc = OP_READ;
+  a.type = "int";
+  a.size = sizeof(int);
+  return a;
+}
+
+// ------------------------------------------------------------------ data out
+
+static bool fetch_range(op_dat dat, char *dst, size_t first, size_t count) {
+  Runtime &r = rt();
+  if (!r.ready()) return false;
+  if (!dat || !dat->data_d) {
+    if (dat && count == 0) return true;
+    set_error("op_fetch_data: invalid dat");
+    return false;
+  }
+  resolve_renumbering_for_fetch(dat);
+  size_t bytes = count * (size_t)dat->size;
+  cudaError_t e = cudaMemcpyAsync(dst, dat->data_d + first * dat->size, bytes,
+                                  cudaMemcpyDeviceToHost, r.stream);
+  if (!cuda_ok(e, "op_fetch_data")) return false;
+  return cuda_ok(cudaStreamSynchronize(r.stream), "op_fetch_data");
+}
+
+void op_fetch_data_char(op_dat dat, char *usr_ptr) {
+  if (!dat) {
+    set_error("op_fetch_data: NULL dat");
+    return;
+  }
+  fetch_range(dat, usr_ptr, 0, (size_t)dat->set->size);
+}
+
+// op_fetch_data_idx_char: elements low..high (inclusive) in the order the
+// application declared them, i.e. with any renumbering undone.
+void op_fetch_data_idx_char(op_dat dat, char *usr_ptr, int low, int high) {
+  if (!dat || low < 0 || high >= dat->set->size || low > high + 1) {
+    set_error("op_fetch_data_idx: invalid dat or range [%d, %d]", low, high);
+    return;
+  }
+  fetch_original_order(dat, usr_ptr, low, high);
+}
+
+static std::vector<char> host_copy(op_dat dat) {
+  std::vector<char> buf((size_t)dat->set->size * (size_t)dat->size);
+  if (!buf.empty()) fetch_original_order(dat, buf.data(), 0, dat->set->size - 1);
+  return buf;
+}
+
+// op_print_dat_to_binfile_core (op_lib_core.cpp:1283-1307): int count,
+// int dim, then the raw AoS elements.
+void op_print_dat_to_binfile(op_dat dat, const char *file_name) {
+  if (!dat) return;
+  std::vector<char> buf = host_copy(dat);
+  FILE *fp = fopen(file_name, "wb");
+  if (!fp) {
+    set_error("op_print_dat_to_binfile: cannot open %s", file_name);
+    return;
+  }
+  int count = dat->set->size, dim = dat->dim;
+  fwrite(&count, sizeof(int), 1, fp);
+  fwrite(&dim, sizeof(int), 1, fp);
+  if (!buf.empty()) fwrite(buf.data(), 1, buf.size(), fp);
+  fclose(fp);
+}
+
+// op_print_dat_to_txtfile_core (op_lib_core.cpp:1309-1370): "size dim" then
+// one line per element, " %+2.15lE" per double (-0.0 printed as +0.0),
+// " %+f" per float, " %+d" per int.
+void op_print_dat_to_txtfile(op_dat dat, const char *file_name) {
+  if (!dat) return;
+  std::vector<char> buf = host_copy(dat);
+  FILE *fp = fopen(file_name, "w");
+  if (!fp) {
+    set_error("op_print_dat_to_txtfile: cannot open %s", file_name);
+    return;
+  }
+  fprintf(fp, "%d %d\n", dat->set->size, dat->dim);
+  int tb = type_bytes(dat->type);
+  std::string t(dat->type);
+  if (t.find(':') != std::string::npos) t = t.substr(0, t.find(':'));
+  for (int i = 0; i < dat->set->size; i++) {
+    for (int j = 0; j < dat->dim; j++) {
+      size_t k = (size_t)i * dat->dim + j;
+      if (t == "double" && tb == 8) {
+        double v = reinterpret_cast<double *>(buf.data())[k];
+        if (v == -0.0) v = +0.0;
+        fprintf(fp, " %+2.15lE", v);
+      } else if (t == "float") {
+        fprintf(fp, " %+f", reinterpret_cast<float *>(buf.data())[k]);
+      } else if (t == "int") {
+        fprintf(fp, " %+d", reinterpret_cast<int *>(buf.data())[k]);
+      } else {
+        fclose(fp);
+        set_error("op_print_dat_to_txtfile: unknown type %s", dat->type);
+        return;
+      }
+    }
+    fprintf(fp, "\n");
+  }
+  fclose(fp);
+}
+
+// ------------------------------------------------------------------ misc
+
+int op_get_size(op_set set) { return set ? set->size : 0; }
+
+void op_rank(int *rank) {
+  if (rank) *rank = 0;
+}
+
+void op_timers(double *cpu, double *et) {
+  using namespace std::chrono;
+  double t = duration<double>(steady_clock::now().time_since_epoch()).count();
+  if (cpu) *cpu = (double)clock() / CLOCKS_PER_SEC;
+  if (et) *et = t;
+}
+
+void op_diagnostic_output(void) {
+  Runtime &r = rt();
+  if (r.opt_diags <= 1) return;
+  printf("\n  OP diagnostic output\n  --------------------\n\n       set       size\n"
+         "  -------------------\n");
+  for (auto &s : r.sets)
+    if (s) printf("%10s %10d\n", s->name, s->size);
+  printf("\n       map        dim       from         to\n  ------------------------------\n");
+  for (auto &m : r.maps)
+    if (m) printf("%10s %10d %10s %10s\n", m->name, m->dim, m->from->name, m->to->name);
+  printf("\n       dat        dim        set\n  ------------------------------\n");
+  for (auto &d : r.dats)
+    if (d) printf("%10s %10d %10s\n", d->name, d->dim, d->set->name);
+  printf("\n");
+}
+
+// op_timing_output_core (op_lib_core.cpp:1096-1167): count, plan time, device
+// time and GB/s per loop, sorted by time.  Times are CUDA-event device times;
+// GB/s uses each loop's algorithmic bytes per call.
+void op_timing_output(void) {
+  Runtime &r = rt();
+  r.resolve_timing();
+  std::vector<std::pair<std::string, LoopStat>> v(r.stats.begin(), r.stats.end());
+  std::sort(v.begin(), v.end(),
+            [](auto &a, auto &b) { return a.second.total_ms > b.second.total_ms; });
+  printf("\n  count   plan time     device time      GB/s   kernel name\n"
+         " -----------------------------------------------------------\n");
+  for (auto &kv : v) {
+    const LoopStat &s = kv.second;
+    double sec = s.total_ms * 1e-3;
+    double gbs = sec > 0 ? s.bytes_per_call * (double)s.timed / sec * 1e-9 : 0.0;
+    printf(" %6ld;  %8.4f;  %12.6f;  %8.2f;   %s\n", s.calls, s.plan_ms * 1e-3, sec, gbs,
+           kv.first.c_str());
+  }
+}
+
+// ------------------------------------------------------------------ extensions
+
+int op2b_dat_upload(op_dat dat, const char *src, size_t bytes) {
+  Runtime &r = rt();
+  if (!r.ready()) return -1;
+  if (!dat || !src || bytes != (size_t)dat->set->size * (size_t)dat->size) {
+    set_error("op2b_dat_upload: invalid dat or size");
+    return -1;
+  }
+  if (bytes == 0) return 0;
+  if (!cuda_ok(cudaMemcpyAsync(dat->data_d, src, bytes, cudaMemcpyHostToDevice, r.stream),
+               "op2b_dat_upload"))
+    return -1;
+  return cuda_ok(cudaStreamSynchronize(r.stream), "op2b_dat_upload") ? 0 : -1;
+}
+
+void *op2b_dat_device_ptr(op_dat dat) { return dat ? dat->data_d : nullptr; }
+void *op2b_map_device_ptr(op_map map) { return map ? map->map_d : nullptr; }
+
+int op2b_set_option(const char *key, long value) {
+  Runtime &r = rt();
+  std::string k = key ? key : "";
+  if (k == "inc_mode") {
+    if (value < 0 || value > 2) {
+      set_error("op2b_set_option: inc_mode must be 0, 1 or 2");
+      return -1;
+    }
+    r.opt_inc_mode = (int)value;
+  } else if (k == "timing") {
+    r.opt_timing = value != 0;
+  } else if (k == "diags") {
+    r.opt_diags = (int)value;
+  } else if (k == "abort_on_error") {
+    r.opt_abort = value != 0;
+  } else if (k == "part_size") {
+    r.opt_part_size = (int)value;
+  } else if (k == "block_size") {
+    r.opt_block_size = (int)value;
+  } else if (k == "plan_mode") {
+    r.opt_plan_mode = (int)value;
+  } else if (k == "check_plans") {
+    r.opt_check_plans = value != 0;
+  } else {
+    set_error("op2b_set_option: unknown option '%s'", k.c_str());
+    return -1;
+  }
+  return 0;
+}
+
+long op2b_get_option(const char *key) {
+  Runtime &r = rt();
+  std::string k = key ? key : "";
+  if (k == "inc_mode") return r.opt_inc_mode;
+  if (k == "timing") return r.opt_timing;
+  if (k == "diags") return r.opt_diags;
+  if (k == "abort_on_error") return r.opt_abort;
+  if (k == "part_size") return r.opt_part_size;
+  if (k == "block_size") return r.opt_block_size;
+  if (k == "plan_mode") return r.opt_plan_mode;
+  if (k == "check_plans") return r.opt_check_plans;
+  if (k == "nsm") return r.nsm;
+  return -1;
+}
+
+int op2b_loop_stats(const char *name, double *total_ms, long *calls, double *bytes_per_call,
+                    double *last_ms) {
+  Runtime &r = rt();
+  r.resolve_timing();
+  auto it = r.stats.find(name ? name : "");
+  if (it == r.stats.end()) return -1;
+  if (total_ms) *total_ms = it->second.total_ms;
+  if (calls) *calls = it->second.calls;
+  if (bytes_per_call) *bytes_per_call = it->second.bytes_per_call;
+  if (last_ms) *last_ms = it->second.last_ms;
+  return 0;
+}
+
+void op2b_reset_stats(void) {
+  Runtime &r = rt();
+  r.resolve_timing();
+  for (auto &kv : r.stats) {
+    double plan = kv.second.plan_ms;
+    kv.second = LoopStat();
+    kv.second.plan_ms = plan;
+  }
+}
+
+long op2b_kernel_launches(void) { return rt().launches; }
+
+int op2b_set_stream(void *stream) {
+  Runtime &r = rt();
+  if (!r.ready()) return -1;
+  cudaStreamSynchronize(r.stream);
+  r.stream = stream ? (cudaStream_t)stream : r.own_stream;
+  return 0;
+}
+
+void *op2b_get_stream(void) { return (void *)rt().stream; }
+
+int op2b_synchronize(void) {
+  Runtime &r = rt();
+  if (!r.ready()) return -1;
+  cudaError_t e = cudaStreamSynchronize(r.stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) cuda_ok(e, "op2b_synchronize");
+  return (int)e;
+}
+
+}  // extern "C"

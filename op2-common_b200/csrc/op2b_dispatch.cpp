@@ -1,0 +1,394 @@
+// op_par_loop dispatch: a loop is identified by its name and must match the
+// argument signature of the device loop registered under that name.  The
+// signatures are those of the Airfoil calls in
+// apps/c/airfoil/airfoil_plain/dp/airfoil.cpp:225-277 (and the rms-only
+// update of apps/c/airfoil/airfoil_tempdats/dp/airfoil.cpp); a dat of type
+// "double" selects the FP64 kernels, "float" the FP32-storage kernels of the
+// mixed-precision form.  Anything else is an error -- there is no host
+// execution path.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "op2b_runtime.h"
+#include "staged.h"
+
+using namespace op2b;
+
+namespace {
+
+const char *acc_name(int a) {
+  static const char *n[] = {"OP_READ", "OP_WRITE", "OP_RW", "OP_INC", "OP_MIN", "OP_MAX",
+                            "OP_WORK"};
+  return (a >= 0 && a <= 6) ? n[a] : "?";
+}
+
+struct Sig {
+  const char *loop;
+  op_set set;
+  op_arg *a;
+  int nargs;
+  bool ok = true;
+
+  bool fail(int i, const char *what) {
+    if (ok) set_error("op_par_loop(%s): argument %d: %s", loop, i, what);
+    ok = false;
+    return false;
+  }
+  // a dat argument with the given dimension, access, map (NULL = direct) and index
+  bool dat(int i, int dim, int acc, op_map map, int idx) {
+    if (!ok) return false;
+    if (i >= nargs) return fail(i, "missing");
+    const op_arg &x = a[i];
+    char buf[256];
+    if (x.argtype != OP_ARG_DAT || !x.dat) return fail(i, "expected an op_arg_dat");
+    if (!x.opt) return fail(i, "optional argument switched off; this loop needs it");
+    if (x.dat->dim != dim || x.dim != dim) {
+      snprintf(buf, sizeof(buf), "expected dim %d, got dat dim %d / arg dim %d", dim,
+               x.dat->dim, x.dim);
+      return fail(i, buf);
+    }
+    if (x.acc != acc) {
+      snprintf(buf, sizeof(buf), "expected %s, got %s", acc_name(acc), acc_name(x.acc));
+      return fail(i, buf);
+    }
+    if (x.type && x.dat->type && type_bytes(x.type) != type_bytes(x.dat->type)) {
+      snprintf(buf, sizeof(buf), "type '%s' does not match dat type '%s'", x.type, x.dat->type);
+      return fail(i, buf);
+    }
+    if (map == nullptr) {
+      if (x.map != nullptr || x.idx != -1) return fail(i, "expected a direct (OP_ID) argument");
+      if (x.dat->set != set) return fail(i, "dat is not defined on the loop's set");
+    } else {
+      if (x.map != map) return fail(i, "expected the same map as the loop's other arguments");
+      if (x.idx != idx) {
+        snprintf(buf, sizeof(buf), "expected map index %d, got %d", idx, x.idx);
+        return fail(i, buf);
+      }
+      if (map->from != set) return fail(i, "map does not start from the loop's set");
+      if (map->to != x.dat->set) return fail(i, "map does not point to the dat's set");
+    }
+    return true;
+  }
+  bool gbl(int i, int dim, int acc, int bytes) {
+    if (!ok) return false;
+    if (i >= nargs) return fail(i, "missing");
+    const op_arg &x = a[i];
+    if (x.argtype != OP_ARG_GBL) return fail(i, "expected an op_arg_gbl");
+    if (x.dim != dim || x.size != dim * bytes || x.acc != acc || !x.data)
+      return fail(i, "global argument of the wrong dimension, type or access");
+    return true;
+  }
+  int real_bytes(std::initializer_list<int> idx) {
+    int b = 0;
+    for (int i : idx) {
+      if (!ok) return 0;
+      const op_arg &x = a[i];
+      int tb = type_bytes(x.dat->type);
+      if (!is_real(x.dat->type, tb)) {
+        fail(i, "dat must be of type double or float");
+        return 0;
+      }
+      if (b && tb != b) {
+        fail(i, "all real dats of this loop must have the same precision");
+        return 0;
+      }
+      b = tb;
+    }
+    return b;
+  }
+};
+
+template <typename T> AirConst<T> air_consts(bool &ok) {
+  AirConst<T> k{};
+  Runtime &r = rt();
+  const double *gam = r.const_ptr("gam", 1), *gm1 = r.const_ptr("gm1", 1),
+               *cfl = r.const_ptr("cfl", 1), *eps = r.const_ptr("eps", 1),
+               *qinf = r.const_ptr("qinf", 4);
+  ok = gam && gm1 && cfl && eps && qinf;
+  if (!ok) return k;
+  k.gam = (T)*gam;
+  k.gm1 = (T)*gm1;
+  k.cfl = (T)*cfl;
+  k.eps = (T)*eps;
+  for (int i = 0; i < 4; i++) k.qinf[i] = (T)qinf[i];
+  return k;
+}
+
+int finish(cudaError_t e, const char *loop) {
+  if (e != cudaSuccess) {
+    set_error("op_par_loop(%s): kernel launch failed: %s", loop, cudaGetErrorString(e));
+    return -1;
+  }
+  return 0;
+}
+
+// ---------------------------------------------------------------- save_soln
+int loop_save_soln(const char *name, op_set set, int nargs, op_arg *a) {
+  Sig s{name, set, a, nargs};
+  if (nargs != 2) return s.fail(nargs, "save_soln takes 2 arguments"), -1;
+  int dim = a[0].dat ? a[0].dat->dim : 0;
+  s.dat(0, dim, OP_READ, nullptr, -1);
+  s.dat(1, dim, OP_WRITE, nullptr, -1);
+  if (!s.ok) return -1;
+  if (a[0].dat->size != a[1].dat->size) return s.fail(1, "element size differs from argument 0"), -1;
+  Runtime &r = rt();
+  size_t bytes = (size_t)set->size * (size_t)a[0].dat->size;
+  r.begin_loop(name);
+  cudaError_t e = launch_copy(r.ctx(), a[0].dat->data_d, a[1].dat->data_d, bytes);
+  r.end_loop(2.0 * (double)bytes);
+  return finish(e, name);
+}
+
+// ---------------------------------------------------------------- adt_calc
+int loop_adt_calc(const char *name, op_set set, int nargs, op_arg *a) {
+  Sig s{name, set, a, nargs};
+  if (nargs != 6) return s.fail(nargs, "adt_calc takes 6 arguments"), -1;
+  op_map pcell = a[0].map;
+  if (!pcell || pcell->dim != 4) return s.fail(0, "expected a dim-4 map (cells -> nodes)"), -1;
+  for (int i = 0; i < 4; i++) s.dat(i, 2, OP_READ, pcell, i);
+  if (s.ok && (a[1].dat != a[0].dat || a[2].dat != a[0].dat || a[3].dat != a[0].dat))
+    return s.fail(1, "arguments 0-3 must be the same dat"), -1;
+  s.dat(4, 4, OP_READ, nullptr, -1);
+  s.dat(5, 1, OP_WRITE, nullptr, -1);
+  int rb = s.real_bytes({0, 4, 5});
+  if (!s.ok) return -1;
+  Runtime &r = rt();
+  int C = set->size, N = a[0].dat->set->size;
+  double bytes = 16.0 * C + (double)rb * (2.0 * N + 5.0 * C);
+  r.begin_loop(name);
+  cudaError_t e;
+  bool ok;
+  if (rb == 8) {
+    AirConst<double> k = air_consts<double>(ok);
+    if (!ok) return -1;
+    e = launch_adt_calc<double>(r.ctx(), C, pcell->map_d, (const double *)a[0].dat->data_d,
+                                (const double *)a[4].dat->data_d, (double *)a[5].dat->data_d, k);
+  } else {
+    AirConst<float> k = air_consts<float>(ok);
+    if (!ok) return -1;
+    e = launch_adt_calc<float>(r.ctx(), C, pcell->map_d, (const float *)a[0].dat->data_d,
+                               (const float *)a[4].dat->data_d, (float *)a[5].dat->data_d, k);
+  }
+  r.end_loop(bytes);
+  return finish(e, name);
+}
+
+// ---------------------------------------------------------------- res_calc
+int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
+  Sig s{name, set, a, nargs};
+  if (nargs != 8) return s.fail(nargs, "res_calc takes 8 arguments"), -1;
+  op_map pedge = a[0].map, pecell = a[2].map;
+  if (!pedge || pedge->dim != 2) return s.fail(0, "expected a dim-2 map (edges -> nodes)"), -1;
+  if (!pecell || pecell->dim != 2) return s.fail(2, "expected a dim-2 map (edges -> cells)"), -1;
+  s.dat(0, 2, OP_READ, pedge, 0);
+  s.dat(1, 2, OP_READ, pedge, 1);
+  s.dat(2, 4, OP_READ, pecell, 0);
+  s.dat(3, 4, OP_READ, pecell, 1);
+  s.dat(4, 1, OP_READ, pecell, 0);
+  s.dat(5, 1, OP_READ, pecell, 1);
+  s.dat(6, 4, OP_INC, pecell, 0);
+  s.dat(7, 4, OP_INC, pecell, 1);
+  if (s.ok && (a[1].dat != a[0].dat || a[3].dat != a[2].dat || a[5].dat != a[4].dat ||
+               a[7].dat != a[6].dat))
+    return s.fail(1, "paired arguments must name the same dat"), -1;
+  int rb = s.real_bytes({0, 2, 4, 6});
+  if (!s.ok) return -1;
+  Runtime &r = rt();
+  int E = set->size, N = a[0].dat->set->size, C = a[2].dat->set->size;
+  double bytes = 16.0 * E + (double)rb * (2.0 * N + 13.0 * C);
+  ResCalcArgs<double> d{};
+  bool ok;
+  cudaError_t e;
+  if (rb == 8) {
+    AirConst<double> k = air_consts<double>(ok);
+    if (!ok) return -1;
+    ResCalcArgs<double> p{E, pedge->map_d, pecell->map_d, (const double *)a[0].dat->data_d,
+                          (const double *)a[2].dat->data_d, (const double *)a[4].dat->data_d,
+                          (double *)a[6].dat->data_d, k};
+    const Plan *plan = nullptr;
+    if (r.opt_inc_mode != OP2B_INC_ATOMIC) {
+      plan = get_res_plan(name, set, nargs, a);
+      if (!plan) return -1;
+    }
+    r.begin_loop(name);
+    e = run_res_calc<double>(r.ctx(), p, plan, r.opt_inc_mode);
+  } else {
+    AirConst<float> k = air_consts<float>(ok);
+    if (!ok) return -1;
+    ResCalcArgs<float> p{E, pedge->map_d, pecell->map_d, (const float *)a[0].dat->data_d,
+                         (const float *)a[2].dat->data_d, (const float *)a[4].dat->data_d,
+                         (float *)a[6].dat->data_d, k};
+    const Plan *plan = nullptr;
+    if (r.opt_inc_mode != OP2B_INC_ATOMIC) {
+      plan = get_res_plan(name, set, nargs, a);
+      if (!plan) return -1;
+    }
+    r.begin_loop(name);
+    e = run_res_calc<float>(r.ctx(), p, plan, r.opt_inc_mode);
+  }
+  (void)d;
+  r.end_loop(bytes);
+  return finish(e, name);
+}
+
+// ---------------------------------------------------------------- bres_calc
+int loop_bres_calc(const char *name, op_set set, int nargs, op_arg *a) {
+  Sig s{name, set, a, nargs};
+  if (nargs != 6) return s.fail(nargs, "bres_calc takes 6 arguments"), -1;
+  op_map pbedge = a[0].map, pbecell = a[2].map;
+  if (!pbedge || pbedge->dim != 2) return s.fail(0, "expected a dim-2 map (bedges -> nodes)"), -1;
+  if (!pbecell || pbecell->dim != 1) return s.fail(2, "expected a dim-1 map (bedges -> cells)"), -1;
+  s.dat(0, 2, OP_READ, pbedge, 0);
+  s.dat(1, 2, OP_READ, pbedge, 1);
+  s.dat(2, 4, OP_READ, pbecell, 0);
+  s.dat(3, 1, OP_READ, pbecell, 0);
+  s.dat(4, 4, OP_INC, pbecell, 0);
+  s.dat(5, 1, OP_READ, nullptr, -1);
+  if (s.ok && a[1].dat != a[0].dat) return s.fail(1, "arguments 0 and 1 must be the same dat"), -1;
+  if (s.ok && (type_bytes(a[5].dat->type) != 4 || std::string(a[5].dat->type).rfind("int", 0) != 0))
+    return s.fail(5, "the boundary flag must be an int dat"), -1;
+  int rb = s.real_bytes({0, 2, 3, 4});
+  if (!s.ok) return -1;
+  Runtime &r = rt();
+  int B = set->size;
+  double bytes = 16.0 * B + (double)rb * (2.0 + 4.0 + 1.0 + 8.0) * B;
+  bool ok;
+  cudaError_t e;
+  r.begin_loop(name);
+  if (rb == 8) {
+    AirConst<double> k = air_consts<double>(ok);
+    if (!ok) return -1;
+    e = launch_bres_calc_atomic<double>(r.ctx(), B, pbedge->map_d, pbecell->map_d,
+                                        (const int *)a[5].dat->data_d,
+                                        (const double *)a[0].dat->data_d,
+                                        (const double *)a[2].dat->data_d,
+                                        (const double *)a[3].dat->data_d,
+                                        (double *)a[4].dat->data_d, k);
+  } else {
+    AirConst<float> k = air_consts<float>(ok);
+    if (!ok) return -1;
+    e = launch_bres_calc_atomic<float>(r.ctx(), B, pbedge->map_d, pbecell->map_d,
+                                       (const int *)a[5].dat->data_d,
+                                       (const float *)a[0].dat->data_d,
+                                       (const float *)a[2].dat->data_d,
+                                       (const float *)a[3].dat->data_d,
+                                       (float *)a[4].dat->data_d, k);
+  }
+  r.end_loop(bytes);
+  return finish(e, name);
+}
+
+// ---------------------------------------------------------------- update
+// 8-argument form of airfoil_plain/dp/update.h (rms INC, maxerr MAX,
+// op_arg_idx, op_arg_info of arg 5) or the 5-argument rms-only form of
+// airfoil_tempdats/dp/update.h.
+int loop_update(const char *name, op_set set, int nargs, op_arg *a) {
+  Sig s{name, set, a, nargs};
+  if (nargs != 5 && nargs != 8) return s.fail(nargs, "update takes 5 or 8 arguments"), -1;
+  s.dat(0, 4, OP_READ, nullptr, -1);
+  s.dat(1, 4, OP_WRITE, nullptr, -1);
+  s.dat(2, 4, OP_RW, nullptr, -1);
+  s.dat(3, 1, OP_READ, nullptr, -1);
+  s.gbl(4, 1, OP_INC, 8);
+  if (nargs == 8) {
+    s.gbl(5, 1, OP_MAX, 8);
+    if (s.ok && (a[6].argtype != OP_ARG_IDX || a[6].idx != -1 || a[6].map != nullptr))
+      s.fail(6, "expected op_arg_idx(-1, OP_ID)");
+    if (s.ok && (a[7].argtype != OP_ARG_INFO || a[7].idx != 5 || a[7].dim != 1 ||
+                 a[7].size != 4 || !a[7].data))
+      s.fail(7, "expected op_arg_info(&int, 1, \"int\", 5)");
+  }
+  int rb = s.real_bytes({0, 1, 2, 3});
+  if (!s.ok) return -1;
+  if (a[4].type && strcmp(a[4].type, "double") != 0) return s.fail(4, "rms must be double"), -1;
+  Runtime &r = rt();
+  int C = set->size;
+  double bytes = (double)rb * 17.0 * C;
+  r.begin_loop(name);
+  cudaError_t e;
+  if (rb == 8)
+    e = launch_update<double>(r.ctx(), C, (const double *)a[0].dat->data_d,
+                              (double *)a[1].dat->data_d, (double *)a[2].dat->data_d,
+                              (const double *)a[3].dat->data_d, r.red);
+  else
+    e = launch_update<float>(r.ctx(), C, (const float *)a[0].dat->data_d,
+                             (float *)a[1].dat->data_d, (float *)a[2].dat->data_d,
+                             (const float *)a[3].dat->data_d, r.red);
+  r.end_loop(bytes);
+  if (finish(e, name)) return -1;
+  // gbl results are valid when op_par_loop returns
+  RedSlot *h = reinterpret_cast<RedSlot *>(r.pinned);
+  if (!cuda_ok(cudaMemcpyAsync(h, r.red.out, sizeof(RedSlot), cudaMemcpyDeviceToHost, r.stream),
+               "op_par_loop(update): reduction read-back") ||
+      !cuda_ok(cudaStreamSynchronize(r.stream), "op_par_loop(update): reduction read-back"))
+    return -1;
+  if (C == 0) return 0;
+  *reinterpret_cast<double *>(a[4].data) += h->sum;
+  if (nargs == 8) {
+    double *mx = reinterpret_cast<double *>(a[5].data);
+    if (h->maxv > *mx) {
+      *mx = h->maxv;
+      *reinterpret_cast<int *>(a[7].data) = (int)h->idx;
+    }
+  }
+  return 0;
+}
+
+struct Entry {
+  const char *name;
+  int (*fn)(const char *, op_set, int, op_arg *);
+};
+const Entry kLoops[] = {{"save_soln", loop_save_soln},
+                        {"adt_calc", loop_adt_calc},
+                        {"res_calc", loop_res_calc},
+                        {"bres_calc", loop_bres_calc},
+                        {"update", loop_update}};
+
+}  // namespace
+
+extern "C" {
+
+int op_par_loop_c(char const *name, op_set set, int nargs, op_arg *args) {
+  Runtime &r = rt();
+  if (!r.ready()) return -1;
+  if (!name || !set || (nargs > 0 && !args)) {
+    set_error("op_par_loop: needs a name, a set and the argument list");
+    return -1;
+  }
+  for (const Entry &e : kLoops)
+    if (strcmp(e.name, name) == 0) return e.fn(name, set, nargs, args);
+  set_error("op_par_loop(%s): no device implementation of this loop is registered "
+            "(libop2b runs loops on the GPU only)",
+            name);
+  return -1;
+}
+
+static void stub(const char *name, op_set set, std::initializer_list<op_arg> args) {
+  std::vector<op_arg> v(args);
+  if (op_par_loop_c(name, set, (int)v.size(), v.data()) != 0 && !rt().opt_abort)
+    fprintf(stderr, "op2b: %s\n", op2b_last_error());
+}
+
+void op_par_loop_save_soln(char const *name, op_set set, op_arg a0, op_arg a1) {
+  stub(name, set, {a0, a1});
+}
+void op_par_loop_adt_calc(char const *name, op_set set, op_arg a0, op_arg a1, op_arg a2,
+                          op_arg a3, op_arg a4, op_arg a5) {
+  stub(name, set, {a0, a1, a2, a3, a4, a5});
+}
+void op_par_loop_res_calc(char const *name, op_set set, op_arg a0, op_arg a1, op_arg a2,
+                          op_arg a3, op_arg a4, op_arg a5, op_arg a6, op_arg a7) {
+  stub(name, set, {a0, a1, a2, a3, a4, a5, a6, a7});
+}
+void op_par_loop_bres_calc(char const *name, op_set set, op_arg a0, op_arg a1, op_arg a2,
+                           op_arg a3, op_arg a4, op_arg a5) {
+  stub(name, set, {a0, a1, a2, a3, a4, a5});
+}
+void op_par_loop_update(char const *name, op_set set, op_arg a0, op_arg a1, op_arg a2,
+                        op_arg a3, op_arg a4, op_arg a5, op_arg a6, op_arg a7) {
+  stub(name, set, {a0, a1, a2, a3, a4, a5, a6, a7});
+}
+
+}  // extern "C"

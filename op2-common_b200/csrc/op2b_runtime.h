@@ -1,0 +1,87 @@
+// Internal state of libop2b's host runtime.  Not part of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "loops.h"
+#include "op2b.h"
+
+namespace op2b {
+
+struct LoopStat {
+  double total_ms = 0.0;  // summed CUDA-event device time
+  double last_ms = 0.0;
+  double bytes_per_call = 0.0;  // algorithmic bytes of one call
+  double plan_ms = 0.0;   // plan construction time (device)
+  long calls = 0;
+  long timed = 0;
+};
+
+struct PendingTime {
+  std::string name;
+  cudaEvent_t e0, e1;
+};
+
+struct Plan;  // plan.h
+
+struct Runtime {
+  bool initialised = false;
+  int device = 0, nsm = 148, cc_major = 0, cc_minor = 0;
+  cudaStream_t stream = nullptr, own_stream = nullptr;
+  long launches = 0;
+
+  // options (argv tokens of op_set_args, env, op2b_set_option)
+  int opt_diags = 0;
+  bool opt_abort = false;
+  bool opt_timing = true;
+  int opt_block_size = 0;
+  int opt_part_size = 0;
+  int opt_cache_line = 128;
+  int opt_maps_base = 0;
+  int opt_inc_mode = OP2B_INC_ATOMIC;
+  int opt_plan_mode = 0;      // 0 = parallel block colouring, 1 = serial greedy (bit-exact)
+  bool opt_check_plans = false;
+
+  std::vector<std::unique_ptr<op_set_core>> sets;
+  std::vector<std::unique_ptr<op_map_core>> maps;
+  std::vector<std::unique_ptr<op_dat_core>> dats;
+  std::map<std::string, std::vector<double>> consts;
+
+  // fused-update reduction
+  RedScratch red{};
+  void *red_base = nullptr;
+  void *pinned = nullptr;  // 4 KiB pinned host buffer for reduction read-back
+
+  // timing
+  std::map<std::string, LoopStat> stats;
+  std::vector<cudaEvent_t> ev_free;
+  std::vector<PendingTime> pending;
+  std::string cur_loop;
+  cudaEvent_t cur_ev0 = nullptr, cur_ev1 = nullptr;
+
+  LaunchCtx ctx();
+  bool ready();
+  void begin_loop(const char *name);
+  void end_loop(double bytes);
+  void resolve_timing();
+  const double *const_ptr(const char *name, int dim);
+};
+
+Runtime &rt();
+void set_error(const char *fmt, ...);
+bool cuda_ok(cudaError_t e, const char *what);
+int type_bytes(const char *type);
+bool is_real(const char *type, int bytes);
+
+// renumber.cpp
+void resolve_renumbering_for_fetch(op_dat dat);
+void fetch_original_order(op_dat dat, char *dst, int low, int high);
+// plan.cu
+void release_plans();
+
+}  // namespace op2b

@@ -1,0 +1,104 @@
+"""Build libop2b.so in-tree for sm_100a (nvcc + g++, no torch extension).
+
+Objects go to op2-common_b200/_build/, the library to op2-common_b200/op2b/.
+Only sources newer than their object are recompiled.  The Airfoil loop files
+are compiled with --fmad=false so every FP64 operation is rounded once, as in
+the reference's sequential build (direct loops then match it bit for bit).
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)                      # op2-common_b200/
+REPO = os.path.dirname(ROOT)
+CSRC = os.path.join(ROOT, "csrc")
+BUILD = os.path.join(ROOT, "_build")
+INCLUDE = os.path.join(REPO, "include")
+LIB = os.path.join(PKG, "libop2b.so")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-v",
+              f"-I{INCLUDE}", f"-I{CSRC}"]
+CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wno-unused-function", f"-I{INCLUDE}",
+             f"-I{CSRC}"]
+# files whose floating-point results are compared bit for bit with the reference
+FMAD_OFF = {"airfoil_loops.cu", "airfoil_staged.cu", "batch.cu"}
+# sources not (yet) part of the library
+EXCLUDE = set()
+
+
+def _nvcc():
+    for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if c and os.path.exists(c):
+            return c
+    raise RuntimeError("nvcc not found")
+
+
+def _cuda_include():
+    return os.path.join(os.path.dirname(os.path.dirname(_nvcc())), "include")
+
+
+def sources():
+    out = []
+    for f in sorted(os.listdir(CSRC)):
+        if f in EXCLUDE:
+            continue
+        if f.endswith(".cu") or f.endswith(".cpp"):
+            out.append(os.path.join(CSRC, f))
+    return out
+
+
+def _deps_mtime():
+    t = 0.0
+    for d in (CSRC, INCLUDE):
+        for f in os.listdir(d):
+            if f.endswith((".h", ".cuh")):
+                t = max(t, os.path.getmtime(os.path.join(d, f)))
+    return t
+
+
+def build(verbose: bool = False, force: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    nvcc = _nvcc()
+    hdr_t = _deps_mtime()
+    objs = []
+    changed = force or not os.path.exists(LIB)
+    for src in sources():
+        base = os.path.basename(src)
+        obj = os.path.join(BUILD, base + ".o")
+        objs.append(obj)
+        if not force and os.path.exists(obj) and os.path.getmtime(obj) >= max(
+                os.path.getmtime(src), hdr_t):
+            continue
+        changed = True
+        if src.endswith(".cu"):
+            cmd = [nvcc, *ARCH, *NVCC_FLAGS, "-c", src, "-o", obj]
+            if base in FMAD_OFF:
+                cmd.insert(1, "--fmad=false")
+        else:
+            cmd = ["g++", *CXX_FLAGS, f"-I{_cuda_include()}", "-c", src, "-o", obj]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        log = os.path.join(BUILD, base + ".log")
+        with open(log, "w") as f:
+            f.write(" ".join(cmd) + "\n" + res.stdout + res.stderr)
+        if res.returncode != 0:
+            raise RuntimeError(f"compiling {base} failed:\n{res.stdout[-6000:]}{res.stderr[-6000:]}")
+        if verbose:
+            print("compiled", base, file=sys.stderr)
+    if changed:
+        cmd = [nvcc, *ARCH, "-shared", "-o", LIB + ".tmp", *objs, "-lcuda"]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError(f"linking libop2b.so failed:\n{res.stdout}{res.stderr}")
+        os.replace(LIB + ".tmp", LIB)
+        if verbose:
+            print("linked", LIB, file=sys.stderr)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose=True, force="--force" in sys.argv))

@@ -1,0 +1,310 @@
+"""ctypes binding of libop2b's C ABI (include/op2b.h).
+
+The functions mirror the OP2 C/C++ API (op2/include/op_lib_c.h:75-121,
+op_lib_cpp.h:127-203): same names, same argument meaning.  Python-side
+conveniences: op_decl_dat takes a numpy array and derives type and size,
+op_arg_gbl takes a numpy array (written back in place for INC/MIN/MAX, as the
+reference writes back into the caller's variable), op_fetch_data returns a
+new numpy array.  Errors raise Op2Error with the library's message.
+
+The library must exist (build with op2b.build.build()); there is no fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+OP_READ, OP_WRITE, OP_RW, OP_INC, OP_MIN, OP_MAX, OP_WORK = range(7)
+OP_ARG_GBL, OP_ARG_DAT, OP_ARG_IDX, OP_ARG_INFO = range(4)
+OP_STAGE_NONE, OP_STAGE_INC, OP_STAGE_ALL, OP_STAGE_PERMUTE, OP_COLOR2 = range(5)
+OP2B_INC_ATOMIC, OP2B_INC_COLOR, OP2B_INC_HYBRID = range(3)
+OP_ID = None
+OP_GBL = None
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libop2b.so")
+
+
+class Op2Error(RuntimeError):
+    pass
+
+
+class op_set_core(ctypes.Structure):
+    _fields_ = [("index", ctypes.c_int), ("size", ctypes.c_int), ("name", ctypes.c_char_p),
+                ("core_size", ctypes.c_int), ("exec_size", ctypes.c_int),
+                ("nonexec_size", ctypes.c_int)]
+
+
+class op_map_core(ctypes.Structure):
+    pass
+
+
+op_map_core._fields_ = [("index", ctypes.c_int), ("from_", ctypes.POINTER(op_set_core)),
+                        ("to", ctypes.POINTER(op_set_core)), ("dim", ctypes.c_int),
+                        ("map", ctypes.POINTER(ctypes.c_int)),
+                        ("map_d", ctypes.POINTER(ctypes.c_int)), ("name", ctypes.c_char_p)]
+
+
+class op_dat_core(ctypes.Structure):
+    _fields_ = [("index", ctypes.c_int), ("set", ctypes.POINTER(op_set_core)),
+                ("dim", ctypes.c_int), ("size", ctypes.c_int), ("data", ctypes.c_void_p),
+                ("data_d", ctypes.c_void_p), ("type", ctypes.c_char_p), ("name", ctypes.c_char_p)]
+
+
+op_set = ctypes.POINTER(op_set_core)
+op_map = ctypes.POINTER(op_map_core)
+op_dat = ctypes.POINTER(op_dat_core)
+
+
+class op_arg(ctypes.Structure):
+    _fields_ = [("index", ctypes.c_int), ("dat", op_dat), ("map", op_map),
+                ("dim", ctypes.c_int), ("idx", ctypes.c_int), ("size", ctypes.c_int),
+                ("data", ctypes.c_void_p), ("data_d", ctypes.c_void_p),
+                ("map_data", ctypes.POINTER(ctypes.c_int)),
+                ("map_data_d", ctypes.POINTER(ctypes.c_int)), ("type", ctypes.c_char_p),
+                ("acc", ctypes.c_int), ("argtype", ctypes.c_int), ("sent", ctypes.c_int),
+                ("opt", ctypes.c_int)]
+
+
+# every exported symbol and its (restype, argtypes); the header lists the same set
+_SIGS = {
+    "op_init": (None, [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.c_int]),
+    "op_exit": (None, []),
+    "op_decl_set": (op_set, [ctypes.c_int, ctypes.c_char_p]),
+    "op_decl_map": (op_map, [op_set, op_set, ctypes.c_int, ctypes.c_void_p, ctypes.c_char_p]),
+    "op_decl_dat_char": (op_dat, [op_set, ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
+                                  ctypes.c_void_p, ctypes.c_char_p]),
+    "op_decl_dat_temp_char": (op_dat, [op_set, ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
+                                       ctypes.c_char_p]),
+    "op_free_dat_temp_char": (ctypes.c_int, [op_dat]),
+    "op_decl_const_char": (None, [ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_void_p,
+                                  ctypes.c_char_p]),
+    "op_arg_dat": (op_arg, [op_dat, ctypes.c_int, op_map, ctypes.c_int, ctypes.c_char_p,
+                            ctypes.c_int]),
+    "op_opt_arg_dat": (op_arg, [ctypes.c_int, op_dat, ctypes.c_int, op_map, ctypes.c_int,
+                                ctypes.c_char_p, ctypes.c_int]),
+    "op_arg_gbl_char": (op_arg, [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
+                                 ctypes.c_int]),
+    "op_opt_arg_gbl_char": (op_arg, [ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                     ctypes.c_char_p, ctypes.c_int, ctypes.c_int]),
+    "op_arg_info_char": (op_arg, [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
+                                  ctypes.c_int]),
+    "op_arg_idx": (op_arg, [ctypes.c_int, op_map]),
+    "op_par_loop_c": (ctypes.c_int, [ctypes.c_char_p, op_set, ctypes.c_int,
+                                     ctypes.POINTER(op_arg)]),
+    "op_par_loop_save_soln": (None, [ctypes.c_char_p, op_set] + [op_arg] * 2),
+    "op_par_loop_adt_calc": (None, [ctypes.c_char_p, op_set] + [op_arg] * 6),
+    "op_par_loop_res_calc": (None, [ctypes.c_char_p, op_set] + [op_arg] * 8),
+    "op_par_loop_bres_calc": (None, [ctypes.c_char_p, op_set] + [op_arg] * 6),
+    "op_par_loop_update": (None, [ctypes.c_char_p, op_set] + [op_arg] * 8),
+    "op_fetch_data_char": (None, [op_dat, ctypes.c_void_p]),
+    "op_fetch_data_idx_char": (None, [op_dat, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "op_print_dat_to_binfile": (None, [op_dat, ctypes.c_char_p]),
+    "op_print_dat_to_txtfile": (None, [op_dat, ctypes.c_char_p]),
+    "op_get_size": (ctypes.c_int, [op_set]),
+    "op_timers": (None, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "op_timing_output": (None, []),
+    "op_diagnostic_output": (None, []),
+    "op_rank": (None, [ctypes.POINTER(ctypes.c_int)]),
+    "op2b_last_error": (ctypes.c_char_p, []),
+    "op2b_status": (ctypes.c_int, []),
+    "op2b_dat_upload": (ctypes.c_int, [op_dat, ctypes.c_void_p, ctypes.c_size_t]),
+    "op2b_dat_device_ptr": (ctypes.c_void_p, [op_dat]),
+    "op2b_map_device_ptr": (ctypes.c_void_p, [op_map]),
+    "op2b_set_option": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_long]),
+    "op2b_get_option": (ctypes.c_long, [ctypes.c_char_p]),
+    "op2b_loop_stats": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double),
+                                       ctypes.POINTER(ctypes.c_long),
+                                       ctypes.POINTER(ctypes.c_double),
+                                       ctypes.POINTER(ctypes.c_double)]),
+    "op2b_reset_stats": (None, []),
+    "op2b_kernel_launches": (ctypes.c_long, []),
+    "op2b_set_stream": (ctypes.c_int, [ctypes.c_void_p]),
+    "op2b_get_stream": (ctypes.c_void_p, []),
+    "op2b_synchronize": (ctypes.c_int, []),
+}
+
+_lib = None
+
+
+def load(path: str | None = None):
+    """Load libop2b.so (built in-tree).  Raises if it is missing: no fallback."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise Op2Error(f"{p} is missing: build it with `python op2-common_b200/op2b/build.py`")
+    L = ctypes.CDLL(p)
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def exported_symbols():
+    return sorted(_SIGS)
+
+
+def _check(ok: bool = True, what: str = ""):
+    msg = load().op2b_last_error().decode()
+    if not ok:
+        raise Op2Error(msg or what)
+
+
+def _b(s):
+    return None if s is None else s.encode()
+
+
+_TYPES = {np.dtype(np.float64): "double", np.dtype(np.float32): "float",
+          np.dtype(np.int32): "int"}
+
+# arrays handed to the library whose lifetime must cover the call
+_keep = []
+
+
+def op_init(argv=(), diags: int = 0):
+    L = load()
+    arr = (ctypes.c_char_p * (len(argv) + 1))(*[_b(a) for a in argv], None)
+    L.op_init(len(argv), arr, diags)
+    if L.op2b_status() != 0:
+        raise Op2Error("op_init failed: " + L.op2b_last_error().decode())
+
+
+def op_exit():
+    load().op_exit()
+    _keep.clear()
+
+
+def op_decl_set(size: int, name: str):
+    s = load().op_decl_set(int(size), _b(name))
+    if not s:
+        _check(False, "op_decl_set")
+    return s
+
+
+def op_decl_map(frm, to, dim: int, data, name: str):
+    a = np.ascontiguousarray(data, dtype=np.int32)
+    m = load().op_decl_map(frm, to, int(dim), a.ctypes.data if a.size else None, _b(name))
+    if not m:
+        _check(False, "op_decl_map")
+    return m
+
+
+def op_decl_dat(set_, dim: int, type_: str | None, data, name: str):
+    """op_decl_dat<T> (op_lib_cpp.h:127-137): the numpy dtype must match `type_`."""
+    if data is None:
+        if type_ is None:
+            raise Op2Error("op_decl_dat: needs data or a type")
+        tb = {"double": 8, "float": 4, "int": 4}[type_.split(":")[0]]
+        d = load().op_decl_dat_temp_char(set_, int(dim), _b(type_), tb, _b(name))
+    else:
+        a = np.ascontiguousarray(data)
+        t = _TYPES.get(a.dtype)
+        if t is None or (type_ is not None and type_.split(":")[0] != t):
+            raise Op2Error(f"incorrect type specified for dataset \"{name}\"")
+        d = load().op_decl_dat_char(set_, int(dim), _b(type_ or t), a.dtype.itemsize,
+                                    a.ctypes.data if a.size else None, _b(name))
+    if not d:
+        _check(False, "op_decl_dat")
+    return d
+
+
+def op_decl_const(dim: int, type_: str, value, name: str):
+    a = np.ascontiguousarray(np.atleast_1d(value),
+                             dtype={"double": np.float64, "float": np.float32,
+                                    "int": np.int32}[type_])
+    load().op_decl_const_char(int(dim), _b(type_), a.dtype.itemsize, a.ctypes.data, _b(name))
+
+
+def op_arg_dat(dat, idx: int, map_, dim: int, type_: str, acc: int):
+    return load().op_arg_dat(dat, int(idx), map_, int(dim), _b(type_), int(acc))
+
+
+def op_opt_arg_dat(opt: int, dat, idx: int, map_, dim: int, type_: str, acc: int):
+    return load().op_opt_arg_dat(int(opt), dat, int(idx), map_, int(dim), _b(type_), int(acc))
+
+
+def op_arg_gbl(data: np.ndarray, dim: int, type_: str, acc: int):
+    if not isinstance(data, np.ndarray) or not data.flags.c_contiguous:
+        raise Op2Error("op_arg_gbl: pass a contiguous numpy array (written back in place)")
+    t = _TYPES.get(data.dtype)
+    if t != type_:
+        return load().op_arg_gbl_char(data.ctypes.data, int(dim), b"error", data.dtype.itemsize,
+                                      int(acc))
+    _keep.append(data)
+    return load().op_arg_gbl_char(data.ctypes.data, int(dim), _b(type_), data.dtype.itemsize,
+                                  int(acc))
+
+
+def op_arg_info(data: np.ndarray, dim: int, type_: str, ref: int):
+    _keep.append(data)
+    return load().op_arg_info_char(data.ctypes.data, int(dim), _b(type_), data.dtype.itemsize,
+                                   int(ref))
+
+
+def op_arg_idx(idx: int, map_):
+    return load().op_arg_idx(int(idx), map_)
+
+
+def op_par_loop(name: str, set_, *args):
+    """op_par_loop(kernel, name, set, args...) without the host kernel pointer."""
+    arr = (op_arg * len(args))(*args)
+    rc = load().op_par_loop_c(_b(name), set_, len(args), arr)
+    if len(_keep) > 64:
+        del _keep[:-16]
+    if rc != 0:
+        _check(False, f"op_par_loop({name})")
+
+
+def op_fetch_data(dat) -> np.ndarray:
+    d = dat.contents
+    t = d.type.decode().split(":")[0]
+    dt = {"double": np.float64, "float": np.float32, "int": np.int32}[t]
+    n = d.set.contents.size
+    out = np.empty((n, d.dim), dtype=dt)
+    before = load().op2b_last_error()
+    load().op_fetch_data_char(dat, out.ctypes.data)
+    after = load().op2b_last_error()
+    if after and after != before:
+        raise Op2Error(after.decode())
+    return out
+
+
+def op_fetch_data_idx(dat, low: int, high: int) -> np.ndarray:
+    d = dat.contents
+    t = d.type.decode().split(":")[0]
+    dt = {"double": np.float64, "float": np.float32, "int": np.int32}[t]
+    out = np.empty((max(high - low + 1, 0), d.dim), dtype=dt)
+    load().op_fetch_data_idx_char(dat, out.ctypes.data, int(low), int(high))
+    return out
+
+
+def op_get_size(set_) -> int:
+    return load().op_get_size(set_)
+
+
+def set_option(key: str, value: int):
+    if load().op2b_set_option(_b(key), int(value)) != 0:
+        _check(False, "op2b_set_option")
+
+
+def get_option(key: str) -> int:
+    return load().op2b_get_option(_b(key))
+
+
+def loop_stats(name: str):
+    t, c, b, last = ctypes.c_double(), ctypes.c_long(), ctypes.c_double(), ctypes.c_double()
+    if load().op2b_loop_stats(_b(name), ctypes.byref(t), ctypes.byref(c), ctypes.byref(b),
+                              ctypes.byref(last)) != 0:
+        return None
+    return dict(total_ms=t.value, calls=c.value, bytes_per_call=b.value, last_ms=last.value)
+
+
+def synchronize():
+    rc = load().op2b_synchronize()
+    if rc != 0:
+        _check(False, "op2b_synchronize")

@@ -1,0 +1,159 @@
+"""GPU parity of the Airfoil loops against the oracle, through the C ABI.
+
+Tolerances (north star: q and rms within 1e-12 relative after 100
+iterations, increment order differing):
+* direct loops (save_soln, adt_calc, update's q) are compared bit for bit:
+  the kernels keep the reference's expression trees and are compiled without
+  FMA contraction, like the oracle;
+* indirect increments (res_calc, bres_calc) differ only in summation order:
+  |res_gpu - res_oracle| <= 1e-12 * max|res_oracle| per component;
+* q after 100 iterations: |dq| <= 1e-12 * max|q| per component; rms within
+  1e-12 relative; maxerr within 1e-10 relative.
+"""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from op2b import lib as L
+from op2b import mesh as M
+from op2b.airfoil import Airfoil
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+MODES = [L.OP2B_INC_ATOMIC]
+
+
+def _state_after(m, c, niter):
+    st, *_ = O.airfoil_run(m, c, niter)
+    return st
+
+
+def _upload(app, st):
+    lib = L.load()
+    for dat, arr in ((app.p_q, st.q), (app.p_qold, st.qold), (app.p_adt, st.adt),
+                     (app.p_res, st.res)):
+        a = np.ascontiguousarray(arr, dtype=app.dtype)
+        assert lib.op2b_dat_upload(dat, a.ctypes.data, a.nbytes) == 0
+
+
+def _close(a, b, rel):
+    scale = np.maximum(np.abs(b).max(axis=0), 1e-300)
+    return np.all(np.abs(a - b).max(axis=0) <= rel * scale)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_each_loop_against_oracle(op2, mode):
+    op2.set_option("inc_mode", mode)
+    m = M.channel_bump(60, 30, seed=21)
+    c = M.airfoil_constants()
+    st = _state_after(m, c, 3)
+    st.res[:] = np.random.default_rng(0).standard_normal(st.res.shape) * 1e-3
+    app = Airfoil(m, c)
+    _upload(app, st)
+
+    ref = st.copy()
+    O.loop("save_soln", m, c, ref)
+    app._loop(0)
+    g = app.fetch()
+    assert np.array_equal(g["qold"], ref.qold)
+
+    O.loop("adt_calc", m, c, ref)
+    app._loop(1)
+    g = app.fetch()
+    assert np.array_equal(g["adt"], ref.adt), "adt_calc must be bit-exact"
+
+    O.loop("res_calc", m, c, ref)
+    app._loop(2)
+    g = app.fetch()
+    assert _close(g["res"], ref.res, 1e-12)
+
+    O.loop("bres_calc", m, c, ref)
+    app._loop(3)
+    g = app.fetch()
+    assert _close(g["res"], ref.res, 1e-12)
+
+    # update on the oracle's own res, so q is comparable bit for bit
+    _upload(app, ref)
+    app.rms[0] = 0.0
+    app.maxerr[0] = 0.0
+    app.errloc[0] = 0
+    rms, mx, el = O.loop("update", m, c, ref)
+    app._loop(4)
+    g = app.fetch()
+    assert np.array_equal(g["q"], ref.q), "update must be bit-exact in q"
+    assert not g["res"].any()
+    assert abs(app.rms[0] / rms - 1) < 1e-14
+    assert app.maxerr[0] == mx and app.errloc[0] == el
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("fixture", ["airfoil_24x12_s3.npz", "airfoil_240x120_s1.npz"])
+def test_100_iterations_match_reference_golden(op2, mode, fixture):
+    op2.set_option("inc_mode", mode)
+    gd = np.load(f"{GOLDEN}/{fixture}")
+    m = M.channel_bump(int(gd["I"]), int(gd["J"]), seed=int(gd["seed"]))
+    app = Airfoil(m)
+    hist = app.iterate(int(gd["niter"]))
+    rms = np.array([h[0] for h in hist])
+    mx = np.array([h[1] for h in hist])
+    el = np.array([h[2] for h in hist])
+    assert np.max(np.abs(rms / gd["rms"] - 1)) < 1e-12
+    assert np.max(np.abs(mx / gd["maxerr"] - 1)) < 1e-10
+    assert (el == gd["errloc"]).mean() > 0.95
+    q = app.fetch()["q"]
+    if "q" in gd:
+        assert _close(q, gd["q"], 1e-12)
+    else:
+        idx = gd["q_sample_idx"]
+        assert _close(q[idx], gd["q_sample"], 1e-12)
+        assert np.allclose(q.sum(axis=0), gd["q_sum"], rtol=1e-12, atol=0)
+
+
+def test_large_mesh_one_iteration_against_oracle(op2):
+    """The full 2400x1200 configuration: GPU vs oracle after 2 iterations, plus
+    conservation of the interior flux (sum of res_calc's increments is 0)."""
+    m = M.channel_bump(2400, 1200, seed=1)
+    c = M.airfoil_constants()
+    st, rms_o, _, _ = O.airfoil_run(m, c, 2)
+    app = Airfoil(m, c)
+    hist = app.iterate(2)
+    assert np.max(np.abs(np.array([h[0] for h in hist]) / rms_o - 1)) < 1e-12
+    assert _close(app.fetch()["q"], st.q, 1e-12)
+    # res_calc alone on the converged-ish state: increments cancel pairwise
+    app._loop(1)
+    app._loop(2)
+    r = app.fetch()["res"]
+    assert np.all(np.abs(r.sum(axis=0)) <= 1e-9 * np.abs(r).sum(axis=0))
+
+
+def test_mixed_precision_against_fp32_restatement(op2):
+    m = M.channel_bump(120, 60, seed=4)
+    c = M.airfoil_constants()
+    st32, rms32 = O.airfoil_run_mixed(m, c, 50)
+    _, rms64, _, _ = O.airfoil_run(m, c, 50)
+    app = Airfoil(m, c, dtype=np.float32)
+    hist = app.iterate(50)
+    rms = np.array([h[0] for h in hist])
+    q = app.fetch()["q"]
+    # float increments in a different order: agreement at float rounding level
+    assert np.max(np.abs(rms / rms32 - 1)) < 1e-4
+    assert _close(q, st32.q, 1e-5)
+    # and the stated error of the form against the FP64 oracle
+    assert np.max(np.abs(rms / rms64 - 1)) < 1e-3
+
+
+def test_errors_are_reported_not_run_on_host(op2):
+    m = M.channel_bump(8, 4, seed=1)
+    app = Airfoil(m)
+    with pytest.raises(L.Op2Error, match="no device implementation"):
+        L.op_par_loop("not_a_loop", app.cells, *app.a_save)
+    with pytest.raises(L.Op2Error, match="argument"):
+        L.op_par_loop("res_calc", app.edges, *app.a_res[:7])
+    bad = L.op_arg_dat(app.p_q, -1, L.OP_ID, 4, "double", L.OP_WRITE)
+    with pytest.raises(L.Op2Error, match="OP_READ"):
+        L.op_par_loop("save_soln", app.cells, bad, app.a_save[1])
+    with pytest.raises(L.Op2Error, match="invalid data for map"):
+        L.op_decl_map(app.edges, app.cells, 2, np.full(2 * m.nedge, m.ncell), "bad")
+    launches = L.load().op2b_kernel_launches()
+    assert launches >= 0
