@@ -425,6 +425,22 @@ void op_decl_const_char(int dim, char const *type, int type_size, char *dat, cha
 
 // ------------------------------------------------------------------ op_arg
 
+// op_arg keeps the type string beyond the call (the reference keeps the
+// caller's pointer, normally a literal); interning makes callers whose
+// strings are temporaries (e.g. other language bindings) safe too.
+static const char *intern_type(const char *t) {
+  static const char *known[] = {"double", "float", "int", "uint", "ll", "ull", "bool",
+                                "double:soa", "float:soa", "int:soa", "error"};
+  static std::vector<std::unique_ptr<std::string>> extra;
+  if (!t) return nullptr;
+  for (const char *k : known)
+    if (strcmp(k, t) == 0) return k;
+  for (auto &e : extra)
+    if (*e == t) return e->c_str();
+  extra.push_back(std::make_unique<std::string>(t));
+  return extra.back()->c_str();
+}
+
 static op_arg blank_arg() {
   op_arg a;
   memset(&a, 0, sizeof(a));
@@ -440,7 +456,7 @@ op_arg op_arg_dat(op_dat dat, int idx, op_map map, int dim, char const *type, op
   a.map = map;
   a.dim = dim;
   a.idx = idx;
-  a.type = type;
+  a.type = intern_type(type);
   a.acc = acc;
   if (dat) {
     a.size = dat->size;
@@ -467,7 +483,7 @@ op_arg op_arg_gbl_char(char *data, int dim, const char *type, int type_size, op_
   a.data = data;
   a.dim = dim;
   a.size = dim * type_size;
-  a.type = type;
+  a.type = intern_type(type);
   a.acc = acc;
   return a;
 }
@@ -487,7 +503,7 @@ op_arg op_arg_info_char(char *data, int dim, const char *type, int type_size, in
   a.data = data;
   a.dim = dim;
   a.size = dim * type_size;
-  a.type = type;
+  a.type = intern_type(type);
   a.acc = ref;  // the reference keeps the referenced argument's position here too
   a.idx = ref;
   return a;

@@ -91,7 +91,7 @@ class Airfoil:
     def _loop(self, i):
         name, s, arr, n = self._c[i]
         if L.load().op_par_loop_c(name, s, n, arr) != 0:
-            raise L.Op2Error(L.load().op2b_last_error().decode())
+            raise L.Op2Error(L.last_error())
 
     def iterate(self, niter: int, history: bool = True):
         """Run `niter` outer iterations; returns [(rms, maxerr, errloc)] per iteration."""

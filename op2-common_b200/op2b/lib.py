@@ -149,8 +149,12 @@ def exported_symbols():
     return sorted(_SIGS)
 
 
+def last_error() -> str:
+    return load().op2b_last_error().decode(errors="replace")
+
+
 def _check(ok: bool = True, what: str = ""):
-    msg = load().op2b_last_error().decode()
+    msg = last_error()
     if not ok:
         raise Op2Error(msg or what)
 
