@@ -206,6 +206,28 @@ void *op2b_get_stream(void);
 /* Block until every launched kernel has finished; returns a CUDA error code. */
 int op2b_synchronize(void);
 
+/* The update loop (q = qold - res/adt, res = 0, rms += sum of del^2, maxerr
+ * and errloc from the largest del^2) for callers that cannot allocate device
+ * memory: an application whose device memory is all held by its own pool, or
+ * a latency-critical path that must not pay the device-wide synchronisation
+ * of cudaMalloc/cudaFree.  It allocates nothing: the reduction scratch is a
+ * fixed array inside the library (about 512 KiB held on every GPU that loads
+ * the library, until exit).  No counterpart in the reference.
+ *   qold, q, res (4 doubles per cell), adt (1 per cell): the caller's device
+ *   arrays; rms, maxerr, errloc: the caller's device scalars, updated as
+ *   op_arg_gbl OP_INC / OP_MAX / op_arg_info do (rms += ..., maxerr and
+ *   errloc replaced only when beaten).  Results are in device memory when the
+ *   work on `stream` (a cudaStream_t; NULL = legacy default stream) is done.
+ *   ncell must not exceed 4,194,304; larger values return -1 with a message.
+ *   The first call on a device looks up the scratch array's device address;
+ *   make that first call before any stream capture.  Calls share the one
+ *   scratch array, so calls whose work can overlap on the GPU race: serialise
+ *   them.  Works without op_init (the device current on the calling thread is
+ *   used). */
+int op2b_update_noalloc(int ncell, const double *qold, double *q, double *res,
+                        const double *adt, double *rms, double *maxerr, int *errloc,
+                        void *stream);
+
 #ifdef __cplusplus
 }
 #endif

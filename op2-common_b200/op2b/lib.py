@@ -123,6 +123,7 @@ _SIGS = {
     "op2b_set_stream": (ctypes.c_int, [ctypes.c_void_p]),
     "op2b_get_stream": (ctypes.c_void_p, []),
     "op2b_synchronize": (ctypes.c_int, []),
+    "op2b_update_noalloc": (ctypes.c_int, [ctypes.c_int] + [ctypes.c_void_p] * 8),
 }
 
 _lib = None
