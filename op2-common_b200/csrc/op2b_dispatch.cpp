@@ -198,7 +198,11 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
   Runtime &r = rt();
   int E = set->size, N = a[0].dat->set->size, C = a[2].dat->set->size;
   double bytes = 16.0 * E + (double)rb * (2.0 * N + 13.0 * C);
-  ResCalcArgs<double> d{};
+  Plan *plan = nullptr;
+  if (r.opt_inc_mode != OP2B_INC_ATOMIC) {
+    plan = get_res_plan(name, set, nargs, a);
+    if (!plan) return -1;
+  }
   bool ok;
   cudaError_t e;
   if (rb == 8) {
@@ -207,11 +211,6 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
     ResCalcArgs<double> p{E, pedge->map_d, pecell->map_d, (const double *)a[0].dat->data_d,
                           (const double *)a[2].dat->data_d, (const double *)a[4].dat->data_d,
                           (double *)a[6].dat->data_d, k};
-    const Plan *plan = nullptr;
-    if (r.opt_inc_mode != OP2B_INC_ATOMIC) {
-      plan = get_res_plan(name, set, nargs, a);
-      if (!plan) return -1;
-    }
     r.begin_loop(name);
     e = run_res_calc<double>(r.ctx(), p, plan, r.opt_inc_mode);
   } else {
@@ -220,15 +219,9 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
     ResCalcArgs<float> p{E, pedge->map_d, pecell->map_d, (const float *)a[0].dat->data_d,
                          (const float *)a[2].dat->data_d, (const float *)a[4].dat->data_d,
                          (float *)a[6].dat->data_d, k};
-    const Plan *plan = nullptr;
-    if (r.opt_inc_mode != OP2B_INC_ATOMIC) {
-      plan = get_res_plan(name, set, nargs, a);
-      if (!plan) return -1;
-    }
     r.begin_loop(name);
     e = run_res_calc<float>(r.ctx(), p, plan, r.opt_inc_mode);
   }
-  (void)d;
   r.end_loop(bytes);
   return finish(e, name);
 }
@@ -254,27 +247,29 @@ int loop_bres_calc(const char *name, op_set set, int nargs, op_arg *a) {
   Runtime &r = rt();
   int B = set->size;
   double bytes = 16.0 * B + (double)rb * (2.0 + 4.0 + 1.0 + 8.0) * B;
+  Plan *plan = nullptr;
+  if (r.opt_inc_mode == OP2B_INC_COLOR) {
+    plan = get_bres_plan(name, set, nargs, a);
+    if (!plan) return -1;
+  }
   bool ok;
   cudaError_t e;
-  r.begin_loop(name);
   if (rb == 8) {
     AirConst<double> k = air_consts<double>(ok);
     if (!ok) return -1;
-    e = launch_bres_calc_atomic<double>(r.ctx(), B, pbedge->map_d, pbecell->map_d,
-                                        (const int *)a[5].dat->data_d,
-                                        (const double *)a[0].dat->data_d,
-                                        (const double *)a[2].dat->data_d,
-                                        (const double *)a[3].dat->data_d,
-                                        (double *)a[4].dat->data_d, k);
+    BresCalcArgs<double> p{B, pbedge->map_d, pbecell->map_d, (const int *)a[5].dat->data_d,
+                           (const double *)a[0].dat->data_d, (const double *)a[2].dat->data_d,
+                           (const double *)a[3].dat->data_d, (double *)a[4].dat->data_d, k};
+    r.begin_loop(name);
+    e = run_bres_calc<double>(r.ctx(), p, plan, r.opt_inc_mode);
   } else {
     AirConst<float> k = air_consts<float>(ok);
     if (!ok) return -1;
-    e = launch_bres_calc_atomic<float>(r.ctx(), B, pbedge->map_d, pbecell->map_d,
-                                       (const int *)a[5].dat->data_d,
-                                       (const float *)a[0].dat->data_d,
-                                       (const float *)a[2].dat->data_d,
-                                       (const float *)a[3].dat->data_d,
-                                       (float *)a[4].dat->data_d, k);
+    BresCalcArgs<float> p{B, pbedge->map_d, pbecell->map_d, (const int *)a[5].dat->data_d,
+                          (const float *)a[0].dat->data_d, (const float *)a[2].dat->data_d,
+                          (const float *)a[3].dat->data_d, (float *)a[4].dat->data_d, k};
+    r.begin_loop(name);
+    e = run_bres_calc<float>(r.ctx(), p, plan, r.opt_inc_mode);
   }
   r.end_loop(bytes);
   return finish(e, name);

@@ -126,6 +126,95 @@ _SIGS = {
     "op2b_update_noalloc": (ctypes.c_int, [ctypes.c_int] + [ctypes.c_void_p] * 8),
 }
 
+
+class op_plan(ctypes.Structure):
+    """include/op2b_plan.h (field order of op2/include/op_rt_support.h:46-88)."""
+
+
+_ip = ctypes.POINTER(ctypes.c_int)
+op_plan._fields_ = [
+    ("name", ctypes.c_char_p), ("set", op_set), ("nargs", ctypes.c_int), ("ninds", ctypes.c_int),
+    ("ninds_staged", ctypes.c_int), ("part_size", ctypes.c_int),
+    ("maps", ctypes.POINTER(op_map)), ("dats", ctypes.POINTER(op_dat)), ("idxs", _ip),
+    ("optflags", _ip), ("accs", _ip), ("inds_staged", _ip),
+    ("nthrcol", _ip), ("thrcol", _ip), ("col_reord", _ip), ("col_offsets", ctypes.POINTER(_ip)),
+    ("color2_offsets", _ip), ("offset", _ip), ("offset_d", _ip), ("ind_map", _ip),
+    ("ind_maps", ctypes.POINTER(_ip)), ("ind_offs", _ip), ("ind_sizes", _ip),
+    ("nindirect", _ip), ("loc_map", ctypes.POINTER(ctypes.c_short)),
+    ("loc_maps", ctypes.POINTER(ctypes.POINTER(ctypes.c_short))), ("nblocks", ctypes.c_int),
+    ("nelems", _ip), ("nelems_d", _ip), ("ncolors_core", ctypes.c_int),
+    ("ncolors_owned", ctypes.c_int), ("ncolors", ctypes.c_int), ("ncolblk", _ip),
+    ("blkmap", _ip), ("blkmap_d", _ip), ("nsharedCol", _ip), ("nshared", ctypes.c_int),
+    ("transfer", ctypes.c_float), ("transfer2", ctypes.c_float), ("count", ctypes.c_int)]
+
+_SIGS.update({
+    "op_plan_get_stage": (ctypes.POINTER(op_plan), [ctypes.c_char_p, op_set, ctypes.c_int,
+                                                     ctypes.c_int, ctypes.POINTER(op_arg),
+                                                     ctypes.c_int, _ip, ctypes.c_int]),
+    "op_plan_get_stage_upload": (ctypes.POINTER(op_plan),
+                                 [ctypes.c_char_p, op_set, ctypes.c_int, ctypes.c_int,
+                                  ctypes.POINTER(op_arg), ctypes.c_int, _ip, ctypes.c_int,
+                                  ctypes.c_int]),
+    "op_plan_get": (ctypes.POINTER(op_plan), [ctypes.c_char_p, op_set, ctypes.c_int,
+                                              ctypes.c_int, ctypes.POINTER(op_arg),
+                                              ctypes.c_int, _ip]),
+    "op_plan_check": (None, [op_plan, ctypes.c_int, _ip]),
+    "op2b_plan_validate": (ctypes.c_int, [ctypes.POINTER(op_plan),
+                                          ctypes.POINTER(ctypes.c_long)]),
+    "op2b_plan_build_ms": (ctypes.c_double, [ctypes.POINTER(op_plan)]),
+    "op2b_plan_device_blkmap": (ctypes.c_void_p, [ctypes.POINTER(op_plan)]),
+    "op2b_plan_device_thrcol": (ctypes.c_void_p, [ctypes.POINTER(op_plan)]),
+    "op2b_plan_release_all": (None, []),
+})
+
+
+def op_plan_get_stage(name: str, set_, part_size: int, args, inds, staging: int):
+    arr = (op_arg * len(args))(*args)
+    ind = (ctypes.c_int * len(inds))(*inds)
+    p = load().op_plan_get_stage(_b(name), set_, int(part_size), len(args), arr, max(inds) + 1,
+                                 ind, int(staging))
+    if not p:
+        _check(False, "op_plan_get_stage")
+    return p
+
+
+def plan_arrays(p) -> dict:
+    """Host copies of a plan's arrays as numpy arrays (names of op_rt_support.h)."""
+    o = p.contents
+    nb, nst, ninds = o.nblocks, o.ninds_staged, o.ninds
+    n = o.set.contents.size
+    A = lambda ptr, cnt, dt=np.int32: np.ctypeslib.as_array(ptr, shape=(cnt,)).astype(dt).copy() \
+        if cnt > 0 else np.zeros(0, dt)
+    d = dict(nblocks=nb, ncolors=o.ncolors, ninds_staged=nst, nshared=o.nshared,
+             transfer=o.transfer, transfer2=o.transfer2, count=o.count,
+             nthrcol=A(o.nthrcol, nb), thrcol=A(o.thrcol, n), offset=A(o.offset, nb),
+             nelems=A(o.nelems, nb), ind_offs=A(o.ind_offs, nb * nst),
+             ind_sizes=A(o.ind_sizes, nb * nst), nindirect=A(o.nindirect, ninds),
+             inds_staged=A(o.inds_staged, o.nargs))
+    ncb = max(o.ncolors, 0)
+    d["ncolblk"] = A(o.ncolblk, ncb if ncb else 0)
+    d["blkmap"] = A(o.blkmap, nb)
+    d["nsharedCol"] = A(o.nsharedCol, ncb)
+    for m in range(nst):
+        used = int(d["ind_sizes"][m::nst].sum()) if nb else 0
+        d[f"ind_map{m}"] = A(o.ind_maps[m], used)
+    for a in range(o.nargs):
+        if o.loc_maps[a]:
+            d[f"loc_map{a}"] = A(o.loc_maps[a], n, np.int16)
+    if o.col_reord:
+        d["col_reord"] = A(o.col_reord, n)
+        tot = int((d["nthrcol"] + 1).sum())
+        d["col_offsets"] = A(o.col_offsets[0], tot)
+    return d
+
+
+def plan_validate(p):
+    det = (ctypes.c_long * 8)()
+    n = load().op2b_plan_validate(p, det)
+    if n < 0:
+        _check(False, "op2b_plan_validate")
+    return n, list(det)
+
 _lib = None
 
 

@@ -21,7 +21,7 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-MODES = [L.OP2B_INC_ATOMIC]
+MODES = [L.OP2B_INC_ATOMIC, L.OP2B_INC_COLOR, L.OP2B_INC_HYBRID]
 
 
 def _state_after(m, c, niter):
@@ -108,6 +108,22 @@ def test_100_iterations_match_reference_golden(op2, mode, fixture):
         idx = gd["q_sample_idx"]
         assert _close(q[idx], gd["q_sample"], 1e-12)
         assert np.allclose(q.sum(axis=0), gd["q_sum"], rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("part", [0, 1024])
+def test_colouring_is_deterministic_and_matches_atomics(op2, part):
+    m = M.channel_bump(300, 150, seed=8)
+    op2.set_option("part_size", part)
+    runs = {}
+    for mode in (L.OP2B_INC_ATOMIC, L.OP2B_INC_COLOR, L.OP2B_INC_COLOR, L.OP2B_INC_HYBRID):
+        op2.set_option("inc_mode", mode)
+        app = Airfoil(m)
+        hist = app.iterate(20)
+        runs.setdefault(mode, []).append(np.array([h[0] for h in hist]))
+    c1, c2 = runs[L.OP2B_INC_COLOR]
+    assert np.array_equal(c1, c2), "colouring must be deterministic"
+    for mode in (L.OP2B_INC_ATOMIC, L.OP2B_INC_HYBRID):
+        assert np.max(np.abs(runs[mode][0] / c1 - 1)) < 1e-12
 
 
 def test_large_mesh_one_iteration_against_oracle(op2):
