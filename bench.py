@@ -11,23 +11,26 @@ path does not shard; there is no collective on the data path), timing is the
 max over ranks.  Prints one JSON line on rank 0.
 
 * value      device-timed ms/iteration, inputs resident in HBM (CUDA events on
-             the library's stream, K iterations between a barrier and
-             synchronize on both sides).  The working set (~690 MB) is larger
-             than L2 (126 MB), so no flush is needed between iterations.
-* e2e        the same metric through the public API with host buffers:
-             op_decl_* uploads from pinned host memory, K iterations, and
-             op_fetch_data of q, all inside the timed region, per iteration.
-* roofline   the dominant loop's algorithmic bytes per call / its average
+             the library's stream, K iterations between a barrier and a
+             synchronize on both sides).  The working set (~0.7 GB) is larger
+             than the 126 MB L2, so no flush is needed between iterations.
+             Default configuration: the mesh renumbered on the GPU
+             (op_renumber, reverse Cuthill-McKee) and the staged-hybrid
+             increment strategy.
+* e2e        the whole job through the public API with host buffers, per
+             iteration: op_decl_* uploads from pinned host memory, op_renumber,
+             K iterations, op_fetch_data of q.
+* roofline   the dominant loop's algorithmic bytes per call / its mean
              CUDA-event duration, against MEASURED_PEAKS.json hbm_gbs.
-* cpu_baseline  the reference's own OpenMP build (oracle/_ref, compiled from
-             the reference sources) on a bounded sample of the same mesh.
+* variants   the same timing for random/RCM numbering x atomics/colouring/hybrid.
+* cpu_baseline  the reference's own OpenMP build (oracle/_ref, compiled from the
+             reference sources) on a bounded sample of the same mesh.
 * --impl reference   times that reference build alone (rank 0; others exit).
 """
 from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -43,21 +46,25 @@ sys.path.insert(0, REPO)
 
 FALLBACK_HBM_GBS = 6650.0
 LOOPS = ("save_soln", "adt_calc", "res_calc", "bres_calc", "update")
+METRIC = "Airfoil ms/iter (2400x1200 FP64)"
 
 
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--steps", type=int, default=100)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="op2b", choices=["op2b", "reference"])
     p.add_argument("--mesh", type=int, nargs=2, default=[2400, 1200])
     p.add_argument("--seed", type=int, default=1)
-    p.add_argument("--inc-mode", type=int, default=None,
-                   help="0 atomics, 1 colouring, 2 staged+atomics (default: library default)")
+    p.add_argument("--numbering", default="rcm", choices=["rcm", "random"])
+    p.add_argument("--inc-mode", type=int, default=2,
+                   help="0 atomics, 1 block/thread colouring, 2 staged hybrid")
+    p.add_argument("--part-size", type=int, default=0)
     p.add_argument("--precision", default="f64", choices=["f64", "mixed"])
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-variants", action="store_true")
     p.add_argument("--cpu-iters", type=int, default=4)
     return p.parse_args()
 
@@ -90,14 +97,14 @@ def peaks():
     return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
 
 
-def traffic_from_profiles(loop, workload_key):
+def traffic_from_profiles(key, loop):
     """dram bytes per launch of `loop` from the committed ncu summary, if any."""
     p = os.path.join(REPO, "profiles", "traffic.json")
     if not os.path.exists(p):
         return None
     with open(p) as f:
         d = json.load(f)
-    return d.get(workload_key, {}).get(loop)
+    return d.get(key, {}).get(loop)
 
 
 class Clocks:
@@ -154,15 +161,16 @@ class Clocks:
 def run_reference(args, m_path, ncell, iters, skip, threads):
     from oracle import oracle as O
     binary = O.ref_binary("ref_airfoil_openmp")
-    kind = "reference"
     if binary is None:
         return None
-    env = {"OMP_NUM_THREADS": str(threads)}
-    summary, _ = O.run_reference_airfoil_timed(binary, m_path, iters, skip, env=env)
-    return dict(value=summary["ms_per_iter"], unit="ms/iter", cores=summary.get("threads", threads),
-                kind=kind, sample=f"{summary['timed_iters']} iterations of the {args.mesh[0]}x"
-                f"{args.mesh[1]} mesh ({ncell} cells) after {skip} untimed, OpenMP build of the "
-                "reference (v1 translator output), OMP_NUM_THREADS=" + str(threads))
+    summary, _ = O.run_reference_airfoil_timed(binary, m_path, iters, skip,
+                                               env={"OMP_NUM_THREADS": str(threads)})
+    return dict(value=summary["ms_per_iter"], unit="ms/iter",
+                cores=summary.get("threads", threads), kind="reference",
+                sample=f"{summary['timed_iters']} iterations of the {args.mesh[0]}x{args.mesh[1]} "
+                       f"mesh ({ncell} cells, random numbering) after {skip} untimed, the "
+                       "reference's OpenMP build (v1 translator output), "
+                       f"OMP_NUM_THREADS={threads}")
 
 
 def impl_reference(args):
@@ -172,24 +180,67 @@ def impl_reference(args):
     m, path = mesh_file(*args.mesh, args.seed)
     threads = os.cpu_count() or 1
     # one step = one iteration of the reference's OpenMP build on the same mesh;
-    # warm-up iterations (plan construction included) are run but not timed
+    # warm-up iterations (its plan construction included) run but are not timed
     res = run_reference(args, path, m.ncell, args.warmup + args.steps, args.warmup, threads)
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable":
                           "oracle/_ref/ref_airfoil_openmp not built (make -C oracle)"}))
         return 0
     v = res["value"]
-    line = {"metric": "Airfoil ms/iter (2400x1200 FP64)", "value": v, "unit": "ms/iter",
-            "impl": "reference", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": v, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"airfoil {args.mesh[0]}x{args.mesh[1]} plain FP64, "
-                       "random numbering", "cells": m.ncell, "edges": m.nedge},
-            "cpu_baseline": res,
-            "e2e": {"value": v, "unit": "ms/iter", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
-    print(json.dumps(line))
+    print(json.dumps({
+        "metric": METRIC, "value": v, "unit": "ms/iter", "impl": "reference", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"airfoil {args.mesh[0]}x{args.mesh[1]} plain FP64",
+                   "cells": m.ncell, "edges": m.nedge},
+        "cpu_baseline": res,
+        "e2e": {"value": v, "unit": "ms/iter", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
     return 0
+
+
+def timed_run(L, Airfoil, mesh, dtype, numbering, inc_mode, part, steps, warmup, torch,
+              barrier=None, clocks=None):
+    """Declare, optionally renumber, warm up, then time `steps` iterations."""
+    L.op_init()
+    L.set_option("inc_mode", inc_mode)
+    L.set_option("part_size", part)
+    app = Airfoil(mesh, dtype=dtype)
+    ren = None
+    if numbering == "rcm":
+        t0 = time.perf_counter()
+        ren = app.renumber()
+        ren["ms"] = 1e3 * (time.perf_counter() - t0)
+    stream = torch.cuda.ExternalStream(L.load().op2b_get_stream())
+    app.iterate(warmup, history=False)
+    L.synchronize()
+    L.load().op2b_reset_stats()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    if barrier:
+        barrier()
+    L.synchronize()
+    launches0 = L.load().op2b_kernel_launches()
+    if clocks:
+        clocks.start()
+    e0.record(stream)
+    hist = app.iterate(steps)
+    e1.record(stream)
+    L.synchronize()
+    if barrier:
+        barrier()
+    clk = clocks.stop() if clocks else None
+    launches = L.load().op2b_kernel_launches() - launches0
+    ms = e0.elapsed_time(e1) / max(steps, 1)
+    stats = {n: L.loop_stats(n) for n in LOOPS}
+    L.op_exit()
+    loops = {}
+    for n, s in stats.items():
+        if s and s["calls"]:
+            avg = s["total_ms"] / s["calls"]
+            loops[n] = {"calls": s["calls"], "avg_ms": avg, "alg_bytes": s["bytes_per_call"],
+                        "gbs": s["bytes_per_call"] / (avg * 1e-3) / 1e9 if avg > 0 else None}
+    return dict(ms=ms, loops=loops, launches=launches, clocks=clk, renumber=ren,
+                rms=hist[-1][0] if hist else None)
 
 
 def main():
@@ -226,38 +277,28 @@ def main():
         return float(t.item())
 
     # ---------------------------------------------------------- device-resident timing
-    L.op_init()
-    if args.inc_mode is not None:
-        L.set_option("inc_mode", args.inc_mode)
-    app = Airfoil(m, dtype=dtype)
-    stream = torch.cuda.ExternalStream(L.load().op2b_get_stream())
-    app.iterate(args.warmup, history=False)
-    L.synchronize()
-    L.load().op2b_reset_stats()
-    clocks = Clocks(local)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    barrier()
-    L.synchronize()
-    launches0 = L.load().op2b_kernel_launches()
-    clocks.start()
-    e0.record(stream)
-    hist = app.iterate(args.steps)
-    e1.record(stream)
-    L.synchronize()
-    barrier()
-    clk = clocks.stop()
-    launches = L.load().op2b_kernel_launches() - launches0
-    ms = e0.elapsed_time(e1) / max(args.steps, 1)
-    ms = max_over_ranks(ms)
-    stats = {n: L.loop_stats(n) for n in LOOPS}
-    final_rms = hist[-1][0] if hist else float("nan")
-    L.op_exit()
+    main_run = timed_run(L, Airfoil, m, dtype, args.numbering, args.inc_mode, args.part_size,
+                         args.steps, args.warmup, torch, barrier, Clocks(local))
+    ms = max_over_ranks(main_run["ms"])
+
+    # ---------------------------------------------------------- variants (same rank-local work)
+    variants = []
+    if not args.no_variants:
+        for numbering in ("random", "rcm"):
+            for mode in (0, 1, 2):
+                if numbering == "random" and mode == 1:
+                    continue  # hundreds of block colours: one launch each
+                v = timed_run(L, Airfoil, m, dtype, numbering, mode, args.part_size, 20, 3, torch,
+                              barrier)
+                variants.append({"numbering": numbering, "inc_mode": mode,
+                                 "ms_per_iter": max_over_ranks(v["ms"]),
+                                 "res_calc_gbs": v["loops"].get("res_calc", {}).get("gbs"),
+                                 "launches_per_iter": v["launches"] / 20})
 
     # ---------------------------------------------------------- end to end through the API
     e2e = None
     if not args.no_e2e:
-        pinned = {}
+        keep = []
 
         def pin(a):
             t = torch.empty(a.shape, dtype={np.float64: torch.float64, np.float32: torch.float32,
@@ -265,7 +306,7 @@ def main():
                             pin_memory=True)
             arr = t.numpy()
             arr[...] = a
-            pinned[id(arr)] = t
+            keep.append(t)
             return arr
 
         from op2b.mesh import Mesh
@@ -273,18 +314,14 @@ def main():
                   ecell=pin(m.ecell), bedge=pin(m.bedge), becell=pin(m.becell),
                   bound=pin(m.bound))
         L.op_init()
-        if args.inc_mode is not None:
-            L.set_option("inc_mode", args.inc_mode)
-        warm = Airfoil(hm, dtype=dtype)      # warm the plan/alloc paths once
-        warm.iterate(1, history=False)
-        L.op_exit()
-        L.op_init()
-        if args.inc_mode is not None:
-            L.set_option("inc_mode", args.inc_mode)
+        L.set_option("inc_mode", args.inc_mode)
+        L.set_option("part_size", args.part_size)
         barrier()
         t0 = time.perf_counter()
         app2 = Airfoil(hm, dtype=dtype)
-        h2 = app2.iterate(args.steps)
+        if args.numbering == "rcm":
+            app2.renumber()
+        app2.iterate(args.steps)
         q = L.op_fetch_data(app2.p_q)
         t1 = time.perf_counter()
         barrier()
@@ -292,13 +329,14 @@ def main():
         es = np.dtype(dtype).itemsize
         h2d = (m.x.size * es + (m.cell.size + m.edge.size + m.ecell.size + m.bedge.size
                                 + m.becell.size + m.bound.size) * 4
-               + m.ncell * 4 * es * 3 + m.ncell * es)
+               + m.ncell * 4 * es * 3 + m.ncell * es + args.steps * 2 * 8 * 3)
         d2h = q.nbytes + args.steps * 2 * 32
         e2e = {"value": ms_e2e, "unit": "ms/iter",
                "h2d_bytes_per_step": int(h2d / max(args.steps, 1)),
                "d2h_bytes_per_step": int(d2h / max(args.steps, 1)),
-               "note": "op_decl_* uploads from pinned host memory + K iterations + "
-                       "op_fetch_data(q), per iteration"}
+               "note": "per iteration of a whole job through the API: op_decl_* uploads from "
+                       "pinned host memory, op_renumber, K iterations (rms read back every "
+                       "update), op_fetch_data(q)"}
         L.op_exit()
 
     # ---------------------------------------------------------- CPU baseline (rank 0, N=1)
@@ -308,44 +346,45 @@ def main():
         cpu = run_reference(args, m_path, m.ncell, 1 + args.cpu_iters, 1, threads)
         if cpu is None:
             from oracle import oracle as O
+            from op2b.mesh import airfoil_constants
             t0 = time.perf_counter()
-            O.airfoil_run(m, __import__("op2b.mesh", fromlist=["x"]).airfoil_constants(), 2)
+            O.airfoil_run(m, airfoil_constants(), 2)
             cpu = dict(value=1e3 * (time.perf_counter() - t0) / 2, unit="ms/iter", cores=1,
                        kind="port", sample="2 iterations of the C restatement (oracle)")
 
     if rank == 0:
         peak, peak_src = peaks()
         work = f"{args.mesh[0]}x{args.mesh[1]}"
-        loops = {}
-        for n, s in stats.items():
-            if s and s["calls"]:
-                avg = s["total_ms"] / s["calls"]
-                loops[n] = {"calls": s["calls"], "avg_ms": avg,
-                            "alg_bytes": s["bytes_per_call"],
-                            "gbs": s["bytes_per_call"] / (avg * 1e-3) / 1e9 if avg > 0 else None}
+        loops = main_run["loops"]
         dom = max(loops, key=lambda n: loops[n]["avg_ms"] * loops[n]["calls"])
         d = loops[dom]
-        traffic = traffic_from_profiles(dom, f"{work}_{args.precision}_mode{args.inc_mode}")
+        key = f"{work}_{args.precision}_{args.numbering}_mode{args.inc_mode}"
         line = {
-            "metric": "Airfoil ms/iter (2400x1200 FP64)", "value": ms, "unit": "ms/iter",
-            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "metric": METRIC, "value": ms, "unit": "ms/iter", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "f64" else "f32-storage/f64-update",
-            "data": "synthetic (seeded channel-with-bump mesh, random numbering)",
-            "config": {"workload": f"airfoil {work} plain {'FP64' if args.precision == 'f64' else 'mixed'}"
-                                   f", random numbering, inc_mode {args.inc_mode if args.inc_mode is not None else 'default'}",
+            "data": "synthetic (seeded channel-with-bump mesh)",
+            "config": {"workload": f"airfoil {work} plain "
+                                   f"{'FP64' if args.precision == 'f64' else 'mixed'}, "
+                                   f"{args.numbering} numbering, inc_mode {args.inc_mode}",
                        "cells": m.ncell, "edges": m.nedge, "nodes": m.nnode,
-                       "bedges": m.nbedge, "parallelism": "replicas" if ws > 1 else "single",
+                       "bedges": m.nbedge, "numbering": args.numbering,
+                       "inc_mode": args.inc_mode, "part_size": args.part_size,
+                       "parallelism": "replicas" if ws > 1 else "single",
                        "l2": "inputs larger than L2 (working set ~0.7 GB > 126 MB), no flush"},
             "roofline": {"bound": "hbm", "loop": dom, "achieved": d["gbs"], "peak": peak,
                          "unit": "GB/s", "frac": d["gbs"] / peak if d["gbs"] else None,
-                         "traffic": traffic, "peak_source": peak_src},
+                         "traffic": traffic_from_profiles(key, dom),
+                         "peak_source": peak_src},
             "loops": loops,
-            "rms_final": final_rms,
+            "renumber": main_run["renumber"],
+            "rms_final": main_run["rms"],
+            "variants": variants,
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": int(launches),
-            "clocks": clk,
+            "gpu_launches": int(main_run["launches"]),
+            "clocks": main_run["clocks"],
         }
         print(json.dumps(line))
     if dist is not None:

@@ -165,7 +165,25 @@ void op_timing_output(void);
 void op_diagnostic_output(void);
 void op_rank(int *rank);
 
+/* ---- renumbering: op_renumber / op_renumber_ptr of
+ * op2/src/externlib/op_renumber.cpp:224-516 (declared for MPI builds in the
+ * reference).  The base map's target set is ordered by a GPU reverse
+ * Cuthill-McKee (the reference uses PT-Scotch's Gibbs-Poole-Stockmeyer), the
+ * order is propagated to every set reachable through declared maps, and maps
+ * and dats are reordered on the device.  Plans built before are dropped.
+ * op_fetch_data_idx keeps returning data in the original numbering. */
+void op_renumber(op_map base);
+void op_renumber_ptr(int *ptr);
+
 /* ---- op2b extensions (no reference counterpart unless stated) ---------- */
+
+/* op_renumber returning a status; stats (may be NULL) receives the base
+ * map's bandwidth {max, average} before and after, as the reference prints
+ * (op_renumber.cpp:489-502). */
+int op2b_renumber(op_map base, long stats[4]);
+/* perm[i] = current index of the element declared as i (identity if the set
+ * was never renumbered; returns 1 then, 0 otherwise, -1 on error). */
+int op2b_set_permutation(op_set set, int *perm);
 
 /* Message of the last failed call on this thread ("" if none). */
 const char *op2b_last_error(void);

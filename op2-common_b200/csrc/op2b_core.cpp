@@ -228,6 +228,7 @@ void op_exit(void) {
   if (!r.initialised) return;
   cudaStreamSynchronize(r.stream);
   release_plans();
+  release_renumbering();
   for (auto &d : r.dats)
     if (d) {
       cudaFree(d->data_d);
@@ -247,6 +248,7 @@ void op_exit(void) {
   r.maps.clear();
   r.sets.clear();
   r.consts.clear();
+  r.map_ptrs.clear();
   for (auto &p : r.pending) {
     cudaEventDestroy(p.e0);
     cudaEventDestroy(p.e1);
@@ -327,6 +329,7 @@ op_map op_decl_map(op_set from, op_set to, int dim, int *imap, char const *name)
       return nullptr;
     }
   }
+  if (imap) r.map_ptrs[imap] = m.get();  // op_register_map_ptr (op_lib_core.cpp:493-495)
   r.maps.push_back(std::move(m));
   return r.maps.back().get();
 }

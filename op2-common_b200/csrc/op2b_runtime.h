@@ -51,6 +51,7 @@ struct Runtime {
   std::vector<std::unique_ptr<op_map_core>> maps;
   std::vector<std::unique_ptr<op_dat_core>> dats;
   std::map<std::string, std::vector<double>> consts;
+  std::map<const int *, op_map> map_ptrs;  // user array -> map (op_renumber_ptr)
 
   // fused-update reduction
   RedScratch red{};
@@ -78,9 +79,10 @@ bool cuda_ok(cudaError_t e, const char *what);
 int type_bytes(const char *type);
 bool is_real(const char *type, int bytes);
 
-// renumber.cpp
+// renumber.cu
 void resolve_renumbering_for_fetch(op_dat dat);
 void fetch_original_order(op_dat dat, char *dst, int low, int high);
+void release_renumbering();
 // plan.cu
 void release_plans();
 

@@ -1,0 +1,797 @@
+// Mesh renumbering on the GPU: op_renumber of the reference
+// (op2/src/externlib/op_renumber.cpp:224-505) with the base ordering from a
+// GPU reverse Cuthill-McKee instead of PT-Scotch's Gibbs-Poole-Stockmeyer
+// (SCOTCH_graphOrder with strategy "g", :452-461 -- a third-party library not
+// in the reference tree).
+//
+//   1. graph of the base map's target set (:274-350): for a map from another
+//      set (e.g. pecell, edges -> cells) two targets are adjacent when one
+//      element maps to both; for a map onto its own set the rows are the
+//      adjacency.  Built with a count / scan / fill / per-row sort+unique.
+//   2. reverse Cuthill-McKee, by one CTA: George-Liu pseudo-peripheral start
+//      (repeated BFS, min-degree vertex of the last level, lowest id on
+//      ties), then BFS levels; a level's new vertices are ordered by
+//      (position of their first parent in the previous level, degree, id) --
+//      the order sequential Cuthill-McKee produces -- and the whole order is
+//      reversed.  Disconnected graphs continue from the lowest unvisited id.
+//   3. propagation to the other sets, in the reference's recursive order over
+//      the declared maps (propagate_reordering, :72-151):
+//      * a map to -> from: elements sorted by the new index of their first
+//        target, ties by original index (the reference leaves ties to qsort);
+//      * else a map from -> to that covers `to`: first touch, walking `from`
+//        in its new order.
+//   4. reordering (reorder_set, :153-222): rows of maps from a set move,
+//      entries of maps to a set are renumbered, dats on a set move; all on
+//      the device, host copies of maps refreshed.
+// The permutation of every set is kept so op_fetch_data_idx can return data
+// in the application's original numbering.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <vector>
+
+#include "op2b_runtime.h"
+
+namespace op2b {
+
+// ------------------------------------------------------------------ scans
+
+__global__ void k_scan_blocks(const int *in, long long *out, long long n, long long *bsum) {
+  __shared__ long long s[1024];
+  long long i = (long long)blockIdx.x * 1024 + threadIdx.x;
+  long long v = i < n ? in[i] : 0;
+  s[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    long long t = threadIdx.x >= (unsigned)o ? s[threadIdx.x - o] : 0;
+    __syncthreads();
+    s[threadIdx.x] += t;
+    __syncthreads();
+  }
+  if (i < n) out[i] = s[threadIdx.x] - v;
+  if (threadIdx.x == 1023) bsum[blockIdx.x] = s[1023];
+}
+
+__global__ void k_scan_bsum(long long *bsum, long long nb, long long *total) {
+  if (threadIdx.x != 0) return;
+  long long acc = 0;
+  for (long long b = 0; b < nb; b++) {
+    long long t = bsum[b];
+    bsum[b] = acc;
+    acc += t;
+  }
+  *total = acc;
+}
+
+__global__ void k_scan_add(long long *out, long long n, const long long *bsum) {
+  long long i = (long long)blockIdx.x * 1024 + threadIdx.x;
+  if (i < n) out[i] += bsum[blockIdx.x];
+}
+
+// exclusive scan of n ints into out (n+1 entries: out[n] = total)
+static bool scan_exclusive(const int *in, long long *out, long long n, cudaStream_t s) {
+  long long nb = (n + 1023) / 1024;
+  long long *bsum = nullptr;
+  if (cudaMalloc(&bsum, sizeof(long long) * (nb + 1)) != cudaSuccess) return false;
+  if (nb > 0) {
+    k_scan_blocks<<<(unsigned)nb, 1024, 0, s>>>(in, out, n, bsum);
+    k_scan_bsum<<<1, 32, 0, s>>>(bsum, nb, out + n);
+    k_scan_add<<<(unsigned)nb, 1024, 0, s>>>(out, n, bsum);
+  } else {
+    cudaMemsetAsync(out, 0, sizeof(long long), s);
+  }
+  bool ok = cudaStreamSynchronize(s) == cudaSuccess;
+  cudaFree(bsum);
+  return ok;
+}
+
+// ------------------------------------------------------------------ graph
+
+__global__ void k_adj_count(int nfrom, int dim, const int *map, int nto, int *deg) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nfrom) return;
+  for (int a = 0; a < dim; a++) {
+    int u = map[(size_t)i * dim + a];
+    if (u < 0 || u >= nto) continue;
+    for (int b = 0; b < dim; b++) {
+      int v = map[(size_t)i * dim + b];
+      if (b != a && v != u && v >= 0 && v < nto) atomicAdd(&deg[u], 1);
+    }
+  }
+}
+
+__global__ void k_adj_fill(int nfrom, int dim, const int *map, int nto, const long long *row,
+                           int *fill, int *col) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nfrom) return;
+  for (int a = 0; a < dim; a++) {
+    int u = map[(size_t)i * dim + a];
+    if (u < 0 || u >= nto) continue;
+    for (int b = 0; b < dim; b++) {
+      int v = map[(size_t)i * dim + b];
+      if (b != a && v != u && v >= 0 && v < nto) col[row[u] + atomicAdd(&fill[u], 1)] = v;
+    }
+  }
+}
+
+// self map (to == from): the row of u lists its neighbours
+__global__ void k_adj_self(int n, int dim, const int *map, int *deg, int *col) {
+  int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= n) return;
+  int k = 0;
+  for (int a = 0; a < dim; a++) {
+    int v = map[(size_t)u * dim + a];
+    if (v >= 0 && v < n && v != u) col[(size_t)u * dim + k++] = v;
+  }
+  deg[u] = k;
+}
+
+// sort each row and drop duplicates; deg[u] becomes the unique count
+__global__ void k_adj_unique(int n, const long long *row, int *col, int *deg) {
+  int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= n) return;
+  int *c = col + row[u];
+  int m = deg[u];
+  for (int i = 1; i < m; i++) {
+    int v = c[i], j = i - 1;
+    while (j >= 0 && c[j] > v) {
+      c[j + 1] = c[j];
+      j--;
+    }
+    c[j + 1] = v;
+  }
+  int k = 0;
+  for (int i = 0; i < m; i++)
+    if (i == 0 || c[i] != c[i - 1]) c[k++] = c[i];
+  deg[u] = k;
+}
+
+// ------------------------------------------------------------------ RCM (one CTA)
+
+struct RcmWork {
+  int n;
+  const long long *row;  // row start; row[u] + deg[u] = end
+  const int *deg;
+  const int *col;
+  int *newidx;           // CM position of each vertex, -1 = unvisited
+  int *mark;             // BFS stamp of the pseudo-peripheral search
+  int *lev_a, *lev_b;    // current and next level
+  int *pkey;             // first-parent position of a discovered vertex (INT_MAX = none)
+  unsigned long long *keys;  // sort buffer (n entries, for levels that do not fit in smem)
+  int *status;           // [0] = vertices ordered, [1] = error
+};
+
+constexpr int kRcmThreads = 1024;
+constexpr int kRcmSmemKeys = 4096;
+
+__device__ void rcm_sort(unsigned long long *k, int len) {
+  int pad = 1;
+  while (pad < len) pad <<= 1;
+  for (int i = len + threadIdx.x; i < pad; i += blockDim.x) k[i] = ~0ull;
+  __syncthreads();
+  for (int kk = 2; kk <= pad; kk <<= 1)
+    for (int j = kk >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < pad; i += blockDim.x) {
+        int ixj = i ^ j;
+        if (ixj > i) {
+          unsigned long long x = k[i], y = k[ixj];
+          if ((x > y) == ((i & kk) == 0)) {
+            k[i] = y;
+            k[ixj] = x;
+          }
+        }
+      }
+      __syncthreads();
+    }
+}
+
+// BFS from `start` over vertices not yet ordered; marks with `stamp`.
+// Returns the number of levels; the last level is left in *last (lev_a or lev_b).
+__device__ int rcm_bfs(RcmWork &w, int start, int stamp, int **last, int *last_len) {
+  __shared__ int s_len, s_next;
+  int *cur = w.lev_a, *nxt = w.lev_b;
+  if (threadIdx.x == 0) {
+    cur[0] = start;
+    w.mark[start] = stamp;
+    s_len = 1;
+  }
+  __syncthreads();
+  int nlev = 0;
+  while (true) {
+    int len = s_len;
+    nlev++;
+    if (threadIdx.x == 0) s_next = 0;
+    __syncthreads();
+    for (int j = threadIdx.x; j < len; j += blockDim.x) {
+      int u = cur[j];
+      long long r = w.row[u];
+      int d = w.deg[u];
+      for (int t = 0; t < d; t++) {
+        int v = w.col[r + t];
+        if (w.newidx[v] < 0 && atomicExch(&w.mark[v], stamp) != stamp) nxt[atomicAdd(&s_next, 1)] = v;
+      }
+    }
+    __syncthreads();
+    int nl = s_next;
+    if (nl == 0) {
+      *last = cur;
+      *last_len = len;
+      return nlev;
+    }
+    int *t = cur;
+    cur = nxt;
+    nxt = t;
+    if (threadIdx.x == 0) s_len = nl;
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kRcmThreads) k_rcm(RcmWork w) {
+  __shared__ unsigned long long s_keys[kRcmSmemKeys];
+  __shared__ int s_start, s_len, s_next, s_best, s_bestdeg;
+  __shared__ int s_pos;
+  int stamp = 1;
+  if (threadIdx.x == 0) s_pos = 0;
+  __syncthreads();
+  int scan_from = 0;
+  while (s_pos < w.n) {
+    // lowest unvisited vertex
+    if (threadIdx.x == 0) {
+      while (scan_from < w.n && w.newidx[scan_from] >= 0) scan_from++;
+      s_start = scan_from;
+    }
+    __syncthreads();
+    int start = s_start;
+    // George-Liu pseudo-peripheral vertex
+    int *last;
+    int last_len;
+    int ecc = rcm_bfs(w, start, stamp++, &last, &last_len);
+    for (int round = 0; round < 8; round++) {
+      if (threadIdx.x == 0) {
+        s_best = INT_MAX;
+        s_bestdeg = INT_MAX;
+      }
+      __syncthreads();
+      for (int j = threadIdx.x; j < last_len; j += blockDim.x) atomicMin(&s_bestdeg, w.deg[last[j]]);
+      __syncthreads();
+      for (int j = threadIdx.x; j < last_len; j += blockDim.x) {
+        int v = last[j];
+        if (w.deg[v] == s_bestdeg) atomicMin(&s_best, v);
+      }
+      __syncthreads();
+      int cand = s_best;
+      int e2 = rcm_bfs(w, cand, stamp++, &last, &last_len);
+      if (e2 <= ecc) break;  // no longer eccentricity: keep the current start
+      ecc = e2;
+      start = cand;
+    }
+    // Cuthill-McKee from `start`
+    int *cur = w.lev_a, *nxt = w.lev_b;
+    if (threadIdx.x == 0) {
+      cur[0] = start;
+      w.newidx[start] = s_pos++;
+      s_len = 1;
+    }
+    __syncthreads();
+    while (true) {
+      int len = s_len;
+      if (threadIdx.x == 0) s_next = 0;
+      __syncthreads();
+      // first parent (lowest position in this level) of every new vertex
+      for (int j = threadIdx.x; j < len; j += blockDim.x) {
+        int u = cur[j];
+        long long r = w.row[u];
+        for (int t = 0; t < w.deg[u]; t++) {
+          int v = w.col[r + t];
+          if (w.newidx[v] < 0) atomicMin(&w.pkey[v], j);
+        }
+      }
+      __syncthreads();
+      for (int j = threadIdx.x; j < len; j += blockDim.x) {
+        int u = cur[j];
+        long long r = w.row[u];
+        for (int t = 0; t < w.deg[u]; t++) {
+          int v = w.col[r + t];
+          if (w.newidx[v] < 0 && w.pkey[v] == j) nxt[atomicAdd(&s_next, 1)] = v;
+        }
+      }
+      __syncthreads();
+      int nl = s_next;
+      if (nl == 0) break;
+      unsigned long long *keys = nl <= kRcmSmemKeys ? s_keys : w.keys;
+      for (int k = threadIdx.x; k < nl; k += blockDim.x) {
+        int v = nxt[k];
+        unsigned long long d = (unsigned)min(w.deg[v], 63);
+        keys[k] = ((unsigned long long)(unsigned)w.pkey[v] << 38) | (d << 32) | (unsigned)v;
+      }
+      __syncthreads();
+      rcm_sort(keys, nl);
+      int base = s_pos;
+      for (int k = threadIdx.x; k < nl; k += blockDim.x) {
+        int v = (int)(keys[k] & 0xffffffffull);
+        nxt[k] = v;
+        w.newidx[v] = base + k;
+        w.pkey[v] = INT_MAX;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        s_pos = base + nl;
+        s_len = nl;
+      }
+      int *t = cur;
+      cur = nxt;
+      nxt = t;
+      __syncthreads();
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) w.status[0] = s_pos;
+}
+
+// reverse: perm[v] = n - 1 - CM position
+__global__ void k_reverse(int n, const int *cm, int *perm) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < n) perm[v] = n - 1 - cm[v];
+}
+
+// ------------------------------------------------------------------ propagation
+
+// key of each `to` element: new index of its first target
+__global__ void k_first_target_key(int n, int dim, const int *map, const int *perm_from,
+                                   int *key, int *cnt) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int k = perm_from[map[(size_t)i * dim]];
+  key[i] = k;
+  atomicAdd(&cnt[k], 1);
+}
+
+__global__ void k_bucket_fill(int n, const int *key, const long long *start, int *fill,
+                              int *order) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int k = key[i];
+  order[start[k] + atomicAdd(&fill[k], 1)] = i;
+}
+
+// sort each bucket by original index (stable order); perm[order[p]] = p
+__global__ void k_bucket_sort(int nkeys, const long long *start, int *order, int *perm) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nkeys) return;
+  long long b = start[k], e = start[k + 1];
+  for (long long i = b + 1; i < e; i++) {
+    int v = order[i];
+    long long j = i - 1;
+    while (j >= b && order[j] > v) {
+      order[j + 1] = order[j];
+      j--;
+    }
+    order[j + 1] = v;
+  }
+  for (long long i = b; i < e; i++) perm[order[i]] = (int)i;
+}
+
+// first touch: the `to` element reached first when walking `from` in its new
+// order, slot by slot (:101-125) -- key = new position * dim + slot
+__global__ void k_first_touch(int nfrom, int dim, const int *map, const int *perm_from, int nto,
+                              int *key) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nfrom) return;
+  for (int d = 0; d < dim; d++) {
+    int t = map[(size_t)i * dim + d];
+    if (t >= 0 && t < nto) atomicMin(&key[t], (int)((long long)perm_from[i] * dim + d));
+  }
+}
+
+__global__ void k_flag_keys(int n, const int *key, int *flag, int *missing) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (key[i] == INT_MAX) atomicAdd(missing, 1);
+  else flag[key[i]] = 1;
+}
+
+__global__ void k_rank_keys(int n, const int *key, const long long *pos, int *perm) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) perm[i] = (int)pos[key[i]];
+}
+
+// ------------------------------------------------------------------ reordering
+
+__global__ void k_move_rows(int n, int words, const int *src, int *dst, const int *perm) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * words) return;
+  long long i = t / words, w = t % words;
+  dst[(size_t)perm[i] * words + w] = src[t];
+}
+
+__global__ void k_renumber_entries(long long m, int *map, const int *perm) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < m) map[t] = perm[map[t]];
+}
+
+__global__ void k_gather_rows(int n, int words, const int *src, int *dst, const int *perm,
+                              int low) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * words) return;
+  long long j = t / words, w = t % words;
+  dst[t] = src[(size_t)perm[low + j] * words + w];
+}
+
+// ------------------------------------------------------------------ host
+
+struct Renumbering {
+  std::map<int, int *> perm_d;  // set index -> device permutation (original -> current)
+};
+
+static Renumbering &ren() {
+  static Renumbering r;
+  return r;
+}
+
+static inline unsigned grid1(long long n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+// RCM order of the base map's target set; perm[v] = new index of v
+static bool base_rcm(op_map base, int *perm_d, cudaStream_t s) {
+  op_set to = base->to;
+  int n = to->size;
+  std::vector<void *> tmp;
+  auto A = [&](size_t bytes) {
+    void *p = nullptr;
+    if (cudaMalloc(&p, bytes ? bytes : 1) != cudaSuccess) return (void *)nullptr;
+    tmp.push_back(p);
+    return p;
+  };
+  auto cleanup = [&]() {
+    cudaStreamSynchronize(s);
+    for (void *p : tmp) cudaFree(p);
+  };
+  int *deg = (int *)A(sizeof(int) * (n + 1));
+  long long *row = (long long *)A(sizeof(long long) * (n + 1));
+  int *col = nullptr;
+  if (!deg || !row) return cleanup(), false;
+  cudaMemsetAsync(deg, 0, sizeof(int) * (n + 1), s);
+  if (base->from == to) {
+    col = (int *)A(sizeof(int) * (size_t)n * base->dim);
+    k_adj_self<<<grid1(n), 256, 0, s>>>(n, base->dim, base->map_d, deg, col);
+    // rows are dim apart
+    std::vector<long long> h(n + 1);
+    for (int u = 0; u <= n; u++) h[u] = (long long)u * base->dim;
+    cudaMemcpyAsync(row, h.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice, s);
+    cudaStreamSynchronize(s);
+  } else {
+    int nf = base->from->size;
+    k_adj_count<<<grid1(nf), 256, 0, s>>>(nf, base->dim, base->map_d, n, deg);
+    if (!scan_exclusive(deg, row, n, s)) return cleanup(), false;
+    long long nnz = 0;
+    cudaMemcpy(&nnz, row + n, sizeof(long long), cudaMemcpyDeviceToHost);
+    col = (int *)A(sizeof(int) * (size_t)std::max(nnz, 1LL));
+    int *fill = (int *)A(sizeof(int) * n);
+    cudaMemsetAsync(fill, 0, sizeof(int) * n, s);
+    k_adj_fill<<<grid1(nf), 256, 0, s>>>(nf, base->dim, base->map_d, n, row, fill, col);
+  }
+  k_adj_unique<<<grid1(n), 256, 0, s>>>(n, row, col, deg);
+  RcmWork w{};
+  w.n = n;
+  w.row = row;
+  w.deg = deg;
+  w.col = col;
+  w.newidx = (int *)A(sizeof(int) * n);
+  w.mark = (int *)A(sizeof(int) * n);
+  w.lev_a = (int *)A(sizeof(int) * n);
+  w.lev_b = (int *)A(sizeof(int) * n);
+  w.pkey = (int *)A(sizeof(int) * n);
+  w.keys = (unsigned long long *)A(sizeof(unsigned long long) * 2 * (size_t)std::max(n, 1));
+  w.status = (int *)A(sizeof(int) * 2);
+  if (!w.newidx || !w.mark || !w.lev_a || !w.lev_b || !w.pkey || !w.keys || !w.status)
+    return cleanup(), false;
+  cudaMemsetAsync(w.newidx, 0xff, sizeof(int) * n, s);
+  cudaMemsetAsync(w.mark, 0, sizeof(int) * n, s);
+  cudaMemsetAsync(w.pkey, 0x7f, sizeof(int) * n, s);  // 0x7f7f7f7f > any position
+  cudaMemsetAsync(w.status, 0, sizeof(int) * 2, s);
+  // pkey must read as "none": 0x7f7f7f7f is used as the no-parent value
+  k_rcm<<<1, kRcmThreads, 0, s>>>(w);
+  k_reverse<<<grid1(n), 256, 0, s>>>(n, w.newidx, perm_d);
+  int st[2] = {0, 0};
+  cudaMemcpyAsync(st, w.status, sizeof(st), cudaMemcpyDeviceToHost, s);
+  bool ok = cudaStreamSynchronize(s) == cudaSuccess && st[0] == n;
+  if (!ok) set_error("op_renumber: reverse Cuthill-McKee ordered %d of %d elements", st[0], n);
+  cleanup();
+  return ok;
+}
+
+// propagate_reordering (:72-151)
+static void propagate(op_set from, op_set to, std::vector<int *> &perm, cudaStream_t s,
+                      bool &ok) {
+  Runtime &r = rt();
+  if (!ok || to->size == 0) return;
+  int n = to->size;
+  if (!perm[to->index]) {
+    for (auto &mp : r.maps) {  // a map to -> from: sort by first target's new index
+      op_map m = mp.get();
+      if (!m || m->to != from || m->from != to) continue;
+      int *key, *cnt, *fill, *order, *pd;
+      long long *start;
+      int nk = from->size;
+      cudaMalloc(&key, sizeof(int) * n);
+      cudaMalloc(&cnt, sizeof(int) * (nk + 1));
+      cudaMalloc(&fill, sizeof(int) * (nk + 1));
+      cudaMalloc(&order, sizeof(int) * n);
+      cudaMalloc(&start, sizeof(long long) * (nk + 1));
+      cudaMalloc(&pd, sizeof(int) * n);
+      cudaMemsetAsync(cnt, 0, sizeof(int) * (nk + 1), s);
+      cudaMemsetAsync(fill, 0, sizeof(int) * (nk + 1), s);
+      k_first_target_key<<<grid1(n), 256, 0, s>>>(n, m->dim, m->map_d, perm[from->index], key, cnt);
+      ok = scan_exclusive(cnt, start, nk, s);
+      k_bucket_fill<<<grid1(n), 256, 0, s>>>(n, key, start, fill, order);
+      k_bucket_sort<<<grid1(nk), 256, 0, s>>>(nk, start, order, pd);
+      ok = ok && cudaStreamSynchronize(s) == cudaSuccess;
+      cudaFree(key);
+      cudaFree(cnt);
+      cudaFree(fill);
+      cudaFree(order);
+      cudaFree(start);
+      perm[to->index] = pd;
+      break;
+    }
+  }
+  if (!perm[to->index]) {
+    for (auto &mp : r.maps) {  // a map from -> to covering `to`: first touch
+      op_map m = mp.get();
+      if (!m || m->to != to || m->from != from) continue;
+      int *key, *flag, *missing, *pd;
+      long long *pos;
+      long long nslots = (long long)from->size * m->dim;
+      cudaMalloc(&key, sizeof(int) * n);
+      cudaMalloc(&flag, sizeof(int) * (nslots + 1));
+      cudaMalloc(&missing, sizeof(int));
+      cudaMalloc(&pos, sizeof(long long) * (nslots + 1));
+      cudaMemsetAsync(key, 0x7f, sizeof(int) * n, s);
+      cudaMemsetAsync(flag, 0, sizeof(int) * (nslots + 1), s);
+      cudaMemsetAsync(missing, 0, sizeof(int), s);
+      // 0x7f7f7f7f stands for "not reached"; map the sentinel to INT_MAX
+      k_first_touch<<<grid1(from->size), 256, 0, s>>>(from->size, m->dim, m->map_d,
+                                                       perm[from->index], n, key);
+      std::vector<int> hk(n);
+      cudaMemcpyAsync(hk.data(), key, sizeof(int) * n, cudaMemcpyDeviceToHost, s);
+      cudaStreamSynchronize(s);
+      int nmiss = 0;
+      for (int i = 0; i < n; i++) nmiss += hk[i] == 0x7f7f7f7f;
+      if (nmiss) {  // not onto: try the next map (:113-117)
+        cudaFree(key);
+        cudaFree(flag);
+        cudaFree(missing);
+        cudaFree(pos);
+        continue;
+      }
+      k_flag_keys<<<grid1(n), 256, 0, s>>>(n, key, flag, missing);
+      ok = scan_exclusive(flag, pos, nslots, s);
+      cudaMalloc(&pd, sizeof(int) * n);
+      k_rank_keys<<<grid1(n), 256, 0, s>>>(n, key, pos, pd);
+      ok = ok && cudaStreamSynchronize(s) == cudaSuccess;
+      cudaFree(key);
+      cudaFree(flag);
+      cudaFree(missing);
+      cudaFree(pos);
+      perm[to->index] = pd;
+      break;
+    }
+  }
+  if (!perm[to->index]) return;
+  for (auto &mp : r.maps) {  // maps (*) -> to
+    op_map m = mp.get();
+    if (m && m->to == to && !perm[m->from->index]) propagate(to, m->from, perm, s, ok);
+  }
+  for (auto &mp : r.maps) {  // maps to -> (*)
+    op_map m = mp.get();
+    if (m && m->from == to && !perm[m->to->index]) propagate(to, m->to, perm, s, ok);
+  }
+}
+
+static void bandwidth(op_map base, long &mx, long &avg) {
+  mx = 0;
+  avg = 0;
+  int n = base->from->size, d = base->dim;
+  for (int i = 0; i < n; i++) {
+    long dist = 0;
+    for (int a = 0; a < d; a++)
+      for (int b = 0; b < d; b++)
+        dist = std::max(dist, (long)std::abs(base->map[(size_t)i * d + a] - base->map[(size_t)i * d + b]));
+    mx = std::max(mx, dist);
+    avg += dist;
+  }
+  if (n) avg /= n;
+}
+
+int renumber(op_map base, long stats[4]) {
+  Runtime &r = rt();
+  if (!r.ready()) return -1;
+  if (!base || !base->map_d) {
+    set_error("op_renumber: invalid base map");
+    return -1;
+  }
+  cudaStream_t s = r.stream;
+  cudaStreamSynchronize(s);
+  long bmx, bavg;
+  bandwidth(base, bmx, bavg);
+  std::vector<int *> perm(r.sets.size(), nullptr);
+  op_set to = base->to;
+  int *pb = nullptr;
+  if (cudaMalloc(&pb, sizeof(int) * std::max(to->size, 1)) != cudaSuccess) {
+    set_error("op_renumber: out of device memory");
+    return -1;
+  }
+  perm[to->index] = pb;
+  if (!base_rcm(base, pb, s)) {
+    cudaFree(pb);
+    return -1;
+  }
+  bool ok = true;
+  propagate(to, to, perm, s, ok);
+  if (!ok) {
+    set_error("op_renumber: propagation failed");
+    for (int *p : perm) cudaFree(p);
+    return -1;
+  }
+  // reorder_set (:153-222) for every set that received a permutation
+  for (auto &sp : r.sets) {
+    op_set set = sp.get();
+    if (!set || !perm[set->index] || set->size == 0) continue;
+    const int *pd = perm[set->index];
+    for (auto &mp : r.maps) {
+      op_map m = mp.get();
+      if (!m || !m->map_d) continue;
+      if (m->from == set) {
+        int *t;
+        size_t bytes = sizeof(int) * (size_t)set->size * m->dim;
+        cudaMalloc(&t, bytes);
+        k_move_rows<<<grid1((long long)set->size * m->dim), 256, 0, s>>>(set->size, m->dim, m->map_d,
+                                                                          t, pd);
+        cudaMemcpyAsync(m->map_d, t, bytes, cudaMemcpyDeviceToDevice, s);
+        cudaStreamSynchronize(s);
+        cudaFree(t);
+      }
+    }
+    for (auto &mp : r.maps) {
+      op_map m = mp.get();
+      if (!m || !m->map_d || m->to != set) continue;
+      long long cnt = (long long)m->from->size * m->dim;
+      k_renumber_entries<<<grid1(cnt), 256, 0, s>>>(cnt, m->map_d, pd);
+    }
+    for (auto &dp : r.dats) {
+      op_dat d = dp.get();
+      if (!d || d->set != set || !d->data_d) continue;
+      if (d->size % 4) {
+        set_error("op_renumber: dat %s has elements of %d bytes (not a multiple of 4)", d->name,
+                  d->size);
+        ok = false;
+        continue;
+      }
+      int words = d->size / 4;
+      size_t bytes = (size_t)set->size * d->size;
+      int *t;
+      cudaMalloc(&t, bytes);
+      k_move_rows<<<grid1((long long)set->size * words), 256, 0, s>>>(
+          set->size, words, reinterpret_cast<const int *>(d->data_d), t, pd);
+      cudaMemcpyAsync(d->data_d, t, bytes, cudaMemcpyDeviceToDevice, s);
+      cudaStreamSynchronize(s);
+      cudaFree(t);
+    }
+  }
+  // host copies of the maps follow the device
+  for (auto &mp : r.maps) {
+    op_map m = mp.get();
+    if (m && m->map_d && m->map)
+      cudaMemcpy(m->map, m->map_d, sizeof(int) * (size_t)m->from->size * m->dim,
+                 cudaMemcpyDeviceToHost);
+  }
+  // compose with earlier renumberings: original -> current
+  for (auto &sp : r.sets) {
+    op_set set = sp.get();
+    if (!set || !perm[set->index]) continue;
+    auto it = ren().perm_d.find(set->index);
+    if (it == ren().perm_d.end()) {
+      ren().perm_d[set->index] = perm[set->index];
+    } else {
+      // current = perm[old current]
+      long long n = set->size;
+      int *t = it->second;
+      k_renumber_entries<<<grid1(n), 256, 0, s>>>(n, t, perm[set->index]);
+      cudaStreamSynchronize(s);
+      cudaFree(perm[set->index]);
+    }
+  }
+  release_plans();  // plans refer to the old numbering
+  bool good = cuda_ok(cudaStreamSynchronize(s), "op_renumber") && ok;
+  long amx, aavg;
+  bandwidth(base, amx, aavg);
+  if (stats) {
+    stats[0] = bmx;
+    stats[1] = bavg;
+    stats[2] = amx;
+    stats[3] = aavg;
+  }
+  if (r.opt_diags > 1) {
+    printf("Before renumbering: maximum bandwidth = %ld average bandwidth = %ld\n", bmx, bavg);
+    printf("After renumbering: maximum bandwidth = %ld average bandwidth = %ld\n", amx, aavg);
+  }
+  return good ? 0 : -1;
+}
+
+void resolve_renumbering_for_fetch(op_dat) {}
+
+void fetch_original_order(op_dat dat, char *dst, int low, int high) {
+  Runtime &r = rt();
+  if (!r.ready() || high < low) return;
+  size_t cnt = (size_t)(high - low + 1);
+  size_t bytes = cnt * dat->size;
+  auto it = ren().perm_d.find(dat->set->index);
+  if (it == ren().perm_d.end() || dat->size % 4) {
+    cudaMemcpyAsync(dst, dat->data_d + (size_t)low * dat->size, bytes, cudaMemcpyDeviceToHost,
+                    r.stream);
+    cuda_ok(cudaStreamSynchronize(r.stream), "op_fetch_data_idx");
+    return;
+  }
+  int *t = nullptr;
+  if (!cuda_ok(cudaMalloc(&t, bytes), "op_fetch_data_idx")) return;
+  int words = dat->size / 4;
+  k_gather_rows<<<grid1((long long)cnt * words), 256, 0, r.stream>>>(
+      (int)cnt, words, reinterpret_cast<const int *>(dat->data_d), t, it->second, low);
+  cudaMemcpyAsync(dst, t, bytes, cudaMemcpyDeviceToHost, r.stream);
+  cuda_ok(cudaStreamSynchronize(r.stream), "op_fetch_data_idx");
+  cudaFree(t);
+}
+
+void release_renumbering() {
+  for (auto &kv : ren().perm_d) cudaFree(kv.second);
+  ren().perm_d.clear();
+}
+
+int set_permutation(op_set set, int *host_perm) {
+  auto it = ren().perm_d.find(set->index);
+  if (it == ren().perm_d.end()) {
+    for (int i = 0; i < set->size; i++) host_perm[i] = i;
+    return 1;
+  }
+  return cuda_ok(cudaMemcpy(host_perm, it->second, sizeof(int) * (size_t)set->size,
+                            cudaMemcpyDeviceToHost),
+                 "op2b_set_permutation")
+             ? 0
+             : -1;
+}
+
+}  // namespace op2b
+
+using namespace op2b;
+
+extern "C" {
+
+void op_renumber(op_map base) {
+  if (renumber(base, nullptr) != 0 && !rt().opt_abort)
+    fprintf(stderr, "op2b: %s\n", op2b_last_error());
+}
+
+void op_renumber_ptr(int *ptr) {
+  auto it = rt().map_ptrs.find(ptr);
+  if (it == rt().map_ptrs.end()) {
+    set_error("op_renumber: op_map not found for %p pointer", (void *)ptr);
+    fprintf(stderr, "op2b: %s\n", op2b_last_error());
+    return;
+  }
+  op_renumber(it->second);
+}
+
+int op2b_renumber(op_map base, long stats[4]) { return renumber(base, stats); }
+
+int op2b_set_permutation(op_set set, int *perm) {
+  if (!set || !perm) {
+    set_error("op2b_set_permutation: invalid arguments");
+    return -1;
+  }
+  return set_permutation(set, perm);
+}
+
+}  // extern "C"

@@ -112,6 +112,15 @@ class Airfoil:
                 hist.append((r, float(self.maxerr[0]), int(self.errloc[0])))
         return hist
 
+    def renumber(self):
+        """op_renumber(pecell): RCM on the cell graph, propagated to edges,
+        boundary edges and nodes (the call the reference's MPI Airfoil makes)."""
+        return L.op_renumber(self.pecell)
+
+    def fetch_original(self):
+        """q in the order the cells were declared (op_fetch_data_idx)."""
+        return L.op_fetch_data_idx(self.p_q, 0, self.mesh.ncell - 1)
+
     def fetch(self):
         return dict(q=L.op_fetch_data(self.p_q), qold=L.op_fetch_data(self.p_qold),
                     res=L.op_fetch_data(self.p_res), adt=L.op_fetch_data(self.p_adt)[:, 0])

@@ -165,7 +165,29 @@ _SIGS.update({
     "op2b_plan_device_blkmap": (ctypes.c_void_p, [ctypes.POINTER(op_plan)]),
     "op2b_plan_device_thrcol": (ctypes.c_void_p, [ctypes.POINTER(op_plan)]),
     "op2b_plan_release_all": (None, []),
+    "op_renumber": (None, [op_map]),
+    "op_renumber_ptr": (None, [ctypes.c_void_p]),
+    "op2b_renumber": (ctypes.c_int, [op_map, ctypes.POINTER(ctypes.c_long)]),
+    "op2b_set_permutation": (ctypes.c_int, [op_set, ctypes.c_void_p]),
 })
+
+
+def op_renumber(base):
+    """Renumber the mesh from `base` (GPU reverse Cuthill-McKee); returns the
+    base map's bandwidth (max, avg) before and after."""
+    st = (ctypes.c_long * 4)()
+    if load().op2b_renumber(base, st) != 0:
+        _check(False, "op_renumber")
+    return dict(before_max=st[0], before_avg=st[1], after_max=st[2], after_avg=st[3])
+
+
+def set_permutation(set_) -> np.ndarray:
+    """perm[i] = current index of the element declared as i."""
+    n = set_.contents.size
+    out = np.zeros(max(n, 1), np.int32)
+    if load().op2b_set_permutation(set_, out.ctypes.data) < 0:
+        _check(False, "op2b_set_permutation")
+    return out[:n]
 
 
 def op_plan_get_stage(name: str, set_, part_size: int, args, inds, staging: int):

@@ -141,6 +141,32 @@ def loop(name: str, mesh, consts: dict, st: State, dtype=np.float64):
     return None
 
 
+def airfoil_maps(mesh):
+    """Airfoil's sets and maps in the reference's declaration order
+    (airfoil.cpp:175-189): sets nodes, edges, bedges, cells; maps pedge,
+    pecell, pbedge, pbecell, pcell."""
+    sizes = [mesh.nnode, mesh.nedge, mesh.nbedge, mesh.ncell]
+    maps = [(1, 0, 2, mesh.edge), (1, 3, 2, mesh.ecell), (2, 0, 2, mesh.bedge),
+            (2, 3, 1, mesh.becell), (3, 0, 4, mesh.cell)]
+    return sizes, maps
+
+
+def renumber(sizes, maps, base: int):
+    """Restated renumbering: returns [perm or None per set], perm[i] = new index."""
+    L = lib()
+    nsets, nmaps = len(sizes), len(maps)
+    set_size = np.array(sizes, np.int32)
+    flat = np.array([[f, t, d] for f, t, d, _ in maps], np.int32).ravel()
+    datas = [np.ascontiguousarray(m, np.int32).ravel() for *_, m in maps]
+    ptrs = (ctypes.POINTER(ctypes.c_int) * nmaps)(*[_p(d, _ip) for d in datas])
+    outs = [np.zeros(max(s, 1), np.int32) for s in sizes]
+    optrs = (ctypes.POINTER(ctypes.c_int) * nsets)(*[_p(o, _ip) for o in outs])
+    has = np.zeros(nsets, np.int32)
+    L.orc_renumber(nsets, _p(set_size, _ip), nmaps, _p(flat, _ip), ptrs, base, optrs,
+                   _p(has, _ip))
+    return [outs[s][:sizes[s]] if has[s] else None for s in range(nsets)]
+
+
 # ---------------------------------------------------------------- reference builds
 
 def ref_binary(name: str) -> str | None:
