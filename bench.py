@@ -15,8 +15,8 @@ max over ranks.  Prints one JSON line on rank 0.
              synchronize on both sides).  The working set (~0.7 GB) is larger
              than the 126 MB L2, so no flush is needed between iterations.
              Default configuration: the mesh renumbered on the GPU
-             (op_renumber, reverse Cuthill-McKee) and the staged-hybrid
-             increment strategy.
+             (op_renumber, reverse Cuthill-McKee) and the owner-computes
+             (gather) increment strategy.
 * e2e        the whole job through the public API with host buffers, per
              iteration: op_decl_* uploads from pinned host memory, op_renumber,
              K iterations, op_fetch_data of q.
@@ -58,8 +58,8 @@ def parse():
     p.add_argument("--mesh", type=int, nargs=2, default=[2400, 1200])
     p.add_argument("--seed", type=int, default=1)
     p.add_argument("--numbering", default="rcm", choices=["rcm", "random"])
-    p.add_argument("--inc-mode", type=int, default=2,
-                   help="0 atomics, 1 block/thread colouring, 2 staged hybrid")
+    p.add_argument("--inc-mode", type=int, default=3,
+                   help="0 atomics, 1 block/thread colouring, 2 staged hybrid, 3 gather")
     p.add_argument("--part-size", type=int, default=0)
     p.add_argument("--precision", default="f64", choices=["f64", "mixed"])
     p.add_argument("--no-e2e", action="store_true")
@@ -285,7 +285,7 @@ def main():
     variants = []
     if not args.no_variants:
         for numbering in ("random", "rcm"):
-            for mode in (0, 1, 2):
+            for mode in (0, 1, 2, 3):
                 if numbering == "random" and mode == 1:
                     continue  # hundreds of block colours: one launch each
                 v = timed_run(L, Airfoil, m, dtype, numbering, mode, args.part_size, 20, 3, torch,

@@ -205,6 +205,10 @@ void *op2b_map_device_ptr(op_map map);
 #define OP2B_INC_ATOMIC 0
 #define OP2B_INC_COLOR 1
 #define OP2B_INC_HYBRID 2
+/* 3 = owner computes: each target element sums its increments, in element
+ * order, through the map's inverse (no atomics, no colours; bit-exact with
+ * the reference's sequential loop on the same numbering). */
+#define OP2B_INC_GATHER 3
 int op2b_set_option(const char *key, long value);
 long op2b_get_option(const char *key);
 

@@ -228,6 +228,7 @@ void op_exit(void) {
   if (!r.initialised) return;
   cudaStreamSynchronize(r.stream);
   release_plans();
+  release_inverse_maps();
   release_renumbering();
   for (auto &d : r.dats)
     if (d) {
@@ -693,8 +694,8 @@ int op2b_set_option(const char *key, long value) {
   Runtime &r = rt();
   std::string k = key ? key : "";
   if (k == "inc_mode") {
-    if (value < 0 || value > 2) {
-      set_error("op2b_set_option: inc_mode must be 0, 1 or 2");
+    if (value < 0 || value > 3) {
+      set_error("op2b_set_option: inc_mode must be 0, 1, 2 or 3");
       return -1;
     }
     r.opt_inc_mode = (int)value;

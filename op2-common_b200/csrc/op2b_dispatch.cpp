@@ -12,6 +12,7 @@
 #include <string>
 
 #include "op2b_runtime.h"
+#include "gather.h"
 #include "staged.h"
 
 using namespace op2b;
@@ -199,7 +200,11 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
   int E = set->size, N = a[0].dat->set->size, C = a[2].dat->set->size;
   double bytes = 16.0 * E + (double)rb * (2.0 * N + 13.0 * C);
   Plan *plan = nullptr;
-  if (r.opt_inc_mode != OP2B_INC_ATOMIC) {
+  const InvMap *inv = nullptr;
+  if (r.opt_inc_mode == OP2B_INC_GATHER) {
+    inv = get_inverse_map(pecell);
+    if (!inv) return -1;
+  } else if (r.opt_inc_mode != OP2B_INC_ATOMIC) {
     plan = get_res_plan(name, set, nargs, a);
     if (!plan) return -1;
   }
@@ -212,7 +217,9 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
                           (const double *)a[2].dat->data_d, (const double *)a[4].dat->data_d,
                           (double *)a[6].dat->data_d, k};
     r.begin_loop(name);
-    e = run_res_calc<double>(r.ctx(), p, plan, r.opt_inc_mode);
+    e = inv ? launch_res_calc_gather<double>(r.ctx(), *inv, p.pedge, p.pecell, p.x, p.q, p.adt,
+                                             p.res, k)
+            : run_res_calc<double>(r.ctx(), p, plan, r.opt_inc_mode);
   } else {
     AirConst<float> k = air_consts<float>(ok);
     if (!ok) return -1;
@@ -220,7 +227,9 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
                          (const float *)a[2].dat->data_d, (const float *)a[4].dat->data_d,
                          (float *)a[6].dat->data_d, k};
     r.begin_loop(name);
-    e = run_res_calc<float>(r.ctx(), p, plan, r.opt_inc_mode);
+    e = inv ? launch_res_calc_gather<float>(r.ctx(), *inv, p.pedge, p.pecell, p.x, p.q, p.adt,
+                                            p.res, k)
+            : run_res_calc<float>(r.ctx(), p, plan, r.opt_inc_mode);
   }
   r.end_loop(bytes);
   return finish(e, name);
@@ -248,7 +257,11 @@ int loop_bres_calc(const char *name, op_set set, int nargs, op_arg *a) {
   int B = set->size;
   double bytes = 16.0 * B + (double)rb * (2.0 + 4.0 + 1.0 + 8.0) * B;
   Plan *plan = nullptr;
-  if (r.opt_inc_mode == OP2B_INC_COLOR) {
+  const InvMap *inv = nullptr;
+  if (r.opt_inc_mode == OP2B_INC_GATHER) {
+    inv = get_inverse_map(pbecell);
+    if (!inv) return -1;
+  } else if (r.opt_inc_mode == OP2B_INC_COLOR) {
     plan = get_bres_plan(name, set, nargs, a);
     if (!plan) return -1;
   }
@@ -261,7 +274,9 @@ int loop_bres_calc(const char *name, op_set set, int nargs, op_arg *a) {
                            (const double *)a[0].dat->data_d, (const double *)a[2].dat->data_d,
                            (const double *)a[3].dat->data_d, (double *)a[4].dat->data_d, k};
     r.begin_loop(name);
-    e = run_bres_calc<double>(r.ctx(), p, plan, r.opt_inc_mode);
+    e = inv ? launch_bres_calc_gather<double>(r.ctx(), *inv, p.pbedge, p.bound, p.x, p.q, p.adt,
+                                              p.res, k)
+            : run_bres_calc<double>(r.ctx(), p, plan, r.opt_inc_mode);
   } else {
     AirConst<float> k = air_consts<float>(ok);
     if (!ok) return -1;
@@ -269,7 +284,9 @@ int loop_bres_calc(const char *name, op_set set, int nargs, op_arg *a) {
                           (const float *)a[0].dat->data_d, (const float *)a[2].dat->data_d,
                           (const float *)a[3].dat->data_d, (float *)a[4].dat->data_d, k};
     r.begin_loop(name);
-    e = run_bres_calc<float>(r.ctx(), p, plan, r.opt_inc_mode);
+    e = inv ? launch_bres_calc_gather<float>(r.ctx(), *inv, p.pbedge, p.bound, p.x, p.q, p.adt,
+                                             p.res, k)
+            : run_bres_calc<float>(r.ctx(), p, plan, r.opt_inc_mode);
   }
   r.end_loop(bytes);
   return finish(e, name);

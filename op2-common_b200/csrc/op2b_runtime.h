@@ -43,7 +43,7 @@ struct Runtime {
   int opt_part_size = 0;
   int opt_cache_line = 128;
   int opt_maps_base = 0;
-  int opt_inc_mode = OP2B_INC_ATOMIC;
+  int opt_inc_mode = OP2B_INC_GATHER;
   int opt_plan_mode = 0;      // 0 = parallel block colouring, 1 = serial greedy (bit-exact)
   bool opt_check_plans = false;
 
@@ -85,5 +85,7 @@ void fetch_original_order(op_dat dat, char *dst, int low, int high);
 void release_renumbering();
 // plan.cu
 void release_plans();
+// airfoil_gather.cu
+void release_inverse_maps();
 
 }  // namespace op2b

@@ -704,7 +704,8 @@ int renumber(op_map base, long stats[4]) {
       cudaFree(perm[set->index]);
     }
   }
-  release_plans();  // plans refer to the old numbering
+  release_plans();  // plans and inverse maps refer to the old numbering
+  release_inverse_maps();
   bool good = cuda_ok(cudaStreamSynchronize(s), "op_renumber") && ok;
   long amx, aavg;
   bandwidth(base, amx, aavg);

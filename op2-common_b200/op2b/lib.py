@@ -19,7 +19,7 @@ import numpy as np
 OP_READ, OP_WRITE, OP_RW, OP_INC, OP_MIN, OP_MAX, OP_WORK = range(7)
 OP_ARG_GBL, OP_ARG_DAT, OP_ARG_IDX, OP_ARG_INFO = range(4)
 OP_STAGE_NONE, OP_STAGE_INC, OP_STAGE_ALL, OP_STAGE_PERMUTE, OP_COLOR2 = range(5)
-OP2B_INC_ATOMIC, OP2B_INC_COLOR, OP2B_INC_HYBRID = range(3)
+OP2B_INC_ATOMIC, OP2B_INC_COLOR, OP2B_INC_HYBRID, OP2B_INC_GATHER = range(4)
 OP_ID = None
 OP_GBL = None
 

@@ -21,7 +21,7 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-MODES = [L.OP2B_INC_ATOMIC, L.OP2B_INC_COLOR, L.OP2B_INC_HYBRID]
+MODES = [L.OP2B_INC_ATOMIC, L.OP2B_INC_COLOR, L.OP2B_INC_HYBRID, L.OP2B_INC_GATHER]
 
 
 def _state_after(m, c, niter):
@@ -115,15 +115,40 @@ def test_colouring_is_deterministic_and_matches_atomics(op2, part):
     m = M.channel_bump(300, 150, seed=8)
     op2.set_option("part_size", part)
     runs = {}
-    for mode in (L.OP2B_INC_ATOMIC, L.OP2B_INC_COLOR, L.OP2B_INC_COLOR, L.OP2B_INC_HYBRID):
+    for mode in (L.OP2B_INC_ATOMIC, L.OP2B_INC_COLOR, L.OP2B_INC_COLOR, L.OP2B_INC_HYBRID,
+                 L.OP2B_INC_GATHER):
         op2.set_option("inc_mode", mode)
         app = Airfoil(m)
         hist = app.iterate(20)
         runs.setdefault(mode, []).append(np.array([h[0] for h in hist]))
     c1, c2 = runs[L.OP2B_INC_COLOR]
     assert np.array_equal(c1, c2), "colouring must be deterministic"
-    for mode in (L.OP2B_INC_ATOMIC, L.OP2B_INC_HYBRID):
+    for mode in (L.OP2B_INC_ATOMIC, L.OP2B_INC_HYBRID, L.OP2B_INC_GATHER):
         assert np.max(np.abs(runs[mode][0] / c1 - 1)) < 1e-12
+
+
+@pytest.mark.parametrize("fixture", ["airfoil_24x12_s3.npz", "airfoil_240x120_s1.npz"])
+def test_gather_mode_is_bit_exact_with_reference(op2, fixture):
+    """inc_mode 3 adds each cell's increments in element order starting from
+    res, as the reference's sequential loop does: q after 100 iterations is
+    bit-identical to the reference's own build (rms differs only by the order
+    of its global sum)."""
+    op2.set_option("inc_mode", L.OP2B_INC_GATHER)
+    gd = np.load(f"{GOLDEN}/{fixture}")
+    m = M.channel_bump(int(gd["I"]), int(gd["J"]), seed=int(gd["seed"]))
+    app = Airfoil(m)
+    hist = app.iterate(int(gd["niter"]))
+    g = app.fetch()
+    if "q" in gd:
+        assert np.array_equal(g["q"], gd["q"])
+        assert np.array_equal(g["adt"], gd["adt"])
+    else:
+        assert np.array_equal(g["q"][gd["q_sample_idx"]], gd["q_sample"])
+        assert np.array_equal(g["q"].sum(axis=0), gd["q_sum"])
+    assert np.array_equal(np.array([h[1] for h in hist]), gd["maxerr"])
+    assert np.array_equal(np.array([h[2] for h in hist]), gd["errloc"])
+    # the rms sum over ~1e5 terms in a different order: ~1e-14 relative
+    assert np.max(np.abs(np.array([h[0] for h in hist]) / gd["rms"] - 1)) < 1e-13
 
 
 def test_large_mesh_one_iteration_against_oracle(op2):

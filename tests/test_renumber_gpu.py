@@ -45,7 +45,8 @@ def test_permutations_match_restatement(op2, I, J, seed):
     assert np.array_equal(cur, expect)
 
 
-@pytest.mark.parametrize("mode", [L.OP2B_INC_ATOMIC, L.OP2B_INC_COLOR, L.OP2B_INC_HYBRID])
+@pytest.mark.parametrize("mode", [L.OP2B_INC_ATOMIC, L.OP2B_INC_COLOR, L.OP2B_INC_HYBRID,
+                                  L.OP2B_INC_GATHER])
 def test_renumbered_run_matches_reference_golden(op2, mode):
     gd = np.load(f"{GOLDEN}/airfoil_240x120_s1.npz")
     m = M.channel_bump(240, 120, seed=1)
