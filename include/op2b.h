@@ -164,6 +164,13 @@ void op_timers(double *cpu, double *et);
 void op_timing_output(void);
 void op_diagnostic_output(void);
 void op_rank(int *rank);
+/* op_printf (op_lib_core.h:289) and the allocation wrappers (op_lib_core.h:
+ * 423-429): host memory, 64-byte aligned, for application code. */
+void op_printf(const char *format, ...);
+void *op_malloc(size_t size);
+void *op_calloc(size_t num, size_t size);
+void *op_realloc(void *ptr, size_t size);
+void op_free(void *ptr);
 
 /* ---- renumbering: op_renumber / op_renumber_ptr of
  * op2/src/externlib/op_renumber.cpp:224-516 (declared for MPI builds in the

@@ -105,7 +105,10 @@ static std::vector<std::unique_ptr<InvMapCache>> &inv_cache() {
   return v;
 }
 
-void release_inverse_maps() { inv_cache().clear(); }
+void release_inverse_maps() {
+  release_slot_records();
+  inv_cache().clear();
+}
 
 const InvMap *get_inverse_map(op_map map) {
   for (auto &c : inv_cache())
@@ -159,8 +162,8 @@ const InvMap *get_inverse_map(op_map map) {
 
 // ------------------------------------------------------------------ res_calc
 
-template <typename T>
-__global__ void __launch_bounds__(256)
+template <typename T, int MINB>
+__global__ void __launch_bounds__(256, MINB)
 k_res_gather(InvMap inv, const int2 *__restrict__ pedge, const int2 *__restrict__ pecell,
              const T *__restrict__ x, const T *__restrict__ q, const T *__restrict__ adt,
              T *__restrict__ res, AirConst<T> k) {
@@ -201,12 +204,273 @@ cudaError_t launch_res_calc_gather(const LaunchCtx &c, const InvMap &inv, const 
                                    const int *pecell, const T *x, const T *q, const T *adt,
                                    T *res, const AirConst<T> &k) {
   if (inv.nrows <= 0) return cudaSuccess;
-  k_res_gather<T><<<(inv.nrows + 255) / 256, 256, 0, c.stream>>>(
-      inv, reinterpret_cast<const int2 *>(pedge), reinterpret_cast<const int2 *>(pecell), x, q,
-      adt, res, k);
+  unsigned g = (inv.nrows + 255) / 256;
+  const int2 *pe = reinterpret_cast<const int2 *>(pedge);
+  const int2 *pc = reinterpret_cast<const int2 *>(pecell);
+  switch (rt().opt_gather_minb) {  // occupancy / register trade-off (tuning)
+    case 4: k_res_gather<T, 4><<<g, 256, 0, c.stream>>>(inv, pe, pc, x, q, adt, res, k); break;
+    case 5: k_res_gather<T, 5><<<g, 256, 0, c.stream>>>(inv, pe, pc, x, q, adt, res, k); break;
+    case 6: k_res_gather<T, 6><<<g, 256, 0, c.stream>>>(inv, pe, pc, x, q, adt, res, k); break;
+    default: k_res_gather<T, 1><<<g, 256, 0, c.stream>>>(inv, pe, pc, x, q, adt, res, k);
+  }
   c.count();
   return cudaGetLastError();
 }
+
+// ------------------------------------------------------------------ res_calc, 4 lanes per cell
+//
+// One thread per (cell, incident edge) slot, four slots per cell (quad
+// meshes; cells with fewer edges leave slots empty).  Slot records hold what
+// the thread needs directly -- the other cell and the edge's two nodes, with
+// the cell's role (first or second cell of the edge) and a valid bit in the
+// top bits of n2 -- in three coalesced int arrays, so every load of a thread
+// is independent of the others (two dependent steps instead of four).  Each
+// lane computes its edge's flux, negated when the cell is the edge's second
+// cell; lane 0 of the cell then adds the four lanes' increments to res[c] in
+// slot order, i.e. ascending edge order -- the sequential reference's order.
+
+constexpr unsigned kRoleBit = 1u << 30;
+constexpr unsigned kValidBit = 1u << 31;
+
+__global__ void k_build_slots(int ncell, const long long *off, const int *ent,
+                              const int2 *pedge, const int2 *pecell, int *rec_o, int *rec_n1,
+                              unsigned *rec_n2) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  long long b = off[c], e = off[c + 1];
+  for (int k = 0; k < 4; k++) {
+    size_t s = (size_t)c * 4 + k;
+    if (b + k < e) {
+      int en = ent[b + k];
+      int ed = en >> 1, slot = en & 1;
+      int2 cc = pecell[ed], nn = pedge[ed];
+      rec_o[s] = slot ? cc.x : cc.y;
+      rec_n1[s] = nn.x;
+      rec_n2[s] = (unsigned)nn.y | (slot ? kRoleBit : 0u) | kValidBit;
+    } else {
+      rec_o[s] = c;
+      rec_n1[s] = 0;
+      rec_n2[s] = 0u;
+    }
+  }
+}
+
+__global__ void k_max_degree(int ncell, const long long *off, int *mx) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < ncell) atomicMax(mx, (int)(off[c + 1] - off[c]));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_res_gather4(int ncell, const int *__restrict__ rec_o, const int *__restrict__ rec_n1,
+              const unsigned *__restrict__ rec_n2, const T *__restrict__ x,
+              const T *__restrict__ q, const T *__restrict__ adt, T *__restrict__ res,
+              AirConst<T> k) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = t >> 2, slot = t & 3;
+  const bool in = c < ncell;
+  unsigned r2 = in ? __ldg(rec_n2 + t) : 0u;
+  const bool valid = (r2 & kValidBit) != 0;
+  T g[4] = {(T)0, (T)0, (T)0, (T)0};
+  if (valid) {
+    int o = __ldg(rec_o + t), n1 = __ldg(rec_n1 + t), n2 = (int)(r2 & (kRoleBit - 1));
+    T qc[4], qo[4], x1x, x1y, x2x, x2y;
+    Vec<T>::ld4(q + 4 * (size_t)c, qc);
+    Vec<T>::ld4(q + 4 * (size_t)o, qo);
+    T ac = __ldg(adt + c), ao = __ldg(adt + o);
+    Vec<T>::ld2(x + 2 * (size_t)n1, x1x, x1y);
+    Vec<T>::ld2(x + 2 * (size_t)n2, x2x, x2y);
+    if (r2 & kRoleBit) {
+      air_flux<T>(x1x, x1y, x2x, x2y, qo, qc, ao, ac, k, g);
+#pragma unroll
+      for (int m = 0; m < 4; m++) g[m] = -g[m];  // acc - f == acc + (-f) exactly
+    } else {
+      air_flux<T>(x1x, x1y, x2x, x2y, qc, qo, ac, ao, k, g);
+    }
+  }
+  // lane 0 of each cell gathers its slots in order
+  T h[3][4];
+  bool v[3];
+#pragma unroll
+  for (int j = 1; j <= 3; j++) {
+#pragma unroll
+    for (int m = 0; m < 4; m++) h[j - 1][m] = __shfl_down_sync(0xffffffffu, g[m], j, 4);
+    v[j - 1] = __shfl_down_sync(0xffffffffu, (int)valid, j, 4);
+  }
+  if (in && slot == 0) {
+    T acc[4];
+    Vec<T>::ld4_rw(res + 4 * (size_t)c, acc);
+    if (valid) {
+#pragma unroll
+      for (int m = 0; m < 4; m++) acc[m] += g[m];
+    }
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+      if (v[j]) {
+#pragma unroll
+        for (int m = 0; m < 4; m++) acc[m] += h[j][m];
+      }
+    Vec<T>::st4(res + 4 * (size_t)c, acc);
+  }
+}
+
+// One thread per cell over the same slot records: the four records arrive as
+// three int4 loads, the loop over the slots is unrolled so every gather of the
+// cell is issued before the first flux, and the cell's own terms are computed
+// once.  Increments are added in slot order, starting from res[c].
+template <typename T, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+k_res_gather_cell4(int ncell, const int4 *__restrict__ rec_o, const int4 *__restrict__ rec_n1,
+                   const uint4 *__restrict__ rec_n2, const T *__restrict__ x,
+                   const T *__restrict__ q, const T *__restrict__ adt, T *__restrict__ res,
+                   AirConst<T> k) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  const int4 o4 = __ldg(rec_o + c), a4 = __ldg(rec_n1 + c);
+  const uint4 b4 = __ldg(rec_n2 + c);
+  const int o[4] = {o4.x, o4.y, o4.z, o4.w}, n1[4] = {a4.x, a4.y, a4.z, a4.w};
+  const unsigned r2[4] = {b4.x, b4.y, b4.z, b4.w};
+  T qc[4], acc[4];
+  Vec<T>::ld4(q + 4 * (size_t)c, qc);
+  T ac = __ldg(adt + c);
+  T qo[4][4], ao[4], xa[4][2], xb[4][2];
+#pragma unroll
+  for (int s = 0; s < 4; s++) {
+    const bool v = (r2[s] & kValidBit) != 0;
+    const int oo = v ? o[s] : c;
+    const int na = v ? n1[s] : 0, nb = v ? (int)(r2[s] & (kRoleBit - 1)) : 0;
+    Vec<T>::ld4(q + 4 * (size_t)oo, qo[s]);
+    ao[s] = __ldg(adt + oo);
+    Vec<T>::ld2(x + 2 * (size_t)na, xa[s][0], xa[s][1]);
+    Vec<T>::ld2(x + 2 * (size_t)nb, xb[s][0], xb[s][1]);
+  }
+  Vec<T>::ld4_rw(res + 4 * (size_t)c, acc);
+#pragma unroll
+  for (int s = 0; s < 4; s++) {
+    if (!(r2[s] & kValidBit)) continue;
+    T f[4];
+    if (r2[s] & kRoleBit) {
+      air_flux<T>(xa[s][0], xa[s][1], xb[s][0], xb[s][1], qo[s], qc, ao[s], ac, k, f);
+#pragma unroll
+      for (int m = 0; m < 4; m++) acc[m] -= f[m];
+    } else {
+      air_flux<T>(xa[s][0], xa[s][1], xb[s][0], xb[s][1], qc, qo[s], ac, ao[s], k, f);
+#pragma unroll
+      for (int m = 0; m < 4; m++) acc[m] += f[m];
+    }
+  }
+  Vec<T>::st4(res + 4 * (size_t)c, acc);
+}
+
+template <typename T>
+cudaError_t launch_res_calc_gather_cell4(const LaunchCtx &c, const SlotRecords &s, const T *x,
+                                         const T *q, const T *adt, T *res,
+                                         const AirConst<T> &k) {
+  if (s.ncell <= 0) return cudaSuccess;
+  unsigned g = (s.ncell + 255) / 256;
+  const int4 *o = reinterpret_cast<const int4 *>(s.o), *n1 = reinterpret_cast<const int4 *>(s.n1);
+  const uint4 *n2 = reinterpret_cast<const uint4 *>(s.n2);
+  switch (rt().opt_gather_minb) {  // occupancy / register trade-off (tuning)
+    case 2: k_res_gather_cell4<T, 2><<<g, 256, 0, c.stream>>>(s.ncell, o, n1, n2, x, q, adt, res, k); break;
+    case 3: k_res_gather_cell4<T, 3><<<g, 256, 0, c.stream>>>(s.ncell, o, n1, n2, x, q, adt, res, k); break;
+    case 4: k_res_gather_cell4<T, 4><<<g, 256, 0, c.stream>>>(s.ncell, o, n1, n2, x, q, adt, res, k); break;
+    default: k_res_gather_cell4<T, 1><<<g, 256, 0, c.stream>>>(s.ncell, o, n1, n2, x, q, adt, res, k);
+  }
+  c.count();
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_res_calc_gather_cell4<double>(const LaunchCtx &,
+                                                          const SlotRecords &, const double *,
+                                                          const double *, const double *,
+                                                          double *, const AirConst<double> &);
+template cudaError_t launch_res_calc_gather_cell4<float>(const LaunchCtx &, const SlotRecords &,
+                                                         const float *, const float *,
+                                                         const float *, float *,
+                                                         const AirConst<float> &);
+
+struct SlotCache {
+  op_map inc = nullptr, nodes = nullptr;
+  SlotRecords rec{};
+  std::vector<void *> owned;
+  ~SlotCache() {
+    for (void *p : owned) cudaFree(p);
+  }
+};
+
+static std::vector<std::unique_ptr<SlotCache>> &slot_cache() {
+  static std::vector<std::unique_ptr<SlotCache>> v;
+  return v;
+}
+
+const SlotRecords *get_slot_records(op_map pecell, op_map pedge) {
+  for (auto &s : slot_cache())
+    if (s->inc == pecell && s->nodes == pedge) return &s->rec;
+  const InvMap *inv = get_inverse_map(pecell);
+  if (!inv) return nullptr;
+  Runtime &r = rt();
+  cudaStream_t s = r.stream;
+  auto sc = std::make_unique<SlotCache>();
+  sc->inc = pecell;
+  sc->nodes = pedge;
+  int n = pecell->to->size;
+  int *mx = nullptr;
+  cudaMalloc(&mx, sizeof(int));
+  cudaMemsetAsync(mx, 0, sizeof(int), s);
+  unsigned g = (unsigned)((n + 255) / 256);
+  if (n > 0) k_max_degree<<<g, 256, 0, s>>>(n, inv->off, mx);
+  int h_mx = 0;
+  cudaMemcpyAsync(&h_mx, mx, sizeof(int), cudaMemcpyDeviceToHost, s);
+  bool ok = cuda_ok(cudaStreamSynchronize(s), "slot records");
+  cudaFree(mx);
+  if (!ok) return nullptr;
+  sc->rec.ncell = n;
+  sc->rec.usable = h_mx <= 4 && (long long)n * 4 < (1LL << 31) && pedge->to->size < (int)kRoleBit;
+  if (sc->rec.usable && n > 0) {
+    size_t cnt = (size_t)n * 4;
+    int *o = nullptr, *n1 = nullptr;
+    unsigned *n2 = nullptr;
+    if (cudaMalloc(&o, cnt * 4) != cudaSuccess || cudaMalloc(&n1, cnt * 4) != cudaSuccess ||
+        cudaMalloc(&n2, cnt * 4) != cudaSuccess) {
+      cudaFree(o);
+      cudaFree(n1);
+      set_error("slot records: out of device memory");
+      return nullptr;
+    }
+    sc->owned = {o, n1, n2};
+    k_build_slots<<<g, 256, 0, s>>>(n, inv->off, inv->ent,
+                                    reinterpret_cast<const int2 *>(pedge->map_d),
+                                    reinterpret_cast<const int2 *>(pecell->map_d), o, n1, n2);
+    r.launches += 2;
+    if (!cuda_ok(cudaStreamSynchronize(s), "slot records")) return nullptr;
+    sc->rec.o = o;
+    sc->rec.n1 = n1;
+    sc->rec.n2 = n2;
+  }
+  slot_cache().push_back(std::move(sc));
+  return &slot_cache().back()->rec;
+}
+
+void release_slot_records() { slot_cache().clear(); }
+
+template <typename T>
+cudaError_t launch_res_calc_gather4(const LaunchCtx &c, const SlotRecords &s, const T *x,
+                                    const T *q, const T *adt, T *res, const AirConst<T> &k) {
+  if (s.ncell <= 0) return cudaSuccess;
+  long long threads = 4LL * s.ncell;
+  k_res_gather4<T><<<(unsigned)((threads + 255) / 256), 256, 0, c.stream>>>(
+      s.ncell, s.o, s.n1, s.n2, x, q, adt, res, k);
+  c.count();
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_res_calc_gather4<double>(const LaunchCtx &, const SlotRecords &,
+                                                     const double *, const double *,
+                                                     const double *, double *,
+                                                     const AirConst<double> &);
+template cudaError_t launch_res_calc_gather4<float>(const LaunchCtx &, const SlotRecords &,
+                                                    const float *, const float *, const float *,
+                                                    float *, const AirConst<float> &);
 
 // ------------------------------------------------------------------ bres_calc
 

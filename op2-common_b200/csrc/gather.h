@@ -19,7 +19,32 @@ struct InvMap {
 };
 
 const InvMap *get_inverse_map(op_map map);
-void release_inverse_maps();
+void release_inverse_maps();  // also drops the slot records built on them
+
+// Four slots per cell for res_calc's 4-lanes-per-cell gather: other cell,
+// the edge's nodes, role (bit 30 of n2) and valid (bit 31 of n2).  usable is
+// false when some cell has more than four incident edges.
+struct SlotRecords {
+  const int *o, *n1;
+  const unsigned *n2;
+  int ncell;
+  bool usable;
+};
+const SlotRecords *get_slot_records(op_map pecell, op_map pedge);
+void release_slot_records();
+
+template <typename T>
+cudaError_t launch_res_calc_gather4(const LaunchCtx &c, const SlotRecords &s, const T *x,
+                                    const T *q, const T *adt, T *res, const AirConst<T> &k);
+template <typename T>
+cudaError_t launch_res_calc_gather_cell4(const LaunchCtx &c, const SlotRecords &s, const T *x,
+                                         const T *q, const T *adt, T *res,
+                                         const AirConst<T> &k);
+
+// which gather kernel res_calc uses (option "gather_kernel")
+#define OP2B_GATHER_CSR 1    // one thread per cell walking the inverse map
+#define OP2B_GATHER_LANES 2  // four threads per cell, shuffled together
+#define OP2B_GATHER_CELL4 3  // one thread per cell, four slot records, unrolled
 
 template <typename T>
 cudaError_t launch_res_calc_gather(const LaunchCtx &c, const InvMap &inv, const int *pedge,

@@ -624,6 +624,18 @@ void op_print_dat_to_txtfile(op_dat dat, const char *file_name) {
 
 int op_get_size(op_set set) { return set ? set->size : 0; }
 
+void op_printf(const char *format, ...) {
+  va_list ap;
+  va_start(ap, format);
+  vprintf(format, ap);
+  va_end(ap);
+}
+
+void *op_malloc(size_t size) { return size ? malloc(size) : nullptr; }
+void *op_calloc(size_t num, size_t size) { return calloc(num, size); }
+void *op_realloc(void *ptr, size_t size) { return realloc(ptr, size); }
+void op_free(void *ptr) { free(ptr); }
+
 void op_rank(int *rank) {
   if (rank) *rank = 0;
 }
@@ -711,6 +723,14 @@ int op2b_set_option(const char *key, long value) {
     r.opt_block_size = (int)value;
   } else if (k == "plan_mode") {
     r.opt_plan_mode = (int)value;
+  } else if (k == "gather_kernel") {
+    if (value < 1 || value > 3) {
+      set_error("op2b_set_option: gather_kernel must be 1 (csr), 2 (lanes) or 3 (cell4)");
+      return -1;
+    }
+    r.opt_gather_kernel = (int)value;
+  } else if (k == "gather_minblocks") {
+    r.opt_gather_minb = (int)value;
   } else if (k == "check_plans") {
     r.opt_check_plans = value != 0;
   } else {
@@ -730,6 +750,7 @@ long op2b_get_option(const char *key) {
   if (k == "part_size") return r.opt_part_size;
   if (k == "block_size") return r.opt_block_size;
   if (k == "plan_mode") return r.opt_plan_mode;
+  if (k == "gather_kernel") return r.opt_gather_kernel;
   if (k == "check_plans") return r.opt_check_plans;
   if (k == "nsm") return r.nsm;
   return -1;

@@ -201,9 +201,17 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
   double bytes = 16.0 * E + (double)rb * (2.0 * N + 13.0 * C);
   Plan *plan = nullptr;
   const InvMap *inv = nullptr;
+  const SlotRecords *slots = nullptr;
   if (r.opt_inc_mode == OP2B_INC_GATHER) {
-    inv = get_inverse_map(pecell);
-    if (!inv) return -1;
+    if (r.opt_gather_kernel != OP2B_GATHER_CSR) {
+      slots = get_slot_records(pecell, pedge);
+      if (!slots) return -1;
+    }
+    if (!slots || !slots->usable) {  // CSR walk (also when a cell has more than 4 edges)
+      slots = nullptr;
+      inv = get_inverse_map(pecell);
+      if (!inv) return -1;
+    }
   } else if (r.opt_inc_mode != OP2B_INC_ATOMIC) {
     plan = get_res_plan(name, set, nargs, a);
     if (!plan) return -1;
@@ -217,9 +225,13 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
                           (const double *)a[2].dat->data_d, (const double *)a[4].dat->data_d,
                           (double *)a[6].dat->data_d, k};
     r.begin_loop(name);
-    e = inv ? launch_res_calc_gather<double>(r.ctx(), *inv, p.pedge, p.pecell, p.x, p.q, p.adt,
-                                             p.res, k)
-            : run_res_calc<double>(r.ctx(), p, plan, r.opt_inc_mode);
+    e = slots ? (r.opt_gather_kernel == OP2B_GATHER_LANES
+                     ? launch_res_calc_gather4<double>(r.ctx(), *slots, p.x, p.q, p.adt, p.res, k)
+                     : launch_res_calc_gather_cell4<double>(r.ctx(), *slots, p.x, p.q, p.adt,
+                                                         p.res, k))
+        : inv ? launch_res_calc_gather<double>(r.ctx(), *inv, p.pedge, p.pecell, p.x, p.q,
+                                               p.adt, p.res, k)
+              : run_res_calc<double>(r.ctx(), p, plan, r.opt_inc_mode);
   } else {
     AirConst<float> k = air_consts<float>(ok);
     if (!ok) return -1;
@@ -227,9 +239,13 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
                          (const float *)a[2].dat->data_d, (const float *)a[4].dat->data_d,
                          (float *)a[6].dat->data_d, k};
     r.begin_loop(name);
-    e = inv ? launch_res_calc_gather<float>(r.ctx(), *inv, p.pedge, p.pecell, p.x, p.q, p.adt,
-                                            p.res, k)
-            : run_res_calc<float>(r.ctx(), p, plan, r.opt_inc_mode);
+    e = slots ? (r.opt_gather_kernel == OP2B_GATHER_LANES
+                     ? launch_res_calc_gather4<float>(r.ctx(), *slots, p.x, p.q, p.adt, p.res, k)
+                     : launch_res_calc_gather_cell4<float>(r.ctx(), *slots, p.x, p.q, p.adt,
+                                                         p.res, k))
+        : inv ? launch_res_calc_gather<float>(r.ctx(), *inv, p.pedge, p.pecell, p.x, p.q,
+                                              p.adt, p.res, k)
+              : run_res_calc<float>(r.ctx(), p, plan, r.opt_inc_mode);
   }
   r.end_loop(bytes);
   return finish(e, name);

@@ -1,0 +1,49 @@
+"""The drop-in proof: the reference's unmodified Airfoil application
+(apps/c/airfoil/airfoil_plain/dp/airfoil.cpp), compiled against this
+repository's include/op_seq.h and linked with libop2b.so (oracle/Makefile,
+target `dropin`), runs its 1000 iterations on the GPU from a new_grid.dat
+written by op2b.mesh.  Its printed history (rms every 100 iterations, maxerr,
+errloc) and its binary dump of q (out_grid_seq.bin, op_print_dat_to_binfile)
+are compared with the oracle: with the default owner-computes increments
+q is bit-identical to the reference's sequential build.
+"""
+import os
+import re
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from op2b import mesh as M
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.skipif(not O.ref_binary("airfoil_dropin"), reason="drop-in binary not built")
+def test_reference_airfoil_app_runs_on_libop2b():
+    m = M.channel_bump(240, 120, seed=1)
+    with tempfile.TemporaryDirectory() as tmp:
+        M.write_grid_dat(m, os.path.join(tmp, "new_grid.dat"))
+        out = subprocess.run([O.ref_binary("airfoil_dropin")], cwd=tmp, capture_output=True,
+                             text=True, timeout=600)
+        assert out.returncode == 0, out.stdout[-3000:] + out.stderr[-3000:]
+        with open(os.path.join(tmp, "out_grid_seq.bin"), "rb") as f:
+            count, dim = np.frombuffer(f.read(8), np.int32)
+            q = np.frombuffer(f.read(), np.float64).reshape(count, dim)
+        txt = open(os.path.join(tmp, "out_grid_seq.dat")).read().split("\n")
+    hist = re.findall(r"^\s*(\d+)\s+([0-9.eE+-]+), max err: ([0-9.eE+-]+) at (\d+)",
+                      out.stdout, flags=re.M)
+    assert [int(h[0]) for h in hist] == list(range(100, 1001, 100)), out.stdout[-2000:]
+    st, rms, mx, el = O.airfoil_run(m, M.airfoil_constants(), 1000)
+    for it, r, e, loc in hist:
+        i = int(it) - 1
+        assert abs(float(r) / rms[i] - 1) < 1e-5          # printed with 6 digits
+        assert abs(float(e) / mx[i] - 1) < 1e-14          # printed with 16 digits
+        assert int(loc) == el[i]
+    assert count == m.ncell and dim == 4
+    assert np.array_equal(q, st.q), "q after 1000 iterations must equal the reference's"
+    assert txt[0].split() == [str(m.ncell), "4"]
+    first = np.array([float(v) for v in txt[1].split()])
+    assert np.allclose(first, st.q[0], rtol=1e-15, atol=0)
