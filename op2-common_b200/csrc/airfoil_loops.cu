@@ -242,7 +242,7 @@ template <typename T, int THREADS>
 __global__ void __launch_bounds__(THREADS)
 k_update(int ncell, const T *__restrict__ qold, T *__restrict__ q, T *__restrict__ res,
          const T *__restrict__ adt, RedSlot *__restrict__ parts, unsigned *__restrict__ counter,
-         RedSlot *__restrict__ out) {
+         RedSlot *__restrict__ out, RedSlot *host_out, long long seq) {
   RedTriple t{0.0, -INFINITY, LLONG_MAX};
   int stride = gridDim.x * THREADS;
   for (int n = blockIdx.x * THREADS + threadIdx.x; n < ncell; n += stride) {
@@ -284,6 +284,14 @@ k_update(int ncell, const T *__restrict__ qold, T *__restrict__ q, T *__restrict
   a = block_reduce<THREADS>(a);
   if (threadIdx.x == 0) {
     *out = RedSlot{a.sum, a.maxv, a.idx, 0};
+    if (host_out) {
+      volatile RedSlot *h = host_out;
+      h->sum = a.sum;
+      h->maxv = a.maxv;
+      h->idx = a.idx;
+      __threadfence_system();
+      h->pad = seq;  // published last
+    }
     *counter = 0u;  // ready for the next launch (same stream, so ordered)
   }
 }
@@ -295,7 +303,7 @@ cudaError_t launch_update(const LaunchCtx &c, int ncell, const T *qold, T *q, T 
   int grid = grid_for(c, ncell, TH, 4);
   if (grid > s.capacity) grid = s.capacity;
   k_update<T, TH><<<grid, TH, 0, c.stream>>>(ncell, qold, q, res, adt, s.parts, s.counter,
-                                             s.out);
+                                             s.out, s.host_out, s.seq);
   c.count();
   return cudaGetLastError();
 }

@@ -33,6 +33,10 @@ struct RedScratch {
   unsigned *counter;
   RedSlot *out;
   int capacity;
+  // mapped pinned host copy of the result; `pad` receives `seq` after the
+  // values, so the host can poll it instead of copying and synchronising
+  RedSlot *host_out;
+  long long seq;
 };
 
 cudaError_t launch_copy(const LaunchCtx &c, const void *src, void *dst, size_t bytes);

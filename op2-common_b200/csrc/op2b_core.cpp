@@ -216,7 +216,13 @@ void op_init(int argc, char **argv, int diags) {
   r.red.parts = reinterpret_cast<RedSlot *>(p);
   r.red.out = r.red.parts + r.red.capacity;
   r.red.counter = reinterpret_cast<unsigned *>(reinterpret_cast<char *>(r.red.out + 1));
-  if (!cuda_ok(cudaMallocHost(&r.pinned, 4096), "op_init: pinned buffer")) return;
+  // mapped pinned page: the update kernel writes its reduction result here
+  if (!cuda_ok(cudaHostAlloc(&r.pinned, 4096, cudaHostAllocMapped), "op_init: pinned buffer"))
+    return;
+  memset(r.pinned, 0, 4096);
+  if (!cuda_ok(cudaHostGetDevicePointer(&r.pinned_dev, r.pinned, 0), "op_init: mapped pointer"))
+    return;
+  r.red.host_out = reinterpret_cast<RedSlot *>(r.pinned_dev);
   r.initialised = true;
   if (diags > 1)
     printf(" op2b: device %d (%s, %d SMs), stream %p\n", dev, prop.name, r.nsm,

@@ -6,6 +6,8 @@
 // "double" selects the FP64 kernels, "float" the FP32-storage kernels of the
 // mixed-precision form.  Anything else is an error -- there is no host
 // execution path.
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -115,6 +117,30 @@ template <typename T> AirConst<T> air_consts(bool &ok) {
   k.eps = (T)*eps;
   for (int i = 0; i < 4; i++) k.qinf[i] = (T)qinf[i];
   return k;
+}
+
+// Spin until the device publishes `seq` at *flag.  Every few thousand spins
+// the stream is queried so a failed kernel is reported instead of waited
+// for; the wait gives up after 120 s.
+bool wait_for_sequence(volatile long long *flag, long long seq, const char *what) {
+  Runtime &r = rt();
+  auto t0 = std::chrono::steady_clock::now();
+  for (long spins = 0; *flag != seq; spins++) {
+    if ((spins & 4095) == 4095) {
+      cudaError_t q = cudaStreamQuery(r.stream);
+      if (q != cudaSuccess && q != cudaErrorNotReady) return cuda_ok(q, what);
+      if (q == cudaSuccess && *flag != seq) {
+        set_error("%s: the stream finished without publishing the result", what);
+        return false;
+      }
+      if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(120)) {
+        set_error("%s: no result after 120 s", what);
+        return false;
+      }
+    }
+  }
+  std::atomic_thread_fence(std::memory_order_acquire);
+  return true;
 }
 
 int finish(cudaError_t e, const char *loop) {
@@ -334,6 +360,7 @@ int loop_update(const char *name, op_set set, int nargs, op_arg *a) {
   Runtime &r = rt();
   int C = set->size;
   double bytes = (double)rb * 17.0 * C;
+  r.red.seq = ++r.red_seq;
   r.begin_loop(name);
   cudaError_t e;
   if (rb == 8)
@@ -346,11 +373,10 @@ int loop_update(const char *name, op_set set, int nargs, op_arg *a) {
                              (const float *)a[3].dat->data_d, r.red);
   r.end_loop(bytes);
   if (finish(e, name)) return -1;
-  // gbl results are valid when op_par_loop returns
-  RedSlot *h = reinterpret_cast<RedSlot *>(r.pinned);
-  if (!cuda_ok(cudaMemcpyAsync(h, r.red.out, sizeof(RedSlot), cudaMemcpyDeviceToHost, r.stream),
-               "op_par_loop(update): reduction read-back") ||
-      !cuda_ok(cudaStreamSynchronize(r.stream), "op_par_loop(update): reduction read-back"))
+  // gbl results are valid when op_par_loop returns: the kernel's last block
+  // publishes them in the mapped page, sequence number last
+  volatile RedSlot *h = reinterpret_cast<volatile RedSlot *>(r.pinned);
+  if (!wait_for_sequence(&h->pad, r.red.seq, "op_par_loop(update): reduction read-back"))
     return -1;
   if (C == 0) return 0;
   *reinterpret_cast<double *>(a[4].data) += h->sum;

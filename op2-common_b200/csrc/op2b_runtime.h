@@ -58,7 +58,9 @@ struct Runtime {
   // fused-update reduction
   RedScratch red{};
   void *red_base = nullptr;
-  void *pinned = nullptr;  // 4 KiB pinned host buffer for reduction read-back
+  void *pinned = nullptr;      // 4 KiB mapped pinned host page for reduction read-back
+  void *pinned_dev = nullptr;  // its device address
+  long long red_seq = 0;       // sequence number of the last update launch
 
   // timing
   std::map<std::string, LoopStat> stats;
