@@ -1,0 +1,453 @@
+// BF16 GEMM on the 5th-generation tensor cores (tcgen05, sm_100a) with FP32
+// accumulation in tensor memory, for the learned warm start's MLPs.
+//
+//   C[M x N] = sum_k A(m, k) * B(n, k)          (A, B bf16; accumulate FP32)
+//
+// One CTA of 128 threads computes a 128 x NT tile (NT <= 128, multiple of 16):
+//   * tensor memory: warp 0 allocates 128 columns; accumulator row m sits in
+//     TMEM lane m, column n in TMEM column n (M = 128, cta_group::1);
+//   * K is walked in tiles of 64; the CTA stages 16-byte chunks of A and B
+//     from global memory into shared memory in the no-swizzle K-major "core
+//     matrix" layout: a core matrix is 8 rows x 16 bytes (8 bf16 of K) stored
+//     contiguously (128 B); K-adjacent core matrices are 128 B apart (the
+//     descriptor's leading byte offset) and 8-row groups 1024 B apart (its
+//     stride byte offset).  A transposed operand is transposed on the way;
+//   * two shared-memory stages: while the tensor core consumes one, the CTA
+//     fills the other; one thread issues four tcgen05.mma (K = 16 each) per
+//     tile and a tcgen05.commit to the stage's mbarrier, which the CTA waits
+//     on before refilling that stage;
+//   * epilogue: warp w reads rows 32w..32w+31 from TMEM (tcgen05.ld 32x32b,
+//     16 columns at a time) and applies bias / SiLU / SiLU' / residual /
+//     split-K atomics before storing.
+// Every mbarrier wait is bounded in time (%globaltimer): on expiry the kernel
+// records an error, stops issuing, waits (bounded) for its outstanding
+// commits, frees its tensor memory and returns.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "op2b_gnn.h"
+#include "op2b_runtime.h"
+
+namespace op2b {
+namespace {
+
+constexpr int kTileM = 128;
+constexpr int kTileN = 128;
+constexpr int kTileK = 64;
+constexpr int kThreads = 128;
+constexpr int kStageBytes = kTileM * kTileK * 2;  // one operand tile (16 KiB)
+constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s per mbarrier wait
+
+// i over the first n of 16 columns, unrolled so per-column arrays stay in registers
+#define FOR_LT_N(i) _Pragma("unroll") for (int i = 0; i < 16; i++) if (i < n)
+
+struct GemmArgs {
+  int M, N, K;
+  const __nv_bfloat16 *A;
+  long a_m, a_k;
+  const __nv_bfloat16 *B;
+  long b_n, b_k;
+  void *C;
+  long ldc;
+  const float *bias;
+  __nv_bfloat16 *Z;
+  const __nv_bfloat16 *R;
+  long ldr;
+  int epi;
+  int k_per_split;
+  int *err;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// shared-memory matrix descriptor: no swizzle, K-major, version 1 (sm_100)
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
+}
+
+// instruction descriptor, kind::f16: FP32 accumulator (bits 4-5 = 1), A and B
+// bf16 (bits 7-9 = 1, 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 in
+// bits 17-22, M >> 4 in bits 24-28
+__device__ __forceinline__ uint32_t umma_idesc(int nt) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(nt >> 3) << 17) |
+         ((uint32_t)(kTileM >> 4) << 24);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = globaltimer();
+  while (!mbar_try(bar, parity))
+    if (globaltimer() - t0 > kWaitNs) return false;
+  return true;
+}
+
+__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+__device__ __forceinline__ float silu_grad(float z) {
+  const float s = 1.0f / (1.0f + __expf(-z));
+  return s * (1.0f + z * (1.0f - s));
+}
+
+// Stage one operand tile (128 rows x 64 k) into the core-matrix layout;
+// rows >= nrows and k >= kend read as zero.
+__device__ __forceinline__ void stage_tile(uint8_t *dst, const __nv_bfloat16 *src, long s_row,
+                                           long s_k, int row0, int nrows, int k0, int kend) {
+  if (s_k == 1) {  // k contiguous: one 16-byte chunk = 8 k values of one row
+    for (int c = threadIdx.x; c < kTileM * 8; c += kThreads) {
+      const int row = c >> 3, kc = c & 7;
+      const int gr = row0 + row, gk = k0 + kc * 8;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (gr < nrows && gk < kend)
+        v = __ldg(reinterpret_cast<const uint4 *>(src + (long)gr * s_row + gk));
+      *reinterpret_cast<uint4 *>(dst + (row >> 3) * 1024 + kc * 128 + (row & 7) * 16) = v;
+    }
+  } else {  // rows contiguous: one 16-byte chunk = 8 rows of one k
+    for (int c = threadIdx.x; c < kTileK * 16; c += kThreads) {
+      const int k = c & 63, rc = c >> 6;
+      const int gk = k0 + k, gr = row0 + rc * 8;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (gk < kend && gr < nrows)
+        v = __ldg(reinterpret_cast<const uint4 *>(src + (long)gk * s_k + gr));
+      const unsigned short *e = reinterpret_cast<const unsigned short *>(&v);
+      uint8_t *base = dst + rc * 1024 + (k >> 3) * 128 + (k & 7) * 2;
+#pragma unroll
+      for (int i = 0; i < 8; i++) *reinterpret_cast<unsigned short *>(base + i * 16) = e[i];
+    }
+  }
+}
+
+__device__ __forceinline__ void store_bf16x16(__nv_bfloat16 *dst, const float *v, int n) {
+  if (n == 16 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+    uint4 w[2];
+    __nv_bfloat162 *p = reinterpret_cast<__nv_bfloat162 *>(w);
+#pragma unroll
+    for (int i = 0; i < 8; i++) p[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+    reinterpret_cast<uint4 *>(dst)[0] = w[0];
+    reinterpret_cast<uint4 *>(dst)[1] = w[1];
+  } else {
+    FOR_LT_N(i) dst[i] = __float2bfloat16(v[i]);
+  }
+}
+
+__device__ __forceinline__ void load_bf16x16(const __nv_bfloat16 *src, float *v, int n) {
+  if (n == 16 && (reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+    uint4 w[2];
+    w[0] = reinterpret_cast<const uint4 *>(src)[0];
+    w[1] = reinterpret_cast<const uint4 *>(src)[1];
+    const __nv_bfloat162 *p = reinterpret_cast<const __nv_bfloat162 *>(w);
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      float2 f = __bfloat1622float2(p[i]);
+      v[2 * i] = f.x;
+      v[2 * i + 1] = f.y;
+    }
+  } else {
+    FOR_LT_N(i) v[i] = __bfloat162float(src[i]);
+  }
+}
+
+__device__ void epilogue16(const GemmArgs &g, int row, int col, const uint32_t *r) {
+  const int n = min(16, g.N - col);
+  if (n <= 0) return;
+  float v[16];
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+  const long o = (long)row * g.ldc + col;
+  switch (g.epi) {
+    case OP2B_EPI_STORE_F32: {
+      float *c = reinterpret_cast<float *>(g.C) + o;
+      if (g.bias) FOR_LT_N(i) v[i] += g.bias[col + i];
+      if (n == 16 && (reinterpret_cast<uintptr_t>(c) & 15) == 0) {
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+          reinterpret_cast<float4 *>(c)[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2],
+                                                         v[4 * i + 3]);
+      } else {
+        FOR_LT_N(i) c[i] = v[i];
+      }
+      return;
+    }
+    case OP2B_EPI_ATOMIC_F32: {
+      float *c = reinterpret_cast<float *>(g.C) + o;
+      FOR_LT_N(i) atomicAdd(c + i, v[i]);
+      return;
+    }
+    case OP2B_EPI_BIAS_BF16: {
+      if (g.bias)
+        FOR_LT_N(i) v[i] += g.bias[col + i];
+      if (g.R) {
+        float rr[16];
+        load_bf16x16(g.R + (long)row * g.ldr + col, rr, n);
+        FOR_LT_N(i) v[i] += rr[i];
+      }
+      store_bf16x16(reinterpret_cast<__nv_bfloat16 *>(g.C) + o, v, n);
+      return;
+    }
+    case OP2B_EPI_BIAS_SILU_BF16: {
+      if (g.bias)
+        FOR_LT_N(i) v[i] += g.bias[col + i];
+      if (g.Z) store_bf16x16(g.Z + o, v, n);
+      FOR_LT_N(i) v[i] = silu(v[i]);
+      store_bf16x16(reinterpret_cast<__nv_bfloat16 *>(g.C) + o, v, n);
+      return;
+    }
+    case OP2B_EPI_SILU_GRAD_BF16: {
+      float z[16];
+      load_bf16x16(g.R + (long)row * g.ldr + col, z, n);
+      FOR_LT_N(i) v[i] *= silu_grad(z[i]);
+      store_bf16x16(reinterpret_cast<__nv_bfloat16 *>(g.C) + o, v, n);
+      return;
+    }
+    default:
+      store_bf16x16(reinterpret_cast<__nv_bfloat16 *>(g.C) + o, v, n);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 1) k_gemm_tc(GemmArgs g) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ __align__(8) uint64_t bars[2];
+  __shared__ uint32_t s_taddr;
+  __shared__ int s_fail;
+  const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * kTileN;
+  const int rem = g.N - n0;
+  const int nt = rem >= kTileN ? kTileN : ((rem + 15) & ~15);
+  const int kb = blockIdx.z * g.k_per_split;
+  const int ke = min(g.K, kb + g.k_per_split);
+  const int nk = ke > kb ? (ke - kb + kTileK - 1) / kTileK : 0;
+  uint8_t *sA[2] = {smem, smem + 2 * kStageBytes};
+  uint8_t *sB[2] = {smem + kStageBytes, smem + 3 * kStageBytes};
+  const uint32_t bar[2] = {smem_u32(&bars[0]), smem_u32(&bars[1])};
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    mbar_init(bar[0], 1);
+    mbar_init(bar[1], 1);
+    s_fail = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&s_taddr)),
+                 "r"(128u));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t taddr = s_taddr;
+  const uint32_t idesc = umma_idesc(nt);
+  uint32_t phase[2] = {0u, 0u};
+  int pending[2] = {0, 0};  // commits on each stage not yet waited for
+  int issued = 0;
+
+  for (int kt = 0; kt < nk; kt++) {
+    const int s = kt & 1;
+    if (pending[s]) {  // the MMAs of tile kt-2 read this stage
+      if (!mbar_wait(bar[s], phase[s])) s_fail = 1;
+      phase[s] ^= 1u;
+      pending[s] = 0;
+    }
+    __syncthreads();
+    if (s_fail) break;
+    const int k0 = kb + kt * kTileK;
+    stage_tile(sA[s], g.A, g.a_m, g.a_k, m0, g.M, k0, ke);
+    stage_tile(sB[s], g.B, g.b_n, g.b_k, n0, g.N, k0, ke);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a0 = smem_u32(sA[s]), b0 = smem_u32(sB[s]);
+#pragma unroll
+      for (int j = 0; j < kTileK / 16; j++) {
+        const uint64_t da = umma_desc(a0 + j * 256, 128, 1024);
+        const uint64_t db = umma_desc(b0 + j * 256, 128, 1024);
+        const uint32_t acc = (kt > 0 || j > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(taddr),
+            "l"(da), "l"(db), "r"(idesc), "r"(acc));
+      }
+      asm volatile(
+          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+              bar[s])
+          : "memory");
+    }
+    pending[s] = 1;
+    issued = kt + 1;
+  }
+  // drain: wait for every commit not yet waited for (the later one covers all
+  // earlier MMAs, but each arrival must land before the CTA exits)
+  for (int i = 0; i < 2; i++) {
+    const int s = (issued + i) & 1;  // older stage first
+    if (pending[s]) {
+      if (!mbar_wait(bar[s], phase[s])) s_fail = 1;
+      pending[s] = 0;
+    }
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+  if (!s_fail) {
+    const int row = m0 + warp * 32 + lane;
+    for (int cc = 0; cc < nt; cc += 16) {
+      uint32_t r[16];
+      if (issued > 0) {
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+            "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+              "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+              "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)cc));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      } else {
+#pragma unroll
+        for (int i = 0; i < 16; i++) r[i] = 0u;
+      }
+      if (row < g.M) epilogue16(g, row, n0 + cc, r);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(128u));
+  if (threadIdx.x == 0 && s_fail) atomicExch(g.err, 1);
+}
+
+// the same product on the CUDA cores (FP32 accumulation), as a cross-check
+__global__ void k_gemm_simt(GemmArgs g) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x, row = blockIdx.y;
+  if (col >= g.N || row >= g.M) return;
+  float acc = 0.f;
+  for (int k = 0; k < g.K; k++)
+    acc += __bfloat162float(g.A[row * g.a_m + k * g.a_k]) *
+           __bfloat162float(g.B[col * g.b_n + k * g.b_k]);
+  reinterpret_cast<float *>(g.C)[(long)row * g.ldc + col] = acc;
+}
+
+int *g_err_dev[16] = {};
+
+}  // namespace
+}  // namespace op2b
+
+using namespace op2b;
+
+extern "C" int op2b_gemm_bf16(int M, int N, int K, const void *A, long a_m, long a_k,
+                              const void *B, long b_n, long b_k, void *C, long ldc, int epi,
+                              const float *bias, void *Z, const void *R, long ldr, int split_k,
+                              int engine, void *stream) {
+  if (M <= 0 || N <= 0 || K <= 0 || !A || !B || !C) {
+    set_error("op2b_gemm_bf16: empty or null operands (M=%d N=%d K=%d)", M, N, K);
+    return -1;
+  }
+  if ((a_m != 1 && a_k != 1) || (b_n != 1 && b_k != 1) || N % 8 ||
+      ((a_k == 1 || b_k == 1) && K % 8)) {
+    set_error("op2b_gemm_bf16: each operand needs a unit stride; N, and K of a k-contiguous "
+              "operand, multiples of 8");
+    return -1;
+  }
+  if ((a_k != 1 && (M % 8 || a_k % 8)) || (b_k != 1 && (N % 8 || b_k % 8)) ||
+      (a_k == 1 && a_m % 8) || (b_k == 1 && b_n % 8)) {
+    set_error("op2b_gemm_bf16: rows of 16-byte chunks need strides and transposed row counts "
+              "that are multiples of 8");
+    return -1;
+  }
+  if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15) {
+    set_error("op2b_gemm_bf16: A and B must be 16-byte aligned");
+    return -1;
+  }
+  if (epi < OP2B_EPI_STORE_F32 || epi > OP2B_EPI_SILU_GRAD_BF16 ||
+      (epi == OP2B_EPI_SILU_GRAD_BF16 && !R)) {
+    set_error("op2b_gemm_bf16: bad epilogue %d (SILU_GRAD needs R)", epi);
+    return -1;
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 16) {
+    set_error("op2b_gemm_bf16: device %d out of range", dev);
+    return -1;
+  }
+  if (!g_err_dev[dev]) {
+    if (!cuda_ok(cudaMalloc(&g_err_dev[dev], sizeof(int)), "op2b_gemm_bf16: error flag"))
+      return -1;
+    cudaMemset(g_err_dev[dev], 0, sizeof(int));
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  GemmArgs g{M,   N,   K,   (const __nv_bfloat16 *)A, a_m, a_k, (const __nv_bfloat16 *)B,
+             b_n, b_k, C,   ldc, bias, (__nv_bfloat16 *)Z,     (const __nv_bfloat16 *)R,
+             ldr, epi, 0,   g_err_dev[dev]};
+  if (engine == 1) {
+    if (epi != OP2B_EPI_STORE_F32) {
+      set_error("op2b_gemm_bf16: the CUDA-core path stores FP32 only");
+      return -1;
+    }
+    k_gemm_simt<<<dim3((N + 127) / 128, M), 128, 0, s>>>(g);
+    if (rt().initialised) rt().launches++;
+    return cuda_ok(cudaGetLastError(), "op2b_gemm_bf16") ? 0 : -1;
+  }
+  if (split_k < 1) split_k = 1;
+  const int kps = ((K + split_k - 1) / split_k + kTileK - 1) / kTileK * kTileK;
+  split_k = (K + kps - 1) / kps;
+  if (split_k > 1 && epi != OP2B_EPI_ATOMIC_F32) {
+    set_error("op2b_gemm_bf16: split-K needs the atomic FP32 epilogue");
+    return -1;
+  }
+  if (split_k > 65535) {
+    set_error("op2b_gemm_bf16: split_k above 65535");
+    return -1;
+  }
+  g.k_per_split = kps;
+  const size_t smem = 4 * (size_t)kStageBytes;
+  static bool attr[16] = {};
+  if (!attr[dev]) {
+    if (!cuda_ok(cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem),
+                 "op2b_gemm_bf16: shared memory attribute"))
+      return -1;
+    attr[dev] = true;
+  }
+  dim3 grid((M + kTileM - 1) / kTileM, (N + kTileN - 1) / kTileN, split_k);
+  k_gemm_tc<<<grid, kThreads, smem, s>>>(g);
+  if (rt().initialised) rt().launches++;
+  return cuda_ok(cudaGetLastError(), "op2b_gemm_bf16") ? 0 : -1;
+}
+
+extern "C" int op2b_gemm_error(int reset) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 16 || !g_err_dev[dev]) return 0;
+  int h = 0;
+  cudaMemcpy(&h, g_err_dev[dev], sizeof(int), cudaMemcpyDeviceToHost);
+  if (reset) cudaMemset(g_err_dev[dev], 0, sizeof(int));
+  return h;
+}
