@@ -91,9 +91,14 @@ def concat(meshes):
 
 
 class AirfoilBatch:
-    def __init__(self, specs, fp32: bool = True, renumber: bool = True):
+    def __init__(self, specs, fp32: bool = True, renumber: bool = True, meshes=None):
+        """specs: per instance I, J, mach, alpha, bump, seed; `meshes` (optional)
+        supplies the instances' meshes instead of generating them from I, J, seed."""
         self.specs = list(specs)
-        meshes = [channel_bump(s["I"], s["J"], seed=s["seed"], bump=s["bump"]) for s in specs]
+        if meshes is None:
+            meshes = [channel_bump(s["I"], s["J"], seed=s["seed"], bump=s["bump"]) for s in specs]
+        if len(meshes) != len(self.specs):
+            raise L.Op2Error("one mesh per instance")
         self.meshes = meshes
         mesh, off = concat(meshes)
         self.mesh = mesh
@@ -198,10 +203,28 @@ class AirfoilBatch:
 
     def q_instance(self, i: int, precision: str = "fp64") -> np.ndarray:
         """q of instance i (caller's order) in its declared cell order."""
-        d = self.d64 if precision == "fp64" else self.d32
-        full = L.op_fetch_data_idx(d.p_q, 0, self.mesh.ncell - 1)
+        full = self.q_all(precision)
         c0 = sum(m.ncell for m in self.meshes[:i])
         return full[c0:c0 + self.meshes[i].ncell]
+
+    def q_all(self, precision: str = "fp64") -> np.ndarray:
+        """q of every instance, concatenated in the caller's order, declared cell order."""
+        d = self.d64 if precision == "fp64" else self.d32
+        return L.op_fetch_data_idx(d.p_q, 0, self.mesh.ncell - 1)
+
+    def q_final(self) -> list:
+        """Each instance's q from the precision it finished in (FP32 if it never
+        left the FP32 phase, FP64 otherwise), as float64 arrays."""
+        st = self.stats()
+        need32 = bool(np.any(st["iters32"] == st["iters"])) and self.d32 is not None
+        q64 = self.q_all("fp64")
+        q32 = self.q_all("fp32").astype(np.float64) if need32 else None
+        out, c0 = [], 0
+        for i, m in enumerate(self.meshes):
+            src = q32 if (need32 and st["iters32"][i] == st["iters"][i]) else q64
+            out.append(src[c0:c0 + m.ncell].copy())
+            c0 += m.ncell
+        return out
 
     def close(self):
         if getattr(self, "h", None):
