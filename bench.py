@@ -61,6 +61,9 @@ def parse():
     p.add_argument("--inc-mode", type=int, default=3,
                    help="0 atomics, 1 block/thread colouring, 2 staged hybrid, 3 gather")
     p.add_argument("--part-size", type=int, default=0)
+    p.add_argument("--gather-kernel", type=int, default=5,
+                   help="inc_mode 3 kernel: 1 csr, 2 lanes, 3 cell4, 4 shared-memory pipeline, 5 register pipeline")
+    p.add_argument("--pipe-block", type=int, default=128)
     p.add_argument("--precision", default="f64", choices=["f64", "mixed"])
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
@@ -199,11 +202,13 @@ def impl_reference(args):
 
 
 def timed_run(L, Airfoil, mesh, dtype, numbering, inc_mode, part, steps, warmup, torch,
-              barrier=None, clocks=None):
+              barrier=None, clocks=None, opts=None):
     """Declare, optionally renumber, warm up, then time `steps` iterations."""
     L.op_init()
     L.set_option("inc_mode", inc_mode)
     L.set_option("part_size", part)
+    for k, v in (opts or {}).items():
+        L.set_option(k, v)
     app = Airfoil(mesh, dtype=dtype)
     ren = None
     if numbering == "rcm":
@@ -277,8 +282,9 @@ def main():
         return float(t.item())
 
     # ---------------------------------------------------------- device-resident timing
+    gopts = {"gather_kernel": args.gather_kernel, "pipe_block": args.pipe_block}
     main_run = timed_run(L, Airfoil, m, dtype, args.numbering, args.inc_mode, args.part_size,
-                         args.steps, args.warmup, torch, barrier, Clocks(local))
+                         args.steps, args.warmup, torch, barrier, Clocks(local), opts=gopts)
     ms = max_over_ranks(main_run["ms"])
 
     # ---------------------------------------------------------- variants (same rank-local work)
@@ -294,6 +300,19 @@ def main():
                                  "ms_per_iter": max_over_ranks(v["ms"]),
                                  "res_calc_gbs": v["loops"].get("res_calc", {}).get("gbs"),
                                  "launches_per_iter": v["launches"] / 20})
+        # gather kernels of inc_mode 3, and the pipelined direct loop's switches
+        for o in ({"gather_kernel": 1}, {"gather_kernel": 3}, {"gather_kernel": 4},
+                  {"gather_kernel": 5, "pipe_block": 64}, {"gather_kernel": 5, "pipe_block": 128},
+                  {"gather_kernel": 5, "pipe_block": 256},
+                  {"gather_kernel": 5, "pipe_block": 128, "pipe_hints": 1}):
+            v = timed_run(L, Airfoil, m, dtype, "rcm", 3, args.part_size, 20, 3, torch, barrier,
+                          opts=o)
+            lp = v["loops"]
+            variants.append({"numbering": "rcm", "inc_mode": 3, **o,
+                             "ms_per_iter": max_over_ranks(v["ms"]),
+                             "res_calc_gbs": lp.get("res_calc", {}).get("gbs"),
+                             "res_calc_us": 1e3 * lp.get("res_calc", {}).get("avg_ms", 0),
+                             "adt_calc_gbs": lp.get("adt_calc", {}).get("gbs")})
 
     # ---------------------------------------------------------- end to end through the API
     e2e = None
@@ -316,6 +335,8 @@ def main():
         L.op_init()
         L.set_option("inc_mode", args.inc_mode)
         L.set_option("part_size", args.part_size)
+        for k, v in gopts.items():
+            L.set_option(k, v)
         barrier()
         t0 = time.perf_counter()
         app2 = Airfoil(hm, dtype=dtype)
@@ -371,6 +392,7 @@ def main():
                        "cells": m.ncell, "edges": m.nedge, "nodes": m.nnode,
                        "bedges": m.nbedge, "numbering": args.numbering,
                        "inc_mode": args.inc_mode, "part_size": args.part_size,
+                       "gather_kernel": args.gather_kernel if args.inc_mode == 3 else None,
                        "parallelism": "replicas" if ws > 1 else "single",
                        "l2": "inputs larger than L2 (working set ~0.7 GB > 126 MB), no flush"},
             "roofline": {"bound": "hbm", "loop": dom, "achieved": d["gbs"], "peak": peak,

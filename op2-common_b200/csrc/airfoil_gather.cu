@@ -345,16 +345,21 @@ k_res_gather_cell4(int ncell, const int4 *__restrict__ rec_o, const int4 *__rest
     Vec<T>::ld2(x + 2 * (size_t)nb, xb[s][0], xb[s][1]);
   }
   Vec<T>::ld4_rw(res + 4 * (size_t)c, acc);
+  T ric, pc;  // the cell's own terms, once for its edges (bit-identical)
+  air_prim<T>(qc, k, ric, pc);
 #pragma unroll
   for (int s = 0; s < 4; s++) {
     if (!(r2[s] & kValidBit)) continue;
-    T f[4];
+    T f[4], rio, po;
+    air_prim<T>(qo[s], k, rio, po);
     if (r2[s] & kRoleBit) {
-      air_flux<T>(xa[s][0], xa[s][1], xb[s][0], xb[s][1], qo[s], qc, ao[s], ac, k, f);
+      air_flux_prim<T>(xa[s][0], xa[s][1], xb[s][0], xb[s][1], qo[s], qc, rio, po, ric, pc,
+                       ao[s], ac, k, f);
 #pragma unroll
       for (int m = 0; m < 4; m++) acc[m] -= f[m];
     } else {
-      air_flux<T>(xa[s][0], xa[s][1], xb[s][0], xb[s][1], qc, qo[s], ac, ao[s], k, f);
+      air_flux_prim<T>(xa[s][0], xa[s][1], xb[s][0], xb[s][1], qc, qo[s], ric, pc, rio, po,
+                       ac, ao[s], k, f);
 #pragma unroll
       for (int m = 0; m < 4; m++) acc[m] += f[m];
     }

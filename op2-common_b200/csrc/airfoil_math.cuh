@@ -77,6 +77,35 @@ __device__ __forceinline__ void air_flux(T x1x, T x1y, T x2x, T x2y,
          mu * (q1[3] - q2[3]);
 }
 
+// The per-cell terms of res_calc.h:8-13 -- ri = 1/q[0] and the pressure p --
+// which depend on the cell alone.  air_flux_prim is air_flux with them passed
+// in: the same operations in the same order, so a cell that owns several
+// edges computes its own terms once and gets bit-identical fluxes.
+template <typename T>
+__device__ __forceinline__ void air_prim(const T *q, const AirConst<T> &k, T &ri, T &p) {
+  ri = (T)1.0f / q[0];
+  p = k.gm1 * (q[3] - (T)0.5f * ri * (q[1] * q[1] + q[2] * q[2]));
+}
+
+template <typename T>
+__device__ __forceinline__ void air_flux_prim(T x1x, T x1y, T x2x, T x2y, const T *q1,
+                                              const T *q2, T ri1, T p1, T ri2, T p2, T adt1,
+                                              T adt2, const AirConst<T> &k, T *f) {
+  T dx, dy, mu, vol1, vol2;
+  dx = x1x - x2x;
+  dy = x1y - x2y;
+  vol1 = ri1 * (q1[1] * dy - q1[2] * dx);
+  vol2 = ri2 * (q2[1] * dy - q2[2] * dx);
+  mu = (T)0.5f * (adt1 + adt2) * k.eps;
+  f[0] = (T)0.5f * (vol1 * q1[0] + vol2 * q2[0]) + mu * (q1[0] - q2[0]);
+  f[1] = (T)0.5f * (vol1 * q1[1] + p1 * dy + vol2 * q2[1] + p2 * dy) +
+         mu * (q1[1] - q2[1]);
+  f[2] = (T)0.5f * (vol1 * q1[2] - p1 * dx + vol2 * q2[2] - p2 * dx) +
+         mu * (q1[2] - q2[2]);
+  f[3] = (T)0.5f * (vol1 * (q1[3] + p1) + vol2 * (q2[3] + p2)) +
+         mu * (q1[3] - q2[3]);
+}
+
 // bres_calc.h:1-35 -- increment r[4] of the cell on a boundary edge
 // (wall: pressure only, r[0] = r[3] = 0; far field: flux against qinf).
 template <typename T>

@@ -40,11 +40,25 @@ template <typename T>
 cudaError_t launch_res_calc_gather_cell4(const LaunchCtx &c, const SlotRecords &s, const T *x,
                                          const T *q, const T *adt, T *res,
                                          const AirConst<T> &k);
+// airfoil_pipe.cu: slot records, operands staged in shared memory by cp.async
+// one cell ahead (block = threads per CTA: 64, 96, 128 or 256)
+template <typename T>
+cudaError_t launch_res_calc_gather_pipe(const LaunchCtx &c, const SlotRecords &s, const T *x,
+                                        const T *q, const T *adt, T *res, const AirConst<T> &k,
+                                        int block);
+// airfoil_pipe.cu: slot records, operands of the next cell prefetched into
+// registers while the current one is computed (persistent grid)
+template <typename T>
+cudaError_t launch_res_calc_gather_regpipe(const LaunchCtx &c, const SlotRecords &s, const T *x,
+                                           const T *q, const T *adt, T *res,
+                                           const AirConst<T> &k, int block);
 
 // which gather kernel res_calc uses (option "gather_kernel")
 #define OP2B_GATHER_CSR 1    // one thread per cell walking the inverse map
 #define OP2B_GATHER_LANES 2  // four threads per cell, shuffled together
 #define OP2B_GATHER_CELL4 3  // one thread per cell, four slot records, unrolled
+#define OP2B_GATHER_PIPE 4   // cell4's order, shared-memory software pipeline
+#define OP2B_GATHER_REGPIPE 5  // cell4's order, register software pipeline
 
 template <typename T>
 cudaError_t launch_res_calc_gather(const LaunchCtx &c, const InvMap &inv, const int *pedge,

@@ -7,11 +7,10 @@
 //   * tensor memory: warp 0 allocates 128 columns; accumulator row m sits in
 //     TMEM lane m, column n in TMEM column n (M = 128, cta_group::1);
 //   * K is walked in tiles of 64; the CTA stages 16-byte chunks of A and B
-//     from global memory into shared memory in the no-swizzle K-major "core
-//     matrix" layout: a core matrix is 8 rows x 16 bytes (8 bf16 of K) stored
-//     contiguously (128 B); K-adjacent core matrices are 128 B apart (the
-//     descriptor's leading byte offset) and 8-row groups 1024 B apart (its
-//     stride byte offset).  A transposed operand is transposed on the way;
+//     from global memory into shared memory in the K-major layout with the
+//     128-byte swizzle (one 128-byte row of 64 bf16 per tile row, 8-row
+//     groups 1024 B apart, 16-byte chunks XOR-permuted by the row); a
+//     transposed operand is transposed in registers on the way;
 //   * two shared-memory stages: while the tensor core consumes one, the CTA
 //     fills the other; one thread issues four tcgen05.mma (K = 16 each) per
 //     tile and a tcgen05.commit to the stage's mbarrier, which the CTA waits
@@ -69,13 +68,18 @@ __device__ __forceinline__ unsigned long long globaltimer() {
   return t;
 }
 
-// shared-memory matrix descriptor: no swizzle, K-major, version 1 (sm_100)
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+// shared-memory matrix descriptor, version 1 (sm_100), K-major with the
+// 128-byte swizzle (layout type 2 in bits 61-63): start address >> 4 in bits
+// 0-13, leading byte offset >> 4 in 16-29 (unused by a swizzled K-major
+// operand whose K step fits in the 128-byte row; 1 by convention), stride
+// byte offset >> 4 in 32-45 (1024: the distance between 8-row groups)
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
   uint64_t d = 0;
   d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(1024 >> 4) << 32;
   d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
   return d;
 }
 
@@ -117,30 +121,63 @@ __device__ __forceinline__ float silu_grad(float z) {
   return s * (1.0f + z * (1.0f - s));
 }
 
-// Stage one operand tile (128 rows x 64 k) into the core-matrix layout;
-// rows >= nrows and k >= kend read as zero.
+// Shared-memory tile layout: K-major with the 128-byte swizzle.  Row r of the
+// 128 x 64 tile is 128 bytes (64 bf16) at (r / 8) * 1024 + (r % 8) * 128; its
+// 16-byte chunk j (k = 8j .. 8j+7) sits at chunk position j ^ (r % 8).  The
+// XOR spreads both the k-contiguous and the transposed staging stores over
+// all 32 banks; the tensor core undoes it from the descriptor's swizzle mode.
+__device__ __forceinline__ uint32_t sw128(int row, int kc) {
+  return (uint32_t)((row >> 3) * 1024 + (row & 7) * 128 + ((kc ^ (row & 7)) << 4));
+}
+
+// Stage one operand tile (128 rows x 64 k); rows >= nrows and k >= kend read
+// as zero.
 __device__ __forceinline__ void stage_tile(uint8_t *dst, const __nv_bfloat16 *src, long s_row,
                                            long s_k, int row0, int nrows, int k0, int kend) {
   if (s_k == 1) {  // k contiguous: one 16-byte chunk = 8 k values of one row
-    for (int c = threadIdx.x; c < kTileM * 8; c += kThreads) {
+    uint4 v[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int c = threadIdx.x + i * kThreads;
       const int row = c >> 3, kc = c & 7;
       const int gr = row0 + row, gk = k0 + kc * 8;
-      uint4 v = make_uint4(0, 0, 0, 0);
+      v[i] = make_uint4(0, 0, 0, 0);
       if (gr < nrows && gk < kend)
-        v = __ldg(reinterpret_cast<const uint4 *>(src + (long)gr * s_row + gk));
-      *reinterpret_cast<uint4 *>(dst + (row >> 3) * 1024 + kc * 128 + (row & 7) * 16) = v;
+        v[i] = __ldg(reinterpret_cast<const uint4 *>(src + (long)gr * s_row + gk));
     }
-  } else {  // rows contiguous: one 16-byte chunk = 8 rows of one k
-    for (int c = threadIdx.x; c < kTileK * 16; c += kThreads) {
-      const int k = c & 63, rc = c >> 6;
-      const int gk = k0 + k, gr = row0 + rc * 8;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int c = threadIdx.x + i * kThreads;
+      *reinterpret_cast<uint4 *>(dst + sw128(c >> 3, c & 7)) = v[i];
+    }
+  } else {
+    // rows contiguous: thread (rc, kc) loads the 8 x 8 block of rows
+    // 8rc..8rc+7 and k 8kc..8kc+7 (eight 16-byte loads, one per k), transposes
+    // it in registers and stores eight 16-byte row chunks
+    const int kc = threadIdx.x & 7, rc = threadIdx.x >> 3;
+    const int gr = row0 + rc * 8;
+    uint32_t in[8][4];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const int gk = k0 + kc * 8 + j;
       uint4 v = make_uint4(0, 0, 0, 0);
       if (gk < kend && gr < nrows)
         v = __ldg(reinterpret_cast<const uint4 *>(src + (long)gk * s_k + gr));
-      const unsigned short *e = reinterpret_cast<const unsigned short *>(&v);
-      uint8_t *base = dst + rc * 1024 + (k >> 3) * 128 + (k & 7) * 2;
+      in[j][0] = v.x, in[j][1] = v.y, in[j][2] = v.z, in[j][3] = v.w;
+    }
+    // in[j] word w = (row 2w, row 2w+1) of k j; out[r] word w = (k 2w, k 2w+1) of row r
 #pragma unroll
-      for (int i = 0; i < 8; i++) *reinterpret_cast<unsigned short *>(base + i * 16) = e[i];
+    for (int r2 = 0; r2 < 4; r2++) {
+      uint32_t lo[4], hi[4];
+#pragma unroll
+      for (int w = 0; w < 4; w++) {
+        lo[w] = __byte_perm(in[2 * w][r2], in[2 * w + 1][r2], 0x5410);
+        hi[w] = __byte_perm(in[2 * w][r2], in[2 * w + 1][r2], 0x7632);
+      }
+      *reinterpret_cast<uint4 *>(dst + sw128(rc * 8 + 2 * r2, kc)) =
+          make_uint4(lo[0], lo[1], lo[2], lo[3]);
+      *reinterpret_cast<uint4 *>(dst + sw128(rc * 8 + 2 * r2 + 1, kc)) =
+          make_uint4(hi[0], hi[1], hi[2], hi[3]);
     }
   }
 }
@@ -233,10 +270,13 @@ __device__ void epilogue16(const GemmArgs &g, int row, int col, const uint32_t *
 }
 
 __global__ void __launch_bounds__(kThreads, 1) k_gemm_tc(GemmArgs g) {
-  extern __shared__ __align__(1024) uint8_t smem[];
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t bars[2];
   __shared__ uint32_t s_taddr;
   __shared__ int s_fail;
+  // the swizzle pattern repeats every 1024 bytes of shared address: align the
+  // tiles to it (the launch reserves 1 KiB of slack)
+  uint8_t *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * kTileN;
   const int rem = g.N - n0;
   const int nt = rem >= kTileN ? kTileN : ((rem + 15) & ~15);
@@ -288,8 +328,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tc(GemmArgs g) {
       const uint32_t a0 = smem_u32(sA[s]), b0 = smem_u32(sB[s]);
 #pragma unroll
       for (int j = 0; j < kTileK / 16; j++) {
-        const uint64_t da = umma_desc(a0 + j * 256, 128, 1024);
-        const uint64_t db = umma_desc(b0 + j * 256, 128, 1024);
+        // K step j = 16 bf16 = 32 bytes along the (swizzled) 128-byte rows
+        const uint64_t da = umma_desc(a0 + j * 32);
+        const uint64_t db = umma_desc(b0 + j * 32);
         const uint32_t acc = (kt > 0 || j > 0) ? 1u : 0u;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -427,7 +468,7 @@ extern "C" int op2b_gemm_bf16(int M, int N, int K, const void *A, long a_m, long
     return -1;
   }
   g.k_per_split = kps;
-  const size_t smem = 4 * (size_t)kStageBytes;
+  const size_t smem = 4 * (size_t)kStageBytes + 1024;
   static bool attr[16] = {};
   if (!attr[dev]) {
     if (!cuda_ok(cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -730,11 +730,20 @@ int op2b_set_option(const char *key, long value) {
   } else if (k == "plan_mode") {
     r.opt_plan_mode = (int)value;
   } else if (k == "gather_kernel") {
-    if (value < 1 || value > 3) {
-      set_error("op2b_set_option: gather_kernel must be 1 (csr), 2 (lanes) or 3 (cell4)");
+    if (value < 1 || value > 5) {
+      set_error("op2b_set_option: gather_kernel must be 1 (csr), 2 (lanes), 3 (cell4), 4 "
+                "(shared-memory pipeline) or 5 (register pipeline)");
       return -1;
     }
     r.opt_gather_kernel = (int)value;
+  } else if (k == "pipe_block") {
+    if (value != 64 && value != 96 && value != 128 && value != 256) {
+      set_error("op2b_set_option: pipe_block must be 64, 96, 128 or 256");
+      return -1;
+    }
+    r.opt_pipe_block = (int)value;
+  } else if (k == "pipe_hints") {
+    r.opt_pipe_hints = value != 0;
   } else if (k == "gather_minblocks") {
     r.opt_gather_minb = (int)value;
   } else if (k == "check_plans") {
@@ -757,6 +766,8 @@ long op2b_get_option(const char *key) {
   if (k == "block_size") return r.opt_block_size;
   if (k == "plan_mode") return r.opt_plan_mode;
   if (k == "gather_kernel") return r.opt_gather_kernel;
+  if (k == "pipe_block") return r.opt_pipe_block;
+  if (k == "pipe_hints") return r.opt_pipe_hints;
   if (k == "check_plans") return r.opt_check_plans;
   if (k == "nsm") return r.nsm;
   return -1;

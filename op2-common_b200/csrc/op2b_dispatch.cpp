@@ -203,6 +203,24 @@ int loop_adt_calc(const char *name, op_set set, int nargs, op_arg *a) {
 }
 
 // ---------------------------------------------------------------- res_calc
+// the slot-record gather kernels (option gather_kernel), all bit-identical
+template <typename T>
+static cudaError_t res_gather_slots(Runtime &r, const SlotRecords &s, const ResCalcArgs<T> &p,
+                                    const AirConst<T> &k) {
+  switch (r.opt_gather_kernel) {
+    case OP2B_GATHER_LANES:
+      return launch_res_calc_gather4<T>(r.ctx(), s, p.x, p.q, p.adt, p.res, k);
+    case OP2B_GATHER_PIPE:
+      return launch_res_calc_gather_pipe<T>(r.ctx(), s, p.x, p.q, p.adt, p.res, k,
+                                            r.opt_pipe_block);
+    case OP2B_GATHER_REGPIPE:
+      return launch_res_calc_gather_regpipe<T>(r.ctx(), s, p.x, p.q, p.adt, p.res, k,
+                                               r.opt_pipe_block);
+    default:
+      return launch_res_calc_gather_cell4<T>(r.ctx(), s, p.x, p.q, p.adt, p.res, k);
+  }
+}
+
 int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
   Sig s{name, set, a, nargs};
   if (nargs != 8) return s.fail(nargs, "res_calc takes 8 arguments"), -1;
@@ -251,10 +269,7 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
                           (const double *)a[2].dat->data_d, (const double *)a[4].dat->data_d,
                           (double *)a[6].dat->data_d, k};
     r.begin_loop(name);
-    e = slots ? (r.opt_gather_kernel == OP2B_GATHER_LANES
-                     ? launch_res_calc_gather4<double>(r.ctx(), *slots, p.x, p.q, p.adt, p.res, k)
-                     : launch_res_calc_gather_cell4<double>(r.ctx(), *slots, p.x, p.q, p.adt,
-                                                         p.res, k))
+    e = slots ? res_gather_slots<double>(r, *slots, p, k)
         : inv ? launch_res_calc_gather<double>(r.ctx(), *inv, p.pedge, p.pecell, p.x, p.q,
                                                p.adt, p.res, k)
               : run_res_calc<double>(r.ctx(), p, plan, r.opt_inc_mode);
@@ -265,10 +280,7 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
                          (const float *)a[2].dat->data_d, (const float *)a[4].dat->data_d,
                          (float *)a[6].dat->data_d, k};
     r.begin_loop(name);
-    e = slots ? (r.opt_gather_kernel == OP2B_GATHER_LANES
-                     ? launch_res_calc_gather4<float>(r.ctx(), *slots, p.x, p.q, p.adt, p.res, k)
-                     : launch_res_calc_gather_cell4<float>(r.ctx(), *slots, p.x, p.q, p.adt,
-                                                         p.res, k))
+    e = slots ? res_gather_slots<float>(r, *slots, p, k)
         : inv ? launch_res_calc_gather<float>(r.ctx(), *inv, p.pedge, p.pecell, p.x, p.q,
                                               p.adt, p.res, k)
               : run_res_calc<float>(r.ctx(), p, plan, r.opt_inc_mode);

@@ -44,8 +44,10 @@ struct Runtime {
   int opt_cache_line = 128;
   int opt_maps_base = 0;
   int opt_inc_mode = OP2B_INC_GATHER;
-  int opt_gather_kernel = 3;  // OP2B_GATHER_CELL4 (gather.h)
+  int opt_gather_kernel = 5;  // OP2B_GATHER_REGPIPE (gather.h)
   int opt_gather_minb = 0;    // __launch_bounds__ minimum blocks of the gather kernels
+  int opt_pipe_block = 128;   // threads per CTA of the pipelined gather (64, 96, 128, 256)
+  int opt_pipe_hints = 0;     // register pipeline: evict-first hints on once-read streams
   int opt_plan_mode = 0;      // 0 = parallel block colouring, 1 = serial greedy (bit-exact)
   bool opt_check_plans = false;
 

@@ -26,7 +26,7 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas"
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wno-unused-function", f"-I{INCLUDE}",
              f"-I{CSRC}"]
 # files whose floating-point results are compared bit for bit with the reference
-FMAD_OFF = {"airfoil_loops.cu", "airfoil_staged.cu", "airfoil_gather.cu", "batch.cu",
+FMAD_OFF = {"airfoil_loops.cu", "airfoil_staged.cu", "airfoil_gather.cu", "airfoil_pipe.cu", "batch.cu",
             "update_noalloc.cu"}
 # sources not (yet) part of the library
 EXCLUDE = set()

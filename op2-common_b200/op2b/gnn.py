@@ -415,13 +415,15 @@ class GraphNet:
         self._mlp_bwd("enc_edge", E, dyE, w, ws["_edge_in"].data_ptr(), EDGE_IN, ws=ws)
         self.launches += 2
 
-    def loss_grad(self, dg, node_in, edge_in, target, ws=None):
+    def loss_grad(self, dg, node_in, edge_in, target, ws=None, zero_loss=True):
         """Forward, MSE against target (N x 4 float device tensor, normalised
-        units), backward.  Returns the loss as a device tensor (1 float)."""
+        units), backward.  Returns the device loss accumulator (1 float): this
+        step's loss, or the running sum when zero_loss is False."""
         N = dg["N"]
         ws = ws or self.workspace(N, dg["E"], True)
         out = self.forward(dg, node_in, edge_in, train=True, ws=ws)
-        _call("op2b_gnn_memset", ws["loss"].data_ptr(), 0, 4, self.stream)
+        if zero_loss:
+            _call("op2b_gnn_memset", ws["loss"].data_ptr(), 0, 4, self.stream)
         _call("op2b_gnn_mse", N, 4, out.data_ptr(), OUT, target.data_ptr(), ws["dOut"].data_ptr(),
               ws["loss"].data_ptr(), 1.0 / (4.0 * N), self.stream)
         self.launches += 1

@@ -234,7 +234,7 @@ def solve(mesh: Mesh, consts, q0=None, tol_abs=None, tol_rel=None, max_iter=4000
         rms0 = h[0][0]
         tol = tol_abs if tol_abs is not None else tol_rel * rms0
         it, rms = 1, rms0
-        aborted = abort_above is not None and rms0 > abort_above
+        aborted = abort_above is not None and not (rms0 <= abort_above)   # NaN aborts too
         while not aborted and rms >= tol and it < max_iter:
             rms = app.iterate(1)[0][0]
             it += 1

@@ -127,13 +127,22 @@ def test_colouring_is_deterministic_and_matches_atomics(op2, part):
         assert np.max(np.abs(runs[mode][0] / c1 - 1)) < 1e-12
 
 
+GATHER_KERNELS = [(1, 0), (2, 0), (3, 0), (4, 64), (4, 96), (4, 128), (4, 256), (5, 64), (5, 96),
+                  (5, 128), (5, 256)]
+
+
+@pytest.mark.parametrize("kernel", GATHER_KERNELS, ids=lambda k: f"g{k[0]}b{k[1]}")
 @pytest.mark.parametrize("fixture", ["airfoil_24x12_s3.npz", "airfoil_240x120_s1.npz"])
-def test_gather_mode_is_bit_exact_with_reference(op2, fixture):
+def test_gather_mode_is_bit_exact_with_reference(op2, fixture, kernel):
     """inc_mode 3 adds each cell's increments in element order starting from
     res, as the reference's sequential loop does: q after 100 iterations is
     bit-identical to the reference's own build (rms differs only by the order
-    of its global sum)."""
+    of its global sum) -- for every gather kernel (CSR walk, 4 lanes, unrolled
+    slot records, shared-memory pipeline at each block size)."""
     op2.set_option("inc_mode", L.OP2B_INC_GATHER)
+    op2.set_option("gather_kernel", kernel[0])
+    if kernel[1]:
+        op2.set_option("pipe_block", kernel[1])
     gd = np.load(f"{GOLDEN}/{fixture}")
     m = M.channel_bump(int(gd["I"]), int(gd["J"]), seed=int(gd["seed"]))
     app = Airfoil(m)
@@ -149,6 +158,22 @@ def test_gather_mode_is_bit_exact_with_reference(op2, fixture):
     assert np.array_equal(np.array([h[2] for h in hist]), gd["errloc"])
     # the rms sum over ~1e5 terms in a different order: ~1e-14 relative
     assert np.max(np.abs(np.array([h[0] for h in hist]) / gd["rms"] - 1)) < 1e-13
+
+
+@pytest.mark.parametrize("hints", [0, 1])
+def test_pipelined_kernels_are_bit_identical(op2, hints):
+    """res_calc's register pipeline, with and without cache hints, against the
+    one-pass slot-record kernel."""
+    m = M.channel_bump(240, 120, seed=6)
+    out = []
+    for gk in (3, 5):
+        op2.set_option("gather_kernel", gk)
+        op2.set_option("pipe_hints", hints)
+        app = Airfoil(m)
+        app.iterate(5)
+        out.append(app.fetch())
+    for k in ("q", "adt", "res"):
+        assert np.array_equal(out[0][k], out[1][k]), k
 
 
 def test_large_mesh_one_iteration_against_oracle(op2):
@@ -168,7 +193,9 @@ def test_large_mesh_one_iteration_against_oracle(op2):
     assert np.all(np.abs(r.sum(axis=0)) <= 1e-9 * np.abs(r).sum(axis=0))
 
 
-def test_mixed_precision_against_fp32_restatement(op2):
+@pytest.mark.parametrize("kernel", [3, 4, 5])
+def test_mixed_precision_against_fp32_restatement(op2, kernel):
+    op2.set_option("gather_kernel", kernel)
     m = M.channel_bump(120, 60, seed=4)
     c = M.airfoil_constants()
     st32, rms32 = O.airfoil_run_mixed(m, c, 50)
