@@ -61,9 +61,13 @@ def parse():
     p.add_argument("--inc-mode", type=int, default=3,
                    help="0 atomics, 1 block/thread colouring, 2 staged hybrid, 3 gather")
     p.add_argument("--part-size", type=int, default=0)
-    p.add_argument("--gather-kernel", type=int, default=5,
-                   help="inc_mode 3 kernel: 1 csr, 2 lanes, 3 cell4, 4 shared-memory pipeline, 5 register pipeline")
-    p.add_argument("--pipe-block", type=int, default=128)
+    p.add_argument("--gather-kernel", type=int, default=6,
+                   help="inc_mode 3 kernel: 1 csr, 2 lanes, 3 cell4, 4 shared-memory pipeline, "
+                        "5 register pipeline, 6 register pipeline over corner records")
+    p.add_argument("--pipe-block", type=int, default=256)
+    p.add_argument("--e2e-iters", type=int, default=1000,
+                   help="length of the end-to-end job (the 2400x1200 configuration runs 1000 "
+                        "iterations)")
     p.add_argument("--precision", default="f64", choices=["f64", "mixed"])
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
@@ -302,9 +306,9 @@ def main():
                                  "launches_per_iter": v["launches"] / 20})
         # gather kernels of inc_mode 3, and the pipelined direct loop's switches
         for o in ({"gather_kernel": 1}, {"gather_kernel": 3}, {"gather_kernel": 4},
-                  {"gather_kernel": 5, "pipe_block": 64}, {"gather_kernel": 5, "pipe_block": 128},
-                  {"gather_kernel": 5, "pipe_block": 256},
-                  {"gather_kernel": 5, "pipe_block": 128, "pipe_hints": 1}):
+                  {"gather_kernel": 5, "pipe_block": 128}, {"gather_kernel": 5, "pipe_block": 256},
+                  {"gather_kernel": 6, "pipe_block": 128}, {"gather_kernel": 6, "pipe_block": 256},
+                  {"gather_kernel": 6, "pipe_block": 256, "bres_kernel": 0}):
             v = timed_run(L, Airfoil, m, dtype, "rcm", 3, args.part_size, 20, 3, torch, barrier,
                           opts=o)
             lp = v["loops"]
@@ -338,26 +342,29 @@ def main():
         for k, v in gopts.items():
             L.set_option(k, v)
         barrier()
+        K = max(args.e2e_iters, 1)
         t0 = time.perf_counter()
         app2 = Airfoil(hm, dtype=dtype)
         if args.numbering == "rcm":
             app2.renumber()
-        app2.iterate(args.steps)
+        app2.iterate(K)
         q = L.op_fetch_data(app2.p_q)
         t1 = time.perf_counter()
         barrier()
-        ms_e2e = max_over_ranks(1e3 * (t1 - t0) / max(args.steps, 1))
+        ms_e2e = max_over_ranks(1e3 * (t1 - t0) / K)
         es = np.dtype(dtype).itemsize
+        # x, the maps, the bound flags and q are uploaded; qold/adt/res are
+        # declared without data (zeroed on the device)
         h2d = (m.x.size * es + (m.cell.size + m.edge.size + m.ecell.size + m.bedge.size
                                 + m.becell.size + m.bound.size) * 4
-               + m.ncell * 4 * es * 3 + m.ncell * es + args.steps * 2 * 8 * 3)
-        d2h = q.nbytes + args.steps * 2 * 32
-        e2e = {"value": ms_e2e, "unit": "ms/iter",
-               "h2d_bytes_per_step": int(h2d / max(args.steps, 1)),
-               "d2h_bytes_per_step": int(d2h / max(args.steps, 1)),
-               "note": "per iteration of a whole job through the API: op_decl_* uploads from "
-                       "pinned host memory, op_renumber, K iterations (rms read back every "
-                       "update), op_fetch_data(q)"}
+               + m.ncell * 4 * es)
+        d2h = q.nbytes + K * 2 * 32  # q, and the update's reduction read back per call
+        e2e = {"value": ms_e2e, "unit": "ms/iter", "iterations": K,
+               "h2d_bytes_per_step": int(h2d / K),
+               "d2h_bytes_per_step": int(d2h / K),
+               "note": f"per iteration of a whole {K}-iteration job through the API: "
+                       "op_decl_* uploads (mesh arrays pinned), op_renumber, the iterations "
+                       "(rms read back after every update), op_fetch_data(q)"}
         L.op_exit()
 
     # ---------------------------------------------------------- CPU baseline (rank 0, N=1)

@@ -397,6 +397,7 @@ template cudaError_t launch_res_calc_gather_cell4<float>(const LaunchCtx &, cons
 struct SlotCache {
   op_map inc = nullptr, nodes = nullptr;
   SlotRecords rec{};
+  bool corners_tried = false;
   std::vector<void *> owned;
   ~SlotCache() {
     for (void *p : owned) cudaFree(p);
@@ -456,7 +457,216 @@ const SlotRecords *get_slot_records(op_map pecell, op_map pedge) {
   return &slot_cache().back()->rec;
 }
 
-void release_slot_records() { slot_cache().clear(); }
+// corner records of every cell from its slot records (see gather.h); *bad is
+// set when a cell's valid slots touch more than four distinct nodes
+__global__ void k_build_corners(int ncell, const int4 *rec_o, const int4 *rec_n1,
+                                const uint4 *rec_n2, int4 *cn, unsigned *meta, int *bad) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  const int4 a4 = rec_n1[c];
+  const uint4 b4 = rec_n2[c];
+  const int na[4] = {a4.x, a4.y, a4.z, a4.w};
+  const unsigned nb[4] = {b4.x, b4.y, b4.z, b4.w};
+  int node[4] = {0, 0, 0, 0};
+  int cnt = 0;
+  unsigned m = 0;
+  bool over = false;
+  for (int s = 0; s < 4; s++) {
+    if (!(nb[s] & kValidBit)) continue;
+    const int ends[2] = {na[s], (int)(nb[s] & (kRoleBit - 1))};
+    unsigned idx[2];
+    for (int e = 0; e < 2; e++) {
+      int j = 0;
+      while (j < cnt && node[j] != ends[e]) j++;
+      if (j == cnt) {
+        if (cnt == 4) {
+          over = true;
+          j = 0;
+        } else {
+          node[cnt++] = ends[e];
+        }
+      }
+      idx[e] = (unsigned)j;
+    }
+    m |= (1u | ((nb[s] & kRoleBit) ? 2u : 0u) | (idx[0] << 2) | (idx[1] << 4)) << (8 * s);
+  }
+  for (int j = cnt; j < 4; j++) node[j] = node[0];
+  cn[c] = make_int4(node[0], node[1], node[2], node[3]);
+  meta[c] = m;
+  if (over) atomicOr(bad, 1);
+}
+
+const SlotRecords *get_corner_records(op_map pecell, op_map pedge) {
+  const SlotRecords *base = get_slot_records(pecell, pedge);
+  if (!base) return nullptr;
+  SlotCache *sc = nullptr;
+  for (auto &p : slot_cache())
+    if (&p->rec == base) sc = p.get();
+  if (!sc || sc->corners_tried) return base;
+  sc->corners_tried = true;
+  int n = base->ncell;
+  // an isolated cell's unused corners read node 0: there must be one
+  if (!base->usable || n <= 0 || pedge->to->size <= 0) return base;
+  Runtime &r = rt();
+  cudaStream_t s = r.stream;
+  int4 *cn = nullptr;
+  unsigned *meta = nullptr;
+  int *bad = nullptr;
+  if (cudaMalloc(&cn, sizeof(int4) * (size_t)n) != cudaSuccess ||
+      cudaMalloc(&meta, sizeof(unsigned) * (size_t)n) != cudaSuccess ||
+      cudaMalloc(&bad, sizeof(int)) != cudaSuccess) {
+    cudaFree(cn);
+    cudaFree(meta);
+    set_error("corner records: out of device memory");
+    return nullptr;
+  }
+  cudaMemsetAsync(bad, 0, sizeof(int), s);
+  k_build_corners<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
+      n, reinterpret_cast<const int4 *>(base->o), reinterpret_cast<const int4 *>(base->n1),
+      reinterpret_cast<const uint4 *>(base->n2), cn, meta, bad);
+  r.launches += 1;
+  int h_bad = 1;
+  cudaMemcpyAsync(&h_bad, bad, sizeof(int), cudaMemcpyDeviceToHost, s);
+  bool ok = cuda_ok(cudaStreamSynchronize(s), "corner records");
+  cudaFree(bad);
+  if (!ok) {
+    cudaFree(cn);
+    cudaFree(meta);
+    return nullptr;
+  }
+  if (h_bad) {  // not a quadrilateral-style mesh: the slot-record kernels serve it
+    cudaFree(cn);
+    cudaFree(meta);
+    return base;
+  }
+  sc->owned.push_back(cn);
+  sc->owned.push_back(meta);
+  sc->rec.cn = reinterpret_cast<const int *>(cn);
+  sc->rec.meta = meta;
+  sc->rec.corners = true;
+  return base;
+}
+
+// ------------------------------------------------------------------ bres_calc records
+
+__global__ void k_build_bres_records(int nrows, const int *rows, const long long *off,
+                                     const int *ent, const int2 *pbedge, int4 *rec) {
+  int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nrows) return;
+  const int c = rows[r];
+  for (long long i = off[c]; i < off[c + 1]; i++) {
+    const int be = ent[i];  // dim-1 map: entry = boundary edge
+    const int2 nn = pbedge[be];
+    rec[i] = make_int4(i == off[c] ? c : -1 - c, nn.x, nn.y, be);
+  }
+}
+
+struct BresCache {
+  op_map inc = nullptr, nodes = nullptr;
+  BresRecords rec{};
+  int4 *buf = nullptr;
+  ~BresCache() { cudaFree(buf); }
+};
+
+static std::vector<std::unique_ptr<BresCache>> &bres_cache() {
+  static std::vector<std::unique_ptr<BresCache>> v;
+  return v;
+}
+
+const BresRecords *get_bres_records(op_map pbecell, op_map pbedge) {
+  for (auto &b : bres_cache())
+    if (b->inc == pbecell && b->nodes == pbedge) return &b->rec;
+  if (pbecell->dim != 1) {
+    set_error("bres_calc records: expected a dim-1 map (bedges -> cells)");
+    return nullptr;
+  }
+  const InvMap *inv = get_inverse_map(pbecell);
+  if (!inv) return nullptr;
+  Runtime &r = rt();
+  auto bc = std::make_unique<BresCache>();
+  bc->inc = pbecell;
+  bc->nodes = pbedge;
+  const int n = pbecell->from->size;
+  if (n > 0) {
+    if (cudaMalloc(&bc->buf, sizeof(int4) * (size_t)n) != cudaSuccess) {
+      set_error("bres_calc records: out of device memory");
+      return nullptr;
+    }
+    if (inv->nrows > 0) {
+      k_build_bres_records<<<(unsigned)((inv->nrows + 255) / 256), 256, 0, r.stream>>>(
+          inv->nrows, inv->rows, inv->off, inv->ent,
+          reinterpret_cast<const int2 *>(pbedge->map_d), bc->buf);
+      r.launches += 1;
+    }
+    if (!cuda_ok(cudaStreamSynchronize(r.stream), "bres_calc records")) return nullptr;
+  }
+  bc->rec = BresRecords{bc->buf, n};
+  bres_cache().push_back(std::move(bc));
+  return &bres_cache().back()->rec;
+}
+
+// One thread per record; the thread of a cell's first record adds all of the
+// cell's boundary increments in ascending edge order, starting from res[c]
+// (the sequential reference's order).  Two dependent load levels: the record,
+// then the nodes, the flag and the cell's q, adt and res.
+template <typename T>
+__global__ void __launch_bounds__(128)
+k_bres_records(int n, const int4 *__restrict__ rec, const int *__restrict__ bound,
+               const T *__restrict__ x, const T *__restrict__ q, const T *__restrict__ adt,
+               T *__restrict__ res, AirConst<T> k) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int4 r = __ldg(rec + i);
+  if (r.x < 0) return;  // continuation: handled by the cell's first record
+  const int c = r.x;
+  T qc[4], acc[4];
+  Vec<T>::ld4(q + 4 * (size_t)c, qc);
+  Vec<T>::ld4_rw(res + 4 * (size_t)c, acc);
+  const T ac = __ldg(adt + c);
+  for (int j = i;;) {
+    T x1x, x1y, x2x, x2y, rr[4];
+    Vec<T>::ld2(x + 2 * (size_t)r.y, x1x, x1y);
+    Vec<T>::ld2(x + 2 * (size_t)r.z, x2x, x2y);
+    const int bnd = __ldg(bound + r.w);
+    air_bflux<T>(x1x, x1y, x2x, x2y, qc, ac, bnd, k, rr);
+    if (bnd == 1) {  // a wall edge leaves components 0 and 3 untouched
+      acc[1] += rr[1];
+      acc[2] += rr[2];
+    } else {
+#pragma unroll
+      for (int m = 0; m < 4; m++) acc[m] += rr[m];
+    }
+    if (++j >= n) break;
+    r = __ldg(rec + j);
+    if (r.x >= 0) break;
+  }
+  Vec<T>::st4(res + 4 * (size_t)c, acc);
+}
+
+template <typename T>
+cudaError_t launch_bres_calc_records(const LaunchCtx &c, const BresRecords &b, const int *bound,
+                                     const T *x, const T *q, const T *adt, T *res,
+                                     const AirConst<T> &k) {
+  if (b.n <= 0) return cudaSuccess;
+  k_bres_records<T><<<(unsigned)((b.n + 127) / 128), 128, 0, c.stream>>>(b.n, b.rec, bound, x, q,
+                                                                        adt, res, k);
+  c.count();
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_bres_calc_records<double>(const LaunchCtx &, const BresRecords &,
+                                                      const int *, const double *,
+                                                      const double *, const double *, double *,
+                                                      const AirConst<double> &);
+template cudaError_t launch_bres_calc_records<float>(const LaunchCtx &, const BresRecords &,
+                                                     const int *, const float *, const float *,
+                                                     const float *, float *,
+                                                     const AirConst<float> &);
+
+void release_slot_records() {
+  slot_cache().clear();
+  bres_cache().clear();
+}
 
 template <typename T>
 cudaError_t launch_res_calc_gather4(const LaunchCtx &c, const SlotRecords &s, const T *x,

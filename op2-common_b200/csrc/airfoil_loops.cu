@@ -76,9 +76,9 @@ cudaError_t launch_copy(const LaunchCtx &c, const void *src, void *dst, size_t b
 // ---------------------------------------------------------------- adt_calc
 
 template <typename T>
-__global__ void __launch_bounds__(256)
-k_adt_calc(int ncell, const int4 *__restrict__ pcell, const T *__restrict__ x,
-           const T *__restrict__ q, T *__restrict__ adt, AirConst<T> k) {
+__device__ __forceinline__ void adt_calc_cells(int ncell, const int4 *__restrict__ pcell,
+                                               const T *__restrict__ x, const T *__restrict__ q,
+                                               T *__restrict__ adt, const AirConst<T> &k) {
   int stride = gridDim.x * blockDim.x;
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < ncell; n += stride) {
     int4 c = __ldg(pcell + n);
@@ -93,16 +93,37 @@ k_adt_calc(int ncell, const int4 *__restrict__ pcell, const T *__restrict__ x,
   }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_adt_calc(int ncell, const int4 *__restrict__ pcell, const T *__restrict__ x,
+           const T *__restrict__ q, T *__restrict__ adt, AirConst<T> k) {
+  adt_calc_cells<T>(ncell, pcell, x, q, adt, k);
+}
+
+// the same loop with a register cap (MINB CTAs of 256 threads per SM)
+template <typename T, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+k_adt_calc_mb(int ncell, const int4 *__restrict__ pcell, const T *__restrict__ x,
+              const T *__restrict__ q, T *__restrict__ adt, AirConst<T> k) {
+  adt_calc_cells<T>(ncell, pcell, x, q, adt, k);
+}
+
 // (A register-pipelined persistent form of this loop -- the next cell's node
 // gathers in flight during the current cell's square roots -- needs 92
 // registers instead of 54 and measured 3.93 TB/s against this kernel's 4.14 TB/s
 // at 2400x1200: for adt_calc the occupancy is worth more than the prefetch.)
 template <typename T>
 cudaError_t launch_adt_calc(const LaunchCtx &c, int ncell, const int *pcell, const T *x,
-                            const T *q, T *adt, const AirConst<T> &k) {
+                            const T *q, T *adt, const AirConst<T> &k, int minb) {
   if (ncell <= 0) return cudaSuccess;
-  k_adt_calc<T><<<grid_for(c, ncell, 256, 8), 256, 0, c.stream>>>(
-      ncell, reinterpret_cast<const int4 *>(pcell), x, q, adt, k);
+  const int g = grid_for(c, ncell, 256, 8);
+  const int4 *pc = reinterpret_cast<const int4 *>(pcell);
+  if (minb >= 8)
+    k_adt_calc_mb<T, 8><<<g, 256, 0, c.stream>>>(ncell, pc, x, q, adt, k);
+  else if (minb >= 6)
+    k_adt_calc_mb<T, 6><<<g, 256, 0, c.stream>>>(ncell, pc, x, q, adt, k);
+  else
+    k_adt_calc<T><<<g, 256, 0, c.stream>>>(ncell, pc, x, q, adt, k);
   c.count();
   return cudaGetLastError();
 }
@@ -315,9 +336,10 @@ cudaError_t launch_update(const LaunchCtx &c, int ncell, const T *qold, T *q, T 
 // ---------------------------------------------------------------- instantiations
 
 template cudaError_t launch_adt_calc<double>(const LaunchCtx &, int, const int *, const double *,
-                                             const double *, double *, const AirConst<double> &);
+                                             const double *, double *, const AirConst<double> &,
+                                             int);
 template cudaError_t launch_adt_calc<float>(const LaunchCtx &, int, const int *, const float *,
-                                            const float *, float *, const AirConst<float> &);
+                                            const float *, float *, const AirConst<float> &, int);
 template cudaError_t launch_res_calc_atomic<double>(const LaunchCtx &, int, const int *,
                                                     const int *, const double *, const double *,
                                                     const double *, double *,

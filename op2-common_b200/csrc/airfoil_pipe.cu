@@ -336,7 +336,160 @@ cudaError_t launch_regpipe(K kern, int nt, const LaunchCtx &ctx, const SlotRecor
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// The register pipeline over corner records (option gather_kernel 6): a
+// cell's four corner nodes are gathered once (four 16-byte loads for FP64
+// instead of eight) and each slot picks its edge's two nodes from them by the
+// 2-bit corner indices of meta; the record is 36 bytes a cell instead of 48.
+// The picked coordinates are the same doubles, so fluxes and sums are
+// bit-identical to the slot-record kernels.
+
+struct CornerRec {
+  int4 o, cn;
+  unsigned meta;
+};
+
+__device__ __forceinline__ CornerRec load_crec(const int4 *ro, const int4 *rcn,
+                                               const unsigned *rmeta, int c, int ncell) {
+  CornerRec r;
+  if (c < ncell) {
+    r.o = __ldg(ro + c);
+    r.cn = __ldg(rcn + c);
+    r.meta = __ldg(rmeta + c);
+  } else {
+    r.o = r.cn = make_int4(0, 0, 0, 0);
+    r.meta = 0u;
+  }
+  return r;
+}
+
+template <typename T> struct CornerOps {
+  T qc[4], rs[4], qo[4][4], ao[4], xn[4][2], ac;
+  unsigned meta;
+};
+
+template <typename T>
+__device__ __forceinline__ void load_corner_cell(CornerOps<T> &d, int c, const CornerRec &r,
+                                                 const T *__restrict__ x,
+                                                 const T *__restrict__ q,
+                                                 const T *__restrict__ adt,
+                                                 const T *__restrict__ res) {
+  Vec<T>::ld4(q + 4 * (size_t)c, d.qc);
+  Vec<T>::ld4_rw(res + 4 * (size_t)c, d.rs);
+  d.ac = __ldg(adt + c);
+  const int nd[4] = {r.cn.x, r.cn.y, r.cn.z, r.cn.w};
+#pragma unroll
+  for (int j = 0; j < 4; j++) Vec<T>::ld2(x + 2 * (size_t)nd[j], d.xn[j][0], d.xn[j][1]);
+  const int o[4] = {r.o.x, r.o.y, r.o.z, r.o.w};
+#pragma unroll
+  for (int s = 0; s < 4; s++) {
+    const int oo = ((r.meta >> (8 * s)) & 1u) ? o[s] : c;
+    Vec<T>::ld4(q + 4 * (size_t)oo, d.qo[s]);
+    d.ao[s] = __ldg(adt + oo);
+  }
+  d.meta = r.meta;
+}
+
+// coordinate `comp` of corner i (0..3), by selects (no local-memory indexing)
+template <typename T>
+__device__ __forceinline__ T corner(const T (&xn)[4][2], unsigned i, int comp) {
+  const T lo = (i & 1u) ? xn[1][comp] : xn[0][comp];
+  const T hi = (i & 1u) ? xn[3][comp] : xn[2][comp];
+  return (i & 2u) ? hi : lo;
+}
+
+template <typename T>
+__device__ __forceinline__ void compute_corner(const CornerOps<T> &d, int c, T *__restrict__ res,
+                                               const AirConst<T> &k) {
+  T acc[4] = {d.rs[0], d.rs[1], d.rs[2], d.rs[3]};
+  T ric, pc;  // the cell's own terms, once for its <= 4 edges
+  air_prim<T>(d.qc, k, ric, pc);
+#pragma unroll
+  for (int s = 0; s < 4; s++) {
+    const unsigned m = (d.meta >> (8 * s)) & 0xffu;
+    if (!(m & 1u)) continue;
+    const unsigned a = (m >> 2) & 3u, b = (m >> 4) & 3u;
+    const T x1x = corner<T>(d.xn, a, 0), x1y = corner<T>(d.xn, a, 1);
+    const T x2x = corner<T>(d.xn, b, 0), x2y = corner<T>(d.xn, b, 1);
+    T f[4], rio, po;
+    air_prim<T>(d.qo[s], k, rio, po);
+    if (m & 2u) {
+      air_flux_prim<T>(x1x, x1y, x2x, x2y, d.qo[s], d.qc, rio, po, ric, pc, d.ao[s], d.ac, k, f);
+#pragma unroll
+      for (int j = 0; j < 4; j++) acc[j] -= f[j];
+    } else {
+      air_flux_prim<T>(x1x, x1y, x2x, x2y, d.qc, d.qo[s], ric, pc, rio, po, d.ac, d.ao[s], k, f);
+#pragma unroll
+      for (int j = 0; j < 4; j++) acc[j] += f[j];
+    }
+  }
+  Vec<T>::st4(res + 4 * (size_t)c, acc);
+}
+
+template <typename T, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
+k_res_gather_corner(int ncell, const int4 *__restrict__ rec_o, const int4 *__restrict__ rec_cn,
+                    const unsigned *__restrict__ rec_meta, const T *__restrict__ x,
+                    const T *__restrict__ q, const T *__restrict__ adt, T *__restrict__ res,
+                    AirConst<T> k) {
+  const int G = gridDim.x * NT;
+  int c = blockIdx.x * NT + threadIdx.x;
+  if (c >= ncell) return;
+  CornerOps<T> cur, nxt;
+  CornerRec r1 = load_crec(rec_o, rec_cn, rec_meta, c + G, ncell);
+  {
+    const CornerRec r0 = load_crec(rec_o, rec_cn, rec_meta, c, ncell);
+    load_corner_cell<T>(cur, c, r0, x, q, adt, res);
+  }
+  for (; c < ncell; c += G) {
+    const CornerRec r2 = load_crec(rec_o, rec_cn, rec_meta, c + 2 * G, ncell);
+    if (c + G < ncell) load_corner_cell<T>(nxt, c + G, r1, x, q, adt, res);
+    compute_corner<T>(cur, c, res, k);
+    cur = nxt;
+    r1 = r2;
+  }
+}
+
+template <typename T, typename K>
+cudaError_t launch_corner(K kern, int nt, const LaunchCtx &ctx, const SlotRecords &s,
+                          const T *x, const T *q, const T *adt, T *res, const AirConst<T> &k) {
+  int per_sm = 1;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nt, 0);
+  if (e != cudaSuccess) return e;
+  long long blocks = (long long)ctx.nsm * (per_sm < 1 ? 1 : per_sm);
+  const long long need = (s.ncell + nt - 1) / nt;
+  if (blocks > need) blocks = need;
+  kern<<<(unsigned)blocks, nt, 0, ctx.stream>>>(
+      s.ncell, reinterpret_cast<const int4 *>(s.o), reinterpret_cast<const int4 *>(s.cn),
+      s.meta, x, q, adt, res, k);
+  ctx.count();
+  return cudaGetLastError();
+}
+
 }  // namespace
+
+template <typename T>
+cudaError_t launch_res_calc_gather_corner(const LaunchCtx &ctx, const SlotRecords &s, const T *x,
+                                          const T *q, const T *adt, T *res,
+                                          const AirConst<T> &k, int block, int minb) {
+  if (s.ncell <= 0) return cudaSuccess;
+  if (block == 64)
+    return minb >= 6 ? launch_corner(k_res_gather_corner<T, 64, 6>, 64, ctx, s, x, q, adt, res, k)
+                     : launch_corner(k_res_gather_corner<T, 64, 5>, 64, ctx, s, x, q, adt, res, k);
+  if (block == 256)
+    return launch_corner(k_res_gather_corner<T, 256, 1>, 256, ctx, s, x, q, adt, res, k);
+  return minb >= 3 ? launch_corner(k_res_gather_corner<T, 128, 3>, 128, ctx, s, x, q, adt, res, k)
+                   : launch_corner(k_res_gather_corner<T, 128, 1>, 128, ctx, s, x, q, adt, res, k);
+}
+
+template cudaError_t launch_res_calc_gather_corner<double>(const LaunchCtx &, const SlotRecords &,
+                                                           const double *, const double *,
+                                                           const double *, double *,
+                                                           const AirConst<double> &, int, int);
+template cudaError_t launch_res_calc_gather_corner<float>(const LaunchCtx &, const SlotRecords &,
+                                                          const float *, const float *,
+                                                          const float *, float *,
+                                                          const AirConst<float> &, int, int);
 
 template <typename T>
 cudaError_t launch_res_calc_gather_regpipe(const LaunchCtx &ctx, const SlotRecords &s,

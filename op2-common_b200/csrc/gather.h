@@ -29,8 +29,19 @@ struct SlotRecords {
   const unsigned *n2;
   int ncell;
   bool usable;
+  // Corner form (built on request by get_corner_records): in a quadrilateral
+  // mesh the <= 4 interior edges of a cell touch at most four distinct nodes.
+  // cn[c] lists them (first appearance over slots 0..3, an edge's first node
+  // before its second; unused corners repeat the first one) and byte s of
+  // meta[c] describes slot s: bit 0 valid, bit 1 role (the cell is the edge's
+  // second cell), bits 2-3 / 4-5 the corners of the edge's first / second
+  // node.  corners is false when some cell's edges touch more than four nodes.
+  const int *cn;
+  const unsigned *meta;
+  bool corners;
 };
 const SlotRecords *get_slot_records(op_map pecell, op_map pedge);
+const SlotRecords *get_corner_records(op_map pecell, op_map pedge);
 void release_slot_records();
 
 template <typename T>
@@ -59,6 +70,29 @@ cudaError_t launch_res_calc_gather_regpipe(const LaunchCtx &c, const SlotRecords
 #define OP2B_GATHER_CELL4 3  // one thread per cell, four slot records, unrolled
 #define OP2B_GATHER_PIPE 4   // cell4's order, shared-memory software pipeline
 #define OP2B_GATHER_REGPIPE 5  // cell4's order, register software pipeline
+#define OP2B_GATHER_CORNER 6   // the register pipeline over corner records
+
+// airfoil_pipe.cu: the register pipeline over corner records (four node
+// gathers per cell instead of eight); block 64, 128 or 256 threads, minb the
+// __launch_bounds__ minimum CTAs per SM (1 = no register cap)
+template <typename T>
+cudaError_t launch_res_calc_gather_corner(const LaunchCtx &c, const SlotRecords &s, const T *x,
+                                          const T *q, const T *adt, T *res,
+                                          const AirConst<T> &k, int block, int minb);
+
+// Boundary records for bres_calc's gather, one per (cell, boundary edge) in
+// ascending (cell, edge) order: {cell, node 1, node 2, edge}; a record that
+// continues the previous record's cell stores -1 - cell there.  Built from
+// the maps (immutable between renumberings) and cached like the slot records.
+struct BresRecords {
+  const int4 *rec;
+  int n;
+};
+const BresRecords *get_bres_records(op_map pbecell, op_map pbedge);
+template <typename T>
+cudaError_t launch_bres_calc_records(const LaunchCtx &c, const BresRecords &b, const int *bound,
+                                     const T *x, const T *q, const T *adt, T *res,
+                                     const AirConst<T> &k);
 
 template <typename T>
 cudaError_t launch_res_calc_gather(const LaunchCtx &c, const InvMap &inv, const int *pedge,

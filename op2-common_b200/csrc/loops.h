@@ -41,9 +41,16 @@ struct RedScratch {
 
 cudaError_t launch_copy(const LaunchCtx &c, const void *src, void *dst, size_t bytes);
 
+// map_check.cu: *first_bad = lowest i with map[i] outside [0, nto); the
+// caller initialises it to ~0ull
+cudaError_t launch_map_check(const LaunchCtx &c, const int *map, long long n, int nto,
+                             unsigned long long *first_bad);
+
+// minb: __launch_bounds__ minimum CTAs of 256 threads per SM (0 or 1 = no
+// register cap; 6 caps registers at 40, 8 at 32)
 template <typename T>
 cudaError_t launch_adt_calc(const LaunchCtx &c, int ncell, const int *pcell, const T *x,
-                            const T *q, T *adt, const AirConst<T> &k);
+                            const T *q, T *adt, const AirConst<T> &k, int minb = 0);
 template <typename T>
 cudaError_t launch_res_calc_atomic(const LaunchCtx &c, int nedge, const int *pedge,
                                    const int *pecell, const T *x, const T *q, const T *adt,

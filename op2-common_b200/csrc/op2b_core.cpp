@@ -223,6 +223,7 @@ void op_init(int argc, char **argv, int diags) {
   if (!cuda_ok(cudaHostGetDevicePointer(&r.pinned_dev, r.pinned, 0), "op_init: mapped pointer"))
     return;
   r.red.host_out = reinterpret_cast<RedSlot *>(r.pinned_dev);
+  if (!cuda_ok(cudaMalloc((void **)&r.check_d, 256), "op_init: map check word")) return;
   r.initialised = true;
   if (diags > 1)
     printf(" op2b: device %d (%s, %d SMs), stream %p\n", dev, prop.name, r.nsm,
@@ -264,6 +265,8 @@ void op_exit(void) {
   for (auto e : r.ev_free) cudaEventDestroy(e);
   r.ev_free.clear();
   cudaFree(r.red_base);
+  cudaFree(r.check_d);
+  r.check_d = nullptr;
   cudaFreeHost(r.pinned);
   cudaStreamDestroy(r.own_stream);
   r.red_base = nullptr;
@@ -272,6 +275,24 @@ void op_exit(void) {
   r.stats.clear();
   r.launches = 0;
   r.initialised = false;
+  // options return to their defaults: a later op_init starts from a clean state
+  const Runtime d{};
+  r.opt_diags = d.opt_diags;
+  r.opt_abort = d.opt_abort;
+  r.opt_timing = d.opt_timing;
+  r.opt_block_size = d.opt_block_size;
+  r.opt_part_size = d.opt_part_size;
+  r.opt_cache_line = d.opt_cache_line;
+  r.opt_maps_base = d.opt_maps_base;
+  r.opt_inc_mode = d.opt_inc_mode;
+  r.opt_gather_kernel = d.opt_gather_kernel;
+  r.opt_gather_minb = d.opt_gather_minb;
+  r.opt_bres_kernel = d.opt_bres_kernel;
+  r.opt_adt_minb = d.opt_adt_minb;
+  r.opt_pipe_block = d.opt_pipe_block;
+  r.opt_pipe_hints = d.opt_pipe_hints;
+  r.opt_plan_mode = d.opt_plan_mode;
+  r.opt_check_plans = d.opt_check_plans;
 }
 
 op_set op_decl_set(int size, char const *name) {
@@ -308,16 +329,57 @@ op_map op_decl_map(op_set from, op_set to, int dim, int *imap, char const *name)
     return nullptr;
   }
   int *h = (int *)malloc(sizeof(int) * (n ? n : 1));
-  for (size_t i = 0; i < n; i++) {
-    int v = imap[i] - r.opt_maps_base;
-    if (v < 0 || v >= to->size) {
+  int *map_d = nullptr;
+  auto bad_entry = [&](size_t i) {
+    set_error("op_decl_map: invalid data for map %s: element %zu, dimension %zu, value %d "
+              "outside [0, %d)",
+              name ? name : "", i / dim, i % dim, imap[i], to->size);
+    free(h);
+    cudaFree(map_d);
+    return nullptr;
+  };
+  if (n > 0 && !cuda_ok(cudaMalloc((void **)&map_d, n * sizeof(int)), "op_decl_map: cudaMalloc")) {
+    free(h);
+    return nullptr;
+  }
+  if (r.opt_maps_base == 0) {
+    // upload the caller's array as it is (a pinned array goes by DMA), check
+    // the range on the device and take the host copy while the copy runs
+    unsigned long long bad = ~0ull;
+    if (n > 0) {
+      if (!cuda_ok(cudaMemsetAsync(r.check_d, 0xff, sizeof(bad), r.stream), "op_decl_map") ||
+          !cuda_ok(cudaMemcpyAsync(map_d, imap, n * sizeof(int), cudaMemcpyHostToDevice,
+                                   r.stream),
+                   "op_decl_map: upload") ||
+          !cuda_ok(launch_map_check(r.ctx(), map_d, (long long)n, to->size, r.check_d),
+                   "op_decl_map: range check")) {
+        free(h);
+        cudaFree(map_d);
+        return nullptr;
+      }
+      memcpy(h, imap, sizeof(int) * n);
+      if (!cuda_ok(cudaMemcpyAsync(&bad, r.check_d, sizeof(bad), cudaMemcpyDeviceToHost,
+                                   r.stream),
+                   "op_decl_map: range check") ||
+          !cuda_ok(cudaStreamSynchronize(r.stream), "op_decl_map: upload")) {
+        free(h);
+        cudaFree(map_d);
+        return nullptr;
+      }
+    }
+    if (bad != ~0ull) return bad_entry((size_t)bad);
+  } else {
+    for (size_t i = 0; i < n; i++) {
+      int v = imap[i] - r.opt_maps_base;
+      if (v < 0 || v >= to->size) return bad_entry(i);
+      h[i] = v;
+    }
+    if (n > 0 && !cuda_ok(cudaMemcpy(map_d, h, n * sizeof(int), cudaMemcpyHostToDevice),
+                          "op_decl_map: upload")) {
       free(h);
-      set_error("op_decl_map: invalid data for map %s: element %zu, dimension %zu, value %d "
-                "outside [0, %d)",
-                name ? name : "", i / dim, i % dim, imap[i], to->size);
+      cudaFree(map_d);
       return nullptr;
     }
-    h[i] = v;
   }
   auto m = std::make_unique<op_map_core>();
   m->index = (int)r.maps.size();
@@ -325,17 +387,8 @@ op_map op_decl_map(op_set from, op_set to, int dim, int *imap, char const *name)
   m->to = to;
   m->dim = dim;
   m->map = h;
-  m->map_d = nullptr;
+  m->map_d = map_d;
   m->name = copy_str(name);
-  if (n > 0) {
-    if (!cuda_ok(cudaMalloc((void **)&m->map_d, n * sizeof(int)), "op_decl_map: cudaMalloc") ||
-        !cuda_ok(cudaMemcpy(m->map_d, h, n * sizeof(int), cudaMemcpyHostToDevice),
-                 "op_decl_map: upload")) {
-      free(h);
-      cudaFree(m->map_d);
-      return nullptr;
-    }
-  }
   if (imap) r.map_ptrs[imap] = m.get();  // op_register_map_ptr (op_lib_core.cpp:493-495)
   r.maps.push_back(std::move(m));
   return r.maps.back().get();
@@ -730,9 +783,10 @@ int op2b_set_option(const char *key, long value) {
   } else if (k == "plan_mode") {
     r.opt_plan_mode = (int)value;
   } else if (k == "gather_kernel") {
-    if (value < 1 || value > 5) {
+    if (value < 1 || value > 6) {
       set_error("op2b_set_option: gather_kernel must be 1 (csr), 2 (lanes), 3 (cell4), 4 "
-                "(shared-memory pipeline) or 5 (register pipeline)");
+                "(shared-memory pipeline), 5 (register pipeline) or 6 (register pipeline "
+                "over corner records)");
       return -1;
     }
     r.opt_gather_kernel = (int)value;
@@ -746,6 +800,18 @@ int op2b_set_option(const char *key, long value) {
     r.opt_pipe_hints = value != 0;
   } else if (k == "gather_minblocks") {
     r.opt_gather_minb = (int)value;
+  } else if (k == "bres_kernel") {
+    if (value != 0 && value != 1) {
+      set_error("op2b_set_option: bres_kernel must be 0 (inverse-map walk) or 1 (records)");
+      return -1;
+    }
+    r.opt_bres_kernel = (int)value;
+  } else if (k == "adt_minblocks") {
+    if (value < 0 || value > 8) {
+      set_error("op2b_set_option: adt_minblocks must be 0..8");
+      return -1;
+    }
+    r.opt_adt_minb = (int)value;
   } else if (k == "check_plans") {
     r.opt_check_plans = value != 0;
   } else {
@@ -769,6 +835,9 @@ long op2b_get_option(const char *key) {
   if (k == "pipe_block") return r.opt_pipe_block;
   if (k == "pipe_hints") return r.opt_pipe_hints;
   if (k == "check_plans") return r.opt_check_plans;
+  if (k == "gather_minblocks") return r.opt_gather_minb;
+  if (k == "bres_kernel") return r.opt_bres_kernel;
+  if (k == "adt_minblocks") return r.opt_adt_minb;
   if (k == "nsm") return r.nsm;
   return -1;
 }

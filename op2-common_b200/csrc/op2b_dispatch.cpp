@@ -191,12 +191,14 @@ int loop_adt_calc(const char *name, op_set set, int nargs, op_arg *a) {
     AirConst<double> k = air_consts<double>(ok);
     if (!ok) return -1;
     e = launch_adt_calc<double>(r.ctx(), C, pcell->map_d, (const double *)a[0].dat->data_d,
-                                (const double *)a[4].dat->data_d, (double *)a[5].dat->data_d, k);
+                                (const double *)a[4].dat->data_d, (double *)a[5].dat->data_d, k,
+                                r.opt_adt_minb);
   } else {
     AirConst<float> k = air_consts<float>(ok);
     if (!ok) return -1;
     e = launch_adt_calc<float>(r.ctx(), C, pcell->map_d, (const float *)a[0].dat->data_d,
-                               (const float *)a[4].dat->data_d, (float *)a[5].dat->data_d, k);
+                               (const float *)a[4].dat->data_d, (float *)a[5].dat->data_d, k,
+                               r.opt_adt_minb);
   }
   r.end_loop(bytes);
   return finish(e, name);
@@ -214,6 +216,13 @@ static cudaError_t res_gather_slots(Runtime &r, const SlotRecords &s, const ResC
       return launch_res_calc_gather_pipe<T>(r.ctx(), s, p.x, p.q, p.adt, p.res, k,
                                             r.opt_pipe_block);
     case OP2B_GATHER_REGPIPE:
+      return launch_res_calc_gather_regpipe<T>(r.ctx(), s, p.x, p.q, p.adt, p.res, k,
+                                               r.opt_pipe_block);
+    case OP2B_GATHER_CORNER:
+      if (s.corners)
+        return launch_res_calc_gather_corner<T>(r.ctx(), s, p.x, p.q, p.adt, p.res, k,
+                                                r.opt_pipe_block, r.opt_gather_minb);
+      // edges touching more than four nodes per cell: the slot-record pipeline
       return launch_res_calc_gather_regpipe<T>(r.ctx(), s, p.x, p.q, p.adt, p.res, k,
                                                r.opt_pipe_block);
     default:
@@ -247,7 +256,10 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
   const InvMap *inv = nullptr;
   const SlotRecords *slots = nullptr;
   if (r.opt_inc_mode == OP2B_INC_GATHER) {
-    if (r.opt_gather_kernel != OP2B_GATHER_CSR) {
+    if (r.opt_gather_kernel == OP2B_GATHER_CORNER) {
+      slots = get_corner_records(pecell, pedge);
+      if (!slots) return -1;
+    } else if (r.opt_gather_kernel != OP2B_GATHER_CSR) {
       slots = get_slot_records(pecell, pedge);
       if (!slots) return -1;
     }
@@ -312,7 +324,11 @@ int loop_bres_calc(const char *name, op_set set, int nargs, op_arg *a) {
   double bytes = 16.0 * B + (double)rb * (2.0 + 4.0 + 1.0 + 8.0) * B;
   Plan *plan = nullptr;
   const InvMap *inv = nullptr;
-  if (r.opt_inc_mode == OP2B_INC_GATHER) {
+  const BresRecords *brec = nullptr;
+  if (r.opt_inc_mode == OP2B_INC_GATHER && r.opt_bres_kernel == 1) {
+    brec = get_bres_records(pbecell, pbedge);
+    if (!brec) return -1;
+  } else if (r.opt_inc_mode == OP2B_INC_GATHER) {
     inv = get_inverse_map(pbecell);
     if (!inv) return -1;
   } else if (r.opt_inc_mode == OP2B_INC_COLOR) {
@@ -328,9 +344,10 @@ int loop_bres_calc(const char *name, op_set set, int nargs, op_arg *a) {
                            (const double *)a[0].dat->data_d, (const double *)a[2].dat->data_d,
                            (const double *)a[3].dat->data_d, (double *)a[4].dat->data_d, k};
     r.begin_loop(name);
-    e = inv ? launch_bres_calc_gather<double>(r.ctx(), *inv, p.pbedge, p.bound, p.x, p.q, p.adt,
-                                              p.res, k)
-            : run_bres_calc<double>(r.ctx(), p, plan, r.opt_inc_mode);
+    e = brec ? launch_bres_calc_records<double>(r.ctx(), *brec, p.bound, p.x, p.q, p.adt, p.res, k)
+        : inv ? launch_bres_calc_gather<double>(r.ctx(), *inv, p.pbedge, p.bound, p.x, p.q,
+                                                p.adt, p.res, k)
+              : run_bres_calc<double>(r.ctx(), p, plan, r.opt_inc_mode);
   } else {
     AirConst<float> k = air_consts<float>(ok);
     if (!ok) return -1;
@@ -338,9 +355,10 @@ int loop_bres_calc(const char *name, op_set set, int nargs, op_arg *a) {
                           (const float *)a[0].dat->data_d, (const float *)a[2].dat->data_d,
                           (const float *)a[3].dat->data_d, (float *)a[4].dat->data_d, k};
     r.begin_loop(name);
-    e = inv ? launch_bres_calc_gather<float>(r.ctx(), *inv, p.pbedge, p.bound, p.x, p.q, p.adt,
-                                             p.res, k)
-            : run_bres_calc<float>(r.ctx(), p, plan, r.opt_inc_mode);
+    e = brec ? launch_bres_calc_records<float>(r.ctx(), *brec, p.bound, p.x, p.q, p.adt, p.res, k)
+        : inv ? launch_bres_calc_gather<float>(r.ctx(), *inv, p.pbedge, p.bound, p.x, p.q,
+                                               p.adt, p.res, k)
+              : run_bres_calc<float>(r.ctx(), p, plan, r.opt_inc_mode);
   }
   r.end_loop(bytes);
   return finish(e, name);

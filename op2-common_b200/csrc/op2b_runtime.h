@@ -44,9 +44,11 @@ struct Runtime {
   int opt_cache_line = 128;
   int opt_maps_base = 0;
   int opt_inc_mode = OP2B_INC_GATHER;
-  int opt_gather_kernel = 5;  // OP2B_GATHER_REGPIPE (gather.h)
+  int opt_gather_kernel = 6;  // OP2B_GATHER_CORNER (gather.h)
   int opt_gather_minb = 0;    // __launch_bounds__ minimum blocks of the gather kernels
-  int opt_pipe_block = 128;   // threads per CTA of the pipelined gather (64, 96, 128, 256)
+  int opt_bres_kernel = 1;    // bres_calc gather: 0 = inverse-map walk, 1 = boundary records
+  int opt_adt_minb = 0;       // __launch_bounds__ minimum blocks of adt_calc (0 = 1)
+  int opt_pipe_block = 256;   // threads per CTA of the pipelined gather (64, 96, 128, 256)
   int opt_pipe_hints = 0;     // register pipeline: evict-first hints on once-read streams
   int opt_plan_mode = 0;      // 0 = parallel block colouring, 1 = serial greedy (bit-exact)
   bool opt_check_plans = false;
@@ -63,6 +65,7 @@ struct Runtime {
   void *pinned = nullptr;      // 4 KiB mapped pinned host page for reduction read-back
   void *pinned_dev = nullptr;  // its device address
   long long red_seq = 0;       // sequence number of the last update launch
+  unsigned long long *check_d = nullptr;  // device word for op_decl_map's range check
 
   // timing
   std::map<std::string, LoopStat> stats;

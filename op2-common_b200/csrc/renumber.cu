@@ -28,6 +28,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <climits>
 #include <cstdio>
 #include <cstring>
@@ -161,32 +162,36 @@ struct RcmWork {
   int *mark;             // BFS stamp of the pseudo-peripheral search
   int *lev_a, *lev_b;    // current and next level
   int *pkey;             // first-parent position of a discovered vertex (INT_MAX = none)
-  unsigned long long *keys;  // sort buffer (n entries, for levels that do not fit in smem)
   int *status;           // [0] = vertices ordered, [1] = error
 };
 
 constexpr int kRcmThreads = 1024;
-constexpr int kRcmSmemKeys = 4096;
 
-__device__ void rcm_sort(unsigned long long *k, int len) {
-  int pad = 1;
-  while (pad < len) pad <<= 1;
-  for (int i = len + threadIdx.x; i < pad; i += blockDim.x) k[i] = ~0ull;
+// Exclusive block-wide scan of v (blockDim.x a multiple of 32, <= 1024);
+// *total receives the sum over the block.
+__device__ int rcm_block_scan(int v, int *total) {
+  __shared__ int s_warp[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_warp[wid] = x;
   __syncthreads();
-  for (int kk = 2; kk <= pad; kk <<= 1)
-    for (int j = kk >> 1; j > 0; j >>= 1) {
-      for (int i = threadIdx.x; i < pad; i += blockDim.x) {
-        int ixj = i ^ j;
-        if (ixj > i) {
-          unsigned long long x = k[i], y = k[ixj];
-          if ((x > y) == ((i & kk) == 0)) {
-            k[i] = y;
-            k[ixj] = x;
-          }
-        }
-      }
-      __syncthreads();
+  if (wid == 0) {
+    int t = lane < nw ? s_warp[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
     }
+    if (lane < nw) s_warp[lane] = t;
+  }
+  __syncthreads();
+  const int before = (wid > 0 ? s_warp[wid - 1] : 0) + x - v;
+  *total = s_warp[nw - 1];
+  __syncthreads();  // s_warp is reused by the next call
+  return before;
 }
 
 // BFS from `start` over vertices not yet ordered; marks with `stamp`.
@@ -231,8 +236,7 @@ __device__ int rcm_bfs(RcmWork &w, int start, int stamp, int **last, int *last_l
 }
 
 __global__ void __launch_bounds__(kRcmThreads) k_rcm(RcmWork w) {
-  __shared__ unsigned long long s_keys[kRcmSmemKeys];
-  __shared__ int s_start, s_len, s_next, s_best, s_bestdeg;
+  __shared__ int s_start, s_len, s_best, s_bestdeg;
   __shared__ int s_pos;
   int stamp = 1;
   if (threadIdx.x == 0) s_pos = 0;
@@ -278,9 +282,8 @@ __global__ void __launch_bounds__(kRcmThreads) k_rcm(RcmWork w) {
     }
     __syncthreads();
     while (true) {
-      int len = s_len;
-      if (threadIdx.x == 0) s_next = 0;
-      __syncthreads();
+      const int len = s_len;
+      const int base = s_pos;
       // first parent (lowest position in this level) of every new vertex
       for (int j = threadIdx.x; j < len; j += blockDim.x) {
         int u = cur[j];
@@ -291,31 +294,53 @@ __global__ void __launch_bounds__(kRcmThreads) k_rcm(RcmWork w) {
         }
       }
       __syncthreads();
-      for (int j = threadIdx.x; j < len; j += blockDim.x) {
+      // The next level is the parents' claimed vertices, parent by parent in
+      // level order and, within a parent, by (degree capped at 63, id): the
+      // order sequential Cuthill-McKee appends them in.  Each thread takes a
+      // contiguous run of parents; a block scan of the runs' counts places
+      // them, so no sort of the level is needed.
+      const int chunk = (len + (int)blockDim.x - 1) / (int)blockDim.x;
+      const int jb = min(len, (int)threadIdx.x * chunk), je = min(len, jb + chunk);
+      int mine = 0;
+      for (int j = jb; j < je; j++) {
         int u = cur[j];
         long long r = w.row[u];
         for (int t = 0; t < w.deg[u]; t++) {
           int v = w.col[r + t];
-          if (w.newidx[v] < 0 && w.pkey[v] == j) nxt[atomicAdd(&s_next, 1)] = v;
+          if (w.newidx[v] < 0 && w.pkey[v] == j) mine++;
         }
       }
-      __syncthreads();
-      int nl = s_next;
+      int nl = 0;
+      int pos = rcm_block_scan(mine, &nl);
       if (nl == 0) break;
-      unsigned long long *keys = nl <= kRcmSmemKeys ? s_keys : w.keys;
-      for (int k = threadIdx.x; k < nl; k += blockDim.x) {
-        int v = nxt[k];
-        unsigned long long d = (unsigned)min(w.deg[v], 63);
-        keys[k] = ((unsigned long long)(unsigned)w.pkey[v] << 38) | (d << 32) | (unsigned)v;
-      }
-      __syncthreads();
-      rcm_sort(keys, nl);
-      int base = s_pos;
-      for (int k = threadIdx.x; k < nl; k += blockDim.x) {
-        int v = (int)(keys[k] & 0xffffffffull);
-        nxt[k] = v;
-        w.newidx[v] = base + k;
-        w.pkey[v] = INT_MAX;
+      for (int j = jb; j < je; j++) {
+        int u = cur[j];
+        long long r = w.row[u];
+        const int d = w.deg[u];
+        const int first = pos;
+        // selection: the smallest claimed key above the last one emitted
+        unsigned long long last = 0;
+        bool any = false;
+        while (true) {
+          unsigned long long best = ~0ull;
+          for (int t = 0; t < d; t++) {
+            int v = w.col[r + t];
+            if (w.newidx[v] < 0 && w.pkey[v] == j) {
+              unsigned long long key =
+                  ((unsigned long long)(unsigned)min(w.deg[v], 63) << 32) | (unsigned)v;
+              if ((!any || key > last) && key < best) best = key;
+            }
+          }
+          if (best == ~0ull) break;
+          nxt[pos++] = (int)(best & 0xffffffffull);
+          last = best;
+          any = true;
+        }
+        for (int k = first; k < pos; k++) {
+          int v = nxt[k];
+          w.newidx[v] = base + k;
+          w.pkey[v] = INT_MAX;
+        }
       }
       __syncthreads();
       if (threadIdx.x == 0) {
@@ -434,6 +459,32 @@ static Renumbering &ren() {
 
 static inline unsigned grid1(long long n, int t = 256) { return (unsigned)((n + t - 1) / t); }
 
+// bandwidth statistics of a map (op_renumber's diagnostics): per element the
+// largest difference between two of its targets; out[0] = max, out[1] = sum
+__global__ void k_map_bandwidth(int n, int dim, const int *__restrict__ map,
+                                unsigned long long *out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  long long dist = 0;
+  if (i < n) {
+    const int *row = map + (size_t)i * dim;
+    int lo = row[0], hi = row[0];
+    for (int a = 1; a < dim; a++) {
+      lo = min(lo, row[a]);
+      hi = max(hi, row[a]);
+    }
+    dist = (long long)hi - lo;
+  }
+  unsigned long long mx = (unsigned long long)dist, sum = (unsigned long long)dist;
+  for (int o = 16; o > 0; o >>= 1) {
+    mx = max(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    sum += __shfl_down_sync(0xffffffffu, sum, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(out, mx);
+    atomicAdd(out + 1, sum);
+  }
+}
+
 // RCM order of the base map's target set; perm[v] = new index of v
 static bool base_rcm(op_map base, int *perm_d, cudaStream_t s) {
   op_set to = base->to;
@@ -484,9 +535,8 @@ static bool base_rcm(op_map base, int *perm_d, cudaStream_t s) {
   w.lev_a = (int *)A(sizeof(int) * n);
   w.lev_b = (int *)A(sizeof(int) * n);
   w.pkey = (int *)A(sizeof(int) * n);
-  w.keys = (unsigned long long *)A(sizeof(unsigned long long) * 2 * (size_t)std::max(n, 1));
   w.status = (int *)A(sizeof(int) * 2);
-  if (!w.newidx || !w.mark || !w.lev_a || !w.lev_b || !w.pkey || !w.keys || !w.status)
+  if (!w.newidx || !w.mark || !w.lev_a || !w.lev_b || !w.pkey || !w.status)
     return cleanup(), false;
   cudaMemsetAsync(w.newidx, 0xff, sizeof(int) * n, s);
   cudaMemsetAsync(w.mark, 0, sizeof(int) * n, s);
@@ -591,19 +641,24 @@ static void propagate(op_set from, op_set to, std::vector<int *> &perm, cudaStre
   }
 }
 
-static void bandwidth(op_map base, long &mx, long &avg) {
+// maximum and average over elements of the largest distance between two
+// targets of one element (the figures op_renumber prints, :489-503), on the
+// device from the map's device copy
+static bool bandwidth(op_map base, long &mx, long &avg, cudaStream_t s) {
   mx = 0;
   avg = 0;
-  int n = base->from->size, d = base->dim;
-  for (int i = 0; i < n; i++) {
-    long dist = 0;
-    for (int a = 0; a < d; a++)
-      for (int b = 0; b < d; b++)
-        dist = std::max(dist, (long)std::abs(base->map[(size_t)i * d + a] - base->map[(size_t)i * d + b]));
-    mx = std::max(mx, dist);
-    avg += dist;
-  }
-  if (n) avg /= n;
+  const int n = base->from->size;
+  if (n == 0) return true;
+  Runtime &r = rt();
+  unsigned long long *out = r.check_d + 1;  // two words of the runtime's check scratch
+  unsigned long long h[2] = {0, 0};
+  cudaMemsetAsync(out, 0, 2 * sizeof(unsigned long long), s);
+  k_map_bandwidth<<<grid1(n), 256, 0, s>>>(n, base->dim, base->map_d, out);
+  cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return false;
+  mx = (long)h[0];
+  avg = (long)(h[1] / (unsigned long long)n);
+  return true;
 }
 
 int renumber(op_map base, long stats[4]) {
@@ -615,8 +670,19 @@ int renumber(op_map base, long stats[4]) {
   }
   cudaStream_t s = r.stream;
   cudaStreamSynchronize(s);
+  const auto t_begin = std::chrono::steady_clock::now();
+  auto t_last = t_begin;
+  auto lap = [&](const char *what) {  // phase times with diags > 2
+    if (r.opt_diags <= 2) return;
+    cudaStreamSynchronize(s);
+    const auto now = std::chrono::steady_clock::now();
+    fprintf(stderr, "op_renumber: %-22s %8.2f ms\n", what,
+            std::chrono::duration<double, std::milli>(now - t_last).count());
+    t_last = now;
+  };
   long bmx, bavg;
-  bandwidth(base, bmx, bavg);
+  bandwidth(base, bmx, bavg, s);
+  lap("bandwidth before");
   std::vector<int *> perm(r.sets.size(), nullptr);
   op_set to = base->to;
   int *pb = nullptr;
@@ -629,8 +695,10 @@ int renumber(op_map base, long stats[4]) {
     cudaFree(pb);
     return -1;
   }
+  lap("reverse Cuthill-McKee");
   bool ok = true;
   propagate(to, to, perm, s, ok);
+  lap("propagation");
   if (!ok) {
     set_error("op_renumber: propagation failed");
     for (int *p : perm) cudaFree(p);
@@ -681,6 +749,7 @@ int renumber(op_map base, long stats[4]) {
       cudaFree(t);
     }
   }
+  lap("reordering");
   // host copies of the maps follow the device
   for (auto &mp : r.maps) {
     op_map m = mp.get();
@@ -704,11 +773,13 @@ int renumber(op_map base, long stats[4]) {
       cudaFree(perm[set->index]);
     }
   }
+  lap("host maps, composition");
   release_plans();  // plans and inverse maps refer to the old numbering
   release_inverse_maps();
   bool good = cuda_ok(cudaStreamSynchronize(s), "op_renumber") && ok;
   long amx, aavg;
-  bandwidth(base, amx, aavg);
+  bandwidth(base, amx, aavg, s);
+  lap("release, bandwidth after");
   if (stats) {
     stats[0] = bmx;
     stats[1] = bavg;

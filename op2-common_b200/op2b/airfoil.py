@@ -41,13 +41,20 @@ class Airfoil:
         self.pbecell = L.op_decl_map(self.bedges, self.cells, 1, mesh.becell, "pbecell")
         self.pcell = L.op_decl_map(self.cells, self.nodes, 4, mesh.cell, "pcell")
         qinf = np.asarray(self.c["qinf"], np.float64)
-        q = np.tile(qinf, (ncell, 1)) if q0 is None else np.asarray(q0, np.float64)
+        if q0 is None:
+            q = np.empty((ncell, 4), self.dtype)
+            q[:] = qinf.astype(self.dtype)
+        else:
+            q = np.ascontiguousarray(q0, dtype=self.dtype)
         self.p_bound = L.op_decl_dat(self.bedges, 1, "int", mesh.bound, "p_bound")
-        self.p_x = L.op_decl_dat(self.nodes, 2, t, mesh.x.astype(self.dtype), "p_x")
-        self.p_q = L.op_decl_dat(self.cells, 4, t, q.astype(self.dtype), "p_q")
-        self.p_qold = L.op_decl_dat(self.cells, 4, t, np.zeros((ncell, 4), self.dtype), "p_qold")
-        self.p_adt = L.op_decl_dat(self.cells, 1, t, np.zeros(ncell, self.dtype), "p_adt")
-        self.p_res = L.op_decl_dat(self.cells, 4, t, np.zeros((ncell, 4), self.dtype), "p_res")
+        self.p_x = L.op_decl_dat(self.nodes, 2, t, np.ascontiguousarray(mesh.x, dtype=self.dtype),
+                                 "p_x")
+        self.p_q = L.op_decl_dat(self.cells, 4, t, q, "p_q")
+        # qold, adt and res start at zero, as airfoil.cpp's arrays do: declared
+        # without data they are zeroed on the device instead of uploaded
+        self.p_qold = L.op_decl_dat(self.cells, 4, t, None, "p_qold")
+        self.p_adt = L.op_decl_dat(self.cells, 1, t, None, "p_adt")
+        self.p_res = L.op_decl_dat(self.cells, 4, t, None, "p_res")
         for name in ("gam", "gm1", "cfl", "eps", "mach", "alpha"):
             L.op_decl_const(1, "double", self.c[name], name)
         L.op_decl_const(4, "double", qinf, "qinf")

@@ -311,12 +311,14 @@ def op_decl_map(frm, to, dim: int, data, name: str):
 
 
 def op_decl_dat(set_, dim: int, type_: str | None, data, name: str):
-    """op_decl_dat<T> (op_lib_cpp.h:127-137): the numpy dtype must match `type_`."""
+    """op_decl_dat<T> (op_lib_cpp.h:127-137): the numpy dtype must match `type_`.
+    data=None declares a zero-initialised dat (the reference callocs when it is
+    given no data, op2/src/core/op_lib_core.cpp:520-537); nothing is uploaded."""
     if data is None:
         if type_ is None:
             raise Op2Error("op_decl_dat: needs data or a type")
         tb = {"double": 8, "float": 4, "int": 4}[type_.split(":")[0]]
-        d = load().op_decl_dat_temp_char(set_, int(dim), _b(type_), tb, _b(name))
+        d = load().op_decl_dat_char(set_, int(dim), _b(type_), tb, None, _b(name))
     else:
         a = np.ascontiguousarray(data)
         t = _TYPES.get(a.dtype)

@@ -127,22 +127,29 @@ def test_colouring_is_deterministic_and_matches_atomics(op2, part):
         assert np.max(np.abs(runs[mode][0] / c1 - 1)) < 1e-12
 
 
-GATHER_KERNELS = [(1, 0), (2, 0), (3, 0), (4, 64), (4, 96), (4, 128), (4, 256), (5, 64), (5, 96),
-                  (5, 128), (5, 256)]
+# (gather_kernel, pipe_block, gather_minblocks, bres_kernel)
+GATHER_KERNELS = [(1, 0, 0, 0), (2, 0, 0, 1), (3, 0, 0, 1), (4, 64, 0, 1), (4, 96, 0, 1),
+                  (4, 128, 0, 1), (4, 256, 0, 1), (5, 64, 0, 1), (5, 96, 0, 1), (5, 128, 0, 0),
+                  (5, 256, 0, 1), (6, 64, 5, 1), (6, 64, 6, 1), (6, 128, 0, 1), (6, 128, 3, 0),
+                  (6, 256, 0, 1)]
 
 
-@pytest.mark.parametrize("kernel", GATHER_KERNELS, ids=lambda k: f"g{k[0]}b{k[1]}")
+@pytest.mark.parametrize("kernel", GATHER_KERNELS,
+                         ids=lambda k: f"g{k[0]}b{k[1]}m{k[2]}r{k[3]}")
 @pytest.mark.parametrize("fixture", ["airfoil_24x12_s3.npz", "airfoil_240x120_s1.npz"])
 def test_gather_mode_is_bit_exact_with_reference(op2, fixture, kernel):
     """inc_mode 3 adds each cell's increments in element order starting from
     res, as the reference's sequential loop does: q after 100 iterations is
     bit-identical to the reference's own build (rms differs only by the order
     of its global sum) -- for every gather kernel (CSR walk, 4 lanes, unrolled
-    slot records, shared-memory pipeline at each block size)."""
+    slot records, shared-memory and register pipelines at each block size,
+    the register pipeline over corner records) and both bres_calc gathers."""
     op2.set_option("inc_mode", L.OP2B_INC_GATHER)
     op2.set_option("gather_kernel", kernel[0])
     if kernel[1]:
         op2.set_option("pipe_block", kernel[1])
+    op2.set_option("gather_minblocks", kernel[2])
+    op2.set_option("bres_kernel", kernel[3])
     gd = np.load(f"{GOLDEN}/{fixture}")
     m = M.channel_bump(int(gd["I"]), int(gd["J"]), seed=int(gd["seed"]))
     app = Airfoil(m)
@@ -166,14 +173,47 @@ def test_pipelined_kernels_are_bit_identical(op2, hints):
     one-pass slot-record kernel."""
     m = M.channel_bump(240, 120, seed=6)
     out = []
-    for gk in (3, 5):
+    for gk in (3, 5, 6):
         op2.set_option("gather_kernel", gk)
         op2.set_option("pipe_hints", hints)
         app = Airfoil(m)
         app.iterate(5)
         out.append(app.fetch())
+    for o in out[1:]:
+        for k in ("q", "adt", "res"):
+            assert np.array_equal(out[0][k], o[k]), k
+
+
+def test_corner_kernel_falls_back_when_edges_are_not_cell_corners(op2):
+    """Corner records need a cell's edges to touch at most four nodes; with
+    the edges' node pairs shuffled they touch up to eight, and gather_kernel 6
+    must serve the loop through the slot-record pipeline, bit-identically."""
+    m = M.channel_bump(48, 24, seed=9)
+    rng = np.random.default_rng(3)
+    m.edge = np.ascontiguousarray(m.edge[rng.permutation(m.nedge)])
+    out = []
+    for gk in (3, 6):
+        op2.set_option("gather_kernel", gk)
+        app = Airfoil(m)
+        app.iterate(3)
+        out.append(app.fetch())
     for k in ("q", "adt", "res"):
         assert np.array_equal(out[0][k], out[1][k]), k
+
+
+def test_options_return_to_defaults_at_exit(op2):
+    defaults = {k: op2.get_option(k) for k in ("inc_mode", "gather_kernel", "bres_kernel",
+                                                "adt_minblocks", "pipe_block")}
+    op2.set_option("inc_mode", L.OP2B_INC_ATOMIC)
+    op2.set_option("gather_kernel", 3)
+    op2.set_option("bres_kernel", 0)
+    op2.set_option("adt_minblocks", 6)
+    op2.set_option("pipe_block", 256)
+    op2.op_exit()
+    op2.op_init()
+    assert {k: op2.get_option(k) for k in defaults} == defaults
+    with pytest.raises(L.Op2Error):
+        op2.set_option("gather_kernel", 7)
 
 
 def test_large_mesh_one_iteration_against_oracle(op2):
@@ -193,7 +233,7 @@ def test_large_mesh_one_iteration_against_oracle(op2):
     assert np.all(np.abs(r.sum(axis=0)) <= 1e-9 * np.abs(r).sum(axis=0))
 
 
-@pytest.mark.parametrize("kernel", [3, 4, 5])
+@pytest.mark.parametrize("kernel", [3, 4, 5, 6])
 def test_mixed_precision_against_fp32_restatement(op2, kernel):
     op2.set_option("gather_kernel", kernel)
     m = M.channel_bump(120, 60, seed=4)
