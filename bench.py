@@ -15,14 +15,20 @@ max over ranks.  Prints one JSON line on rank 0.
              synchronize on both sides).  The working set (~0.7 GB) is larger
              than the 126 MB L2, so no flush is needed between iterations.
              Default configuration: the mesh renumbered on the GPU
-             (op_renumber, reverse Cuthill-McKee) and the owner-computes
-             (gather) increment strategy.
-* e2e        the whole job through the public API with host buffers, per
-             iteration: op_decl_* uploads from pinned host memory, op_renumber,
-             K iterations, op_fetch_data of q.
+             (op_renumber, reverse Cuthill-McKee), owner-computes increments
+             over corner records, and the runtime's loop fusion (save_soln
+             into adt_calc, res_calc with bres_calc).
+* loops      per loop (or fused loop pair) device time, algorithmic bytes per
+             call and GB/s.
+* e2e        the whole 1000-iteration job (the configuration's length) through
+             the public API from host buffers, per iteration: op_decl_*
+             uploads from pinned mesh arrays, op_renumber, the iterations,
+             op_fetch_data of q.
 * roofline   the dominant loop's algorithmic bytes per call / its mean
-             CUDA-event duration, against MEASURED_PEAKS.json hbm_gbs.
-* variants   the same timing for random/RCM numbering x atomics/colouring/hybrid.
+             CUDA-event duration, against MEASURED_PEAKS.json hbm_gbs; traffic
+             = ncu DRAM bytes per launch (profiles/traffic.json).
+* variants   the same timing for random/RCM numbering x increment strategies,
+             gather kernels, and fusion off (per-loop figures).
 * cpu_baseline  the reference's own OpenMP build (oracle/_ref, compiled from the
              reference sources) on a bounded sample of the same mesh.
 * --impl reference   times that reference build alone (rank 0; others exit).
@@ -45,7 +51,8 @@ sys.path.insert(0, os.path.join(REPO, "op2-common_b200"))
 sys.path.insert(0, REPO)
 
 FALLBACK_HBM_GBS = 6650.0
-LOOPS = ("save_soln", "adt_calc", "res_calc", "bres_calc", "update")
+LOOPS = ("save_soln", "adt_calc", "res_calc", "bres_calc", "update",
+         "save_soln+adt_calc", "res_calc+bres_calc")  # the pairs the runtime fuses
 METRIC = "Airfoil ms/iter (2400x1200 FP64)"
 
 
@@ -308,15 +315,16 @@ def main():
         for o in ({"gather_kernel": 1}, {"gather_kernel": 3}, {"gather_kernel": 4},
                   {"gather_kernel": 5, "pipe_block": 128}, {"gather_kernel": 5, "pipe_block": 256},
                   {"gather_kernel": 6, "pipe_block": 128}, {"gather_kernel": 6, "pipe_block": 256},
-                  {"gather_kernel": 6, "pipe_block": 256, "bres_kernel": 0}):
+                  {"gather_kernel": 6, "pipe_block": 256, "bres_kernel": 0},
+                  {"fuse": 0}):
             v = timed_run(L, Airfoil, m, dtype, "rcm", 3, args.part_size, 20, 3, torch, barrier,
                           opts=o)
             lp = v["loops"]
             variants.append({"numbering": "rcm", "inc_mode": 3, **o,
                              "ms_per_iter": max_over_ranks(v["ms"]),
-                             "res_calc_gbs": lp.get("res_calc", {}).get("gbs"),
-                             "res_calc_us": 1e3 * lp.get("res_calc", {}).get("avg_ms", 0),
-                             "adt_calc_gbs": lp.get("adt_calc", {}).get("gbs")})
+                             "loops": {n: {"us": round(1e3 * x["avg_ms"], 2),
+                                           "gbs": round(x["gbs"])}
+                                       for n, x in lp.items()}})
 
     # ---------------------------------------------------------- end to end through the API
     e2e = None

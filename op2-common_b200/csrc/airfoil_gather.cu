@@ -26,6 +26,7 @@
 #include "airfoil_math.cuh"
 #include "gather.h"
 #include "op2b_runtime.h"
+#include "scan.h"
 #include "vec.cuh"
 
 namespace op2b {
@@ -64,33 +65,6 @@ __global__ void k_inv_sort(int nto, const long long *off, int *ent) {
   }
 }
 
-__global__ void k_scan_serial_ll(const int *cnt, long long *off, int n) {
-  // small-to-medium scans: one CTA, chunked (n up to a few million)
-  __shared__ long long part[1024];
-  int T = blockDim.x;
-  long long chunk = (n + T - 1) / T;
-  long long b = threadIdx.x * chunk, e = min((long long)n, b + chunk);
-  long long s = 0;
-  for (long long i = b; i < e; i++) s += cnt[i];
-  part[threadIdx.x] = s;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    long long acc = 0;
-    for (int k = 0; k < T; k++) {
-      long long t = part[k];
-      part[k] = acc;
-      acc += t;
-    }
-    off[n] = acc;
-  }
-  __syncthreads();
-  long long acc = part[threadIdx.x];
-  for (long long i = b; i < e; i++) {
-    off[i] = acc;
-    acc += cnt[i];
-  }
-}
-
 struct InvMapCache {
   op_map map = nullptr;
   InvMap inv;
@@ -120,7 +94,7 @@ const InvMap *get_inverse_map(op_map map) {
   int n = map->from->size, nto = map->to->size, dim = map->dim;
   auto A = [&](size_t bytes) -> void * {
     void *p = nullptr;
-    if (cudaMalloc(&p, bytes ? bytes : 1) != cudaSuccess) return nullptr;
+    if (cudaMallocAsync(&p, bytes ? bytes : 1, s) != cudaSuccess) return nullptr;
     c->owned.push_back(p);
     return p;
   };
@@ -140,22 +114,23 @@ const InvMap *get_inverse_map(op_map map) {
   cudaMemsetAsync(fill, 0, sizeof(int) * ((size_t)nto + 1), s);
   unsigned g = (unsigned)((n + 255) / 256);
   if (n > 0) k_inv_count<<<g, 256, 0, s>>>(n, dim, map->map_d, cnt);
-  k_scan_serial_ll<<<1, 1024, 0, s>>>(cnt, off, nto);
+  if (!scan_exclusive(cnt, off, nto, s)) {
+    set_error("inverse map of %s: scan failed", map->name);
+    return nullptr;
+  }
   if (n > 0) k_inv_fill<<<g, 256, 0, s>>>(n, dim, map->map_d, off, fill, ent);
   if (nto > 0) k_inv_sort<<<(unsigned)((nto + 255) / 256), 256, 0, s>>>(nto, off, ent);
-  r.launches += 4;
-  if (!cuda_ok(cudaStreamSynchronize(s), "inverse map")) return nullptr;
-  // compact list of targets that have entries (rows)
-  std::vector<long long> h_off((size_t)nto + 1);
-  cudaMemcpy(h_off.data(), off, sizeof(long long) * h_off.size(), cudaMemcpyDeviceToHost);
-  std::vector<int> rows;
-  rows.reserve(nto);
-  for (int t = 0; t < nto; t++)
-    if (h_off[t + 1] > h_off[t]) rows.push_back(t);
-  int *rows_d = (int *)A(sizeof(int) * (rows.size() + 1));
-  if (!rows.empty())
-    cudaMemcpy(rows_d, rows.data(), sizeof(int) * rows.size(), cudaMemcpyHostToDevice);
-  c->inv = InvMap{off, ent, rows_d, (int)rows.size(), nto, dim, rows.size() == (size_t)nto};
+  r.launches += 6;
+  // the targets that have entries (rows), compacted on the device
+  int *rows_d = (int *)A(sizeof(int) * ((size_t)nto + 1));
+  long long *pos = (long long *)A(sizeof(long long) * ((size_t)nto + 1));
+  int nrows = 0;
+  if (!rows_d || !pos || !compact_nonzero(cnt, nto, rows_d, pos, &nrows, s)) {
+    set_error("inverse map of %s: row compaction failed", map->name);
+    return nullptr;
+  }
+  r.launches += 5;
+  c->inv = InvMap{off, ent, rows_d, nrows, nto, dim, nrows == nto};
   inv_cache().push_back(std::move(c));
   return &inv_cache().back()->inv;
 }
@@ -398,6 +373,8 @@ struct SlotCache {
   op_map inc = nullptr, nodes = nullptr;
   SlotRecords rec{};
   bool corners_tried = false;
+  op_map linked = nullptr;  // pbecell whose boundary records are linked in (fused bres_calc)
+  int link_state = 0;       // 0 not tried, 1 linked, -1 not linkable
   std::vector<void *> owned;
   ~SlotCache() {
     for (void *p : owned) cudaFree(p);
@@ -421,14 +398,14 @@ const SlotRecords *get_slot_records(op_map pecell, op_map pedge) {
   sc->nodes = pedge;
   int n = pecell->to->size;
   int *mx = nullptr;
-  cudaMalloc(&mx, sizeof(int));
+  cudaMallocAsync(&mx, sizeof(int), s);
   cudaMemsetAsync(mx, 0, sizeof(int), s);
   unsigned g = (unsigned)((n + 255) / 256);
   if (n > 0) k_max_degree<<<g, 256, 0, s>>>(n, inv->off, mx);
   int h_mx = 0;
   cudaMemcpyAsync(&h_mx, mx, sizeof(int), cudaMemcpyDeviceToHost, s);
+  cudaFreeAsync(mx, s);
   bool ok = cuda_ok(cudaStreamSynchronize(s), "slot records");
-  cudaFree(mx);
   if (!ok) return nullptr;
   sc->rec.ncell = n;
   sc->rec.usable = h_mx <= 4 && (long long)n * 4 < (1LL << 31) && pedge->to->size < (int)kRoleBit;
@@ -436,8 +413,9 @@ const SlotRecords *get_slot_records(op_map pecell, op_map pedge) {
     size_t cnt = (size_t)n * 4;
     int *o = nullptr, *n1 = nullptr;
     unsigned *n2 = nullptr;
-    if (cudaMalloc(&o, cnt * 4) != cudaSuccess || cudaMalloc(&n1, cnt * 4) != cudaSuccess ||
-        cudaMalloc(&n2, cnt * 4) != cudaSuccess) {
+    if (cudaMallocAsync(&o, cnt * 4, s) != cudaSuccess ||
+        cudaMallocAsync(&n1, cnt * 4, s) != cudaSuccess ||
+        cudaMallocAsync(&n2, cnt * 4, s) != cudaSuccess) {
       cudaFree(o);
       cudaFree(n1);
       set_error("slot records: out of device memory");
@@ -512,9 +490,9 @@ const SlotRecords *get_corner_records(op_map pecell, op_map pedge) {
   int4 *cn = nullptr;
   unsigned *meta = nullptr;
   int *bad = nullptr;
-  if (cudaMalloc(&cn, sizeof(int4) * (size_t)n) != cudaSuccess ||
-      cudaMalloc(&meta, sizeof(unsigned) * (size_t)n) != cudaSuccess ||
-      cudaMalloc(&bad, sizeof(int)) != cudaSuccess) {
+  if (cudaMallocAsync(&cn, sizeof(int4) * (size_t)n, s) != cudaSuccess ||
+      cudaMallocAsync(&meta, sizeof(unsigned) * (size_t)n, s) != cudaSuccess ||
+      cudaMallocAsync(&bad, sizeof(int), s) != cudaSuccess) {
     cudaFree(cn);
     cudaFree(meta);
     set_error("corner records: out of device memory");
@@ -527,8 +505,8 @@ const SlotRecords *get_corner_records(op_map pecell, op_map pedge) {
   r.launches += 1;
   int h_bad = 1;
   cudaMemcpyAsync(&h_bad, bad, sizeof(int), cudaMemcpyDeviceToHost, s);
+  cudaFreeAsync(bad, s);
   bool ok = cuda_ok(cudaStreamSynchronize(s), "corner records");
-  cudaFree(bad);
   if (!ok) {
     cudaFree(cn);
     cudaFree(meta);
@@ -545,6 +523,99 @@ const SlotRecords *get_corner_records(op_map pecell, op_map pedge) {
   sc->rec.meta = meta;
   sc->rec.corners = true;
   return base;
+}
+
+// ------------------------------------------------------------------ fused res_calc + bres_calc
+
+// Place every boundary edge of a cell into the cell's corner record, after
+// its interior slots and in edge order: the slot's o becomes the boundary
+// edge, its meta byte 0x40 | corner of node 1 << 2 | corner of node 2 << 4.
+// A node that is not yet a corner takes a free corner entry (a corner cell's
+// outer node lies on its boundary edges only).  One thread per cell, on its
+// first record.  With write == false only *bad is set (an edge without a free
+// slot, or more than four nodes).
+__global__ void k_link(int n, const int4 *__restrict__ rec, int4 *cn, int *o, unsigned *meta,
+                       int *bad, bool write) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int4 r0 = rec[i];
+  if (r0.x < 0) return;  // a continuation: handled with the cell's first record
+  const int c = r0.x;
+  unsigned m = meta[c];
+  int nvalid = 0;
+  for (int s = 0; s < 4; s++) nvalid += (int)((m >> (8 * s)) & 1u);
+  const int4 k4 = cn[c];
+  int corners[4] = {k4.x, k4.y, k4.z, k4.w};
+  int cnt = 1;  // unused entries repeat the first corner
+  for (int j = 1; j < 4; j++) cnt += corners[j] != corners[0] ? 1 : 0;
+  int oo[4];
+  for (int s = 0; s < 4; s++) oo[s] = o[(size_t)c * 4 + s];
+  bool ok = true;
+  for (int j = i, ord = 0; j < n; j++, ord++) {
+    const int4 r = rec[j];
+    if (j > i && r.x >= 0) break;  // the next cell's first record
+    int ab[2];
+    const int nodes[2] = {r.y, r.z};
+    for (int e = 0; e < 2; e++) {
+      int f = -1;
+      for (int q = 0; q < cnt; q++)
+        if (corners[q] == nodes[e]) f = q;
+      if (f < 0 && cnt < 4) {
+        f = cnt;
+        corners[cnt++] = nodes[e];
+      }
+      ab[e] = f;
+    }
+    const int s = nvalid + ord;
+    if (s >= 4 || ab[0] < 0 || ab[1] < 0) {
+      ok = false;
+      break;
+    }
+    oo[s] = r.w;
+    m |= (0x40u | ((unsigned)ab[0] << 2) | ((unsigned)ab[1] << 4)) << (8 * s);
+  }
+  if (!ok) {
+    atomicOr(bad, 1);
+    return;
+  }
+  if (!write) return;
+  for (int j = cnt; j < 4; j++) corners[j] = corners[0];
+  cn[c] = make_int4(corners[0], corners[1], corners[2], corners[3]);
+  for (int s = 0; s < 4; s++) o[(size_t)c * 4 + s] = oo[s];
+  meta[c] = m;
+}
+
+bool link_boundary_records(const SlotRecords *rec, const BresRecords *b, op_map pbecell) {
+  SlotCache *sc = nullptr;
+  for (auto &p : slot_cache())
+    if (&p->rec == rec) sc = p.get();
+  if (!sc || !rec->corners) return false;
+  if (sc->link_state != 0) return sc->link_state == 1 && sc->linked == pbecell;
+  sc->link_state = -1;
+  if (pbecell->to != sc->inc->to) return false;  // boundary cells must be the same set
+  Runtime &r = rt();
+  cudaStream_t s = r.stream;
+  unsigned *meta = const_cast<unsigned *>(rec->meta);
+  int *o = const_cast<int *>(rec->o);
+  int4 *cn = reinterpret_cast<int4 *>(const_cast<int *>(rec->cn));
+  int *bad = reinterpret_cast<int *>(r.check_d + 3);  // a word of the runtime's check scratch
+  int h_bad = 1;
+  const unsigned g = (unsigned)((b->n + 255) / 256);
+  cudaMemsetAsync(bad, 0, sizeof(int), s);
+  if (b->n > 0) {
+    k_link<<<g, 256, 0, s>>>(b->n, b->rec, cn, o, meta, bad, false);
+    r.launches += 1;
+  }
+  cudaMemcpyAsync(&h_bad, bad, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (!cuda_ok(cudaStreamSynchronize(s), "boundary link") || h_bad) return false;
+  if (b->n > 0) {
+    k_link<<<g, 256, 0, s>>>(b->n, b->rec, cn, o, meta, bad, true);
+    r.launches += 1;
+  }
+  if (!cuda_ok(cudaStreamSynchronize(s), "boundary link")) return false;
+  sc->link_state = 1;
+  sc->linked = pbecell;
+  return true;
 }
 
 // ------------------------------------------------------------------ bres_calc records
@@ -588,7 +659,7 @@ const BresRecords *get_bres_records(op_map pbecell, op_map pbedge) {
   bc->nodes = pbedge;
   const int n = pbecell->from->size;
   if (n > 0) {
-    if (cudaMalloc(&bc->buf, sizeof(int4) * (size_t)n) != cudaSuccess) {
+    if (cudaMallocAsync(&bc->buf, sizeof(int4) * (size_t)n, r.stream) != cudaSuccess) {
       set_error("bres_calc records: out of device memory");
       return nullptr;
     }

@@ -139,4 +139,35 @@ __device__ __forceinline__ void air_bflux(T x1x, T x1y, T x2x, T x2y,
   }
 }
 
+// air_bflux with the cell's own terms ri = 1/q1[0] and p1 (air_prim) passed
+// in: the same operations in the same order, so the values are bit-identical.
+template <typename T>
+__device__ __forceinline__ void air_bflux_prim(T x1x, T x1y, T x2x, T x2y, const T *q1, T ri1,
+                                               T p1, T adt1, int bound, const AirConst<T> &k,
+                                               T *r) {
+  T dx, dy, mu, ri, p2, vol1, vol2;
+  dx = x1x - x2x;
+  dy = x1y - x2y;
+  if (bound == 1) {
+    r[0] = (T)0;
+    r[1] = +p1 * dy;
+    r[2] = -p1 * dx;
+    r[3] = (T)0;
+  } else {
+    const T *qi = k.qinf;
+    vol1 = ri1 * (q1[1] * dy - q1[2] * dx);
+    ri = (T)1.0f / qi[0];
+    p2 = k.gm1 * (qi[3] - (T)0.5f * ri * (qi[1] * qi[1] + qi[2] * qi[2]));
+    vol2 = ri * (qi[1] * dy - qi[2] * dx);
+    mu = adt1 * k.eps;
+    r[0] = (T)0.5f * (vol1 * q1[0] + vol2 * qi[0]) + mu * (q1[0] - qi[0]);
+    r[1] = (T)0.5f * (vol1 * q1[1] + p1 * dy + vol2 * qi[1] + p2 * dy) +
+           mu * (q1[1] - qi[1]);
+    r[2] = (T)0.5f * (vol1 * q1[2] - p1 * dx + vol2 * qi[2] - p2 * dx) +
+           mu * (q1[2] - qi[2]);
+    r[3] = (T)0.5f * (vol1 * (q1[3] + p1) + vol2 * (qi[3] + p2)) +
+           mu * (q1[3] - qi[3]);
+  }
+}
+
 } // namespace op2b

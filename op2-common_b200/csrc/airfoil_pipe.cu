@@ -366,14 +366,24 @@ __device__ __forceinline__ CornerRec load_crec(const int4 *ro, const int4 *rcn,
 template <typename T> struct CornerOps {
   T qc[4], rs[4], qo[4][4], ao[4], xn[4][2], ac;
   unsigned meta;
+  int bnd[4];  // fused bres_calc: boundary flag of each boundary slot
 };
 
-template <typename T>
+// The fused res_calc + bres_calc keeps a boundary cell's boundary edges in the
+// unused slots of its corner record (after its interior slots, in edge order):
+// meta bit 6 marks such a slot, bits 2-5 give the edge's nodes as corners and
+// o holds the boundary edge, whose flag is read from the bound dat.
+struct BresLink {
+  const int *bound;
+};
+
+template <typename T, bool BRES = false>
 __device__ __forceinline__ void load_corner_cell(CornerOps<T> &d, int c, const CornerRec &r,
                                                  const T *__restrict__ x,
                                                  const T *__restrict__ q,
                                                  const T *__restrict__ adt,
-                                                 const T *__restrict__ res) {
+                                                 const T *__restrict__ res,
+                                                 const BresLink &bl = BresLink{}) {
   Vec<T>::ld4(q + 4 * (size_t)c, d.qc);
   Vec<T>::ld4_rw(res + 4 * (size_t)c, d.rs);
   d.ac = __ldg(adt + c);
@@ -388,6 +398,13 @@ __device__ __forceinline__ void load_corner_cell(CornerOps<T> &d, int c, const C
     d.ao[s] = __ldg(adt + oo);
   }
   d.meta = r.meta;
+  if constexpr (BRES) {
+    if (r.meta & 0x40404040u) {  // a boundary cell: its boundary edges' flags
+#pragma unroll
+      for (int s = 0; s < 4; s++)
+        d.bnd[s] = ((r.meta >> (8 * s + 6)) & 1u) ? __ldg(bl.bound + o[s]) : 0;
+    }
+  }
 }
 
 // coordinate `comp` of corner i (0..3), by selects (no local-memory indexing)
@@ -398,7 +415,7 @@ __device__ __forceinline__ T corner(const T (&xn)[4][2], unsigned i, int comp) {
   return (i & 2u) ? hi : lo;
 }
 
-template <typename T>
+template <typename T, bool BRES = false>
 __device__ __forceinline__ void compute_corner(const CornerOps<T> &d, int c, T *__restrict__ res,
                                                const AirConst<T> &k) {
   T acc[4] = {d.rs[0], d.rs[1], d.rs[2], d.rs[3]};
@@ -423,6 +440,28 @@ __device__ __forceinline__ void compute_corner(const CornerOps<T> &d, int c, T *
       for (int j = 0; j < 4; j++) acc[j] += f[j];
     }
   }
+  if constexpr (BRES) {
+    // then bres_calc's increments: the boundary slots follow every interior
+    // slot, in boundary-edge order (the two loops' order)
+    if (d.meta & 0x40404040u) {
+#pragma unroll
+      for (int s = 0; s < 4; s++) {
+        const unsigned m = (d.meta >> (8 * s)) & 0xffu;
+        if (!(m & 0x40u)) continue;
+        const unsigned a = (m >> 2) & 3u, b = (m >> 4) & 3u;
+        T rr[4];
+        air_bflux_prim<T>(corner<T>(d.xn, a, 0), corner<T>(d.xn, a, 1), corner<T>(d.xn, b, 0),
+                          corner<T>(d.xn, b, 1), d.qc, ric, pc, d.ac, d.bnd[s], k, rr);
+        if (d.bnd[s] == 1) {  // a wall edge leaves components 0 and 3 untouched
+          acc[1] += rr[1];
+          acc[2] += rr[2];
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; j++) acc[j] += rr[j];
+        }
+      }
+    }
+  }
   Vec<T>::st4(res + 4 * (size_t)c, acc);
 }
 
@@ -445,6 +484,33 @@ k_res_gather_corner(int ncell, const int4 *__restrict__ rec_o, const int4 *__res
     const CornerRec r2 = load_crec(rec_o, rec_cn, rec_meta, c + 2 * G, ncell);
     if (c + G < ncell) load_corner_cell<T>(nxt, c + G, r1, x, q, adt, res);
     compute_corner<T>(cur, c, res, k);
+    cur = nxt;
+    r1 = r2;
+  }
+}
+
+// res_calc and the bres_calc that follows it in one launch (the runtime
+// defers res_calc until the next loop call; when that is bres_calc on the
+// same res, q, adt and x, this kernel runs instead of both)
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT, 1)
+k_res_bres_corner(int ncell, const int4 *__restrict__ rec_o, const int4 *__restrict__ rec_cn,
+                  const unsigned *__restrict__ rec_meta, const T *__restrict__ x,
+                  const T *__restrict__ q, const T *__restrict__ adt, T *__restrict__ res,
+                  AirConst<T> k, BresLink bl) {
+  const int G = gridDim.x * NT;
+  int c = blockIdx.x * NT + threadIdx.x;
+  if (c >= ncell) return;
+  CornerOps<T> cur, nxt;
+  CornerRec r1 = load_crec(rec_o, rec_cn, rec_meta, c + G, ncell);
+  {
+    const CornerRec r0 = load_crec(rec_o, rec_cn, rec_meta, c, ncell);
+    load_corner_cell<T, true>(cur, c, r0, x, q, adt, res, bl);
+  }
+  for (; c < ncell; c += G) {
+    const CornerRec r2 = load_crec(rec_o, rec_cn, rec_meta, c + 2 * G, ncell);
+    if (c + G < ncell) load_corner_cell<T, true>(nxt, c + G, r1, x, q, adt, res, bl);
+    compute_corner<T, true>(cur, c, res, k);
     cur = nxt;
     r1 = r2;
   }
@@ -481,6 +547,40 @@ cudaError_t launch_res_calc_gather_corner(const LaunchCtx &ctx, const SlotRecord
   return minb >= 3 ? launch_corner(k_res_gather_corner<T, 128, 3>, 128, ctx, s, x, q, adt, res, k)
                    : launch_corner(k_res_gather_corner<T, 128, 1>, 128, ctx, s, x, q, adt, res, k);
 }
+
+template <typename T>
+cudaError_t launch_res_bres_corner(const LaunchCtx &ctx, const SlotRecords &s,
+                                   const BresRecords &b, const int *bound, const T *x,
+                                   const T *q, const T *adt, T *res, const AirConst<T> &k,
+                                   int block) {
+  if (s.ncell <= 0) return cudaSuccess;
+  (void)b;
+  const BresLink bl{bound};
+  auto run = [&](auto kern, int nt) -> cudaError_t {
+    int per_sm = 1;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nt, 0);
+    if (e != cudaSuccess) return e;
+    long long blocks = (long long)ctx.nsm * (per_sm < 1 ? 1 : per_sm);
+    const long long need = (s.ncell + nt - 1) / nt;
+    if (blocks > need) blocks = need;
+    kern<<<(unsigned)blocks, nt, 0, ctx.stream>>>(
+        s.ncell, reinterpret_cast<const int4 *>(s.o), reinterpret_cast<const int4 *>(s.cn),
+        s.meta, x, q, adt, res, k, bl);
+    ctx.count();
+    return cudaGetLastError();
+  };
+  return block == 128 ? run(k_res_bres_corner<T, 128>, 128) : run(k_res_bres_corner<T, 256>, 256);
+}
+
+template cudaError_t launch_res_bres_corner<double>(const LaunchCtx &, const SlotRecords &,
+                                                    const BresRecords &, const int *,
+                                                    const double *, const double *,
+                                                    const double *, double *,
+                                                    const AirConst<double> &, int);
+template cudaError_t launch_res_bres_corner<float>(const LaunchCtx &, const SlotRecords &,
+                                                   const BresRecords &, const int *, const float *,
+                                                   const float *, const float *, float *,
+                                                   const AirConst<float> &, int);
 
 template cudaError_t launch_res_calc_gather_corner<double>(const LaunchCtx &, const SlotRecords &,
                                                            const double *, const double *,

@@ -94,6 +94,20 @@ cudaError_t launch_bres_calc_records(const LaunchCtx &c, const BresRecords &b, c
                                      const T *x, const T *q, const T *adt, T *res,
                                      const AirConst<T> &k);
 
+// Link the boundary edges into the corner records for the fused res_calc +
+// bres_calc: a boundary cell's boundary edges go into the unused slots of its
+// corner record, after its interior slots and in edge order (meta bit 6, the
+// edge's nodes as corners, o = the boundary edge).  False when some boundary
+// edge finds no unused slot or has a node that is not a corner of its cell, or
+// the corner records are not usable; the loops then run one after the other.
+bool link_boundary_records(const SlotRecords *s, const BresRecords *b, op_map pbecell);
+// airfoil_pipe.cu: the fused kernel (block 128 or 256)
+template <typename T>
+cudaError_t launch_res_bres_corner(const LaunchCtx &c, const SlotRecords &s,
+                                   const BresRecords &b, const int *bound, const T *x,
+                                   const T *q, const T *adt, T *res, const AirConst<T> &k,
+                                   int block);
+
 template <typename T>
 cudaError_t launch_res_calc_gather(const LaunchCtx &c, const InvMap &inv, const int *pedge,
                                    const int *pecell, const T *x, const T *q, const T *adt,

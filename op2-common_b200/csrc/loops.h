@@ -51,6 +51,10 @@ cudaError_t launch_map_check(const LaunchCtx &c, const int *map, long long n, in
 template <typename T>
 cudaError_t launch_adt_calc(const LaunchCtx &c, int ncell, const int *pcell, const T *x,
                             const T *q, T *adt, const AirConst<T> &k, int minb = 0);
+// save_soln (q -> qold) fused into adt_calc: one pass over q
+template <typename T>
+cudaError_t launch_adt_save(const LaunchCtx &c, int ncell, const int *pcell, const T *x,
+                            const T *q, T *adt, T *qold, const AirConst<T> &k);
 template <typename T>
 cudaError_t launch_res_calc_atomic(const LaunchCtx &c, int nedge, const int *pedge,
                                    const int *pecell, const T *x, const T *q, const T *adt,

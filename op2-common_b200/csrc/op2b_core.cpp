@@ -24,6 +24,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -91,12 +92,18 @@ bool is_real(const char *type, int bytes) {
 
 LaunchCtx Runtime::ctx() { return LaunchCtx{stream, nsm, &launches}; }
 
+// launch a deferred loop before a call that observes the library's state
+static void flush_quiet() {
+  Runtime &r = rt();
+  if (r.initialised && r.pend.kind) r.flush_pending();
+}
+
 bool Runtime::ready() {
   if (!initialised) {
     set_error("op_init has not been called");
     return false;
   }
-  return true;
+  return pend.kind == 0 || flush_pending();
 }
 
 // ------------------------------------------------------------------ timing
@@ -224,6 +231,14 @@ void op_init(int argc, char **argv, int diags) {
     return;
   r.red.host_out = reinterpret_cast<RedSlot *>(r.pinned_dev);
   if (!cuda_ok(cudaMalloc((void **)&r.check_d, 256), "op_init: map check word")) return;
+  // setup temporaries (renumbering, inverse maps, records) come from the
+  // device's stream-ordered pool: kept in the pool between uses instead of
+  // returned to the driver, so repeated setup makes no driver calls
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   r.initialised = true;
   if (diags > 1)
     printf(" op2b: device %d (%s, %d SMs), stream %p\n", dev, prop.name, r.nsm,
@@ -233,6 +248,7 @@ void op_init(int argc, char **argv, int diags) {
 void op_exit(void) {
   Runtime &r = rt();
   if (!r.initialised) return;
+  if (r.pend.kind) r.flush_pending();
   cudaStreamSynchronize(r.stream);
   release_plans();
   release_inverse_maps();
@@ -268,7 +284,10 @@ void op_exit(void) {
   cudaFree(r.check_d);
   r.check_d = nullptr;
   cudaFreeHost(r.pinned);
+  cudaStreamSynchronize(r.own_stream);
   cudaStreamDestroy(r.own_stream);
+  cudaMemPool_t pool;  // give the pooled setup memory back
+  if (cudaDeviceGetDefaultMemPool(&pool, r.device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
   r.red_base = nullptr;
   r.pinned = nullptr;
   r.stream = r.own_stream = nullptr;
@@ -289,6 +308,8 @@ void op_exit(void) {
   r.opt_gather_minb = d.opt_gather_minb;
   r.opt_bres_kernel = d.opt_bres_kernel;
   r.opt_adt_minb = d.opt_adt_minb;
+  r.opt_fuse = d.opt_fuse;
+  r.pend = PendingLoop{};
   r.opt_pipe_block = d.opt_pipe_block;
   r.opt_pipe_hints = d.opt_pipe_hints;
   r.opt_plan_mode = d.opt_plan_mode;
@@ -727,6 +748,7 @@ void op_diagnostic_output(void) {
 // GB/s uses each loop's algorithmic bytes per call.
 void op_timing_output(void) {
   Runtime &r = rt();
+  flush_quiet();
   r.resolve_timing();
   std::vector<std::pair<std::string, LoopStat>> v(r.stats.begin(), r.stats.end());
   std::sort(v.begin(), v.end(),
@@ -758,11 +780,18 @@ int op2b_dat_upload(op_dat dat, const char *src, size_t bytes) {
   return cuda_ok(cudaStreamSynchronize(r.stream), "op2b_dat_upload") ? 0 : -1;
 }
 
-void *op2b_dat_device_ptr(op_dat dat) { return dat ? dat->data_d : nullptr; }
-void *op2b_map_device_ptr(op_map map) { return map ? map->map_d : nullptr; }
+void *op2b_dat_device_ptr(op_dat dat) {
+  flush_quiet();
+  return dat ? dat->data_d : nullptr;
+}
+void *op2b_map_device_ptr(op_map map) {
+  flush_quiet();
+  return map ? map->map_d : nullptr;
+}
 
 int op2b_set_option(const char *key, long value) {
   Runtime &r = rt();
+  if (r.initialised && r.pend.kind && !r.flush_pending()) return -1;
   std::string k = key ? key : "";
   if (k == "inc_mode") {
     if (value < 0 || value > 3) {
@@ -806,6 +835,8 @@ int op2b_set_option(const char *key, long value) {
       return -1;
     }
     r.opt_bres_kernel = (int)value;
+  } else if (k == "fuse") {
+    r.opt_fuse = value != 0;
   } else if (k == "adt_minblocks") {
     if (value < 0 || value > 8) {
       set_error("op2b_set_option: adt_minblocks must be 0..8");
@@ -838,6 +869,7 @@ long op2b_get_option(const char *key) {
   if (k == "gather_minblocks") return r.opt_gather_minb;
   if (k == "bres_kernel") return r.opt_bres_kernel;
   if (k == "adt_minblocks") return r.opt_adt_minb;
+  if (k == "fuse") return r.opt_fuse;
   if (k == "nsm") return r.nsm;
   return -1;
 }
@@ -845,6 +877,7 @@ long op2b_get_option(const char *key) {
 int op2b_loop_stats(const char *name, double *total_ms, long *calls, double *bytes_per_call,
                     double *last_ms) {
   Runtime &r = rt();
+  flush_quiet();
   r.resolve_timing();
   auto it = r.stats.find(name ? name : "");
   if (it == r.stats.end()) return -1;
@@ -857,6 +890,7 @@ int op2b_loop_stats(const char *name, double *total_ms, long *calls, double *byt
 
 void op2b_reset_stats(void) {
   Runtime &r = rt();
+  flush_quiet();
   r.resolve_timing();
   for (auto &kv : r.stats) {
     double plan = kv.second.plan_ms;
@@ -865,7 +899,10 @@ void op2b_reset_stats(void) {
   }
 }
 
-long op2b_kernel_launches(void) { return rt().launches; }
+long op2b_kernel_launches(void) {
+  flush_quiet();
+  return rt().launches;
+}
 
 int op2b_set_stream(void *stream) {
   Runtime &r = rt();
@@ -875,7 +912,10 @@ int op2b_set_stream(void *stream) {
   return 0;
 }
 
-void *op2b_get_stream(void) { return (void *)rt().stream; }
+void *op2b_get_stream(void) {
+  flush_quiet();
+  return (void *)rt().stream;
+}
 
 int op2b_synchronize(void) {
   Runtime &r = rt();

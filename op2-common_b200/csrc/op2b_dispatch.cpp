@@ -161,7 +161,21 @@ int loop_save_soln(const char *name, op_set set, int nargs, op_arg *a) {
   if (!s.ok) return -1;
   if (a[0].dat->size != a[1].dat->size) return s.fail(1, "element size differs from argument 0"), -1;
   Runtime &r = rt();
+  if (r.pend.kind && !r.flush_pending()) return -1;
   size_t bytes = (size_t)set->size * (size_t)a[0].dat->size;
+  int tb = a[0].dat->type ? type_bytes(a[0].dat->type) : 0;
+  if (r.opt_fuse && dim == 4 && is_real(a[0].dat->type, tb) && a[0].dat != a[1].dat) {
+    // deferred: launched with the next loop call (fused into an adt_calc on
+    // the same q) or alone before any other call
+    r.pend = PendingLoop{};
+    r.pend.kind = 1;
+    r.pend.set = set;
+    r.pend.src = a[0].dat;
+    r.pend.dst = a[1].dat;
+    r.pend.rb = tb;
+    r.pend.bytes = 2.0 * (double)bytes;
+    return 0;
+  }
   r.begin_loop(name);
   cudaError_t e = launch_copy(r.ctx(), a[0].dat->data_d, a[1].dat->data_d, bytes);
   r.end_loop(2.0 * (double)bytes);
@@ -184,6 +198,34 @@ int loop_adt_calc(const char *name, op_set set, int nargs, op_arg *a) {
   Runtime &r = rt();
   int C = set->size, N = a[0].dat->set->size;
   double bytes = 16.0 * C + (double)rb * (2.0 * N + 5.0 * C);
+  PendingLoop &pd = r.pend;
+  if (pd.kind == 1 && pd.src == a[4].dat && pd.set == set && pd.rb == rb &&
+      pd.dst != a[0].dat && pd.dst != a[5].dat) {
+    // save_soln (q -> qold) and this adt_calc in one pass over q: the fused
+    // call moves adt_calc's bytes plus qold's write
+    op_dat qold = pd.dst;
+    const double fused = bytes + 4.0 * rb * (double)C;
+    pd = PendingLoop{};
+    bool ok;
+    cudaError_t e;
+    r.begin_loop("save_soln+adt_calc");
+    if (rb == 8) {
+      AirConst<double> k = air_consts<double>(ok);
+      if (!ok) return -1;
+      e = launch_adt_save<double>(r.ctx(), C, pcell->map_d, (const double *)a[0].dat->data_d,
+                                  (const double *)a[4].dat->data_d, (double *)a[5].dat->data_d,
+                                  (double *)qold->data_d, k);
+    } else {
+      AirConst<float> k = air_consts<float>(ok);
+      if (!ok) return -1;
+      e = launch_adt_save<float>(r.ctx(), C, pcell->map_d, (const float *)a[0].dat->data_d,
+                                 (const float *)a[4].dat->data_d, (float *)a[5].dat->data_d,
+                                 (float *)qold->data_d, k);
+    }
+    r.end_loop(fused);
+    return finish(e, name);
+  }
+  if (pd.kind && !r.flush_pending()) return -1;
   r.begin_loop(name);
   cudaError_t e;
   bool ok;
@@ -250,8 +292,38 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
   int rb = s.real_bytes({0, 2, 4, 6});
   if (!s.ok) return -1;
   Runtime &r = rt();
+  if (r.pend.kind && !r.flush_pending()) return -1;
   int E = set->size, N = a[0].dat->set->size, C = a[2].dat->set->size;
   double bytes = 16.0 * E + (double)rb * (2.0 * N + 13.0 * C);
+  if (r.opt_fuse && r.opt_inc_mode == OP2B_INC_GATHER &&
+      r.opt_gather_kernel == OP2B_GATHER_CORNER && r.opt_bres_kernel == 1) {
+    const SlotRecords *cr = get_corner_records(pecell, pedge);
+    if (!cr) return -1;
+    bool ok = true;
+    if (cr->corners) {
+      // deferred: fused with a following bres_calc on the same res, or
+      // launched alone before any other call
+      PendingLoop &pd = r.pend;
+      pd = PendingLoop{};
+      pd.kind = 2;
+      pd.set = set;
+      pd.pedge = pedge;
+      pd.pecell = pecell;
+      pd.x = a[0].dat;
+      pd.q = a[2].dat;
+      pd.adt = a[4].dat;
+      pd.res = a[6].dat;
+      pd.rb = rb;
+      pd.bytes = bytes;
+      if (rb == 8) pd.kd = air_consts<double>(ok);
+      else pd.kf = air_consts<float>(ok);
+      if (!ok) {
+        pd = PendingLoop{};
+        return -1;
+      }
+      return 0;
+    }
+  }
   Plan *plan = nullptr;
   const InvMap *inv = nullptr;
   const SlotRecords *slots = nullptr;
@@ -322,6 +394,40 @@ int loop_bres_calc(const char *name, op_set set, int nargs, op_arg *a) {
   Runtime &r = rt();
   int B = set->size;
   double bytes = 16.0 * B + (double)rb * (2.0 + 4.0 + 1.0 + 8.0) * B;
+  PendingLoop &pd = r.pend;
+  if (pd.kind == 2 && pd.res == a[4].dat && pd.q == a[2].dat && pd.adt == a[3].dat &&
+      pd.x == a[0].dat && pd.rb == rb && r.opt_inc_mode == OP2B_INC_GATHER &&
+      r.opt_bres_kernel == 1) {
+    const SlotRecords *cr = get_corner_records(pd.pecell, pd.pedge);
+    const BresRecords *br = cr ? get_bres_records(pbecell, pbedge) : nullptr;
+    if (cr && br && link_boundary_records(cr, br, pbecell)) {
+      // res_calc's and this bres_calc's increments in one launch, in the order
+      // of the two loops run one after the other; beyond res_calc's bytes the
+      // fused call reads the boundary maps, flags and nodes (q, adt and res of
+      // the boundary cells move with res_calc's)
+      const double fused = pd.bytes + 16.0 * B + 4.0 * rb * B;
+      const int *bound = (const int *)a[5].dat->data_d;
+      cudaError_t e;
+      r.begin_loop("res_calc+bres_calc");
+      if (rb == 8)
+        e = launch_res_bres_corner<double>(r.ctx(), *cr, *br, bound,
+                                           (const double *)pd.x->data_d,
+                                           (const double *)pd.q->data_d,
+                                           (const double *)pd.adt->data_d,
+                                           (double *)pd.res->data_d, pd.kd, r.opt_pipe_block);
+      else
+        e = launch_res_bres_corner<float>(r.ctx(), *cr, *br, bound,
+                                          (const float *)pd.x->data_d,
+                                          (const float *)pd.q->data_d,
+                                          (const float *)pd.adt->data_d,
+                                          (float *)pd.res->data_d, pd.kf, r.opt_pipe_block);
+      r.end_loop(fused);
+      pd = PendingLoop{};
+      return finish(e, name);
+    }
+    if (!cr || (r.opt_bres_kernel == 1 && !br)) return -1;
+  }
+  if (pd.kind && !r.flush_pending()) return -1;
   Plan *plan = nullptr;
   const InvMap *inv = nullptr;
   const BresRecords *brec = nullptr;
@@ -388,6 +494,7 @@ int loop_update(const char *name, op_set set, int nargs, op_arg *a) {
   if (!s.ok) return -1;
   if (a[4].type && strcmp(a[4].type, "double") != 0) return s.fail(4, "rms must be double"), -1;
   Runtime &r = rt();
+  if (r.pend.kind && !r.flush_pending()) return -1;
   int C = set->size;
   double bytes = (double)rb * 17.0 * C;
   r.red.seq = ++r.red_seq;
@@ -432,17 +539,56 @@ const Entry kLoops[] = {{"save_soln", loop_save_soln},
 
 }  // namespace
 
+// Launch the deferred loop on its own (the calls it could have been fused
+// with did not follow).  Errors are reported by the call that triggered it.
+bool op2b::Runtime::flush_pending() {
+  PendingLoop pd = pend;
+  pend = PendingLoop{};
+  cudaError_t e = cudaSuccess;
+  if (pd.kind == 1) {
+    size_t bytes = (size_t)pd.set->size * (size_t)pd.src->size;
+    begin_loop("save_soln");
+    e = launch_copy(ctx(), pd.src->data_d, pd.dst->data_d, bytes);
+    end_loop(pd.bytes);
+    return finish(e, "save_soln") == 0;
+  }
+  if (pd.kind == 2) {
+    const SlotRecords *cr = get_corner_records(pd.pecell, pd.pedge);
+    if (!cr) return false;
+    begin_loop("res_calc");
+    if (pd.rb == 8)
+      e = launch_res_calc_gather_corner<double>(ctx(), *cr, (const double *)pd.x->data_d,
+                                                (const double *)pd.q->data_d,
+                                                (const double *)pd.adt->data_d,
+                                                (double *)pd.res->data_d, pd.kd, opt_pipe_block,
+                                                opt_gather_minb);
+    else
+      e = launch_res_calc_gather_corner<float>(ctx(), *cr, (const float *)pd.x->data_d,
+                                               (const float *)pd.q->data_d,
+                                               (const float *)pd.adt->data_d,
+                                               (float *)pd.res->data_d, pd.kf, opt_pipe_block,
+                                               opt_gather_minb);
+    end_loop(pd.bytes);
+    return finish(e, "res_calc") == 0;
+  }
+  return true;
+}
+
 extern "C" {
 
 int op_par_loop_c(char const *name, op_set set, int nargs, op_arg *args) {
   Runtime &r = rt();
-  if (!r.ready()) return -1;
+  if (!r.initialised) {
+    set_error("op_init has not been called");
+    return -1;
+  }
   if (!name || !set || (nargs > 0 && !args)) {
     set_error("op_par_loop: needs a name, a set and the argument list");
     return -1;
   }
   for (const Entry &e : kLoops)
     if (strcmp(e.name, name) == 0) return e.fn(name, set, nargs, args);
+  if (r.pend.kind) r.flush_pending();
   set_error("op_par_loop(%s): no device implementation of this loop is registered "
             "(libop2b runs loops on the GPU only)",
             name);

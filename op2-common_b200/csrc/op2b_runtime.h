@@ -29,6 +29,21 @@ struct PendingTime {
 
 struct Plan;  // plan.h
 
+// A loop call whose launch is deferred to the next library call, so that it
+// can be fused with the loop that follows it (save_soln into adt_calc,
+// res_calc with bres_calc).  Any other call launches it first, alone.
+struct PendingLoop {
+  int kind = 0;  // 0 none, 1 save_soln, 2 res_calc
+  op_set set = nullptr;
+  op_dat src = nullptr, dst = nullptr;  // save_soln: q (read), qold (written)
+  op_map pedge = nullptr, pecell = nullptr;
+  op_dat x = nullptr, q = nullptr, adt = nullptr, res = nullptr;  // res_calc
+  int rb = 0;           // bytes per real (8 double, 4 float)
+  double bytes = 0.0;   // algorithmic bytes of the deferred call
+  AirConst<double> kd{};
+  AirConst<float> kf{};
+};
+
 struct Runtime {
   bool initialised = false;
   int device = 0, nsm = 148, cc_major = 0, cc_minor = 0;
@@ -47,7 +62,8 @@ struct Runtime {
   int opt_gather_kernel = 6;  // OP2B_GATHER_CORNER (gather.h)
   int opt_gather_minb = 0;    // __launch_bounds__ minimum blocks of the gather kernels
   int opt_bres_kernel = 1;    // bres_calc gather: 0 = inverse-map walk, 1 = boundary records
-  int opt_adt_minb = 0;       // __launch_bounds__ minimum blocks of adt_calc (0 = 1)
+  int opt_fuse = 1;           // defer save_soln / res_calc to fuse them with the next loop
+  int opt_adt_minb = 0;       // adt_calc: __launch_bounds__ minimum blocks (0 = none)
   int opt_pipe_block = 256;   // threads per CTA of the pipelined gather (64, 96, 128, 256)
   int opt_pipe_hints = 0;     // register pipeline: evict-first hints on once-read streams
   int opt_plan_mode = 0;      // 0 = parallel block colouring, 1 = serial greedy (bit-exact)
@@ -74,8 +90,12 @@ struct Runtime {
   std::string cur_loop;
   cudaEvent_t cur_ev0 = nullptr, cur_ev1 = nullptr;
 
+  PendingLoop pend;
+
   LaunchCtx ctx();
+  // initialised, with any deferred loop launched (false on error)
   bool ready();
+  bool flush_pending();  // op2b_dispatch.cpp
   void begin_loop(const char *name);
   void end_loop(double bytes);
   void resolve_timing();

@@ -36,59 +36,9 @@
 #include <vector>
 
 #include "op2b_runtime.h"
+#include "scan.h"
 
 namespace op2b {
-
-// ------------------------------------------------------------------ scans
-
-__global__ void k_scan_blocks(const int *in, long long *out, long long n, long long *bsum) {
-  __shared__ long long s[1024];
-  long long i = (long long)blockIdx.x * 1024 + threadIdx.x;
-  long long v = i < n ? in[i] : 0;
-  s[threadIdx.x] = v;
-  __syncthreads();
-  for (int o = 1; o < 1024; o <<= 1) {
-    long long t = threadIdx.x >= (unsigned)o ? s[threadIdx.x - o] : 0;
-    __syncthreads();
-    s[threadIdx.x] += t;
-    __syncthreads();
-  }
-  if (i < n) out[i] = s[threadIdx.x] - v;
-  if (threadIdx.x == 1023) bsum[blockIdx.x] = s[1023];
-}
-
-__global__ void k_scan_bsum(long long *bsum, long long nb, long long *total) {
-  if (threadIdx.x != 0) return;
-  long long acc = 0;
-  for (long long b = 0; b < nb; b++) {
-    long long t = bsum[b];
-    bsum[b] = acc;
-    acc += t;
-  }
-  *total = acc;
-}
-
-__global__ void k_scan_add(long long *out, long long n, const long long *bsum) {
-  long long i = (long long)blockIdx.x * 1024 + threadIdx.x;
-  if (i < n) out[i] += bsum[blockIdx.x];
-}
-
-// exclusive scan of n ints into out (n+1 entries: out[n] = total)
-static bool scan_exclusive(const int *in, long long *out, long long n, cudaStream_t s) {
-  long long nb = (n + 1023) / 1024;
-  long long *bsum = nullptr;
-  if (cudaMalloc(&bsum, sizeof(long long) * (nb + 1)) != cudaSuccess) return false;
-  if (nb > 0) {
-    k_scan_blocks<<<(unsigned)nb, 1024, 0, s>>>(in, out, n, bsum);
-    k_scan_bsum<<<1, 32, 0, s>>>(bsum, nb, out + n);
-    k_scan_add<<<(unsigned)nb, 1024, 0, s>>>(out, n, bsum);
-  } else {
-    cudaMemsetAsync(out, 0, sizeof(long long), s);
-  }
-  bool ok = cudaStreamSynchronize(s) == cudaSuccess;
-  cudaFree(bsum);
-  return ok;
-}
 
 // ------------------------------------------------------------------ graph
 
@@ -194,6 +144,82 @@ __device__ int rcm_block_scan(int v, int *total) {
   return before;
 }
 
+constexpr int kB = 2;   // vertices a thread handles per round
+constexpr int kNb = 4;  // neighbours per vertex loaded unrolled (the rest in a loop)
+
+// The first kNb unvisited neighbours of up to kB level vertices
+// (cur[j0 + k * blockDim.x]); v = -1 where there is none.
+struct LevelBatch {
+  int d[kB];
+  long long r[kB];
+  int v[kB][kNb];
+  __device__ void load(const RcmWork &w, const int *cur, int len, int j0) {
+    int u[kB];
+#pragma unroll
+    for (int k = 0; k < kB; k++) {
+      const int j = j0 + k * (int)blockDim.x;
+      u[k] = j < len ? cur[j] : -1;
+    }
+#pragma unroll
+    for (int k = 0; k < kB; k++) {
+      d[k] = u[k] >= 0 ? w.deg[u[k]] : 0;
+      r[k] = u[k] >= 0 ? w.row[u[k]] : 0;
+    }
+#pragma unroll
+    for (int k = 0; k < kB; k++)
+#pragma unroll
+      for (int t = 0; t < kNb; t++) v[k][t] = t < d[k] ? w.col[r[k] + t] : -1;
+#pragma unroll
+    for (int k = 0; k < kB; k++)
+#pragma unroll
+      for (int t = 0; t < kNb; t++)
+        if (v[k][t] >= 0 && w.newidx[v[k][t]] >= 0) v[k][t] = -1;
+  }
+};
+
+// Up to kB consecutive parents j0 .. min(j0 + kB, je) - 1 of a level with
+// their first kNb neighbours, each neighbour's claim (pkey) and degree.
+struct ParentBatch {
+  int d[kB];
+  long long r[kB];
+  int v[kB][kNb], pk[kB][kNb], vd[kB][kNb];
+  __device__ void load(const RcmWork &w, const int *cur, int j0, int je) {
+    int u[kB];
+#pragma unroll
+    for (int k = 0; k < kB; k++) u[k] = j0 + k < je ? cur[j0 + k] : -1;
+#pragma unroll
+    for (int k = 0; k < kB; k++) {
+      d[k] = u[k] >= 0 ? w.deg[u[k]] : 0;
+      r[k] = u[k] >= 0 ? w.row[u[k]] : 0;
+    }
+#pragma unroll
+    for (int k = 0; k < kB; k++)
+#pragma unroll
+      for (int t = 0; t < kNb; t++) v[k][t] = t < d[k] ? w.col[r[k] + t] : -1;
+#pragma unroll
+    for (int k = 0; k < kB; k++)
+#pragma unroll
+      for (int t = 0; t < kNb; t++) {
+        const int x = v[k][t];
+        const bool open = x >= 0 && w.newidx[x] < 0;
+        pk[k][t] = open ? w.pkey[x] : -1;
+        vd[k][t] = open ? w.deg[x] : 0;
+      }
+  }
+  __device__ bool claimed(int k, int t, int j) const { return v[k][t] >= 0 && pk[k][t] == j; }
+  // children of parent k (position j) that it claimed
+  __device__ int count(const RcmWork &w, int k, int j) const {
+    int c = 0;
+#pragma unroll
+    for (int t = 0; t < kNb; t++) c += claimed(k, t, j) ? 1 : 0;
+    for (int t = kNb; t < d[k]; t++) {
+      int x = w.col[r[k] + t];
+      if (w.newidx[x] < 0 && w.pkey[x] == j) c++;
+    }
+    return c;
+  }
+};
+
 // BFS from `start` over vertices not yet ordered; marks with `stamp`.
 // Returns the number of levels; the last level is left in *last (lev_a or lev_b).
 __device__ int rcm_bfs(RcmWork &w, int start, int stamp, int **last, int *last_len) {
@@ -211,14 +237,31 @@ __device__ int rcm_bfs(RcmWork &w, int start, int stamp, int **last, int *last_l
     nlev++;
     if (threadIdx.x == 0) s_next = 0;
     __syncthreads();
-    for (int j = threadIdx.x; j < len; j += blockDim.x) {
-      int u = cur[j];
-      long long r = w.row[u];
-      int d = w.deg[u];
-      for (int t = 0; t < d; t++) {
-        int v = w.col[r + t];
-        if (w.newidx[v] < 0 && atomicExch(&w.mark[v], stamp) != stamp) nxt[atomicAdd(&s_next, 1)] = v;
-      }
+    // kB vertices per thread per round, their first kNb neighbours unrolled:
+    // every load of a round is independent of the others, so one round costs
+    // a handful of memory latencies however many vertices it covers
+    for (int j0 = threadIdx.x; j0 < len; j0 += kB * blockDim.x) {
+      LevelBatch b;
+      b.load(w, cur, len, j0);
+      // all exchanges first (none waits on another's result), then the appends
+      int old[kB][kNb];
+#pragma unroll
+      for (int k = 0; k < kB; k++)
+#pragma unroll
+        for (int t = 0; t < kNb; t++)
+          old[k][t] = b.v[k][t] >= 0 ? atomicExch(&w.mark[b.v[k][t]], stamp) : stamp;
+#pragma unroll
+      for (int k = 0; k < kB; k++)
+#pragma unroll
+        for (int t = 0; t < kNb; t++)
+          if (old[k][t] != stamp) nxt[atomicAdd(&s_next, 1)] = b.v[k][t];
+#pragma unroll
+      for (int k = 0; k < kB; k++)
+        for (int t = kNb; t < b.d[k]; t++) {  // vertices of higher degree
+          int v = w.col[b.r[k] + t];
+          if (w.newidx[v] < 0 && atomicExch(&w.mark[v], stamp) != stamp)
+            nxt[atomicAdd(&s_next, 1)] = v;
+        }
     }
     __syncthreads();
     int nl = s_next;
@@ -285,12 +328,19 @@ __global__ void __launch_bounds__(kRcmThreads) k_rcm(RcmWork w) {
       const int len = s_len;
       const int base = s_pos;
       // first parent (lowest position in this level) of every new vertex
-      for (int j = threadIdx.x; j < len; j += blockDim.x) {
-        int u = cur[j];
-        long long r = w.row[u];
-        for (int t = 0; t < w.deg[u]; t++) {
-          int v = w.col[r + t];
-          if (w.newidx[v] < 0) atomicMin(&w.pkey[v], j);
+      for (int j0 = threadIdx.x; j0 < len; j0 += kB * blockDim.x) {
+        LevelBatch b;
+        b.load(w, cur, len, j0);
+#pragma unroll
+        for (int k = 0; k < kB; k++) {
+          const int j = j0 + k * (int)blockDim.x;
+#pragma unroll
+          for (int t = 0; t < kNb; t++)
+            if (b.v[k][t] >= 0) atomicMin(&w.pkey[b.v[k][t]], j);
+          for (int t = kNb; t < b.d[k]; t++) {
+            int v = w.col[b.r[k] + t];
+            if (w.newidx[v] < 0) atomicMin(&w.pkey[v], j);
+          }
         }
       }
       __syncthreads();
@@ -302,44 +352,69 @@ __global__ void __launch_bounds__(kRcmThreads) k_rcm(RcmWork w) {
       const int chunk = (len + (int)blockDim.x - 1) / (int)blockDim.x;
       const int jb = min(len, (int)threadIdx.x * chunk), je = min(len, jb + chunk);
       int mine = 0;
-      for (int j = jb; j < je; j++) {
-        int u = cur[j];
-        long long r = w.row[u];
-        for (int t = 0; t < w.deg[u]; t++) {
-          int v = w.col[r + t];
-          if (w.newidx[v] < 0 && w.pkey[v] == j) mine++;
-        }
+      for (int j0 = jb; j0 < je; j0 += kB) {
+        ParentBatch pb;
+        pb.load(w, cur, j0, je);
+#pragma unroll
+        for (int k = 0; k < kB; k++) mine += pb.count(w, k, j0 + k);
       }
       int nl = 0;
       int pos = rcm_block_scan(mine, &nl);
       if (nl == 0) break;
-      for (int j = jb; j < je; j++) {
-        int u = cur[j];
-        long long r = w.row[u];
-        const int d = w.deg[u];
-        const int first = pos;
-        // selection: the smallest claimed key above the last one emitted
-        unsigned long long last = 0;
-        bool any = false;
-        while (true) {
-          unsigned long long best = ~0ull;
-          for (int t = 0; t < d; t++) {
-            int v = w.col[r + t];
-            if (w.newidx[v] < 0 && w.pkey[v] == j) {
-              unsigned long long key =
-                  ((unsigned long long)(unsigned)min(w.deg[v], 63) << 32) | (unsigned)v;
-              if ((!any || key > last) && key < best) best = key;
+      for (int j0 = jb; j0 < je; j0 += kB) {
+        ParentBatch pb;
+        pb.load(w, cur, j0, je);
+#pragma unroll
+        for (int k = 0; k < kB; k++) {
+          const int j = j0 + k;
+          if (j >= je) break;
+          const int first = pos;
+          if (pb.d[k] <= kNb) {
+            // the claimed children's (degree capped at 63, id) keys, sorted in registers
+            unsigned long long key[kNb];
+#pragma unroll
+            for (int t = 0; t < kNb; t++)
+              key[t] = pb.claimed(k, t, j)
+                           ? ((unsigned long long)(unsigned)min(pb.vd[k][t], 63) << 32) |
+                                 (unsigned)pb.v[k][t]
+                           : ~0ull;
+#pragma unroll
+            for (int i = 1; i < kNb; i++)
+#pragma unroll
+              for (int m = i; m > 0; m--)
+                if (key[m] < key[m - 1]) {
+                  unsigned long long x = key[m];
+                  key[m] = key[m - 1];
+                  key[m - 1] = x;
+                }
+#pragma unroll
+            for (int t = 0; t < kNb; t++)
+              if (key[t] != ~0ull) nxt[pos++] = (int)(key[t] & 0xffffffffull);
+          } else {
+            // higher degree: selection of the smallest claimed key above the last
+            unsigned long long last = 0;
+            bool any = false;
+            while (true) {
+              unsigned long long best = ~0ull;
+              for (int t = 0; t < pb.d[k]; t++) {
+                int v = w.col[pb.r[k] + t];
+                if (w.newidx[v] < 0 && w.pkey[v] == j) {
+                  unsigned long long key =
+                      ((unsigned long long)(unsigned)min(w.deg[v], 63) << 32) | (unsigned)v;
+                  if ((!any || key > last) && key < best) best = key;
+                }
+              }
+              if (best == ~0ull) break;
+              nxt[pos++] = (int)(best & 0xffffffffull);
+              last = best;
+              any = true;
             }
           }
-          if (best == ~0ull) break;
-          nxt[pos++] = (int)(best & 0xffffffffull);
-          last = best;
-          any = true;
-        }
-        for (int k = first; k < pos; k++) {
-          int v = nxt[k];
-          w.newidx[v] = base + k;
-          w.pkey[v] = INT_MAX;
+          for (int q = first; q < pos; q++) {
+            int v = nxt[q];
+            w.newidx[v] = base + q;
+            w.pkey[v] = INT_MAX;
+          }
         }
       }
       __syncthreads();
@@ -492,13 +567,13 @@ static bool base_rcm(op_map base, int *perm_d, cudaStream_t s) {
   std::vector<void *> tmp;
   auto A = [&](size_t bytes) {
     void *p = nullptr;
-    if (cudaMalloc(&p, bytes ? bytes : 1) != cudaSuccess) return (void *)nullptr;
+    if (cudaMallocAsync(&p, bytes ? bytes : 1, s) != cudaSuccess) return (void *)nullptr;
     tmp.push_back(p);
     return p;
   };
   auto cleanup = [&]() {
     cudaStreamSynchronize(s);
-    for (void *p : tmp) cudaFree(p);
+    for (void *p : tmp) cudaFreeAsync(p, s);
   };
   int *deg = (int *)A(sizeof(int) * (n + 1));
   long long *row = (long long *)A(sizeof(long long) * (n + 1));
@@ -566,12 +641,12 @@ static void propagate(op_set from, op_set to, std::vector<int *> &perm, cudaStre
       int *key, *cnt, *fill, *order, *pd;
       long long *start;
       int nk = from->size;
-      cudaMalloc(&key, sizeof(int) * n);
-      cudaMalloc(&cnt, sizeof(int) * (nk + 1));
-      cudaMalloc(&fill, sizeof(int) * (nk + 1));
-      cudaMalloc(&order, sizeof(int) * n);
-      cudaMalloc(&start, sizeof(long long) * (nk + 1));
-      cudaMalloc(&pd, sizeof(int) * n);
+      cudaMallocAsync(&key, sizeof(int) * n, s);
+      cudaMallocAsync(&cnt, sizeof(int) * (nk + 1), s);
+      cudaMallocAsync(&fill, sizeof(int) * (nk + 1), s);
+      cudaMallocAsync(&order, sizeof(int) * n, s);
+      cudaMallocAsync(&start, sizeof(long long) * (nk + 1), s);
+      cudaMallocAsync(&pd, sizeof(int) * n, s);
       cudaMemsetAsync(cnt, 0, sizeof(int) * (nk + 1), s);
       cudaMemsetAsync(fill, 0, sizeof(int) * (nk + 1), s);
       k_first_target_key<<<grid1(n), 256, 0, s>>>(n, m->dim, m->map_d, perm[from->index], key, cnt);
@@ -579,11 +654,11 @@ static void propagate(op_set from, op_set to, std::vector<int *> &perm, cudaStre
       k_bucket_fill<<<grid1(n), 256, 0, s>>>(n, key, start, fill, order);
       k_bucket_sort<<<grid1(nk), 256, 0, s>>>(nk, start, order, pd);
       ok = ok && cudaStreamSynchronize(s) == cudaSuccess;
-      cudaFree(key);
-      cudaFree(cnt);
-      cudaFree(fill);
-      cudaFree(order);
-      cudaFree(start);
+      cudaFreeAsync(key, s);
+      cudaFreeAsync(cnt, s);
+      cudaFreeAsync(fill, s);
+      cudaFreeAsync(order, s);
+      cudaFreeAsync(start, s);
       perm[to->index] = pd;
       break;
     }
@@ -595,10 +670,10 @@ static void propagate(op_set from, op_set to, std::vector<int *> &perm, cudaStre
       int *key, *flag, *missing, *pd;
       long long *pos;
       long long nslots = (long long)from->size * m->dim;
-      cudaMalloc(&key, sizeof(int) * n);
-      cudaMalloc(&flag, sizeof(int) * (nslots + 1));
-      cudaMalloc(&missing, sizeof(int));
-      cudaMalloc(&pos, sizeof(long long) * (nslots + 1));
+      cudaMallocAsync(&key, sizeof(int) * n, s);
+      cudaMallocAsync(&flag, sizeof(int) * (nslots + 1), s);
+      cudaMallocAsync(&missing, sizeof(int), s);
+      cudaMallocAsync(&pos, sizeof(long long) * (nslots + 1), s);
       cudaMemsetAsync(key, 0x7f, sizeof(int) * n, s);
       cudaMemsetAsync(flag, 0, sizeof(int) * (nslots + 1), s);
       cudaMemsetAsync(missing, 0, sizeof(int), s);
@@ -611,21 +686,21 @@ static void propagate(op_set from, op_set to, std::vector<int *> &perm, cudaStre
       int nmiss = 0;
       for (int i = 0; i < n; i++) nmiss += hk[i] == 0x7f7f7f7f;
       if (nmiss) {  // not onto: try the next map (:113-117)
-        cudaFree(key);
-        cudaFree(flag);
-        cudaFree(missing);
-        cudaFree(pos);
+        cudaFreeAsync(key, s);
+        cudaFreeAsync(flag, s);
+        cudaFreeAsync(missing, s);
+        cudaFreeAsync(pos, s);
         continue;
       }
       k_flag_keys<<<grid1(n), 256, 0, s>>>(n, key, flag, missing);
       ok = scan_exclusive(flag, pos, nslots, s);
-      cudaMalloc(&pd, sizeof(int) * n);
+      cudaMallocAsync(&pd, sizeof(int) * n, s);
       k_rank_keys<<<grid1(n), 256, 0, s>>>(n, key, pos, pd);
       ok = ok && cudaStreamSynchronize(s) == cudaSuccess;
-      cudaFree(key);
-      cudaFree(flag);
-      cudaFree(missing);
-      cudaFree(pos);
+      cudaFreeAsync(key, s);
+      cudaFreeAsync(flag, s);
+      cudaFreeAsync(missing, s);
+      cudaFreeAsync(pos, s);
       perm[to->index] = pd;
       break;
     }
@@ -686,7 +761,7 @@ int renumber(op_map base, long stats[4]) {
   std::vector<int *> perm(r.sets.size(), nullptr);
   op_set to = base->to;
   int *pb = nullptr;
-  if (cudaMalloc(&pb, sizeof(int) * std::max(to->size, 1)) != cudaSuccess) {
+  if (cudaMallocAsync(&pb, sizeof(int) * std::max(to->size, 1), s) != cudaSuccess) {
     set_error("op_renumber: out of device memory");
     return -1;
   }
@@ -715,12 +790,11 @@ int renumber(op_map base, long stats[4]) {
       if (m->from == set) {
         int *t;
         size_t bytes = sizeof(int) * (size_t)set->size * m->dim;
-        cudaMalloc(&t, bytes);
+        cudaMallocAsync(&t, bytes, s);
         k_move_rows<<<grid1((long long)set->size * m->dim), 256, 0, s>>>(set->size, m->dim, m->map_d,
                                                                           t, pd);
         cudaMemcpyAsync(m->map_d, t, bytes, cudaMemcpyDeviceToDevice, s);
-        cudaStreamSynchronize(s);
-        cudaFree(t);
+        cudaFreeAsync(t, s);
       }
     }
     for (auto &mp : r.maps) {
@@ -741,12 +815,11 @@ int renumber(op_map base, long stats[4]) {
       int words = d->size / 4;
       size_t bytes = (size_t)set->size * d->size;
       int *t;
-      cudaMalloc(&t, bytes);
+      cudaMallocAsync(&t, bytes, s);
       k_move_rows<<<grid1((long long)set->size * words), 256, 0, s>>>(
           set->size, words, reinterpret_cast<const int *>(d->data_d), t, pd);
       cudaMemcpyAsync(d->data_d, t, bytes, cudaMemcpyDeviceToDevice, s);
-      cudaStreamSynchronize(s);
-      cudaFree(t);
+      cudaFreeAsync(t, s);
     }
   }
   lap("reordering");
@@ -769,8 +842,7 @@ int renumber(op_map base, long stats[4]) {
       long long n = set->size;
       int *t = it->second;
       k_renumber_entries<<<grid1(n), 256, 0, s>>>(n, t, perm[set->index]);
-      cudaStreamSynchronize(s);
-      cudaFree(perm[set->index]);
+      cudaFreeAsync(perm[set->index], s);
     }
   }
   lap("host maps, composition");
@@ -808,13 +880,13 @@ void fetch_original_order(op_dat dat, char *dst, int low, int high) {
     return;
   }
   int *t = nullptr;
-  if (!cuda_ok(cudaMalloc(&t, bytes), "op_fetch_data_idx")) return;
+  if (!cuda_ok(cudaMallocAsync(&t, bytes, r.stream), "op_fetch_data_idx")) return;
   int words = dat->size / 4;
   k_gather_rows<<<grid1((long long)cnt * words), 256, 0, r.stream>>>(
       (int)cnt, words, reinterpret_cast<const int *>(dat->data_d), t, it->second, low);
   cudaMemcpyAsync(dst, t, bytes, cudaMemcpyDeviceToHost, r.stream);
+  cudaFreeAsync(t, r.stream);
   cuda_ok(cudaStreamSynchronize(r.stream), "op_fetch_data_idx");
-  cudaFree(t);
 }
 
 void release_renumbering() {

@@ -184,6 +184,62 @@ def test_pipelined_kernels_are_bit_identical(op2, hints):
             assert np.array_equal(out[0][k], o[k]), k
 
 
+def test_fused_loop_pairs_are_bit_identical_to_separate_loops(op2):
+    """The runtime defers save_soln and res_calc and fuses them with the
+    adt_calc / bres_calc that follow; with fusion off every loop launches on
+    its own.  q, adt, res, rms, maxerr and errloc agree bit for bit, in both
+    precisions, and a deferred loop is launched before anything observes it."""
+    m = M.channel_bump(96, 48, seed=12)
+    for dtype in (np.float64, np.float32):
+        out, hists, stats = [], [], []
+        for fuse in (0, 1):
+            op2.set_option("fuse", fuse)
+            op2.load().op2b_reset_stats()
+            app = Airfoil(m, dtype=dtype)
+            hists.append(app.iterate(4))
+            out.append(app.fetch())
+            stats.append({n: op2.loop_stats(n) for n in
+                          ("save_soln", "res_calc", "save_soln+adt_calc", "res_calc+bres_calc")})
+            op2.op_exit()
+            op2.op_init()
+        assert hists[0] == hists[1], dtype
+        for k in ("q", "qold", "adt", "res"):
+            assert np.array_equal(out[0][k], out[1][k]), (dtype, k)
+        assert stats[0]["res_calc+bres_calc"] is None and stats[1]["res_calc+bres_calc"]
+        assert stats[1]["save_soln+adt_calc"]["calls"] == 4
+    # a deferred save_soln / res_calc is launched before a fetch observes it
+    app = Airfoil(m)
+    app.iterate(1)
+    app._loop(0)                                    # save_soln, deferred
+    q = app.fetch()["q"]
+    assert np.array_equal(app.fetch()["qold"], q)
+    app._loop(1)                                    # adt_calc
+    app._loop(2)                                    # res_calc, deferred
+    r_deferred = app.fetch()["res"]
+    op2.set_option("fuse", 0)
+    app2 = Airfoil(m)
+    app2.iterate(1)
+    for i in (0, 1, 2):
+        app2._loop(i)
+    assert np.array_equal(r_deferred, app2.fetch()["res"])
+
+
+@pytest.mark.parametrize("adt", [6, 8])
+def test_adt_calc_variants_are_bit_identical(op2, adt):
+    """adt_calc under a register cap (6 or 8 CTAs per SM) against the default
+    kernel, in both precisions."""
+    m = M.channel_bump(120, 60, seed=8)
+    for dtype in (np.float64, np.float32):
+        out = []
+        for v in (0, adt):
+            op2.set_option("adt_minblocks", v)
+            app = Airfoil(m, dtype=dtype)
+            app.iterate(3)
+            out.append(app.fetch())
+        for k in ("q", "adt", "res"):
+            assert np.array_equal(out[0][k], out[1][k]), (dtype, k)
+
+
 def test_corner_kernel_falls_back_when_edges_are_not_cell_corners(op2):
     """Corner records need a cell's edges to touch at most four nodes; with
     the edges' node pairs shuffled they touch up to eight, and gather_kernel 6
