@@ -31,6 +31,7 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace op2b {
@@ -59,6 +60,28 @@ bool cuda_ok(cudaError_t e, const char *what) {
   if (e == cudaSuccess) return true;
   set_error("%s: CUDA error %d (%s)", what, (int)e, cudaGetErrorString(e));
   return false;
+}
+
+// memcpy of a large host array by up to 8 threads: copying into freshly
+// allocated memory is bound by its page faults, which the kernel serves in
+// parallel
+static void host_copy(void *dst, const void *src, size_t bytes) {
+  const size_t kParallel = (size_t)8 << 20;
+  unsigned nt = std::min(8u, std::max(1u, std::thread::hardware_concurrency()));
+  if (bytes < kParallel || nt < 2) {
+    memcpy(dst, src, bytes);
+    return;
+  }
+  const size_t chunk = ((bytes + nt - 1) / nt + 4095) & ~(size_t)4095;
+  std::vector<std::thread> th;
+  for (unsigned i = 1; i < nt; i++) {
+    const size_t b = i * chunk;
+    if (b >= bytes) break;
+    const size_t e = std::min(bytes, b + chunk);
+    th.emplace_back([=] { memcpy((char *)dst + b, (const char *)src + b, e - b); });
+  }
+  memcpy(dst, src, std::min(chunk, bytes));
+  for (auto &t : th) t.join();
 }
 
 static char *copy_str(const char *s) {
@@ -378,7 +401,7 @@ op_map op_decl_map(op_set from, op_set to, int dim, int *imap, char const *name)
         cudaFree(map_d);
         return nullptr;
       }
-      memcpy(h, imap, sizeof(int) * n);
+      host_copy(h, imap, sizeof(int) * n);
       if (!cuda_ok(cudaMemcpyAsync(&bad, r.check_d, sizeof(bad), cudaMemcpyDeviceToHost,
                                    r.stream),
                    "op_decl_map: range check") ||

@@ -9,11 +9,12 @@
 //      element maps to both; for a map onto its own set the rows are the
 //      adjacency.  Built with a count / scan / fill / per-row sort+unique.
 //   2. reverse Cuthill-McKee, by one CTA: George-Liu pseudo-peripheral start
-//      (repeated BFS, min-degree vertex of the last level, lowest id on
-//      ties), then BFS levels; a level's new vertices are ordered by
+//      (from a minimum-degree vertex, repeated BFS, min-degree vertex of the
+//      last level, lowest id on ties), then BFS levels; a level's new vertices are ordered by
 //      (position of their first parent in the previous level, degree, id) --
 //      the order sequential Cuthill-McKee produces -- and the whole order is
-//      reversed.  Disconnected graphs continue from the lowest unvisited id.
+//      reversed.  Each connected component starts from an unvisited vertex of
+//      minimum degree (lowest id on ties).
 //   3. propagation to the other sets, in the reference's recursive order over
 //      the declared maps (propagate_reordering, :72-151):
 //      * a map to -> from: elements sorted by the new index of their first
@@ -284,14 +285,31 @@ __global__ void __launch_bounds__(kRcmThreads) k_rcm(RcmWork w) {
   int stamp = 1;
   if (threadIdx.x == 0) s_pos = 0;
   __syncthreads();
-  int scan_from = 0;
   while (s_pos < w.n) {
-    // lowest unvisited vertex
-    if (threadIdx.x == 0) {
-      while (scan_from < w.n && w.newidx[scan_from] >= 0) scan_from++;
-      s_start = scan_from;
+    // an unvisited vertex of minimum degree, lowest id on ties (a corner of a
+    // structured mesh region: usually already pseudo-peripheral, which saves
+    // the pseudo-peripheral search a BFS)
+    {
+      __shared__ unsigned long long s_key[kRcmThreads / 32];
+      unsigned long long best = ~0ull;
+      for (int v = threadIdx.x; v < w.n; v += blockDim.x)
+        if (w.newidx[v] < 0) {
+          const unsigned long long key =
+              ((unsigned long long)(unsigned)w.deg[v] << 32) | (unsigned)v;
+          best = key < best ? key : best;
+        }
+      for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long other = __shfl_down_sync(0xffffffffu, best, o);
+        best = other < best ? other : best;
+      }
+      if ((threadIdx.x & 31) == 0) s_key[threadIdx.x >> 5] = best;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        for (int k = 1; k < (int)(blockDim.x >> 5); k++) best = s_key[k] < best ? s_key[k] : best;
+        s_start = (int)(best & 0xffffffffull);
+      }
+      __syncthreads();
     }
-    __syncthreads();
     int start = s_start;
     // George-Liu pseudo-peripheral vertex
     int *last;
@@ -755,6 +773,23 @@ int renumber(op_map base, long stats[4]) {
             std::chrono::duration<double, std::milli>(now - t_last).count());
     t_last = now;
   };
+  // Reserve the temporaries' memory in the stream-ordered pool with one
+  // allocation: the many allocations below are then carved from it instead of
+  // each asking the driver (whose calls are slow and of uneven cost on a
+  // device shared with other processes).  The estimate covers the graph and
+  // Cuthill-McKee work arrays, the propagation keys and the largest moved row.
+  {
+    size_t nt = (size_t)base->to->size, nf = (size_t)base->from->size, d = (size_t)base->dim;
+    size_t largest = 0;
+    for (auto &dp : r.dats)
+      if (dp) largest = std::max(largest, (size_t)dp->set->size * (size_t)dp->size);
+    for (auto &mp : r.maps)
+      if (mp) largest = std::max(largest, (size_t)mp->from->size * (size_t)mp->dim * sizeof(int));
+    const size_t est = 64 * nt + 4 * nf * d * (d > 1 ? d - 1 : 1) + 32 * nf + largest;
+    void *reserve = nullptr;
+    if (cudaMallocAsync(&reserve, est, s) == cudaSuccess) cudaFreeAsync(reserve, s);
+    else cudaGetLastError();  // no reservation: the allocations below ask one by one
+  }
   long bmx, bavg;
   bandwidth(base, bmx, bavg, s);
   lap("bandwidth before");

@@ -9,8 +9,9 @@
  *  - base order: reverse Cuthill-McKee as the product defines it (the
  *    reference's base order comes from PT-Scotch, an unvendored library, so
  *    this part of the parity is unpinned): George-Liu pseudo-peripheral
- *    start from the lowest unvisited vertex (min-degree vertex of the last
- *    BFS level, lowest id on ties, at most 8 rounds, stop when the
+ *    start from an unvisited vertex of minimum degree, lowest id on ties
+ *    (then the min-degree vertex of the last BFS level, lowest id on ties,
+ *    at most 8 rounds, stop when the
  *    eccentricity stops growing); sequential Cuthill-McKee visiting each
  *    vertex's unvisited neighbours by (degree capped at 63, id); reversed;
  *  - propagation (propagate_reordering, :72-151) in the reference's
@@ -142,10 +143,16 @@ void orc_rcm(int n, const int *row, const int *col, int *perm) {
   int *b = malloc(sizeof(int) * ((size_t)n + 1));
   uint64_t *keys = malloc(sizeof(uint64_t) * ((size_t)n + 1));
   for (int i = 0; i < n; i++) newidx[i] = -1;
-  int pos = 0, stamp = 1, scan = 0;
+  int pos = 0, stamp = 1;
   while (pos < n) {
-    while (scan < n && newidx[scan] >= 0) scan++;
-    int start = scan, *last, last_len;
+    /* an unvisited vertex of minimum degree, lowest id on ties */
+    int start = -1, sd = 0x7fffffff;
+    for (int v = 0; v < n; v++)
+      if (newidx[v] < 0 && row[v + 1] - row[v] < sd) {
+        sd = row[v + 1] - row[v];
+        start = v;
+      }
+    int *last, last_len;
     int ecc = bfs_levels(n, row, col, newidx, mark, stamp++, start, a, b, &last, &last_len);
     for (int round = 0; round < 8; round++) {
       int bd = 0x7fffffff, best = 0x7fffffff;
