@@ -52,7 +52,10 @@ sys.path.insert(0, REPO)
 
 FALLBACK_HBM_GBS = 6650.0
 LOOPS = ("save_soln", "adt_calc", "res_calc", "bres_calc", "update",
-         "save_soln+adt_calc", "res_calc+bres_calc")  # the pairs the runtime fuses
+         # the runtime's fused launches: loop pairs, update computing the next
+         # adt_calc ahead, and the copies that hand its result over
+         "save_soln+adt_calc", "res_calc+bres_calc", "update+adt_calc", "adt_calc(copy)",
+         "save_soln+adt_calc(copy)")
 METRIC = "Airfoil ms/iter (2400x1200 FP64)"
 
 
@@ -316,7 +319,7 @@ def main():
                   {"gather_kernel": 5, "pipe_block": 128}, {"gather_kernel": 5, "pipe_block": 256},
                   {"gather_kernel": 6, "pipe_block": 128}, {"gather_kernel": 6, "pipe_block": 256},
                   {"gather_kernel": 6, "pipe_block": 256, "bres_kernel": 0},
-                  {"fuse": 0}):
+                  {"speculate_adt": 0}, {"fuse": 0, "speculate_adt": 0}):
             v = timed_run(L, Airfoil, m, dtype, "rcm", 3, args.part_size, 20, 3, torch, barrier,
                           opts=o)
             lp = v["loops"]

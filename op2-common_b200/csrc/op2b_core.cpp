@@ -303,6 +303,8 @@ void op_exit(void) {
   r.pending.clear();
   for (auto e : r.ev_free) cudaEventDestroy(e);
   r.ev_free.clear();
+  cudaFree(r.spec.shadow);
+  r.spec = SpecAdt{};
   cudaFree(r.red_base);
   cudaFree(r.check_d);
   r.check_d = nullptr;
@@ -332,6 +334,7 @@ void op_exit(void) {
   r.opt_bres_kernel = d.opt_bres_kernel;
   r.opt_adt_minb = d.opt_adt_minb;
   r.opt_fuse = d.opt_fuse;
+  r.opt_speculate = d.opt_speculate;
   r.pend = PendingLoop{};
   r.opt_pipe_block = d.opt_pipe_block;
   r.opt_pipe_hints = d.opt_pipe_hints;
@@ -491,6 +494,9 @@ op_dat op_decl_dat_temp_char(op_set set, int dim, char const *type, int type_siz
 
 int op_free_dat_temp_char(op_dat dat) {
   Runtime &r = rt();
+  flush_quiet();
+  r.spec = SpecAdt{r.spec.pcell, nullptr, nullptr, nullptr, 0, false, r.spec.shadow,
+                   r.spec.shadow_bytes};  // forget the learned arguments, keep the buffer
   for (auto &d : r.dats)
     if (d.get() == dat) {
       cudaStreamSynchronize(r.stream);
@@ -792,6 +798,7 @@ void op_timing_output(void) {
 int op2b_dat_upload(op_dat dat, const char *src, size_t bytes) {
   Runtime &r = rt();
   if (!r.ready()) return -1;
+  r.spec.ready = false;  // a dat changed outside the loops
   if (!dat || !src || bytes != (size_t)dat->set->size * (size_t)dat->size) {
     set_error("op2b_dat_upload: invalid dat or size");
     return -1;
@@ -805,10 +812,12 @@ int op2b_dat_upload(op_dat dat, const char *src, size_t bytes) {
 
 void *op2b_dat_device_ptr(op_dat dat) {
   flush_quiet();
+  rt().spec.ready = false;  // the caller may write through the pointer
   return dat ? dat->data_d : nullptr;
 }
 void *op2b_map_device_ptr(op_map map) {
   flush_quiet();
+  rt().spec.ready = false;
   return map ? map->map_d : nullptr;
 }
 
@@ -860,6 +869,9 @@ int op2b_set_option(const char *key, long value) {
     r.opt_bres_kernel = (int)value;
   } else if (k == "fuse") {
     r.opt_fuse = value != 0;
+  } else if (k == "speculate_adt") {
+    r.opt_speculate = value != 0;
+    r.spec.ready = false;
   } else if (k == "adt_minblocks") {
     if (value < 0 || value > 8) {
       set_error("op2b_set_option: adt_minblocks must be 0..8");
@@ -893,6 +905,7 @@ long op2b_get_option(const char *key) {
   if (k == "bres_kernel") return r.opt_bres_kernel;
   if (k == "adt_minblocks") return r.opt_adt_minb;
   if (k == "fuse") return r.opt_fuse;
+  if (k == "speculate_adt") return r.opt_speculate;
   if (k == "nsm") return r.nsm;
   return -1;
 }

@@ -119,6 +119,17 @@ template <typename T> AirConst<T> air_consts(bool &ok) {
   return k;
 }
 
+// the constants of a speculative adt equal the current ones
+bool consts_match(const SpecAdt &sp, int rb) {
+  bool ok;
+  if (rb == 8) {
+    AirConst<double> k = air_consts<double>(ok);
+    return ok && memcmp(&k, &sp.kd, sizeof(k)) == 0;
+  }
+  AirConst<float> k = air_consts<float>(ok);
+  return ok && memcmp(&k, &sp.kf, sizeof(k)) == 0;
+}
+
 // Spin until the device publishes `seq` at *flag.  Every few thousand spins
 // the stream is queried so a failed kernel is reported instead of waited
 // for; the wait gives up after 120 s.
@@ -162,6 +173,8 @@ int loop_save_soln(const char *name, op_set set, int nargs, op_arg *a) {
   if (a[0].dat->size != a[1].dat->size) return s.fail(1, "element size differs from argument 0"), -1;
   Runtime &r = rt();
   if (r.pend.kind && !r.flush_pending()) return -1;
+  if (a[1].dat == r.spec.x || a[1].dat == r.spec.q || a[1].dat == r.spec.adt)
+    r.spec.ready = false;  // it overwrites what the speculation read or will replace
   size_t bytes = (size_t)set->size * (size_t)a[0].dat->size;
   int tb = a[0].dat->type ? type_bytes(a[0].dat->type) : 0;
   if (r.opt_fuse && dim == 4 && is_real(a[0].dat->type, tb) && a[0].dat != a[1].dat) {
@@ -199,6 +212,37 @@ int loop_adt_calc(const char *name, op_set set, int nargs, op_arg *a) {
   int C = set->size, N = a[0].dat->set->size;
   double bytes = 16.0 * C + (double)rb * (2.0 * N + 5.0 * C);
   PendingLoop &pd = r.pend;
+  SpecAdt &sp = r.spec;
+  const bool hit = sp.ready && sp.pcell == pcell && sp.x == a[0].dat && sp.q == a[4].dat &&
+                   sp.adt == a[5].dat && sp.rb == rb && consts_match(sp, rb);
+  sp.ready = false;
+  sp.pcell = pcell;  // what the next update may compute ahead
+  sp.x = a[0].dat;
+  sp.q = a[4].dat;
+  sp.adt = a[5].dat;
+  sp.rb = rb;
+  if (hit) {
+    // the update before this call already computed adt from this q: copy it
+    // in (together with a deferred save_soln's q -> qold when there is one)
+    const size_t abytes = ((size_t)C * rb + 255) & ~(size_t)255;
+    cudaError_t e;
+    if (pd.kind == 1 && pd.src == a[4].dat && pd.set == set && pd.dst != a[0].dat &&
+        pd.dst != a[5].dat) {
+      const size_t qbytes = (size_t)C * (size_t)pd.src->size;
+      op_dat qold = pd.dst;
+      pd = PendingLoop{};
+      r.begin_loop("save_soln+adt_calc(copy)");
+      e = launch_copy2(r.ctx(), a[4].dat->data_d, qold->data_d, qbytes, sp.shadow,
+                       a[5].dat->data_d, abytes);
+      r.end_loop(2.0 * (double)qbytes + 2.0 * (double)rb * C);
+    } else {
+      if (pd.kind && !r.flush_pending()) return -1;
+      r.begin_loop("adt_calc(copy)");
+      e = launch_copy(r.ctx(), sp.shadow, a[5].dat->data_d, abytes);
+      r.end_loop(2.0 * (double)rb * C);
+    }
+    return finish(e, name);
+  }
   if (pd.kind == 1 && pd.src == a[4].dat && pd.set == set && pd.rb == rb &&
       pd.dst != a[0].dat && pd.dst != a[5].dat) {
     // save_soln (q -> qold) and this adt_calc in one pass over q: the fused
@@ -395,9 +439,20 @@ int loop_bres_calc(const char *name, op_set set, int nargs, op_arg *a) {
   int B = set->size;
   double bytes = 16.0 * B + (double)rb * (2.0 + 4.0 + 1.0 + 8.0) * B;
   PendingLoop &pd = r.pend;
-  if (pd.kind == 2 && pd.res == a[4].dat && pd.q == a[2].dat && pd.adt == a[3].dat &&
-      pd.x == a[0].dat && pd.rb == rb && r.opt_inc_mode == OP2B_INC_GATHER &&
-      r.opt_bres_kernel == 1) {
+  bool same_consts = false;  // bres_calc would use the constants res_calc was called with
+  if (pd.kind == 2) {
+    bool ok;
+    if (rb == 8) {
+      AirConst<double> k = air_consts<double>(ok);
+      same_consts = ok && memcmp(&k, &pd.kd, sizeof(k)) == 0;
+    } else {
+      AirConst<float> k = air_consts<float>(ok);
+      same_consts = ok && memcmp(&k, &pd.kf, sizeof(k)) == 0;
+    }
+  }
+  if (pd.kind == 2 && same_consts && pd.res == a[4].dat && pd.q == a[2].dat &&
+      pd.adt == a[3].dat && pd.x == a[0].dat && pd.rb == rb &&
+      r.opt_inc_mode == OP2B_INC_GATHER && r.opt_bres_kernel == 1) {
     const SlotRecords *cr = get_corner_records(pd.pecell, pd.pedge);
     const BresRecords *br = cr ? get_bres_records(pbecell, pbedge) : nullptr;
     if (cr && br && link_boundary_records(cr, br, pbecell)) {
@@ -498,17 +553,47 @@ int loop_update(const char *name, op_set set, int nargs, op_arg *a) {
   int C = set->size;
   double bytes = (double)rb * 17.0 * C;
   r.red.seq = ++r.red_seq;
-  r.begin_loop(name);
+  // speculation: this update's q is the q the last adt_calc read, and adt
+  // is what it wrote -- compute the next adt_calc's result now, into the
+  // shadow buffer, in the same pass over the cells
+  SpecAdt &sp = r.spec;
+  sp.ready = false;
+  bool spec = r.opt_speculate && sp.pcell && sp.q == a[1].dat && sp.adt == a[3].dat &&
+              sp.rb == rb && sp.pcell->from == set && sp.x && sp.pcell->to == sp.x->set;
+  const size_t abytes = ((size_t)C * rb + 255) & ~(size_t)255;
+  if (spec && sp.shadow_bytes < abytes) {
+    cudaFree(sp.shadow);
+    sp.shadow = nullptr;
+    sp.shadow_bytes = 0;
+    if (cudaMalloc(&sp.shadow, abytes) == cudaSuccess) sp.shadow_bytes = abytes;
+    else spec = false, cudaGetLastError();
+  }
+  bool ok = true;
+  if (spec) {
+    if (rb == 8) sp.kd = air_consts<double>(ok);
+    else sp.kf = air_consts<float>(ok);
+    spec = ok;
+  }
+  const int N = spec ? sp.x->set->size : 0;
+  r.begin_loop(spec ? "update+adt_calc" : name);
   cudaError_t e;
   if (rb == 8)
     e = launch_update<double>(r.ctx(), C, (const double *)a[0].dat->data_d,
                               (double *)a[1].dat->data_d, (double *)a[2].dat->data_d,
-                              (const double *)a[3].dat->data_d, r.red);
+                              (const double *)a[3].dat->data_d, r.red,
+                              spec ? sp.pcell->map_d : nullptr,
+                              spec ? (const double *)sp.x->data_d : nullptr,
+                              spec ? (double *)sp.shadow : nullptr, &sp.kd);
   else
     e = launch_update<float>(r.ctx(), C, (const float *)a[0].dat->data_d,
                              (float *)a[1].dat->data_d, (float *)a[2].dat->data_d,
-                             (const float *)a[3].dat->data_d, r.red);
-  r.end_loop(bytes);
+                             (const float *)a[3].dat->data_d, r.red,
+                             spec ? sp.pcell->map_d : nullptr,
+                             spec ? (const float *)sp.x->data_d : nullptr,
+                             spec ? (float *)sp.shadow : nullptr, &sp.kf);
+  // with the speculation the pass also reads pcell and x and writes adt
+  r.end_loop(spec ? bytes + 16.0 * C + (double)rb * (2.0 * N + C) : bytes);
+  sp.ready = spec && e == cudaSuccess;
   if (finish(e, name)) return -1;
   // gbl results are valid when op_par_loop returns: the kernel's last block
   // publishes them in the mapped page, sequence number last

@@ -44,6 +44,22 @@ struct PendingLoop {
   AirConst<float> kf{};
 };
 
+// Speculative adt_calc: update also computes the time step of its new q into
+// `shadow`, for the adt_calc (over the last adt_calc's arguments) that
+// usually follows.  That adt_calc copies the shadow into adt instead of
+// recomputing it when `ready` still holds: nothing changed q, x, the map or
+// the constants in between.  adt itself keeps its old values until then.
+struct SpecAdt {
+  op_map pcell = nullptr;                               // the last adt_calc's arguments
+  op_dat x = nullptr, q = nullptr, adt = nullptr;
+  int rb = 0;
+  bool ready = false;      // shadow = adt of q as the last update left it
+  void *shadow = nullptr;  // device buffer of adt's allocation size
+  size_t shadow_bytes = 0;
+  AirConst<double> kd{};   // constants the shadow was computed with
+  AirConst<float> kf{};
+};
+
 struct Runtime {
   bool initialised = false;
   int device = 0, nsm = 148, cc_major = 0, cc_minor = 0;
@@ -63,6 +79,7 @@ struct Runtime {
   int opt_gather_minb = 0;    // __launch_bounds__ minimum blocks of the gather kernels
   int opt_bres_kernel = 1;    // bres_calc gather: 0 = inverse-map walk, 1 = boundary records
   int opt_fuse = 1;           // defer save_soln / res_calc to fuse them with the next loop
+  int opt_speculate = 1;      // update also computes the next adt_calc's result (SpecAdt)
   int opt_adt_minb = 0;       // adt_calc: __launch_bounds__ minimum blocks (0 = none)
   int opt_pipe_block = 256;   // threads per CTA of the pipelined gather (64, 96, 128, 256)
   int opt_pipe_hints = 0;     // register pipeline: evict-first hints on once-read streams
@@ -91,6 +108,7 @@ struct Runtime {
   cudaEvent_t cur_ev0 = nullptr, cur_ev1 = nullptr;
 
   PendingLoop pend;
+  SpecAdt spec;
 
   LaunchCtx ctx();
   // initialised, with any deferred loop launched (false on error)

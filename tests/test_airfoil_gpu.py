@@ -184,6 +184,69 @@ def test_pipelined_kernels_are_bit_identical(op2, hints):
             assert np.array_equal(out[0][k], o[k]), k
 
 
+@pytest.mark.parametrize("fuse", [0, 1])
+def test_speculative_adt_is_bit_identical(op2, fuse):
+    """update computing the next adt_calc's result ahead (speculate_adt) gives
+    the same q, qold, adt, res and history as recomputing it, in both
+    precisions, with and without loop fusion."""
+    m = M.channel_bump(96, 48, seed=13)
+    for dtype in (np.float64, np.float32):
+        out, hists, stats = [], [], []
+        for spec in (0, 1):
+            op2.set_option("fuse", fuse)
+            op2.set_option("speculate_adt", spec)
+            app = Airfoil(m, dtype=dtype)
+            hists.append(app.iterate(5))
+            out.append(app.fetch())
+            stats.append(op2.loop_stats("update+adt_calc"))
+            op2.op_exit()
+            op2.op_init()
+        assert hists[0] == hists[1], dtype
+        for k in ("q", "qold", "adt", "res"):
+            assert np.array_equal(out[0][k], out[1][k]), (dtype, k)
+        assert stats[0] is None and stats[1]["calls"] == 10  # every update follows an adt_calc
+
+
+def test_speculative_adt_is_invisible_and_invalidated(op2):
+    """Between update and adt_calc the adt dat keeps its old values; a q
+    uploaded, or a constant changed, in between makes adt_calc recompute."""
+    m = M.channel_bump(64, 32, seed=14)
+    c = M.airfoil_constants()
+
+    def run(spec, between):
+        op2.set_option("speculate_adt", spec)
+        app = Airfoil(m, c)
+        app.iterate(1)
+        for i in (1, 2, 3, 4):        # adt_calc, res_calc, bres_calc, update
+            app._loop(i)
+        seen = app.fetch()["adt"]     # before the next adt_calc
+        between(app)
+        app._loop(1)
+        got = app.fetch()["adt"]
+        op2.op_exit()
+        op2.op_init()
+        return seen, got
+
+    def nothing(app):
+        pass
+
+    def upload(app):
+        q = app.fetch()["q"] * 1.01
+        a = np.ascontiguousarray(q)
+        assert op2.load().op2b_dat_upload(app.p_q, a.ctypes.data, a.nbytes) == 0
+
+    def new_cfl(app):
+        op2.op_decl_const(1, "double", 0.8, "cfl")
+
+    for between in (nothing, upload, new_cfl):
+        s0, g0 = run(0, between)
+        s1, g1 = run(1, between)
+        assert np.array_equal(s0, s1), between.__name__
+        assert np.array_equal(g0, g1), between.__name__
+        if between is not nothing:
+            assert not np.array_equal(g1, run(1, nothing)[1]), between.__name__
+
+
 def test_fused_loop_pairs_are_bit_identical_to_separate_loops(op2):
     """The runtime defers save_soln and res_calc and fuses them with the
     adt_calc / bres_calc that follow; with fusion off every loop launches on
@@ -194,6 +257,7 @@ def test_fused_loop_pairs_are_bit_identical_to_separate_loops(op2):
         out, hists, stats = [], [], []
         for fuse in (0, 1):
             op2.set_option("fuse", fuse)
+            op2.set_option("speculate_adt", 0)  # every adt_calc computed, fused or not
             op2.load().op2b_reset_stats()
             app = Airfoil(m, dtype=dtype)
             hists.append(app.iterate(4))
@@ -208,6 +272,7 @@ def test_fused_loop_pairs_are_bit_identical_to_separate_loops(op2):
         assert stats[0]["res_calc+bres_calc"] is None and stats[1]["res_calc+bres_calc"]
         assert stats[1]["save_soln+adt_calc"]["calls"] == 4
     # a deferred save_soln / res_calc is launched before a fetch observes it
+    op2.set_option("speculate_adt", 0)
     app = Airfoil(m)
     app.iterate(1)
     app._loop(0)                                    # save_soln, deferred
