@@ -53,9 +53,8 @@ sys.path.insert(0, REPO)
 FALLBACK_HBM_GBS = 6650.0
 LOOPS = ("save_soln", "adt_calc", "res_calc", "bres_calc", "update",
          # the runtime's fused launches: loop pairs, update computing the next
-         # adt_calc ahead, and the copies that hand its result over
-         "save_soln+adt_calc", "res_calc+bres_calc", "update+adt_calc", "adt_calc(copy)",
-         "save_soln+adt_calc(copy)")
+         # adt_calc ahead (and putting adt back when another call came first)
+         "save_soln+adt_calc", "res_calc+bres_calc", "update+adt_calc", "adt restore")
 METRIC = "Airfoil ms/iter (2400x1200 FP64)"
 
 

@@ -200,7 +200,9 @@ int op2b_status(void);
 /* Upload host data into an existing dat (op_upload_dat of
  * op2/include/op_lib_core.h:349 with the data supplied by the caller). */
 int op2b_dat_upload(op_dat dat, const char *src, size_t bytes);
-/* Device pointer of a dat / map (for interop; plain device addresses). */
+/* Device pointer of a dat / map (for interop; plain device addresses).  Any
+ * deferred loop is launched first, and the runtime no longer computes ahead
+ * (speculate_adt) into a dat whose pointer was handed out. */
 void *op2b_dat_device_ptr(op_dat dat);
 void *op2b_map_device_ptr(op_map map);
 

@@ -57,43 +57,6 @@ __global__ void k_copy_tail(const unsigned char *src, unsigned char *dst, long l
   if (i < n) dst[i] = src[i];
 }
 
-// Two independent 16-byte-vector copies in one grid (the first n1 chunks copy
-// src1 -> dst1, the rest src2 -> dst2), four loads in flight per thread.
-__global__ void __launch_bounds__(256) k_copy2(const uint4 *__restrict__ src1,
-                                               uint4 *__restrict__ dst1, long long n1,
-                                               const uint4 *__restrict__ src2,
-                                               uint4 *__restrict__ dst2, long long n2) {
-  const long long stride = (long long)gridDim.x * blockDim.x, n = n1 + n2;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += 4 * stride) {
-    uint4 v[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      const long long j = i + k * stride;
-      if (j < n) v[k] = j < n1 ? __ldcs(src1 + j) : __ldcs(src2 + (j - n1));
-    }
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      const long long j = i + k * stride;
-      if (j < n) {
-        if (j < n1) __stcs(dst1 + j, v[k]);
-        else __stcs(dst2 + (j - n1), v[k]);
-      }
-    }
-  }
-}
-
-// both sizes multiples of 16 bytes
-cudaError_t launch_copy2(const LaunchCtx &c, const void *src1, void *dst1, size_t bytes1,
-                         const void *src2, void *dst2, size_t bytes2) {
-  const long long n1 = (long long)(bytes1 / 16), n2 = (long long)(bytes2 / 16);
-  if (n1 + n2 == 0) return cudaSuccess;
-  k_copy2<<<grid_for(c, n1 + n2, 256, 8), 256, 0, c.stream>>>(
-      static_cast<const uint4 *>(src1), static_cast<uint4 *>(dst1), n1,
-      static_cast<const uint4 *>(src2), static_cast<uint4 *>(dst2), n2);
-  c.count();
-  return cudaGetLastError();
-}
-
 cudaError_t launch_copy(const LaunchCtx &c, const void *src, void *dst, size_t bytes) {
   long long n16 = (long long)(bytes / 16);
   if (n16 > 0) {
@@ -335,20 +298,21 @@ __device__ __forceinline__ RedTriple block_reduce(RedTriple t) {
 // arrive reduces all partials in block order and writes `out`.
 // With ADT the kernel also computes, from each cell's new q, the time step
 // that the following adt_calc computes (same arithmetic on the same stored q
-// values) into adt_next, a buffer of the runtime's: the runtime hands it to
-// that adt_calc when nothing changed q, x or the map in between (option
-// speculate_adt).
+// values) and writes it into adt itself, after saving the old adt into
+// `backup`, a buffer of the runtime's (option speculate_adt).  Each cell's
+// adt is read and written by the same thread only.
 template <typename T> struct AdtNext {
   const int4 *pcell;
   const T *x;
-  T *out;
+  T *adt;      // the adt dat (the update's own adt argument), written in place
+  T *backup;   // receives the old adt
   AirConst<T> k;
 };
 
 template <typename T, int THREADS, bool ADT>
 __global__ void __launch_bounds__(THREADS)
 k_update(int ncell, const T *__restrict__ qold, T *__restrict__ q, T *__restrict__ res,
-         const T *__restrict__ adt, RedSlot *__restrict__ parts, unsigned *__restrict__ counter,
+         const T *adt, RedSlot *__restrict__ parts, unsigned *__restrict__ counter,
          RedSlot *__restrict__ out, RedSlot *host_out, long long seq, AdtNext<T> an) {
   RedTriple t{0.0, -INFINITY, LLONG_MAX};
   int stride = gridDim.x * THREADS;
@@ -364,7 +328,14 @@ k_update(int ncell, const T *__restrict__ qold, T *__restrict__ q, T *__restrict
     }
     Vec<T>::ld4(qold + 4 * (size_t)n, qo);
     Vec<T>::ld4_rw(res + 4 * (size_t)n, r);
-    double adti = 1.0f / (double)__ldg(adt + n);
+    T a_old;
+    if constexpr (ADT) {
+      a_old = adt[n];  // coherent load: this kernel rewrites adt
+      an.backup[n] = a_old;
+    } else {
+      a_old = __ldg(adt + n);
+    }
+    double adti = 1.0f / (double)a_old;
 #pragma unroll
     for (int m = 0; m < 4; m++) {
       double del = adti * (double)r[m];
@@ -380,7 +351,7 @@ k_update(int ncell, const T *__restrict__ qold, T *__restrict__ q, T *__restrict
     T z[4] = {(T)0, (T)0, (T)0, (T)0};
     Vec<T>::st4(res + 4 * (size_t)n, z);
     if constexpr (ADT)
-      an.out[n] = air_adt<T>(x1x, x1y, x2x, x2y, x3x, x3y, x4x, x4y, qn[0], qn[1], qn[2],
+      an.adt[n] = air_adt<T>(x1x, x1y, x2x, x2y, x3x, x3y, x4x, x4y, qn[0], qn[1], qn[2],
                              qn[3], an.k);
   }
   t = block_reduce<THREADS>(t);
@@ -417,12 +388,13 @@ k_update(int ncell, const T *__restrict__ qold, T *__restrict__ q, T *__restrict
 template <typename T>
 cudaError_t launch_update(const LaunchCtx &c, int ncell, const T *qold, T *q, T *res,
                           const T *adt, const RedScratch &s, const int *pcell, const T *x,
-                          T *adt_next, const AirConst<T> *k) {
+                          T *adt_backup, const AirConst<T> *k) {
   constexpr int TH = 256;
   int grid = grid_for(c, ncell, TH, 4);
   if (grid > s.capacity) grid = s.capacity;
-  if (adt_next) {
-    const AdtNext<T> an{reinterpret_cast<const int4 *>(pcell), x, adt_next, *k};
+  if (adt_backup) {
+    const AdtNext<T> an{reinterpret_cast<const int4 *>(pcell), x, const_cast<T *>(adt),
+                        adt_backup, *k};
     k_update<T, TH, true><<<grid, TH, 0, c.stream>>>(ncell, qold, q, res, adt, s.parts,
                                                      s.counter, s.out, s.host_out, s.seq, an);
   } else {

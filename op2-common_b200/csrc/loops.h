@@ -40,9 +40,6 @@ struct RedScratch {
 };
 
 cudaError_t launch_copy(const LaunchCtx &c, const void *src, void *dst, size_t bytes);
-// two copies in one launch; both sizes multiples of 16 bytes
-cudaError_t launch_copy2(const LaunchCtx &c, const void *src1, void *dst1, size_t bytes1,
-                         const void *src2, void *dst2, size_t bytes2);
 
 // map_check.cu: *first_bad = lowest i with map[i] outside [0, nto); the
 // caller initialises it to ~0ull
@@ -66,12 +63,13 @@ template <typename T>
 cudaError_t launch_bres_calc_atomic(const LaunchCtx &c, int nbedge, const int *pbedge,
                                     const int *pbecell, const int *bound, const T *x,
                                     const T *q, const T *adt, T *res, const AirConst<T> &k);
-// adt_next (optional): also each cell's time step from its new q, pcell and
-// x with constants k, as adt_calc computes it
+// adt_backup (optional): also each cell's time step from its new q, pcell and
+// x with constants k, as adt_calc computes it, written into adt after the old
+// adt is saved into adt_backup
 template <typename T>
 cudaError_t launch_update(const LaunchCtx &c, int ncell, const T *qold, T *q, T *res,
                           const T *adt, const RedScratch &s, const int *pcell = nullptr,
-                          const T *x = nullptr, T *adt_next = nullptr,
+                          const T *x = nullptr, T *adt_backup = nullptr,
                           const AirConst<T> *k = nullptr);
 
 }  // namespace op2b

@@ -116,9 +116,12 @@ bool is_real(const char *type, int bytes) {
 LaunchCtx Runtime::ctx() { return LaunchCtx{stream, nsm, &launches}; }
 
 // launch a deferred loop before a call that observes the library's state
-static void flush_quiet() {
+// (restore: also put adt back if an update wrote it early -- for calls that
+// hand out access to the data; bookkeeping calls only launch deferred loops)
+static void flush_quiet(bool restore = true) {
   Runtime &r = rt();
   if (r.initialised && r.pend.kind) r.flush_pending();
+  if (restore && r.initialised && r.spec.inplace) r.restore_spec();
 }
 
 bool Runtime::ready() {
@@ -126,7 +129,7 @@ bool Runtime::ready() {
     set_error("op_init has not been called");
     return false;
   }
-  return pend.kind == 0 || flush_pending();
+  return (pend.kind == 0 || flush_pending()) && (!spec.inplace || restore_spec());
 }
 
 // ------------------------------------------------------------------ timing
@@ -317,6 +320,7 @@ void op_exit(void) {
   r.pinned = nullptr;
   r.stream = r.own_stream = nullptr;
   r.stats.clear();
+  r.exposed.clear();
   r.launches = 0;
   r.initialised = false;
   // options return to their defaults: a later op_init starts from a clean state
@@ -495,8 +499,9 @@ op_dat op_decl_dat_temp_char(op_set set, int dim, char const *type, int type_siz
 int op_free_dat_temp_char(op_dat dat) {
   Runtime &r = rt();
   flush_quiet();
-  r.spec = SpecAdt{r.spec.pcell, nullptr, nullptr, nullptr, 0, false, r.spec.shadow,
-                   r.spec.shadow_bytes};  // forget the learned arguments, keep the buffer
+  // forget the learned arguments (flush_quiet put adt back), keep the buffer
+  r.spec = SpecAdt{nullptr, nullptr, nullptr, nullptr, 0, false, r.spec.shadow,
+                   r.spec.shadow_bytes};
   for (auto &d : r.dats)
     if (d.get() == dat) {
       cudaStreamSynchronize(r.stream);
@@ -777,7 +782,7 @@ void op_diagnostic_output(void) {
 // GB/s uses each loop's algorithmic bytes per call.
 void op_timing_output(void) {
   Runtime &r = rt();
-  flush_quiet();
+  flush_quiet(false);
   r.resolve_timing();
   std::vector<std::pair<std::string, LoopStat>> v(r.stats.begin(), r.stats.end());
   std::sort(v.begin(), v.end(),
@@ -798,7 +803,6 @@ void op_timing_output(void) {
 int op2b_dat_upload(op_dat dat, const char *src, size_t bytes) {
   Runtime &r = rt();
   if (!r.ready()) return -1;
-  r.spec.ready = false;  // a dat changed outside the loops
   if (!dat || !src || bytes != (size_t)dat->set->size * (size_t)dat->size) {
     set_error("op2b_dat_upload: invalid dat or size");
     return -1;
@@ -812,18 +816,20 @@ int op2b_dat_upload(op_dat dat, const char *src, size_t bytes) {
 
 void *op2b_dat_device_ptr(op_dat dat) {
   flush_quiet();
-  rt().spec.ready = false;  // the caller may write through the pointer
+  // the caller may read or write through the pointer at any later time: no
+  // speculation on this dat from now on
+  if (dat) rt().exposed.insert(dat);
   return dat ? dat->data_d : nullptr;
 }
 void *op2b_map_device_ptr(op_map map) {
   flush_quiet();
-  rt().spec.ready = false;
   return map ? map->map_d : nullptr;
 }
 
 int op2b_set_option(const char *key, long value) {
   Runtime &r = rt();
   if (r.initialised && r.pend.kind && !r.flush_pending()) return -1;
+  if (r.initialised && r.spec.inplace && !r.restore_spec()) return -1;
   std::string k = key ? key : "";
   if (k == "inc_mode") {
     if (value < 0 || value > 3) {
@@ -871,7 +877,6 @@ int op2b_set_option(const char *key, long value) {
     r.opt_fuse = value != 0;
   } else if (k == "speculate_adt") {
     r.opt_speculate = value != 0;
-    r.spec.ready = false;
   } else if (k == "adt_minblocks") {
     if (value < 0 || value > 8) {
       set_error("op2b_set_option: adt_minblocks must be 0..8");
@@ -913,7 +918,7 @@ long op2b_get_option(const char *key) {
 int op2b_loop_stats(const char *name, double *total_ms, long *calls, double *bytes_per_call,
                     double *last_ms) {
   Runtime &r = rt();
-  flush_quiet();
+  flush_quiet(false);
   r.resolve_timing();
   auto it = r.stats.find(name ? name : "");
   if (it == r.stats.end()) return -1;
@@ -926,7 +931,7 @@ int op2b_loop_stats(const char *name, double *total_ms, long *calls, double *byt
 
 void op2b_reset_stats(void) {
   Runtime &r = rt();
-  flush_quiet();
+  flush_quiet(false);
   r.resolve_timing();
   for (auto &kv : r.stats) {
     double plan = kv.second.plan_ms;
@@ -936,7 +941,7 @@ void op2b_reset_stats(void) {
 }
 
 long op2b_kernel_launches(void) {
-  flush_quiet();
+  flush_quiet(false);
   return rt().launches;
 }
 
@@ -949,13 +954,17 @@ int op2b_set_stream(void *stream) {
 }
 
 void *op2b_get_stream(void) {
-  flush_quiet();
+  flush_quiet(false);
   return (void *)rt().stream;
 }
 
 int op2b_synchronize(void) {
   Runtime &r = rt();
-  if (!r.ready()) return -1;
+  if (!r.initialised) {
+    set_error("op_init has not been called");
+    return -1;
+  }
+  flush_quiet(false);  // waiting observes no dat
   cudaError_t e = cudaStreamSynchronize(r.stream);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) cuda_ok(e, "op2b_synchronize");

@@ -173,8 +173,10 @@ int loop_save_soln(const char *name, op_set set, int nargs, op_arg *a) {
   if (a[0].dat->size != a[1].dat->size) return s.fail(1, "element size differs from argument 0"), -1;
   Runtime &r = rt();
   if (r.pend.kind && !r.flush_pending()) return -1;
-  if (a[1].dat == r.spec.x || a[1].dat == r.spec.q || a[1].dat == r.spec.adt)
-    r.spec.ready = false;  // it overwrites what the speculation read or will replace
+  if (r.spec.inplace && (a[1].dat == r.spec.x || a[1].dat == r.spec.q ||
+                         a[1].dat == r.spec.adt || a[0].dat == r.spec.adt) &&
+      !r.restore_spec())
+    return -1;
   size_t bytes = (size_t)set->size * (size_t)a[0].dat->size;
   int tb = a[0].dat->type ? type_bytes(a[0].dat->type) : 0;
   if (r.opt_fuse && dim == 4 && is_real(a[0].dat->type, tb) && a[0].dat != a[1].dat) {
@@ -213,36 +215,20 @@ int loop_adt_calc(const char *name, op_set set, int nargs, op_arg *a) {
   double bytes = 16.0 * C + (double)rb * (2.0 * N + 5.0 * C);
   PendingLoop &pd = r.pend;
   SpecAdt &sp = r.spec;
-  const bool hit = sp.ready && sp.pcell == pcell && sp.x == a[0].dat && sp.q == a[4].dat &&
+  const bool hit = sp.inplace && sp.pcell == pcell && sp.x == a[0].dat && sp.q == a[4].dat &&
                    sp.adt == a[5].dat && sp.rb == rb && consts_match(sp, rb);
-  sp.ready = false;
+  if (hit) {
+    // the update before this call already wrote this adt_calc's result
+    sp.inplace = false;
+    r.count_call("adt_calc(in update)");
+    return 0;
+  }
+  if (sp.inplace && !r.restore_spec()) return -1;
   sp.pcell = pcell;  // what the next update may compute ahead
   sp.x = a[0].dat;
   sp.q = a[4].dat;
   sp.adt = a[5].dat;
   sp.rb = rb;
-  if (hit) {
-    // the update before this call already computed adt from this q: copy it
-    // in (together with a deferred save_soln's q -> qold when there is one)
-    const size_t abytes = ((size_t)C * rb + 255) & ~(size_t)255;
-    cudaError_t e;
-    if (pd.kind == 1 && pd.src == a[4].dat && pd.set == set && pd.dst != a[0].dat &&
-        pd.dst != a[5].dat) {
-      const size_t qbytes = (size_t)C * (size_t)pd.src->size;
-      op_dat qold = pd.dst;
-      pd = PendingLoop{};
-      r.begin_loop("save_soln+adt_calc(copy)");
-      e = launch_copy2(r.ctx(), a[4].dat->data_d, qold->data_d, qbytes, sp.shadow,
-                       a[5].dat->data_d, abytes);
-      r.end_loop(2.0 * (double)qbytes + 2.0 * (double)rb * C);
-    } else {
-      if (pd.kind && !r.flush_pending()) return -1;
-      r.begin_loop("adt_calc(copy)");
-      e = launch_copy(r.ctx(), sp.shadow, a[5].dat->data_d, abytes);
-      r.end_loop(2.0 * (double)rb * C);
-    }
-    return finish(e, name);
-  }
   if (pd.kind == 1 && pd.src == a[4].dat && pd.set == set && pd.rb == rb &&
       pd.dst != a[0].dat && pd.dst != a[5].dat) {
     // save_soln (q -> qold) and this adt_calc in one pass over q: the fused
@@ -337,6 +323,7 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
   if (!s.ok) return -1;
   Runtime &r = rt();
   if (r.pend.kind && !r.flush_pending()) return -1;
+  if (r.spec.inplace && !r.restore_spec()) return -1;
   int E = set->size, N = a[0].dat->set->size, C = a[2].dat->set->size;
   double bytes = 16.0 * E + (double)rb * (2.0 * N + 13.0 * C);
   if (r.opt_fuse && r.opt_inc_mode == OP2B_INC_GATHER &&
@@ -436,6 +423,7 @@ int loop_bres_calc(const char *name, op_set set, int nargs, op_arg *a) {
   int rb = s.real_bytes({0, 2, 3, 4});
   if (!s.ok) return -1;
   Runtime &r = rt();
+  if (r.spec.inplace && !r.restore_spec()) return -1;
   int B = set->size;
   double bytes = 16.0 * B + (double)rb * (2.0 + 4.0 + 1.0 + 8.0) * B;
   PendingLoop &pd = r.pend;
@@ -557,9 +545,10 @@ int loop_update(const char *name, op_set set, int nargs, op_arg *a) {
   // is what it wrote -- compute the next adt_calc's result now, into the
   // shadow buffer, in the same pass over the cells
   SpecAdt &sp = r.spec;
-  sp.ready = false;
+  if (sp.inplace && !r.restore_spec()) return -1;  // update reads the program's adt
   bool spec = r.opt_speculate && sp.pcell && sp.q == a[1].dat && sp.adt == a[3].dat &&
-              sp.rb == rb && sp.pcell->from == set && sp.x && sp.pcell->to == sp.x->set;
+              sp.rb == rb && sp.pcell->from == set && sp.x && sp.pcell->to == sp.x->set &&
+              !r.exposed.count(sp.x) && !r.exposed.count(sp.q) && !r.exposed.count(sp.adt);
   const size_t abytes = ((size_t)C * rb + 255) & ~(size_t)255;
   if (spec && sp.shadow_bytes < abytes) {
     cudaFree(sp.shadow);
@@ -593,7 +582,7 @@ int loop_update(const char *name, op_set set, int nargs, op_arg *a) {
                              spec ? (float *)sp.shadow : nullptr, &sp.kf);
   // with the speculation the pass also reads pcell and x and writes adt
   r.end_loop(spec ? bytes + 16.0 * C + (double)rb * (2.0 * N + C) : bytes);
-  sp.ready = spec && e == cudaSuccess;
+  sp.inplace = spec && e == cudaSuccess;
   if (finish(e, name)) return -1;
   // gbl results are valid when op_par_loop returns: the kernel's last block
   // publishes them in the mapped page, sequence number last
@@ -626,6 +615,18 @@ const Entry kLoops[] = {{"save_soln", loop_save_soln},
 
 // Launch the deferred loop on its own (the calls it could have been fused
 // with did not follow).  Errors are reported by the call that triggered it.
+// Put the program's adt back: the update before wrote the next adt_calc's
+// result into adt early, and something other than that adt_calc came first.
+bool op2b::Runtime::restore_spec() {
+  if (!spec.inplace) return true;
+  spec.inplace = false;
+  const size_t bytes = ((size_t)spec.adt->set->size * (size_t)spec.rb + 255) & ~(size_t)255;
+  begin_loop("adt restore");
+  cudaError_t e = launch_copy(ctx(), spec.shadow, spec.adt->data_d, bytes);
+  end_loop(2.0 * (double)bytes);
+  return finish(e, "adt restore") == 0;
+}
+
 bool op2b::Runtime::flush_pending() {
   PendingLoop pd = pend;
   pend = PendingLoop{};
@@ -674,6 +675,7 @@ int op_par_loop_c(char const *name, op_set set, int nargs, op_arg *args) {
   for (const Entry &e : kLoops)
     if (strcmp(e.name, name) == 0) return e.fn(name, set, nargs, args);
   if (r.pend.kind) r.flush_pending();
+  if (r.spec.inplace) r.restore_spec();
   set_error("op_par_loop(%s): no device implementation of this loop is registered "
             "(libop2b runs loops on the GPU only)",
             name);

@@ -5,6 +5,7 @@
 
 #include <map>
 #include <memory>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -44,19 +45,21 @@ struct PendingLoop {
   AirConst<float> kf{};
 };
 
-// Speculative adt_calc: update also computes the time step of its new q into
-// `shadow`, for the adt_calc (over the last adt_calc's arguments) that
-// usually follows.  That adt_calc copies the shadow into adt instead of
-// recomputing it when `ready` still holds: nothing changed q, x, the map or
-// the constants in between.  adt itself keeps its old values until then.
+// Speculative adt_calc: update also computes, for the adt_calc that usually
+// follows it (over the last adt_calc's arguments), the time step of its new q
+// and writes it into adt, after saving the old adt into `shadow`.  While
+// `inplace` holds, adt is ahead of the program: the matching adt_calc then
+// has nothing left to do, and any other call that could read adt first
+// restores it from the shadow (restore_spec), so nothing observes the early
+// values.
 struct SpecAdt {
   op_map pcell = nullptr;                               // the last adt_calc's arguments
   op_dat x = nullptr, q = nullptr, adt = nullptr;
   int rb = 0;
-  bool ready = false;      // shadow = adt of q as the last update left it
+  bool inplace = false;    // adt holds the next adt_calc's result, shadow the old adt
   void *shadow = nullptr;  // device buffer of adt's allocation size
   size_t shadow_bytes = 0;
-  AirConst<double> kd{};   // constants the shadow was computed with
+  AirConst<double> kd{};   // constants the early adt was computed with
   AirConst<float> kf{};
 };
 
@@ -109,12 +112,15 @@ struct Runtime {
 
   PendingLoop pend;
   SpecAdt spec;
+  std::set<op_dat> exposed;  // dats whose device pointer was handed out (no speculation)
 
   LaunchCtx ctx();
   // initialised, with any deferred loop launched (false on error)
   bool ready();
   bool flush_pending();  // op2b_dispatch.cpp
+  bool restore_spec();   // op2b_dispatch.cpp: put the old adt back if adt is ahead
   void begin_loop(const char *name);
+  void count_call(const char *name) { stats[name].calls++; }  // a call with no launch
   void end_loop(double bytes);
   void resolve_timing();
   const double *const_ptr(const char *name, int dim);

@@ -881,7 +881,6 @@ int renumber(op_map base, long stats[4]) {
     }
   }
   lap("host maps, composition");
-  r.spec.ready = false;  // q, x and the maps moved
   release_plans();  // plans and inverse maps refer to the old numbering
   release_inverse_maps();
   bool good = cuda_ok(cudaStreamSynchronize(s), "op_renumber") && ok;

@@ -247,6 +247,24 @@ def test_speculative_adt_is_invisible_and_invalidated(op2):
             assert not np.array_equal(g1, run(1, nothing)[1]), between.__name__
 
 
+def test_speculative_adt_restored_for_other_readers(op2):
+    """A loop that reads adt right after update (res_calc without the
+    adt_calc in between) sees the program's adt, not the early one."""
+    m = M.channel_bump(64, 32, seed=15)
+    res = []
+    for spec in (0, 1):
+        op2.set_option("speculate_adt", spec)
+        app = Airfoil(m)
+        app.iterate(1)
+        for i in (1, 2, 3, 4, 2, 3):   # ..., update, then res_calc and bres_calc again
+            app._loop(i)
+        res.append(app.fetch())
+        op2.op_exit()
+        op2.op_init()
+    for k in ("res", "adt", "q"):
+        assert np.array_equal(res[0][k], res[1][k]), k
+
+
 def test_fused_loop_pairs_are_bit_identical_to_separate_loops(op2):
     """The runtime defers save_soln and res_calc and fuses them with the
     adt_calc / bres_calc that follow; with fusion off every loop launches on
