@@ -16,8 +16,9 @@ max over ranks.  Prints one JSON line on rank 0.
              than the 126 MB L2, so no flush is needed between iterations.
              Default configuration: the mesh renumbered on the GPU
              (op_renumber, reverse Cuthill-McKee), owner-computes increments
-             over corner records, and the runtime's loop fusion (save_soln
-             into adt_calc, res_calc with bres_calc).
+             over corner records, the runtime's loop fusion (save_soln
+             into adt_calc, res_calc with bres_calc) and its speculative
+             adt_calc (computed by the update before it).
 * loops      per loop (or fused loop pair) device time, algorithmic bytes per
              call and GB/s.
 * e2e        the whole 1000-iteration job (the configuration's length) through
