@@ -219,6 +219,21 @@ void *op2b_map_device_ptr(op_map map);
  * the reference's sequential loop on the same numbering). */
 #define OP2B_INC_GATHER 3
 int op2b_set_option(const char *key, long value);
+
+/* Kernel sources for loops that have no hand-written device kernel.  The
+ * reference's code generator compiles each user kernel into a device loop
+ * before the application is built (translator-v2); libop2b compiles it at
+ * the loop's first call instead, for sm_100a with NVRTC, from the source
+ * registered here under the loop's name, or else from the file <name>.h on
+ * OP2B_KERNEL_PATH (default: the working directory), the reference's
+ * one-kernel-per-header convention.  Preludes (helper functions, types; or
+ * user_types.h where it exists) are placed before every kernel.  Direct
+ * arguments in every access mode, indirect OP_READ and OP_INC, op_arg_idx and
+ * op_arg_gbl OP_READ/OP_INC/OP_MIN/OP_MAX are supported; anything else is an
+ * error.  A NULL source forgets the name's registration.  Registering drops
+ * the compiled modules.  Return 0, -1 on error. */
+int op2b_register_kernel(const char *name, const char *source);
+int op2b_register_prelude(const char *source);
 long op2b_get_option(const char *key);
 
 /* Per-loop device time (CUDA events on the library stream), launches and

@@ -1,0 +1,609 @@
+// Loops without a hand-written kernel: the application's own kernel function,
+// compiled for sm_100a at run time (NVRTC) inside a generated loop.
+//
+// OP2's code generator turns each op_par_loop's user kernel into a device
+// loop at build time (translator-v2/resources/templates/cuda/*.jinja); this
+// file does the same at run time from the kernel's source text:
+//   * the source is the one registered with op2b_register_kernel, or the file
+//     <name>.h on OP2B_KERNEL_PATH (default: the working directory) -- the
+//     reference's applications keep each kernel in a header of that name
+//     (apps/c/jac1/dp/res.h, update.h); preludes (op2b_register_prelude, or
+//     user_types.h where it exists) come first; quoted includes are inlined
+//     and system includes dropped (NVRTC provides the device math and printf);
+//   * constants declared with op_decl_const become __constant__ variables of
+//     the same name, type and dimension, refreshed when they change;
+//   * the generated kernel runs the user function once per set element
+//     (grid-stride): direct dats by pointer, indirect OP_READ through the map,
+//     indirect OP_INC into a per-element local added atomically, op_arg_idx
+//     as the element's (or its target's) index, op_arg_gbl OP_READ from a
+//     device copy, OP_INC/MIN/MAX into per-thread partials reduced by warp
+//     shuffles and device atomics, then combined with the caller's value;
+//   * indirect OP_WRITE/OP_RW (which need colouring), vector map arguments,
+//     op_arg_info and switched-off optional arguments are rejected with an
+//     error, not run on the host;
+//   * compiled with --fmad=false (each operation rounded once, like the
+//     reference's strictly compiled sequential build); modules are cached per
+//     loop signature and source until op_exit.
+// Summation order of OP_INC increments and gbl reductions is that of the
+// atomics, so results equal the sequential reference's to rounding, not bit
+// for bit (the hand-written Airfoil loops keep the reference's order).
+#include <cuda_runtime.h>
+#include <nvrtc.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <functional>
+#include <map>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "op2b_runtime.h"
+
+namespace op2b {
+namespace {
+
+struct Sources {
+  std::map<std::string, std::string> kernels;
+  std::vector<std::string> preludes;
+};
+Sources &sources() {
+  static Sources s;
+  return s;
+}
+
+bool read_file(const std::string &path, std::string &out) {
+  std::ifstream f(path, std::ios::binary);
+  if (!f) return false;
+  std::ostringstream ss;
+  ss << f.rdbuf();
+  out = ss.str();
+  return true;
+}
+
+std::vector<std::string> search_path() {
+  std::vector<std::string> dirs;
+  const char *p = getenv("OP2B_KERNEL_PATH");
+  std::string s = p ? p : ".";
+  size_t b = 0;
+  while (b <= s.size()) {
+    size_t e = s.find(':', b);
+    if (e == std::string::npos) e = s.size();
+    if (e > b) dirs.push_back(s.substr(b, e - b));
+    b = e + 1;
+  }
+  return dirs;
+}
+
+// a registered source or a file on the search path
+bool find_file(const std::string &name, std::string &out) {
+  auto it = sources().kernels.find(name);
+  if (it != sources().kernels.end()) {
+    out = it->second;
+    return true;
+  }
+  for (const std::string &d : search_path())
+    if (read_file(d + "/" + name, out)) return true;
+  return false;
+}
+
+// inline quoted includes (once each), drop system includes
+std::string expand(const std::string &src, std::vector<std::string> &seen, int depth) {
+  std::istringstream in(src);
+  std::ostringstream out;
+  std::string line;
+  while (std::getline(in, line)) {
+    size_t p = line.find_first_not_of(" \t");
+    if (p != std::string::npos && line.compare(p, 8, "#include") == 0) {
+      size_t q1 = line.find('"', p), q2 = q1 == std::string::npos ? q1 : line.find('"', q1 + 1);
+      if (q1 != std::string::npos && q2 != std::string::npos && depth < 8) {
+        std::string inc = line.substr(q1 + 1, q2 - q1 - 1), text;
+        bool done = false;
+        for (auto &s : seen) done |= s == inc;
+        if (!done && find_file(inc, text)) {
+          seen.push_back(inc);
+          out << expand(text, seen, depth + 1) << "\n";
+        }
+      }
+      out << "\n";  // keep line numbers close for compiler messages
+      continue;
+    }
+    out << line << "\n";
+  }
+  return out.str();
+}
+
+enum ArgKind { DIRECT, INDIRECT, GBL, IDX };
+
+struct ArgPlan {
+  ArgKind kind;
+  std::string ctype;
+  int dim = 1, acc = OP_READ, mdim = 0, idx = -1, bytes = 8;
+};
+
+std::string base_type(const char *t) {
+  std::string s = t ? t : "";
+  size_t c = s.find(':');
+  if (c != std::string::npos) s = s.substr(0, c);
+  return s;
+}
+
+int type_size(const std::string &t) {
+  if (t == "double") return 8;
+  if (t == "float" || t == "int") return 4;
+  return 0;
+}
+
+struct Jit {
+  cudaLibrary_t lib = nullptr;
+  cudaKernel_t fn = nullptr;
+  std::vector<std::string> cnames, clowered;
+  long const_version = -1;
+  void *gbl_d = nullptr;
+  size_t gbl_cap = 0;
+};
+
+std::map<std::string, Jit> &cache() {
+  static std::map<std::string, Jit> c;
+  return c;
+}
+
+std::string identity(const std::string &t, int acc) {
+  if (acc == OP_INC) return "0";
+  const bool mn = acc == OP_MIN;
+  if (t == "double") return mn ? "__longlong_as_double(0x7ff0000000000000LL)"
+                               : "__longlong_as_double((long long)0xfff0000000000000ULL)";
+  if (t == "float") return mn ? "__int_as_float(0x7f800000)" : "__int_as_float((int)0xff800000u)";
+  return mn ? "2147483647" : "(-2147483647 - 1)";
+}
+
+const char *kHelpers = R"(
+__device__ void op2b_amin(double *a, double v) {
+  unsigned long long *p = (unsigned long long *)a, old = *p, as;
+  do { as = old; if (__longlong_as_double((long long)as) <= v) return;
+       old = atomicCAS(p, as, (unsigned long long)__double_as_longlong(v)); } while (old != as);
+}
+__device__ void op2b_amax(double *a, double v) {
+  unsigned long long *p = (unsigned long long *)a, old = *p, as;
+  do { as = old; if (__longlong_as_double((long long)as) >= v) return;
+       old = atomicCAS(p, as, (unsigned long long)__double_as_longlong(v)); } while (old != as);
+}
+__device__ void op2b_amin(float *a, float v) {
+  int *p = (int *)a, old = *p, as;
+  do { as = old; if (__int_as_float(as) <= v) return;
+       old = atomicCAS(p, as, __float_as_int(v)); } while (old != as);
+}
+__device__ void op2b_amax(float *a, float v) {
+  int *p = (int *)a, old = *p, as;
+  do { as = old; if (__int_as_float(as) >= v) return;
+       old = atomicCAS(p, as, __float_as_int(v)); } while (old != as);
+}
+__device__ void op2b_amin(int *a, int v) { atomicMin(a, v); }
+__device__ void op2b_amax(int *a, int v) { atomicMax(a, v); }
+template <typename T> __device__ T op2b_min(T a, T b) { return b < a ? b : a; }
+template <typename T> __device__ T op2b_max(T a, T b) { return b > a ? b : a; }
+)";
+
+std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std::string &body) {
+  Runtime &r = rt();
+  std::ostringstream s;
+  s << "// libop2b: generated loop for the user kernel '" << name << "'\n";
+  for (auto &kv : r.consts) {
+    const std::string &t = r.const_types[kv.first];
+    s << "__constant__ " << (t.empty() ? "double" : t) << " " << kv.first;
+    if (kv.second.size() > 1) s << "[" << kv.second.size() << "]";
+    s << ";\n";
+  }
+  s << kHelpers << "\n" << body << "\n";
+  s << "extern \"C\" __global__ void op2b_loop(int op2b_n";
+  for (size_t i = 0; i < ap.size(); i++) {
+    const ArgPlan &a = ap[i];
+    if (a.kind == DIRECT || a.kind == INDIRECT || a.kind == GBL)
+      s << ", " << a.ctype << " *op2b_d" << i;
+    if (a.kind == INDIRECT || (a.kind == IDX && a.mdim > 0)) s << ", const int *op2b_m" << i;
+  }
+  s << ") {\n";
+  for (size_t i = 0; i < ap.size(); i++) {
+    const ArgPlan &a = ap[i];
+    if (a.kind == GBL && a.acc != OP_READ)
+      s << "  " << a.ctype << " op2b_l" << i << "[" << a.dim << "];\n  for (int k = 0; k < "
+        << a.dim << "; k++) op2b_l" << i << "[k] = " << identity(a.ctype, a.acc) << ";\n";
+  }
+  s << "  for (int op2b_e = blockIdx.x * blockDim.x + threadIdx.x; op2b_e < op2b_n;"
+       " op2b_e += gridDim.x * blockDim.x) {\n";
+  std::ostringstream call;
+  call << "    " << name << "(";
+  for (size_t i = 0; i < ap.size(); i++) {
+    const ArgPlan &a = ap[i];
+    if (i) call << ", ";
+    switch (a.kind) {
+      case DIRECT:
+        call << "op2b_d" << i << " + (size_t)op2b_e * " << a.dim;
+        break;
+      case INDIRECT:
+        s << "    const int op2b_t" << i << " = op2b_m" << i << "[(size_t)op2b_e * " << a.mdim
+          << " + " << a.idx << "];\n";
+        if (a.acc == OP_INC) {
+          s << "    " << a.ctype << " op2b_l" << i << "[" << a.dim << "];\n    for (int k = 0; k < "
+            << a.dim << "; k++) op2b_l" << i << "[k] = 0;\n";
+          call << "op2b_l" << i;
+        } else {
+          call << "op2b_d" << i << " + (size_t)op2b_t" << i << " * " << a.dim;
+        }
+        break;
+      case GBL:
+        if (a.acc == OP_READ) call << "op2b_d" << i;
+        else call << "op2b_l" << i;
+        break;
+      case IDX:
+        if (a.mdim > 0)
+          s << "    int op2b_x" << i << " = op2b_m" << i << "[(size_t)op2b_e * " << a.mdim
+            << " + " << a.idx << "];\n";
+        else
+          s << "    int op2b_x" << i << " = op2b_e;\n";
+        call << "&op2b_x" << i;
+        break;
+    }
+  }
+  call << ");\n";
+  s << call.str();
+  for (size_t i = 0; i < ap.size(); i++) {
+    const ArgPlan &a = ap[i];
+    if (a.kind == INDIRECT && a.acc == OP_INC)
+      s << "    for (int k = 0; k < " << a.dim << "; k++) atomicAdd(op2b_d" << i
+        << " + (size_t)op2b_t" << i << " * " << a.dim << " + k, op2b_l" << i << "[k]);\n";
+  }
+  s << "  }\n";
+  for (size_t i = 0; i < ap.size(); i++) {
+    const ArgPlan &a = ap[i];
+    if (a.kind != GBL || a.acc == OP_READ) continue;
+    const char *op = a.acc == OP_INC ? "v + w" : a.acc == OP_MIN ? "op2b_min(v, w)" : "op2b_max(v, w)";
+    s << "  for (int k = 0; k < " << a.dim << "; k++) {\n    " << a.ctype << " v = op2b_l" << i
+      << "[k];\n    for (int o = 16; o > 0; o >>= 1) { " << a.ctype
+      << " w = __shfl_down_sync(0xffffffffu, v, o); v = " << op << "; }\n"
+      << "    if ((threadIdx.x & 31) == 0) ";
+    if (a.acc == OP_INC) s << "atomicAdd(op2b_d" << i << " + k, v);\n";
+    else s << (a.acc == OP_MIN ? "op2b_amin" : "op2b_amax") << "(op2b_d" << i << " + k, v);\n";
+    s << "  }\n";
+  }
+  s << "}\n";
+  return s.str();
+}
+
+bool compile(const char *name, const std::string &src, Jit &j) {
+  Runtime &r = rt();
+  nvrtcProgram prog;
+  if (nvrtcCreateProgram(&prog, src.c_str(), (std::string(name) + "_op2b.cu").c_str(), 0,
+                         nullptr, nullptr) != NVRTC_SUCCESS) {
+    set_error("op_par_loop(%s): NVRTC could not create the program", name);
+    return false;
+  }
+  for (auto &kv : r.consts) {
+    j.cnames.push_back(kv.first);
+    nvrtcAddNameExpression(prog, ("&" + kv.first).c_str());
+  }
+  const char *opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "-default-device",
+                        "--fmad=false"};
+  nvrtcResult rc = nvrtcCompileProgram(prog, 4, opts);
+  if (rc != NVRTC_SUCCESS) {
+    size_t n = 0;
+    nvrtcGetProgramLogSize(prog, &n);
+    std::string log(n, '\0');
+    if (n) nvrtcGetProgramLog(prog, &log[0]);
+    set_error("op_par_loop(%s): compiling the kernel failed:\n%s", name, log.c_str());
+    nvrtcDestroyProgram(&prog);
+    return false;
+  }
+  for (auto &c : j.cnames) {
+    const char *low = nullptr;
+    nvrtcGetLoweredName(prog, ("&" + c).c_str(), &low);
+    j.clowered.push_back(low ? low : c);
+  }
+  size_t cubin_size = 0;
+  nvrtcGetCUBINSize(prog, &cubin_size);
+  std::vector<char> cubin(cubin_size);
+  nvrtcGetCUBIN(prog, cubin.data());
+  nvrtcDestroyProgram(&prog);
+  if (!cuda_ok(cudaLibraryLoadData(&j.lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr,
+                                   0),
+               "op_par_loop: loading the compiled kernel"))
+    return false;
+  return cuda_ok(cudaLibraryGetKernel(&j.fn, j.lib, "op2b_loop"), "op_par_loop: kernel entry");
+}
+
+bool upload_constants(Jit &j) {
+  Runtime &r = rt();
+  if (j.const_version == r.const_version) return true;
+  if (!cuda_ok(cudaStreamSynchronize(r.stream), "op_par_loop: constants")) return false;
+  for (size_t i = 0; i < j.cnames.size(); i++) {
+    auto it = r.consts.find(j.cnames[i]);
+    if (it == r.consts.end()) continue;
+    void *p = nullptr;
+    size_t bytes = 0;
+    if (!cuda_ok(cudaLibraryGetGlobal(&p, &bytes, j.lib, j.clowered[i].c_str()),
+                 "op_par_loop: constant lookup"))
+      return false;
+    const std::string &t = r.const_types[j.cnames[i]];
+    std::vector<char> buf(bytes, 0);
+    for (size_t k = 0; k < it->second.size(); k++) {
+      if (t == "float" && (k + 1) * 4 <= bytes) {
+        float v = (float)it->second[k];
+        memcpy(&buf[k * 4], &v, 4);
+      } else if (t == "int" && (k + 1) * 4 <= bytes) {
+        int v = (int)it->second[k];
+        memcpy(&buf[k * 4], &v, 4);
+      } else if ((k + 1) * 8 <= bytes) {
+        memcpy(&buf[k * 8], &it->second[k], 8);
+      }
+    }
+    if (!cuda_ok(cudaMemcpyAsync(p, buf.data(), bytes, cudaMemcpyHostToDevice, r.stream),
+                 "op_par_loop: constant upload") ||
+        !cuda_ok(cudaStreamSynchronize(r.stream), "op_par_loop: constant upload"))
+      return false;
+  }
+  j.const_version = r.const_version;
+  return true;
+}
+
+}  // namespace
+
+bool jit_has_kernel(const char *name) {
+  std::string src;
+  return name && find_file(std::string(name) + ".h", src);
+}
+
+void release_jit() {
+  for (auto &kv : cache()) {
+    if (kv.second.lib) cudaLibraryUnload(kv.second.lib);
+    cudaFree(kv.second.gbl_d);
+  }
+  cache().clear();
+}
+
+int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
+  Runtime &r = rt();
+  std::vector<ArgPlan> ap((size_t)nargs);
+  std::ostringstream key;
+  key << name;
+  for (int i = 0; i < nargs; i++) {
+    const op_arg &x = args[i];
+    ArgPlan &a = ap[(size_t)i];
+    if (!x.opt) {
+      set_error("op_par_loop(%s): argument %d: optional arguments that are switched off are "
+                "not supported for run-time compiled loops", name, i);
+      return -1;
+    }
+    if (x.argtype == OP_ARG_DAT) {
+      if (!x.dat) return set_error("op_par_loop(%s): argument %d: no dat", name, i), -1;
+      a.ctype = base_type(x.dat->type);
+      a.bytes = type_size(a.ctype);
+      a.dim = x.dat->dim;
+      a.acc = x.acc;
+      if (!a.bytes || a.bytes * a.dim != x.dat->size) {
+        set_error("op_par_loop(%s): argument %d: dat type '%s' is not double, float or int",
+                  name, i, x.dat->type);
+        return -1;
+      }
+      if (x.map == nullptr) {
+        if (x.dat->set != set) return set_error("op_par_loop(%s): argument %d: dat is not on the loop's set", name, i), -1;
+        a.kind = DIRECT;
+      } else {
+        if (x.idx < 0 || x.idx >= x.map->dim) {
+          set_error("op_par_loop(%s): argument %d: map index %d (vector map arguments are not "
+                    "supported for run-time compiled loops)", name, i, x.idx);
+          return -1;
+        }
+        if (x.map->from != set || x.map->to != x.dat->set)
+          return set_error("op_par_loop(%s): argument %d: map does not match the loop's set and the dat", name, i), -1;
+        if (x.acc != OP_READ && x.acc != OP_INC) {
+          set_error("op_par_loop(%s): argument %d: indirect %s needs colouring, which "
+                    "run-time compiled loops do not do; use OP_INC or OP_READ", name, i,
+                    x.acc == OP_WRITE ? "OP_WRITE" : "OP_RW");
+          return -1;
+        }
+        a.kind = INDIRECT;
+        a.mdim = x.map->dim;
+        a.idx = x.idx;
+      }
+    } else if (x.argtype == OP_ARG_GBL) {
+      a.kind = GBL;
+      a.ctype = base_type(x.type);
+      a.bytes = type_size(a.ctype);
+      a.dim = x.dim;
+      a.acc = x.acc;
+      if (!a.bytes || !x.data || a.dim <= 0)
+        return set_error("op_par_loop(%s): argument %d: global of unsupported type '%s'", name, i, x.type ? x.type : ""), -1;
+      if (a.acc != OP_READ && a.acc != OP_INC && a.acc != OP_MIN && a.acc != OP_MAX)
+        return set_error("op_par_loop(%s): argument %d: globals are OP_READ, OP_INC, OP_MIN or OP_MAX", name, i), -1;
+    } else if (x.argtype == OP_ARG_IDX) {
+      a.kind = IDX;
+      a.ctype = "int";
+      if (x.map) {
+        if (x.map->from != set || x.idx < 0 || x.idx >= x.map->dim)
+          return set_error("op_par_loop(%s): argument %d: op_arg_idx map or index does not fit the loop", name, i), -1;
+        a.mdim = x.map->dim;
+        a.idx = x.idx;
+      }
+    } else {
+      set_error("op_par_loop(%s): argument %d: op_arg_info is not supported for run-time "
+                "compiled loops", name, i);
+      return -1;
+    }
+    key << "|" << a.kind << ":" << a.ctype << ":" << a.dim << ":" << a.acc << ":" << a.mdim
+        << ":" << a.idx;
+  }
+  std::string body;
+  std::vector<std::string> seen;
+  for (auto &p : sources().preludes) body += expand(p, seen, 0) + "\n";
+  std::string types;
+  if (sources().preludes.empty() && find_file("user_types.h", types)) {
+    seen.push_back("user_types.h");
+    body += expand(types, seen, 0) + "\n";
+  }
+  std::string ksrc;
+  if (!find_file(std::string(name) + ".h", ksrc)) {
+    set_error("op_par_loop(%s): no device implementation of this loop is registered, and no "
+              "kernel source %s.h was registered or found on OP2B_KERNEL_PATH", name, name);
+    return -1;
+  }
+  seen.push_back(std::string(name) + ".h");
+  body += expand(ksrc, seen, 0);
+  for (auto &kv : r.consts) key << "|c:" << kv.first << ":" << r.const_types[kv.first] << ":" << kv.second.size();
+  key << "|s:" << std::hash<std::string>()(body);
+  Jit &j = cache()[key.str()];
+  if (!j.fn) {
+    const std::string src = generate(name, ap, body);
+    if (!compile(name, src, j)) {
+      cache().erase(key.str());
+      return -1;
+    }
+  }
+  if (!upload_constants(j)) return -1;
+  // globals: device copies (OP_READ values, reduction identities)
+  std::vector<size_t> goff((size_t)nargs, 0);
+  size_t gbytes = 0;
+  for (int i = 0; i < nargs; i++)
+    if (ap[(size_t)i].kind == GBL) {
+      goff[(size_t)i] = gbytes;
+      gbytes += ((size_t)ap[(size_t)i].dim * ap[(size_t)i].bytes + 15) & ~(size_t)15;
+    }
+  std::vector<char> gh(gbytes, 0);
+  for (int i = 0; i < nargs; i++) {
+    const ArgPlan &a = ap[(size_t)i];
+    if (a.kind != GBL) continue;
+    char *dst = gh.data() + goff[(size_t)i];
+    if (a.acc == OP_READ || a.acc == OP_INC) {
+      if (a.acc == OP_READ) memcpy(dst, args[i].data, (size_t)a.dim * a.bytes);
+      continue;  // OP_INC starts from zero
+    }
+    for (int k = 0; k < a.dim; k++) {  // MIN / MAX start from the identity
+      const bool mn = a.acc == OP_MIN;
+      if (a.ctype == "double") {
+        double v = mn ? HUGE_VAL : -HUGE_VAL;
+        memcpy(dst + 8 * k, &v, 8);
+      } else if (a.ctype == "float") {
+        float v = mn ? HUGE_VALF : -HUGE_VALF;
+        memcpy(dst + 4 * k, &v, 4);
+      } else {
+        int v = mn ? 2147483647 : (-2147483647 - 1);
+        memcpy(dst + 4 * k, &v, 4);
+      }
+    }
+  }
+  if (gbytes > j.gbl_cap) {
+    cudaStreamSynchronize(r.stream);
+    cudaFree(j.gbl_d);
+    j.gbl_d = nullptr;
+    j.gbl_cap = 0;
+    if (!cuda_ok(cudaMalloc(&j.gbl_d, gbytes), "op_par_loop: globals")) return -1;
+    j.gbl_cap = gbytes;
+  }
+  if (gbytes && !cuda_ok(cudaMemcpyAsync(j.gbl_d, gh.data(), gbytes, cudaMemcpyHostToDevice,
+                                         r.stream),
+                         "op_par_loop: globals"))
+    return -1;
+  // parameters
+  std::vector<void *> ptrs;
+  ptrs.reserve((size_t)nargs * 2 + 1);
+  std::vector<void *> kp;
+  int n = set->size;
+  kp.push_back(&n);
+  double bytes = 0.0;
+  for (int i = 0; i < nargs; i++) {
+    const ArgPlan &a = ap[(size_t)i];
+    const op_arg &x = args[i];
+    if (a.kind == DIRECT || a.kind == INDIRECT) {
+      ptrs.push_back(x.dat->data_d);
+      bytes += (double)x.dat->size * (a.kind == DIRECT ? n : x.dat->set->size);
+    } else if (a.kind == GBL) {
+      ptrs.push_back((char *)j.gbl_d + goff[(size_t)i]);
+    }
+    if (a.kind == DIRECT || a.kind == INDIRECT || a.kind == GBL) kp.push_back(&ptrs.back());
+    if (a.kind == INDIRECT || (a.kind == IDX && a.mdim > 0)) {
+      ptrs.push_back(x.map->map_d);
+      kp.push_back(&ptrs.back());
+      bytes += 4.0 * n;
+    }
+  }
+  r.begin_loop(name);
+  if (n > 0) {
+    unsigned grid = (unsigned)std::min<long long>(((long long)n + 255) / 256, (long long)r.nsm * 8);
+    if (!cuda_ok(cudaLaunchKernel((const void *)j.fn, dim3(grid), dim3(256), kp.data(), 0,
+                                  r.stream),
+                 "op_par_loop: launch")) {
+      r.end_loop(bytes);
+      return -1;
+    }
+    r.launches++;
+  }
+  r.end_loop(bytes);
+  // reductions: combine with the caller's values once the loop has finished
+  bool reduce = false;
+  for (auto &a : ap) reduce |= a.kind == GBL && a.acc != OP_READ;
+  if (!reduce) return 0;
+  if (!cuda_ok(cudaMemcpyAsync(gh.data(), j.gbl_d, gbytes, cudaMemcpyDeviceToHost, r.stream),
+               "op_par_loop: globals") ||
+      !cuda_ok(cudaStreamSynchronize(r.stream), "op_par_loop: globals"))
+    return -1;
+  for (int i = 0; i < nargs; i++) {
+    const ArgPlan &a = ap[(size_t)i];
+    if (a.kind != GBL || a.acc == OP_READ || n == 0) continue;
+    const char *src = gh.data() + goff[(size_t)i];
+    char *dst = args[i].data;
+    for (int k = 0; k < a.dim; k++) {
+      if (a.ctype == "double") {
+        double v, u;
+        memcpy(&v, src + 8 * k, 8);
+        memcpy(&u, dst + 8 * k, 8);
+        u = a.acc == OP_INC ? u + v : a.acc == OP_MIN ? (v < u ? v : u) : (v > u ? v : u);
+        memcpy(dst + 8 * k, &u, 8);
+      } else if (a.ctype == "float") {
+        float v, u;
+        memcpy(&v, src + 4 * k, 4);
+        memcpy(&u, dst + 4 * k, 4);
+        u = a.acc == OP_INC ? u + v : a.acc == OP_MIN ? (v < u ? v : u) : (v > u ? v : u);
+        memcpy(dst + 4 * k, &u, 4);
+      } else {
+        int v, u;
+        memcpy(&v, src + 4 * k, 4);
+        memcpy(&u, dst + 4 * k, 4);
+        u = a.acc == OP_INC ? u + v : a.acc == OP_MIN ? (v < u ? v : u) : (v > u ? v : u);
+        memcpy(dst + 4 * k, &u, 4);
+      }
+    }
+  }
+  return 0;
+}
+
+}  // namespace op2b
+
+extern "C" {
+
+int op2b_register_kernel(const char *name, const char *source) {
+  if (!name || !*name) {
+    op2b::set_error("op2b_register_kernel: needs a kernel name");
+    return -1;
+  }
+  std::string n(name);
+  if (n.size() < 2 || n.compare(n.size() - 2, 2, ".h") != 0) n += ".h";
+  if (source) op2b::sources().kernels[n] = source;
+  else op2b::sources().kernels.erase(n);  // forget it
+  op2b::release_jit();  // sources changed: compile afresh
+  return 0;
+}
+
+int op2b_register_prelude(const char *source) {
+  if (!source) {
+    op2b::set_error("op2b_register_prelude: needs a source");
+    return -1;
+  }
+  op2b::sources().preludes.push_back(source);
+  op2b::release_jit();
+  return 0;
+}
+
+}  // extern "C"

@@ -298,6 +298,8 @@ void op_exit(void) {
   r.maps.clear();
   r.sets.clear();
   r.consts.clear();
+  r.const_types.clear();
+  release_jit();
   r.map_ptrs.clear();
   for (auto &p : r.pending) {
     cudaEventDestroy(p.e0);
@@ -539,6 +541,8 @@ void op_decl_const_char(int dim, char const *type, int type_size, char *dat, cha
   std::string n(name);
   while (!n.empty() && (n[0] == '&' || n[0] == ' ')) n.erase(0, 1);
   r.consts[n] = v;
+  r.const_types[n] = t;
+  r.const_version++;
 }
 
 // ------------------------------------------------------------------ op_arg

@@ -27,6 +27,10 @@ const char *acc_name(int a) {
   return (a >= 0 && a <= 6) ? n[a] : "?";
 }
 
+// a loop function's return value when the arguments do not match its
+// signature (nothing launched, nothing changed)
+constexpr int kSigMismatch = -2;
+
 struct Sig {
   const char *loop;
   op_set set;
@@ -165,12 +169,12 @@ int finish(cudaError_t e, const char *loop) {
 // ---------------------------------------------------------------- save_soln
 int loop_save_soln(const char *name, op_set set, int nargs, op_arg *a) {
   Sig s{name, set, a, nargs};
-  if (nargs != 2) return s.fail(nargs, "save_soln takes 2 arguments"), -1;
+  if (nargs != 2) return s.fail(nargs, "save_soln takes 2 arguments"), kSigMismatch;
   int dim = a[0].dat ? a[0].dat->dim : 0;
   s.dat(0, dim, OP_READ, nullptr, -1);
   s.dat(1, dim, OP_WRITE, nullptr, -1);
-  if (!s.ok) return -1;
-  if (a[0].dat->size != a[1].dat->size) return s.fail(1, "element size differs from argument 0"), -1;
+  if (!s.ok) return kSigMismatch;
+  if (a[0].dat->size != a[1].dat->size) return s.fail(1, "element size differs from argument 0"), kSigMismatch;
   Runtime &r = rt();
   if (r.pend.kind && !r.flush_pending()) return -1;
   if (r.spec.inplace && (a[1].dat == r.spec.x || a[1].dat == r.spec.q ||
@@ -200,16 +204,16 @@ int loop_save_soln(const char *name, op_set set, int nargs, op_arg *a) {
 // ---------------------------------------------------------------- adt_calc
 int loop_adt_calc(const char *name, op_set set, int nargs, op_arg *a) {
   Sig s{name, set, a, nargs};
-  if (nargs != 6) return s.fail(nargs, "adt_calc takes 6 arguments"), -1;
+  if (nargs != 6) return s.fail(nargs, "adt_calc takes 6 arguments"), kSigMismatch;
   op_map pcell = a[0].map;
-  if (!pcell || pcell->dim != 4) return s.fail(0, "expected a dim-4 map (cells -> nodes)"), -1;
+  if (!pcell || pcell->dim != 4) return s.fail(0, "expected a dim-4 map (cells -> nodes)"), kSigMismatch;
   for (int i = 0; i < 4; i++) s.dat(i, 2, OP_READ, pcell, i);
   if (s.ok && (a[1].dat != a[0].dat || a[2].dat != a[0].dat || a[3].dat != a[0].dat))
-    return s.fail(1, "arguments 0-3 must be the same dat"), -1;
+    return s.fail(1, "arguments 0-3 must be the same dat"), kSigMismatch;
   s.dat(4, 4, OP_READ, nullptr, -1);
   s.dat(5, 1, OP_WRITE, nullptr, -1);
   int rb = s.real_bytes({0, 4, 5});
-  if (!s.ok) return -1;
+  if (!s.ok) return kSigMismatch;
   Runtime &r = rt();
   int C = set->size, N = a[0].dat->set->size;
   double bytes = 16.0 * C + (double)rb * (2.0 * N + 5.0 * C);
@@ -304,10 +308,10 @@ static cudaError_t res_gather_slots(Runtime &r, const SlotRecords &s, const ResC
 
 int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
   Sig s{name, set, a, nargs};
-  if (nargs != 8) return s.fail(nargs, "res_calc takes 8 arguments"), -1;
+  if (nargs != 8) return s.fail(nargs, "res_calc takes 8 arguments"), kSigMismatch;
   op_map pedge = a[0].map, pecell = a[2].map;
-  if (!pedge || pedge->dim != 2) return s.fail(0, "expected a dim-2 map (edges -> nodes)"), -1;
-  if (!pecell || pecell->dim != 2) return s.fail(2, "expected a dim-2 map (edges -> cells)"), -1;
+  if (!pedge || pedge->dim != 2) return s.fail(0, "expected a dim-2 map (edges -> nodes)"), kSigMismatch;
+  if (!pecell || pecell->dim != 2) return s.fail(2, "expected a dim-2 map (edges -> cells)"), kSigMismatch;
   s.dat(0, 2, OP_READ, pedge, 0);
   s.dat(1, 2, OP_READ, pedge, 1);
   s.dat(2, 4, OP_READ, pecell, 0);
@@ -318,9 +322,9 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
   s.dat(7, 4, OP_INC, pecell, 1);
   if (s.ok && (a[1].dat != a[0].dat || a[3].dat != a[2].dat || a[5].dat != a[4].dat ||
                a[7].dat != a[6].dat))
-    return s.fail(1, "paired arguments must name the same dat"), -1;
+    return s.fail(1, "paired arguments must name the same dat"), kSigMismatch;
   int rb = s.real_bytes({0, 2, 4, 6});
-  if (!s.ok) return -1;
+  if (!s.ok) return kSigMismatch;
   Runtime &r = rt();
   if (r.pend.kind && !r.flush_pending()) return -1;
   if (r.spec.inplace && !r.restore_spec()) return -1;
@@ -407,21 +411,21 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
 // ---------------------------------------------------------------- bres_calc
 int loop_bres_calc(const char *name, op_set set, int nargs, op_arg *a) {
   Sig s{name, set, a, nargs};
-  if (nargs != 6) return s.fail(nargs, "bres_calc takes 6 arguments"), -1;
+  if (nargs != 6) return s.fail(nargs, "bres_calc takes 6 arguments"), kSigMismatch;
   op_map pbedge = a[0].map, pbecell = a[2].map;
-  if (!pbedge || pbedge->dim != 2) return s.fail(0, "expected a dim-2 map (bedges -> nodes)"), -1;
-  if (!pbecell || pbecell->dim != 1) return s.fail(2, "expected a dim-1 map (bedges -> cells)"), -1;
+  if (!pbedge || pbedge->dim != 2) return s.fail(0, "expected a dim-2 map (bedges -> nodes)"), kSigMismatch;
+  if (!pbecell || pbecell->dim != 1) return s.fail(2, "expected a dim-1 map (bedges -> cells)"), kSigMismatch;
   s.dat(0, 2, OP_READ, pbedge, 0);
   s.dat(1, 2, OP_READ, pbedge, 1);
   s.dat(2, 4, OP_READ, pbecell, 0);
   s.dat(3, 1, OP_READ, pbecell, 0);
   s.dat(4, 4, OP_INC, pbecell, 0);
   s.dat(5, 1, OP_READ, nullptr, -1);
-  if (s.ok && a[1].dat != a[0].dat) return s.fail(1, "arguments 0 and 1 must be the same dat"), -1;
+  if (s.ok && a[1].dat != a[0].dat) return s.fail(1, "arguments 0 and 1 must be the same dat"), kSigMismatch;
   if (s.ok && (type_bytes(a[5].dat->type) != 4 || std::string(a[5].dat->type).rfind("int", 0) != 0))
-    return s.fail(5, "the boundary flag must be an int dat"), -1;
+    return s.fail(5, "the boundary flag must be an int dat"), kSigMismatch;
   int rb = s.real_bytes({0, 2, 3, 4});
-  if (!s.ok) return -1;
+  if (!s.ok) return kSigMismatch;
   Runtime &r = rt();
   if (r.spec.inplace && !r.restore_spec()) return -1;
   int B = set->size;
@@ -519,7 +523,7 @@ int loop_bres_calc(const char *name, op_set set, int nargs, op_arg *a) {
 // airfoil_tempdats/dp/update.h.
 int loop_update(const char *name, op_set set, int nargs, op_arg *a) {
   Sig s{name, set, a, nargs};
-  if (nargs != 5 && nargs != 8) return s.fail(nargs, "update takes 5 or 8 arguments"), -1;
+  if (nargs != 5 && nargs != 8) return s.fail(nargs, "update takes 5 or 8 arguments"), kSigMismatch;
   s.dat(0, 4, OP_READ, nullptr, -1);
   s.dat(1, 4, OP_WRITE, nullptr, -1);
   s.dat(2, 4, OP_RW, nullptr, -1);
@@ -534,8 +538,8 @@ int loop_update(const char *name, op_set set, int nargs, op_arg *a) {
       s.fail(7, "expected op_arg_info(&int, 1, \"int\", 5)");
   }
   int rb = s.real_bytes({0, 1, 2, 3});
-  if (!s.ok) return -1;
-  if (a[4].type && strcmp(a[4].type, "double") != 0) return s.fail(4, "rms must be double"), -1;
+  if (!s.ok) return kSigMismatch;
+  if (a[4].type && strcmp(a[4].type, "double") != 0) return s.fail(4, "rms must be double"), kSigMismatch;
   Runtime &r = rt();
   if (r.pend.kind && !r.flush_pending()) return -1;
   int C = set->size;
@@ -673,9 +677,19 @@ int op_par_loop_c(char const *name, op_set set, int nargs, op_arg *args) {
     return -1;
   }
   for (const Entry &e : kLoops)
-    if (strcmp(e.name, name) == 0) return e.fn(name, set, nargs, args);
-  if (r.pend.kind) r.flush_pending();
-  if (r.spec.inplace) r.restore_spec();
+    if (strcmp(e.name, name) == 0) {
+      int rc = e.fn(name, set, nargs, args);
+      if (rc != kSigMismatch) return rc;
+      // an application's own loop that shares a name with an Airfoil loop
+      // but not its arguments: run its kernel source if it has one
+      if (!jit_has_kernel(name)) return -1;
+      break;
+    }
+  if (r.pend.kind && !r.flush_pending()) return -1;
+  if (r.spec.inplace && !r.restore_spec()) return -1;
+  // no hand-written kernel: the application's own kernel source, compiled at
+  // run time, if it has one
+  if (jit_has_kernel(name)) return jit_par_loop(name, set, nargs, args);
   set_error("op_par_loop(%s): no device implementation of this loop is registered "
             "(libop2b runs loops on the GPU only)",
             name);

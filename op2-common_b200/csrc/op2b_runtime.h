@@ -93,6 +93,8 @@ struct Runtime {
   std::vector<std::unique_ptr<op_map_core>> maps;
   std::vector<std::unique_ptr<op_dat_core>> dats;
   std::map<std::string, std::vector<double>> consts;
+  std::map<std::string, std::string> const_types;  // "double", "float" or "int"
+  long const_version = 0;                          // bumped by every op_decl_const
   std::map<const int *, op_map> map_ptrs;  // user array -> map (op_renumber_ptr)
 
   // fused-update reduction
@@ -138,6 +140,11 @@ void fetch_original_order(op_dat dat, char *dst, int low, int high);
 void release_renumbering();
 // plan.cu
 void release_plans();
+// jit.cpp: loops without a hand-written kernel, compiled from the user's
+// kernel source at run time
+bool jit_has_kernel(const char *name);
+int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args);
+void release_jit();
 // airfoil_gather.cu
 void release_inverse_maps();
 

@@ -91,7 +91,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
         if verbose:
             print("compiled", base, file=sys.stderr)
     if changed:
-        cmd = [nvcc, *ARCH, "-shared", "-o", LIB + ".tmp", *objs, "-lcuda"]
+        cmd = [nvcc, *ARCH, "-shared", "-o", LIB + ".tmp", *objs, "-lcuda", "-lnvrtc"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"linking libop2b.so failed:\n{res.stdout}{res.stderr}")

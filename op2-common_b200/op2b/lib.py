@@ -113,6 +113,8 @@ _SIGS = {
     "op2b_dat_device_ptr": (ctypes.c_void_p, [op_dat]),
     "op2b_map_device_ptr": (ctypes.c_void_p, [op_map]),
     "op2b_set_option": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_long]),
+    "op2b_register_kernel": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p]),
+    "op2b_register_prelude": (ctypes.c_int, [ctypes.c_char_p]),
     "op2b_get_option": (ctypes.c_long, [ctypes.c_char_p]),
     "op2b_loop_stats": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double),
                                        ctypes.POINTER(ctypes.c_long),
@@ -403,6 +405,18 @@ def op_fetch_data_idx(dat, low: int, high: int) -> np.ndarray:
 
 def op_get_size(set_) -> int:
     return load().op_get_size(set_)
+
+
+def register_kernel(name: str, source: str | None):
+    """Kernel source for a loop without a hand-written device kernel (compiled
+    at its first op_par_loop call, op2b_register_kernel); None forgets it."""
+    if load().op2b_register_kernel(_b(name), None if source is None else source.encode()) != 0:
+        _check(False, "op2b_register_kernel")
+
+
+def register_prelude(source: str):
+    if load().op2b_register_prelude(source.encode()) != 0:
+        _check(False, "op2b_register_prelude")
 
 
 def set_option(key: str, value: int):

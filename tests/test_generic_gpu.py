@@ -1,0 +1,202 @@
+"""Loops without a hand-written kernel: the application's kernel source
+compiled at run time (NVRTC, sm_100a) into a generated loop, against numpy.
+
+Tolerances: direct arguments and OP_MIN/OP_MAX are exact (each element's
+arithmetic is the kernel's, compiled without FMA contraction, as numpy
+computes it); OP_INC increments and OP_INC globals are summed by atomics in
+no fixed order: within 1e-12 relative of the sequential sum.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from op2b import lib as L
+
+pytestmark = pytest.mark.gpu
+
+DIRECT = """
+inline void gen_scale(const double *a, double *b, const int *i, double *s, double *mx,
+                      double *mn, const double *g) {
+  *b = fac * (*a) + g[0] * (*i) + g[1];
+  *s += *b;
+  *mx = (*b > *mx) ? *b : *mx;
+  *mn = (*b < *mn) ? *b : *mn;
+}
+"""
+
+EDGES = """
+inline void gen_scatter(const double *A, const double *u, double *du, const double *beta,
+                        const int *e, const int *n0) {
+  du[0] += (*beta) * (*A) * u[0];
+  du[1] += (*beta) * u[1] - (double)(*e) + 0.5 * (*n0);
+}
+"""
+
+
+def _rng_mesh(n_nodes=5000, n_edges=16000, seed=0):
+    rng = np.random.default_rng(seed)
+    pp = rng.integers(0, n_nodes, size=(n_edges, 2)).astype(np.int32)
+    return rng, pp
+
+
+def test_direct_loop_with_globals_index_and_constant(op2):
+    op2.register_kernel("gen_scale", DIRECT)
+    rng = np.random.default_rng(1)
+    n = 20000
+    a = rng.standard_normal(n)
+    s = op2.op_decl_set(n, "cells")
+    pa = op2.op_decl_dat(s, 1, "double", a, "a")
+    pb = op2.op_decl_dat(s, 1, "double", None, "b")
+    op2.op_decl_const(1, "double", 2.5, "fac")
+    tot = np.array([10.0])
+    mx = np.array([-1e300])
+    mn = np.array([1e300])
+    g = np.array([1e-3, -0.25])
+    for _ in range(2):  # the second call runs the cached module
+        tot[0] = 10.0
+        op2.op_par_loop("gen_scale", s,
+                        op2.op_arg_dat(pa, -1, op2.OP_ID, 1, "double", op2.OP_READ),
+                        op2.op_arg_dat(pb, -1, op2.OP_ID, 1, "double", op2.OP_WRITE),
+                        op2.op_arg_idx(-1, op2.OP_ID),
+                        op2.op_arg_gbl(tot, 1, "double", op2.OP_INC),
+                        op2.op_arg_gbl(mx, 1, "double", op2.OP_MAX),
+                        op2.op_arg_gbl(mn, 1, "double", op2.OP_MIN),
+                        op2.op_arg_gbl(g, 2, "double", op2.OP_READ))
+    b = 2.5 * a + g[0] * np.arange(n) + g[1]
+    got = op2.op_fetch_data(pb)[:, 0]
+    assert np.array_equal(got, b)
+    assert abs(tot[0] - (10.0 + b.sum())) <= 1e-12 * np.abs(b).sum()
+    assert mx[0] == b.max() and mn[0] == b.min()
+    # a changed constant reaches the compiled module
+    op2.op_decl_const(1, "double", -1.0, "fac")
+    op2.op_par_loop("gen_scale", s,
+                    op2.op_arg_dat(pa, -1, op2.OP_ID, 1, "double", op2.OP_READ),
+                    op2.op_arg_dat(pb, -1, op2.OP_ID, 1, "double", op2.OP_WRITE),
+                    op2.op_arg_idx(-1, op2.OP_ID),
+                    op2.op_arg_gbl(np.zeros(1), 1, "double", op2.OP_INC),
+                    op2.op_arg_gbl(np.array([-1e300]), 1, "double", op2.OP_MAX),
+                    op2.op_arg_gbl(np.array([1e300]), 1, "double", op2.OP_MIN),
+                    op2.op_arg_gbl(g, 2, "double", op2.OP_READ))
+    assert np.array_equal(op2.op_fetch_data(pb)[:, 0], -a + g[0] * np.arange(n) + g[1])
+
+
+def test_indirect_increment_and_read_through_a_map(op2):
+    op2.register_kernel("gen_scatter", EDGES)
+    rng, pp = _rng_mesh()
+    nn, ne = 5000, pp.shape[0]
+    A = rng.standard_normal(ne)
+    u = rng.standard_normal((nn, 2))
+    nodes = op2.op_decl_set(nn, "nodes")
+    edges = op2.op_decl_set(ne, "edges")
+    m = op2.op_decl_map(edges, nodes, 2, pp, "ppedge")
+    pA = op2.op_decl_dat(edges, 1, "double", A, "A")
+    pu = op2.op_decl_dat(nodes, 2, "double", u, "u")
+    pdu = op2.op_decl_dat(nodes, 2, "double", None, "du")
+    beta = np.array([0.75])
+    op2.op_par_loop("gen_scatter", edges,
+                    op2.op_arg_dat(pA, -1, op2.OP_ID, 1, "double", op2.OP_READ),
+                    op2.op_arg_dat(pu, 1, m, 2, "double", op2.OP_READ),
+                    op2.op_arg_dat(pdu, 0, m, 2, "double", op2.OP_INC),
+                    op2.op_arg_gbl(beta, 1, "double", op2.OP_READ),
+                    op2.op_arg_idx(-1, op2.OP_ID),
+                    op2.op_arg_idx(0, m))
+    ref = np.zeros((nn, 2))
+    e = np.arange(ne)
+    np.add.at(ref[:, 0], pp[:, 0], 0.75 * A * u[pp[:, 1], 0])
+    np.add.at(ref[:, 1], pp[:, 0], 0.75 * u[pp[:, 1], 1] - e + 0.5 * pp[:, 0])
+    got = op2.op_fetch_data(pdu)
+    scale = np.abs(ref).max(axis=0)
+    assert np.all(np.abs(got - ref).max(axis=0) <= 1e-12 * scale)
+
+
+def test_float_and_int_and_kernel_file_with_prelude(op2, tmp_path):
+    (tmp_path / "user_types.h").write_text(
+        "#include <math.h>\nstatic inline float gen_sq(float v) { return v * v; }\n")
+    (tmp_path / "gen_norm.h").write_text(
+        "inline void gen_norm(const float *x, float *y, int *cnt, int *top) {\n"
+        "  *y = sqrtf(gen_sq(x[0]) + gen_sq(x[1]));\n"
+        "  *cnt += 1;\n"
+        "  *top = (int)(*y) > *top ? (int)(*y) : *top;\n"
+        "}\n")
+    old = os.environ.get("OP2B_KERNEL_PATH")
+    os.environ["OP2B_KERNEL_PATH"] = str(tmp_path)
+    try:
+        rng = np.random.default_rng(2)
+        n = 7777
+        x = (rng.standard_normal((n, 2)) * 10).astype(np.float32)
+        s = op2.op_decl_set(n, "pts")
+        px = op2.op_decl_dat(s, 2, "float", x, "x")
+        py = op2.op_decl_dat(s, 1, "float", None, "y")
+        cnt = np.array([3], np.int32)
+        top = np.array([-5], np.int32)
+        op2.op_par_loop("gen_norm", s,
+                        op2.op_arg_dat(px, -1, op2.OP_ID, 2, "float", op2.OP_READ),
+                        op2.op_arg_dat(py, -1, op2.OP_ID, 1, "float", op2.OP_WRITE),
+                        op2.op_arg_gbl(cnt, 1, "int", op2.OP_INC),
+                        op2.op_arg_gbl(top, 1, "int", op2.OP_MAX))
+        y = np.sqrt(x[:, 0] * x[:, 0] + x[:, 1] * x[:, 1])
+        assert np.array_equal(op2.op_fetch_data(py)[:, 0], y)
+        assert cnt[0] == 3 + n and top[0] == int(y.astype(np.int32).max())
+    finally:
+        if old is None:
+            os.environ.pop("OP2B_KERNEL_PATH")
+        else:
+            os.environ["OP2B_KERNEL_PATH"] = old
+
+
+def test_unsupported_forms_and_compile_errors_are_reported(op2):
+    op2.register_kernel("gen_rw", "inline void gen_rw(double *v) { *v += 1.0; }\n")
+    op2.register_kernel("gen_bad", "inline void gen_bad(double *v) { *v = undeclared; }\n")
+    rng, pp = _rng_mesh(100, 300)
+    nodes = op2.op_decl_set(100, "nodes")
+    edges = op2.op_decl_set(300, "edges")
+    m = op2.op_decl_map(edges, nodes, 2, pp, "ppedge")
+    pv = op2.op_decl_dat(nodes, 1, "double", None, "v")
+    with pytest.raises(L.Op2Error, match="needs colouring"):
+        op2.op_par_loop("gen_rw", edges, op2.op_arg_dat(pv, 0, m, 1, "double", op2.OP_RW))
+    with pytest.raises(L.Op2Error, match="compiling the kernel failed"):
+        op2.op_par_loop("gen_bad", nodes, op2.op_arg_dat(pv, -1, op2.OP_ID, 1, "double",
+                                                         op2.OP_RW))
+    with pytest.raises(L.Op2Error, match="no device implementation"):
+        op2.op_par_loop("gen_missing", nodes, op2.op_arg_dat(pv, -1, op2.OP_ID, 1, "double",
+                                                             op2.OP_RW))
+
+
+def test_application_loop_sharing_an_airfoil_name(op2):
+    """An application's own 'update' (jac1's signature) is not Airfoil's: its
+    source is compiled and run instead of the hand-written update loop."""
+    op2.register_kernel("update", """
+inline void update(const double *r, double *du, double *u, int *index, double *u_sum,
+                   double *u_max) {
+  *u += *du + gen_alpha * (*r);
+  *du = 0.0f;
+  *u_sum += (*u) * (*u);
+  *u_max = (*u_max > *u) ? *u_max : *u;
+}
+""")
+    try:
+        rng = np.random.default_rng(3)
+        n = 4096
+        r_, du, u = (rng.standard_normal(n) for _ in range(3))
+        s = op2.op_decl_set(n, "nodes")
+        pr = op2.op_decl_dat(s, 1, "double", r_, "r")
+        pdu = op2.op_decl_dat(s, 1, "double", du, "du")
+        pu = op2.op_decl_dat(s, 1, "double", u, "u")
+        op2.op_decl_const(1, "double", 1.0, "gen_alpha")
+        usum = np.zeros(1)
+        umax = np.zeros(1)
+        op2.op_par_loop("update", s,
+                        op2.op_arg_dat(pr, -1, op2.OP_ID, 1, "double", op2.OP_READ),
+                        op2.op_arg_dat(pdu, -1, op2.OP_ID, 1, "double", op2.OP_RW),
+                        op2.op_arg_dat(pu, -1, op2.OP_ID, 1, "double", op2.OP_INC),
+                        op2.op_arg_idx(-1, op2.OP_ID),
+                        op2.op_arg_gbl(usum, 1, "double", op2.OP_INC),
+                        op2.op_arg_gbl(umax, 1, "double", op2.OP_MAX))
+        ref = u + (du + 1.0 * r_)  # *u += *du + alpha * (*r)
+        assert np.array_equal(op2.op_fetch_data(pu)[:, 0], ref)
+        assert np.all(op2.op_fetch_data(pdu) == 0)
+        assert abs(usum[0] - (ref * ref).sum()) <= 1e-12 * (ref * ref).sum()
+        assert umax[0] == max(0.0, ref.max())
+    finally:
+        op2.register_kernel("update", None)  # leave no source under an Airfoil name
