@@ -50,6 +50,7 @@ void set_error(const char *fmt, ...) {
   vsnprintf(buf, sizeof(buf), fmt, ap);
   va_end(ap);
   g_last_error = buf;
+  if (rt().quiet_errors) return;  // a tentative call: the caller decides
   if (rt().opt_diags > 0 || rt().opt_abort)
     fprintf(stderr, "op2b error: %s\n", buf);
   if (rt().opt_abort)

@@ -678,8 +678,16 @@ int op_par_loop_c(char const *name, op_set set, int nargs, op_arg *args) {
   }
   for (const Entry &e : kLoops)
     if (strcmp(e.name, name) == 0) {
+      // with a kernel source to fall back on, a signature mismatch is not
+      // reported: the application's own loop of that name runs instead
+      const bool fallback = jit_has_kernel(name);
+      r.quiet_errors = fallback;
       int rc = e.fn(name, set, nargs, args);
-      if (rc != kSigMismatch) return rc;
+      r.quiet_errors = false;
+      if (rc != kSigMismatch) {
+        if (rc != 0 && fallback) set_error("%s", op2b_last_error());  // report it now
+        return rc;
+      }
       // an application's own loop that shares a name with an Airfoil loop
       // but not its arguments: run its kernel source if it has one
       if (!jit_has_kernel(name)) return -1;

@@ -88,6 +88,7 @@ struct Runtime {
   int opt_pipe_hints = 0;     // register pipeline: evict-first hints on once-read streams
   int opt_plan_mode = 0;      // 0 = parallel block colouring, 1 = serial greedy (bit-exact)
   bool opt_check_plans = false;
+  bool quiet_errors = false;  // set_error records without printing or aborting
 
   std::vector<std::unique_ptr<op_set_core>> sets;
   std::vector<std::unique_ptr<op_map_core>> maps;

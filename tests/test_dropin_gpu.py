@@ -47,3 +47,29 @@ def test_reference_airfoil_app_runs_on_libop2b():
     assert txt[0].split() == [str(m.ncell), "4"]
     first = np.array([float(v) for v in txt[1].split()])
     assert np.allclose(first, st.q[0], rtol=1e-15, atol=0)
+
+
+@pytest.mark.skipif(not (O.ref_binary("jac1_dropin") and O.ref_binary("ref_jac1_seq")),
+                    reason="jac1 binaries not built")
+def test_reference_jac1_app_runs_on_libop2b():
+    """A second application: the reference's unmodified jac1 (apps/c/jac1/dp),
+    whose loops have no hand-written device kernel -- libop2b compiles its own
+    kernel headers at run time.  Its printed history (u max/rms per
+    iteration), its solution grid, its result check and the per-edge lines
+    its res kernel prints (in any order: they come from GPU threads) equal
+    those of the same application on the reference's sequential library."""
+    out = {}
+    for b in ("jac1_dropin", "ref_jac1_seq"):
+        with tempfile.TemporaryDirectory() as tmp:
+            r = subprocess.run([O.ref_binary(b)], cwd=tmp, capture_output=True, text=True,
+                               timeout=300)
+            assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+            out[b] = r.stdout
+    got, ref = out["jac1_dropin"], out["ref_jac1_seq"]
+    hist = lambda s: re.findall(r"u max/rms = ([0-9.]+) ([0-9.]+)", s)
+    grid = lambda s: re.findall(r"^(?:[ \t]+-?[0-9]+\.[0-9]{4}){5}[ \t]*$", s, flags=re.M)
+    edges = lambda s: sorted(re.findall(r"^edge \d+, nodes \d+, \d+$", s, flags=re.M))
+    assert hist(got) == hist(ref) and len(hist(ref)) == 2
+    assert grid(got) == grid(ref) and len(grid(ref)) == 5
+    assert edges(got) == edges(ref) and len(edges(ref)) == 210
+    assert "Results check PASSED" in got
