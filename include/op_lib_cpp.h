@@ -21,6 +21,14 @@
 #include "op2b.h"
 #include "op2b_plan.h"
 
+/* op2/include/op_lib_core.h:246-249 */
+#ifndef MIN
+#define MIN(a, b) ((a < b) ? (a) : (b))
+#endif
+#ifndef MAX
+#define MAX(a, b) ((a > b) ? (a) : (b))
+#endif
+
 typedef unsigned int uint;
 typedef long long ll;
 typedef unsigned long long ull;

@@ -18,15 +18,21 @@
 //     as the element's (or its target's) index, op_arg_gbl OP_READ from a
 //     device copy, OP_INC/MIN/MAX into per-thread partials reduced by warp
 //     shuffles and device atomics, then combined with the caller's value;
-//   * indirect OP_WRITE/OP_RW (which need colouring), vector map arguments,
-//     op_arg_info and switched-off optional arguments are rejected with an
-//     error, not run on the host;
+//   * a loop with an indirect OP_WRITE or OP_RW argument runs colour by
+//     colour over the device-built OP_COLOR2 plan (op_plan_get_stage, the
+//     reference's flat element colouring, op_rt_support.cpp:684-754), one
+//     launch per colour, so that no two elements of a launch share a target;
+//     the colouring covers indirect OP_INC, OP_RW and OP_WRITE arguments;
+//   * vector map arguments, op_arg_info and switched-off optional arguments
+//     are rejected with an error, not run on the host;
 //   * compiled with --fmad=false (each operation rounded once, like the
 //     reference's strictly compiled sequential build); modules are cached per
 //     loop signature and source until op_exit.
 // Summation order of OP_INC increments and gbl reductions is that of the
 // atomics, so results equal the sequential reference's to rounding, not bit
-// for bit (the hand-written Airfoil loops keep the reference's order).
+// for bit (the hand-written Airfoil loops keep the reference's order).  In a
+// coloured loop the indirect increments of one launch reach distinct
+// targets, so they are deterministic; only the gbl reductions are not.
 #include <cuda_runtime.h>
 #include <nvrtc.h>
 
@@ -42,7 +48,9 @@
 #include <string>
 #include <vector>
 
+#include "op2b_plan.h"
 #include "op2b_runtime.h"
+#include "plan.h"
 
 namespace op2b {
 namespace {
@@ -188,7 +196,8 @@ template <typename T> __device__ T op2b_min(T a, T b) { return b < a ? b : a; }
 template <typename T> __device__ T op2b_max(T a, T b) { return b > a ? b : a; }
 )";
 
-std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std::string &body) {
+std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std::string &body,
+                     bool coloured) {
   Runtime &r = rt();
   std::ostringstream s;
   s << "// libop2b: generated loop for the user kernel '" << name << "'\n";
@@ -198,6 +207,9 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
     if (kv.second.size() > 1) s << "[" << kv.second.size() << "]";
     s << ";\n";
   }
+  // the min/max macros kernels find in OP2's headers (op_lib_core.h:246-249)
+  s << "#ifndef MIN\n#define MIN(a, b) ((a < b) ? (a) : (b))\n#endif\n"
+       "#ifndef MAX\n#define MAX(a, b) ((a > b) ? (a) : (b))\n#endif\n";
   s << kHelpers << "\n" << body << "\n";
   s << "extern \"C\" __global__ void op2b_loop(int op2b_n";
   for (size_t i = 0; i < ap.size(); i++) {
@@ -206,6 +218,8 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
       s << ", " << a.ctype << " *op2b_d" << i;
     if (a.kind == INDIRECT || (a.kind == IDX && a.mdim > 0)) s << ", const int *op2b_m" << i;
   }
+  // coloured: this launch runs the elements op2b_perm[op2b_first, +op2b_n)
+  if (coloured) s << ", const int *op2b_perm, int op2b_first";
   s << ") {\n";
   for (size_t i = 0; i < ap.size(); i++) {
     const ArgPlan &a = ap[i];
@@ -213,8 +227,13 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
       s << "  " << a.ctype << " op2b_l" << i << "[" << a.dim << "];\n  for (int k = 0; k < "
         << a.dim << "; k++) op2b_l" << i << "[k] = " << identity(a.ctype, a.acc) << ";\n";
   }
-  s << "  for (int op2b_e = blockIdx.x * blockDim.x + threadIdx.x; op2b_e < op2b_n;"
-       " op2b_e += gridDim.x * blockDim.x) {\n";
+  if (coloured)
+    s << "  for (int op2b_i = blockIdx.x * blockDim.x + threadIdx.x; op2b_i < op2b_n;"
+         " op2b_i += gridDim.x * blockDim.x) {\n"
+         "    const int op2b_e = op2b_perm[op2b_first + op2b_i];\n";
+  else
+    s << "  for (int op2b_e = blockIdx.x * blockDim.x + threadIdx.x; op2b_e < op2b_n;"
+         " op2b_e += gridDim.x * blockDim.x) {\n";
   std::ostringstream call;
   call << "    " << name << "(";
   for (size_t i = 0; i < ap.size(); i++) {
@@ -364,9 +383,37 @@ void release_jit() {
   cache().clear();
 }
 
+// The OP_COLOR2 plan of a loop with indirect OP_WRITE/OP_RW arguments: every
+// indirect dat is one indirection (the reference's generated stubs number
+// them the same way), and OP_WRITE is planned as OP_RW so that the colouring,
+// which the reference restricts to OP_INC and OP_RW (op_rt_support.cpp:
+// 716-739), keeps writers of one target apart as well.
+const Plan *colour_plan(const char *name, op_set set, int nargs, const op_arg *args) {
+  std::vector<op_arg> pa(args, args + nargs);
+  std::vector<int> inds((size_t)nargs, -1);
+  std::vector<op_dat> seen;
+  for (int i = 0; i < nargs; i++) {
+    if (pa[(size_t)i].argtype != OP_ARG_DAT || pa[(size_t)i].map == nullptr) continue;
+    if (pa[(size_t)i].acc == OP_WRITE) pa[(size_t)i].acc = OP_RW;
+    auto it = std::find(seen.begin(), seen.end(), pa[(size_t)i].dat);
+    inds[(size_t)i] = (int)(it - seen.begin());
+    if (it == seen.end()) seen.push_back(pa[(size_t)i].dat);
+  }
+  const std::string pname = std::string(name) + "#coloured";
+  op_plan *o = op_plan_get_stage(pname.c_str(), set, 0, nargs, pa.data(), (int)seen.size(),
+                                 inds.data(), OP_COLOR2);
+  const Plan *pl = o ? find_plan(o) : nullptr;
+  if (!pl || !pl->col_reord_d || !o->color2_offsets) {
+    if (op2b_last_error()[0] == 0) set_error("op_par_loop(%s): colouring the loop failed", name);
+    return nullptr;
+  }
+  return pl;
+}
+
 int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
   Runtime &r = rt();
   std::vector<ArgPlan> ap((size_t)nargs);
+  bool coloured = false;
   std::ostringstream key;
   key << name;
   for (int i = 0; i < nargs; i++) {
@@ -399,12 +446,9 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
         }
         if (x.map->from != set || x.map->to != x.dat->set)
           return set_error("op_par_loop(%s): argument %d: map does not match the loop's set and the dat", name, i), -1;
-        if (x.acc != OP_READ && x.acc != OP_INC) {
-          set_error("op_par_loop(%s): argument %d: indirect %s needs colouring, which "
-                    "run-time compiled loops do not do; use OP_INC or OP_READ", name, i,
-                    x.acc == OP_WRITE ? "OP_WRITE" : "OP_RW");
-          return -1;
-        }
+        if (x.acc != OP_READ && x.acc != OP_INC && x.acc != OP_WRITE && x.acc != OP_RW)
+          return set_error("op_par_loop(%s): argument %d: indirect dats are OP_READ, OP_WRITE, OP_RW or OP_INC", name, i), -1;
+        coloured |= x.acc == OP_WRITE || x.acc == OP_RW;
         a.kind = INDIRECT;
         a.mdim = x.map->dim;
         a.idx = x.idx;
@@ -453,10 +497,13 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
   seen.push_back(std::string(name) + ".h");
   body += expand(ksrc, seen, 0);
   for (auto &kv : r.consts) key << "|c:" << kv.first << ":" << r.const_types[kv.first] << ":" << kv.second.size();
-  key << "|s:" << std::hash<std::string>()(body);
+  key << "|s:" << std::hash<std::string>()(body) << "|col:" << coloured;
+  // the colouring (built once per loop signature and cached with the plans)
+  const Plan *plan = nullptr;
+  if (coloured && set->size > 0 && !(plan = colour_plan(name, set, nargs, args))) return -1;
   Jit &j = cache()[key.str()];
   if (!j.fn) {
-    const std::string src = generate(name, ap, body);
+    const std::string src = generate(name, ap, body, coloured);
     if (!compile(name, src, j)) {
       cache().erase(key.str());
       return -1;
@@ -530,7 +577,20 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
     }
   }
   r.begin_loop(name);
-  if (n > 0) {
+  // one launch over the set, or one per colour over its slice of col_reord
+  const int ncol = plan ? plan->pub.ncolors : 1;
+  const int *perm = plan ? plan->col_reord_d : nullptr;
+  int first = 0;
+  if (plan) {
+    kp.push_back(&perm);
+    kp.push_back(&first);
+  }
+  for (int c = 0; c < ncol && set->size > 0; c++) {
+    if (plan) {
+      first = plan->pub.color2_offsets[c];
+      n = plan->pub.color2_offsets[c + 1] - first;
+    }
+    if (n <= 0) continue;
     unsigned grid = (unsigned)std::min<long long>(((long long)n + 255) / 256, (long long)r.nsm * 8);
     if (!cuda_ok(cudaLaunchKernel((const void *)j.fn, dim3(grid), dim3(256), kp.data(), 0,
                                   r.stream),
@@ -540,6 +600,7 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
     }
     r.launches++;
   }
+  n = set->size;
   r.end_loop(bytes);
   // reductions: combine with the caller's values once the loop has finished
   bool reduce = false;

@@ -838,6 +838,7 @@ Plan *build_plan(const char *name, op_set set, int part_size, int nargs, op_arg 
     long long *cb_d = dalloc<long long>(coloff_base.size(), own);
     cudaMemcpyAsync(cb_d, coloff_base.data(), sizeof(long long) * coloff_base.size(), cudaMemcpyHostToDevice, s);
     col_reord_d = dalloc<int>((size_t)exec_length + 16, own);
+    pl->col_reord_d = col_reord_d;
     col_offsets_d = dalloc<int>((size_t)acc, own);
     cudaMemsetAsync(col_reord_d, 0, sizeof(int) * ((size_t)exec_length + 16), s);
     k_plan_permute<<<(nblocks + 127) / 128, 128, 0, s>>>(p, pl->thrcol_d, pl->nthrcol_d, cb_d,

@@ -21,6 +21,7 @@ struct Plan {
   int *thrcol_d = nullptr, *nthrcol_d = nullptr, *blk_col_d = nullptr, *blkmap_d = nullptr;
   int *ind_map_d = nullptr, *ind_offs_d = nullptr, *ind_sizes_d = nullptr;
   short *loc_map_d = nullptr;
+  int *col_reord_d = nullptr;  // OP_STAGE_PERMUTE / OP_COLOR2: elements by thread colour
   std::vector<void *> owned;
   double build_ms = 0.0;
   int max_ind_size[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // per staged slot, max over blocks

@@ -207,6 +207,24 @@ def write_grid_dat(mesh: Mesh, path: str) -> None:
                                      axis=1), fmt="%d %d %d %d")
 
 
+def write_fe_grid_dat(mesh: Mesh, path: str) -> None:
+    """Write the mesh as the reference's aero application reads it from
+    FE_grid.dat (apps/c/aero/aero_plain/aero.cpp:79-117): a header
+    ``nnode ncell nbnodes``, ``x y`` per node, four node ids per cell in the
+    bilinear element's tensor order -- (0,0), (1,0), (0,1), (1,1), the order
+    its shape-function derivatives Ng2_xi assume -- and one id per boundary
+    node, ascending.  The boundary nodes (aero's Dirichlet set, where the
+    potential stays at its free-stream value) are the far-field ones (bound
+    2); the walls keep the natural no-flux condition, so the flow has to go
+    round the bump."""
+    bnode = np.unique(mesh.bedge[mesh.bound == 2].reshape(-1))
+    with open(path, "w") as f:
+        f.write(f"{mesh.nnode} {mesh.ncell} {bnode.size} \n")
+        np.savetxt(f, mesh.x, fmt="%.17g %.17g")
+        np.savetxt(f, mesh.cell[:, [0, 1, 3, 2]], fmt="%d %d %d %d")
+        np.savetxt(f, bnode, fmt="%d")
+
+
 def read_grid_dat(path: str) -> Mesh:
     with open(path) as f:
         nnode, ncell, nedge, nbedge = (int(v) for v in f.readline().split())

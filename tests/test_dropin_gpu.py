@@ -73,3 +73,78 @@ def test_reference_jac1_app_runs_on_libop2b():
     assert grid(got) == grid(ref) and len(grid(ref)) == 5
     assert edges(got) == edges(ref) and len(edges(ref)) == 210
     assert "Results check PASSED" in got
+
+
+@pytest.mark.skipif(not (O.ref_binary("jac2_dropin") and O.ref_binary("ref_jac2_seq")),
+                    reason="jac2 binaries not built")
+def test_reference_jac2_app_runs_on_libop2b():
+    """The reference's jac2 (apps/c/jac2): mixed float/double arguments, a
+    float constant, dats declared wider than the kernel uses (dims 2 and 3)
+    and OP2's MAX macro in the kernel.  History, solution grid and result
+    check equal those of its sequential build."""
+    out = {}
+    for b in ("jac2_dropin", "ref_jac2_seq"):
+        with tempfile.TemporaryDirectory() as tmp:
+            r = subprocess.run([O.ref_binary(b)], cwd=tmp, capture_output=True, text=True,
+                               timeout=300)
+            assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+            out[b] = r.stdout
+    got, ref = out["jac2_dropin"], out["ref_jac2_seq"]
+    hist = lambda s: re.findall(r"u max/rms = ([0-9.]+) ([0-9.]+)", s)
+    grid = lambda s: re.findall(r"^(?:[ \t]+-?[0-9]+\.[0-9]{4}){5}[ \t]*$", s, flags=re.M)
+    assert hist(got) == hist(ref) and len(hist(ref)) == 2
+    assert grid(got) == grid(ref) and len(grid(ref)) == 5
+    assert "Results check PASSED" in got
+
+
+@pytest.mark.skipif(not (O.ref_binary("reduction_dropin") and O.ref_binary("ref_reduction_seq")),
+                    reason="reduction binaries not built")
+def test_reference_reduction_app_runs_on_libop2b():
+    """The reference's reduction application (apps/c/reduction): an indirect
+    OP_INC loop and a direct OP_RW loop, each counting its set elements into
+    an int OP_INC global, on a new_grid.dat of 2.88k cells (its loops share
+    Airfoil's names, res_calc and update, with other signatures)."""
+    m = M.channel_bump(80, 36, seed=2)
+    out = {}
+    for b in ("reduction_dropin", "ref_reduction_seq"):
+        with tempfile.TemporaryDirectory() as tmp:
+            M.write_grid_dat(m, os.path.join(tmp, "new_grid.dat"))
+            r = subprocess.run([O.ref_binary(b)], cwd=tmp, capture_output=True, text=True,
+                               timeout=300)
+            assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+            out[b] = r.stdout
+    got, ref = out["reduction_dropin"], out["ref_reduction_seq"]
+    counts = lambda s: re.findall(r"number of (edges|cells):+ (\d+) should be: (\d+)", s)
+    assert counts(got) == counts(ref) and len(counts(ref)) == 2
+    assert "indirect reduction Passed" in got and "direct reduction Passed" in got
+    assert "Reduction application PASSED" in got
+
+
+@pytest.mark.skipif(not (O.ref_binary("aero_dropin") and O.ref_binary("ref_aero_seq")),
+                    reason="aero binaries not built")
+def test_reference_aero_app_runs_on_libop2b():
+    """The reference's aero application (apps/c/aero/aero_plain): a finite-
+    element potential-flow solver, Newton iterations of conjugate gradients,
+    nine loops among them an indirect OP_WRITE (dirichlet, run colour by
+    colour) and five global reductions per CG step.  On an FE_grid.dat of the
+    1800-cell channel with a bump: the same inner CG iteration counts while
+    the residual is well above rounding (the first five Newton steps), the
+    printed rms within 1e-6 relative there (the CG dot products sum in
+    another order), and both runs converged to below 1e-14 at the end."""
+    m = M.channel_bump(60, 30, seed=1)
+    out = {}
+    for b in ("aero_dropin", "ref_aero_seq"):
+        with tempfile.TemporaryDirectory() as tmp:
+            M.write_fe_grid_dat(m, os.path.join(tmp, "FE_grid.dat"))
+            r = subprocess.run([O.ref_binary(b)], cwd=tmp, capture_output=True, text=True,
+                               timeout=300)
+            assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+            out[b] = r.stdout
+    hist = lambda s: [(int(a), int(b), float(c)) for a, b, c in
+                      re.findall(r"^(\d+) (\d+) ([0-9.]+E[-+]\d+)$", s, flags=re.M)]
+    got, ref = hist(out["aero_dropin"]), hist(out["ref_aero_seq"])
+    assert len(got) == len(ref) == 20
+    for (i, n, r_), (j, k, s_) in zip(got[:5], ref[:5]):
+        assert i == j and n == k
+        assert abs(r_ - s_) <= 1e-6 * s_
+    assert got[-1][2] < 1e-14 and ref[-1][2] < 1e-14

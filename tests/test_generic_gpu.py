@@ -4,7 +4,9 @@ compiled at run time (NVRTC, sm_100a) into a generated loop, against numpy.
 Tolerances: direct arguments and OP_MIN/OP_MAX are exact (each element's
 arithmetic is the kernel's, compiled without FMA contraction, as numpy
 computes it); OP_INC increments and OP_INC globals are summed by atomics in
-no fixed order: within 1e-12 relative of the sequential sum.
+no fixed order: within 1e-12 relative of the sequential sum.  Loops with
+indirect OP_RW/OP_WRITE run colour by colour; their test sums integers, so
+any order is exact.
 """
 import os
 
@@ -153,14 +155,61 @@ def test_unsupported_forms_and_compile_errors_are_reported(op2):
     edges = op2.op_decl_set(300, "edges")
     m = op2.op_decl_map(edges, nodes, 2, pp, "ppedge")
     pv = op2.op_decl_dat(nodes, 1, "double", None, "v")
-    with pytest.raises(L.Op2Error, match="needs colouring"):
-        op2.op_par_loop("gen_rw", edges, op2.op_arg_dat(pv, 0, m, 1, "double", op2.OP_RW))
+    with pytest.raises(L.Op2Error, match="vector map arguments"):
+        op2.op_par_loop("gen_rw", edges, op2.op_arg_dat(pv, -2, m, 1, "double", op2.OP_READ))
     with pytest.raises(L.Op2Error, match="compiling the kernel failed"):
         op2.op_par_loop("gen_bad", nodes, op2.op_arg_dat(pv, -1, op2.OP_ID, 1, "double",
                                                          op2.OP_RW))
     with pytest.raises(L.Op2Error, match="no device implementation"):
         op2.op_par_loop("gen_missing", nodes, op2.op_arg_dat(pv, -1, op2.OP_ID, 1, "double",
                                                              op2.OP_RW))
+
+
+def test_indirect_rw_and_write_run_colour_by_colour(op2):
+    """Indirect OP_RW and OP_WRITE arguments: the loop runs one launch per
+    colour of the device-built OP_COLOR2 plan, so no two elements of a launch
+    share a target.  Integer-valued increments make any order exact."""
+    op2.register_kernel("gen_rw2", """
+inline void gen_rw2(double *a, double *b, const double *w, const int *e) {
+  *a += *w;
+  *b += 2.0 * (*w) + (*e % 3);
+}
+""")
+    op2.register_kernel("gen_pin", "inline void gen_pin(double *v, const int *i) { *v = 100.0 + *i; }\n")
+    rng, pp = _rng_mesh(3000, 12000, seed=4)
+    pp = pp[pp[:, 0] != pp[:, 1]]
+    nn, ne = 3000, pp.shape[0]
+    w = rng.integers(-50, 50, size=ne).astype(np.float64)
+    v0 = rng.integers(-1000, 1000, size=nn).astype(np.float64)
+    nodes = op2.op_decl_set(nn, "nodes")
+    edges = op2.op_decl_set(ne, "edges")
+    m = op2.op_decl_map(edges, nodes, 2, pp, "ppedge")
+    pv = op2.op_decl_dat(nodes, 1, "double", v0, "v")
+    pw = op2.op_decl_dat(edges, 1, "double", w, "w")
+    before = L.load().op2b_kernel_launches()
+    for _ in range(2):  # the second call reuses the cached colouring
+        op2.op_par_loop("gen_rw2", edges,
+                        op2.op_arg_dat(pv, 0, m, 1, "double", op2.OP_RW),
+                        op2.op_arg_dat(pv, 1, m, 1, "double", op2.OP_RW),
+                        op2.op_arg_dat(pw, -1, op2.OP_ID, 1, "double", op2.OP_READ),
+                        op2.op_arg_idx(-1, op2.OP_ID))
+    ref = v0.copy()
+    for _ in range(2):
+        np.add.at(ref, pp[:, 0], w)
+        np.add.at(ref, pp[:, 1], 2.0 * w + np.arange(ne) % 3)
+    assert np.array_equal(op2.op_fetch_data(pv)[:, 0], ref)
+    # one launch per colour; a colour needs at least the largest degree
+    deg = np.bincount(pp.reshape(-1), minlength=nn).max()
+    assert L.load().op2b_kernel_launches() - before >= 2 * deg
+    # indirect OP_WRITE through a one-to-one map (boundary pinning)
+    nb = 500
+    bn = rng.permutation(nn)[:nb].astype(np.int32)
+    bset = op2.op_decl_set(nb, "bnodes")
+    bm = op2.op_decl_map(bset, nodes, 1, bn.reshape(-1, 1), "pbnode")
+    op2.op_par_loop("gen_pin", bset, op2.op_arg_dat(pv, 0, bm, 1, "double", op2.OP_WRITE),
+                    op2.op_arg_idx(-1, op2.OP_ID))
+    ref[bn] = 100.0 + np.arange(nb)
+    assert np.array_equal(op2.op_fetch_data(pv)[:, 0], ref)
 
 
 def test_application_loop_sharing_an_airfoil_name(op2):
