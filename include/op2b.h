@@ -164,6 +164,16 @@ void op_timers(double *cpu, double *et);
 void op_timing_output(void);
 void op_diagnostic_output(void);
 void op_rank(int *rank);
+/* partitioning (op_lib_core.h:395-402): one rank owns every set, so these
+ * do nothing, as in the reference's single-node builds
+ * (op_dummy_singlenode.cpp:144-200); op_is_root returns 1. */
+void op_partition(const char *lib_name, const char *lib_routine, op_set prime_set,
+                  op_map prime_map, op_dat coords);
+void op_partition_ptr(const char *lib_name, const char *lib_routine, op_set prime_set,
+                      int *prime_map, double *coords);
+void op_partition_reverse(void);
+void op_partition_destroy(void);
+int op_is_root(void);
 /* op_printf (op_lib_core.h:289) and the allocation wrappers (op_lib_core.h:
  * 423-429): host memory, 64-byte aligned, for application code. */
 void op_printf(const char *format, ...);

@@ -14,9 +14,20 @@
 #ifndef OP2B_OP_LIB_CPP_H
 #define OP2B_OP_LIB_CPP_H
 
+/* the standard headers an application gets through the reference's
+ * op_lib_core.h:43-68 */
+#include <math.h>
+#include <stdarg.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <strings.h>
+
+#include <cstddef>
+#include <iostream>
+#include <limits>
+#include <stdexcept>
+#include <utility>
 
 #include "op2b.h"
 #include "op2b_plan.h"

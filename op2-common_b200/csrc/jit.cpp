@@ -169,6 +169,19 @@ std::string identity(const std::string &t, int acc) {
   return mn ? "2147483647" : "(-2147483647 - 1)";
 }
 
+// NVRTC has no C++ standard library: the std:: names kernels written for a
+// host compiler use (std::min in apps/c/min/min_direct.cpp:9-11, the math
+// functions), mapped onto the device's own.
+const char *kStd = R"(
+namespace std {
+template <typename T> __device__ const T &min(const T &a, const T &b) { return b < a ? b : a; }
+template <typename T> __device__ const T &max(const T &a, const T &b) { return a < b ? b : a; }
+using ::abs; using ::fabs; using ::sqrt; using ::cbrt; using ::pow; using ::exp; using ::log;
+using ::log10; using ::sin; using ::cos; using ::tan; using ::atan; using ::atan2; using ::tanh;
+using ::floor; using ::ceil; using ::fmin; using ::fmax; using ::hypot;
+}
+)";
+
 const char *kHelpers = R"(
 __device__ void op2b_amin(double *a, double v) {
   unsigned long long *p = (unsigned long long *)a, old = *p, as;
@@ -210,6 +223,7 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
   // the min/max macros kernels find in OP2's headers (op_lib_core.h:246-249)
   s << "#ifndef MIN\n#define MIN(a, b) ((a < b) ? (a) : (b))\n#endif\n"
        "#ifndef MAX\n#define MAX(a, b) ((a > b) ? (a) : (b))\n#endif\n";
+  s << kStd << "\n";
   s << kHelpers << "\n" << body << "\n";
   s << "extern \"C\" __global__ void op2b_loop(int op2b_n";
   for (size_t i = 0; i < ap.size(); i++) {

@@ -759,6 +759,15 @@ void op_rank(int *rank) {
   if (rank) *rank = 0;
 }
 
+// One rank owns every set: partitioning has nothing to do, as in the
+// reference's single-node builds (op2/src/core/op_dummy_singlenode.cpp:
+// 144-200).
+void op_partition(const char *, const char *, op_set, op_map, op_dat) {}
+void op_partition_ptr(const char *, const char *, op_set, int *, double *) {}
+void op_partition_reverse(void) {}
+void op_partition_destroy(void) {}
+int op_is_root(void) { return 1; }
+
 void op_timers(double *cpu, double *et) {
   using namespace std::chrono;
   double t = duration<double>(steady_clock::now().time_since_epoch()).count();

@@ -1,17 +1,34 @@
 """Test infrastructure: embed an OP2 application's kernel headers in a C++
 source that registers them with libop2b at start-up.
 
-  python embed_kernels.py OUT.cpp [prelude=PATH ...] [NAME=PATH ...]
+  python embed_kernels.py OUT.cpp [prelude=PATH ...] [NAME=PATH ...] [NAME=PATH#FUNC ...]
 
 The reference's applications keep each loop's kernel in a header named after
 it (apps/c/jac1/dp/res.h ...), which OP2's code generator turns into device
 code before the application is built.  For the drop-in checks, oracle/Makefile
 links the generated file into the unmodified application; its static
 initialiser hands the sources to op2b_register_prelude / op2b_register_kernel,
-and libop2b compiles each loop at its first call.  The output goes to
+and libop2b compiles each loop at its first call.  PATH#FUNC takes only the
+definition of function FUNC out of PATH, for applications that define their
+kernel in the main source (apps/c/min/min_direct.cpp).  The output goes to
 oracle/_ref/ (a build product, never committed).
 """
+import re
 import sys
+
+
+def function_text(src: str, func: str) -> str:
+    """The definition of `func` in `src`: from its return type to the brace
+    that closes its body."""
+    m = re.search(r"^[^\n;{}]*\b" + re.escape(func) + r"\s*\([^)]*\)\s*\{", src, flags=re.M)
+    if not m:
+        raise SystemExit(f"embed_kernels: no definition of {func}")
+    depth, i = 0, m.end() - 1
+    while True:
+        depth += {"{": 1, "}": -1}.get(src[i], 0)
+        i += 1
+        if depth == 0:
+            return src[m.start():i] + "\n"
 
 
 def c_bytes(data: bytes) -> str:
@@ -23,8 +40,12 @@ def main(argv):
     lines = ['#include "op2b.h"', ""]
     regs = []
     for k, (name, path) in enumerate(items):
+        path, _, func = path.partition("#")
         with open(path, "rb") as f:
-            lines.append(f"static const char op2b_src_{k}[] = {{{c_bytes(f.read())}}};")
+            data = f.read()
+        if func:
+            data = function_text(data.decode(), func).encode()
+        lines.append(f"static const char op2b_src_{k}[] = {{{c_bytes(data)}}};")
         if name == "prelude":
             regs.append(f"    op2b_register_prelude(op2b_src_{k});")
         else:

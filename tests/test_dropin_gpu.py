@@ -148,3 +148,17 @@ def test_reference_aero_app_runs_on_libop2b():
         assert i == j and n == k
         assert abs(r_ - s_) <= 1e-6 * s_
     assert got[-1][2] < 1e-14 and ref[-1][2] < 1e-14
+
+
+@pytest.mark.parametrize("app", ["min_direct", "min_indirect"])
+def test_reference_min_apps_run_on_libop2b(app):
+    """The reference's min applications (apps/c/min): an int OP_MIN global
+    over a direct and over an indirect argument, their kernel defined in the
+    application source.  Each checks its own result and exits 1 on a wrong
+    minimum."""
+    b = O.ref_binary(f"{app}_dropin")
+    if not b:
+        pytest.skip(f"{app} binary not built")
+    r = subprocess.run([b], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+    assert re.search(r"^min: 5 \(expected: 5\)$", r.stdout, flags=re.M)
