@@ -83,6 +83,9 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-variants", action="store_true")
     p.add_argument("--cpu-iters", type=int, default=4)
+    p.add_argument("--option", action="append", default=[], metavar="KEY=VALUE",
+                   help="a library option (op2b_set_option) for the timed runs and the "
+                        "end-to-end job; repeatable")
     return p.parse_args()
 
 
@@ -297,6 +300,9 @@ def main():
 
     # ---------------------------------------------------------- device-resident timing
     gopts = {"gather_kernel": args.gather_kernel, "pipe_block": args.pipe_block}
+    for kv in args.option:
+        k, _, v = kv.partition("=")
+        gopts[k] = int(v)
     main_run = timed_run(L, Airfoil, m, dtype, args.numbering, args.inc_mode, args.part_size,
                          args.steps, args.warmup, torch, barrier, Clocks(local), opts=gopts)
     ms = max_over_ranks(main_run["ms"])

@@ -74,8 +74,12 @@ typedef struct op_map_core {
 } op_map_core;
 typedef op_map_core *op_map;
 
-/* op_dat_core: op2/include/op_lib_core.h:164-179.  `data` is NULL unless
- * the host copy was requested; data_d is the device array. */
+/* op_dat_core: op2/include/op_lib_core.h:164-179.  data_d is the device
+ * array.  `data` is a host copy of the values as declared (zeros for a NULL
+ * source), as the reference's op_decl_dat keeps one, in the current
+ * numbering (op_renumber reorders it with the device copy); loops run on the
+ * device and leave it as it was -- op_fetch_data returns current values.
+ * With the option host_mirror = 0 it is NULL. */
 typedef struct op_dat_core {
   int index;
   op_set set;

@@ -32,6 +32,8 @@
 #include <memory>
 #include <string>
 #include <thread>
+
+#include <sys/mman.h>
 #include <vector>
 
 namespace op2b {
@@ -83,6 +85,49 @@ static void host_copy(void *dst, const void *src, size_t bytes) {
   }
   memcpy(dst, src, std::min(chunk, bytes));
   for (auto &t : th) t.join();
+}
+
+bool download_host(void *dst, const void *src_d, size_t bytes, const char *what) {
+  Runtime &r = rt();
+  const size_t kChunk = (size_t)16 << 20;
+  if (bytes <= kChunk) {
+    return cuda_ok(cudaMemcpyAsync(dst, src_d, bytes, cudaMemcpyDeviceToHost, r.stream), what) &&
+           cuda_ok(cudaStreamSynchronize(r.stream), what);
+  }
+  if (!r.stage) {
+    if (!cuda_ok(cudaHostAlloc((void **)&r.stage, 2 * kChunk, cudaHostAllocDefault), what))
+      return false;
+    for (auto &e : r.stage_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+  }
+  // chunk k goes through buffer k % 2: the copy of chunk i + 1 is under way
+  // while the host threads empty buffer i % 2
+  const size_t n = (bytes + kChunk - 1) / kChunk;
+  auto issue = [&](size_t k) {
+    const size_t off = k * kChunk, len = std::min(kChunk, bytes - off);
+    return cuda_ok(cudaMemcpyAsync(r.stage + (k % 2) * kChunk, (const char *)src_d + off, len,
+                                   cudaMemcpyDeviceToHost, r.stream),
+                   what) &&
+           cuda_ok(cudaEventRecord(r.stage_ev[k % 2], r.stream), what);
+  };
+  if (!issue(0)) return false;
+  for (size_t i = 0; i < n; i++) {
+    if (i + 1 < n && !issue(i + 1)) return false;
+    if (!cuda_ok(cudaEventSynchronize(r.stage_ev[i % 2]), what)) return false;
+    const size_t off = i * kChunk;
+    host_copy((char *)dst + off, r.stage + (i % 2) * kChunk, std::min(kChunk, bytes - off));
+  }
+  return true;
+}
+
+// Host memory for large copies: 2 MiB aligned with a transparent-huge-page
+// hint, so that filling it takes few page faults (free() releases it).
+static void *host_alloc(size_t bytes) {
+  const size_t kHuge = (size_t)2 << 20;
+  if (bytes < 2 * kHuge) return malloc(bytes);
+  void *p = nullptr;
+  if (posix_memalign(&p, kHuge, bytes) != 0) return nullptr;
+  madvise(p, (bytes + kHuge - 1) & ~(kHuge - 1), MADV_HUGEPAGE);
+  return p;
 }
 
 static char *copy_str(const char *s) {
@@ -315,6 +360,12 @@ void op_exit(void) {
   cudaFree(r.check_d);
   r.check_d = nullptr;
   cudaFreeHost(r.pinned);
+  cudaFreeHost(r.stage);
+  r.stage = nullptr;
+  for (auto &e : r.stage_ev) {
+    if (e) cudaEventDestroy(e);
+    e = nullptr;
+  }
   cudaStreamSynchronize(r.own_stream);
   cudaStreamDestroy(r.own_stream);
   cudaMemPool_t pool;  // give the pooled setup memory back
@@ -324,6 +375,7 @@ void op_exit(void) {
   r.stream = r.own_stream = nullptr;
   r.stats.clear();
   r.exposed.clear();
+  r.zero_mirror.clear();
   r.launches = 0;
   r.initialised = false;
   // options return to their defaults: a later op_init starts from a clean state
@@ -342,6 +394,7 @@ void op_exit(void) {
   r.opt_adt_minb = d.opt_adt_minb;
   r.opt_fuse = d.opt_fuse;
   r.opt_speculate = d.opt_speculate;
+  r.opt_host_mirror = d.opt_host_mirror;
   r.pend = PendingLoop{};
   r.opt_pipe_block = d.opt_pipe_block;
   r.opt_pipe_hints = d.opt_pipe_hints;
@@ -482,14 +535,30 @@ op_dat op_decl_dat_char(op_set set, int dim, char const *type, int type_size, ch
     // record and 16/32-byte vector access stays in bounds
     size_t alloc = (bytes + 255) & ~(size_t)255;
     if (!cuda_ok(cudaMalloc((void **)&d->data_d, alloc), "op_decl_dat: cudaMalloc")) return nullptr;
+    // the host copy behind dat->data, as op_decl_dat_core keeps one
+    // (op_lib_core.cpp:581-680; zeros for a NULL source), taken by host
+    // threads while this one uploads the same source
+    std::thread mirror;
+    if (r.opt_host_mirror) {
+      d->data = (char *)(data ? host_alloc(bytes) : calloc(bytes, 1));
+      if (!d->data) {
+        cudaFree(d->data_d);
+        set_error("op_decl_dat: out of host memory for data %s", d->name);
+        return nullptr;
+      }
+      if (data) mirror = std::thread([&] { host_copy(d->data, data, bytes); });
+    }
     cudaError_t e = data ? cudaMemcpyAsync(d->data_d, data, bytes, cudaMemcpyHostToDevice, r.stream)
                          : cudaMemsetAsync(d->data_d, 0, alloc, r.stream);
-    if (!cuda_ok(e, "op_decl_dat: upload") ||
-        !cuda_ok(cudaStreamSynchronize(r.stream), "op_decl_dat: upload")) {
+    if (e == cudaSuccess) e = cudaStreamSynchronize(r.stream);
+    if (mirror.joinable()) mirror.join();
+    if (!cuda_ok(e, "op_decl_dat: upload")) {
       cudaFree(d->data_d);
+      free(d->data);
       return nullptr;
     }
   }
+  if (d->data && !data) r.zero_mirror.insert(d.get());
   r.dats.push_back(std::move(d));
   return r.dats.back().get();
 }
@@ -505,6 +574,7 @@ int op_free_dat_temp_char(op_dat dat) {
   // forget the learned arguments (flush_quiet put adt back), keep the buffer
   r.spec = SpecAdt{nullptr, nullptr, nullptr, nullptr, 0, false, r.spec.shadow,
                    r.spec.shadow_bytes};
+  r.zero_mirror.erase(dat);
   for (auto &d : r.dats)
     if (d.get() == dat) {
       cudaStreamSynchronize(r.stream);
@@ -899,6 +969,8 @@ int op2b_set_option(const char *key, long value) {
     r.opt_adt_minb = (int)value;
   } else if (k == "check_plans") {
     r.opt_check_plans = value != 0;
+  } else if (k == "host_mirror") {
+    r.opt_host_mirror = value != 0;
   } else {
     set_error("op2b_set_option: unknown option '%s'", k.c_str());
     return -1;
@@ -925,6 +997,7 @@ long op2b_get_option(const char *key) {
   if (k == "adt_minblocks") return r.opt_adt_minb;
   if (k == "fuse") return r.opt_fuse;
   if (k == "speculate_adt") return r.opt_speculate;
+  if (k == "host_mirror") return r.opt_host_mirror;
   if (k == "nsm") return r.nsm;
   return -1;
 }

@@ -84,6 +84,7 @@ struct Runtime {
   int opt_fuse = 1;           // defer save_soln / res_calc to fuse them with the next loop
   int opt_speculate = 1;      // update also computes the next adt_calc's result (SpecAdt)
   int opt_adt_minb = 0;       // adt_calc: __launch_bounds__ minimum blocks (0 = none)
+  int opt_host_mirror = 1;    // op_dat::data holds a host copy of the declared values
   int opt_pipe_block = 256;   // threads per CTA of the pipelined gather (64, 96, 128, 256)
   int opt_pipe_hints = 0;     // register pipeline: evict-first hints on once-read streams
   int opt_plan_mode = 0;      // 0 = parallel block colouring, 1 = serial greedy (bit-exact)
@@ -103,6 +104,8 @@ struct Runtime {
   void *red_base = nullptr;
   void *pinned = nullptr;      // 4 KiB mapped pinned host page for reduction read-back
   void *pinned_dev = nullptr;  // its device address
+  char *stage = nullptr;       // 2 x 16 MiB pinned buffers for large device -> host copies
+  cudaEvent_t stage_ev[2] = {nullptr, nullptr};
   long long red_seq = 0;       // sequence number of the last update launch
   unsigned long long *check_d = nullptr;  // device word for op_decl_map's range check
 
@@ -116,6 +119,7 @@ struct Runtime {
   PendingLoop pend;
   SpecAdt spec;
   std::set<op_dat> exposed;  // dats whose device pointer was handed out (no speculation)
+  std::set<op_dat> zero_mirror;  // dats declared without data: their host copy is zeros
 
   LaunchCtx ctx();
   // initialised, with any deferred loop launched (false on error)
@@ -132,6 +136,9 @@ struct Runtime {
 Runtime &rt();
 void set_error(const char *fmt, ...);
 bool cuda_ok(cudaError_t e, const char *what);
+// Device -> pageable host copy on the library stream, through pinned buffers
+// with the host-side copies spread over threads (synchronous).
+bool download_host(void *dst, const void *src_d, size_t bytes, const char *what);
 int type_bytes(const char *type);
 bool is_real(const char *type, int bytes);
 

@@ -1,17 +1,19 @@
 """Test infrastructure: embed an OP2 application's kernel headers in a C++
 source that registers them with libop2b at start-up.
 
-  python embed_kernels.py OUT.cpp [prelude=PATH ...] [NAME=PATH ...] [NAME=PATH#FUNC ...]
+  python embed_kernels.py OUT.cpp [prelude=PATH ...] [NAME=PATH ...] [loops=PATH ...]
 
 The reference's applications keep each loop's kernel in a header named after
 it (apps/c/jac1/dp/res.h ...), which OP2's code generator turns into device
 code before the application is built.  For the drop-in checks, oracle/Makefile
 links the generated file into the unmodified application; its static
 initialiser hands the sources to op2b_register_prelude / op2b_register_kernel,
-and libop2b compiles each loop at its first call.  PATH#FUNC takes only the
-definition of function FUNC out of PATH, for applications that define their
-kernel in the main source (apps/c/min/min_direct.cpp).  The output goes to
-oracle/_ref/ (a build product, never committed).
+and libop2b compiles each loop at its first call.  loops=PATH is for
+programs that define their kernels in the main source (apps/c/min,
+tests/functional/*): the definitions of every kernel an op_par_loop in PATH
+names become one prelude (a kernel may call another), and each loop name is
+registered as defined there.  The output goes to oracle/_ref/ (a build
+product, never committed).
 """
 import re
 import sys
@@ -40,13 +42,18 @@ def main(argv):
     lines = ['#include "op2b.h"', ""]
     regs = []
     for k, (name, path) in enumerate(items):
-        path, _, func = path.partition("#")
         with open(path, "rb") as f:
             data = f.read()
-        if func:
-            data = function_text(data.decode(), func).encode()
+        if name == "loops":
+            src = data.decode()
+            loops = list(dict.fromkeys(re.findall(r"\bop_par_loop\s*\(\s*(\w+)\s*,", src)))
+            data = "".join(function_text(src, f) for f in loops).encode()
         lines.append(f"static const char op2b_src_{k}[] = {{{c_bytes(data)}}};")
-        if name == "prelude":
+        if name == "loops":
+            regs.append(f"    op2b_register_prelude(op2b_src_{k});")
+            regs += [f'    op2b_register_kernel("{f}", "/* defined in the prelude */");'
+                     for f in loops]
+        elif name == "prelude":
             regs.append(f"    op2b_register_prelude(op2b_src_{k});")
         else:
             regs.append(f'    op2b_register_kernel("{name}", op2b_src_{k});')

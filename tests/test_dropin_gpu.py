@@ -162,3 +162,24 @@ def test_reference_min_apps_run_on_libop2b(app):
     r = subprocess.run([b], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
     assert re.search(r"^min: 5 \(expected: 5\)$", r.stdout, flags=re.M)
+
+
+@pytest.mark.parametrize("name", ["const", "gbl", "idx", "stride", "reduc"])
+def test_reference_functional_tests_run_on_libop2b(name):
+    """The reference's C++ functional tests (tests/functional/const, gbl,
+    idx, strides, dat_reductions), unmodified: constants of dims 1 and 4,
+    OP_READ/INC/MIN/MAX globals of dims 1 and 5, op_arg_idx direct and
+    through two maps, dats of dim 5 written by a kernel that calls another,
+    direct and indirect OP_INC of float dats.  Each checks itself (exit 1 on
+    a failure); the checks it reports passed equal the sequential build's."""
+    got, ref = O.ref_binary(f"functional_{name}_tests_dropin"), \
+        O.ref_binary(f"ref_functional_{name}_tests_seq")
+    if not (got and ref):
+        pytest.skip("functional test binaries not built")
+    out = {}
+    for b in (got, ref):
+        with tempfile.TemporaryDirectory() as tmp:
+            r = subprocess.run([b], cwd=tmp, capture_output=True, text=True, timeout=300)
+            assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+            out[b] = [ln for ln in r.stdout.splitlines() if "passed" in ln.lower()]
+    assert out[got] == out[ref] and len(out[ref]) >= 2

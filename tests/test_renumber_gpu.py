@@ -8,6 +8,8 @@ op_renumber.cpp:72-151).  Renumbering must not change the solution: 100
 iterations on the renumbered mesh, fetched in the original order, match the
 reference's golden rms and fields within the parity tolerances.
 """
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -43,6 +45,43 @@ def test_permutations_match_restatement(op2, I, J, seed):
     expect = np.empty_like(m.ecell)
     expect[pe] = pc[m.ecell]
     assert np.array_equal(cur, expect)
+
+
+def _host_copy(dat, n, dim, dtype):
+    d = dat.contents
+    if not d.data:
+        return None
+    return np.ctypeslib.as_array(ctypes.cast(d.data, ctypes.POINTER(np.ctypeslib.as_ctypes_type(dtype))),
+                                 shape=(n * dim,)).reshape(n, dim).copy()
+
+
+def test_host_copy_of_dats_follows_declaration_and_renumbering(op2):
+    """op_dat::data holds the declared values (zeros for a NULL source), as
+    the reference's op_decl_dat keeps them, and op_renumber reorders it with
+    the device copy and the maps' host copies (op_renumber.cpp:180-200)."""
+    m = M.channel_bump(64, 32, seed=5)
+    app = Airfoil(m)
+    x0 = _host_copy(app.p_x, m.nnode, 2, np.float64)
+    assert np.array_equal(x0, m.x)
+    assert np.all(_host_copy(app.p_res, m.ncell, 4, np.float64) == 0)
+    app.renumber()
+    pn = L.set_permutation(app.nodes)  # pn[i] = current index of declared node i
+    x1 = _host_copy(app.p_x, m.nnode, 2, np.float64)
+    expect = np.empty_like(m.x)
+    expect[pn] = m.x
+    assert np.array_equal(x1, expect)
+    assert np.array_equal(L.op_fetch_data(app.p_x), expect)  # the current numbering
+
+
+def test_host_copy_can_be_switched_off(op2):
+    L.set_option("host_mirror", 0)
+    try:
+        s = L.op_decl_set(10, "s")
+        d = L.op_decl_dat(s, 2, "double", np.ones((10, 2)), "d")
+        assert not d.contents.data
+        assert np.all(L.op_fetch_data(d) == 1.0)
+    finally:
+        L.set_option("host_mirror", 1)
 
 
 @pytest.mark.parametrize("mode", [L.OP2B_INC_ATOMIC, L.OP2B_INC_COLOR, L.OP2B_INC_HYBRID,
