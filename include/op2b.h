@@ -118,9 +118,18 @@ op_set op_decl_set(int size, char const *name);
 op_map op_decl_map(op_set from, op_set to, int dim, int *imap, char const *name);
 op_dat op_decl_dat_char(op_set set, int dim, char const *type, int type_size,
                         char *data, char const *name);
+/* op_decl_dat_temp_char fails (NULL) if a dat of the same set, dim, type and
+ * name exists (op_lib_core.cpp:638-651); op_free_dat_temp_char returns 1
+ * when it freed the dat, -1 otherwise (:653-680). */
 op_dat op_decl_dat_temp_char(op_set set, int dim, char const *type,
                              int type_size, char const *name);
 int op_free_dat_temp_char(op_dat dat);
+/* op_lib_c.h:85-86, op_lib_core.cpp:581-636: a dat on `set` sharing the
+ * storage of `dat` (or of the dat declared from the array `dat`), host copy
+ * and device array; `set` may not be larger than the dat's set.  op_renumber
+ * refuses to run while overlays exist. */
+op_dat op_decl_dat_overlay(op_set set, op_dat dat);
+op_dat op_decl_dat_overlay_ptr(op_set set, char *dat);
 void op_decl_const_char(int dim, char const *type, int type_size, char *dat,
                         char const *name);
 

@@ -125,12 +125,15 @@ std::string expand(const std::string &src, std::vector<std::string> &seen, int d
   return out.str();
 }
 
-enum ArgKind { DIRECT, INDIRECT, GBL, IDX };
+// OFF: an optional argument switched off (op_opt_arg_dat / op_opt_arg_gbl
+// with opt = 0): the kernel gets a pointer to zeroed scratch it must not use.
+enum ArgKind { DIRECT, INDIRECT, GBL, IDX, OFF };
 
 struct ArgPlan {
   ArgKind kind;
   std::string ctype;
   int dim = 1, acc = OP_READ, mdim = 0, idx = -1, bytes = 8;
+  int vec = 0;  // vector map argument (idx = -vec): the kernel gets vec pointers
 };
 
 std::string base_type(const char *t) {
@@ -183,6 +186,15 @@ using ::floor; using ::ceil; using ::fmin; using ::fmax; using ::hypot;
 )";
 
 const char *kHelpers = R"(
+// a vector map argument's pointer array, passed to a kernel parameter
+// declared T ** or const T ** (op_seq.h hands the kernel a T ** it typed
+// from the kernel's own signature)
+template <typename T> struct op2b_vec {
+  T **p;
+  __device__ operator T **() const { return p; }
+  __device__ operator const T **() const { return (const T **)p; }
+  __device__ operator const T *const *() const { return p; }
+};
 __device__ void op2b_amin(double *a, double v) {
   unsigned long long *p = (unsigned long long *)a, old = *p, as;
   do { as = old; if (__longlong_as_double((long long)as) <= v) return;
@@ -228,7 +240,7 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
   s << "extern \"C\" __global__ void op2b_loop(int op2b_n";
   for (size_t i = 0; i < ap.size(); i++) {
     const ArgPlan &a = ap[i];
-    if (a.kind == DIRECT || a.kind == INDIRECT || a.kind == GBL)
+    if (a.kind == DIRECT || a.kind == INDIRECT || a.kind == GBL || a.kind == OFF)
       s << ", " << a.ctype << " *op2b_d" << i;
     if (a.kind == INDIRECT || (a.kind == IDX && a.mdim > 0)) s << ", const int *op2b_m" << i;
   }
@@ -257,7 +269,32 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
       case DIRECT:
         call << "op2b_d" << i << " + (size_t)op2b_e * " << a.dim;
         break;
+      case OFF:
+        if (a.vec) {
+          s << "    " << a.ctype << " *op2b_v" << i << "[" << a.vec << "];\n    for (int j = 0; j < "
+            << a.vec << "; j++) op2b_v" << i << "[j] = op2b_d" << i << ";\n";
+          call << "op2b_vec<" << a.ctype << ">{op2b_v" << i << "}";
+        } else {
+          call << "op2b_d" << i;
+        }
+        break;
       case INDIRECT:
+        if (a.vec) {
+          // one pointer per map entry (op_seq.h op_arg_copy_in); increments
+          // into locals added atomically after the call
+          s << "    " << a.ctype << " *op2b_v" << i << "[" << a.vec << "];\n";
+          if (a.acc == OP_INC)
+            s << "    " << a.ctype << " op2b_l" << i << "[" << a.vec * a.dim << "];\n"
+              << "    for (int k = 0; k < " << a.vec * a.dim << "; k++) op2b_l" << i << "[k] = 0;\n";
+          s << "    for (int j = 0; j < " << a.vec << "; j++) op2b_v" << i << "[j] = ";
+          if (a.acc == OP_INC)
+            s << "op2b_l" << i << " + j * " << a.dim << ";\n";
+          else
+            s << "op2b_d" << i << " + (size_t)op2b_m" << i << "[(size_t)op2b_e * " << a.mdim
+              << " + j] * " << a.dim << ";\n";
+          call << "op2b_vec<" << a.ctype << ">{op2b_v" << i << "}";
+          break;
+        }
         s << "    const int op2b_t" << i << " = op2b_m" << i << "[(size_t)op2b_e * " << a.mdim
           << " + " << a.idx << "];\n";
         if (a.acc == OP_INC) {
@@ -286,7 +323,12 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
   s << call.str();
   for (size_t i = 0; i < ap.size(); i++) {
     const ArgPlan &a = ap[i];
-    if (a.kind == INDIRECT && a.acc == OP_INC)
+    if (a.kind == INDIRECT && a.acc == OP_INC && a.vec)
+      s << "    for (int j = 0; j < " << a.vec << "; j++) {\n      const size_t t = (size_t)op2b_m"
+        << i << "[(size_t)op2b_e * " << a.mdim << " + j] * " << a.dim << ";\n"
+        << "      for (int k = 0; k < " << a.dim << "; k++) atomicAdd(op2b_d" << i
+        << " + t + k, op2b_l" << i << "[j * " << a.dim << " + k]);\n    }\n";
+    else if (a.kind == INDIRECT && a.acc == OP_INC)
       s << "    for (int k = 0; k < " << a.dim << "; k++) atomicAdd(op2b_d" << i
         << " + (size_t)op2b_t" << i << " * " << a.dim << " + k, op2b_l" << i << "[k]);\n";
   }
@@ -403,19 +445,33 @@ void release_jit() {
 // which the reference restricts to OP_INC and OP_RW (op_rt_support.cpp:
 // 716-739), keeps writers of one target apart as well.
 const Plan *colour_plan(const char *name, op_set set, int nargs, const op_arg *args) {
-  std::vector<op_arg> pa(args, args + nargs);
-  std::vector<int> inds((size_t)nargs, -1);
+  // the plan sees one argument per map entry a vector argument reaches, and
+  // none for a switched-off one
+  std::vector<op_arg> pa;
+  std::vector<int> inds;
   std::vector<op_dat> seen;
   for (int i = 0; i < nargs; i++) {
-    if (pa[(size_t)i].argtype != OP_ARG_DAT || pa[(size_t)i].map == nullptr) continue;
-    if (pa[(size_t)i].acc == OP_WRITE) pa[(size_t)i].acc = OP_RW;
-    auto it = std::find(seen.begin(), seen.end(), pa[(size_t)i].dat);
-    inds[(size_t)i] = (int)(it - seen.begin());
-    if (it == seen.end()) seen.push_back(pa[(size_t)i].dat);
+    op_arg x = args[i];
+    if (x.argtype == OP_ARG_DAT && !x.opt) continue;
+    if (x.argtype != OP_ARG_DAT || x.map == nullptr) {
+      pa.push_back(x);
+      inds.push_back(-1);
+      continue;
+    }
+    if (x.acc == OP_WRITE) x.acc = OP_RW;
+    auto it = std::find(seen.begin(), seen.end(), x.dat);
+    const int ind = (int)(it - seen.begin());
+    if (it == seen.end()) seen.push_back(x.dat);
+    const int k = x.idx < -1 ? -x.idx : 1;
+    for (int j = 0; j < k; j++) {
+      if (k > 1) x.idx = j;
+      pa.push_back(x);
+      inds.push_back(ind);
+    }
   }
   const std::string pname = std::string(name) + "#coloured";
-  op_plan *o = op_plan_get_stage(pname.c_str(), set, 0, nargs, pa.data(), (int)seen.size(),
-                                 inds.data(), OP_COLOR2);
+  op_plan *o = op_plan_get_stage(pname.c_str(), set, 0, (int)pa.size(), pa.data(),
+                                 (int)seen.size(), inds.data(), OP_COLOR2);
   const Plan *pl = o ? find_plan(o) : nullptr;
   if (!pl || !pl->col_reord_d || !o->color2_offsets) {
     if (op2b_last_error()[0] == 0) set_error("op_par_loop(%s): colouring the loop failed", name);
@@ -433,10 +489,16 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
   for (int i = 0; i < nargs; i++) {
     const op_arg &x = args[i];
     ArgPlan &a = ap[(size_t)i];
-    if (!x.opt) {
-      set_error("op_par_loop(%s): argument %d: optional arguments that are switched off are "
-                "not supported for run-time compiled loops", name, i);
-      return -1;
+    if (!x.opt && (x.argtype == OP_ARG_DAT || x.argtype == OP_ARG_GBL)) {
+      // switched off: typed scratch of the argument's shape
+      a.kind = OFF;
+      a.ctype = base_type(x.argtype == OP_ARG_DAT && x.dat ? x.dat->type : x.type);
+      a.bytes = type_size(a.ctype);
+      if (!a.bytes) a.ctype = "double", a.bytes = 8;
+      a.dim = std::max(x.argtype == OP_ARG_DAT && x.dat ? x.dat->dim : x.dim, 1);
+      a.vec = x.argtype == OP_ARG_DAT && x.map && x.idx < -1 ? -x.idx : 0;
+      key << "|off:" << a.ctype << ":" << a.dim << ":" << a.vec;
+      continue;
     }
     if (x.argtype == OP_ARG_DAT) {
       if (!x.dat) return set_error("op_par_loop(%s): argument %d: no dat", name, i), -1;
@@ -453,11 +515,12 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
         if (x.dat->set != set) return set_error("op_par_loop(%s): argument %d: dat is not on the loop's set", name, i), -1;
         a.kind = DIRECT;
       } else {
-        if (x.idx < 0 || x.idx >= x.map->dim) {
-          set_error("op_par_loop(%s): argument %d: map index %d (vector map arguments are not "
-                    "supported for run-time compiled loops)", name, i, x.idx);
+        if (x.idx >= x.map->dim || x.idx == -1 || -x.idx > x.map->dim) {
+          set_error("op_par_loop(%s): argument %d: map index %d does not fit a map of dimension "
+                    "%d", name, i, x.idx, x.map->dim);
           return -1;
         }
+        a.vec = x.idx < -1 ? -x.idx : 0;
         if (x.map->from != set || x.map->to != x.dat->set)
           return set_error("op_par_loop(%s): argument %d: map does not match the loop's set and the dat", name, i), -1;
         if (x.acc != OP_READ && x.acc != OP_INC && x.acc != OP_WRITE && x.acc != OP_RW)
@@ -492,7 +555,7 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
       return -1;
     }
     key << "|" << a.kind << ":" << a.ctype << ":" << a.dim << ":" << a.acc << ":" << a.mdim
-        << ":" << a.idx;
+        << ":" << a.idx << ":" << a.vec;
   }
   std::string body;
   std::vector<std::string> seen;
@@ -528,7 +591,7 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
   std::vector<size_t> goff((size_t)nargs, 0);
   size_t gbytes = 0;
   for (int i = 0; i < nargs; i++)
-    if (ap[(size_t)i].kind == GBL) {
+    if (ap[(size_t)i].kind == GBL || ap[(size_t)i].kind == OFF) {  // OFF: zeroed scratch
       goff[(size_t)i] = gbytes;
       gbytes += ((size_t)ap[(size_t)i].dim * ap[(size_t)i].bytes + 15) & ~(size_t)15;
     }
@@ -582,8 +645,11 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
       bytes += (double)x.dat->size * (a.kind == DIRECT ? n : x.dat->set->size);
     } else if (a.kind == GBL) {
       ptrs.push_back((char *)j.gbl_d + goff[(size_t)i]);
+    } else if (a.kind == OFF) {
+      ptrs.push_back((char *)j.gbl_d + goff[(size_t)i]);
     }
-    if (a.kind == DIRECT || a.kind == INDIRECT || a.kind == GBL) kp.push_back(&ptrs.back());
+    if (a.kind == DIRECT || a.kind == INDIRECT || a.kind == GBL || a.kind == OFF)
+      kp.push_back(&ptrs.back());
     if (a.kind == INDIRECT || (a.kind == IDX && a.mdim > 0)) {
       ptrs.push_back(x.map->map_d);
       kp.push_back(&ptrs.back());

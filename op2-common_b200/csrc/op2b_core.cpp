@@ -327,10 +327,12 @@ void op_exit(void) {
   release_renumbering();
   for (auto &d : r.dats)
     if (d) {
-      cudaFree(d->data_d);
+      if (!r.overlays.count(d.get())) {  // overlays share their dat's storage
+        cudaFree(d->data_d);
+        free(d->data);
+      }
       free((void *)d->name);
       free((void *)d->type);
-      free(d->data);
     }
   for (auto &m : r.maps)
     if (m) {
@@ -376,6 +378,8 @@ void op_exit(void) {
   r.stats.clear();
   r.exposed.clear();
   r.zero_mirror.clear();
+  r.overlays.clear();
+  r.orig_ptrs.clear();
   r.launches = 0;
   r.initialised = false;
   // options return to their defaults: a later op_init starts from a clean state
@@ -559,34 +563,92 @@ op_dat op_decl_dat_char(op_set set, int dim, char const *type, int type_size, ch
     }
   }
   if (d->data && !data) r.zero_mirror.insert(d.get());
+  if (data) r.orig_ptrs[data] = d.get();  // for op_decl_dat_overlay_ptr
   r.dats.push_back(std::move(d));
   return r.dats.back().get();
 }
 
+// op_decl_dat_temp_core (op_lib_core.cpp:638-651): a dat of the same set,
+// dim, type, size and name must not exist yet.
 op_dat op_decl_dat_temp_char(op_set set, int dim, char const *type, int type_size,
                              char const *name) {
+  Runtime &r = rt();
+  for (auto &d : r.dats)
+    if (d && d->set == set && d->dim == dim && d->size == dim * type_size &&
+        strcmp(d->type, type ? type : "") == 0 && strcmp(d->name, name ? name : "") == 0) {
+      set_error("op_dat with name %s already exists, cannot create temporary op_dat",
+                name ? name : "");
+      return nullptr;
+    }
   return op_decl_dat_char(set, dim, type, type_size, nullptr, name);
 }
 
+// op_free_dat_temp_core (op_lib_core.cpp:653-680): 1 when the dat was
+// found and freed, -1 otherwise.
 int op_free_dat_temp_char(op_dat dat) {
   Runtime &r = rt();
   flush_quiet();
   // forget the learned arguments (flush_quiet put adt back), keep the buffer
   r.spec = SpecAdt{nullptr, nullptr, nullptr, nullptr, 0, false, r.spec.shadow,
                    r.spec.shadow_bytes};
-  r.zero_mirror.erase(dat);
   for (auto &d : r.dats)
     if (d.get() == dat) {
       cudaStreamSynchronize(r.stream);
-      cudaFree(d->data_d);
+      if (!r.overlays.count(dat)) {
+        cudaFree(d->data_d);
+        free(d->data);
+      }
       free((void *)d->name);
       free((void *)d->type);
-      free(d->data);
+      r.overlays.erase(dat);
+      r.zero_mirror.erase(dat);
+      r.exposed.erase(dat);
+      for (auto it = r.orig_ptrs.begin(); it != r.orig_ptrs.end();)
+        it = it->second == dat ? r.orig_ptrs.erase(it) : std::next(it);
       d.reset();
-      return 0;
+      return 1;
     }
   set_error("op_free_dat_temp: unknown dat");
   return -1;
+}
+
+// op_decl_dat_overlay (op_lib_core.cpp:581-636, op_cuda_decl.cpp:101-123):
+// a dat on another set that shares `dat`'s storage, host and device; the
+// set may not be larger than the dat's.
+op_dat op_decl_dat_overlay(op_set set, op_dat dat) {
+  Runtime &r = rt();
+  if (!r.ready()) return nullptr;
+  if (!set || !dat) {
+    set_error("op_decl_dat_overlay error -- invalid set or dat");
+    return nullptr;
+  }
+  if (set->size > dat->set->size) {
+    set_error("op_decl_dat_overlay error -- new set size bigger than overlayed size (%d > %d)",
+              set->size, dat->set->size);
+    return nullptr;
+  }
+  if (r.opt_diags > 1)
+    op_printf("op_decl_dat_overlay: dat: %s, set %s (%d elems) -> %s (%d elems)\n", dat->name,
+              dat->set->name, dat->set->size, set->name, set->size);
+  flush_quiet();
+  auto d = std::make_unique<op_dat_core>(*dat);
+  d->index = (int)r.dats.size();
+  d->set = set;
+  d->name = copy_str(dat->name);
+  d->type = copy_str(dat->type);
+  r.overlays.insert(d.get());
+  r.dats.push_back(std::move(d));
+  return r.dats.back().get();
+}
+
+op_dat op_decl_dat_overlay_ptr(op_set set, char *dat) {
+  Runtime &r = rt();
+  auto it = r.orig_ptrs.find(dat);
+  if (it == r.orig_ptrs.end()) {
+    set_error("op_decl_dat_overlay_ptr: op_dat not found for dat with %p pointer", (void *)dat);
+    return nullptr;
+  }
+  return op_decl_dat_overlay(set, it->second);
 }
 
 void op_decl_const_char(int dim, char const *type, int type_size, char *dat, char const *name) {

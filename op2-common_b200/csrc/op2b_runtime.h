@@ -120,6 +120,8 @@ struct Runtime {
   SpecAdt spec;
   std::set<op_dat> exposed;  // dats whose device pointer was handed out (no speculation)
   std::set<op_dat> zero_mirror;  // dats declared without data: their host copy is zeros
+  std::set<op_dat> overlays;     // op_decl_dat_overlay: storage owned by another dat
+  std::map<const char *, op_dat> orig_ptrs;  // caller's array -> the dat declared from it
 
   LaunchCtx ctx();
   // initialised, with any deferred loop launched (false on error)

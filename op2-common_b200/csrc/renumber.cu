@@ -755,6 +755,11 @@ static bool bandwidth(op_map base, long &mx, long &avg, cudaStream_t s) {
 }
 
 int renumber(op_map base, long stats[4]) {
+  if (!rt().overlays.empty()) {
+    set_error("op_renumber: overlay dats share storage across sets; renumber before "
+              "declaring them");
+    return -1;
+  }
   Runtime &r = rt();
   if (!r.ready()) return -1;
   if (!base || !base->map_d) {

@@ -78,6 +78,8 @@ _SIGS = {
     "op_decl_dat_temp_char": (op_dat, [op_set, ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
                                        ctypes.c_char_p]),
     "op_free_dat_temp_char": (ctypes.c_int, [op_dat]),
+    "op_decl_dat_overlay": (op_dat, [op_set, op_dat]),
+    "op_decl_dat_overlay_ptr": (op_dat, [op_set, ctypes.c_void_p]),
     "op_decl_const_char": (None, [ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_void_p,
                                   ctypes.c_char_p]),
     "op_arg_dat": (op_arg, [op_dat, ctypes.c_int, op_map, ctypes.c_int, ctypes.c_char_p,
@@ -333,6 +335,35 @@ def op_decl_dat(set_, dim: int, type_: str | None, data, name: str):
     return d
 
 
+def op_decl_dat_temp(set_, dim: int, type_: str, name: str):
+    """op_decl_dat_temp<T> (op_lib_cpp.h): a zeroed dat, freed by op_free_dat_temp."""
+    tb = {"double": 8, "float": 4, "int": 4}[type_.split(":")[0]]
+    d = load().op_decl_dat_temp_char(set_, int(dim), _b(type_), tb, _b(name))
+    if not d:
+        _check(False, "op_decl_dat_temp")
+    return d
+
+
+def op_free_dat_temp(dat) -> int:
+    return load().op_free_dat_temp_char(dat)
+
+
+def op_decl_dat_overlay(set_, dat):
+    """op_decl_dat_overlay (op_lib_c.h:85): `dat`'s storage seen as a dat on `set_`."""
+    d = load().op_decl_dat_overlay(set_, dat)
+    if not d:
+        _check(False, "op_decl_dat_overlay")
+    return d
+
+
+def op_decl_dat_overlay_ptr(set_, data: np.ndarray):
+    """op_decl_dat_overlay_ptr (op_lib_c.h:86): the dat declared from `data`."""
+    d = load().op_decl_dat_overlay_ptr(set_, data.ctypes.data)
+    if not d:
+        _check(False, "op_decl_dat_overlay_ptr")
+    return d
+
+
 def op_decl_const(dim: int, type_: str, value, name: str):
     a = np.ascontiguousarray(np.atleast_1d(value),
                              dtype={"double": np.float64, "float": np.float32,
@@ -358,6 +389,14 @@ def op_arg_gbl(data: np.ndarray, dim: int, type_: str, acc: int):
     _keep.append(data)
     return load().op_arg_gbl_char(data.ctypes.data, int(dim), _b(type_), data.dtype.itemsize,
                                   int(acc))
+
+
+def op_opt_arg_gbl(opt: int, data: np.ndarray, dim: int, type_: str, acc: int):
+    if not isinstance(data, np.ndarray) or not data.flags.c_contiguous:
+        raise Op2Error("op_opt_arg_gbl: pass a contiguous numpy array (written back in place)")
+    _keep.append(data)
+    return load().op_opt_arg_gbl_char(int(opt), data.ctypes.data, int(dim), _b(type_),
+                                      data.dtype.itemsize, int(acc))
 
 
 def op_arg_info(data: np.ndarray, dim: int, type_: str, ref: int):

@@ -155,8 +155,10 @@ def test_unsupported_forms_and_compile_errors_are_reported(op2):
     edges = op2.op_decl_set(300, "edges")
     m = op2.op_decl_map(edges, nodes, 2, pp, "ppedge")
     pv = op2.op_decl_dat(nodes, 1, "double", None, "v")
-    with pytest.raises(L.Op2Error, match="vector map arguments"):
-        op2.op_par_loop("gen_rw", edges, op2.op_arg_dat(pv, -2, m, 1, "double", op2.OP_READ))
+    with pytest.raises(L.Op2Error, match="does not fit a map of dimension 2"):
+        op2.op_par_loop("gen_rw", edges, op2.op_arg_dat(pv, 2, m, 1, "double", op2.OP_READ))
+    with pytest.raises(L.Op2Error, match="does not fit a map of dimension 2"):
+        op2.op_par_loop("gen_rw", edges, op2.op_arg_dat(pv, -3, m, 1, "double", op2.OP_READ))
     with pytest.raises(L.Op2Error, match="compiling the kernel failed"):
         op2.op_par_loop("gen_bad", nodes, op2.op_arg_dat(pv, -1, op2.OP_ID, 1, "double",
                                                          op2.OP_RW))
@@ -212,6 +214,92 @@ inline void gen_rw2(double *a, double *b, const double *w, const int *e) {
     assert np.array_equal(op2.op_fetch_data(pv)[:, 0], ref)
 
 
+def test_vector_map_arguments(op2):
+    """Vector map arguments (op_arg_dat with idx = -k): the kernel gets k
+    pointers, one per map entry (op_seq.h op_arg_copy_in) -- OP_READ through
+    a const T ** parameter, OP_INC into per-entry locals added atomically,
+    OP_RW run colour by colour.  Integer-valued data keep every order exact."""
+    op2.register_kernel("gen_vcell", """
+inline void gen_vcell(const double **x, double **r, const double *w) {
+  for (int j = 0; j < 4; j++) {
+    r[j][0] += (*w) * x[j][0];
+    r[j][1] += x[(j + 1) % 4][1] - x[j][1];
+  }
+}
+""")
+    op2.register_kernel("gen_vrw", """
+inline void gen_vrw(double **v, const int *e) {
+  v[0][0] += 1.0 + (*e % 5);
+  v[1][0] -= 2.0;
+}
+""")
+    rng = np.random.default_rng(6)
+    nn, nc = 4000, 9000
+    cell = np.stack([rng.permutation(nn)[:4] for _ in range(nc)]).astype(np.int32)
+    x = rng.integers(-100, 100, size=(nn, 2)).astype(np.float64)
+    w = rng.integers(-9, 9, size=nc).astype(np.float64)
+    nodes = op2.op_decl_set(nn, "nodes")
+    cells = op2.op_decl_set(nc, "cells")
+    pcell = op2.op_decl_map(cells, nodes, 4, cell, "pcell")
+    px = op2.op_decl_dat(nodes, 2, "double", x, "x")
+    pr = op2.op_decl_dat(nodes, 2, "double", None, "r")
+    pw = op2.op_decl_dat(cells, 1, "double", w, "w")
+    op2.op_par_loop("gen_vcell", cells,
+                    op2.op_arg_dat(px, -4, pcell, 2, "double", op2.OP_READ),
+                    op2.op_arg_dat(pr, -4, pcell, 2, "double", op2.OP_INC),
+                    op2.op_arg_dat(pw, -1, op2.OP_ID, 1, "double", op2.OP_READ))
+    ref = np.zeros((nn, 2))
+    for j in range(4):
+        np.add.at(ref[:, 0], cell[:, j], w * x[cell[:, j], 0])
+        np.add.at(ref[:, 1], cell[:, j], x[cell[:, (j + 1) % 4], 1] - x[cell[:, j], 1])
+    assert np.array_equal(op2.op_fetch_data(pr), ref)
+    # RW through a vector argument of two entries (edge endpoints)
+    pp = cell[:, :2].copy()
+    edges = op2.op_decl_set(nc, "edges")
+    pe = op2.op_decl_map(edges, nodes, 2, pp, "ppedge")
+    v0 = rng.integers(-50, 50, size=nn).astype(np.float64)
+    pv = op2.op_decl_dat(nodes, 1, "double", v0, "v")
+    op2.op_par_loop("gen_vrw", edges, op2.op_arg_dat(pv, -2, pe, 1, "double", op2.OP_RW),
+                    op2.op_arg_idx(-1, op2.OP_ID))
+    ref_v = v0.copy()
+    np.add.at(ref_v, pp[:, 0], 1.0 + np.arange(nc) % 5)
+    np.add.at(ref_v, pp[:, 1], -2.0)
+    assert np.array_equal(op2.op_fetch_data(pv)[:, 0], ref_v)
+
+
+def test_optional_arguments_switched_off(op2):
+    """op_opt_arg_dat / op_opt_arg_gbl with opt = 0: the kernel still gets a
+    pointer (to scratch) and must not use it; the dat and the caller's
+    global stay as they were.  With opt = 1 the same loop uses them."""
+    op2.register_kernel("gen_opt", """
+inline void gen_opt(const double *a, double *b, double *extra, double *gsum) {
+  *b = 2.0 * (*a);
+  if (gen_use) { *extra += *a; *gsum += *a; }
+}
+""")
+    rng = np.random.default_rng(7)
+    n = 3000
+    a = rng.integers(-20, 20, size=n).astype(np.float64)
+    s = op2.op_decl_set(n, "s")
+    pa = op2.op_decl_dat(s, 1, "double", a, "a")
+    pb = op2.op_decl_dat(s, 1, "double", None, "b")
+    pe = op2.op_decl_dat(s, 1, "double", np.full(n, 5.0), "extra")
+    for use in (0, 1):
+        op2.op_decl_const(1, "int", np.array([use], np.int32), "gen_use")
+        g = np.array([100.0])
+        op2.op_par_loop("gen_opt", s,
+                        op2.op_arg_dat(pa, -1, op2.OP_ID, 1, "double", op2.OP_READ),
+                        op2.op_arg_dat(pb, -1, op2.OP_ID, 1, "double", op2.OP_WRITE),
+                        op2.op_opt_arg_dat(use, pe, -1, op2.OP_ID, 1, "double", op2.OP_INC),
+                        op2.op_opt_arg_gbl(use, g, 1, "double", op2.OP_INC))
+        assert np.array_equal(op2.op_fetch_data(pb)[:, 0], 2.0 * a)
+        if use:
+            assert np.array_equal(op2.op_fetch_data(pe)[:, 0], 5.0 + a)
+            assert g[0] == 100.0 + a.sum()
+        else:
+            assert np.all(op2.op_fetch_data(pe) == 5.0) and g[0] == 100.0
+
+
 def test_application_loop_sharing_an_airfoil_name(op2):
     """An application's own 'update' (jac1's signature) is not Airfoil's: its
     source is compiled and run instead of the hand-written update loop."""
@@ -249,3 +337,40 @@ inline void update(const double *r, double *du, double *u, int *index, double *u
         assert umax[0] == max(0.0, ref.max())
     finally:
         op2.register_kernel("update", None)  # leave no source under an Airfoil name
+
+
+def test_temporary_and_overlay_dats(op2):
+    """op_decl_dat_temp: zeroed, a second one of the same name is refused,
+    op_free_dat_temp returns 1 then -1 (op_lib_core.cpp:638-680).
+    op_decl_dat_overlay / _ptr: a dat on a smaller set sharing the storage of
+    another, host copy and device array (op_lib_core.cpp:581-636)."""
+    op2.register_kernel("gen_fill", "inline void gen_fill(double *v, const int *i) { v[0] = *i; v[1] = -(*i); }\n")
+    n, m = 1000, 600
+    big = op2.op_decl_set(n, "big")
+    small = op2.op_decl_set(m, "small")
+    t = op2.op_decl_dat_temp(big, 2, "double", "tmp")
+    assert np.all(op2.op_fetch_data(t) == 0)
+    with pytest.raises(L.Op2Error, match="already exists"):
+        op2.op_decl_dat_temp(big, 2, "double", "tmp")
+    src = np.arange(2 * n, dtype=np.float64).reshape(n, 2) * 0.5
+    d = op2.op_decl_dat(big, 2, "double", src, "d")
+    ov = op2.op_decl_dat_overlay(small, d)
+    ov2 = op2.op_decl_dat_overlay_ptr(small, src)
+    assert ov2.contents.data_d == d.contents.data_d == ov.contents.data_d
+    assert ov.contents.data == d.contents.data and ov.contents.set.contents.size == m
+    with pytest.raises(L.Op2Error, match="bigger than overlayed"):
+        op2.op_decl_dat_overlay(big, op2.op_decl_dat(small, 1, "double", None, "s1"))
+    # a loop over the small set through the overlay writes the first m rows of d
+    op2.op_par_loop("gen_fill", small, op2.op_arg_dat(ov, -1, op2.OP_ID, 2, "double", op2.OP_WRITE),
+                    op2.op_arg_idx(-1, op2.OP_ID))
+    got = op2.op_fetch_data(d)
+    i = np.arange(m, dtype=np.float64)
+    assert np.array_equal(got[:m], np.stack([i, -i], axis=1))
+    assert np.array_equal(got[m:], src[m:])
+    assert np.array_equal(op2.op_fetch_data(ov), got[:m])
+    assert op2.op_free_dat_temp(t) == 1
+    assert op2.op_free_dat_temp(t) == -1
+    # overlays share storage across sets: renumbering is refused while they exist
+    mp = op2.op_decl_map(small, big, 1, np.arange(m, dtype=np.int32).reshape(m, 1), "pm")
+    with pytest.raises(L.Op2Error, match="overlay"):
+        op2.op_renumber(mp)
