@@ -166,7 +166,7 @@ LaunchCtx Runtime::ctx() { return LaunchCtx{stream, nsm, &launches}; }
 // hand out access to the data; bookkeeping calls only launch deferred loops)
 static void flush_quiet(bool restore = true) {
   Runtime &r = rt();
-  if (r.initialised && r.pend.kind) r.flush_pending();
+  if (r.initialised && r.outstanding()) r.flush_pending();
   if (restore && r.initialised && r.spec.inplace) r.restore_spec();
 }
 
@@ -175,7 +175,7 @@ bool Runtime::ready() {
     set_error("op_init has not been called");
     return false;
   }
-  return (pend.kind == 0 || flush_pending()) && (!spec.inplace || restore_spec());
+  return (!outstanding() || flush_pending()) && (!spec.inplace || restore_spec());
 }
 
 // ------------------------------------------------------------------ timing
@@ -320,7 +320,7 @@ void op_init(int argc, char **argv, int diags) {
 void op_exit(void) {
   Runtime &r = rt();
   if (!r.initialised) return;
-  if (r.pend.kind) r.flush_pending();
+  if (r.outstanding()) r.flush_pending();
   cudaStreamSynchronize(r.stream);
   release_plans();
   release_inverse_maps();
@@ -399,6 +399,8 @@ void op_exit(void) {
   r.opt_fuse = d.opt_fuse;
   r.opt_speculate = d.opt_speculate;
   r.opt_host_mirror = d.opt_host_mirror;
+  r.opt_rename_save = d.opt_rename_save;
+  r.lazy = LazySave{};
   r.pend = PendingLoop{};
   r.opt_pipe_block = d.opt_pipe_block;
   r.opt_pipe_hints = d.opt_pipe_hints;
@@ -974,7 +976,7 @@ void *op2b_map_device_ptr(op_map map) {
 
 int op2b_set_option(const char *key, long value) {
   Runtime &r = rt();
-  if (r.initialised && r.pend.kind && !r.flush_pending()) return -1;
+  if (r.initialised && r.outstanding() && !r.flush_pending()) return -1;
   if (r.initialised && r.spec.inplace && !r.restore_spec()) return -1;
   std::string k = key ? key : "";
   if (k == "inc_mode") {
@@ -1033,6 +1035,8 @@ int op2b_set_option(const char *key, long value) {
     r.opt_check_plans = value != 0;
   } else if (k == "host_mirror") {
     r.opt_host_mirror = value != 0;
+  } else if (k == "rename_save") {
+    r.opt_rename_save = value != 0;
   } else {
     set_error("op2b_set_option: unknown option '%s'", k.c_str());
     return -1;
@@ -1060,6 +1064,7 @@ long op2b_get_option(const char *key) {
   if (k == "fuse") return r.opt_fuse;
   if (k == "speculate_adt") return r.opt_speculate;
   if (k == "host_mirror") return r.opt_host_mirror;
+  if (k == "rename_save") return r.opt_rename_save;
   if (k == "nsm") return r.nsm;
   return -1;
 }

@@ -166,6 +166,24 @@ int finish(cudaError_t e, const char *loop) {
   return 0;
 }
 
+// A loop may run while a renamed save_soln is outstanding when it neither
+// touches qold nor writes q: qold's array is stale, q's is current.
+bool save_compatible(const Runtime &r, const op_arg *a, int nargs) {
+  for (int i = 0; i < nargs; i++) {
+    if (a[i].argtype != OP_ARG_DAT || !a[i].dat) continue;
+    if (a[i].dat == r.lazy.dst || (a[i].dat == r.lazy.src && a[i].acc != OP_READ)) return false;
+  }
+  return true;
+}
+
+// Launch what is outstanding before a loop with these arguments: the
+// deferred loop, and the renamed save_soln's copy unless the loop can run
+// beside it.
+bool flush_for(Runtime &r, const op_arg *a, int nargs) {
+  if (r.lazy.src && save_compatible(r, a, nargs)) return !r.pend.kind || r.flush_loop();
+  return !r.outstanding() || r.flush_pending();
+}
+
 // ---------------------------------------------------------------- save_soln
 int loop_save_soln(const char *name, op_set set, int nargs, op_arg *a) {
   Sig s{name, set, a, nargs};
@@ -176,13 +194,29 @@ int loop_save_soln(const char *name, op_set set, int nargs, op_arg *a) {
   if (!s.ok) return kSigMismatch;
   if (a[0].dat->size != a[1].dat->size) return s.fail(1, "element size differs from argument 0"), kSigMismatch;
   Runtime &r = rt();
-  if (r.pend.kind && !r.flush_pending()) return -1;
+  if (r.lazy.src == a[0].dat && r.lazy.dst == a[1].dat) {  // qold is already q
+    if (r.pend.kind && !r.flush_loop()) return -1;
+    r.count_call("save_soln(renamed)");
+    return 0;
+  }
+  if (r.outstanding() && !r.flush_pending()) return -1;
   if (r.spec.inplace && (a[1].dat == r.spec.x || a[1].dat == r.spec.q ||
                          a[1].dat == r.spec.adt || a[0].dat == r.spec.adt) &&
       !r.restore_spec())
     return -1;
   size_t bytes = (size_t)set->size * (size_t)a[0].dat->size;
   int tb = a[0].dat->type ? type_bytes(a[0].dat->type) : 0;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(r.stream, &cap);
+  if (r.opt_rename_save && a[0].dat != a[1].dat && a[0].dat->set == a[1].dat->set &&
+      !r.exposed.count(a[0].dat) && !r.exposed.count(a[1].dat) && r.overlays.empty() &&
+      cap == cudaStreamCaptureStatusNone) {
+    // renamed: no launch now; the update that next writes q swaps the arrays
+    r.lazy.src = a[0].dat;
+    r.lazy.dst = a[1].dat;
+    r.count_call("save_soln(renamed)");
+    return 0;
+  }
   if (r.opt_fuse && dim == 4 && is_real(a[0].dat->type, tb) && a[0].dat != a[1].dat) {
     // deferred: launched with the next loop call (fused into an adt_calc on
     // the same q) or alone before any other call
@@ -259,7 +293,7 @@ int loop_adt_calc(const char *name, op_set set, int nargs, op_arg *a) {
     r.end_loop(fused);
     return finish(e, name);
   }
-  if (pd.kind && !r.flush_pending()) return -1;
+  if (!flush_for(r, a, nargs)) return -1;
   r.begin_loop(name);
   cudaError_t e;
   bool ok;
@@ -326,7 +360,7 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
   int rb = s.real_bytes({0, 2, 4, 6});
   if (!s.ok) return kSigMismatch;
   Runtime &r = rt();
-  if (r.pend.kind && !r.flush_pending()) return -1;
+  if (!flush_for(r, a, nargs)) return -1;
   if (r.spec.inplace && !r.restore_spec()) return -1;
   int E = set->size, N = a[0].dat->set->size, C = a[2].dat->set->size;
   double bytes = 16.0 * E + (double)rb * (2.0 * N + 13.0 * C);
@@ -445,6 +479,7 @@ int loop_bres_calc(const char *name, op_set set, int nargs, op_arg *a) {
   if (pd.kind == 2 && same_consts && pd.res == a[4].dat && pd.q == a[2].dat &&
       pd.adt == a[3].dat && pd.x == a[0].dat && pd.rb == rb &&
       r.opt_inc_mode == OP2B_INC_GATHER && r.opt_bres_kernel == 1) {
+    if (r.lazy.src && !save_compatible(r, a, nargs) && !r.materialize_save()) return -1;
     const SlotRecords *cr = get_corner_records(pd.pecell, pd.pedge);
     const BresRecords *br = cr ? get_bres_records(pbecell, pbedge) : nullptr;
     if (cr && br && link_boundary_records(cr, br, pbecell)) {
@@ -474,7 +509,7 @@ int loop_bres_calc(const char *name, op_set set, int nargs, op_arg *a) {
     }
     if (!cr || (r.opt_bres_kernel == 1 && !br)) return -1;
   }
-  if (pd.kind && !r.flush_pending()) return -1;
+  if (!flush_for(r, a, nargs)) return -1;
   Plan *plan = nullptr;
   const InvMap *inv = nullptr;
   const BresRecords *brec = nullptr;
@@ -541,9 +576,15 @@ int loop_update(const char *name, op_set set, int nargs, op_arg *a) {
   if (!s.ok) return kSigMismatch;
   if (a[4].type && strcmp(a[4].type, "double") != 0) return s.fail(4, "rms must be double"), kSigMismatch;
   Runtime &r = rt();
-  if (r.pend.kind && !r.flush_pending()) return -1;
+  // a renamed save_soln of exactly this q into this qold: read q's array as
+  // qold, write the new q into qold's array, then swap the two
+  const bool rename = r.lazy.src == a[1].dat && r.lazy.dst == a[0].dat && a[2].dat != a[0].dat &&
+                      a[2].dat != a[1].dat && a[3].dat != a[0].dat && a[3].dat != a[1].dat;
+  if (rename ? (r.pend.kind && !r.flush_loop()) : (r.outstanding() && !r.flush_pending())) return -1;
   int C = set->size;
   double bytes = (double)rb * 17.0 * C;
+  char *qin = rename ? a[1].dat->data_d : a[0].dat->data_d;
+  char *qout = rename ? a[0].dat->data_d : a[1].dat->data_d;
   r.red.seq = ++r.red_seq;
   // speculation: this update's q is the q the last adt_calc read, and adt
   // is what it wrote -- compute the next adt_calc's result now, into the
@@ -571,15 +612,15 @@ int loop_update(const char *name, op_set set, int nargs, op_arg *a) {
   r.begin_loop(spec ? "update+adt_calc" : name);
   cudaError_t e;
   if (rb == 8)
-    e = launch_update<double>(r.ctx(), C, (const double *)a[0].dat->data_d,
-                              (double *)a[1].dat->data_d, (double *)a[2].dat->data_d,
+    e = launch_update<double>(r.ctx(), C, (const double *)qin, (double *)qout,
+                              (double *)a[2].dat->data_d,
                               (const double *)a[3].dat->data_d, r.red,
                               spec ? sp.pcell->map_d : nullptr,
                               spec ? (const double *)sp.x->data_d : nullptr,
                               spec ? (double *)sp.shadow : nullptr, &sp.kd);
   else
-    e = launch_update<float>(r.ctx(), C, (const float *)a[0].dat->data_d,
-                             (float *)a[1].dat->data_d, (float *)a[2].dat->data_d,
+    e = launch_update<float>(r.ctx(), C, (const float *)qin, (float *)qout,
+                             (float *)a[2].dat->data_d,
                              (const float *)a[3].dat->data_d, r.red,
                              spec ? sp.pcell->map_d : nullptr,
                              spec ? (const float *)sp.x->data_d : nullptr,
@@ -588,6 +629,10 @@ int loop_update(const char *name, op_set set, int nargs, op_arg *a) {
   r.end_loop(spec ? bytes + 16.0 * C + (double)rb * (2.0 * N + C) : bytes);
   sp.inplace = spec && e == cudaSuccess;
   if (finish(e, name)) return -1;
+  if (rename) {
+    std::swap(a[0].dat->data_d, a[1].dat->data_d);
+    r.lazy = LazySave{};
+  }
   // gbl results are valid when op_par_loop returns: the kernel's last block
   // publishes them in the mapped page, sequence number last
   volatile RedSlot *h = reinterpret_cast<volatile RedSlot *>(r.pinned);
@@ -632,6 +677,22 @@ bool op2b::Runtime::restore_spec() {
 }
 
 bool op2b::Runtime::flush_pending() {
+  const bool ok = flush_loop();
+  return materialize_save() && ok;
+}
+
+bool op2b::Runtime::materialize_save() {
+  if (!lazy.src) return true;
+  LazySave ls = lazy;
+  lazy = LazySave{};
+  const size_t bytes = (size_t)ls.src->set->size * (size_t)ls.src->size;
+  begin_loop("save_soln");
+  cudaError_t e = launch_copy(ctx(), ls.src->data_d, ls.dst->data_d, bytes);
+  end_loop(2.0 * (double)bytes);
+  return finish(e, "save_soln") == 0;
+}
+
+bool op2b::Runtime::flush_loop() {
   PendingLoop pd = pend;
   pend = PendingLoop{};
   cudaError_t e = cudaSuccess;
@@ -693,7 +754,7 @@ int op_par_loop_c(char const *name, op_set set, int nargs, op_arg *args) {
       if (!jit_has_kernel(name)) return -1;
       break;
     }
-  if (r.pend.kind && !r.flush_pending()) return -1;
+  if (r.outstanding() && !r.flush_pending()) return -1;
   if (r.spec.inplace && !r.restore_spec()) return -1;
   // no hand-written kernel: the application's own kernel source, compiled at
   // run time, if it has one

@@ -52,6 +52,16 @@ struct PendingLoop {
 // has nothing left to do, and any other call that could read adt first
 // restores it from the shadow (restore_spec), so nothing observes the early
 // values.
+// save_soln by renaming: save_soln (q -> qold) launches nothing; qold is
+// taken to hold q's values until q changes.  Loops that only read q run
+// meanwhile.  The update that reads qold and writes q then reads q's array
+// and writes qold's, and the two dats swap arrays: q holds the new solution
+// and qold the saved one, with no copy.  Any other call first makes the copy
+// (materialize_save).
+struct LazySave {
+  op_dat src = nullptr, dst = nullptr;  // q, qold
+};
+
 struct SpecAdt {
   op_map pcell = nullptr;                               // the last adt_calc's arguments
   op_dat x = nullptr, q = nullptr, adt = nullptr;
@@ -85,6 +95,7 @@ struct Runtime {
   int opt_speculate = 1;      // update also computes the next adt_calc's result (SpecAdt)
   int opt_adt_minb = 0;       // adt_calc: __launch_bounds__ minimum blocks (0 = none)
   int opt_host_mirror = 1;    // op_dat::data holds a host copy of the declared values
+  int opt_rename_save = 1;    // save_soln by renaming (LazySave)
   int opt_pipe_block = 256;   // threads per CTA of the pipelined gather (64, 96, 128, 256)
   int opt_pipe_hints = 0;     // register pipeline: evict-first hints on once-read streams
   int opt_plan_mode = 0;      // 0 = parallel block colouring, 1 = serial greedy (bit-exact)
@@ -117,6 +128,7 @@ struct Runtime {
   cudaEvent_t cur_ev0 = nullptr, cur_ev1 = nullptr;
 
   PendingLoop pend;
+  LazySave lazy;
   SpecAdt spec;
   std::set<op_dat> exposed;  // dats whose device pointer was handed out (no speculation)
   std::set<op_dat> zero_mirror;  // dats declared without data: their host copy is zeros
@@ -126,7 +138,11 @@ struct Runtime {
   LaunchCtx ctx();
   // initialised, with any deferred loop launched (false on error)
   bool ready();
-  bool flush_pending();  // op2b_dispatch.cpp
+  // a deferred loop or a renamed save_soln is outstanding
+  bool outstanding() const { return pend.kind != 0 || lazy.src != nullptr; }
+  bool flush_pending();     // op2b_dispatch.cpp: both launched
+  bool flush_loop();        // op2b_dispatch.cpp: the deferred loop only
+  bool materialize_save();  // op2b_dispatch.cpp: the renamed save_soln's copy
   bool restore_spec();   // op2b_dispatch.cpp: put the old adt back if adt is ahead
   void begin_loop(const char *name);
   void count_call(const char *name) { stats[name].calls++; }  // a call with no launch

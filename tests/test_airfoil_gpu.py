@@ -276,6 +276,7 @@ def test_fused_loop_pairs_are_bit_identical_to_separate_loops(op2):
         for fuse in (0, 1):
             op2.set_option("fuse", fuse)
             op2.set_option("speculate_adt", 0)  # every adt_calc computed, fused or not
+            op2.set_option("rename_save", 0)    # save_soln copies (into the adt_calc)
             op2.load().op2b_reset_stats()
             app = Airfoil(m, dtype=dtype)
             hists.append(app.iterate(4))
@@ -291,6 +292,7 @@ def test_fused_loop_pairs_are_bit_identical_to_separate_loops(op2):
         assert stats[1]["save_soln+adt_calc"]["calls"] == 4
     # a deferred save_soln / res_calc is launched before a fetch observes it
     op2.set_option("speculate_adt", 0)
+    op2.set_option("rename_save", 0)
     app = Airfoil(m)
     app.iterate(1)
     app._loop(0)                                    # save_soln, deferred
@@ -305,6 +307,63 @@ def test_fused_loop_pairs_are_bit_identical_to_separate_loops(op2):
     for i in (0, 1, 2):
         app2._loop(i)
     assert np.array_equal(r_deferred, app2.fetch()["res"])
+
+
+def test_renamed_save_soln_is_bit_identical_and_invisible(op2):
+    """save_soln by renaming: no copy; the update that next reads qold and
+    writes q reads q's array and writes qold's, and the two dats swap arrays.
+    Against rename_save 0, in both precisions: the same history and fields,
+    and no save_soln launch at all inside the iterations.  Every observer
+    sees qold = q after save_soln: a fetch, another loop writing q, a loop
+    reading qold."""
+    m = M.channel_bump(96, 48, seed=13)
+    for dtype in (np.float64, np.float32):
+        out, hists, launches = [], [], []
+        for rename in (0, 1):
+            op2.set_option("rename_save", rename)
+            op2.load().op2b_reset_stats()
+            app = Airfoil(m, dtype=dtype)
+            hists.append(app.iterate(5))
+            out.append(app.fetch())
+            launches.append(op2.loop_stats("save_soln"))
+            renamed = op2.loop_stats("save_soln(renamed)")
+            op2.op_exit()
+            op2.op_init()
+        assert hists[0] == hists[1], dtype
+        for k in ("q", "qold", "adt", "res"):
+            assert np.array_equal(out[0][k], out[1][k]), (dtype, k)
+        # copying: the first save_soln goes out fused with the first adt_calc
+        assert launches[0]["calls"] == 4 and launches[1] is None and renamed["calls"] == 5
+    # observers of a renamed save_soln
+    app = Airfoil(m)
+    app.iterate(2)
+    app._loop(0)                                    # save_soln, renamed
+    assert np.array_equal(app.fetch()["qold"], app.fetch()["q"])
+    q_saved = app.fetch()["q"]
+    app._loop(0)
+    app._loop(1)                                    # adt_calc, reads q
+    # a loop that writes q (not the update) makes the copy first
+    L.op_par_loop("save_soln", app.cells,
+                  L.op_arg_dat(app.p_qold, -1, L.OP_ID, 4, "double", L.OP_READ),
+                  L.op_arg_dat(app.p_q, -1, L.OP_ID, 4, "double", L.OP_WRITE))  # qold -> q
+    assert np.array_equal(app.fetch()["qold"], q_saved)
+    assert np.array_equal(app.fetch()["q"], q_saved)
+    app3 = Airfoil(m)
+    app3.iterate(2)
+    app3._loop(0)
+    # a device pointer handed out for q before the update: no renaming is
+    # done for it, the results stay those of the copying path
+    L.load().op2b_dat_device_ptr(app3.p_q)
+    for i in (1, 2, 3, 4):
+        app3._loop(i)
+    op2.set_option("rename_save", 0)
+    app4 = Airfoil(m)
+    app4.iterate(2)
+    app4._loop(0)
+    for i in (1, 2, 3, 4):
+        app4._loop(i)
+    assert np.array_equal(app3.fetch()["q"], app4.fetch()["q"])
+    assert np.array_equal(app3.fetch()["qold"], app4.fetch()["qold"])
 
 
 @pytest.mark.parametrize("adt", [6, 8])
