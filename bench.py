@@ -18,9 +18,10 @@ max over ranks.  Prints one JSON line on rank 0.
              (op_renumber, reverse Cuthill-McKee), owner-computes increments
              over corner records, the runtime's loop fusion (res_calc with
              bres_calc), its speculative adt_calc (computed by the update
-             before it) and save_soln by renaming (the update after it
+             before it), save_soln by renaming (the update after it
              writes the new q into qold's array and the two dats swap
-             arrays, so no copy is made).
+             arrays, so no copy is made), and the res_calc + bres_calc pair
+             launched by each update's call before it waits for the rms.
 * loops      per loop (or fused loop pair) device time, algorithmic bytes per
              call and GB/s.
 * e2e        the whole 1000-iteration job (the configuration's length) through
@@ -327,7 +328,8 @@ def main():
                   {"gather_kernel": 5, "pipe_block": 128}, {"gather_kernel": 5, "pipe_block": 256},
                   {"gather_kernel": 6, "pipe_block": 128}, {"gather_kernel": 6, "pipe_block": 256},
                   {"gather_kernel": 6, "pipe_block": 256, "bres_kernel": 0},
-                  {"rename_save": 0}, {"speculate_adt": 0, "rename_save": 0},
+                  {"speculate_res": 0}, {"rename_save": 0, "speculate_res": 0},
+                  {"speculate_adt": 0, "rename_save": 0},
                   {"fuse": 0, "speculate_adt": 0, "rename_save": 0}):
             v = timed_run(L, Airfoil, m, dtype, "rcm", 3, args.part_size, 20, 3, torch, barrier,
                           opts=o)

@@ -400,7 +400,10 @@ void op_exit(void) {
   r.opt_speculate = d.opt_speculate;
   r.opt_host_mirror = d.opt_host_mirror;
   r.opt_rename_save = d.opt_rename_save;
+  r.opt_speculate_res = d.opt_speculate_res;
   r.lazy = LazySave{};
+  r.rlearn = ResLearn{};
+  r.sres_stage = 0;
   r.pend = PendingLoop{};
   r.opt_pipe_block = d.opt_pipe_block;
   r.opt_pipe_hints = d.opt_pipe_hints;
@@ -602,6 +605,9 @@ int op_free_dat_temp_char(op_dat dat) {
       }
       free((void *)d->name);
       free((void *)d->type);
+      if (r.rlearn.x == dat || r.rlearn.q == dat || r.rlearn.adt == dat || r.rlearn.res == dat ||
+          r.rlearn.bound == dat)
+        r.rlearn = ResLearn{};
       r.overlays.erase(dat);
       r.zero_mirror.erase(dat);
       r.exposed.erase(dat);
@@ -1037,6 +1043,8 @@ int op2b_set_option(const char *key, long value) {
     r.opt_host_mirror = value != 0;
   } else if (k == "rename_save") {
     r.opt_rename_save = value != 0;
+  } else if (k == "speculate_res") {
+    r.opt_speculate_res = value != 0;
   } else {
     set_error("op2b_set_option: unknown option '%s'", k.c_str());
     return -1;
@@ -1065,6 +1073,7 @@ long op2b_get_option(const char *key) {
   if (k == "speculate_adt") return r.opt_speculate;
   if (k == "host_mirror") return r.opt_host_mirror;
   if (k == "rename_save") return r.opt_rename_save;
+  if (k == "speculate_res") return r.opt_speculate_res;
   if (k == "nsm") return r.nsm;
   return -1;
 }

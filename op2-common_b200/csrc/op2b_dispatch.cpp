@@ -176,12 +176,77 @@ bool save_compatible(const Runtime &r, const op_arg *a, int nargs) {
   return true;
 }
 
-// Launch what is outstanding before a loop with these arguments: the
-// deferred loop, and the renamed save_soln's copy unless the loop can run
-// beside it.
+// A loop may run while a speculative res_calc + bres_calc is outstanding
+// when it neither touches res nor writes what the pair reads.
+bool res_compatible(const Runtime &r, const op_arg *a, int nargs) {
+  const ResLearn &L = r.rlearn;
+  for (int i = 0; i < nargs; i++) {
+    if (a[i].argtype != OP_ARG_DAT || !a[i].dat) continue;
+    const op_dat d = a[i].dat;
+    if (d == L.res) return false;
+    if (a[i].acc != OP_READ && (d == L.x || d == L.q || d == L.adt || d == L.bound)) return false;
+  }
+  return true;
+}
+
+// Settle what is outstanding before a loop with these arguments: a
+// speculative res_calc + bres_calc and a renamed save_soln stay when the
+// loop can run beside them; the deferred loop is launched.
 bool flush_for(Runtime &r, const op_arg *a, int nargs) {
-  if (r.lazy.src && save_compatible(r, a, nargs)) return !r.pend.kind || r.flush_loop();
-  return !r.outstanding() || r.flush_pending();
+  bool ok = true;
+  if (r.sres_stage && !res_compatible(r, a, nargs)) ok = r.settle_res();
+  if (r.pend.kind) ok = r.flush_loop() && ok;
+  if (r.lazy.src && !save_compatible(r, a, nargs)) ok = r.materialize_save() && ok;
+  return ok;
+}
+
+bool consts_are(const AirConst<double> &kd, const AirConst<float> &kf, int rb) {
+  bool ok;
+  if (rb == 8) {
+    AirConst<double> k = air_consts<double>(ok);
+    return ok && memcmp(&k, &kd, sizeof(k)) == 0;
+  }
+  AirConst<float> k = air_consts<float>(ok);
+  return ok && memcmp(&k, &kf, sizeof(k)) == 0;
+}
+
+// the update's call launches the res_calc + bres_calc pair learned last
+// (ResLearn) right behind it, on the arrays it leaves: q, adt (the next
+// adt_calc's, computed ahead) and res (zero)
+void launch_speculative_res(Runtime &r, const op_arg *a, int rb) {
+  const ResLearn &L = r.rlearn;
+  const SpecAdt &sp = r.spec;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(r.stream, &cap);
+  if (!r.opt_speculate_res || !L.valid || !sp.inplace || cap != cudaStreamCaptureStatusNone ||
+      L.rb != rb || L.q != a[1].dat || L.res != a[2].dat || L.adt != a[3].dat ||
+      sp.q != L.q || sp.adt != L.adt || sp.x != L.x || !r.overlays.empty() ||
+      r.exposed.count(L.x) || r.exposed.count(L.q) || r.exposed.count(L.adt) ||
+      r.exposed.count(L.res) || r.exposed.count(L.bound) || !consts_are(L.kd, L.kf, rb) ||
+      memcmp(rb == 8 ? (const void *)&sp.kd : (const void *)&sp.kf,
+             rb == 8 ? (const void *)&L.kd : (const void *)&L.kf,
+             rb == 8 ? sizeof(L.kd) : sizeof(L.kf)) != 0)
+    return;
+  const SlotRecords *cr = get_corner_records(L.pecell, L.pedge);
+  const BresRecords *br = cr && cr->corners ? get_bres_records(L.pbecell, L.pbedge) : nullptr;
+  if (!br || !link_boundary_records(cr, br, L.pbecell)) {
+    cudaGetLastError();
+    return;
+  }
+  const int *bound = (const int *)L.bound->data_d;
+  cudaError_t e;
+  r.begin_loop("res_calc+bres_calc");
+  if (rb == 8)
+    e = launch_res_bres_corner<double>(r.ctx(), *cr, *br, bound, (const double *)L.x->data_d,
+                                       (const double *)L.q->data_d, (const double *)L.adt->data_d,
+                                       (double *)L.res->data_d, L.kd, r.opt_pipe_block);
+  else
+    e = launch_res_bres_corner<float>(r.ctx(), *cr, *br, bound, (const float *)L.x->data_d,
+                                      (const float *)L.q->data_d, (const float *)L.adt->data_d,
+                                      (float *)L.res->data_d, L.kf, r.opt_pipe_block);
+  r.end_loop(L.fused_bytes);
+  if (e == cudaSuccess) r.sres_stage = 1;
+  else cudaGetLastError();  // not launched: the program's calls run as usual
 }
 
 // ---------------------------------------------------------------- save_soln
@@ -199,7 +264,8 @@ int loop_save_soln(const char *name, op_set set, int nargs, op_arg *a) {
     r.count_call("save_soln(renamed)");
     return 0;
   }
-  if (r.outstanding() && !r.flush_pending()) return -1;
+  if (!flush_for(r, a, nargs)) return -1;
+  if (r.lazy.src && !r.materialize_save()) return -1;  // one renamed save_soln at a time
   if (r.spec.inplace && (a[1].dat == r.spec.x || a[1].dat == r.spec.q ||
                          a[1].dat == r.spec.adt || a[0].dat == r.spec.adt) &&
       !r.restore_spec())
@@ -261,6 +327,7 @@ int loop_adt_calc(const char *name, op_set set, int nargs, op_arg *a) {
     r.count_call("adt_calc(in update)");
     return 0;
   }
+  if (r.sres_stage && !r.settle_res()) return -1;  // it read the adt computed ahead
   if (sp.inplace && !r.restore_spec()) return -1;
   sp.pcell = pcell;  // what the next update may compute ahead
   sp.x = a[0].dat;
@@ -360,6 +427,15 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
   int rb = s.real_bytes({0, 2, 4, 6});
   if (!s.ok) return kSigMismatch;
   Runtime &r = rt();
+  const ResLearn &L = r.rlearn;
+  if (r.sres_stage == 1 && !r.spec.inplace && set == L.eset && pedge == L.pedge &&
+      pecell == L.pecell && a[0].dat == L.x && a[2].dat == L.q && a[4].dat == L.adt &&
+      a[6].dat == L.res && rb == L.rb && consts_are(L.kd, L.kf, rb)) {
+    r.sres_stage = 2;  // launched by the update before, with bres_calc's increments
+    r.count_call("res_calc(speculated)");
+    return 0;
+  }
+  if (r.sres_stage && !r.settle_res()) return -1;
   if (!flush_for(r, a, nargs)) return -1;
   if (r.spec.inplace && !r.restore_spec()) return -1;
   int E = set->size, N = a[0].dat->set->size, C = a[2].dat->set->size;
@@ -461,6 +537,18 @@ int loop_bres_calc(const char *name, op_set set, int nargs, op_arg *a) {
   int rb = s.real_bytes({0, 2, 3, 4});
   if (!s.ok) return kSigMismatch;
   Runtime &r = rt();
+  {
+    const ResLearn &L = r.rlearn;
+    if (r.sres_stage == 2 && set == L.bset && pbedge == L.pbedge && pbecell == L.pbecell &&
+        a[0].dat == L.x && a[2].dat == L.q && a[3].dat == L.adt && a[4].dat == L.res &&
+        a[5].dat == L.bound && rb == L.rb && consts_are(L.kd, L.kf, rb)) {
+      r.sres_stage = 0;  // the pair the update launched is the program's
+      r.count_call("bres_calc(speculated)");
+      return 0;
+    }
+    // not the learned pair: res back to zero (and res_calc deferred again)
+    if (r.sres_stage && !r.settle_res()) return -1;
+  }
   if (r.spec.inplace && !r.restore_spec()) return -1;
   int B = set->size;
   double bytes = 16.0 * B + (double)rb * (2.0 + 4.0 + 1.0 + 8.0) * B;
@@ -504,6 +592,26 @@ int loop_bres_calc(const char *name, op_set set, int nargs, op_arg *a) {
                                           (const float *)pd.adt->data_d,
                                           (float *)pd.res->data_d, pd.kf, r.opt_pipe_block);
       r.end_loop(fused);
+      if (e == cudaSuccess) {  // the pair the next update may launch ahead
+        ResLearn &L = r.rlearn;
+        L.valid = true;
+        L.eset = pd.set;
+        L.bset = set;
+        L.pedge = pd.pedge;
+        L.pecell = pd.pecell;
+        L.pbedge = pbedge;
+        L.pbecell = pbecell;
+        L.x = pd.x;
+        L.q = pd.q;
+        L.adt = pd.adt;
+        L.res = pd.res;
+        L.bound = a[5].dat;
+        L.rb = rb;
+        L.res_bytes = pd.bytes;
+        L.fused_bytes = fused;
+        L.kd = pd.kd;
+        L.kf = pd.kf;
+      }
       pd = PendingLoop{};
       return finish(e, name);
     }
@@ -580,6 +688,7 @@ int loop_update(const char *name, op_set set, int nargs, op_arg *a) {
   // qold, write the new q into qold's array, then swap the two
   const bool rename = r.lazy.src == a[1].dat && r.lazy.dst == a[0].dat && a[2].dat != a[0].dat &&
                       a[2].dat != a[1].dat && a[3].dat != a[0].dat && a[3].dat != a[1].dat;
+  if (r.sres_stage && !r.settle_res()) return -1;  // update reads res
   if (rename ? (r.pend.kind && !r.flush_loop()) : (r.outstanding() && !r.flush_pending())) return -1;
   int C = set->size;
   double bytes = (double)rb * 17.0 * C;
@@ -633,6 +742,8 @@ int loop_update(const char *name, op_set set, int nargs, op_arg *a) {
     std::swap(a[0].dat->data_d, a[1].dat->data_d);
     r.lazy = LazySave{};
   }
+  // queue the res_calc + bres_calc that usually follow before waiting
+  launch_speculative_res(r, a, rb);
   // gbl results are valid when op_par_loop returns: the kernel's last block
   // publishes them in the mapped page, sequence number last
   volatile RedSlot *h = reinterpret_cast<volatile RedSlot *>(r.pinned);
@@ -677,8 +788,41 @@ bool op2b::Runtime::restore_spec() {
 }
 
 bool op2b::Runtime::flush_pending() {
-  const bool ok = flush_loop();
+  bool ok = settle_res();
+  ok = flush_loop() && ok;
   return materialize_save() && ok;
+}
+
+// Undo a speculative res_calc + bres_calc: the update before it left res
+// zero.  At stage 2 the program has called res_calc (and not bres_calc):
+// that call is deferred again, to be fused or launched as usual.
+bool op2b::Runtime::settle_res() {
+  if (!sres_stage) return true;
+  const int st = sres_stage;
+  sres_stage = 0;
+  const ResLearn &L = rlearn;
+  count_call("res_calc+bres_calc undone");
+  cudaError_t e = cudaMemsetAsync(L.res->data_d, 0, (size_t)L.res->set->size * L.res->size,
+                                  stream);
+  if (e != cudaSuccess) return finish(e, "res_calc+bres_calc undo") == 0;
+  if (st == 2) {
+    bool ok = pend.kind == 0 || flush_loop();
+    pend = PendingLoop{};
+    pend.kind = 2;
+    pend.set = L.eset;
+    pend.pedge = L.pedge;
+    pend.pecell = L.pecell;
+    pend.x = L.x;
+    pend.q = L.q;
+    pend.adt = L.adt;
+    pend.res = L.res;
+    pend.rb = L.rb;
+    pend.bytes = L.res_bytes;
+    pend.kd = L.kd;
+    pend.kf = L.kf;
+    return ok;
+  }
+  return true;
 }
 
 bool op2b::Runtime::materialize_save() {

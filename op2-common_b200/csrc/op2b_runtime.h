@@ -73,6 +73,27 @@ struct SpecAdt {
   AirConst<float> kf{};
 };
 
+// Speculative res_calc + bres_calc.  After an update that computed the
+// next adt_calc ahead (SpecAdt), Airfoil calls adt_calc, res_calc and
+// bres_calc with the arguments of the last fused res_calc + bres_calc pair.
+// The update call launches that pair right behind the update kernel, before
+// it waits for the update's gbl results, so the GPU never idles on the
+// host's round trip.  The update left res zero, so the launch is undone by
+// zeroing res.  `stage` follows the program: 1 launched, 2 res_calc called
+// with the learned arguments (bres_calc pending); 0 when bres_calc matched
+// too or nothing was launched.  Any other call settles it first
+// (settle_res): res back to zero, and at stage 2 res_calc deferred again.
+struct ResLearn {
+  bool valid = false;
+  op_set eset = nullptr, bset = nullptr;
+  op_map pedge = nullptr, pecell = nullptr, pbedge = nullptr, pbecell = nullptr;
+  op_dat x = nullptr, q = nullptr, adt = nullptr, res = nullptr, bound = nullptr;
+  int rb = 0;
+  double res_bytes = 0.0, fused_bytes = 0.0;
+  AirConst<double> kd{};  // constants of the learned (and the launched) pair
+  AirConst<float> kf{};
+};
+
 struct Runtime {
   bool initialised = false;
   int device = 0, nsm = 148, cc_major = 0, cc_minor = 0;
@@ -96,6 +117,7 @@ struct Runtime {
   int opt_adt_minb = 0;       // adt_calc: __launch_bounds__ minimum blocks (0 = none)
   int opt_host_mirror = 1;    // op_dat::data holds a host copy of the declared values
   int opt_rename_save = 1;    // save_soln by renaming (LazySave)
+  int opt_speculate_res = 1;  // update launches the res_calc + bres_calc after it (ResLearn)
   int opt_pipe_block = 256;   // threads per CTA of the pipelined gather (64, 96, 128, 256)
   int opt_pipe_hints = 0;     // register pipeline: evict-first hints on once-read streams
   int opt_plan_mode = 0;      // 0 = parallel block colouring, 1 = serial greedy (bit-exact)
@@ -129,6 +151,8 @@ struct Runtime {
 
   PendingLoop pend;
   LazySave lazy;
+  ResLearn rlearn;
+  int sres_stage = 0;  // speculative res_calc + bres_calc: 0 none, 1 launched, 2 res_calc seen
   SpecAdt spec;
   std::set<op_dat> exposed;  // dats whose device pointer was handed out (no speculation)
   std::set<op_dat> zero_mirror;  // dats declared without data: their host copy is zeros
@@ -139,8 +163,9 @@ struct Runtime {
   // initialised, with any deferred loop launched (false on error)
   bool ready();
   // a deferred loop or a renamed save_soln is outstanding
-  bool outstanding() const { return pend.kind != 0 || lazy.src != nullptr; }
-  bool flush_pending();     // op2b_dispatch.cpp: both launched
+  bool outstanding() const { return pend.kind != 0 || lazy.src != nullptr || sres_stage != 0; }
+  bool flush_pending();     // op2b_dispatch.cpp: everything settled and launched
+  bool settle_res();        // op2b_dispatch.cpp: undo a speculative res_calc + bres_calc
   bool flush_loop();        // op2b_dispatch.cpp: the deferred loop only
   bool materialize_save();  // op2b_dispatch.cpp: the renamed save_soln's copy
   bool restore_spec();   // op2b_dispatch.cpp: put the old adt back if adt is ahead

@@ -265,6 +265,86 @@ def test_speculative_adt_restored_for_other_readers(op2):
         assert np.array_equal(res[0][k], res[1][k]), k
 
 
+def test_speculative_res_calc_is_bit_identical(op2):
+    """update launching the res_calc + bres_calc pair that follows it
+    (speculate_res) gives the same fields and history as waiting for the
+    program's calls, in both precisions; every pair after the first is
+    launched ahead."""
+    m = M.channel_bump(96, 48, seed=16)
+    for dtype in (np.float64, np.float32):
+        out, hists, seen = [], [], []
+        for spec in (0, 1):
+            op2.set_option("speculate_res", spec)
+            op2.load().op2b_reset_stats()
+            app = Airfoil(m, dtype=dtype)
+            hists.append(app.iterate(5))
+            out.append(app.fetch())
+            seen.append(op2.loop_stats("bres_calc(speculated)"))
+            op2.op_exit()
+            op2.op_init()
+        assert hists[0] == hists[1], dtype
+        for k in ("q", "qold", "adt", "res"):
+            assert np.array_equal(out[0][k], out[1][k]), (dtype, k)
+        assert seen[0] is None and seen[1]["calls"] == 9
+
+
+def test_speculative_res_calc_is_invisible(op2):
+    """Whatever the program does between update and the res_calc /
+    bres_calc it is expected to call, it sees the state of the calls it
+    made: res zero after update, res_calc's increments alone after res_calc,
+    and a changed constant or a skipped loop gives the results of the
+    program's own order."""
+    m = M.channel_bump(64, 32, seed=17)
+
+    def run(spec, between, after):
+        op2.set_option("speculate_res", spec)
+        app = Airfoil(m)
+        app.iterate(1)
+        for i in (1, 2, 3, 4):        # adt_calc, res_calc, bres_calc, update
+            app._loop(i)
+        seen = between(app)
+        for i in after:
+            app._loop(i)
+        got = app.fetch()
+        op2.op_exit()
+        op2.op_init()
+        return seen, got
+
+    def res_now(app):
+        return app.fetch()["res"]
+
+    def res_after_adt(app):
+        app._loop(1)
+        return app.fetch()["res"]
+
+    def res_after_res_calc(app):
+        app._loop(1)
+        app._loop(2)
+        return app.fetch()["res"]
+
+    def new_eps(app):
+        app._loop(1)
+        op2.op_decl_const(1, "double", 0.07, "eps")
+        return None
+
+    def res_calc_then_update(app):   # bres_calc skipped
+        app._loop(1)
+        app._loop(2)
+        return None
+
+    cases = [(res_now, (1, 2, 3, 4)), (res_after_adt, (2, 3, 4)),
+             (res_after_res_calc, (3, 4)), (new_eps, (2, 3, 4)),
+             (res_calc_then_update, (4, 1, 2, 3))]
+    for between, after in cases:
+        s0, g0 = run(0, between, after)
+        s1, g1 = run(1, between, after)
+        if s0 is not None:
+            assert np.array_equal(s0, s1), between.__name__
+        for k in ("q", "qold", "adt", "res"):
+            assert np.array_equal(g0[k], g1[k]), (between.__name__, k)
+    assert np.all(run(1, res_now, ())[0] == 0)
+
+
 def test_fused_loop_pairs_are_bit_identical_to_separate_loops(op2):
     """The runtime defers save_soln and res_calc and fuses them with the
     adt_calc / bres_calc that follow; with fusion off every loop launches on
