@@ -367,9 +367,12 @@ def main():
         K = max(args.e2e_iters, 1)
         t0 = time.perf_counter()
         app2 = Airfoil(hm, dtype=dtype)
+        ta = time.perf_counter()
         if args.numbering == "rcm":
             app2.renumber()
+        tb = time.perf_counter()
         app2.iterate(K)
+        tc = time.perf_counter()
         q = L.op_fetch_data(app2.p_q)
         t1 = time.perf_counter()
         barrier()
@@ -382,6 +385,10 @@ def main():
                + m.ncell * 4 * es)
         d2h = q.nbytes + K * 2 * 32  # q, and the update's reduction read back per call
         e2e = {"value": ms_e2e, "unit": "ms/iter", "iterations": K,
+               "phases_ms": {"declare": round(1e3 * (ta - t0), 1),
+                             "renumber": round(1e3 * (tb - ta), 1),
+                             "iterate": round(1e3 * (tc - tb), 1),
+                             "fetch": round(1e3 * (t1 - tc), 1)},
                "h2d_bytes_per_step": int(h2d / K),
                "d2h_bytes_per_step": int(d2h / K),
                "note": f"per iteration of a whole {K}-iteration job through the API: "

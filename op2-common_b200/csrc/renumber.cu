@@ -148,13 +148,20 @@ __device__ int rcm_block_scan(int v, int *total) {
 constexpr int kB = 2;   // vertices a thread handles per round
 constexpr int kNb = 4;  // neighbours per vertex loaded unrolled (the rest in a loop)
 
+// A vertex is closed to a level walk once ordered before position `thr`
+// (thr = INT_MAX: ordered at all).
+__device__ __forceinline__ bool rcm_open(const RcmWork &w, int v, int thr) {
+  const int p = w.newidx[v];
+  return p < 0 || p >= thr;
+}
+
 // The first kNb unvisited neighbours of up to kB level vertices
 // (cur[j0 + k * blockDim.x]); v = -1 where there is none.
 struct LevelBatch {
   int d[kB];
   long long r[kB];
   int v[kB][kNb];
-  __device__ void load(const RcmWork &w, const int *cur, int len, int j0) {
+  __device__ void load(const RcmWork &w, const int *cur, int len, int j0, int thr = INT_MAX) {
     int u[kB];
 #pragma unroll
     for (int k = 0; k < kB; k++) {
@@ -174,7 +181,7 @@ struct LevelBatch {
     for (int k = 0; k < kB; k++)
 #pragma unroll
       for (int t = 0; t < kNb; t++)
-        if (v[k][t] >= 0 && w.newidx[v[k][t]] >= 0) v[k][t] = -1;
+        if (v[k][t] >= 0 && !rcm_open(w, v[k][t], thr)) v[k][t] = -1;
   }
 };
 
@@ -221,9 +228,11 @@ struct ParentBatch {
   }
 };
 
-// BFS from `start` over vertices not yet ordered; marks with `stamp`.
-// Returns the number of levels; the last level is left in *last (lev_a or lev_b).
-__device__ int rcm_bfs(RcmWork &w, int start, int stamp, int **last, int *last_len) {
+// BFS from `start` over vertices not ordered before position `thr`; marks
+// with `stamp`.  Returns the number of levels; the last level is left in
+// *last (lev_a or lev_b).
+__device__ int rcm_bfs(RcmWork &w, int start, int stamp, int **last, int *last_len,
+                       int thr = INT_MAX) {
   __shared__ int s_len, s_next;
   int *cur = w.lev_a, *nxt = w.lev_b;
   if (threadIdx.x == 0) {
@@ -243,7 +252,7 @@ __device__ int rcm_bfs(RcmWork &w, int start, int stamp, int **last, int *last_l
     // a handful of memory latencies however many vertices it covers
     for (int j0 = threadIdx.x; j0 < len; j0 += kB * blockDim.x) {
       LevelBatch b;
-      b.load(w, cur, len, j0);
+      b.load(w, cur, len, j0, thr);
       // all exchanges first (none waits on another's result), then the appends
       int old[kB][kNb];
 #pragma unroll
@@ -260,7 +269,7 @@ __device__ int rcm_bfs(RcmWork &w, int start, int stamp, int **last, int *last_l
       for (int k = 0; k < kB; k++)
         for (int t = kNb; t < b.d[k]; t++) {  // vertices of higher degree
           int v = w.col[b.r[k] + t];
-          if (w.newidx[v] < 0 && atomicExch(&w.mark[v], stamp) != stamp)
+          if (rcm_open(w, v, thr) && atomicExch(&w.mark[v], stamp) != stamp)
             nxt[atomicAdd(&s_next, 1)] = v;
         }
     }
@@ -279,16 +288,158 @@ __device__ int rcm_bfs(RcmWork &w, int start, int stamp, int **last, int *last_l
   }
 }
 
+// George-Liu candidate of a last level: minimum degree, lowest id on ties
+__device__ int rcm_pick(const RcmWork &w, const int *last, int last_len) {
+  __shared__ int s_best, s_bestdeg;
+  if (threadIdx.x == 0) {
+    s_best = INT_MAX;
+    s_bestdeg = INT_MAX;
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < last_len; j += blockDim.x) atomicMin(&s_bestdeg, w.deg[last[j]]);
+  __syncthreads();
+  for (int j = threadIdx.x; j < last_len; j += blockDim.x) {
+    int v = last[j];
+    if (w.deg[v] == s_bestdeg) atomicMin(&s_best, v);
+  }
+  __syncthreads();
+  const int cand = s_best;
+  __syncthreads();  // s_best is reused by the next call
+  return cand;
+}
+
+// Cuthill-McKee from `start`: appends its component to the order at
+// s_pos (shared).  Its levels are the BFS levels from `start`: returns
+// their number and leaves the last level in *last.
+__device__ int rcm_cm(RcmWork &w, int start, int &s_pos, int &s_len, int **last,
+                      int *last_len) {
+  int *cur = w.lev_a, *nxt = w.lev_b;
+  if (threadIdx.x == 0) {
+    cur[0] = start;
+    w.newidx[start] = s_pos++;
+    s_len = 1;
+  }
+  __syncthreads();
+  int nlev = 0;
+  while (true) {
+    const int len = s_len;
+    const int base = s_pos;
+    nlev++;
+    // first parent (lowest position in this level) of every new vertex
+    for (int j0 = threadIdx.x; j0 < len; j0 += kB * blockDim.x) {
+      LevelBatch b;
+      b.load(w, cur, len, j0);
+#pragma unroll
+      for (int k = 0; k < kB; k++) {
+        const int j = j0 + k * (int)blockDim.x;
+#pragma unroll
+        for (int t = 0; t < kNb; t++)
+          if (b.v[k][t] >= 0) atomicMin(&w.pkey[b.v[k][t]], j);
+        for (int t = kNb; t < b.d[k]; t++) {
+          int v = w.col[b.r[k] + t];
+          if (w.newidx[v] < 0) atomicMin(&w.pkey[v], j);
+        }
+      }
+    }
+    __syncthreads();
+    // The next level is the parents' claimed vertices, parent by parent in
+    // level order and, within a parent, by (degree capped at 63, id): the
+    // order sequential Cuthill-McKee appends them in.  Each thread takes a
+    // contiguous run of parents; a block scan of the runs' counts places
+    // them, so no sort of the level is needed.
+    const int chunk = (len + (int)blockDim.x - 1) / (int)blockDim.x;
+    const int jb = min(len, (int)threadIdx.x * chunk), je = min(len, jb + chunk);
+    int mine = 0;
+    for (int j0 = jb; j0 < je; j0 += kB) {
+      ParentBatch pb;
+      pb.load(w, cur, j0, je);
+#pragma unroll
+      for (int k = 0; k < kB; k++) mine += pb.count(w, k, j0 + k);
+    }
+    int nl = 0;
+    int pos = rcm_block_scan(mine, &nl);
+    if (nl == 0) {
+      *last = cur;
+      *last_len = len;
+      return nlev;
+    }
+    for (int j0 = jb; j0 < je; j0 += kB) {
+      ParentBatch pb;
+      pb.load(w, cur, j0, je);
+#pragma unroll
+      for (int k = 0; k < kB; k++) {
+        const int j = j0 + k;
+        if (j >= je) break;
+        const int first = pos;
+        if (pb.d[k] <= kNb) {
+          // the claimed children's (degree capped at 63, id) keys, sorted in registers
+          unsigned long long key[kNb];
+#pragma unroll
+          for (int t = 0; t < kNb; t++)
+            key[t] = pb.claimed(k, t, j)
+                         ? ((unsigned long long)(unsigned)min(pb.vd[k][t], 63) << 32) |
+                               (unsigned)pb.v[k][t]
+                         : ~0ull;
+#pragma unroll
+          for (int i = 1; i < kNb; i++)
+#pragma unroll
+            for (int m = i; m > 0; m--)
+              if (key[m] < key[m - 1]) {
+                unsigned long long x = key[m];
+                key[m] = key[m - 1];
+                key[m - 1] = x;
+              }
+#pragma unroll
+          for (int t = 0; t < kNb; t++)
+            if (key[t] != ~0ull) nxt[pos++] = (int)(key[t] & 0xffffffffull);
+        } else {
+          // higher degree: selection of the smallest claimed key above the last
+          unsigned long long last = 0;
+          bool any = false;
+          while (true) {
+            unsigned long long best = ~0ull;
+            for (int t = 0; t < pb.d[k]; t++) {
+              int v = w.col[pb.r[k] + t];
+              if (w.newidx[v] < 0 && w.pkey[v] == j) {
+                unsigned long long key =
+                    ((unsigned long long)(unsigned)min(w.deg[v], 63) << 32) | (unsigned)v;
+                if ((!any || key > last) && key < best) best = key;
+              }
+            }
+            if (best == ~0ull) break;
+            nxt[pos++] = (int)(best & 0xffffffffull);
+            last = best;
+            any = true;
+          }
+        }
+        for (int q = first; q < pos; q++) {
+          int v = nxt[q];
+          w.newidx[v] = base + q;
+          w.pkey[v] = INT_MAX;
+        }
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      s_pos = base + nl;
+      s_len = nl;
+    }
+    int *t = cur;
+    cur = nxt;
+    nxt = t;
+    __syncthreads();
+  }
+}
+
 __global__ void __launch_bounds__(kRcmThreads) k_rcm(RcmWork w) {
-  __shared__ int s_start, s_len, s_best, s_bestdeg;
+  __shared__ int s_start, s_len;
   __shared__ int s_pos;
   int stamp = 1;
   if (threadIdx.x == 0) s_pos = 0;
   __syncthreads();
   while (s_pos < w.n) {
     // an unvisited vertex of minimum degree, lowest id on ties (a corner of a
-    // structured mesh region: usually already pseudo-peripheral, which saves
-    // the pseudo-peripheral search a BFS)
+    // structured mesh region: usually already pseudo-peripheral)
     {
       __shared__ unsigned long long s_key[kRcmThreads / 32];
       unsigned long long best = ~0ull;
@@ -311,139 +462,34 @@ __global__ void __launch_bounds__(kRcmThreads) k_rcm(RcmWork w) {
       __syncthreads();
     }
     int start = s_start;
-    // George-Liu pseudo-peripheral vertex
+    const int comp_base = s_pos;
+    // George-Liu pseudo-peripheral vertex.  Its first BFS, from `start`, has
+    // the levels of Cuthill-McKee from `start`: order the component from
+    // `start` straight away and test that order's last level.  When the
+    // candidate found there has no larger eccentricity -- the usual case --
+    // the order stands; otherwise it is undone and the search goes on as
+    // before.
     int *last;
     int last_len;
-    int ecc = rcm_bfs(w, start, stamp++, &last, &last_len);
-    for (int round = 0; round < 8; round++) {
-      if (threadIdx.x == 0) {
-        s_best = INT_MAX;
-        s_bestdeg = INT_MAX;
-      }
+    int ecc = rcm_cm(w, start, s_pos, s_len, &last, &last_len);
+    int cand = rcm_pick(w, last, last_len);
+    int e2 = rcm_bfs(w, cand, stamp++, &last, &last_len, comp_base);
+    if (e2 > ecc) {
+      for (int v = threadIdx.x; v < w.n; v += blockDim.x)
+        if (w.newidx[v] >= comp_base) w.newidx[v] = -1;
       __syncthreads();
-      for (int j = threadIdx.x; j < last_len; j += blockDim.x) atomicMin(&s_bestdeg, w.deg[last[j]]);
+      if (threadIdx.x == 0) s_pos = comp_base;
       __syncthreads();
-      for (int j = threadIdx.x; j < last_len; j += blockDim.x) {
-        int v = last[j];
-        if (w.deg[v] == s_bestdeg) atomicMin(&s_best, v);
-      }
-      __syncthreads();
-      int cand = s_best;
-      int e2 = rcm_bfs(w, cand, stamp++, &last, &last_len);
-      if (e2 <= ecc) break;  // no longer eccentricity: keep the current start
       ecc = e2;
       start = cand;
-    }
-    // Cuthill-McKee from `start`
-    int *cur = w.lev_a, *nxt = w.lev_b;
-    if (threadIdx.x == 0) {
-      cur[0] = start;
-      w.newidx[start] = s_pos++;
-      s_len = 1;
-    }
-    __syncthreads();
-    while (true) {
-      const int len = s_len;
-      const int base = s_pos;
-      // first parent (lowest position in this level) of every new vertex
-      for (int j0 = threadIdx.x; j0 < len; j0 += kB * blockDim.x) {
-        LevelBatch b;
-        b.load(w, cur, len, j0);
-#pragma unroll
-        for (int k = 0; k < kB; k++) {
-          const int j = j0 + k * (int)blockDim.x;
-#pragma unroll
-          for (int t = 0; t < kNb; t++)
-            if (b.v[k][t] >= 0) atomicMin(&w.pkey[b.v[k][t]], j);
-          for (int t = kNb; t < b.d[k]; t++) {
-            int v = w.col[b.r[k] + t];
-            if (w.newidx[v] < 0) atomicMin(&w.pkey[v], j);
-          }
-        }
+      for (int round = 1; round < 8; round++) {
+        cand = rcm_pick(w, last, last_len);
+        e2 = rcm_bfs(w, cand, stamp++, &last, &last_len);
+        if (e2 <= ecc) break;  // no longer eccentricity: keep the current start
+        ecc = e2;
+        start = cand;
       }
-      __syncthreads();
-      // The next level is the parents' claimed vertices, parent by parent in
-      // level order and, within a parent, by (degree capped at 63, id): the
-      // order sequential Cuthill-McKee appends them in.  Each thread takes a
-      // contiguous run of parents; a block scan of the runs' counts places
-      // them, so no sort of the level is needed.
-      const int chunk = (len + (int)blockDim.x - 1) / (int)blockDim.x;
-      const int jb = min(len, (int)threadIdx.x * chunk), je = min(len, jb + chunk);
-      int mine = 0;
-      for (int j0 = jb; j0 < je; j0 += kB) {
-        ParentBatch pb;
-        pb.load(w, cur, j0, je);
-#pragma unroll
-        for (int k = 0; k < kB; k++) mine += pb.count(w, k, j0 + k);
-      }
-      int nl = 0;
-      int pos = rcm_block_scan(mine, &nl);
-      if (nl == 0) break;
-      for (int j0 = jb; j0 < je; j0 += kB) {
-        ParentBatch pb;
-        pb.load(w, cur, j0, je);
-#pragma unroll
-        for (int k = 0; k < kB; k++) {
-          const int j = j0 + k;
-          if (j >= je) break;
-          const int first = pos;
-          if (pb.d[k] <= kNb) {
-            // the claimed children's (degree capped at 63, id) keys, sorted in registers
-            unsigned long long key[kNb];
-#pragma unroll
-            for (int t = 0; t < kNb; t++)
-              key[t] = pb.claimed(k, t, j)
-                           ? ((unsigned long long)(unsigned)min(pb.vd[k][t], 63) << 32) |
-                                 (unsigned)pb.v[k][t]
-                           : ~0ull;
-#pragma unroll
-            for (int i = 1; i < kNb; i++)
-#pragma unroll
-              for (int m = i; m > 0; m--)
-                if (key[m] < key[m - 1]) {
-                  unsigned long long x = key[m];
-                  key[m] = key[m - 1];
-                  key[m - 1] = x;
-                }
-#pragma unroll
-            for (int t = 0; t < kNb; t++)
-              if (key[t] != ~0ull) nxt[pos++] = (int)(key[t] & 0xffffffffull);
-          } else {
-            // higher degree: selection of the smallest claimed key above the last
-            unsigned long long last = 0;
-            bool any = false;
-            while (true) {
-              unsigned long long best = ~0ull;
-              for (int t = 0; t < pb.d[k]; t++) {
-                int v = w.col[pb.r[k] + t];
-                if (w.newidx[v] < 0 && w.pkey[v] == j) {
-                  unsigned long long key =
-                      ((unsigned long long)(unsigned)min(w.deg[v], 63) << 32) | (unsigned)v;
-                  if ((!any || key > last) && key < best) best = key;
-                }
-              }
-              if (best == ~0ull) break;
-              nxt[pos++] = (int)(best & 0xffffffffull);
-              last = best;
-              any = true;
-            }
-          }
-          for (int q = first; q < pos; q++) {
-            int v = nxt[q];
-            w.newidx[v] = base + q;
-            w.pkey[v] = INT_MAX;
-          }
-        }
-      }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        s_pos = base + nl;
-        s_len = nl;
-      }
-      int *t = cur;
-      cur = nxt;
-      nxt = t;
-      __syncthreads();
+      rcm_cm(w, start, s_pos, s_len, &last, &last_len);
     }
     __syncthreads();
   }
