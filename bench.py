@@ -328,9 +328,11 @@ def main():
                   {"gather_kernel": 5, "pipe_block": 128}, {"gather_kernel": 5, "pipe_block": 256},
                   {"gather_kernel": 6, "pipe_block": 128}, {"gather_kernel": 6, "pipe_block": 256},
                   {"gather_kernel": 6, "pipe_block": 256, "bres_kernel": 0},
-                  {"speculate_res": 0}, {"rename_save": 0, "speculate_res": 0},
-                  {"speculate_adt": 0, "rename_save": 0},
-                  {"fuse": 0, "speculate_adt": 0, "rename_save": 0}):
+                  {"lazy_res": 0}, {"speculate_res": 0, "lazy_res": 0},
+                  {"rename_save": 0, "speculate_res": 0, "lazy_res": 0},
+                  {"speculate_adt": 0, "rename_save": 0, "speculate_res": 0, "lazy_res": 0},
+                  {"fuse": 0, "speculate_adt": 0, "rename_save": 0, "speculate_res": 0,
+                   "lazy_res": 0}):
             v = timed_run(L, Airfoil, m, dtype, "rcm", 3, args.part_size, 20, 3, torch, barrier,
                           opts=o)
             lp = v["loops"]

@@ -309,7 +309,7 @@ template <typename T> struct AdtNext {
   AirConst<T> k;
 };
 
-template <typename T, int THREADS, bool ADT>
+template <typename T, int THREADS, bool ADT, bool KEEP_RES = false>
 __global__ void __launch_bounds__(THREADS)
 k_update(int ncell, const T *__restrict__ qold, T *__restrict__ q, T *__restrict__ res,
          const T *adt, RedSlot *__restrict__ parts, unsigned *__restrict__ counter,
@@ -348,8 +348,10 @@ k_update(int ncell, const T *__restrict__ qold, T *__restrict__ q, T *__restrict
       }
     }
     Vec<T>::st4(q + 4 * (size_t)n, qn);
-    T z[4] = {(T)0, (T)0, (T)0, (T)0};
-    Vec<T>::st4(res + 4 * (size_t)n, z);
+    if constexpr (!KEEP_RES) {
+      T z[4] = {(T)0, (T)0, (T)0, (T)0};
+      Vec<T>::st4(res + 4 * (size_t)n, z);
+    }
     if constexpr (ADT)
       an.adt[n] = air_adt<T>(x1x, x1y, x2x, x2y, x3x, x3y, x4x, x4y, qn[0], qn[1], qn[2],
                              qn[3], an.k);
@@ -388,15 +390,24 @@ k_update(int ncell, const T *__restrict__ qold, T *__restrict__ q, T *__restrict
 template <typename T>
 cudaError_t launch_update(const LaunchCtx &c, int ncell, const T *qold, T *q, T *res,
                           const T *adt, const RedScratch &s, const int *pcell, const T *x,
-                          T *adt_backup, const AirConst<T> *k) {
+                          T *adt_backup, const AirConst<T> *k, bool keep_res) {
   constexpr int TH = 256;
   int grid = grid_for(c, ncell, TH, 4);
   if (grid > s.capacity) grid = s.capacity;
   if (adt_backup) {
     const AdtNext<T> an{reinterpret_cast<const int4 *>(pcell), x, const_cast<T *>(adt),
                         adt_backup, *k};
-    k_update<T, TH, true><<<grid, TH, 0, c.stream>>>(ncell, qold, q, res, adt, s.parts,
-                                                     s.counter, s.out, s.host_out, s.seq, an);
+    if (keep_res)
+      k_update<T, TH, true, true><<<grid, TH, 0, c.stream>>>(ncell, qold, q, res, adt, s.parts,
+                                                             s.counter, s.out, s.host_out,
+                                                             s.seq, an);
+    else
+      k_update<T, TH, true><<<grid, TH, 0, c.stream>>>(ncell, qold, q, res, adt, s.parts,
+                                                       s.counter, s.out, s.host_out, s.seq, an);
+  } else if (keep_res) {
+    k_update<T, TH, false, true><<<grid, TH, 0, c.stream>>>(ncell, qold, q, res, adt, s.parts,
+                                                            s.counter, s.out, s.host_out,
+                                                            s.seq, AdtNext<T>{});
   } else {
     k_update<T, TH, false><<<grid, TH, 0, c.stream>>>(ncell, qold, q, res, adt, s.parts,
                                                       s.counter, s.out, s.host_out, s.seq,
@@ -438,10 +449,10 @@ template cudaError_t launch_bres_calc_atomic<float>(const LaunchCtx &, int, cons
 template cudaError_t launch_update<double>(const LaunchCtx &, int, const double *, double *,
                                            double *, const double *, const RedScratch &,
                                            const int *, const double *, double *,
-                                           const AirConst<double> *);
+                                           const AirConst<double> *, bool);
 template cudaError_t launch_update<float>(const LaunchCtx &, int, const float *, float *,
                                           float *, const float *, const RedScratch &,
                                           const int *, const float *, float *,
-                                          const AirConst<float> *);
+                                          const AirConst<float> *, bool);
 
 } // namespace op2b

@@ -377,7 +377,7 @@ struct BresLink {
   const int *bound;
 };
 
-template <typename T, bool BRES = false>
+template <typename T, bool BRES = false, bool ZERO = false>
 __device__ __forceinline__ void load_corner_cell(CornerOps<T> &d, int c, const CornerRec &r,
                                                  const T *__restrict__ x,
                                                  const T *__restrict__ q,
@@ -385,7 +385,12 @@ __device__ __forceinline__ void load_corner_cell(CornerOps<T> &d, int c, const C
                                                  const T *__restrict__ res,
                                                  const BresLink &bl = BresLink{}) {
   Vec<T>::ld4(q + 4 * (size_t)c, d.qc);
-  Vec<T>::ld4_rw(res + 4 * (size_t)c, d.rs);
+  if constexpr (ZERO) {  // res known to be zero: the sums start from +0, as from the array
+#pragma unroll
+    for (int j = 0; j < 4; j++) d.rs[j] = (T)0;
+  } else {
+    Vec<T>::ld4_rw(res + 4 * (size_t)c, d.rs);
+  }
   d.ac = __ldg(adt + c);
   const int nd[4] = {r.cn.x, r.cn.y, r.cn.z, r.cn.w};
 #pragma unroll
@@ -492,7 +497,7 @@ k_res_gather_corner(int ncell, const int4 *__restrict__ rec_o, const int4 *__res
 // res_calc and the bres_calc that follows it in one launch (the runtime
 // defers res_calc until the next loop call; when that is bres_calc on the
 // same res, q, adt and x, this kernel runs instead of both)
-template <typename T, int NT>
+template <typename T, int NT, bool ZERO = false>
 __global__ void __launch_bounds__(NT, 1)
 k_res_bres_corner(int ncell, const int4 *__restrict__ rec_o, const int4 *__restrict__ rec_cn,
                   const unsigned *__restrict__ rec_meta, const T *__restrict__ x,
@@ -505,11 +510,11 @@ k_res_bres_corner(int ncell, const int4 *__restrict__ rec_o, const int4 *__restr
   CornerRec r1 = load_crec(rec_o, rec_cn, rec_meta, c + G, ncell);
   {
     const CornerRec r0 = load_crec(rec_o, rec_cn, rec_meta, c, ncell);
-    load_corner_cell<T, true>(cur, c, r0, x, q, adt, res, bl);
+    load_corner_cell<T, true, ZERO>(cur, c, r0, x, q, adt, res, bl);
   }
   for (; c < ncell; c += G) {
     const CornerRec r2 = load_crec(rec_o, rec_cn, rec_meta, c + 2 * G, ncell);
-    if (c + G < ncell) load_corner_cell<T, true>(nxt, c + G, r1, x, q, adt, res, bl);
+    if (c + G < ncell) load_corner_cell<T, true, ZERO>(nxt, c + G, r1, x, q, adt, res, bl);
     compute_corner<T, true>(cur, c, res, k);
     cur = nxt;
     r1 = r2;
@@ -552,7 +557,7 @@ template <typename T>
 cudaError_t launch_res_bres_corner(const LaunchCtx &ctx, const SlotRecords &s,
                                    const BresRecords &b, const int *bound, const T *x,
                                    const T *q, const T *adt, T *res, const AirConst<T> &k,
-                                   int block) {
+                                   int block, bool zero_res) {
   if (s.ncell <= 0) return cudaSuccess;
   (void)b;
   const BresLink bl{bound};
@@ -569,6 +574,9 @@ cudaError_t launch_res_bres_corner(const LaunchCtx &ctx, const SlotRecords &s,
     ctx.count();
     return cudaGetLastError();
   };
+  if (zero_res)
+    return block == 128 ? run(k_res_bres_corner<T, 128, true>, 128)
+                        : run(k_res_bres_corner<T, 256, true>, 256);
   return block == 128 ? run(k_res_bres_corner<T, 128>, 128) : run(k_res_bres_corner<T, 256>, 256);
 }
 
@@ -576,11 +584,11 @@ template cudaError_t launch_res_bres_corner<double>(const LaunchCtx &, const Slo
                                                     const BresRecords &, const int *,
                                                     const double *, const double *,
                                                     const double *, double *,
-                                                    const AirConst<double> &, int);
+                                                    const AirConst<double> &, int, bool);
 template cudaError_t launch_res_bres_corner<float>(const LaunchCtx &, const SlotRecords &,
                                                    const BresRecords &, const int *, const float *,
                                                    const float *, const float *, float *,
-                                                   const AirConst<float> &, int);
+                                                   const AirConst<float> &, int, bool);
 
 template cudaError_t launch_res_calc_gather_corner<double>(const LaunchCtx &, const SlotRecords &,
                                                            const double *, const double *,

@@ -101,12 +101,14 @@ cudaError_t launch_bres_calc_records(const LaunchCtx &c, const BresRecords &b, c
 // edge finds no unused slot or has a node that is not a corner of its cell, or
 // the corner records are not usable; the loops then run one after the other.
 bool link_boundary_records(const SlotRecords *s, const BresRecords *b, op_map pbecell);
-// airfoil_pipe.cu: the fused kernel (block 128 or 256)
+// airfoil_pipe.cu: the fused kernel (block 128 or 256).  zero_res: res is
+// known to be all zeros (the update before left it so without writing it):
+// the kernel starts each cell's sums from 0 instead of reading res.
 template <typename T>
 cudaError_t launch_res_bres_corner(const LaunchCtx &c, const SlotRecords &s,
                                    const BresRecords &b, const int *bound, const T *x,
                                    const T *q, const T *adt, T *res, const AirConst<T> &k,
-                                   int block);
+                                   int block, bool zero_res = false);
 
 template <typename T>
 cudaError_t launch_res_calc_gather(const LaunchCtx &c, const InvMap &inv, const int *pedge,

@@ -401,6 +401,8 @@ void op_exit(void) {
   r.opt_host_mirror = d.opt_host_mirror;
   r.opt_rename_save = d.opt_rename_save;
   r.opt_speculate_res = d.opt_speculate_res;
+  r.opt_lazy_res = d.opt_lazy_res;
+  r.res_zero = nullptr;
   r.lazy = LazySave{};
   r.rlearn = ResLearn{};
   r.sres_stage = 0;
@@ -1045,6 +1047,8 @@ int op2b_set_option(const char *key, long value) {
     r.opt_rename_save = value != 0;
   } else if (k == "speculate_res") {
     r.opt_speculate_res = value != 0;
+  } else if (k == "lazy_res") {
+    r.opt_lazy_res = value != 0;
   } else {
     set_error("op2b_set_option: unknown option '%s'", k.c_str());
     return -1;
@@ -1074,6 +1078,7 @@ long op2b_get_option(const char *key) {
   if (k == "host_mirror") return r.opt_host_mirror;
   if (k == "rename_save") return r.opt_rename_save;
   if (k == "speculate_res") return r.opt_speculate_res;
+  if (k == "lazy_res") return r.opt_lazy_res;
   if (k == "nsm") return r.nsm;
   return -1;
 }

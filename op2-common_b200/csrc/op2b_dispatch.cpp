@@ -189,14 +189,22 @@ bool res_compatible(const Runtime &r, const op_arg *a, int nargs) {
   return true;
 }
 
+bool touches(const op_arg *a, int nargs, op_dat d) {
+  for (int i = 0; i < nargs; i++)
+    if (a[i].argtype == OP_ARG_DAT && a[i].dat == d) return true;
+  return false;
+}
+
 // Settle what is outstanding before a loop with these arguments: a
-// speculative res_calc + bres_calc and a renamed save_soln stay when the
-// loop can run beside them; the deferred loop is launched.
-bool flush_for(Runtime &r, const op_arg *a, int nargs) {
+// speculative res_calc + bres_calc, a renamed save_soln and a res known to be
+// zero stay when the loop can run beside them; the deferred loop is launched.
+// keep_zero: the caller handles res_zero itself (a res_calc it defers).
+bool flush_for(Runtime &r, const op_arg *a, int nargs, bool keep_zero = false) {
   bool ok = true;
   if (r.sres_stage && !res_compatible(r, a, nargs)) ok = r.settle_res();
   if (r.pend.kind) ok = r.flush_loop() && ok;
   if (r.lazy.src && !save_compatible(r, a, nargs)) ok = r.materialize_save() && ok;
+  if (r.res_zero && !keep_zero && touches(a, nargs, r.res_zero)) ok = r.materialize_res() && ok;
   return ok;
 }
 
@@ -234,17 +242,18 @@ void launch_speculative_res(Runtime &r, const op_arg *a, int rb) {
     return;
   }
   const int *bound = (const int *)L.bound->data_d;
+  const bool zero = r.res_zero == L.res;  // the update left res zero without writing it
   cudaError_t e;
   r.begin_loop("res_calc+bres_calc");
   if (rb == 8)
     e = launch_res_bres_corner<double>(r.ctx(), *cr, *br, bound, (const double *)L.x->data_d,
                                        (const double *)L.q->data_d, (const double *)L.adt->data_d,
-                                       (double *)L.res->data_d, L.kd, r.opt_pipe_block);
+                                       (double *)L.res->data_d, L.kd, r.opt_pipe_block, zero);
   else
     e = launch_res_bres_corner<float>(r.ctx(), *cr, *br, bound, (const float *)L.x->data_d,
                                       (const float *)L.q->data_d, (const float *)L.adt->data_d,
-                                      (float *)L.res->data_d, L.kf, r.opt_pipe_block);
-  r.end_loop(L.fused_bytes);
+                                      (float *)L.res->data_d, L.kf, r.opt_pipe_block, zero);
+  r.end_loop(L.fused_bytes - (zero ? L.res_read_bytes : 0.0));
   if (e == cudaSuccess) r.sres_stage = 1;
   else cudaGetLastError();  // not launched: the program's calls run as usual
 }
@@ -436,7 +445,7 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
     return 0;
   }
   if (r.sres_stage && !r.settle_res()) return -1;
-  if (!flush_for(r, a, nargs)) return -1;
+  if (!flush_for(r, a, nargs, true)) return -1;
   if (r.spec.inplace && !r.restore_spec()) return -1;
   int E = set->size, N = a[0].dat->set->size, C = a[2].dat->set->size;
   double bytes = 16.0 * E + (double)rb * (2.0 * N + 13.0 * C);
@@ -469,6 +478,8 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
       return 0;
     }
   }
+  // launched now: a res known to be zero gets its zeros first
+  if (r.res_zero && touches(a, nargs, r.res_zero) && !r.materialize_res()) return -1;
   Plan *plan = nullptr;
   const InvMap *inv = nullptr;
   const SlotRecords *slots = nullptr;
@@ -543,6 +554,7 @@ int loop_bres_calc(const char *name, op_set set, int nargs, op_arg *a) {
         a[0].dat == L.x && a[2].dat == L.q && a[3].dat == L.adt && a[4].dat == L.res &&
         a[5].dat == L.bound && rb == L.rb && consts_are(L.kd, L.kf, rb)) {
       r.sres_stage = 0;  // the pair the update launched is the program's
+      if (r.res_zero == L.res) r.res_zero = nullptr;  // it wrote every element of res
       r.count_call("bres_calc(speculated)");
       return 0;
     }
@@ -576,7 +588,9 @@ int loop_bres_calc(const char *name, op_set set, int nargs, op_arg *a) {
       // fused call reads the boundary maps, flags and nodes (q, adt and res of
       // the boundary cells move with res_calc's)
       const double fused = pd.bytes + 16.0 * B + 4.0 * rb * B;
+      const double res_read = 4.0 * rb * (double)pd.res->set->size;
       const int *bound = (const int *)a[5].dat->data_d;
+      const bool zero = r.res_zero == pd.res;  // start from 0: the update left res zero
       cudaError_t e;
       r.begin_loop("res_calc+bres_calc");
       if (rb == 8)
@@ -584,14 +598,16 @@ int loop_bres_calc(const char *name, op_set set, int nargs, op_arg *a) {
                                            (const double *)pd.x->data_d,
                                            (const double *)pd.q->data_d,
                                            (const double *)pd.adt->data_d,
-                                           (double *)pd.res->data_d, pd.kd, r.opt_pipe_block);
+                                           (double *)pd.res->data_d, pd.kd, r.opt_pipe_block,
+                                           zero);
       else
         e = launch_res_bres_corner<float>(r.ctx(), *cr, *br, bound,
                                           (const float *)pd.x->data_d,
                                           (const float *)pd.q->data_d,
                                           (const float *)pd.adt->data_d,
-                                          (float *)pd.res->data_d, pd.kf, r.opt_pipe_block);
-      r.end_loop(fused);
+                                          (float *)pd.res->data_d, pd.kf, r.opt_pipe_block, zero);
+      r.end_loop(fused - (zero ? res_read : 0.0));
+      if (zero && e == cudaSuccess) r.res_zero = nullptr;  // every element rewritten
       if (e == cudaSuccess) {  // the pair the next update may launch ahead
         ResLearn &L = r.rlearn;
         L.valid = true;
@@ -609,6 +625,7 @@ int loop_bres_calc(const char *name, op_set set, int nargs, op_arg *a) {
         L.rb = rb;
         L.res_bytes = pd.bytes;
         L.fused_bytes = fused;
+        L.res_read_bytes = res_read;
         L.kd = pd.kd;
         L.kf = pd.kf;
       }
@@ -689,11 +706,19 @@ int loop_update(const char *name, op_set set, int nargs, op_arg *a) {
   const bool rename = r.lazy.src == a[1].dat && r.lazy.dst == a[0].dat && a[2].dat != a[0].dat &&
                       a[2].dat != a[1].dat && a[3].dat != a[0].dat && a[3].dat != a[1].dat;
   if (r.sres_stage && !r.settle_res()) return -1;  // update reads res
+  if (r.res_zero && !r.materialize_res()) return -1;
   if (rename ? (r.pend.kind && !r.flush_loop()) : (r.outstanding() && !r.flush_pending())) return -1;
   int C = set->size;
   double bytes = (double)rb * 17.0 * C;
   char *qin = rename ? a[1].dat->data_d : a[0].dat->data_d;
   char *qout = rename ? a[0].dat->data_d : a[1].dat->data_d;
+  // res: read, and recorded as zero instead of written (res_zero)
+  cudaStreamCaptureStatus rcap = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(r.stream, &rcap);
+  const bool keep_res = r.opt_lazy_res && rcap == cudaStreamCaptureStatusNone &&
+                        !r.exposed.count(a[2].dat) && r.overlays.empty() &&
+                        a[2].dat != a[0].dat && a[2].dat != a[1].dat && a[2].dat != a[3].dat;
+  if (keep_res) bytes -= 4.0 * rb * C;
   r.red.seq = ++r.red_seq;
   // speculation: this update's q is the q the last adt_calc read, and adt
   // is what it wrote -- compute the next adt_calc's result now, into the
@@ -726,18 +751,19 @@ int loop_update(const char *name, op_set set, int nargs, op_arg *a) {
                               (const double *)a[3].dat->data_d, r.red,
                               spec ? sp.pcell->map_d : nullptr,
                               spec ? (const double *)sp.x->data_d : nullptr,
-                              spec ? (double *)sp.shadow : nullptr, &sp.kd);
+                              spec ? (double *)sp.shadow : nullptr, &sp.kd, keep_res);
   else
     e = launch_update<float>(r.ctx(), C, (const float *)qin, (float *)qout,
                              (float *)a[2].dat->data_d,
                              (const float *)a[3].dat->data_d, r.red,
                              spec ? sp.pcell->map_d : nullptr,
                              spec ? (const float *)sp.x->data_d : nullptr,
-                             spec ? (float *)sp.shadow : nullptr, &sp.kf);
+                             spec ? (float *)sp.shadow : nullptr, &sp.kf, keep_res);
   // with the speculation the pass also reads pcell and x and writes adt
   r.end_loop(spec ? bytes + 16.0 * C + (double)rb * (2.0 * N + C) : bytes);
   sp.inplace = spec && e == cudaSuccess;
   if (finish(e, name)) return -1;
+  if (keep_res) r.res_zero = a[2].dat;
   if (rename) {
     std::swap(a[0].dat->data_d, a[1].dat->data_d);
     r.lazy = LazySave{};
@@ -790,7 +816,17 @@ bool op2b::Runtime::restore_spec() {
 bool op2b::Runtime::flush_pending() {
   bool ok = settle_res();
   ok = flush_loop() && ok;
-  return materialize_save() && ok;
+  ok = materialize_save() && ok;
+  return materialize_res() && ok;
+}
+
+bool op2b::Runtime::materialize_res() {
+  if (!res_zero) return true;
+  op_dat d = res_zero;
+  res_zero = nullptr;
+  count_call("res zeroed");
+  cudaError_t e = cudaMemsetAsync(d->data_d, 0, (size_t)d->set->size * d->size, stream);
+  return finish(e, "res zeroed") == 0;
 }
 
 // Undo a speculative res_calc + bres_calc: the update before it left res
@@ -802,9 +838,11 @@ bool op2b::Runtime::settle_res() {
   sres_stage = 0;
   const ResLearn &L = rlearn;
   count_call("res_calc+bres_calc undone");
-  cudaError_t e = cudaMemsetAsync(L.res->data_d, 0, (size_t)L.res->set->size * L.res->size,
-                                  stream);
-  if (e != cudaSuccess) return finish(e, "res_calc+bres_calc undo") == 0;
+  if (res_zero != L.res) {  // (with res recorded as zero, nothing to undo in memory)
+    cudaError_t e = cudaMemsetAsync(L.res->data_d, 0, (size_t)L.res->set->size * L.res->size,
+                                    stream);
+    if (e != cudaSuccess) return finish(e, "res_calc+bres_calc undo") == 0;
+  }
   if (st == 2) {
     bool ok = pend.kind == 0 || flush_loop();
     pend = PendingLoop{};
@@ -850,6 +888,7 @@ bool op2b::Runtime::flush_loop() {
   if (pd.kind == 2) {
     const SlotRecords *cr = get_corner_records(pd.pecell, pd.pedge);
     if (!cr) return false;
+    if (res_zero == pd.res && !materialize_res()) return false;
     begin_loop("res_calc");
     if (pd.rb == 8)
       e = launch_res_calc_gather_corner<double>(ctx(), *cr, (const double *)pd.x->data_d,

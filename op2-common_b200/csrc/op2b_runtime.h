@@ -90,6 +90,7 @@ struct ResLearn {
   op_dat x = nullptr, q = nullptr, adt = nullptr, res = nullptr, bound = nullptr;
   int rb = 0;
   double res_bytes = 0.0, fused_bytes = 0.0;
+  double res_read_bytes = 0.0;  // the pair's read of res, saved when res is known zero
   AirConst<double> kd{};  // constants of the learned (and the launched) pair
   AirConst<float> kf{};
 };
@@ -118,6 +119,7 @@ struct Runtime {
   int opt_host_mirror = 1;    // op_dat::data holds a host copy of the declared values
   int opt_rename_save = 1;    // save_soln by renaming (LazySave)
   int opt_speculate_res = 1;  // update launches the res_calc + bres_calc after it (ResLearn)
+  int opt_lazy_res = 1;       // update leaves res unwritten, recorded as zero (res_zero)
   int opt_pipe_block = 256;   // threads per CTA of the pipelined gather (64, 96, 128, 256)
   int opt_pipe_hints = 0;     // register pipeline: evict-first hints on once-read streams
   int opt_plan_mode = 0;      // 0 = parallel block colouring, 1 = serial greedy (bit-exact)
@@ -153,6 +155,12 @@ struct Runtime {
   LazySave lazy;
   ResLearn rlearn;
   int sres_stage = 0;  // speculative res_calc + bres_calc: 0 none, 1 launched, 2 res_calc seen
+  // A dat the program holds all zeros while its array does not: the update
+  // zeroes res, and the res_calc + bres_calc after it rewrite every element
+  // starting from zero, so the update leaves the array as it is.  The fused
+  // pair then starts from 0 instead of reading res; anything else that
+  // touches the dat first zeroes the array (materialize_res).
+  op_dat res_zero = nullptr;
   SpecAdt spec;
   std::set<op_dat> exposed;  // dats whose device pointer was handed out (no speculation)
   std::set<op_dat> zero_mirror;  // dats declared without data: their host copy is zeros
@@ -163,7 +171,10 @@ struct Runtime {
   // initialised, with any deferred loop launched (false on error)
   bool ready();
   // a deferred loop or a renamed save_soln is outstanding
-  bool outstanding() const { return pend.kind != 0 || lazy.src != nullptr || sres_stage != 0; }
+  bool outstanding() const {
+    return pend.kind != 0 || lazy.src != nullptr || sres_stage != 0 || res_zero != nullptr;
+  }
+  bool materialize_res();   // op2b_dispatch.cpp: zero the array of res_zero
   bool flush_pending();     // op2b_dispatch.cpp: everything settled and launched
   bool settle_res();        // op2b_dispatch.cpp: undo a speculative res_calc + bres_calc
   bool flush_loop();        // op2b_dispatch.cpp: the deferred loop only

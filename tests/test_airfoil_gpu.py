@@ -267,25 +267,34 @@ def test_speculative_adt_restored_for_other_readers(op2):
 
 def test_speculative_res_calc_is_bit_identical(op2):
     """update launching the res_calc + bres_calc pair that follows it
-    (speculate_res) gives the same fields and history as waiting for the
-    program's calls, in both precisions; every pair after the first is
-    launched ahead."""
+    (speculate_res), and leaving res unwritten as a known zero that the pair
+    starts from (lazy_res), each on or off: the same fields and history, in
+    both precisions; with speculate_res every pair after the first is
+    launched ahead, and with lazy_res no zeros are ever written."""
     m = M.channel_bump(96, 48, seed=16)
+    combos = [(0, 0), (1, 0), (0, 1), (1, 1)]
     for dtype in (np.float64, np.float32):
-        out, hists, seen = [], [], []
-        for spec in (0, 1):
+        out, hists, seen, zeroed = [], [], [], []
+        for spec, lazy in combos:
             op2.set_option("speculate_res", spec)
+            op2.set_option("lazy_res", lazy)
             op2.load().op2b_reset_stats()
             app = Airfoil(m, dtype=dtype)
             hists.append(app.iterate(5))
-            out.append(app.fetch())
             seen.append(op2.loop_stats("bres_calc(speculated)"))
+            zeroed.append(op2.loop_stats("res zeroed"))
+            out.append(app.fetch())
             op2.op_exit()
             op2.op_init()
-        assert hists[0] == hists[1], dtype
-        for k in ("q", "qold", "adt", "res"):
-            assert np.array_equal(out[0][k], out[1][k]), (dtype, k)
+        for i in range(1, len(combos)):
+            assert hists[0] == hists[i], (dtype, combos[i])
+            for k in ("q", "qold", "adt", "res"):
+                assert np.array_equal(out[0][k], out[i][k]), (dtype, combos[i], k)
         assert seen[0] is None and seen[1]["calls"] == 9
+        # lazy_res: zeros are written once, when the statistics call observes
+        # the last update's res; the iterations never wrote any
+        assert zeroed[0] is None and zeroed[1] is None
+        assert zeroed[2]["calls"] == 1 and zeroed[3]["calls"] == 1
 
 
 def test_speculative_res_calc_is_invisible(op2):
@@ -298,6 +307,7 @@ def test_speculative_res_calc_is_invisible(op2):
 
     def run(spec, between, after):
         op2.set_option("speculate_res", spec)
+        op2.set_option("lazy_res", spec)
         app = Airfoil(m)
         app.iterate(1)
         for i in (1, 2, 3, 4):        # adt_calc, res_calc, bres_calc, update
