@@ -65,12 +65,13 @@ bool cuda_ok(cudaError_t e, const char *what) {
   return false;
 }
 
-// memcpy of a large host array by up to 8 threads: copying into freshly
-// allocated memory is bound by its page faults, which the kernel serves in
-// parallel
+// memcpy of a large host array by up to `host_threads` threads (option,
+// default 16, at most the host's): copying into freshly allocated memory is bound by its page
+// faults, which the kernel serves in parallel
 static void host_copy(void *dst, const void *src, size_t bytes) {
   const size_t kParallel = (size_t)8 << 20;
-  unsigned nt = std::min(8u, std::max(1u, std::thread::hardware_concurrency()));
+  unsigned nt = std::min((unsigned)std::max(1, rt().opt_host_threads),
+                         std::max(1u, std::thread::hardware_concurrency()));
   if (bytes < kParallel || nt < 2) {
     memcpy(dst, src, bytes);
     return;
@@ -90,7 +91,11 @@ static void host_copy(void *dst, const void *src, size_t bytes) {
 bool download_host(void *dst, const void *src_d, size_t bytes, const char *what) {
   Runtime &r = rt();
   const size_t kChunk = (size_t)16 << 20;
-  if (bytes <= kChunk) {
+  cudaPointerAttributes pa{};
+  const bool pinned = cudaPointerGetAttributes(&pa, dst) == cudaSuccess &&
+                      pa.type == cudaMemoryTypeHost;
+  cudaGetLastError();
+  if (bytes <= kChunk || pinned) {  // a pinned destination takes the DMA directly
     return cuda_ok(cudaMemcpyAsync(dst, src_d, bytes, cudaMemcpyDeviceToHost, r.stream), what) &&
            cuda_ok(cudaStreamSynchronize(r.stream), what);
   }
@@ -402,6 +407,7 @@ void op_exit(void) {
   r.opt_rename_save = d.opt_rename_save;
   r.opt_speculate_res = d.opt_speculate_res;
   r.opt_lazy_res = d.opt_lazy_res;
+  r.opt_host_threads = d.opt_host_threads;
   r.res_zero = nullptr;
   r.lazy = LazySave{};
   r.rlearn = ResLearn{};
@@ -797,10 +803,7 @@ static bool fetch_range(op_dat dat, char *dst, size_t first, size_t count) {
   }
   resolve_renumbering_for_fetch(dat);
   size_t bytes = count * (size_t)dat->size;
-  cudaError_t e = cudaMemcpyAsync(dst, dat->data_d + first * dat->size, bytes,
-                                  cudaMemcpyDeviceToHost, r.stream);
-  if (!cuda_ok(e, "op_fetch_data")) return false;
-  return cuda_ok(cudaStreamSynchronize(r.stream), "op_fetch_data");
+  return download_host(dst, dat->data_d + first * dat->size, bytes, "op_fetch_data");
 }
 
 void op_fetch_data_char(op_dat dat, char *usr_ptr) {
@@ -1049,6 +1052,12 @@ int op2b_set_option(const char *key, long value) {
     r.opt_speculate_res = value != 0;
   } else if (k == "lazy_res") {
     r.opt_lazy_res = value != 0;
+  } else if (k == "host_threads") {
+    if (value < 1 || value > 64) {
+      set_error("op2b_set_option: host_threads must be 1..64");
+      return -1;
+    }
+    r.opt_host_threads = (int)value;
   } else {
     set_error("op2b_set_option: unknown option '%s'", k.c_str());
     return -1;
@@ -1079,6 +1088,7 @@ long op2b_get_option(const char *key) {
   if (k == "rename_save") return r.opt_rename_save;
   if (k == "speculate_res") return r.opt_speculate_res;
   if (k == "lazy_res") return r.opt_lazy_res;
+  if (k == "host_threads") return r.opt_host_threads;
   if (k == "nsm") return r.nsm;
   return -1;
 }

@@ -969,9 +969,7 @@ void fetch_original_order(op_dat dat, char *dst, int low, int high) {
   size_t bytes = cnt * dat->size;
   auto it = ren().perm_d.find(dat->set->index);
   if (it == ren().perm_d.end() || dat->size % 4) {
-    cudaMemcpyAsync(dst, dat->data_d + (size_t)low * dat->size, bytes, cudaMemcpyDeviceToHost,
-                    r.stream);
-    cuda_ok(cudaStreamSynchronize(r.stream), "op_fetch_data_idx");
+    download_host(dst, dat->data_d + (size_t)low * dat->size, bytes, "op_fetch_data_idx");
     return;
   }
   int *t = nullptr;
@@ -979,9 +977,8 @@ void fetch_original_order(op_dat dat, char *dst, int low, int high) {
   int words = dat->size / 4;
   k_gather_rows<<<grid1((long long)cnt * words), 256, 0, r.stream>>>(
       (int)cnt, words, reinterpret_cast<const int *>(dat->data_d), t, it->second, low);
-  cudaMemcpyAsync(dst, t, bytes, cudaMemcpyDeviceToHost, r.stream);
+  download_host(dst, t, bytes, "op_fetch_data_idx");
   cudaFreeAsync(t, r.stream);
-  cuda_ok(cudaStreamSynchronize(r.stream), "op_fetch_data_idx");
 }
 
 void release_renumbering() {
