@@ -66,7 +66,7 @@ bool cuda_ok(cudaError_t e, const char *what) {
 }
 
 // memcpy of a large host array by up to `host_threads` threads (option,
-// default 16, at most the host's): copying into freshly allocated memory is bound by its page
+// default 8, at most the host's): copying into freshly allocated memory is bound by its page
 // faults, which the kernel serves in parallel
 static void host_copy(void *dst, const void *src, size_t bytes) {
   const size_t kParallel = (size_t)8 << 20;

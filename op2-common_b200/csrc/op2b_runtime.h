@@ -120,7 +120,7 @@ struct Runtime {
   int opt_rename_save = 1;    // save_soln by renaming (LazySave)
   int opt_speculate_res = 1;  // update launches the res_calc + bres_calc after it (ResLearn)
   int opt_lazy_res = 1;       // update leaves res unwritten, recorded as zero (res_zero)
-  int opt_host_threads = 16;  // threads of a large host copy (host copies of maps and dats)
+  int opt_host_threads = 8;   // threads of a large host copy (host copies of maps and dats)
   int opt_pipe_block = 256;   // threads per CTA of the pipelined gather (64, 96, 128, 256)
   int opt_pipe_hints = 0;     // register pipeline: evict-first hints on once-read streams
   int opt_plan_mode = 0;      // 0 = parallel block colouring, 1 = serial greedy (bit-exact)

@@ -161,7 +161,11 @@ struct LevelBatch {
   int d[kB];
   long long r[kB];
   int v[kB][kNb];
-  __device__ void load(const RcmWork &w, const int *cur, int len, int j0, int thr = INT_MAX) {
+  // open: drop neighbours already ordered (Cuthill-McKee's walk); a
+  // breadth-first search stays inside one component, none of whose
+  // vertices is ordered before `thr`, and needs no such test
+  __device__ void load(const RcmWork &w, const int *cur, int len, int j0, int thr = INT_MAX,
+                       bool open = true) {
     int u[kB];
 #pragma unroll
     for (int k = 0; k < kB; k++) {
@@ -177,6 +181,7 @@ struct LevelBatch {
     for (int k = 0; k < kB; k++)
 #pragma unroll
       for (int t = 0; t < kNb; t++) v[k][t] = t < d[k] ? w.col[r[k] + t] : -1;
+    if (!open) return;
 #pragma unroll
     for (int k = 0; k < kB; k++)
 #pragma unroll
@@ -228,9 +233,11 @@ struct ParentBatch {
   }
 };
 
-// BFS from `start` over vertices not ordered before position `thr`; marks
-// with `stamp`.  Returns the number of levels; the last level is left in
-// *last (lev_a or lev_b).
+// BFS from `start` over its component; marks with `stamp`.  (The vertices
+// of other components are not reachable, and those of this one are either
+// all unordered or, thr = the component's first position, ordered from thr
+// on: no test of the order is needed.)  Returns the number of levels; the
+// last level is left in *last (lev_a or lev_b).
 __device__ int rcm_bfs(RcmWork &w, int start, int stamp, int **last, int *last_len,
                        int thr = INT_MAX) {
   __shared__ int s_len, s_next;
@@ -252,7 +259,7 @@ __device__ int rcm_bfs(RcmWork &w, int start, int stamp, int **last, int *last_l
     // a handful of memory latencies however many vertices it covers
     for (int j0 = threadIdx.x; j0 < len; j0 += kB * blockDim.x) {
       LevelBatch b;
-      b.load(w, cur, len, j0, thr);
+      b.load(w, cur, len, j0, thr, false);
       // all exchanges first (none waits on another's result), then the appends
       int old[kB][kNb];
 #pragma unroll
@@ -269,8 +276,7 @@ __device__ int rcm_bfs(RcmWork &w, int start, int stamp, int **last, int *last_l
       for (int k = 0; k < kB; k++)
         for (int t = kNb; t < b.d[k]; t++) {  // vertices of higher degree
           int v = w.col[b.r[k] + t];
-          if (rcm_open(w, v, thr) && atomicExch(&w.mark[v], stamp) != stamp)
-            nxt[atomicAdd(&s_next, 1)] = v;
+          if (atomicExch(&w.mark[v], stamp) != stamp) nxt[atomicAdd(&s_next, 1)] = v;
         }
     }
     __syncthreads();
