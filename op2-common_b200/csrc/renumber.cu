@@ -219,6 +219,37 @@ struct ParentBatch {
         vd[k][t] = open ? w.deg[x] : 0;
       }
   }
+  // the same in two steps: the parents and their unordered neighbours
+  // before the level's claims, the neighbours' claims and degrees after
+  __device__ void load_open(const RcmWork &w, const int *cur, int j0, int je) {
+    int u[kB];
+#pragma unroll
+    for (int k = 0; k < kB; k++) u[k] = j0 + k < je ? cur[j0 + k] : -1;
+#pragma unroll
+    for (int k = 0; k < kB; k++) {
+      d[k] = u[k] >= 0 ? w.deg[u[k]] : 0;
+      r[k] = u[k] >= 0 ? w.row[u[k]] : 0;
+    }
+#pragma unroll
+    for (int k = 0; k < kB; k++)
+#pragma unroll
+      for (int t = 0; t < kNb; t++) v[k][t] = t < d[k] ? w.col[r[k] + t] : -1;
+#pragma unroll
+    for (int k = 0; k < kB; k++)
+#pragma unroll
+      for (int t = 0; t < kNb; t++)
+        if (v[k][t] >= 0 && w.newidx[v[k][t]] >= 0) v[k][t] = -1;
+  }
+  __device__ void load_keys(const RcmWork &w) {
+#pragma unroll
+    for (int k = 0; k < kB; k++)
+#pragma unroll
+      for (int t = 0; t < kNb; t++) {
+        const int x = v[k][t];
+        pk[k][t] = x >= 0 ? w.pkey[x] : -1;
+        vd[k][t] = x >= 0 ? w.deg[x] : 0;
+      }
+  }
   __device__ bool claimed(int k, int t, int j) const { return v[k][t] >= 0 && pk[k][t] == j; }
   // children of parent k (position j) that it claimed
   __device__ int count(const RcmWork &w, int k, int j) const {
@@ -314,6 +345,59 @@ __device__ int rcm_pick(const RcmWork &w, const int *last, int last_len) {
   return cand;
 }
 
+// Parent k (level position j) of a batch appends its claimed children to
+// the next level at pos, in sequential Cuthill-McKee's order, and places them.
+__device__ __forceinline__ void rcm_emit(RcmWork &w, const ParentBatch &pb, int k, int j,
+                                         int *nxt, int &pos, int base) {
+  const int first = pos;
+  if (pb.d[k] <= kNb) {
+    // the claimed children's (degree capped at 63, id) keys, sorted in registers
+    unsigned long long key[kNb];
+#pragma unroll
+    for (int t = 0; t < kNb; t++)
+      key[t] = pb.claimed(k, t, j)
+                   ? ((unsigned long long)(unsigned)min(pb.vd[k][t], 63) << 32) |
+                         (unsigned)pb.v[k][t]
+                   : ~0ull;
+#pragma unroll
+    for (int i = 1; i < kNb; i++)
+#pragma unroll
+      for (int m = i; m > 0; m--)
+        if (key[m] < key[m - 1]) {
+          unsigned long long x = key[m];
+          key[m] = key[m - 1];
+          key[m - 1] = x;
+        }
+#pragma unroll
+    for (int t = 0; t < kNb; t++)
+      if (key[t] != ~0ull) nxt[pos++] = (int)(key[t] & 0xffffffffull);
+  } else {
+    // higher degree: selection of the smallest claimed key above the last
+    unsigned long long last = 0;
+    bool any = false;
+    while (true) {
+      unsigned long long best = ~0ull;
+      for (int t = 0; t < pb.d[k]; t++) {
+        int v = w.col[pb.r[k] + t];
+        if (w.newidx[v] < 0 && w.pkey[v] == j) {
+          unsigned long long key =
+              ((unsigned long long)(unsigned)min(w.deg[v], 63) << 32) | (unsigned)v;
+          if ((!any || key > last) && key < best) best = key;
+        }
+      }
+      if (best == ~0ull) break;
+      nxt[pos++] = (int)(best & 0xffffffffull);
+      last = best;
+      any = true;
+    }
+  }
+  for (int q = first; q < pos; q++) {
+    int v = nxt[q];
+    w.newidx[v] = base + q;
+    w.pkey[v] = INT_MAX;
+  }
+}
+
 // Cuthill-McKee from `start`: appends its component to the order at
 // s_pos (shared).  Its levels are the BFS levels from `start`: returns
 // their number and leaves the last level in *last.
@@ -331,6 +415,55 @@ __device__ int rcm_cm(RcmWork &w, int start, int &s_pos, int &s_len, int **last,
     const int len = s_len;
     const int base = s_pos;
     nlev++;
+    const int chunk = (len + (int)blockDim.x - 1) / (int)blockDim.x;
+    const int jb = min(len, (int)threadIdx.x * chunk), je = min(len, jb + chunk);
+    if (chunk <= kB) {
+      // a level of at most kB parents a thread: each thread loads its run of
+      // parents once, claims their children, counts and places them -- the
+      // steps below with the loads shared between them
+      ParentBatch pb;
+      pb.load_open(w, cur, jb, je);
+#pragma unroll
+      for (int k = 0; k < kB; k++) {
+        const int j = jb + k;
+        if (j >= je) break;
+#pragma unroll
+        for (int t = 0; t < kNb; t++)
+          if (pb.v[k][t] >= 0) atomicMin(&w.pkey[pb.v[k][t]], j);
+        for (int t = kNb; t < pb.d[k]; t++) {
+          int v = w.col[pb.r[k] + t];
+          if (w.newidx[v] < 0) atomicMin(&w.pkey[v], j);
+        }
+      }
+      __syncthreads();
+      pb.load_keys(w);
+      int mine = 0;
+#pragma unroll
+      for (int k = 0; k < kB; k++) mine += pb.count(w, k, jb + k);
+      int nl = 0;
+      int pos = rcm_block_scan(mine, &nl);
+      if (nl == 0) {
+        *last = cur;
+        *last_len = len;
+        return nlev;
+      }
+#pragma unroll
+      for (int k = 0; k < kB; k++) {
+        const int j = jb + k;
+        if (j >= je) break;
+        rcm_emit(w, pb, k, j, nxt, pos, base);
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        s_pos = base + nl;
+        s_len = nl;
+      }
+      int *t = cur;
+      cur = nxt;
+      nxt = t;
+      __syncthreads();
+      continue;
+    }
     // first parent (lowest position in this level) of every new vertex
     for (int j0 = threadIdx.x; j0 < len; j0 += kB * blockDim.x) {
       LevelBatch b;
@@ -353,8 +486,6 @@ __device__ int rcm_cm(RcmWork &w, int start, int &s_pos, int &s_len, int **last,
     // order sequential Cuthill-McKee appends them in.  Each thread takes a
     // contiguous run of parents; a block scan of the runs' counts places
     // them, so no sort of the level is needed.
-    const int chunk = (len + (int)blockDim.x - 1) / (int)blockDim.x;
-    const int jb = min(len, (int)threadIdx.x * chunk), je = min(len, jb + chunk);
     int mine = 0;
     for (int j0 = jb; j0 < je; j0 += kB) {
       ParentBatch pb;
@@ -376,53 +507,7 @@ __device__ int rcm_cm(RcmWork &w, int start, int &s_pos, int &s_len, int **last,
       for (int k = 0; k < kB; k++) {
         const int j = j0 + k;
         if (j >= je) break;
-        const int first = pos;
-        if (pb.d[k] <= kNb) {
-          // the claimed children's (degree capped at 63, id) keys, sorted in registers
-          unsigned long long key[kNb];
-#pragma unroll
-          for (int t = 0; t < kNb; t++)
-            key[t] = pb.claimed(k, t, j)
-                         ? ((unsigned long long)(unsigned)min(pb.vd[k][t], 63) << 32) |
-                               (unsigned)pb.v[k][t]
-                         : ~0ull;
-#pragma unroll
-          for (int i = 1; i < kNb; i++)
-#pragma unroll
-            for (int m = i; m > 0; m--)
-              if (key[m] < key[m - 1]) {
-                unsigned long long x = key[m];
-                key[m] = key[m - 1];
-                key[m - 1] = x;
-              }
-#pragma unroll
-          for (int t = 0; t < kNb; t++)
-            if (key[t] != ~0ull) nxt[pos++] = (int)(key[t] & 0xffffffffull);
-        } else {
-          // higher degree: selection of the smallest claimed key above the last
-          unsigned long long last = 0;
-          bool any = false;
-          while (true) {
-            unsigned long long best = ~0ull;
-            for (int t = 0; t < pb.d[k]; t++) {
-              int v = w.col[pb.r[k] + t];
-              if (w.newidx[v] < 0 && w.pkey[v] == j) {
-                unsigned long long key =
-                    ((unsigned long long)(unsigned)min(w.deg[v], 63) << 32) | (unsigned)v;
-                if ((!any || key > last) && key < best) best = key;
-              }
-            }
-            if (best == ~0ull) break;
-            nxt[pos++] = (int)(best & 0xffffffffull);
-            last = best;
-            any = true;
-          }
-        }
-        for (int q = first; q < pos; q++) {
-          int v = nxt[q];
-          w.newidx[v] = base + q;
-          w.pkey[v] = INT_MAX;
-        }
+        rcm_emit(w, pb, k, j, nxt, pos, base);
       }
     }
     __syncthreads();
