@@ -418,6 +418,9 @@ def main():
         dom = max(loops, key=lambda n: loops[n]["avg_ms"] * loops[n]["calls"])
         d = loops[dom]
         key = f"{work}_{args.precision}_{args.numbering}_mode{args.inc_mode}"
+        it_bytes = sum(x["alg_bytes"] * x["calls"] for x in main_run["loops"].values()
+                       if x.get("alg_bytes"))
+        it_gbs = it_bytes / args.steps / (ms * 1e-3) / 1e9 if ms > 0 else None
         line = {
             "metric": METRIC, "value": ms, "unit": "ms/iter", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
@@ -436,7 +439,11 @@ def main():
             "roofline": {"bound": "hbm", "loop": dom, "achieved": d["gbs"], "peak": peak,
                          "unit": "GB/s", "frac": d["gbs"] / peak if d["gbs"] else None,
                          "traffic": traffic_from_profiles(key, dom),
-                         "peak_source": peak_src},
+                         "peak_source": peak_src,
+                         # the whole iteration: every loop's algorithmic bytes per
+                         # iteration over the measured time per iteration
+                         "iteration_achieved": it_gbs,
+                         "iteration_frac": it_gbs / peak if it_gbs else None},
             "loops": loops,
             "renumber": main_run["renumber"],
             "rms_final": main_run["rms"],

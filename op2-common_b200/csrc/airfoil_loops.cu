@@ -298,14 +298,12 @@ __device__ __forceinline__ RedTriple block_reduce(RedTriple t) {
 // arrive reduces all partials in block order and writes `out`.
 // With ADT the kernel also computes, from each cell's new q, the time step
 // that the following adt_calc computes (same arithmetic on the same stored q
-// values) and writes it into adt itself, after saving the old adt into
-// `backup`, a buffer of the runtime's (option speculate_adt).  Each cell's
-// adt is read and written by the same thread only.
+// values) and writes it into `next`, a second array of the runtime's (option
+// speculate_adt); the adt dat itself is only read.
 template <typename T> struct AdtNext {
   const int4 *pcell;
   const T *x;
-  T *adt;      // the adt dat (the update's own adt argument), written in place
-  T *backup;   // receives the old adt
+  T *next;     // receives the next adt_calc's result
   AirConst<T> k;
 };
 
@@ -328,13 +326,7 @@ k_update(int ncell, const T *__restrict__ qold, T *__restrict__ q, T *__restrict
     }
     Vec<T>::ld4(qold + 4 * (size_t)n, qo);
     Vec<T>::ld4_rw(res + 4 * (size_t)n, r);
-    T a_old;
-    if constexpr (ADT) {
-      a_old = adt[n];  // coherent load: this kernel rewrites adt
-      an.backup[n] = a_old;
-    } else {
-      a_old = __ldg(adt + n);
-    }
+    const T a_old = __ldg(adt + n);
     double adti = 1.0f / (double)a_old;
 #pragma unroll
     for (int m = 0; m < 4; m++) {
@@ -353,8 +345,8 @@ k_update(int ncell, const T *__restrict__ qold, T *__restrict__ q, T *__restrict
       Vec<T>::st4(res + 4 * (size_t)n, z);
     }
     if constexpr (ADT)
-      an.adt[n] = air_adt<T>(x1x, x1y, x2x, x2y, x3x, x3y, x4x, x4y, qn[0], qn[1], qn[2],
-                             qn[3], an.k);
+      an.next[n] = air_adt<T>(x1x, x1y, x2x, x2y, x3x, x3y, x4x, x4y, qn[0], qn[1], qn[2],
+                              qn[3], an.k);
   }
   t = block_reduce<THREADS>(t);
   __shared__ bool last;
@@ -390,13 +382,12 @@ k_update(int ncell, const T *__restrict__ qold, T *__restrict__ q, T *__restrict
 template <typename T>
 cudaError_t launch_update(const LaunchCtx &c, int ncell, const T *qold, T *q, T *res,
                           const T *adt, const RedScratch &s, const int *pcell, const T *x,
-                          T *adt_backup, const AirConst<T> *k, bool keep_res) {
+                          T *adt_next, const AirConst<T> *k, bool keep_res) {
   constexpr int TH = 256;
   int grid = grid_for(c, ncell, TH, 4);
   if (grid > s.capacity) grid = s.capacity;
-  if (adt_backup) {
-    const AdtNext<T> an{reinterpret_cast<const int4 *>(pcell), x, const_cast<T *>(adt),
-                        adt_backup, *k};
+  if (adt_next) {
+    const AdtNext<T> an{reinterpret_cast<const int4 *>(pcell), x, adt_next, *k};
     if (keep_res)
       k_update<T, TH, true, true><<<grid, TH, 0, c.stream>>>(ncell, qold, q, res, adt, s.parts,
                                                              s.counter, s.out, s.host_out,

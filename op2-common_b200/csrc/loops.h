@@ -63,15 +63,15 @@ template <typename T>
 cudaError_t launch_bres_calc_atomic(const LaunchCtx &c, int nbedge, const int *pbedge,
                                     const int *pbecell, const int *bound, const T *x,
                                     const T *q, const T *adt, T *res, const AirConst<T> &k);
-// adt_backup (optional): also each cell's time step from its new q, pcell and
-// x with constants k, as adt_calc computes it, written into adt after the old
-// adt is saved into adt_backup.  keep_res: res is read but not zeroed (the
+// adt_next (optional): also each cell's time step from its new q, pcell and
+// x with constants k, as adt_calc computes it, written into adt_next (adt is
+// only read).  keep_res: res is read but not zeroed (the
 // runtime records that it is zero and zeroes it only if something reads it
 // before a res_calc rewrites it)
 template <typename T>
 cudaError_t launch_update(const LaunchCtx &c, int ncell, const T *qold, T *q, T *res,
                           const T *adt, const RedScratch &s, const int *pcell = nullptr,
-                          const T *x = nullptr, T *adt_backup = nullptr,
+                          const T *x = nullptr, T *adt_next = nullptr,
                           const AirConst<T> *k = nullptr, bool keep_res = false);
 
 }  // namespace op2b

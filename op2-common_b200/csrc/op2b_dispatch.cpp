@@ -245,13 +245,14 @@ void launch_speculative_res(Runtime &r, const op_arg *a, int rb) {
   const bool zero = r.res_zero == L.res;  // the update left res zero without writing it
   cudaError_t e;
   r.begin_loop("res_calc+bres_calc");
+  // adt: the next adt_calc's result, still in the second array
   if (rb == 8)
     e = launch_res_bres_corner<double>(r.ctx(), *cr, *br, bound, (const double *)L.x->data_d,
-                                       (const double *)L.q->data_d, (const double *)L.adt->data_d,
+                                       (const double *)L.q->data_d, (const double *)sp.shadow,
                                        (double *)L.res->data_d, L.kd, r.opt_pipe_block, zero);
   else
     e = launch_res_bres_corner<float>(r.ctx(), *cr, *br, bound, (const float *)L.x->data_d,
-                                      (const float *)L.q->data_d, (const float *)L.adt->data_d,
+                                      (const float *)L.q->data_d, (const float *)sp.shadow,
                                       (float *)L.res->data_d, L.kf, r.opt_pipe_block, zero);
   r.end_loop(L.fused_bytes - (zero ? L.res_read_bytes : 0.0));
   if (e == cudaSuccess) r.sres_stage = 1;
@@ -331,8 +332,11 @@ int loop_adt_calc(const char *name, op_set set, int nargs, op_arg *a) {
   const bool hit = sp.inplace && sp.pcell == pcell && sp.x == a[0].dat && sp.q == a[4].dat &&
                    sp.adt == a[5].dat && sp.rb == rb && consts_match(sp, rb);
   if (hit) {
-    // the update before this call already wrote this adt_calc's result
+    // the update before this call already wrote this adt_calc's result into
+    // the second array: it becomes adt's
     sp.inplace = false;
+    std::swap(sp.adt->data_d, *reinterpret_cast<char **>(&sp.shadow));
+    sp.shadow_bytes = ((size_t)C * rb + 255) & ~(size_t)255;
     r.count_call("adt_calc(in update)");
     return 0;
   }
@@ -727,7 +731,8 @@ int loop_update(const char *name, op_set set, int nargs, op_arg *a) {
   if (sp.inplace && !r.restore_spec()) return -1;  // update reads the program's adt
   bool spec = r.opt_speculate && sp.pcell && sp.q == a[1].dat && sp.adt == a[3].dat &&
               sp.rb == rb && sp.pcell->from == set && sp.x && sp.pcell->to == sp.x->set &&
-              !r.exposed.count(sp.x) && !r.exposed.count(sp.q) && !r.exposed.count(sp.adt);
+              !r.exposed.count(sp.x) && !r.exposed.count(sp.q) && !r.exposed.count(sp.adt) &&
+              r.overlays.empty();
   const size_t abytes = ((size_t)C * rb + 255) & ~(size_t)255;
   if (spec && sp.shadow_bytes < abytes) {
     cudaFree(sp.shadow);
@@ -804,13 +809,10 @@ const Entry kLoops[] = {{"save_soln", loop_save_soln},
 // Put the program's adt back: the update before wrote the next adt_calc's
 // result into adt early, and something other than that adt_calc came first.
 bool op2b::Runtime::restore_spec() {
-  if (!spec.inplace) return true;
+  // the adt dat's array still holds the program's adt: drop the early values
+  if (spec.inplace) count_call("adt ahead dropped");
   spec.inplace = false;
-  const size_t bytes = ((size_t)spec.adt->set->size * (size_t)spec.rb + 255) & ~(size_t)255;
-  begin_loop("adt restore");
-  cudaError_t e = launch_copy(ctx(), spec.shadow, spec.adt->data_d, bytes);
-  end_loop(2.0 * (double)bytes);
-  return finish(e, "adt restore") == 0;
+  return true;
 }
 
 bool op2b::Runtime::flush_pending() {

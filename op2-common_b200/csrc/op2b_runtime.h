@@ -47,11 +47,11 @@ struct PendingLoop {
 
 // Speculative adt_calc: update also computes, for the adt_calc that usually
 // follows it (over the last adt_calc's arguments), the time step of its new q
-// and writes it into adt, after saving the old adt into `shadow`.  While
-// `inplace` holds, adt is ahead of the program: the matching adt_calc then
-// has nothing left to do, and any other call that could read adt first
-// restores it from the shadow (restore_spec), so nothing observes the early
-// values.
+// and writes it into `shadow`, a second array of adt's size.  While `inplace`
+// holds, shadow is the program's next adt: the matching adt_calc then only
+// swaps the two arrays (the adt dat takes shadow's, shadow the old one), and
+// any other call drops the early values (restore_spec), so nothing observes
+// them; the adt dat's array was not written.
 // save_soln by renaming: save_soln (q -> qold) launches nothing; qold is
 // taken to hold q's values until q changes.  Loops that only read q run
 // meanwhile.  The update that reads qold and writes q then reads q's array
@@ -66,7 +66,7 @@ struct SpecAdt {
   op_map pcell = nullptr;                               // the last adt_calc's arguments
   op_dat x = nullptr, q = nullptr, adt = nullptr;
   int rb = 0;
-  bool inplace = false;    // adt holds the next adt_calc's result, shadow the old adt
+  bool inplace = false;    // shadow holds the next adt_calc's result
   void *shadow = nullptr;  // device buffer of adt's allocation size
   size_t shadow_bytes = 0;
   AirConst<double> kd{};   // constants the early adt was computed with
