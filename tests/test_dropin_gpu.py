@@ -183,3 +183,33 @@ def test_reference_functional_tests_run_on_libop2b(name):
             assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
             out[b] = [ln for ln in r.stdout.splitlines() if "passed" in ln.lower()]
     assert out[got] == out[ref] and len(out[ref]) >= 2
+
+
+@pytest.mark.parametrize("variant", ["sp", "tempdats"])
+def test_reference_airfoil_variants_run_on_libop2b(variant):
+    """The reference's other Airfoil applications, unmodified:
+    airfoil_plain/sp (float dats and constants, an update whose rms is a
+    float, run from its own kernel source) and airfoil_tempdats (qold, adt
+    and res declared as temporary dats and freed in every outer iteration,
+    the rms-only update).  Their rms history (printed with 6 digits) equals
+    the same application's on the reference's sequential library, to the
+    printing for tempdats (2e-5: the rms sums run in another order) and within
+    1e-4 for sp, whose float solution drifts apart by rounding over the 1000
+    iterations (3e-5 seen at iteration 400)."""
+    got, ref = O.ref_binary(f"airfoil_{variant}_dropin"), O.ref_binary(f"ref_airfoil_{variant}_seq")
+    if not (got and ref):
+        pytest.skip("Airfoil variant binaries not built")
+    m = M.channel_bump(240, 120, seed=1)
+    out = {}
+    for b in (got, ref):
+        with tempfile.TemporaryDirectory() as tmp:
+            M.write_grid_dat(m, os.path.join(tmp, "new_grid.dat"))
+            r = subprocess.run([b], cwd=tmp, capture_output=True, text=True, timeout=600)
+            assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+            out[b] = [(int(i), float(v)) for i, v in
+                      re.findall(r"^\s*(\d+)\s+([0-9.]+e[-+]\d+)\s*$", r.stdout, flags=re.M)]
+    assert [i for i, _ in out[ref]] == list(range(100, 1001, 100))
+    assert [i for i, _ in out[got]] == [i for i, _ in out[ref]]
+    tol = 1e-4 if variant == "sp" else 2e-5
+    for (_, a), (_, b) in zip(out[got], out[ref]):
+        assert abs(a - b) <= tol * b, (variant, out[got], out[ref])
