@@ -69,3 +69,28 @@ def test_constants_match_reference_literals():
     assert c["gam"] == float(np.float32(1.4)) and c["cfl"] == float(np.float32(0.9))
     assert c["gm1"] == c["gam"] - 1.0 and c["eps"] == float(np.float32(0.05))
     assert c["qinf"][2] == 0.0 and c["qinf"][0] == 1.0
+
+
+def test_fe_grid_for_aero():
+    """FE_grid.dat as the reference's aero reads it (aero.cpp:79-117): the
+    header, the nodes, each cell's nodes in the bilinear element's tensor
+    order (the corner opposite node 0 last) and the far-field nodes."""
+    m = M.channel_bump(12, 6, seed=3)
+    with tempfile.TemporaryDirectory() as tmp:
+        p = os.path.join(tmp, "FE_grid.dat")
+        M.write_fe_grid_dat(m, p)
+        lines = open(p).read().split("\n")
+    nnode, ncell, nb = (int(v) for v in lines[0].split())
+    bnode = np.unique(m.bedge[m.bound == 2].reshape(-1))
+    assert (nnode, ncell, nb) == (m.nnode, m.ncell, bnode.size)
+    x = np.array([[float(v) for v in ln.split()] for ln in lines[1:1 + nnode]])
+    assert np.array_equal(x, m.x)
+    cells = np.array([[int(v) for v in ln.split()] for ln in lines[1 + nnode:1 + nnode + ncell]])
+    assert np.array_equal(cells, m.cell[:, [0, 1, 3, 2]])
+    # tensor order: node 3 is the corner diagonal to node 0 (no shared edge)
+    e = {tuple(sorted(p)) for p in m.edge.tolist()} | {tuple(sorted(p)) for p in m.bedge.tolist()}
+    for c in cells[:50]:
+        assert tuple(sorted((c[0], c[1]))) in e and tuple(sorted((c[0], c[2]))) in e
+        assert tuple(sorted((c[0], c[3]))) not in e
+    got = np.array([int(v) for v in lines[1 + nnode + ncell:1 + nnode + ncell + nb]])
+    assert np.array_equal(got, bnode)
