@@ -23,8 +23,13 @@
 //     reference's flat element colouring, op_rt_support.cpp:684-754), one
 //     launch per colour, so that no two elements of a launch share a target;
 //     the colouring covers indirect OP_INC, OP_RW and OP_WRITE arguments;
-//   * vector map arguments, op_arg_info and switched-off optional arguments
-//     are rejected with an error, not run on the host;
+//   * vector map arguments (idx = -k) get k pointers; switched-off optional
+//     arguments a pointer to zeroed scratch;
+//   * op_arg_info: the payload the kernel writes where its OP_MIN/OP_MAX
+//     global improves, kept per thread with the element of the improvement;
+//     the best value over the loop wins, the lowest element on ties (the
+//     reference's CUDA reductions take the argmin/argmax with CUB); not in a
+//     loop that runs colour by colour;
 //   * compiled with --fmad=false (each operation rounded once, like the
 //     reference's strictly compiled sequential build); modules are cached per
 //     loop signature and source until op_exit.
@@ -127,7 +132,10 @@ std::string expand(const std::string &src, std::vector<std::string> &seen, int d
 
 // OFF: an optional argument switched off (op_opt_arg_dat / op_opt_arg_gbl
 // with opt = 0): the kernel gets a pointer to zeroed scratch it must not use.
-enum ArgKind { DIRECT, INDIRECT, GBL, IDX, OFF };
+// INFO: op_arg_info, the payload the kernel writes where its MIN/MAX global
+// (argument `idx`) improves; kept per thread with the element index of the
+// improvement, and the lowest index among equal best values wins.
+enum ArgKind { DIRECT, INDIRECT, GBL, IDX, OFF, INFO };
 
 struct ArgPlan {
   ArgKind kind;
@@ -243,10 +251,23 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
     if (a.kind == DIRECT || a.kind == INDIRECT || a.kind == GBL || a.kind == OFF)
       s << ", " << a.ctype << " *op2b_d" << i;
     if (a.kind == INDIRECT || (a.kind == IDX && a.mdim > 0)) s << ", const int *op2b_m" << i;
+    if (a.kind == INFO)  // per block: best value, its element, its payload
+      s << ", double *op2b_iv" << i << ", long long *op2b_ix" << i << ", " << a.ctype
+        << " *op2b_ip" << i;
   }
   // coloured: this launch runs the elements op2b_perm[op2b_first, +op2b_n)
   if (coloured) s << ", const int *op2b_perm, int op2b_first";
   s << ") {\n";
+  for (size_t i = 0; i < ap.size(); i++) {
+    const ArgPlan &a = ap[i];
+    if (a.kind == INFO) {
+      const ArgPlan &g = ap[(size_t)a.idx];
+      s << "  " << a.ctype << " op2b_l" << i << "[" << a.dim << "];\n  for (int k = 0; k < "
+        << a.dim << "; k++) op2b_l" << i << "[k] = 0;\n  long long op2b_e" << i
+        << " = 0x7fffffffffffffffLL;\n  " << g.ctype << " op2b_pv" << i << " = "
+        << identity(g.ctype, g.acc) << ";\n";
+    }
+  }
   for (size_t i = 0; i < ap.size(); i++) {
     const ArgPlan &a = ap[i];
     if (a.kind == GBL && a.acc != OP_READ)
@@ -309,6 +330,9 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
         if (a.acc == OP_READ) call << "op2b_d" << i;
         else call << "op2b_l" << i;
         break;
+      case INFO:
+        call << "op2b_l" << i;
+        break;
       case IDX:
         if (a.mdim > 0)
           s << "    int op2b_x" << i << " = op2b_m" << i << "[(size_t)op2b_e * " << a.mdim
@@ -321,6 +345,10 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
   }
   call << ");\n";
   s << call.str();
+  for (size_t i = 0; i < ap.size(); i++)
+    if (ap[i].kind == INFO)
+      s << "    if (op2b_l" << ap[i].idx << "[0] != op2b_pv" << i << ") { op2b_pv" << i
+        << " = op2b_l" << ap[i].idx << "[0]; op2b_e" << i << " = op2b_e; }\n";
   for (size_t i = 0; i < ap.size(); i++) {
     const ArgPlan &a = ap[i];
     if (a.kind == INDIRECT && a.acc == OP_INC && a.vec)
@@ -333,6 +361,25 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
         << " + (size_t)op2b_t" << i << " * " << a.dim << " + k, op2b_l" << i << "[k]);\n";
   }
   s << "  }\n";
+  for (size_t i = 0; i < ap.size(); i++) {
+    const ArgPlan &a = ap[i];
+    if (a.kind != INFO) continue;
+    const bool mx = ap[(size_t)a.idx].acc == OP_MAX;
+    // the block's best: thread 0 walks the block's candidates in order
+    s << "  {\n    __shared__ double sv[256];\n    __shared__ long long se[256];\n"
+      << "    __shared__ " << a.ctype << " sp[256 * " << a.dim << "];\n"
+      << "    sv[threadIdx.x] = (double)op2b_pv" << i << ";\n    se[threadIdx.x] = op2b_e" << i
+      << ";\n    for (int k = 0; k < " << a.dim << "; k++) sp[threadIdx.x * " << a.dim
+      << " + k] = op2b_l" << i << "[k];\n    __syncthreads();\n"
+      << "    if (threadIdx.x == 0) {\n      int b = -1;\n"
+      << "      for (int t = 0; t < (int)blockDim.x; t++) {\n"
+      << "        if (se[t] == 0x7fffffffffffffffLL) continue;\n"
+      << "        if (b < 0 || sv[t] " << (mx ? ">" : "<") << " sv[b] || (sv[t] == sv[b] && se[t] < se[b])) b = t;\n"
+      << "      }\n      op2b_ix" << i << "[blockIdx.x] = b < 0 ? 0x7fffffffffffffffLL : se[b];\n"
+      << "      if (b >= 0) {\n        op2b_iv" << i << "[blockIdx.x] = sv[b];\n"
+      << "        for (int k = 0; k < " << a.dim << "; k++) op2b_ip" << i << "[blockIdx.x * "
+      << a.dim << " + k] = sp[b * " << a.dim << " + k];\n      }\n    }\n  }\n";
+  }
   for (size_t i = 0; i < ap.size(); i++) {
     const ArgPlan &a = ap[i];
     if (a.kind != GBL || a.acc == OP_READ) continue;
@@ -549,10 +596,20 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
         a.mdim = x.map->dim;
         a.idx = x.idx;
       }
+    } else if (x.argtype == OP_ARG_INFO) {
+      a.kind = INFO;
+      a.ctype = base_type(x.type);
+      a.bytes = type_size(a.ctype);
+      a.dim = x.dim;
+      a.idx = x.idx;  // the MIN/MAX global it follows
+      const int g = x.idx;
+      if (!a.bytes || a.dim <= 0 || !x.data || g < 0 || g >= nargs ||
+          args[g].argtype != OP_ARG_GBL || args[g].dim != 1 || !args[g].opt ||
+          (args[g].acc != OP_MIN && args[g].acc != OP_MAX))
+        return set_error("op_par_loop(%s): argument %d: op_arg_info must follow a dim-1 "
+                         "OP_MIN or OP_MAX global", name, i), -1;
     } else {
-      set_error("op_par_loop(%s): argument %d: op_arg_info is not supported for run-time "
-                "compiled loops", name, i);
-      return -1;
+      return set_error("op_par_loop(%s): argument %d: unknown argument kind", name, i), -1;
     }
     key << "|" << a.kind << ":" << a.ctype << ":" << a.dim << ":" << a.acc << ":" << a.mdim
         << ":" << a.idx << ":" << a.vec;
@@ -575,6 +632,10 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
   body += expand(ksrc, seen, 0);
   for (auto &kv : r.consts) key << "|c:" << kv.first << ":" << r.const_types[kv.first] << ":" << kv.second.size();
   key << "|s:" << std::hash<std::string>()(body) << "|col:" << coloured;
+  for (auto &a : ap)
+    if (coloured && a.kind == INFO)
+      return set_error("op_par_loop(%s): op_arg_info in a loop that runs colour by colour is "
+                       "not supported", name), -1;
   // the colouring (built once per loop signature and cached with the plans)
   const Plan *plan = nullptr;
   if (coloured && set->size > 0 && !(plan = colour_plan(name, set, nargs, args))) return -1;
@@ -594,6 +655,14 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
     if (ap[(size_t)i].kind == GBL || ap[(size_t)i].kind == OFF) {  // OFF: zeroed scratch
       goff[(size_t)i] = gbytes;
       gbytes += ((size_t)ap[(size_t)i].dim * ap[(size_t)i].bytes + 15) & ~(size_t)15;
+    }
+  // INFO: per launched block, best value (double), its element, its payload
+  const long long max_grid = (long long)r.nsm * 8;
+  for (int i = 0; i < nargs; i++)
+    if (ap[(size_t)i].kind == INFO) {
+      goff[(size_t)i] = gbytes;
+      gbytes += ((size_t)max_grid * (16 + (size_t)ap[(size_t)i].dim * ap[(size_t)i].bytes) + 15) &
+                ~(size_t)15;
     }
   std::vector<char> gh(gbytes, 0);
   for (int i = 0; i < nargs; i++) {
@@ -655,6 +724,15 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
       kp.push_back(&ptrs.back());
       bytes += 4.0 * n;
     }
+    if (a.kind == INFO) {
+      char *base = (char *)j.gbl_d + goff[(size_t)i];
+      ptrs.push_back(base);
+      kp.push_back(&ptrs.back());
+      ptrs.push_back(base + 8 * max_grid);
+      kp.push_back(&ptrs.back());
+      ptrs.push_back(base + 16 * max_grid);
+      kp.push_back(&ptrs.back());
+    }
   }
   r.begin_loop(name);
   // one launch over the set, or one per colour over its slice of col_reord
@@ -665,13 +743,14 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
     kp.push_back(&perm);
     kp.push_back(&first);
   }
+  unsigned grid = 0;  // of the last launch (a loop with op_arg_info has one)
   for (int c = 0; c < ncol && set->size > 0; c++) {
     if (plan) {
       first = plan->pub.color2_offsets[c];
       n = plan->pub.color2_offsets[c + 1] - first;
     }
     if (n <= 0) continue;
-    unsigned grid = (unsigned)std::min<long long>(((long long)n + 255) / 256, (long long)r.nsm * 8);
+    grid = (unsigned)std::min<long long>(((long long)n + 255) / 256, max_grid);
     if (!cuda_ok(cudaLaunchKernel((const void *)j.fn, dim3(grid), dim3(256), kp.data(), 0,
                                   r.stream),
                  "op_par_loop: launch")) {
@@ -690,6 +769,48 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
                "op_par_loop: globals") ||
       !cuda_ok(cudaStreamSynchronize(r.stream), "op_par_loop: globals"))
     return -1;
+  // op_arg_info first, against the caller's value of its global before the
+  // loop: the payload of the best value over the blocks, lowest element on
+  // ties, if that value improves on the caller's (else the kernel would
+  // never have written it)
+  for (int i = 0; i < nargs; i++) {
+    const ArgPlan &a = ap[(size_t)i];
+    if (a.kind != INFO || n == 0) continue;
+    const ArgPlan &g = ap[(size_t)a.idx];
+    const bool mx = g.acc == OP_MAX;
+    const char *base = gh.data() + goff[(size_t)i];
+    int best = -1;
+    double bv = 0.0;
+    long long be = 0;
+    for (unsigned b = 0; b < grid; b++) {
+      double v;
+      long long e;
+      memcpy(&v, base + 8 * b, 8);
+      memcpy(&e, base + 8 * max_grid + 8 * b, 8);
+      if (e == 0x7fffffffffffffffLL) continue;
+      if (best < 0 || (mx ? v > bv : v < bv) || (v == bv && e < be)) {
+        best = (int)b;
+        bv = v;
+        be = e;
+      }
+    }
+    if (best < 0) continue;
+    double u;  // the caller's value of the global
+    const char *ud = args[a.idx].data;
+    if (g.ctype == "double") memcpy(&u, ud, 8);
+    else if (g.ctype == "float") {
+      float f;
+      memcpy(&f, ud, 4);
+      u = f;
+    } else {
+      int k;
+      memcpy(&k, ud, 4);
+      u = k;
+    }
+    if (mx ? bv > u : bv < u)
+      memcpy(args[i].data, base + 16 * max_grid + (size_t)best * a.dim * a.bytes,
+             (size_t)a.dim * a.bytes);
+  }
   for (int i = 0; i < nargs; i++) {
     const ArgPlan &a = ap[(size_t)i];
     if (a.kind != GBL || a.acc == OP_READ || n == 0) continue;

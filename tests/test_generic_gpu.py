@@ -300,6 +300,50 @@ inline void gen_opt(const double *a, double *b, double *extra, double *gsum) {
             assert np.all(op2.op_fetch_data(pe) == 5.0) and g[0] == 100.0
 
 
+def test_arg_info_follows_the_best_element(op2):
+    """op_arg_info in a run-time compiled loop: the payload the kernel
+    writes where its OP_MAX (or OP_MIN) global improves ends at the element
+    with the best value, the lowest such element on ties, as the reference's
+    CUDA reductions give it; a loop that never beats the caller's value
+    leaves the payload alone."""
+    op2.register_kernel("gen_argmax", """
+inline void gen_argmax(const double *v, const int *i, double *best, int *where) {
+  if (*v > *best) { *best = *v; where[0] = *i; where[1] = 7 * (*i); }
+}
+""")
+    op2.register_kernel("gen_argmin", """
+inline void gen_argmin(const double *v, const int *i, double *low, int *where) {
+  if (*v < *low) { *low = *v; *where = *i; }
+}
+""")
+    rng = np.random.default_rng(8)
+    n = 200000
+    v = rng.integers(-1000, 1000, size=n).astype(np.float64)
+    v[[5000, 123456, 199999]] = 5000.0       # ties for the maximum
+    v[[77, 150000]] = -9000.0                 # and for the minimum
+    s = op2.op_decl_set(n, "s")
+    pv = op2.op_decl_dat(s, 1, "double", v, "v")
+    best = np.array([-1e300])
+    where = np.array([-1, -1], np.int32)
+    op2.op_par_loop("gen_argmax", s, op2.op_arg_dat(pv, -1, op2.OP_ID, 1, "double", op2.OP_READ),
+                    op2.op_arg_idx(-1, op2.OP_ID), op2.op_arg_gbl(best, 1, "double", op2.OP_MAX),
+                    op2.op_arg_info(where, 2, "int", 2))
+    assert best[0] == 5000.0 and list(where) == [5000, 35000]
+    low = np.array([1e300])
+    w1 = np.array([-1], np.int32)
+    op2.op_par_loop("gen_argmin", s, op2.op_arg_dat(pv, -1, op2.OP_ID, 1, "double", op2.OP_READ),
+                    op2.op_arg_idx(-1, op2.OP_ID), op2.op_arg_gbl(low, 1, "double", op2.OP_MIN),
+                    op2.op_arg_info(w1, 1, "int", 2))
+    assert low[0] == -9000.0 and w1[0] == 77
+    # the caller's value already better: the payload stays
+    best2 = np.array([6000.0])
+    w2 = np.array([-5, -6], np.int32)
+    op2.op_par_loop("gen_argmax", s, op2.op_arg_dat(pv, -1, op2.OP_ID, 1, "double", op2.OP_READ),
+                    op2.op_arg_idx(-1, op2.OP_ID), op2.op_arg_gbl(best2, 1, "double", op2.OP_MAX),
+                    op2.op_arg_info(w2, 2, "int", 2))
+    assert best2[0] == 6000.0 and list(w2) == [-5, -6]
+
+
 def test_application_loop_sharing_an_airfoil_name(op2):
     """An application's own 'update' (jac1's signature) is not Airfoil's: its
     source is compiled and run instead of the hand-written update loop."""
