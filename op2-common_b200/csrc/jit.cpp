@@ -24,7 +24,8 @@
 //     launch per colour, so that no two elements of a launch share a target;
 //     the colouring covers indirect OP_INC, OP_RW and OP_WRITE arguments;
 //   * vector map arguments (idx = -k) get k pointers; switched-off optional
-//     arguments a pointer to zeroed scratch;
+//     arguments a pointer to zeroed scratch; an OP_WORK global a thread's own
+//     copy of the caller's values (scratch, not written back);
 //   * op_arg_info: the payload the kernel writes where its OP_MIN/OP_MAX
 //     global improves, kept per thread with the element of the improvement;
 //     the best value over the loop wins, the lowest element on ties (the
@@ -270,7 +271,10 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
   }
   for (size_t i = 0; i < ap.size(); i++) {
     const ArgPlan &a = ap[i];
-    if (a.kind == GBL && a.acc != OP_READ)
+    if (a.kind == GBL && a.acc == OP_WORK)  // a thread's own scratch, from the caller's values
+      s << "  " << a.ctype << " op2b_l" << i << "[" << a.dim << "];\n  for (int k = 0; k < "
+        << a.dim << "; k++) op2b_l" << i << "[k] = op2b_d" << i << "[k];\n";
+    else if (a.kind == GBL && a.acc != OP_READ)
       s << "  " << a.ctype << " op2b_l" << i << "[" << a.dim << "];\n  for (int k = 0; k < "
         << a.dim << "; k++) op2b_l" << i << "[k] = " << identity(a.ctype, a.acc) << ";\n";
   }
@@ -382,7 +386,7 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
   }
   for (size_t i = 0; i < ap.size(); i++) {
     const ArgPlan &a = ap[i];
-    if (a.kind != GBL || a.acc == OP_READ) continue;
+    if (a.kind != GBL || a.acc == OP_READ || a.acc == OP_WORK) continue;
     const char *op = a.acc == OP_INC ? "v + w" : a.acc == OP_MIN ? "op2b_min(v, w)" : "op2b_max(v, w)";
     s << "  for (int k = 0; k < " << a.dim << "; k++) {\n    " << a.ctype << " v = op2b_l" << i
       << "[k];\n    for (int o = 16; o > 0; o >>= 1) { " << a.ctype
@@ -585,8 +589,10 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
       a.acc = x.acc;
       if (!a.bytes || !x.data || a.dim <= 0)
         return set_error("op_par_loop(%s): argument %d: global of unsupported type '%s'", name, i, x.type ? x.type : ""), -1;
-      if (a.acc != OP_READ && a.acc != OP_INC && a.acc != OP_MIN && a.acc != OP_MAX)
-        return set_error("op_par_loop(%s): argument %d: globals are OP_READ, OP_INC, OP_MIN or OP_MAX", name, i), -1;
+      if (a.acc != OP_READ && a.acc != OP_INC && a.acc != OP_MIN && a.acc != OP_MAX &&
+          a.acc != OP_WORK)
+        return set_error("op_par_loop(%s): argument %d: globals are OP_READ, OP_INC, OP_MIN, "
+                         "OP_MAX or OP_WORK", name, i), -1;
     } else if (x.argtype == OP_ARG_IDX) {
       a.kind = IDX;
       a.ctype = "int";
@@ -669,8 +675,8 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
     const ArgPlan &a = ap[(size_t)i];
     if (a.kind != GBL) continue;
     char *dst = gh.data() + goff[(size_t)i];
-    if (a.acc == OP_READ || a.acc == OP_INC) {
-      if (a.acc == OP_READ) memcpy(dst, args[i].data, (size_t)a.dim * a.bytes);
+    if (a.acc == OP_READ || a.acc == OP_INC || a.acc == OP_WORK) {
+      if (a.acc != OP_INC) memcpy(dst, args[i].data, (size_t)a.dim * a.bytes);
       continue;  // OP_INC starts from zero
     }
     for (int k = 0; k < a.dim; k++) {  // MIN / MAX start from the identity
@@ -763,7 +769,7 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
   r.end_loop(bytes);
   // reductions: combine with the caller's values once the loop has finished
   bool reduce = false;
-  for (auto &a : ap) reduce |= a.kind == GBL && a.acc != OP_READ;
+  for (auto &a : ap) reduce |= a.kind == GBL && a.acc != OP_READ && a.acc != OP_WORK;
   if (!reduce) return 0;
   if (!cuda_ok(cudaMemcpyAsync(gh.data(), j.gbl_d, gbytes, cudaMemcpyDeviceToHost, r.stream),
                "op_par_loop: globals") ||
@@ -813,7 +819,7 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
   }
   for (int i = 0; i < nargs; i++) {
     const ArgPlan &a = ap[(size_t)i];
-    if (a.kind != GBL || a.acc == OP_READ || n == 0) continue;
+    if (a.kind != GBL || a.acc == OP_READ || a.acc == OP_WORK || n == 0) continue;
     const char *src = gh.data() + goff[(size_t)i];
     char *dst = args[i].data;
     for (int k = 0; k < a.dim; k++) {

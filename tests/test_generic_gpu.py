@@ -344,6 +344,29 @@ inline void gen_argmin(const double *v, const int *i, double *low, int *where) {
     assert best2[0] == 6000.0 and list(w2) == [-5, -6]
 
 
+def test_work_global_is_per_thread_scratch(op2):
+    """An OP_WORK global (op_lib_core.h:114) is scratch: each thread gets
+    the caller's values to work in, and nothing is written back."""
+    op2.register_kernel("gen_work", """
+inline void gen_work(const double *a, double *b, double *w) {
+  w[0] = 2.0 * (*a);
+  w[1] = w[0] + w[2];
+  *b = w[1];
+}
+""")
+    n = 10000
+    a = np.arange(n, dtype=np.float64)
+    s = op2.op_decl_set(n, "s")
+    pa = op2.op_decl_dat(s, 1, "double", a, "a")
+    pb = op2.op_decl_dat(s, 1, "double", None, "b")
+    w = np.array([0.0, 0.0, 0.5])
+    op2.op_par_loop("gen_work", s, op2.op_arg_dat(pa, -1, op2.OP_ID, 1, "double", op2.OP_READ),
+                    op2.op_arg_dat(pb, -1, op2.OP_ID, 1, "double", op2.OP_WRITE),
+                    op2.op_arg_gbl(w, 3, "double", op2.OP_WORK))
+    assert np.array_equal(op2.op_fetch_data(pb)[:, 0], 2.0 * a + 0.5)
+    assert list(w) == [0.0, 0.0, 0.5]
+
+
 def test_application_loop_sharing_an_airfoil_name(op2):
     """An application's own 'update' (jac1's signature) is not Airfoil's: its
     source is compiled and run instead of the hand-written update loop."""
