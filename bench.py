@@ -86,6 +86,10 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-variants", action="store_true")
     p.add_argument("--cpu-iters", type=int, default=4)
+    p.add_argument("--ref-trajectory", type=int, default=1,
+                   help="1: the CPU baseline runs the reference's OpenMP build for the whole "
+                        "end-to-end job's iterations on the same mesh (timing and rms "
+                        "trajectory); 0: a bounded sample of --cpu-iters iterations")
     p.add_argument("--option", action="append", default=[], metavar="KEY=VALUE",
                    help="a library option (op2b_set_option) for the timed runs and the "
                         "end-to-end job; repeatable")
@@ -109,6 +113,49 @@ def mesh_file(I, J, seed):
         os.replace(tmp, path)
         return m, path
     return M.read_grid_bin(path), path
+
+
+def rcm_mesh_file(I, J, seed, m):
+    """The same mesh in the numbering the GPU arm solves on: renumbered by the
+    oracle's restatement of op_renumber (reverse Cuthill-McKee; the library's
+    GPU permutations equal it bit for bit).  For the reference legs only."""
+    from op2b import mesh as M
+    from oracle import oracle as O
+    path = os.path.join(tempfile.gettempdir(), f"op2b_mesh_{I}x{J}_s{seed}_rcm.bin")
+    if not os.path.exists(path):
+        mr, _ = O.rcm_mesh(m)
+        tmp = path + f".{os.getpid()}"
+        M.write_grid_bin(mr, tmp)
+        os.replace(tmp, path)
+    return path
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def survey_bytes(loop, C, N, E, B, es=8):
+    """Compulsory bytes of one call of `loop` (each array element moved once;
+    es-byte reals, int32 maps): save_soln 64 C; adt_calc 16 C + 16 N + 40 C;
+    res_calc 16 E + 16 N + 104 C; bres_calc 12 B + 120 B; update 136 C -- for
+    es = 8.  A fused launch counts the loops it stands for."""
+    r = es / 8.0
+    one = {"save_soln": 64 * r * C,
+           "adt_calc": 16 * C + 16 * r * N + 40 * r * C,
+           "res_calc": 16 * E + 16 * r * N + 104 * r * C,
+           "bres_calc": 12 * B + 120 * r * B,
+           "update": 136 * r * C}
+    parts = loop.split("+")
+    if not all(p in one for p in parts):
+        return None
+    return sum(one[p] for p in parts)
 
 
 def peaks():
@@ -181,19 +228,23 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def run_reference(args, m_path, ncell, iters, skip, threads):
+def run_reference(args, m_path, ncell, iters, skip, threads, numbering):
+    """The reference's OpenMP build on a mesh file; returns (baseline dict, rms history)."""
     from oracle import oracle as O
     binary = O.ref_binary("ref_airfoil_openmp")
     if binary is None:
-        return None
-    summary, _ = O.run_reference_airfoil_timed(binary, m_path, iters, skip,
-                                               env={"OMP_NUM_THREADS": str(threads)})
+        return None, None
+    summary, rms = O.run_reference_airfoil_timed(binary, m_path, iters, skip,
+                                                 env={"OMP_NUM_THREADS": str(threads)})
+    label = ("RCM-renumbered as the GPU arm solves it" if numbering == "rcm"
+             else "random numbering")
     return dict(value=summary["ms_per_iter"], unit="ms/iter",
-                cores=summary.get("threads", threads), kind="reference",
+                cores=summary.get("threads", threads), cpu=cpu_model(), kind="reference",
+                numbering=numbering,
                 sample=f"{summary['timed_iters']} iterations of the {args.mesh[0]}x{args.mesh[1]} "
-                       f"mesh ({ncell} cells, random numbering) after {skip} untimed, the "
+                       f"mesh ({ncell} cells, {label}) after {skip} untimed, the "
                        "reference's OpenMP build (v1 translator output), "
-                       f"OMP_NUM_THREADS={threads}")
+                       f"OMP_NUM_THREADS={threads}"), rms
 
 
 def impl_reference(args):
@@ -202,23 +253,56 @@ def impl_reference(args):
         return 0
     m, path = mesh_file(*args.mesh, args.seed)
     threads = os.cpu_count() or 1
-    # one step = one iteration of the reference's OpenMP build on the same mesh;
-    # warm-up iterations (its plan construction included) run but are not timed
-    res = run_reference(args, path, m.ncell, args.warmup + args.steps, args.warmup, threads)
+    # one step = one iteration of the reference's OpenMP build on the mesh the
+    # GPU arm solves (same numbering); warm-up iterations (its plan
+    # construction included) run but are not timed
+    main_path = rcm_mesh_file(*args.mesh, args.seed, m) if args.numbering == "rcm" else path
+    res, _ = run_reference(args, main_path, m.ncell, args.warmup + args.steps, args.warmup,
+                           threads, args.numbering)
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable":
                           "oracle/_ref/ref_airfoil_openmp not built (make -C oracle)"}))
         return 0
+    # the other numbering, as a second, labelled sample (block colouring
+    # collapses on random order: a few iterations suffice)
+    other = None
+    if args.numbering == "rcm":
+        other, _ = run_reference(args, path, m.ncell, 1 + args.cpu_iters, 1, threads, "random")
     v = res["value"]
     print(json.dumps({
         "metric": METRIC, "value": v, "unit": "ms/iter", "impl": "reference", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"airfoil {args.mesh[0]}x{args.mesh[1]} plain FP64",
-                   "cells": m.ncell, "edges": m.nedge},
+                   "cells": m.ncell, "edges": m.nedge, "numbering": args.numbering},
         "cpu_baseline": res,
+        "other_numbering": other,
         "e2e": {"value": v, "unit": "ms/iter", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
     return 0
+
+
+def trajectory_parity(args, rms, q, ref_rms):
+    """The end-to-end job's rms history and final q against the reference on
+    the same mesh and numbering: the reference's sequential build (committed
+    fixture: rms of every iteration and a digest of q after 1000) and, when it
+    ran, the reference's OpenMP build timed beside (its rms history)."""
+    import hashlib
+    out = {"iterations": int(rms.size)}
+    fx = os.path.join(REPO, "tests", "golden",
+                      f"airfoil_{args.mesh[0]}x{args.mesh[1]}_s{args.seed}_rcm.npz")
+    if (args.numbering == "rcm" and args.precision == "f64" and os.path.exists(fx)):
+        gd = np.load(fx)
+        n = int(gd["niter_traj"])
+        if rms.size == n:
+            out["vs_reference_seq"] = {
+                "rms_traj_max_rel": float(np.max(np.abs(rms / gd["rms_traj"] - 1))),
+                "q_bit_exact": hashlib.sha256(np.ascontiguousarray(q, dtype="<f8").tobytes())
+                .hexdigest() == str(gd["q_digest_traj"]),
+                "source": os.path.relpath(fx, REPO)}
+    if ref_rms is not None and ref_rms.size == rms.size:
+        out["vs_reference_openmp"] = {"rms_traj_max_rel":
+                                      float(np.max(np.abs(rms / ref_rms - 1)))}
+    return out
 
 
 def timed_run(L, Airfoil, mesh, dtype, numbering, inc_mode, part, steps, warmup, torch,
@@ -373,12 +457,15 @@ def main():
         if args.numbering == "rcm":
             app2.renumber()
         tb = time.perf_counter()
-        app2.iterate(K)
+        e2e_hist = app2.iterate(K)
         tc = time.perf_counter()
         q = L.op_fetch_data(app2.p_q)
         t1 = time.perf_counter()
         barrier()
         ms_e2e = max_over_ranks(1e3 * (t1 - t0) / K)
+        # (outside the timed region) q back in the declared cell order
+        e2e_q = q[L.set_permutation(app2.cells)] if args.numbering == "rcm" else q
+        e2e_rms = np.array([h[0] for h in e2e_hist])
         es = np.dtype(dtype).itemsize
         # x, the maps, the bound flags and q are uploaded; qold/adt/res are
         # declared without data (zeroed on the device)
@@ -399,10 +486,21 @@ def main():
         L.op_exit()
 
     # ---------------------------------------------------------- CPU baseline (rank 0, N=1)
-    cpu = None
+    cpu = cpu_other = ref_rms = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        cpu = run_reference(args, m_path, m.ncell, 1 + args.cpu_iters, 1, threads)
+        # on the mesh the GPU arm solves: the whole job's iterations (first one
+        # untimed) when the configuration is the 1000-iteration one, for the
+        # rms trajectory; a bounded sample of the other numbering beside it
+        if args.numbering == "rcm":
+            K_ref = max(args.e2e_iters, 1) if args.ref_trajectory else 1 + args.cpu_iters
+            cpu, ref_rms = run_reference(args, rcm_mesh_file(*args.mesh, args.seed, m), m.ncell,
+                                         K_ref, 1, threads, "rcm")
+            cpu_other, _ = run_reference(args, m_path, m.ncell, 1 + args.cpu_iters, 1, threads,
+                                         "random")
+        else:
+            cpu, _ = run_reference(args, m_path, m.ncell, 1 + args.cpu_iters, 1, threads,
+                                   "random")
         if cpu is None:
             from oracle import oracle as O
             from op2b.mesh import airfoil_constants
@@ -415,12 +513,24 @@ def main():
         peak, peak_src = peaks()
         work = f"{args.mesh[0]}x{args.mesh[1]}"
         loops = main_run["loops"]
+        es = np.dtype(dtype).itemsize
+        sizes = (m.ncell, m.nnode, m.nedge, m.nbedge)
+        for n, x in loops.items():
+            sb = survey_bytes(n, *sizes, es=es)
+            x["moved_bytes"] = x.pop("alg_bytes")       # what the runtime's launch must move
+            x["alg_bytes"] = sb                          # the loops' compulsory bytes
+            x["moved_gbs"] = x.pop("gbs")
+            x["gbs"] = sb / (x["avg_ms"] * 1e-3) / 1e9 if sb and x["avg_ms"] > 0 else None
         dom = max(loops, key=lambda n: loops[n]["avg_ms"] * loops[n]["calls"])
         d = loops[dom]
         key = f"{work}_{args.precision}_{args.numbering}_mode{args.inc_mode}"
-        it_bytes = sum(x["alg_bytes"] * x["calls"] for x in main_run["loops"].values()
-                       if x.get("alg_bytes"))
-        it_gbs = it_bytes / args.steps / (ms * 1e-3) / 1e9 if ms > 0 else None
+        # the iteration: save_soln + 2 x (adt_calc, res_calc, bres_calc, update)
+        it_bytes = (survey_bytes("save_soln", *sizes, es=es) + 2 * survey_bytes(
+            "adt_calc+res_calc+bres_calc+update", *sizes, es=es))
+        it_gbs = it_bytes / (ms * 1e-3) / 1e9 if ms > 0 else None
+        parity = None
+        if e2e is not None:
+            parity = trajectory_parity(args, e2e_rms, e2e_q, ref_rms)
         line = {
             "metric": METRIC, "value": ms, "unit": "ms/iter", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
@@ -439,9 +549,14 @@ def main():
             "roofline": {"bound": "hbm", "loop": dom, "achieved": d["gbs"], "peak": peak,
                          "unit": "GB/s", "frac": d["gbs"] / peak if d["gbs"] else None,
                          "traffic": traffic_from_profiles(key, dom),
+                         "alg_bytes_per_launch": d["alg_bytes"],
+                         "launch_us": 1e3 * d["avg_ms"],
+                         "moved_bytes_per_launch": d["moved_bytes"],
                          "peak_source": peak_src,
-                         # the whole iteration: every loop's algorithmic bytes per
-                         # iteration over the measured time per iteration
+                         # the whole iteration: the five loops' compulsory bytes
+                         # (save_soln + 2 x the other four) over the measured
+                         # time per iteration
+                         "iteration_alg_bytes": it_bytes,
                          "iteration_achieved": it_gbs,
                          "iteration_frac": it_gbs / peak if it_gbs else None},
             "loops": loops,
@@ -449,6 +564,8 @@ def main():
             "rms_final": main_run["rms"],
             "variants": variants,
             "cpu_baseline": cpu,
+            "cpu_other_numbering": cpu_other,
+            "parity": parity,
             "e2e": e2e,
             "gpu_launches": int(main_run["launches"]),
             "clocks": main_run["clocks"],

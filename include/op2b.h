@@ -288,8 +288,12 @@ int op2b_synchronize(void);
  *   errloc replaced only when beaten).  Results are in device memory when the
  *   work on `stream` (a cudaStream_t; NULL = legacy default stream) is done.
  *   ncell must not exceed 4,194,304; larger values return -1 with a message.
- *   The first call on a device looks up the scratch array's device address;
- *   make that first call before any stream capture.  Calls share the one
+ *   qold, q and res must be 16-byte aligned, adt, rms and maxerr 8-byte,
+ *   errloc 4-byte (cudaMalloc'd arrays are); a misaligned pointer returns -1
+ *   with a message before anything is launched.
+ *   The first call on a device (and the first after the device was reset)
+ *   looks up the scratch array's device address; make that call before any
+ *   stream capture.  Calls share the one
  *   scratch array, so calls whose work can overlap on the GPU race: serialise
  *   them.  Works without op_init (the device current on the calling thread is
  *   used). */

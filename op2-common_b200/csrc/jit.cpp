@@ -252,9 +252,9 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
     if (a.kind == DIRECT || a.kind == INDIRECT || a.kind == GBL || a.kind == OFF)
       s << ", " << a.ctype << " *op2b_d" << i;
     if (a.kind == INDIRECT || (a.kind == IDX && a.mdim > 0)) s << ", const int *op2b_m" << i;
-    if (a.kind == INFO)  // per block: best value, its element, its payload
+    if (a.kind == INFO)  // per block: best value, its element, its payload; the caller's payload
       s << ", double *op2b_iv" << i << ", long long *op2b_ix" << i << ", " << a.ctype
-        << " *op2b_ip" << i;
+        << " *op2b_ip" << i << ", const " << a.ctype << " *op2b_ic" << i;
   }
   // coloured: this launch runs the elements op2b_perm[op2b_first, +op2b_n)
   if (coloured) s << ", const int *op2b_perm, int op2b_first";
@@ -263,17 +263,18 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
     const ArgPlan &a = ap[i];
     if (a.kind == INFO) {
       const ArgPlan &g = ap[(size_t)a.idx];
+      // each thread's payload starts as the caller's (as the sequential
+      // build's info temp is a copy of the caller's data)
       s << "  " << a.ctype << " op2b_l" << i << "[" << a.dim << "];\n  for (int k = 0; k < "
-        << a.dim << "; k++) op2b_l" << i << "[k] = 0;\n  long long op2b_e" << i
+        << a.dim << "; k++) op2b_l" << i << "[k] = op2b_ic" << i << "[k];\n  long long op2b_e" << i
         << " = 0x7fffffffffffffffLL;\n  " << g.ctype << " op2b_pv" << i << " = "
         << identity(g.ctype, g.acc) << ";\n";
     }
   }
   for (size_t i = 0; i < ap.size(); i++) {
     const ArgPlan &a = ap[i];
-    if (a.kind == GBL && a.acc == OP_WORK)  // a thread's own scratch, from the caller's values
-      s << "  " << a.ctype << " op2b_l" << i << "[" << a.dim << "];\n  for (int k = 0; k < "
-        << a.dim << "; k++) op2b_l" << i << "[k] = op2b_d" << i << "[k];\n";
+    if (a.kind == GBL && a.acc == OP_WORK)  // a thread's own scratch, reloaded every element
+      s << "  " << a.ctype << " op2b_l" << i << "[" << a.dim << "];\n";
     else if (a.kind == GBL && a.acc != OP_READ)
       s << "  " << a.ctype << " op2b_l" << i << "[" << a.dim << "];\n  for (int k = 0; k < "
         << a.dim << "; k++) op2b_l" << i << "[k] = " << identity(a.ctype, a.acc) << ";\n";
@@ -285,6 +286,17 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
   else
     s << "  for (int op2b_e = blockIdx.x * blockDim.x + threadIdx.x; op2b_e < op2b_n;"
          " op2b_e += gridDim.x * blockDim.x) {\n";
+  // OP_WORK: every element starts from the caller's values
+  for (size_t i = 0; i < ap.size(); i++)
+    if (ap[i].kind == GBL && ap[i].acc == OP_WORK)
+      s << "    for (int k = 0; k < " << ap[i].dim << "; k++) op2b_l" << i << "[k] = op2b_d" << i
+        << "[k];\n";
+  // op_arg_info: a copy of the payload before the call, to see whether the
+  // kernel wrote it (a write on a tie changes the payload, not the value)
+  for (size_t i = 0; i < ap.size(); i++)
+    if (ap[i].kind == INFO)
+      s << "    " << ap[i].ctype << " op2b_s" << i << "[" << ap[i].dim << "];\n    for (int k = 0; k < "
+        << ap[i].dim << "; k++) op2b_s" << i << "[k] = op2b_l" << i << "[k];\n";
   std::ostringstream call;
   call << "    " << name << "(";
   for (size_t i = 0; i < ap.size(); i++) {
@@ -349,10 +361,16 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
   }
   call << ");\n";
   s << call.str();
+  // the thread's candidate: its best value, and the element whose call last
+  // wrote the payload (an improvement, or a write on a tie)
   for (size_t i = 0; i < ap.size(); i++)
-    if (ap[i].kind == INFO)
-      s << "    if (op2b_l" << ap[i].idx << "[0] != op2b_pv" << i << ") { op2b_pv" << i
-        << " = op2b_l" << ap[i].idx << "[0]; op2b_e" << i << " = op2b_e; }\n";
+    if (ap[i].kind == INFO) {
+      s << "    {\n      bool w = op2b_l" << ap[i].idx << "[0] != op2b_pv" << i << ";\n"
+        << "      for (int k = 0; k < " << ap[i].dim << "; k++) w |= op2b_s" << i
+        << "[k] != op2b_l" << i << "[k];\n"
+        << "      if (w) { op2b_pv" << i << " = op2b_l" << ap[i].idx << "[0]; op2b_e" << i
+        << " = op2b_e; }\n    }\n";
+    }
   for (size_t i = 0; i < ap.size(); i++) {
     const ArgPlan &a = ap[i];
     if (a.kind == INDIRECT && a.acc == OP_INC && a.vec)
@@ -638,10 +656,19 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
   body += expand(ksrc, seen, 0);
   for (auto &kv : r.consts) key << "|c:" << kv.first << ":" << r.const_types[kv.first] << ":" << kv.second.size();
   key << "|s:" << std::hash<std::string>()(body) << "|col:" << coloured;
-  for (auto &a : ap)
+  // each op_arg_info's block reduction keeps every thread's value, element and
+  // payload in static shared memory (256 threads a block)
+  size_t info_smem = 0;
+  for (auto &a : ap) {
     if (coloured && a.kind == INFO)
       return set_error("op_par_loop(%s): op_arg_info in a loop that runs colour by colour is "
                        "not supported", name), -1;
+    if (a.kind == INFO) info_smem += 256 * (16 + (size_t)a.dim * a.bytes);
+  }
+  if (info_smem > 40 * 1024)
+    return set_error("op_par_loop(%s): the op_arg_info payloads take %zu bytes of shared memory "
+                     "for a 256-thread block's reduction, above the 40960 bytes allowed: use "
+                     "fewer or smaller payloads (at most 144 bytes for one)", name, info_smem), -1;
   // the colouring (built once per loop signature and cached with the plans)
   const Plan *plan = nullptr;
   if (coloured && set->size > 0 && !(plan = colour_plan(name, set, nargs, args))) return -1;
@@ -667,10 +694,16 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
   for (int i = 0; i < nargs; i++)
     if (ap[(size_t)i].kind == INFO) {
       goff[(size_t)i] = gbytes;
-      gbytes += ((size_t)max_grid * (16 + (size_t)ap[(size_t)i].dim * ap[(size_t)i].bytes) + 15) &
-                ~(size_t)15;
+      gbytes += ((size_t)(max_grid + 1) * (16 + (size_t)ap[(size_t)i].dim * ap[(size_t)i].bytes) +
+                 15) & ~(size_t)15;
     }
   std::vector<char> gh(gbytes, 0);
+  for (int i = 0; i < nargs; i++) {  // INFO: the caller's payload after the per-block ones
+    const ArgPlan &a = ap[(size_t)i];
+    if (a.kind == INFO)
+      memcpy(gh.data() + goff[(size_t)i] + 16 * max_grid + (size_t)max_grid * a.dim * a.bytes,
+             args[i].data, (size_t)a.dim * a.bytes);
+  }
   for (int i = 0; i < nargs; i++) {
     const ArgPlan &a = ap[(size_t)i];
     if (a.kind != GBL) continue;
@@ -707,7 +740,7 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
     return -1;
   // parameters
   std::vector<void *> ptrs;
-  ptrs.reserve((size_t)nargs * 2 + 1);
+  ptrs.reserve((size_t)nargs * 4 + 1);  // kp keeps pointers into ptrs: no reallocation
   std::vector<void *> kp;
   int n = set->size;
   kp.push_back(&n);
@@ -737,6 +770,8 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
       ptrs.push_back(base + 8 * max_grid);
       kp.push_back(&ptrs.back());
       ptrs.push_back(base + 16 * max_grid);
+      kp.push_back(&ptrs.back());
+      ptrs.push_back(base + 16 * max_grid + (size_t)max_grid * a.dim * a.bytes);
       kp.push_back(&ptrs.back());
     }
   }

@@ -21,10 +21,26 @@
 // Calls whose launches can overlap on the GPU (different streams, or
 // different host threads) race on this one array and must be serialised by
 // the caller.
+//
+// Host code cannot pass the array's name to a kernel (on the host it names a
+// stand-in, not device memory), so the first call on a device, with that
+// device current, asks cudaGetSymbolAddress for the device address and keeps
+// it per device, tagged with the current context's unique ID: after the
+// caller resets the device (a new context), the next call looks the address
+// up again instead of using the old context's.  That look-up is not a stream
+// operation, but it may load the module, so the first call on a device (and
+// the first after a reset) must come before any stream capture.
+//
+// Arrays are read and written as 16-byte vectors, so qold, q and res must be
+// 16-byte aligned (adt, rms and maxerr 8-byte, errloc 4-byte); a misaligned
+// pointer is refused on the host, before anything is launched.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <climits>
 #include <cmath>
+#include <cstdint>
 
 #include "op2b.h"
 #include "op2b_runtime.h"
@@ -47,8 +63,10 @@ struct Partial {
 // partials [0, kMaxBlocks), then one slot whose first word is the ticket
 static __device__ __align__(256) Partial g_update_scratch[kMaxBlocks + 1];
 
-// device address of g_update_scratch, looked up once per device
-static Partial *g_scratch_addr[kMaxDevices] = {};
+// device address of g_update_scratch per device, and the ID of the context
+// it was looked up in (0 = not looked up yet)
+static std::atomic<Partial *> g_scratch_addr[kMaxDevices];
+static std::atomic<unsigned long long> g_scratch_ctx[kMaxDevices];
 
 __device__ __forceinline__ void merge(double &s, double &m, long long &i, double s2, double m2,
                                       long long i2) {
@@ -150,6 +168,29 @@ k_update_noalloc(int ncell, const double *__restrict__ qold, double *__restrict_
   }
 }
 
+// The unique ID of the calling thread's current context.  The two driver
+// functions are found through the runtime (the library does not link the
+// driver library itself, so it loads on machines without a GPU driver).
+bool current_context_id(unsigned long long *id) {
+  using GetCurrent = CUresult (*)(CUcontext *);
+  using GetId = CUresult (*)(CUcontext, unsigned long long *);
+  static std::atomic<GetCurrent> get_current{nullptr};
+  static std::atomic<GetId> get_id{nullptr};
+  if (!get_current.load() || !get_id.load()) {
+    void *a = nullptr, *b = nullptr;
+    cudaDriverEntryPointQueryResult qa, qb;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) != cudaSuccess ||
+        cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) != cudaSuccess ||
+        qa != cudaDriverEntryPointSuccess || qb != cudaDriverEntryPointSuccess || !a || !b)
+      return false;
+    get_current.store(reinterpret_cast<GetCurrent>(a));
+    get_id.store(reinterpret_cast<GetId>(b));
+  }
+  CUcontext ctx = nullptr;
+  return get_current.load()(&ctx) == CUDA_SUCCESS && ctx &&
+         get_id.load()(ctx, id) == CUDA_SUCCESS;
+}
+
 }  // namespace
 }  // namespace op2b
 
@@ -169,22 +210,45 @@ extern "C" int op2b_update_noalloc(int ncell, const double *qold, double *q, dou
     set_error("op2b_update_noalloc: every array and output must be a device pointer");
     return -1;
   }
+  const struct {
+    const void *p;
+    unsigned align;
+    const char *name;
+  } need[] = {{qold, 16, "qold"}, {q, 16, "q"},      {res, 16, "res"},      {adt, 8, "adt"},
+              {rms, 8, "rms"},    {maxerr, 8, "maxerr"}, {errloc, 4, "errloc"}};
+  for (const auto &a : need)
+    if (reinterpret_cast<uintptr_t>(a.p) % a.align) {
+      set_error("op2b_update_noalloc: %s = %p is not %u-byte aligned (the kernel accesses "
+                "it in %u-byte units)",
+                a.name, a.p, a.align, a.align);
+      return -1;
+    }
   int dev = 0;
   if (!cuda_ok(cudaGetDevice(&dev), "op2b_update_noalloc: cudaGetDevice")) return -1;
   if (dev < 0 || dev >= kMaxDevices) {
     set_error("op2b_update_noalloc: device ordinal %d above %d", dev, kMaxDevices - 1);
     return -1;
   }
-  if (!g_scratch_addr[dev]) {
-    // first call on this device, with the device current: resolve the
-    // array's device address (host code may not use the symbol itself)
+  // make the device's context current (created if this is the process's
+  // first CUDA work on it) and read its unique ID
+  if (!cuda_ok(cudaSetDevice(dev), "op2b_update_noalloc: cudaSetDevice")) return -1;
+  unsigned long long ctx_id = 0;
+  if (!current_context_id(&ctx_id)) {
+    set_error("op2b_update_noalloc: no current CUDA context on device %d", dev);
+    return -1;
+  }
+  Partial *scratch = g_scratch_addr[dev].load(std::memory_order_acquire);
+  if (!scratch || g_scratch_ctx[dev].load(std::memory_order_acquire) != ctx_id) {
+    // set-up, once per device and context, with the device current: resolve
+    // the array's device address (host code may not use the symbol itself)
     Partial *ptr = nullptr;
     if (!cuda_ok(cudaGetSymbolAddress((void **)&ptr, g_update_scratch),
                  "op2b_update_noalloc: cudaGetSymbolAddress"))
       return -1;
-    g_scratch_addr[dev] = ptr;
+    g_scratch_addr[dev].store(ptr, std::memory_order_release);
+    g_scratch_ctx[dev].store(ctx_id, std::memory_order_release);
+    scratch = ptr;
   }
-  Partial *scratch = g_scratch_addr[dev];
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (!cuda_ok(cudaMemsetAsync(scratch + kMaxBlocks, 0, sizeof(Partial), s),
                "op2b_update_noalloc: clearing the ticket"))

@@ -167,6 +167,19 @@ def renumber(sizes, maps, base: int):
     return [outs[s][:sizes[s]] if has[s] else None for s in range(nsets)]
 
 
+def rcm_mesh(mesh):
+    """The mesh renumbered by the restated op_renumber(pecell): reverse
+    Cuthill-McKee on cells, propagated to edges, boundary edges and nodes (the
+    permutations the library's GPU renumbering builds).  Returns (renumbered
+    mesh, per-set permutations {nodes, edges, bedges, cells}, perm[i] = new
+    index of element i)."""
+    from op2b import mesh as M
+    sizes, maps = airfoil_maps(mesh)
+    pn, pe, pb, pc = renumber(sizes, maps, 1)
+    new2old = [np.argsort(p) for p in (pn, pc, pe, pb)]
+    return M.renumber_mesh(mesh, *new2old), dict(nodes=pn, edges=pe, bedges=pb, cells=pc)
+
+
 # ---------------------------------------------------------------- reference builds
 
 def ref_binary(name: str) -> str | None:
@@ -201,17 +214,20 @@ def run_reference_airfoil(binary: str, mesh_bin: str, niter: int, ncell: int,
 
 def run_reference_airfoil_timed(binary: str, mesh_bin: str, niter: int, skip: int,
                                 env: dict | None = None):
-    """Run a reference Airfoil build for `niter` iterations, timing all but the first `skip`."""
+    """Run a reference Airfoil build for `niter` iterations, timing all but the
+    first `skip`; returns (json summary, rms history)."""
     e = dict(os.environ)
     if env:
         e.update(env)
     with tempfile.TemporaryDirectory(prefix="op2b_ref_") as tmp:
         out = subprocess.run([binary, mesh_bin, str(niter), os.path.join(tmp, "run"), str(skip)],
                              capture_output=True, text=True, env=e)
+        rp = os.path.join(tmp, "run.rms")
+        rms = np.fromfile(rp, dtype=np.float64) if os.path.exists(rp) else None
     if out.returncode != 0:
         raise RuntimeError(f"{binary} failed: {out.stdout[-2000:]} {out.stderr[-2000:]}")
     line = [ln for ln in out.stdout.splitlines() if ln.startswith("{")][-1]
-    return json.loads(line), None
+    return json.loads(line), rms
 
 
 def read_plan_dump(path: str) -> dict:

@@ -344,6 +344,87 @@ inline void gen_argmin(const double *v, const int *i, double *low, int *where) {
     assert best2[0] == 6000.0 and list(w2) == [-5, -6]
 
 
+def test_arg_info_payload_starts_from_the_callers(op2):
+    """Each thread's op_arg_info payload starts as the caller's (the
+    sequential build copies the caller's payload in before the loop): a
+    kernel that writes only part of the payload leaves the rest as the caller
+    had it.  A kernel that also writes on ties (>=) returns the payload of
+    one element that reaches the best value, never a mix of elements."""
+    op2.register_kernel("gen_argmax_part", """
+inline void gen_argmax_part(const double *v, const int *i, double *best, int *where) {
+  if (*v > *best) { *best = *v; where[0] = *i; }
+}
+""")
+    op2.register_kernel("gen_argmax_ge", """
+inline void gen_argmax_ge(const double *v, const int *i, double *best, int *where) {
+  if (*v >= *best) { *best = *v; where[0] = *i; where[1] = 3 * (*i); }
+}
+""")
+    rng = np.random.default_rng(4)
+    n = 1_000_000                      # more elements than threads: each runs several
+    v = rng.integers(0, 100, size=n).astype(np.float64)
+    v[654321] = 500.0
+    s = op2.op_decl_set(n, "s")
+    pv = op2.op_decl_dat(s, 1, "double", v, "v")
+    best = np.array([-1.0])
+    where = np.array([-1, 42], np.int32)
+    op2.op_par_loop("gen_argmax_part", s,
+                    op2.op_arg_dat(pv, -1, op2.OP_ID, 1, "double", op2.OP_READ),
+                    op2.op_arg_idx(-1, op2.OP_ID), op2.op_arg_gbl(best, 1, "double", op2.OP_MAX),
+                    op2.op_arg_info(where, 2, "int", 2))
+    assert best[0] == 500.0 and list(where) == [654321, 42]
+    # ties everywhere: the value 99 is reached by ~10,000 elements
+    v2 = np.minimum(v, 99.0)
+    pv2 = op2.op_decl_dat(s, 1, "double", v2, "v2")
+    best = np.array([-1.0])
+    where = np.array([-1, -1], np.int32)
+    op2.op_par_loop("gen_argmax_ge", s,
+                    op2.op_arg_dat(pv2, -1, op2.OP_ID, 1, "double", op2.OP_READ),
+                    op2.op_arg_idx(-1, op2.OP_ID), op2.op_arg_gbl(best, 1, "double", op2.OP_MAX),
+                    op2.op_arg_info(where, 2, "int", 2))
+    assert best[0] == 99.0
+    assert 0 <= where[0] < n and v2[where[0]] == 99.0 and where[1] == 3 * where[0]
+
+
+def test_arg_info_payload_too_large_for_the_block_reduction_is_refused(op2):
+    op2.register_kernel("gen_argmax_big", """
+inline void gen_argmax_big(const double *v, double *best, double *where) {
+  if (*v > *best) { *best = *v; where[0] = *v; }
+}
+""")
+    s = op2.op_decl_set(100, "s")
+    pv = op2.op_decl_dat(s, 1, "double", np.arange(100.0), "v")
+    best = np.array([-1.0])
+    where = np.zeros(32)                # 256 bytes a thread: 64 KiB a block
+    with pytest.raises(op2.Op2Error, match="shared memory"):
+        op2.op_par_loop("gen_argmax_big", s,
+                        op2.op_arg_dat(pv, -1, op2.OP_ID, 1, "double", op2.OP_READ),
+                        op2.op_arg_gbl(best, 1, "double", op2.OP_MAX),
+                        op2.op_arg_info(where, 32, "double", 1))
+
+
+def test_work_global_is_reloaded_for_every_element(op2):
+    """OP_WORK scratch holds the caller's values at the start of every
+    element's call, also for the second and later elements a thread runs."""
+    op2.register_kernel("gen_work_rd", """
+inline void gen_work_rd(const double *a, double *b, double *w) {
+  *b = w[0] + w[1];
+  w[0] = *a;
+}
+""")
+    n = 1_000_000
+    a = np.arange(n, dtype=np.float64)
+    s = op2.op_decl_set(n, "s")
+    pa = op2.op_decl_dat(s, 1, "double", a, "a")
+    pb = op2.op_decl_dat(s, 1, "double", None, "b")
+    w = np.array([0.25, 0.5])
+    op2.op_par_loop("gen_work_rd", s, op2.op_arg_dat(pa, -1, op2.OP_ID, 1, "double", op2.OP_READ),
+                    op2.op_arg_dat(pb, -1, op2.OP_ID, 1, "double", op2.OP_WRITE),
+                    op2.op_arg_gbl(w, 2, "double", op2.OP_WORK))
+    assert np.all(op2.op_fetch_data(pb)[:, 0] == 0.75)
+    assert list(w) == [0.25, 0.5]
+
+
 def test_work_global_is_per_thread_scratch(op2):
     """An OP_WORK global (op_lib_core.h:114) is scratch: each thread gets
     the caller's values to work in, and nothing is written back."""

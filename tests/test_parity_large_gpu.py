@@ -1,0 +1,110 @@
+"""Parity at the benchmarked configuration: the 2400x1200 (2.88M-cell) mesh,
+seed 1, renumbered on the GPU, against the reference's own sequential build.
+
+The fixture (tests/golden/airfoil_2400x1200_s1_rcm.npz, made by
+tests/golden/make_golden.py from oracle/_ref/ref_airfoil_seq_strict, the
+reference's airfoil kernels and op_seq.h loop compiled with every operation
+rounded once) holds, for the mesh renumbered by the restated reverse
+Cuthill-McKee order (which the GPU's permutations equal bit for bit,
+tests/test_renumber_gpu.py):
+
+* SHA-256 digests of the whole q field after 100 and after 1000 iterations,
+  in the declared cell order;
+* the rms, maxerr and errloc histories (apps/c/airfoil/airfoil_plain/dp/
+  airfoil.cpp:221-297, niter = 1000 there).
+
+The default path -- the one bench.py times: owner-computes increments over
+corner records, res_calc fused with bres_calc, adt_calc computed by the
+update ahead of its call, save_soln by renaming, the res_calc+bres_calc pair
+launched by the update's call, res left unwritten by update -- must give q
+bit for bit, maxerr and errloc exactly, and rms within 1e-13 relative (only
+the rms sum's grouping differs).  The other increment strategies (atomics,
+colouring, staged hybrid) and the randomly numbered mesh reorder the
+increments, so they are held to the north-star tolerance: q within 1e-12 of
+max|q| per component and rms within 1e-12 relative after 100 iterations.
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from op2b import lib as L
+from op2b import mesh as M
+from op2b.airfoil import Airfoil
+
+pytestmark = pytest.mark.gpu
+
+FIXTURE = f"{GOLDEN}/airfoil_2400x1200_s1_rcm.npz"
+
+
+def _digest(q):
+    return hashlib.sha256(np.ascontiguousarray(q, dtype="<f8").tobytes()).hexdigest()
+
+
+def _mesh_digest(m):
+    h = hashlib.sha256()
+    for a in (m.x, m.cell, m.edge, m.ecell, m.bedge, m.becell, m.bound):
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+@pytest.fixture(scope="module")
+def large():
+    gd = np.load(FIXTURE)
+    m = M.channel_bump(int(gd["I"]), int(gd["J"]), seed=int(gd["seed"]))
+    assert _mesh_digest(m) == str(gd["digest"]), "the mesh generator no longer makes the fixture's mesh"
+    return gd, m
+
+
+def test_default_path_is_bit_exact_with_reference_at_2400x1200(op2, large):
+    gd, m = large
+    app = Airfoil(m)
+    app.renumber()
+    hist = app.iterate(int(gd["niter"]))
+    rms = np.array([h[0] for h in hist])
+    mx = np.array([h[1] for h in hist])
+    el = np.array([h[2] for h in hist])
+    assert np.max(np.abs(rms / gd["rms"] - 1)) < 1e-13
+    assert np.array_equal(mx, gd["maxerr"])
+    # errloc is the loop index of the renumbered mesh, as in the fixture's run
+    assert np.array_equal(el, gd["errloc_rcm"])
+    q = app.fetch_original()
+    assert _digest(q) == str(gd["q_digest"]), "q after 100 iterations is not bit-identical"
+    idx = gd["q_sample_idx"]
+    assert np.array_equal(q[idx], gd["q_sample"])
+
+
+def test_default_path_1000_iterations_bit_exact(op2, large):
+    """The configuration's full length: the rms trajectory of all 1000
+    iterations and the final q field."""
+    gd, m = large
+    app = Airfoil(m)
+    app.renumber()
+    n = int(gd["niter_traj"])
+    hist = app.iterate(n)
+    rms = np.array([h[0] for h in hist])
+    assert np.max(np.abs(rms / gd["rms_traj"] - 1)) < 1e-13
+    assert np.array_equal(np.array([h[1] for h in hist]), gd["maxerr_traj"])
+    q = app.fetch_original()
+    assert _digest(q) == str(gd["q_digest_traj"]), "q after 1000 iterations is not bit-identical"
+
+
+@pytest.mark.parametrize("numbering,mode", [("rcm", L.OP2B_INC_ATOMIC), ("rcm", L.OP2B_INC_COLOR),
+                                            ("rcm", L.OP2B_INC_HYBRID),
+                                            ("random", L.OP2B_INC_GATHER),
+                                            ("random", L.OP2B_INC_ATOMIC)])
+def test_other_strategies_within_tolerance_at_2400x1200(op2, large, numbering, mode):
+    gd, m = large
+    op2.set_option("inc_mode", mode)
+    app = Airfoil(m)
+    if numbering == "rcm":
+        app.renumber()
+    hist = app.iterate(int(gd["niter"]))
+    rms = np.array([h[0] for h in hist])
+    assert np.max(np.abs(rms / gd["rms"] - 1)) < 1e-12
+    q = app.fetch_original()
+    idx = gd["q_sample_idx"]
+    scale = np.abs(gd["q_sample"]).max(axis=0)
+    assert np.all(np.abs(q[idx] - gd["q_sample"]).max(axis=0) <= 1e-12 * scale)
+    assert np.allclose(q.sum(axis=0), gd["q_sum"], rtol=1e-12, atol=0)
