@@ -407,10 +407,23 @@ def main():
                                  "ms_per_iter": max_over_ranks(v["ms"]),
                                  "res_calc_gbs": v["loops"].get("res_calc", {}).get("gbs"),
                                  "launches_per_iter": v["launches"] / 20})
+        # per-edge atomics beside the default segmented ones, and the plan-driven
+        # strategies on the parallel (Jones-Plassmann) colouring
+        for numbering, mode, o in (("random", 0, {"atomic_segmented": 0}),
+                                   ("rcm", 0, {"atomic_segmented": 0}),
+                                   ("rcm", 1, {"plan_mode": 1}), ("rcm", 2, {"plan_mode": 1}),
+                                   ("random", 2, {"plan_mode": 1})):
+            v = timed_run(L, Airfoil, m, dtype, numbering, mode, args.part_size, 20, 3, torch,
+                          barrier, opts=o)
+            variants.append({"numbering": numbering, "inc_mode": mode, **o,
+                             "ms_per_iter": max_over_ranks(v["ms"]),
+                             "res_calc_gbs": v["loops"].get("res_calc", {}).get("gbs"),
+                             "launches_per_iter": v["launches"] / 20})
         # gather kernels of inc_mode 3, and the pipelined direct loop's switches
         for o in ({"gather_kernel": 1}, {"gather_kernel": 3}, {"gather_kernel": 4},
                   {"gather_kernel": 5, "pipe_block": 128}, {"gather_kernel": 5, "pipe_block": 256},
                   {"gather_kernel": 6, "pipe_block": 128}, {"gather_kernel": 6, "pipe_block": 256},
+                  {"gather_kernel": 7}, {"gather_kernel": 7, "fuse": 0},
                   {"gather_kernel": 6, "pipe_block": 256, "bres_kernel": 0},
                   {"lazy_res": 0}, {"speculate_res": 0, "lazy_res": 0},
                   {"rename_save": 0, "speculate_res": 0, "lazy_res": 0},
@@ -425,6 +438,25 @@ def main():
                              "loops": {n: {"us": round(1e3 * x["avg_ms"], 2),
                                            "gbs": round(x["gbs"])}
                                        for n, x in lp.items()}})
+
+    # ---------------------------------------------------------- plan construction
+    plans = []
+    if not args.no_variants:
+        for numbering in ("rcm", "random"):
+            for mode, label in ((2, "greedy (reference order)"), (1, "jones-plassmann")):
+                L.op_init()
+                L.set_option("plan_mode", mode)
+                app = Airfoil(m, dtype=dtype)
+                if numbering == "rcm":
+                    app.renumber()
+                p = L.op_plan_get_stage("res_calc", app.edges, args.part_size, app.a_res,
+                                        [0, 0, 1, 1, 2, 2, 3, 3], 2)
+                n_bad, _ = L.plan_validate(p)
+                plans.append({"loop": "res_calc", "numbering": numbering, "colouring": label,
+                              "build_ms": round(L.load().op2b_plan_build_ms(p), 2),
+                              "blocks": p.contents.nblocks, "block_colours": p.contents.ncolors,
+                              "conflicts": n_bad})
+                L.op_exit()
 
     # ---------------------------------------------------------- end to end through the API
     e2e = None
@@ -563,6 +595,7 @@ def main():
             "renumber": main_run["renumber"],
             "rms_final": main_run["rms"],
             "variants": variants,
+            "plans": plans,
             "cpu_baseline": cpu,
             "cpu_other_numbering": cpu_other,
             "parity": parity,

@@ -373,11 +373,15 @@ struct SlotCache {
   op_map inc = nullptr, nodes = nullptr;
   SlotRecords rec{};
   bool corners_tried = false;
+  int ring_state = 0;       // flux-ring records: 0 not tried, 1 built, -1 not possible
+  int ring_ctas = 0, ring_nt = 0;
+  uint2 *ring_buf = nullptr;
   op_map linked = nullptr;  // pbecell whose boundary records are linked in (fused bres_calc)
   int link_state = 0;       // 0 not tried, 1 linked, -1 not linkable
   std::vector<void *> owned;
   ~SlotCache() {
     for (void *p : owned) cudaFree(p);
+    cudaFree(ring_buf);
   }
 };
 
@@ -615,6 +619,139 @@ bool link_boundary_records(const SlotRecords *rec, const BresRecords *b, op_map 
   if (!cuda_ok(cudaStreamSynchronize(s), "boundary link")) return false;
   sc->link_state = 1;
   sc->linked = pbecell;
+  return true;
+}
+
+// ------------------------------------------------------------------ flux-ring records
+
+// the range [rs, re) of cell c: ranges of `span` cells
+__device__ __forceinline__ void ring_range(int c, int span, int ncell, int &rs, int &re) {
+  rs = (c / span) * span;
+  re = min(rs + span, ncell);
+}
+
+// a slot's flux is computed by its cell unless the other cell is earlier in
+// the same range (then that cell computed it)
+__device__ __forceinline__ bool ring_consumes(int c, int nb, int rs, int re) {
+  return nb >= rs && nb < re && nb < c;
+}
+
+// fluxes each cell computes
+__global__ void k_ring_count(int ncell, int span, const int4 *rec_o, const unsigned *meta,
+                             int *cnt) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  int rs, re;
+  ring_range(c, span, ncell, rs, re);
+  const int4 o4 = rec_o[c];
+  const int o[4] = {o4.x, o4.y, o4.z, o4.w};
+  const unsigned m = meta[c];
+  int n = 0;
+  for (int s = 0; s < 4; s++)
+    if ((m >> (8 * s)) & 1u) n += ring_consumes(c, o[s], rs, re) ? 0 : 1;
+  cnt[c] = n;
+}
+
+// ring entries: the k-th flux computed in a range (in cell order, slot order
+// within a cell) goes to entry k mod OP2B_RING_ENTRIES; a consumer finds the
+// entry of the producer's slot that names it.  *bad: a consumed flux whose
+// entry is reused before the consumer's tile has read it, or an edge shared
+// twice by one pair of cells.
+__global__ void k_ring_fill(int ncell, int span, int nt, const int4 *rec_o, const unsigned *meta,
+                            const long long *pre, uint2 *ring, int *bad) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  int rs, re;
+  ring_range(c, span, ncell, rs, re);
+  const long long base = pre[rs];
+  const int4 o4 = rec_o[c];
+  const int o[4] = {o4.x, o4.y, o4.z, o4.w};
+  const unsigned m = meta[c];
+  unsigned f[4] = {0u, 0u, 0u, 0u};
+  int rank = 0;
+  for (int s = 0; s < 4; s++) {
+    if (!((m >> (8 * s)) & 1u)) continue;
+    const int nb = o[s];
+    if (!ring_consumes(c, nb, rs, re)) {
+      const long long k = pre[c] - base + rank++;
+      f[s] = (unsigned)(k & (OP2B_RING_ENTRIES - 1));
+      continue;
+    }
+    const int4 p4 = rec_o[nb];
+    const int po[4] = {p4.x, p4.y, p4.z, p4.w};
+    const unsigned pm = meta[nb];
+    int prank = 0, found = -1, hits = 0;
+    for (int t = 0; t < 4; t++) {
+      if (!((pm >> (8 * t)) & 1u)) continue;
+      if (po[t] == c) {
+        hits++;
+        found = prank;
+      }
+      if (!ring_consumes(nb, po[t], rs, re)) prank++;
+    }
+    const long long k = pre[nb] - base + found;
+    const int tile = (c - rs) / nt;
+    const int tend = min(rs + (tile + 1) * nt, re);
+    const long long pend = pre[tend] - base;  // fluxes computed up to the end of c's tile
+    if (hits != 1 || pend - k > OP2B_RING_ENTRIES) atomicOr(bad, 1);
+    f[s] = 0x8000u | (unsigned)(k & (OP2B_RING_ENTRIES - 1));
+  }
+  ring[c] = make_uint2(f[0] | (f[1] << 16), f[2] | (f[3] << 16));
+}
+
+bool build_ring_records(const SlotRecords *rec, int nctas, int nt) {
+  SlotCache *sc = nullptr;
+  for (auto &p : slot_cache())
+    if (&p->rec == rec) sc = p.get();
+  if (!sc || !rec->corners || nctas <= 0 || nt <= 0) return false;
+  if (sc->ring_state != 0 && sc->ring_ctas == nctas && sc->ring_nt == nt)
+    return sc->ring_state == 1;
+  sc->ring_state = -1;
+  sc->ring_ctas = nctas;
+  sc->ring_nt = nt;
+  sc->rec.ring = nullptr;
+  const int n = rec->ncell;
+  if (n <= 0) return false;
+  Runtime &r = rt();
+  cudaStream_t s = r.stream;
+  const int span = (int)(((long long)n + nctas - 1) / nctas);
+  int *cnt = nullptr, *bad = nullptr;
+  long long *pre = nullptr;
+  if (!sc->ring_buf && cudaMalloc(&sc->ring_buf, sizeof(uint2) * (size_t)n) != cudaSuccess) {
+    sc->ring_buf = nullptr;
+    cudaGetLastError();
+    return false;
+  }
+  if (cudaMallocAsync(&cnt, sizeof(int) * (size_t)n, s) != cudaSuccess ||
+      cudaMallocAsync(&pre, sizeof(long long) * ((size_t)n + 1), s) != cudaSuccess ||
+      cudaMallocAsync(&bad, sizeof(int), s) != cudaSuccess) {
+    cudaGetLastError();
+    if (cnt) cudaFreeAsync(cnt, s);
+    if (pre) cudaFreeAsync(pre, s);
+    return false;
+  }
+  const unsigned g = (unsigned)((n + 255) / 256);
+  cudaMemsetAsync(bad, 0, sizeof(int), s);
+  k_ring_count<<<g, 256, 0, s>>>(n, span, reinterpret_cast<const int4 *>(rec->o), rec->meta, cnt);
+  r.launches++;
+  bool ok = scan_exclusive(cnt, pre, n, s);
+  if (ok) {
+    k_ring_fill<<<g, 256, 0, s>>>(n, span, nt, reinterpret_cast<const int4 *>(rec->o), rec->meta,
+                                  pre, sc->ring_buf, bad);
+    r.launches++;
+  }
+  int h_bad = 1;
+  cudaMemcpyAsync(&h_bad, bad, sizeof(int), cudaMemcpyDeviceToHost, s);
+  cudaFreeAsync(cnt, s);
+  cudaFreeAsync(pre, s);
+  cudaFreeAsync(bad, s);
+  ok = cuda_ok(cudaStreamSynchronize(s), "flux-ring records") && ok;
+  if (!ok || h_bad) return false;
+  sc->ring_state = 1;
+  sc->rec.ring = sc->ring_buf;
+  sc->rec.ring_ctas = nctas;
+  sc->rec.ring_span = span;
+  sc->rec.ring_nt = nt;
   return true;
 }
 

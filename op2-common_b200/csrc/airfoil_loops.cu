@@ -190,14 +190,76 @@ k_res_calc_atomic(int nedge, const int2 *__restrict__ pedge, const int2 *__restr
   }
 }
 
+// Segmented atomics: a warp's 32 edges first combine their increments to the
+// same cell, then one lane of each group issues the atomics.  Each side (the
+// +f into c1 and the -f into c2) is grouped by __match_any_sync on the cell
+// index; the group's lowest lane sums the members' fluxes from shared memory
+// in lane (edge) order and adds the sum with one atomic per component.  On a
+// renumbered mesh edges are sorted by their first cell, so most cells are c1
+// of two edges of one warp, and the two edges that reach a cell as c2 lie in
+// neighbouring segments: the atomics roughly halve.  Results differ from the
+// per-edge atomics only by rounding (the increments are grouped differently).
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT)
+k_res_calc_atomic_seg(int nedge, const int2 *__restrict__ pedge, const int2 *__restrict__ pecell,
+                      const T *__restrict__ x, const T *__restrict__ q,
+                      const T *__restrict__ adt, T *__restrict__ res, AirConst<T> k) {
+  __shared__ T sf[NT / 32][4][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int stride = gridDim.x * NT;
+  // the loop bound is the same for the 32 lanes (warps start at multiples of
+  // 32 and the stride is one), so every lane reaches each __match_any_sync
+  for (int base = blockIdx.x * NT + w * 32; base < nedge; base += stride) {
+    const int e = base + lane;
+    const bool valid = e < nedge;
+    int2 cc = make_int2(-1 - lane, -33 - lane);  // distinct keys: no group for idle lanes
+    T f[4] = {(T)0, (T)0, (T)0, (T)0};
+    if (valid) {
+      int2 nn = __ldg(pedge + e);
+      cc = __ldg(pecell + e);
+      T x1x, x1y, x2x, x2y, q1[4], q2[4];
+      Vec<T>::ld2(x + 2 * (size_t)nn.x, x1x, x1y);
+      Vec<T>::ld2(x + 2 * (size_t)nn.y, x2x, x2y);
+      Vec<T>::ld4(q + 4 * (size_t)cc.x, q1);
+      Vec<T>::ld4(q + 4 * (size_t)cc.y, q2);
+      air_flux<T>(x1x, x1y, x2x, x2y, q1, q2, __ldg(adt + cc.x), __ldg(adt + cc.y), k, f);
+    }
+#pragma unroll
+    for (int m = 0; m < 4; m++) sf[w][m][lane] = f[m];
+    __syncwarp();
+#pragma unroll
+    for (int side = 0; side < 2; side++) {
+      const int cell = side == 0 ? cc.x : cc.y;
+      const unsigned g = __match_any_sync(0xffffffffu, cell);
+      if (valid && lane == __ffs(g) - 1) {
+        T acc[4] = {sf[w][0][lane], sf[w][1][lane], sf[w][2][lane], sf[w][3][lane]};
+        for (unsigned rest = g & (g - 1); rest; rest &= rest - 1) {
+          const int src = __ffs(rest) - 1;
+#pragma unroll
+          for (int m = 0; m < 4; m++) acc[m] += sf[w][m][src];
+        }
+        T *r = res + 4 * (size_t)cell;
+#pragma unroll
+        for (int m = 0; m < 4; m++) red_add(r + m, side == 0 ? acc[m] : -acc[m]);
+      }
+    }
+    __syncwarp();
+  }
+}
+
 template <typename T>
 cudaError_t launch_res_calc_atomic(const LaunchCtx &c, int nedge, const int *pedge,
                                    const int *pecell, const T *x, const T *q, const T *adt,
-                                   T *res, const AirConst<T> &k) {
+                                   T *res, const AirConst<T> &k, bool segmented) {
   if (nedge <= 0) return cudaSuccess;
-  k_res_calc_atomic<T><<<grid_for(c, nedge, 256, 8), 256, 0, c.stream>>>(
-      nedge, reinterpret_cast<const int2 *>(pedge), reinterpret_cast<const int2 *>(pecell), x,
-      q, adt, res, k);
+  if (segmented)
+    k_res_calc_atomic_seg<T, 256><<<grid_for(c, nedge, 256, 8), 256, 0, c.stream>>>(
+        nedge, reinterpret_cast<const int2 *>(pedge), reinterpret_cast<const int2 *>(pecell), x,
+        q, adt, res, k);
+  else
+    k_res_calc_atomic<T><<<grid_for(c, nedge, 256, 8), 256, 0, c.stream>>>(
+        nedge, reinterpret_cast<const int2 *>(pedge), reinterpret_cast<const int2 *>(pecell), x,
+        q, adt, res, k);
   c.count();
   return cudaGetLastError();
 }
@@ -424,11 +486,11 @@ template cudaError_t launch_adt_save<float>(const LaunchCtx &, int, const int *,
 template cudaError_t launch_res_calc_atomic<double>(const LaunchCtx &, int, const int *,
                                                     const int *, const double *, const double *,
                                                     const double *, double *,
-                                                    const AirConst<double> &);
+                                                    const AirConst<double> &, bool);
 template cudaError_t launch_res_calc_atomic<float>(const LaunchCtx &, int, const int *,
                                                    const int *, const float *, const float *,
                                                    const float *, float *,
-                                                   const AirConst<float> &);
+                                                   const AirConst<float> &, bool);
 template cudaError_t launch_bres_calc_atomic<double>(const LaunchCtx &, int, const int *,
                                                      const int *, const int *, const double *,
                                                      const double *, const double *, double *,

@@ -186,12 +186,14 @@ k_bres_colour(BresPlanDev P, int blk_first, int nbedge, const int2 *__restrict__
 
 Plan *get_res_plan(const char *name, op_set set, int nargs, op_arg *args) {
   int inds[8] = {0, 0, 1, 1, 2, 2, 3, 3};
-  return build_plan(name, set, rt().opt_part_size, nargs, args, 4, inds, OP_STAGE_ALL);
+  return build_plan(name, set, rt().opt_part_size, nargs, args, 4, inds, OP_STAGE_ALL,
+                    rt().opt_plan_mode == 1 ? OP2B_COLOUR_JP : OP2B_COLOUR_GREEDY);
 }
 
 Plan *get_bres_plan(const char *name, op_set set, int nargs, op_arg *args) {
   int inds[6] = {0, 0, 1, 2, 3, -1};
-  return build_plan(name, set, rt().opt_part_size, nargs, args, 4, inds, OP_STAGE_ALL);
+  return build_plan(name, set, rt().opt_part_size, nargs, args, 4, inds, OP_STAGE_ALL,
+                    rt().opt_plan_mode == 1 ? OP2B_COLOUR_JP : OP2B_COLOUR_GREEDY);
 }
 
 template <typename T, int EPT, bool HYBRID>
@@ -226,7 +228,8 @@ template <typename T>
 cudaError_t run_res_calc(const LaunchCtx &c, const ResCalcArgs<T> &a, Plan *plan, int mode) {
   if (a.nedge <= 0) return cudaSuccess;
   if (mode == OP2B_INC_ATOMIC || !plan)
-    return launch_res_calc_atomic<T>(c, a.nedge, a.pedge, a.pecell, a.x, a.q, a.adt, a.res, a.k);
+    return launch_res_calc_atomic<T>(c, a.nedge, a.pedge, a.pecell, a.x, a.q, a.adt, a.res, a.k,
+                                     rt().opt_atomic_seg != 0);
   const Plan &pl = *plan;
   ResPlanDev d{};
   d.bsize = pl.bsize;

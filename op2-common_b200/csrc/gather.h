@@ -39,7 +39,19 @@ struct SlotRecords {
   const int *cn;
   const unsigned *meta;
   bool corners;
+  // Flux-ring form (built on request by build_ring_records, for the fused
+  // res_calc + bres_calc and res_calc over corner records): cells are split
+  // into ring_ctas contiguous ranges of ring_span cells, one per CTA, swept in
+  // tiles of ring_nt cells.  16 bits per slot in ring[c] (slots 0-1 in .x,
+  // 2-3 in .y, low half first): bit 15 clear = the cell computes the edge's
+  // flux (its other cell comes later in the range, or lies outside it) and
+  // puts it at entry (bits 0-11) of the CTA's shared-memory ring; bit 15 set
+  // = the flux was put there by the other cell, earlier in the range.
+  const uint2 *ring;
+  int ring_ctas, ring_span, ring_nt;
 };
+// entries of a CTA's flux ring (a power of two: the 12-bit index of ring[])
+#define OP2B_RING_ENTRIES 4096
 const SlotRecords *get_slot_records(op_map pecell, op_map pedge);
 const SlotRecords *get_corner_records(op_map pecell, op_map pedge);
 void release_slot_records();
@@ -64,6 +76,13 @@ cudaError_t launch_res_calc_gather_regpipe(const LaunchCtx &c, const SlotRecords
                                            const T *q, const T *adt, T *res,
                                            const AirConst<T> &k, int block);
 
+// Build the flux-ring records for nctas ranges and tiles of nt cells; false
+// (the corner kernels then serve) when the corner records are missing, two
+// cells share more than one edge, or some flux would have to wait in the
+// ring longer than OP2B_RING_ENTRIES allows (cells' neighbours too far apart
+// in the numbering: renumbering the mesh brings them close).  Cached.
+bool build_ring_records(const SlotRecords *s, int nctas, int nt);
+
 // which gather kernel res_calc uses (option "gather_kernel")
 #define OP2B_GATHER_CSR 1    // one thread per cell walking the inverse map
 #define OP2B_GATHER_LANES 2  // four threads per cell, shuffled together
@@ -71,6 +90,7 @@ cudaError_t launch_res_calc_gather_regpipe(const LaunchCtx &c, const SlotRecords
 #define OP2B_GATHER_PIPE 4   // cell4's order, shared-memory software pipeline
 #define OP2B_GATHER_REGPIPE 5  // cell4's order, register software pipeline
 #define OP2B_GATHER_CORNER 6   // the register pipeline over corner records
+#define OP2B_GATHER_RING 7     // corner records, each in-range flux computed once (flux ring)
 
 // airfoil_pipe.cu: the register pipeline over corner records (four node
 // gathers per cell instead of eight); block 64, 128 or 256 threads, minb the
@@ -109,6 +129,12 @@ cudaError_t launch_res_bres_corner(const LaunchCtx &c, const SlotRecords &s,
                                    const BresRecords &b, const int *bound, const T *x,
                                    const T *q, const T *adt, T *res, const AirConst<T> &k,
                                    int block, bool zero_res = false);
+// airfoil_ring.cu: res_calc (bound = nullptr) or the fused res_calc +
+// bres_calc over the flux-ring records (s.ring set; one CTA per range)
+template <typename T>
+cudaError_t launch_res_ring(const LaunchCtx &c, const SlotRecords &s, const int *bound,
+                            const T *x, const T *q, const T *adt, T *res, const AirConst<T> &k,
+                            bool zero_res);
 
 template <typename T>
 cudaError_t launch_res_calc_gather(const LaunchCtx &c, const InvMap &inv, const int *pedge,

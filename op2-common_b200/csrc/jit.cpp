@@ -538,9 +538,13 @@ const Plan *colour_plan(const char *name, op_set set, int nargs, const op_arg *a
       inds.push_back(ind);
     }
   }
+  // colours by parallel rounds (no reference integers to match here) unless
+  // plan_mode 2 asks for the serial greedy walk
   const std::string pname = std::string(name) + "#coloured";
-  op_plan *o = op_plan_get_stage(pname.c_str(), set, 0, (int)pa.size(), pa.data(),
-                                 (int)seen.size(), inds.data(), OP_COLOR2);
+  Plan *bp = build_plan(pname.c_str(), set, 0, (int)pa.size(), pa.data(), (int)seen.size(),
+                        inds.data(), OP_COLOR2,
+                        rt().opt_plan_mode == 2 ? OP2B_COLOUR_GREEDY : OP2B_COLOUR_JP);
+  op_plan *o = bp ? &bp->pub : nullptr;
   const Plan *pl = o ? find_plan(o) : nullptr;
   if (!pl || !pl->col_reord_d || !o->color2_offsets) {
     if (op2b_last_error()[0] == 0) set_error("op_par_loop(%s): colouring the loop failed", name);

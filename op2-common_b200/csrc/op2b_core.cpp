@@ -207,7 +207,7 @@ void Runtime::end_loop(double bytes) {
   s.bytes_per_call = bytes;
   if (!opt_timing) return;
   cudaEventRecord(cur_ev1, stream);
-  pending.push_back(PendingTime{cur_loop, cur_ev0, cur_ev1});
+  pending.push_back(PendingTime{cur_loop, cur_ev0, cur_ev1, profile_loop_node(cur_loop)});
   if (pending.size() > 4096) resolve_timing();
 }
 
@@ -217,10 +217,13 @@ void Runtime::resolve_timing() {
   for (auto &p : pending) {
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, p.e0, p.e1) == cudaSuccess) {
-      LoopStat &s = stats[p.name];
-      s.total_ms += ms;
-      s.last_ms = ms;
-      s.timed++;
+      if (!p.name.empty()) {
+        LoopStat &s = stats[p.name];
+        s.total_ms += ms;
+        s.last_ms = ms;
+        s.timed++;
+      }
+      if (p.node >= 0) profile_submit(p.node, ms);
     }
     ev_free.push_back(p.e0);
     ev_free.push_back(p.e1);
@@ -354,6 +357,8 @@ void op_exit(void) {
   r.const_types.clear();
   release_jit();
   r.map_ptrs.clear();
+  r.resolve_timing();  // the loop table and the profiler keep their last times
+  profile_on_exit();
   for (auto &p : r.pending) {
     cudaEventDestroy(p.e0);
     cudaEventDestroy(p.e1);
@@ -416,6 +421,8 @@ void op_exit(void) {
   r.opt_pipe_block = d.opt_pipe_block;
   r.opt_pipe_hints = d.opt_pipe_hints;
   r.opt_plan_mode = d.opt_plan_mode;
+  r.opt_atomic_seg = d.opt_atomic_seg;
+  r.ring_used = 0;
   r.opt_check_plans = d.opt_check_plans;
 }
 
@@ -1007,12 +1014,18 @@ int op2b_set_option(const char *key, long value) {
   } else if (k == "block_size") {
     r.opt_block_size = (int)value;
   } else if (k == "plan_mode") {
+    if (value < 0 || value > 2) {
+      set_error("op2b_set_option: plan_mode must be 0, 1 or 2");
+      return -1;
+    }
     r.opt_plan_mode = (int)value;
+  } else if (k == "atomic_segmented") {
+    r.opt_atomic_seg = value != 0;
   } else if (k == "gather_kernel") {
-    if (value < 1 || value > 6) {
+    if (value < 1 || value > 7) {
       set_error("op2b_set_option: gather_kernel must be 1 (csr), 2 (lanes), 3 (cell4), 4 "
-                "(shared-memory pipeline), 5 (register pipeline) or 6 (register pipeline "
-                "over corner records)");
+                "(shared-memory pipeline), 5 (register pipeline), 6 (register pipeline "
+                "over corner records) or 7 (corner records, each flux computed once)");
       return -1;
     }
     r.opt_gather_kernel = (int)value;
@@ -1075,6 +1088,8 @@ long op2b_get_option(const char *key) {
   if (k == "part_size") return r.opt_part_size;
   if (k == "block_size") return r.opt_block_size;
   if (k == "plan_mode") return r.opt_plan_mode;
+  if (k == "atomic_segmented") return r.opt_atomic_seg;
+  if (k == "ring_used") return r.ring_used;  // read-only
   if (k == "gather_kernel") return r.opt_gather_kernel;
   if (k == "pipe_block") return r.opt_pipe_block;
   if (k == "pipe_hints") return r.opt_pipe_hints;

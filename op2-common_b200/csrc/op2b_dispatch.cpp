@@ -218,6 +218,19 @@ bool consts_are(const AirConst<double> &kd, const AirConst<float> &kf, int rb) {
   return ok && memcmp(&k, &kf, sizeof(k)) == 0;
 }
 
+// res_calc and the bres_calc after it in one launch: over the flux-ring
+// records (each in-range flux computed once) when gather_kernel 7 asks for it
+// and the numbering allows it, else the corner kernel
+template <typename T>
+static cudaError_t launch_fused_pair(Runtime &r, const SlotRecords &cr, const BresRecords &br,
+                                     const int *bound, const T *x, const T *q, const T *adt,
+                                     T *res, const AirConst<T> &k, bool zero) {
+  r.ring_used = r.opt_gather_kernel == OP2B_GATHER_RING && build_ring_records(&cr, r.nsm, 256);
+  if (r.ring_used) return launch_res_ring<T>(r.ctx(), cr, bound, x, q, adt, res, k, zero);
+  return launch_res_bres_corner<T>(r.ctx(), cr, br, bound, x, q, adt, res, k, r.opt_pipe_block,
+                                   zero);
+}
+
 // the update's call launches the res_calc + bres_calc pair learned last
 // (ResLearn) right behind it, on the arrays it leaves: q, adt (the next
 // adt_calc's, computed ahead) and res (zero)
@@ -247,13 +260,13 @@ void launch_speculative_res(Runtime &r, const op_arg *a, int rb) {
   r.begin_loop("res_calc+bres_calc");
   // adt: the next adt_calc's result, still in the second array
   if (rb == 8)
-    e = launch_res_bres_corner<double>(r.ctx(), *cr, *br, bound, (const double *)L.x->data_d,
-                                       (const double *)L.q->data_d, (const double *)sp.shadow,
-                                       (double *)L.res->data_d, L.kd, r.opt_pipe_block, zero);
+    e = launch_fused_pair<double>(r, *cr, *br, bound, (const double *)L.x->data_d,
+                                  (const double *)L.q->data_d, (const double *)sp.shadow,
+                                  (double *)L.res->data_d, L.kd, zero);
   else
-    e = launch_res_bres_corner<float>(r.ctx(), *cr, *br, bound, (const float *)L.x->data_d,
-                                      (const float *)L.q->data_d, (const float *)sp.shadow,
-                                      (float *)L.res->data_d, L.kf, r.opt_pipe_block, zero);
+    e = launch_fused_pair<float>(r, *cr, *br, bound, (const float *)L.x->data_d,
+                                 (const float *)L.q->data_d, (const float *)sp.shadow,
+                                 (float *)L.res->data_d, L.kf, zero);
   r.end_loop(L.fused_bytes - (zero ? L.res_read_bytes : 0.0));
   if (e == cudaSuccess) r.sres_stage = 1;
   else cudaGetLastError();  // not launched: the program's calls run as usual
@@ -400,6 +413,15 @@ template <typename T>
 static cudaError_t res_gather_slots(Runtime &r, const SlotRecords &s, const ResCalcArgs<T> &p,
                                     const AirConst<T> &k) {
   switch (r.opt_gather_kernel) {
+    case OP2B_GATHER_RING:
+      r.ring_used = s.corners && build_ring_records(&s, r.nsm, 256);
+      if (r.ring_used)
+        return launch_res_ring<T>(r.ctx(), s, nullptr, p.x, p.q, p.adt, p.res, k, false);
+      if (s.corners)  // neighbours too far apart in the numbering for the ring
+        return launch_res_calc_gather_corner<T>(r.ctx(), s, p.x, p.q, p.adt, p.res, k,
+                                                r.opt_pipe_block, r.opt_gather_minb);
+      return launch_res_calc_gather_regpipe<T>(r.ctx(), s, p.x, p.q, p.adt, p.res, k,
+                                               r.opt_pipe_block);
     case OP2B_GATHER_LANES:
       return launch_res_calc_gather4<T>(r.ctx(), s, p.x, p.q, p.adt, p.res, k);
     case OP2B_GATHER_PIPE:
@@ -598,18 +620,14 @@ int loop_bres_calc(const char *name, op_set set, int nargs, op_arg *a) {
       cudaError_t e;
       r.begin_loop("res_calc+bres_calc");
       if (rb == 8)
-        e = launch_res_bres_corner<double>(r.ctx(), *cr, *br, bound,
-                                           (const double *)pd.x->data_d,
-                                           (const double *)pd.q->data_d,
-                                           (const double *)pd.adt->data_d,
-                                           (double *)pd.res->data_d, pd.kd, r.opt_pipe_block,
-                                           zero);
+        e = launch_fused_pair<double>(r, *cr, *br, bound, (const double *)pd.x->data_d,
+                                      (const double *)pd.q->data_d,
+                                      (const double *)pd.adt->data_d, (double *)pd.res->data_d,
+                                      pd.kd, zero);
       else
-        e = launch_res_bres_corner<float>(r.ctx(), *cr, *br, bound,
-                                          (const float *)pd.x->data_d,
-                                          (const float *)pd.q->data_d,
-                                          (const float *)pd.adt->data_d,
-                                          (float *)pd.res->data_d, pd.kf, r.opt_pipe_block, zero);
+        e = launch_fused_pair<float>(r, *cr, *br, bound, (const float *)pd.x->data_d,
+                                     (const float *)pd.q->data_d, (const float *)pd.adt->data_d,
+                                     (float *)pd.res->data_d, pd.kf, zero);
       r.end_loop(fused - (zero ? res_read : 0.0));
       if (zero && e == cudaSuccess) r.res_zero = nullptr;  // every element rewritten
       if (e == cudaSuccess) {  // the pair the next update may launch ahead

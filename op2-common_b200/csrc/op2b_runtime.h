@@ -24,8 +24,9 @@ struct LoopStat {
 };
 
 struct PendingTime {
-  std::string name;
+  std::string name;     // the loop whose statistics take the time ("" for none)
   cudaEvent_t e0, e1;
+  int node = -1;        // the profiler's region or kernel node that takes it too
 };
 
 struct Plan;  // plan.h
@@ -123,7 +124,12 @@ struct Runtime {
   int opt_host_threads = 8;   // threads of a large host copy (host copies of maps and dats)
   int opt_pipe_block = 256;   // threads per CTA of the pipelined gather (64, 96, 128, 256)
   int opt_pipe_hints = 0;     // register pipeline: evict-first hints on once-read streams
-  int opt_plan_mode = 0;      // 0 = parallel block colouring, 1 = serial greedy (bit-exact)
+  int opt_plan_mode = 0;      // colouring: 0 = serial greedy for op_plan_get and the plan-
+                              // driven loops (bit-exact), Jones-Plassmann for the run-time
+                              // compiled loops' colourings; 1 = Jones-Plassmann for every
+                              // plan; 2 = serial greedy for every plan
+  int opt_atomic_seg = 1;     // inc_mode 0: 1 = segmented (warp-combined) atomics, 0 = per edge
+  int ring_used = 0;          // the last res_calc launch ran over the flux-ring records
   bool opt_check_plans = false;
   bool quiet_errors = false;  // set_error records without printing or aborting
 
@@ -189,6 +195,12 @@ struct Runtime {
 };
 
 Runtime &rt();
+// region profiler (profile.cpp): a resolved time for node `id`; the kernel
+// node a loop starting now is timed into (-1 = none); op_exit's clean-up
+void profile_submit(int id, float ms);
+int profile_loop_node(const std::string &loop);
+void profile_on_exit();
+
 void set_error(const char *fmt, ...);
 bool cuda_ok(cudaError_t e, const char *what);
 // Device -> pageable host copy on the library stream, through pinned buffers

@@ -57,6 +57,7 @@ struct PlanParams {
   int incrw_loc_off[PLAN_MAX_ARGS];// offset of an INC/RW arg's local indices in smem
   int buf_len;                     // power of two >= max gathered values of one indirection
   int work_len, loc_len;
+  int jp;                          // Jones-Plassmann colouring instead of the serial greedy
 };
 
 // ------------------------------------------------------------------ helpers
@@ -161,6 +162,213 @@ __global__ void k_plan_count(PlanParams p, int *counts) {
   }
 }
 
+// ------------------------------------------------------------------ Jones-Plassmann
+// Parallel colouring, the alternative to the reference's serial greedy order
+// (which the default plans keep, bit-exact).  Each round, every uncoloured
+// element (or block) that holds the highest priority among the uncoloured
+// ones sharing any of its OP_INC/OP_RW targets takes the lowest colour its
+// already-coloured neighbours leave free; two winners of a round never share
+// a target, so a round's choices cannot conflict.  Priorities are a hash of
+// the index with the index as tie-break (unique, deterministic: the colouring
+// is the same on every run).  Colours come 32 at a time, as in the greedy
+// passes: a candidate whose neighbours hold all 32 colours of the pass waits
+// for the next pass.  The result is checked like any plan by
+// op2b_plan_validate (no two elements of a colour share a target).
+
+__device__ __forceinline__ unsigned jp_hash(unsigned x) {
+  // an integer mixing function (xorshift-multiply rounds)
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+
+__device__ __forceinline__ unsigned long long jp_prio(long long i) {
+  return ((unsigned long long)jp_hash((unsigned)i ^ (unsigned)(i >> 32)) << 32) |
+         (unsigned long long)(unsigned)(i + 1);
+}
+
+// thread colours of one block by CTA-parallel Jones-Plassmann in shared
+// memory: work[] the colour masks of the block's local targets, tmax[] (as
+// many ints) the round's highest priority per local target; up to 16
+// elements per thread (blocks of at most 4096 elements)
+__device__ void jp_thread_colours(const PlanParams &p, int b, int beg, int n, unsigned *work,
+                                  const short *loc, int *tmax, int *thrcol, int *nthrcol) {
+  __shared__ int s_ncolors;
+  const int T = blockDim.x;
+  for (int i = threadIdx.x; i < n; i += T) thrcol[beg + i] = -1;
+  if (threadIdx.x == 0) s_ncolors = 0;
+  // priorities below 2^31 (21 hash bits above the 12 index bits), unique in the block
+  auto prio = [&](int i) { return (int)(((jp_hash((unsigned)(beg + i)) & 0x7ffffu) << 12) | i); };
+  int base = 0;
+  unsigned blocked = 0;  // per thread: bit k = its k-th element waits for the next pass
+  for (;;) {
+    for (int t = threadIdx.x; t < p.work_len; t += T) work[t] = 0u;
+    blocked = 0;
+    __syncthreads();
+    for (;;) {
+      for (int t = threadIdx.x; t < p.work_len; t += T) tmax[t] = -1;
+      __syncthreads();
+      for (int i = threadIdx.x, k = 0; i < n; i += T, k++) {
+        if (thrcol[beg + i] != -1 || (blocked >> k & 1u)) continue;
+        const int pr = prio(i);
+        for (int a = 0; a < p.nargs; a++)
+          if (p.incrw[a]) atomicMax(&tmax[p.ind_work_off[p.ind[a]] + loc[p.incrw_loc_off[a] + i]], pr);
+      }
+      __syncthreads();
+      int active = 0;
+      for (int i = threadIdx.x, k = 0; i < n; i += T, k++) {
+        if (thrcol[beg + i] != -1 || (blocked >> k & 1u)) continue;
+        const int pr = prio(i);
+        bool win = true;
+        unsigned mask = 0;
+        for (int a = 0; a < p.nargs; a++)
+          if (p.incrw[a]) {
+            const int t = p.ind_work_off[p.ind[a]] + loc[p.incrw_loc_off[a] + i];
+            win &= tmax[t] == pr;
+            mask |= work[t];
+          }
+        if (!win) {
+          active = 1;
+          continue;
+        }
+        const int c = __ffs(~mask) - 1;
+        if (c < 0) {
+          blocked |= 1u << k;
+          continue;
+        }
+        thrcol[beg + i] = base + c;
+        atomicMax(&s_ncolors, base + c + 1);
+        for (int a = 0; a < p.nargs; a++)
+          if (p.incrw[a])
+            atomicOr(&work[p.ind_work_off[p.ind[a]] + loc[p.incrw_loc_off[a] + i]], 1u << c);
+      }
+      if (!__syncthreads_or(active)) break;
+    }
+    if (!__syncthreads_or(blocked != 0)) break;
+    base += 32;
+  }
+  if (threadIdx.x == 0) nthrcol[b] = s_ncolors;
+}
+
+// device-wide rounds over blocks (CTA b stands for plan block b) or over
+// single elements (OP_COLOR2): the round's highest priority per target ...
+__global__ void k_jp_block_max(PlanParams p, unsigned long long *const *tmax, const int *col,
+                               const unsigned char *blocked) {
+  const int b = blockIdx.x;
+  if (col[b] != -1 || blocked[b]) return;
+  int beg, n;
+  block_range(p, b, beg, n);
+  const unsigned long long pr = jp_prio(b);
+  for (int a = 0; a < p.nargs; a++) {
+    if (!p.incrw[a]) continue;
+    unsigned long long *tm = tmax[p.ind[a]];
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+      atomicMax(&tm[p.map[a][p.idx[a] + (size_t)(beg + i) * p.mdim[a]]], pr);
+  }
+}
+
+// ... then each winner's colour; *active counts the candidates left waiting,
+// *nblocked those that found the pass's 32 colours taken
+__global__ void k_jp_block_win(PlanParams p, unsigned long long *const *tmax, unsigned *const *work,
+                               int *col, unsigned char *blocked, int base, int *active,
+                               int *nblocked, int *ncolors) {
+  __shared__ unsigned s_or[32];
+  const int b = blockIdx.x;
+  if (col[b] != -1 || blocked[b]) return;
+  int beg, n;
+  block_range(p, b, beg, n);
+  const unsigned long long pr = jp_prio(b);
+  int lose = 0;
+  unsigned mask = 0;
+  for (int a = 0; a < p.nargs; a++) {
+    if (!p.incrw[a]) continue;
+    const unsigned long long *tm = tmax[p.ind[a]];
+    const unsigned *w = work[p.ind[a]];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const int t = p.map[a][p.idx[a] + (size_t)(beg + i) * p.mdim[a]];
+      lose |= tm[t] != pr;
+      mask |= w[t];
+    }
+  }
+  if (__syncthreads_or(lose)) {
+    if (threadIdx.x == 0) atomicAdd(active, 1);
+    return;
+  }
+  mask = __reduce_or_sync(0xffffffffu, mask);
+  if ((threadIdx.x & 31) == 0) s_or[threadIdx.x >> 5] = mask;
+  __syncthreads();
+  unsigned all = 0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); w++) all |= s_or[w];
+  const int c = __ffs(~all) - 1;
+  if (c < 0) {
+    if (threadIdx.x == 0) {
+      blocked[b] = 1;
+      atomicAdd(nblocked, 1);
+    }
+    return;
+  }
+  if (threadIdx.x == 0) {
+    col[b] = base + c;
+    atomicMax(ncolors, base + c + 1);
+  }
+  for (int a = 0; a < p.nargs; a++) {
+    if (!p.incrw[a]) continue;
+    unsigned *w = work[p.ind[a]];
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+      atomicOr(&w[p.map[a][p.idx[a] + (size_t)(beg + i) * p.mdim[a]]], 1u << c);
+  }
+}
+
+__global__ void k_jp_elem_max(PlanParams p, unsigned long long *const *tmax, const int *col,
+                              const unsigned char *blocked) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < p.exec_length;
+       e += gridDim.x * blockDim.x) {
+    if (col[e] != -1 || blocked[e]) continue;
+    const unsigned long long pr = jp_prio(e);
+    for (int a = 0; a < p.nargs; a++)
+      if (p.incrw[a]) atomicMax(&tmax[p.ind[a]][p.map[a][p.idx[a] + (size_t)e * p.mdim[a]]], pr);
+  }
+}
+
+__global__ void k_jp_elem_win(PlanParams p, unsigned long long *const *tmax, unsigned *const *work,
+                              int *col, unsigned char *blocked, int base, int *active,
+                              int *nblocked, int *ncolors) {
+  int act = 0, blk = 0, nc = 0;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < p.exec_length;
+       e += gridDim.x * blockDim.x) {
+    if (col[e] != -1 || blocked[e]) continue;
+    const unsigned long long pr = jp_prio(e);
+    bool win = true;
+    unsigned mask = 0;
+    for (int a = 0; a < p.nargs; a++)
+      if (p.incrw[a]) {
+        const int t = p.map[a][p.idx[a] + (size_t)e * p.mdim[a]];
+        win &= tmax[p.ind[a]][t] == pr;
+        mask |= work[p.ind[a]][t];
+      }
+    if (!win) {
+      act++;
+      continue;
+    }
+    const int c = __ffs(~mask) - 1;
+    if (c < 0) {
+      blocked[e] = 1;
+      blk++;
+      continue;
+    }
+    col[e] = base + c;
+    nc = max(nc, base + c + 1);
+    for (int a = 0; a < p.nargs; a++)
+      if (p.incrw[a]) atomicOr(&work[p.ind[a]][p.map[a][p.idx[a] + (size_t)e * p.mdim[a]]], 1u << c);
+  }
+  if (act) atomicAdd(active, act);
+  if (blk) atomicAdd(nblocked, blk);
+  if (nc) atomicMax(ncolors, nc);
+}
+
 // ------------------------------------------------------------------ kernel 2
 // ind_maps + loc_maps (staged indirections) and the block's thread colours
 __global__ void k_plan_fill(PlanParams p, const long long *ind_base, const int *ind_offs,
@@ -210,6 +418,11 @@ __global__ void k_plan_fill(PlanParams p, const long long *ind_base, const int *
       }
     }
     __syncthreads();
+  }
+  if (p.jp) {
+    jp_thread_colours(p, b, beg, n, work, loc, reinterpret_cast<int *>(loc) + (p.loc_len + 1) / 2,
+                      thrcol, nthrcol);
+    return;
   }
   // greedy thread colouring (:684-754): elements in order, 32 colours a pass
   if (threadIdx.x == 0) {
@@ -573,8 +786,86 @@ static void host_transfer(Plan &pl, const PlanParams &p, const op_arg *args, con
   }
 }
 
+// Jones-Plassmann rounds over the plan's blocks (elem = false: one CTA a
+// block) or its elements (elem = true, OP_COLOR2) until every candidate has
+// a colour; col receives the colours, *ncolors_d their count.  Temporaries
+// go to `temp` (freed by the caller after the stream has finished).
+static bool jp_rounds(const PlanParams &p, bool elem, int *col, unsigned **work_ptrs,
+                      unsigned **work_d, int *ncolors_d, std::vector<void *> &temp,
+                      cudaStream_t s, int *rounds_out) {
+  Runtime &r = rt();
+  const int n = elem ? p.exec_length : p.nblocks;
+  if (rounds_out) *rounds_out = 0;
+  if (n <= 0) return cuda_ok(cudaMemsetAsync(ncolors_d, 0, sizeof(int), s), "op_plan_get: colouring");
+  std::vector<unsigned long long *> tptrs(PLAN_MAX_INDS, nullptr);
+  auto talloc = [&](size_t bytes) -> void * {
+    void *q = nullptr;
+    if (cudaMalloc(&q, bytes ? bytes : 1) != cudaSuccess) return nullptr;
+    temp.push_back(q);
+    return q;
+  };
+  for (int i = 0; i < p.ninds; i++)
+    if (p.ind_incrw[i] &&
+        !(tptrs[i] = (unsigned long long *)talloc(sizeof(unsigned long long) * p.ind_to_size[i])))
+      return cuda_ok(cudaErrorMemoryAllocation, "op_plan_get: colouring");
+  auto **tmax_d = (unsigned long long **)talloc(sizeof(void *) * PLAN_MAX_INDS);
+  int *cnt_d = (int *)talloc(2 * sizeof(int));
+  auto *blocked_d = (unsigned char *)talloc((size_t)n);
+  if (!tmax_d || !cnt_d || !blocked_d)
+    return cuda_ok(cudaErrorMemoryAllocation, "op_plan_get: colouring");
+  cudaMemcpyAsync(tmax_d, tptrs.data(), sizeof(void *) * PLAN_MAX_INDS, cudaMemcpyHostToDevice, s);
+  cudaMemsetAsync(col, 0xff, sizeof(int) * (size_t)n, s);  // -1: no colour yet
+  cudaMemsetAsync(ncolors_d, 0, sizeof(int), s);
+  const int grid = elem ? (int)std::min<long long>(((long long)n + 255) / 256, (long long)r.nsm * 8)
+                        : n;
+  int base = 0, rounds = 0;
+  int cnt[2] = {0, 0};
+  for (bool pass = true; pass;) {
+    // a pass: its 32 colours free on every target, nobody waiting
+    for (int i = 0; i < p.ninds; i++)
+      if (work_ptrs[i]) cudaMemsetAsync(work_ptrs[i], 0, sizeof(unsigned) * p.ind_to_size[i], s);
+    cudaMemsetAsync(blocked_d, 0, (size_t)n, s);
+    cudaMemsetAsync(cnt_d + 1, 0, sizeof(int), s);
+    // rounds go in batches between looks at the counters (a round after the
+    // pass has finished finds no candidate and changes nothing); the batch
+    // grows while candidates remain, so dense conflict graphs (hundreds of
+    // rounds) pay few host round trips
+    for (int batch = 1;; batch = std::min(2 * batch, 32)) {
+      if ((rounds += batch) > 1000000) {
+        set_error("op_plan_get: the parallel colouring did not finish");
+        return false;
+      }
+      for (int k = 0; k < batch; k++) {
+        for (int i = 0; i < p.ninds; i++)
+          if (tptrs[i])
+            cudaMemsetAsync(tptrs[i], 0, sizeof(unsigned long long) * p.ind_to_size[i], s);
+        cudaMemsetAsync(cnt_d, 0, sizeof(int), s);
+        if (elem) {
+          k_jp_elem_max<<<grid, 256, 0, s>>>(p, tmax_d, col, blocked_d);
+          k_jp_elem_win<<<grid, 256, 0, s>>>(p, tmax_d, work_d, col, blocked_d, base, cnt_d,
+                                             cnt_d + 1, ncolors_d);
+        } else {
+          k_jp_block_max<<<grid, PLAN_THREADS, 0, s>>>(p, tmax_d, col, blocked_d);
+          k_jp_block_win<<<grid, PLAN_THREADS, 0, s>>>(p, tmax_d, work_d, col, blocked_d, base,
+                                                       cnt_d, cnt_d + 1, ncolors_d);
+        }
+        r.launches += 2;
+      }
+      if (!cuda_ok(cudaMemcpyAsync(cnt, cnt_d, 2 * sizeof(int), cudaMemcpyDeviceToHost, s),
+                   "op_plan_get: colouring") ||
+          !cuda_ok(cudaStreamSynchronize(s), "op_plan_get: colouring"))
+        return false;
+      if (cnt[0] == 0) break;  // nobody left waiting in this pass
+    }
+    pass = cnt[1] > 0;  // some found the pass's colours taken: the next 32
+    base += 32;
+  }
+  if (rounds_out) *rounds_out = rounds;
+  return true;
+}
+
 Plan *build_plan(const char *name, op_set set, int part_size, int nargs, op_arg *args, int ninds,
-                 int *inds, int staging) {
+                 int *inds, int staging, int colouring) {
   Runtime &r = rt();
   if (!r.ready()) return nullptr;
   if (nargs > PLAN_MAX_ARGS || ninds > PLAN_MAX_INDS) {
@@ -588,7 +879,8 @@ Plan *build_plan(const char *name, op_set set, int part_size, int nargs, op_arg 
   }
   for (auto &pl : plan_cache()) {
     if (pl->name == name && pl->set == set && pl->nargs == nargs && pl->ninds == ninds &&
-        pl->part_size == part_size && pl->staging == staging && same_args(*pl, nargs, args)) {
+        pl->part_size == part_size && pl->staging == staging && pl->colouring == colouring &&
+        same_args(*pl, nargs, args)) {
       pl->pub.count++;
       return pl.get();
     }
@@ -600,6 +892,7 @@ Plan *build_plan(const char *name, op_set set, int part_size, int nargs, op_arg 
   pl->ninds = ninds;
   pl->part_size = part_size;
   pl->staging = staging;
+  pl->colouring = colouring;
   for (int m = 0; m < nargs; m++) {
     pl->dats.push_back(args[m].dat);
     pl->maps.push_back(args[m].map);
@@ -690,6 +983,7 @@ Plan *build_plan(const char *name, op_set set, int part_size, int nargs, op_arg 
   p.buf_len = buf_len;
   p.work_len = work_len;
   p.loc_len = loc_len;
+  p.jp = colouring == OP2B_COLOUR_JP;
 
   op_plan &o = pl->pub;
   memset(&o, 0, sizeof(o));
@@ -714,13 +1008,20 @@ Plan *build_plan(const char *name, op_set set, int part_size, int nargs, op_arg 
   cudaMemsetAsync(d_err, 0, sizeof(int), s);
   size_t smem_count = sizeof(int) * 3 * (size_t)buf_len;
   size_t smem_fill = smem_count + sizeof(unsigned) * (size_t)work_len + sizeof(short) * (size_t)loc_len + 16;
-  if (smem_fill > 200 * 1024) {
+  if (p.jp) smem_fill += sizeof(int) * (size_t)work_len + 4;  // the round's maxima per target
+  // (OP_COLOR2 runs no per-block kernel: one block is the whole set)
+  if (staging != OP_COLOR2 && smem_fill > 200 * 1024) {
     set_error("op_plan_get(%s): block of %d elements needs %zu bytes of shared memory", name,
               bsize, smem_fill);
     return nullptr;
   }
-  cudaFuncSetAttribute(k_plan_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_count);
-  cudaFuncSetAttribute(k_plan_fill, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fill);
+  if (staging != OP_COLOR2) {  // the per-block kernels (OP_COLOR2 runs neither)
+    if (!cuda_ok(cudaFuncSetAttribute(k_plan_count, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem_count), "op_plan_get: shared memory") ||
+        !cuda_ok(cudaFuncSetAttribute(k_plan_fill, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem_fill), "op_plan_get: shared memory"))
+      return nullptr;
+  }
 
   std::vector<int> h_counts;
   pl->thrcol_d = dalloc<int>(exec_length, own);
@@ -785,18 +1086,54 @@ Plan *build_plan(const char *name, op_set set, int part_size, int nargs, op_arg 
   cudaMemcpyAsync(work_d, work_ptrs.data(), sizeof(unsigned *) * PLAN_MAX_INDS, cudaMemcpyHostToDevice, s);
   int *ncolors_d = dalloc<int>(1, own);
 
+  std::vector<void *> temp;  // freed once the build has finished
+  struct TempFree {
+    std::vector<void *> &t;
+    ~TempFree() {
+      for (void *q : t) cudaFree(q);
+    }
+  } temp_free{temp};
   if (nblocks > 0) {
     if (staging != OP_COLOR2) {
       k_plan_fill<<<nblocks, PLAN_THREADS, smem_fill, s>>>(p, ind_base_d, pl->ind_offs_d,
                                                            pl->ind_map_d, pl->loc_map_d,
                                                            pl->thrcol_d, pl->nthrcol_d, d_err);
+      r.launches++;
+    } else if (p.jp) {
+      if (!jp_rounds(p, true, pl->thrcol_d, work_ptrs.data(), work_d, pl->nthrcol_d, temp, s,
+                     &pl->colour_rounds))
+        return nullptr;
     } else {
       k_color2_serial<<<1, 32, 0, s>>>(p, work_d, pl->thrcol_d, pl->nthrcol_d);
+      r.launches++;
     }
-    r.launches++;
-    k_block_colour_serial<<<1, 1024, 0, s>>>(p, work_d, pl->blk_col_d, ncolblk_d, pl->blkmap_d,
-                                             ncolors_d);
-    r.launches++;
+    if (p.jp && staging != OP_COLOR2) {
+      // block colours by rounds, then ncolblk/blkmap (blocks grouped by
+      // colour, in block order, :886-922) from them on the host
+      if (!jp_rounds(p, false, pl->blk_col_d, work_ptrs.data(), work_d, ncolors_d, temp, s,
+                     &pl->colour_rounds))
+        return nullptr;
+      std::vector<int> bc(nblocks);
+      int nc = 0;
+      if (!cuda_ok(cudaMemcpyAsync(bc.data(), pl->blk_col_d, sizeof(int) * nblocks,
+                                   cudaMemcpyDeviceToHost, s), "op_plan_get: colouring") ||
+          !cuda_ok(cudaMemcpyAsync(&nc, ncolors_d, sizeof(int), cudaMemcpyDeviceToHost, s),
+                   "op_plan_get: colouring") ||
+          !cuda_ok(cudaStreamSynchronize(s), "op_plan_get: colouring"))
+        return nullptr;
+      std::vector<int> ncb(std::max(nc, 1) + 1, 0), start(std::max(nc, 1) + 1, 0), bm(nblocks);
+      for (int b = 0; b < nblocks; b++) ncb[bc[b]]++;
+      for (int c = 1; c <= nc; c++) start[c] = start[c - 1] + ncb[c - 1];
+      for (int b = 0; b < nblocks; b++) bm[start[bc[b]]++] = b;
+      cudaMemcpyAsync(pl->blkmap_d, bm.data(), sizeof(int) * nblocks, cudaMemcpyHostToDevice, s);
+      cudaMemcpyAsync(ncolblk_d, ncb.data(), sizeof(int) * std::max(nc, 1), cudaMemcpyHostToDevice,
+                      s);
+      if (!cuda_ok(cudaStreamSynchronize(s), "op_plan_get: colouring")) return nullptr;
+    } else {
+      k_block_colour_serial<<<1, 1024, 0, s>>>(p, work_d, pl->blk_col_d, ncolblk_d, pl->blkmap_d,
+                                               ncolors_d);
+      r.launches++;
+    }
   }
   int ncolors = 0, h_err = 0;
   cudaMemcpyAsync(&ncolors, ncolors_d, sizeof(int), cudaMemcpyDeviceToHost, s);
@@ -1108,7 +1445,10 @@ extern "C" {
 
 op_plan *op_plan_get_stage(char const *name, op_set set, int part_size, int nargs, op_arg *args,
                            int ninds, int *inds, int staging) {
-  Plan *pl = build_plan(name, set, part_size, nargs, args, ninds, inds, staging);
+  // the reference's greedy order (bit-exact plans) unless plan_mode 1 asks
+  // for the parallel colouring
+  Plan *pl = build_plan(name, set, part_size, nargs, args, ninds, inds, staging,
+                        rt().opt_plan_mode == 1 ? OP2B_COLOUR_JP : OP2B_COLOUR_GREEDY);
   return pl ? &pl->pub : nullptr;
 }
 

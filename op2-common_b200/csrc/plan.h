@@ -13,6 +13,8 @@ struct Plan {
   std::string name;
   op_set set = nullptr;
   int nargs = 0, ninds = 0, part_size = 0, staging = 0, bsize = 0;
+  int colouring = 0;      // OP2B_COLOUR_GREEDY or OP2B_COLOUR_JP
+  int colour_rounds = 0;  // Jones-Plassmann rounds run (0 for the greedy order)
   std::vector<op_dat> dats;
   std::vector<op_map> maps;
   std::vector<int> idxs, accs, optflags, inds;
@@ -45,8 +47,11 @@ struct Plan {
   ~Plan();
 };
 
+// colouring: the reference's serial greedy order (bit-exact integers) or
+// Jones-Plassmann rounds (parallel, validated conflict-free)
+enum { OP2B_COLOUR_GREEDY = 0, OP2B_COLOUR_JP = 1 };
 Plan *build_plan(const char *name, op_set set, int part_size, int nargs, op_arg *args,
-                 int ninds, int *inds, int staging);
+                 int ninds, int *inds, int staging, int colouring = OP2B_COLOUR_GREEDY);
 const Plan *find_plan(const op_plan *o);
 int validate_plan(const Plan &pl, long detail[8]);
 // shared flags of staged indirection `slot`, aligned with its ind_map entries

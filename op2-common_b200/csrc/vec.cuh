@@ -38,6 +38,16 @@ template <> struct Vec<double> {
     __stcs(reinterpret_cast<double2 *>(p), make_double2(v[0], v[1]));
     __stcs(reinterpret_cast<double2 *>(p) + 1, make_double2(v[2], v[3]));
   }
+  // shared-memory records (16-byte aligned)
+  static __device__ __forceinline__ void st4_shared(double *p, const double *v) {
+    reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+  }
+  static __device__ __forceinline__ void ld4_shared(const double *p, double *o) {
+    const double2 v0 = reinterpret_cast<const double2 *>(p)[0];
+    const double2 v1 = reinterpret_cast<const double2 *>(p)[1];
+    o[0] = v0.x; o[1] = v0.y; o[2] = v1.x; o[3] = v1.y;
+  }
 };
 template <> struct Vec<float> {
   static __device__ __forceinline__ void ld2(const float *p, float &a, float &b) {
@@ -62,6 +72,13 @@ template <> struct Vec<float> {
   }
   static __device__ __forceinline__ void st4_cs(float *p, const float *v) {
     __stcs(reinterpret_cast<float4 *>(p), make_float4(v[0], v[1], v[2], v[3]));
+  }
+  static __device__ __forceinline__ void st4_shared(float *p, const float *v) {
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  }
+  static __device__ __forceinline__ void ld4_shared(const float *p, float *o) {
+    const float4 v = *reinterpret_cast<const float4 *>(p);
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
   }
 };
 

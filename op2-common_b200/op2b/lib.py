@@ -128,6 +128,14 @@ _SIGS = {
     "op2b_get_stream": (ctypes.c_void_p, []),
     "op2b_synchronize": (ctypes.c_int, []),
     "op2b_update_noalloc": (ctypes.c_int, [ctypes.c_int] + [ctypes.c_void_p] * 8),
+    "op_profile_start": (None, [ctypes.c_char_p]),
+    "op_profile_enter": (None, [ctypes.c_char_p]),
+    "op_profile_enter_kernel": (None, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p]),
+    "op_profile_next": (None, [ctypes.c_char_p]),
+    "op_profile_exit": (None, []),
+    "op_profile_end": (None, []),
+    "op_profile_output": (None, []),
+    "op_profile_output_json": (None, [ctypes.c_char_p]),
 }
 
 

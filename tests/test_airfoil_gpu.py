@@ -131,7 +131,7 @@ def test_colouring_is_deterministic_and_matches_atomics(op2, part):
 GATHER_KERNELS = [(1, 0, 0, 0), (2, 0, 0, 1), (3, 0, 0, 1), (4, 64, 0, 1), (4, 96, 0, 1),
                   (4, 128, 0, 1), (4, 256, 0, 1), (5, 64, 0, 1), (5, 96, 0, 1), (5, 128, 0, 0),
                   (5, 256, 0, 1), (6, 64, 5, 1), (6, 64, 6, 1), (6, 128, 0, 1), (6, 128, 3, 0),
-                  (6, 256, 0, 1)]
+                  (6, 256, 0, 1), (7, 0, 0, 1), (7, 0, 0, 0)]
 
 
 @pytest.mark.parametrize("kernel", GATHER_KERNELS,
@@ -165,6 +165,40 @@ def test_gather_mode_is_bit_exact_with_reference(op2, fixture, kernel):
     assert np.array_equal(np.array([h[2] for h in hist]), gd["errloc"])
     # the rms sum over ~1e5 terms in a different order: ~1e-14 relative
     assert np.max(np.abs(np.array([h[0] for h in hist]) / gd["rms"] - 1)) < 1e-13
+
+
+@pytest.mark.parametrize("I,J,renumber", [(240, 120, True), (600, 300, True), (600, 300, False),
+                                          (2400, 1200, True), (2400, 1200, False)])
+def test_flux_ring_is_bit_identical_to_corner_kernel(op2, I, J, renumber):
+    """gather_kernel 7 computes each interior flux once (by the cell that
+    comes first in its CTA's range) and sums every cell's fluxes from a
+    shared-memory ring in the same slot order: q, adt and res equal the
+    corner kernel's bit for bit, fused with bres_calc and alone, in both
+    precisions.  On the renumbered mesh the ring records are built and used;
+    on a randomly numbered large mesh they cannot be (neighbours too far
+    apart) and the corner kernel serves."""
+    m = M.channel_bump(I, J, seed=7)
+    for dtype in (np.float64, np.float32):
+        for fuse in (1, 0):
+            out, used = [], []
+            for gk in (6, 7):
+                op2.set_option("gather_kernel", gk)
+                op2.set_option("fuse", fuse)
+                app = Airfoil(m, dtype=dtype)
+                if renumber:
+                    app.renumber()
+                app.iterate(3)
+                out.append(app.fetch())
+                used.append(op2.get_option("ring_used"))
+                op2.op_exit()
+                op2.op_init()
+            for k in ("q", "adt", "res"):
+                assert np.array_equal(out[0][k], out[1][k]), (dtype, fuse, k)
+            assert used[0] == 0
+            if renumber:
+                assert used[1] == 1, (I, J)
+            elif I * J >= 2400 * 1200:
+                assert used[1] == 0
 
 
 @pytest.mark.parametrize("hints", [0, 1])
@@ -501,7 +535,7 @@ def test_options_return_to_defaults_at_exit(op2):
     op2.op_init()
     assert {k: op2.get_option(k) for k in defaults} == defaults
     with pytest.raises(L.Op2Error):
-        op2.set_option("gather_kernel", 7)
+        op2.set_option("gather_kernel", 8)
 
 
 def test_large_mesh_one_iteration_against_oracle(op2):
@@ -521,7 +555,7 @@ def test_large_mesh_one_iteration_against_oracle(op2):
     assert np.all(np.abs(r.sum(axis=0)) <= 1e-9 * np.abs(r).sum(axis=0))
 
 
-@pytest.mark.parametrize("kernel", [3, 4, 5, 6])
+@pytest.mark.parametrize("kernel", [3, 4, 5, 6, 7])
 def test_mixed_precision_against_fp32_restatement(op2, kernel):
     op2.set_option("gather_kernel", kernel)
     m = M.channel_bump(120, 60, seed=4)

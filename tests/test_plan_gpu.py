@@ -116,3 +116,88 @@ def test_full_size_res_calc_plan_matches_reference_live(op2, I, J, part):
     _compare(d, G(g), 2)
     n, det = L.plan_validate(p)
     assert n == 0, det
+
+
+@pytest.mark.parametrize("I,J,staging,part,renumber", [(240, 120, 2, 0, False),
+                                                       (240, 120, 3, 128, True),
+                                                       (240, 120, 4, 0, False),
+                                                       (2400, 1200, 2, 0, False),
+                                                       (2400, 1200, 2, 0, True),
+                                                       (2400, 1200, 4, 0, True)])
+def test_parallel_colouring_is_conflict_free(op2, I, J, staging, part, renumber):
+    """plan_mode 1: block and thread colours (and OP_COLOR2's element
+    colours) by Jones-Plassmann rounds on the device instead of the
+    reference's serial greedy walk (op_rt_support.cpp:684-884).  The colours
+    differ from the greedy ones, so the plan is checked by its invariants: no
+    two elements of a thread colour in a block, no two blocks of a block
+    colour, touch the same OP_INC target; every element in exactly one
+    block.  Its staging arrays (ind_maps, loc_maps) stay the reference's."""
+    mesh = M.channel_bump(I, J, seed=1)
+    app = Airfoil(mesh)
+    if renumber:
+        app.renumber()
+    op2.set_option("plan_mode", 1)
+    p = L.op_plan_get_stage("res_calc", app.edges, part, app.a_res, INDS["res_calc"], staging)
+    d = L.plan_arrays(p)
+    n, det = L.plan_validate(p)
+    assert n == 0, det
+    ms = L.load().op2b_plan_build_ms(p)
+    assert d["ncolors"] >= 2 and ms > 0
+    if staging != 4:
+        # block colours: a partition of the blocks
+        nc = int(d["ncolors"])
+        assert d["ncolblk"][:nc].sum() == d["nblocks"]
+        assert sorted(d["blkmap"][:d["nblocks"]]) == list(range(d["nblocks"]))
+    if staging == 4 and I * J > 240 * 120:
+        print(f"{I}x{J} OP_COLOR2 renumbered {renumber}: parallel colouring "
+              f"{d['ncolors']} colours in {ms:.1f} ms")
+        return  # (the greedy OP_COLOR2 walk is one device thread: seconds at this size)
+    # the greedy plan of the same loop keeps the reference's integers
+    op2.set_option("plan_mode", 2)
+    g = L.plan_arrays(L.op_plan_get_stage("res_calc", app.edges, part, app.a_res,
+                                          INDS["res_calc"], staging))
+    if staging != 4:
+        for k in ("ind_offs", "ind_sizes", "nindirect", "nelems", "offset"):
+            assert np.array_equal(d[k], g[k]), k
+    print(f"{I}x{J} staging {staging} renumbered {renumber}: parallel colouring "
+          f"{d['ncolors']} colours in {ms:.1f} ms; greedy {g['ncolors']} colours")
+
+
+@pytest.mark.parametrize("mode", [L.OP2B_INC_COLOR, L.OP2B_INC_HYBRID])
+def test_loops_on_parallel_colouring_match_reference(op2, mode):
+    gd = np.load(f"{GOLDEN}/airfoil_240x120_s1.npz")
+    m = M.channel_bump(240, 120, seed=1)
+    op2.set_option("plan_mode", 1)
+    op2.set_option("inc_mode", mode)
+    app = Airfoil(m)
+    hist = app.iterate(100)
+    rms = np.array([h[0] for h in hist])
+    assert np.max(np.abs(rms / gd["rms"] - 1)) < 1e-12
+    q = app.fetch()["q"]
+    idx = gd["q_sample_idx"]
+    scale = np.abs(gd["q_sample"]).max(axis=0)
+    assert np.all(np.abs(q[idx] - gd["q_sample"]).max(axis=0) <= 1e-12 * scale)
+
+
+@pytest.mark.parametrize("segmented", [0, 1])
+def test_atomic_increments_match_reference(op2, segmented):
+    """inc_mode 0 with per-edge atomics and with segmented atomics (a warp's
+    increments to one cell combined first): within 1e-12 of the reference
+    after 100 iterations, on the randomly numbered and the renumbered mesh."""
+    gd = np.load(f"{GOLDEN}/airfoil_240x120_s1.npz")
+    for renumber in (False, True):
+        op2.set_option("inc_mode", L.OP2B_INC_ATOMIC)
+        op2.set_option("atomic_segmented", segmented)
+        m = M.channel_bump(240, 120, seed=1)
+        app = Airfoil(m)
+        if renumber:
+            app.renumber()
+        hist = app.iterate(100)
+        rms = np.array([h[0] for h in hist])
+        assert np.max(np.abs(rms / gd["rms"] - 1)) < 1e-12
+        q = app.fetch_original()
+        idx = gd["q_sample_idx"]
+        scale = np.abs(gd["q_sample"]).max(axis=0)
+        assert np.all(np.abs(q[idx] - gd["q_sample"]).max(axis=0) <= 1e-12 * scale)
+        L.op_exit()
+        L.op_init()
