@@ -32,8 +32,9 @@ typedef struct {
 
 typedef struct op2b_batch_s *op2b_batch;
 
-#define OP2B_BATCH_RES_GATHER 0
-#define OP2B_BATCH_RES_ATOMIC 1
+#define OP2B_BATCH_RES_GATHER 0 /* owner computes over cells (no conflicts) */
+#define OP2B_BATCH_RES_ATOMIC 1 /* one thread an edge, atomic increments */
+#define OP2B_BATCH_RES_COLOUR 2 /* edges by colour (parallel OP_COLOR2 plan), no atomics */
 
 /* fp32 may be NULL (FP64 only).  cell_off / edge_off: ninst + 1 offsets of
  * each instance's cells and edges; qinf: 4 doubles per instance.  The
@@ -42,9 +43,12 @@ op2b_batch op2b_batch_create(const op2b_airfoil_dats *fp32, const op2b_airfoil_d
                              int ninst, const int *cell_off, const int *edge_off,
                              const double *qinf);
 /* keys: "tol", "promote_tol", "max_iter", "stall_window", "block" (128, 256,
- * 512), "blocks_per_sm", "res_kernel" (OP2B_BATCH_RES_*). */
+ * 512), "blocks_per_sm", "res_kernel" (OP2B_BATCH_RES_*), "part_size"
+ * (elements per work item, >= 256; the reference's OP_PART_SIZE,
+ * op_lib_core.cpp:205-220). */
 int op2b_batch_set(op2b_batch b, const char *key, double value);
-/* Time every (res_calc strategy x block size) candidate for `iters`
+/* Time every (res_calc strategy: gather, atomics or colouring) x (block size:
+ * 128, 256, 512) x (partition size: 512, 2048, 8192) candidate for `iters`
  * iterations, keep the fastest; the solve's state is left untouched. */
 int op2b_batch_tune(op2b_batch b, int iters, char *report, int report_len);
 /* Run up to max_iterations iterations (graphs when use_graph), checking for

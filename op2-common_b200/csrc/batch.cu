@@ -33,9 +33,12 @@
 #include "gather.h"
 #include "op2b_batch.h"
 #include "op2b_runtime.h"
+#include "plan.h"
 #include "vec.cuh"
 
 namespace op2b {
+
+constexpr int kMinChunk = 256;  // smallest partition size (elements per work item)
 
 // ------------------------------------------------------------------ stage kernels
 
@@ -137,6 +140,42 @@ __global__ void k_b_res_atomic(const WorkItem *items, const int *count, const in
         atomicAdd(res + 4 * (size_t)cc.y + m, -f[m]);
       }
     }
+  }
+}
+
+// coloured res_calc: the edges of one colour (elems[0..n) of the batch's
+// OP_COLOR2 plan) share no cell, so each adds its flux to both cells without
+// atomics; an edge whose instance is not in this precision's phase is skipped
+template <typename T>
+__global__ void k_b_res_colour(const int *elems, int n, const int *edge_off, int ninst,
+                               const int *phase, int fp64, const int2 *pedge, const int2 *pecell,
+                               const T *x, const T *q, const T *adt, T *res, AirConst<T> k) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int e = __ldg(elems + i);
+    int lo = 0, hi = ninst - 1;  // the instance owning edge e: edge_off[lo] <= e < edge_off[lo+1]
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(edge_off + mid) <= e) lo = mid;
+      else hi = mid - 1;
+    }
+    const int p = __ldg(phase + lo);
+    if (fp64 ? !(p == 1 || p == 3) : p != 0) continue;
+    int2 nn = __ldg(pedge + e), cc = __ldg(pecell + e);
+    T x1x, x1y, x2x, x2y, q1[4], q2[4], f[4], r1[4], r2[4];
+    Vec<T>::ld2(x + 2 * (size_t)nn.x, x1x, x1y);
+    Vec<T>::ld2(x + 2 * (size_t)nn.y, x2x, x2y);
+    Vec<T>::ld4(q + 4 * (size_t)cc.x, q1);
+    Vec<T>::ld4(q + 4 * (size_t)cc.y, q2);
+    air_flux<T>(x1x, x1y, x2x, x2y, q1, q2, __ldg(adt + cc.x), __ldg(adt + cc.y), k, f);
+    Vec<T>::ld4_rw(res + 4 * (size_t)cc.x, r1);
+    Vec<T>::ld4_rw(res + 4 * (size_t)cc.y, r2);
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+      r1[m] += f[m];
+      r2[m] -= f[m];
+    }
+    Vec<T>::st4(res + 4 * (size_t)cc.x, r1);
+    Vec<T>::st4(res + 4 * (size_t)cc.y, r2);
   }
 }
 
@@ -339,6 +378,11 @@ struct op2b_batch_s {
   int ninst = 0, ncells = 0;
   int block = 256, blocks_per_sm = 4;
   int res_kernel = OP2B_BATCH_RES_GATHER;
+  // OP2B_BATCH_RES_COLOUR: the edges grouped by colour (device) and each
+  // colour's first element (host, ncolours + 1 entries), from a parallel
+  // OP_COLOR2 colouring of the batch's edges
+  const int *colour_elems = nullptr;
+  std::vector<int> colour_off;
   cudaGraphExec_t graph = nullptr;
   bool graph_dirty = true;
   std::string tune_report;
@@ -378,6 +422,15 @@ static void enqueue_stage(op2b_batch_s *b, const PrecisionDats &d, const WorkLis
                                             reinterpret_cast<const int2 *>(d.pedge),
                                             reinterpret_cast<const int2 *>(d.pecell), x, q, adt,
                                             res, k);
+    else if (b->res_kernel == OP2B_BATCH_RES_COLOUR)
+      for (size_t c = 0; c + 1 < b->colour_off.size(); c++) {
+        const int n = b->colour_off[c + 1] - b->colour_off[c];
+        if (n <= 0) continue;
+        k_b_res_colour<T><<<std::min(grid, (n + th - 1) / th), th, 0, s>>>(
+            b->colour_elems + b->colour_off[c], n, b->dev.edge_off, b->ninst, b->dev.phase,
+            sizeof(T) == 8, reinterpret_cast<const int2 *>(d.pedge),
+            reinterpret_cast<const int2 *>(d.pecell), x, q, adt, res, k);
+      }
     else
       k_b_res_gather<T><<<grid, th, 0, s>>>(w.cells, w.count,
                                             reinterpret_cast<const int4 *>(b->slots->o),
@@ -422,6 +475,24 @@ static bool fill_dats(const op2b_airfoil_dats *h, PrecisionDats &d, int want_byt
   d.qold = h->p_qold->data_d;
   d.adt = h->p_adt->data_d;
   d.res = h->p_res->data_d;
+  return true;
+}
+
+// the colours of the batch's edges for OP2B_BATCH_RES_COLOUR: a parallel
+// (Jones-Plassmann) OP_COLOR2 plan of res_calc's two increments over pecell,
+// built once (before any capture) and kept in the plan cache
+static bool build_colouring(op2b_batch_s *b) {
+  op_arg args[2] = {op_arg_dat(b->h64.p_res, 0, b->h64.pecell, 4, "double", OP_INC),
+                    op_arg_dat(b->h64.p_res, 1, b->h64.pecell, 4, "double", OP_INC)};
+  int inds[2] = {0, 0};
+  Plan *pl = build_plan("batch res_calc#coloured", b->h64.pecell->from, 0, 2, args, 1, inds,
+                        OP_COLOR2, OP2B_COLOUR_JP);
+  if (!pl || !pl->col_reord_d || !pl->pub.color2_offsets) {
+    if (!op2b_last_error()[0]) set_error("op2b_batch: colouring the edges failed");
+    return false;
+  }
+  b->colour_elems = pl->col_reord_d;
+  b->colour_off.assign(pl->pub.color2_offsets, pl->pub.color2_offsets + pl->pub.ncolors + 1);
   return true;
 }
 
@@ -504,12 +575,13 @@ op2b_batch op2b_batch_create(const op2b_airfoil_dats *fp32, const op2b_airfoil_d
   double *qi = (double *)A(sizeof(double) * 4 * ninst);
   cudaMemcpy(qi, qinf, sizeof(double) * 4 * ninst, cudaMemcpyHostToDevice);
   d.qinf = qi;
-  // list capacities: every instance active
+  // list capacities: every instance active, at the smallest partition size
   size_t cap_c = 0, cap_b = 0, cap_e = 0;
+  const int cmin = kMinChunk;
   for (int i = 0; i < ninst; i++) {
-    cap_c += (cell_off[i + 1] - cell_off[i] + d.chunk - 1) / d.chunk;
-    cap_b += (brow_off[i + 1] - brow_off[i] + d.chunk - 1) / d.chunk;
-    cap_e += (edge_off[i + 1] - edge_off[i] + d.chunk - 1) / d.chunk;
+    cap_c += (cell_off[i + 1] - cell_off[i] + cmin - 1) / cmin;
+    cap_b += (brow_off[i + 1] - brow_off[i] + cmin - 1) / cmin;
+    cap_e += (edge_off[i + 1] - edge_off[i] + cmin - 1) / cmin;
   }
   for (WorkLists *w : {&d.w32, &d.w64}) {
     w->cells = (WorkItem *)A(sizeof(WorkItem) * (cap_c + 1));
@@ -553,8 +625,19 @@ int op2b_batch_set(op2b_batch b, const char *key, double value) {
   else if (k == "stall_window") d.stall_window = std::max(1, (int)value);
   else if (k == "block") b->block = (int)value;
   else if (k == "blocks_per_sm") b->blocks_per_sm = std::max(1, (int)value);
-  else if (k == "res_kernel") b->res_kernel = (int)value;
-  else {
+  else if (k == "res_kernel") {
+    if (value < OP2B_BATCH_RES_GATHER || value > OP2B_BATCH_RES_COLOUR) {
+      set_error("op2b_batch_set: res_kernel must be OP2B_BATCH_RES_GATHER, _ATOMIC or _COLOUR");
+      return -1;
+    }
+    b->res_kernel = (int)value;
+  } else if (k == "part_size") {
+    if (value < kMinChunk || value > (1 << 24)) {
+      set_error("op2b_batch_set: part_size must be in [%d, %d]", kMinChunk, 1 << 24);
+      return -1;
+    }
+    d.chunk = (int)value;  // the work lists of the next iteration use it
+  } else {
     set_error("op2b_batch_set: unknown key '%s'", key);
     return -1;
   }
@@ -573,6 +656,8 @@ int op2b_batch_run(op2b_batch b, int max_iterations, int check_every, int use_gr
   if (!b || !r.ready()) return -1;
   cudaStream_t s = r.stream;
   if (check_every < 1) check_every = 1;
+  if (b->res_kernel == OP2B_BATCH_RES_COLOUR && !b->colour_elems && !build_colouring(b))
+    return -1;
   if (use_graph && b->graph_dirty) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
@@ -662,17 +747,20 @@ int op2b_batch_tune(op2b_batch b, int iters, char *report, int report_len) {
   void *sq64 = save(b->p64.q, qb64);
   void *sph = save(d.phase, sizeof(int) * n);
   struct Cand {
-    int res_kernel, block;
+    int res_kernel, block, part;
   };
   std::vector<Cand> cands;
-  for (int rk : {OP2B_BATCH_RES_GATHER, OP2B_BATCH_RES_ATOMIC})
-    for (int blk : {128, 256, 512}) cands.push_back({rk, blk});
+  for (int rk : {OP2B_BATCH_RES_GATHER, OP2B_BATCH_RES_ATOMIC, OP2B_BATCH_RES_COLOUR})
+    for (int blk : {128, 256, 512})
+      for (int part : {512, 2048, 8192}) cands.push_back({rk, blk, part});
   double best = 1e30;
-  Cand bestc = {b->res_kernel, b->block};
+  Cand bestc = {b->res_kernel, b->block, d.chunk};
   std::string rep;
+  static const char *kRes[] = {"gather", "atomic", "colour"};
   for (const Cand &c : cands) {
     b->res_kernel = c.res_kernel;
     b->block = c.block;
+    d.chunk = c.part;
     b->graph_dirty = true;
     // reset state before each candidate
     if (sq32) restore(b->p32.q, sq32, qb32);
@@ -688,8 +776,8 @@ int op2b_batch_tune(op2b_batch b, int iters, char *report, int report_len) {
     if (op2b_batch_run(b, iters, iters, 1, &ms) < 0) return -1;
     double per = ms / std::max(iters, 1);
     char line[160];
-    snprintf(line, sizeof(line), "res_kernel=%s block=%d: %.4f ms/iter\n",
-             c.res_kernel == OP2B_BATCH_RES_ATOMIC ? "atomic" : "gather", c.block, per);
+    snprintf(line, sizeof(line), "res_kernel=%s block=%d part_size=%d: %.4f ms/iter\n",
+             kRes[c.res_kernel], c.block, c.part, per);
     rep += line;
     if (per < best) {
       best = per;
@@ -698,6 +786,7 @@ int op2b_batch_tune(op2b_batch b, int iters, char *report, int report_len) {
   }
   b->res_kernel = bestc.res_kernel;
   b->block = bestc.block;
+  d.chunk = bestc.part;
   b->graph_dirty = true;
   if (sq32) restore(b->p32.q, sq32, qb32);
   restore(b->p64.q, sq64, qb64);
@@ -712,8 +801,8 @@ int op2b_batch_tune(op2b_batch b, int iters, char *report, int report_len) {
   bool ok = cuda_ok(cudaStreamSynchronize(s), "op2b_batch_tune");
   for (void *p : snap) cudaFree(p);
   char line[160];
-  snprintf(line, sizeof(line), "chosen: res_kernel=%s block=%d\n",
-           bestc.res_kernel == OP2B_BATCH_RES_ATOMIC ? "atomic" : "gather", bestc.block);
+  snprintf(line, sizeof(line), "chosen: res_kernel=%s block=%d part_size=%d\n",
+           kRes[bestc.res_kernel], bestc.block, bestc.part);
   rep += line;
   b->tune_report = rep;
   if (report && report_len > 0) {

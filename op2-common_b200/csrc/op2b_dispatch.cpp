@@ -476,7 +476,8 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
   int E = set->size, N = a[0].dat->set->size, C = a[2].dat->set->size;
   double bytes = 16.0 * E + (double)rb * (2.0 * N + 13.0 * C);
   if (r.opt_fuse && r.opt_inc_mode == OP2B_INC_GATHER &&
-      r.opt_gather_kernel == OP2B_GATHER_CORNER && r.opt_bres_kernel == 1) {
+      (r.opt_gather_kernel == OP2B_GATHER_CORNER || r.opt_gather_kernel == OP2B_GATHER_RING) &&
+      r.opt_bres_kernel == 1) {
     const SlotRecords *cr = get_corner_records(pecell, pedge);
     if (!cr) return -1;
     bool ok = true;
@@ -510,7 +511,7 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
   const InvMap *inv = nullptr;
   const SlotRecords *slots = nullptr;
   if (r.opt_inc_mode == OP2B_INC_GATHER) {
-    if (r.opt_gather_kernel == OP2B_GATHER_CORNER) {
+    if (r.opt_gather_kernel == OP2B_GATHER_CORNER || r.opt_gather_kernel == OP2B_GATHER_RING) {
       slots = get_corner_records(pecell, pedge);
       if (!slots) return -1;
     } else if (r.opt_gather_kernel != OP2B_GATHER_CSR) {
@@ -910,18 +911,28 @@ bool op2b::Runtime::flush_loop() {
     if (!cr) return false;
     if (res_zero == pd.res && !materialize_res()) return false;
     begin_loop("res_calc");
+    ring_used = opt_gather_kernel == OP2B_GATHER_RING && build_ring_records(cr, nsm, 256);
     if (pd.rb == 8)
-      e = launch_res_calc_gather_corner<double>(ctx(), *cr, (const double *)pd.x->data_d,
-                                                (const double *)pd.q->data_d,
-                                                (const double *)pd.adt->data_d,
-                                                (double *)pd.res->data_d, pd.kd, opt_pipe_block,
-                                                opt_gather_minb);
+      e = ring_used
+              ? launch_res_ring<double>(ctx(), *cr, nullptr, (const double *)pd.x->data_d,
+                                        (const double *)pd.q->data_d,
+                                        (const double *)pd.adt->data_d, (double *)pd.res->data_d,
+                                        pd.kd, false)
+              : launch_res_calc_gather_corner<double>(ctx(), *cr, (const double *)pd.x->data_d,
+                                                      (const double *)pd.q->data_d,
+                                                      (const double *)pd.adt->data_d,
+                                                      (double *)pd.res->data_d, pd.kd,
+                                                      opt_pipe_block, opt_gather_minb);
     else
-      e = launch_res_calc_gather_corner<float>(ctx(), *cr, (const float *)pd.x->data_d,
-                                               (const float *)pd.q->data_d,
-                                               (const float *)pd.adt->data_d,
-                                               (float *)pd.res->data_d, pd.kf, opt_pipe_block,
-                                               opt_gather_minb);
+      e = ring_used
+              ? launch_res_ring<float>(ctx(), *cr, nullptr, (const float *)pd.x->data_d,
+                                       (const float *)pd.q->data_d, (const float *)pd.adt->data_d,
+                                       (float *)pd.res->data_d, pd.kf, false)
+              : launch_res_calc_gather_corner<float>(ctx(), *cr, (const float *)pd.x->data_d,
+                                                     (const float *)pd.q->data_d,
+                                                     (const float *)pd.adt->data_d,
+                                                     (float *)pd.res->data_d, pd.kf,
+                                                     opt_pipe_block, opt_gather_minb);
     end_loop(pd.bytes);
     return finish(e, "res_calc") == 0;
   }

@@ -29,10 +29,16 @@ def _oracle_q(spec, niter):
     return st.q, rms
 
 
-@pytest.mark.parametrize("graph", [True, False])
-def test_fp64_batch_matches_each_instance(op2, graph):
+@pytest.mark.parametrize("graph,res_kernel,part", [(True, 0, 2048), (False, 0, 2048),
+                                                   (True, 1, 512), (True, 2, 256),
+                                                   (False, 2, 8192)])
+def test_fp64_batch_matches_each_instance(op2, graph, res_kernel, part):
+    """Every res_calc strategy of the batch engine (owner computes, atomics,
+    edges by colour without atomics) and partition size."""
     b = AirfoilBatch(SPECS, fp32=False)
     b.set("tol", 0.0)
+    b.set("res_kernel", res_kernel)
+    b.set("part_size", part)
     active, _ = b.run(40, check_every=10, graph=graph)
     assert active == len(SPECS)
     st = b.stats()
@@ -79,7 +85,10 @@ def test_mixed_batch_converges_through_promotion(op2):
 def test_autotuner_picks_and_keeps_state(op2):
     b = AirfoilBatch(SPECS, fp32=True)
     rep = b.tune(iters=5)
-    assert "chosen:" in rep and rep.count("ms/iter") == 6
+    # res_calc strategy (gather, atomic, colour) x block size x partition size
+    assert "chosen:" in rep and rep.count("ms/iter") == 27
+    for word in ("gather", "atomic", "colour", "part_size=512", "part_size=8192"):
+        assert word in rep
     b.set("tol", 0.0)
     b.run(10, check_every=10)
     st = b.stats()

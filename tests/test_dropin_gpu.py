@@ -213,3 +213,33 @@ def test_reference_airfoil_variants_run_on_libop2b(variant):
     tol = 1e-4 if variant == "sp" else 2e-5
     for (_, a), (_, b) in zip(out[got], out[ref]):
         assert abs(a - b) <= tol * b, (variant, out[got], out[ref])
+
+
+@pytest.mark.skipif(not (O.ref_binary("airfoil_sp_harness_dropin") and
+                         O.ref_binary("ref_airfoil_sp_harness")),
+                    reason="sp harness binaries not built")
+def test_sp_airfoil_q_is_bit_identical_to_reference():
+    """The single-precision Airfoil (the reference's airfoil_plain/sp kernels
+    and loop calls, in oracle/ref_airfoil_sp.cpp, which dumps q through
+    op_fetch_data) on libop2b and on the reference's sequential library: q
+    after 1000 iterations is bit-identical -- every float operation rounds as
+    in the sequential build and each cell's increments add in its order.  Only
+    the sp update's float rms differs, by the order of its sum over the
+    cells (a few 1e-6 relative; the printed history of the unmodified sp
+    application shows that difference)."""
+    m = M.channel_bump(240, 120, seed=1)
+    res = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "m.bin")
+        M.write_grid_bin(m, path)
+        for b in ("airfoil_sp_harness_dropin", "ref_airfoil_sp_harness"):
+            prefix = os.path.join(tmp, b)
+            r = subprocess.run([O.ref_binary(b), path, "1000", prefix], capture_output=True,
+                               text=True, timeout=600)
+            assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+            res[b] = (np.fromfile(prefix + ".q", np.float32).reshape(m.ncell, 4),
+                      np.fromfile(prefix + ".rms", np.float32))
+    (q_gpu, rms_gpu), (q_ref, rms_ref) = res["airfoil_sp_harness_dropin"], res["ref_airfoil_sp_harness"]
+    assert np.array_equal(q_gpu.view(np.uint32), q_ref.view(np.uint32)), \
+        "q after 1000 iterations must equal the reference's bit for bit"
+    assert np.max(np.abs(rms_gpu / rms_ref - 1)) < 1e-4
