@@ -37,7 +37,9 @@ extern "C" {
  * residual (OP2B_EPI_BIAS_BF16) or the pre-activation whose silu' multiplies
  * the product (OP2B_EPI_SILU_GRAD_BF16), bf16.  split_k > 1 splits K over
  * CTAs and requires OP2B_EPI_ATOMIC_F32.  engine 0 = tensor cores, 1 = CUDA
- * cores (FP32 store only; a cross-check of the tensor-core path).
+ * cores (FP32 store only; a cross-check of the tensor-core path), 2 = tensor
+ * cores fed by TMA (k-contiguous A and B only; engine 0 takes this path too
+ * when the option gemm_tma is set).
  * Replaces: nothing in the reference (no learned component). */
 int op2b_gemm_bf16(int M, int N, int K, const void *A, long a_m, long a_k, const void *B,
                    long b_n, long b_k, void *C, long ldc, int epi, const float *bias, void *Z,

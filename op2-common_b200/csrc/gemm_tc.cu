@@ -21,6 +21,7 @@
 // Every mbarrier wait is bounded in time (%globaltimer): on expiry the kernel
 // records an error, stops issuing, waits (bounded) for its outstanding
 // commits, frees its tensor memory and returns.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -385,6 +386,175 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tc(GemmArgs g) {
   if (threadIdx.x == 0 && s_fail) atomicExch(g.err, 1);
 }
 
+// ---------------------------------------------------------------------------
+// The TMA-fed form, for K-major A and B (k contiguous in both: the forward
+// products X W^T of the MLPs).  Operand tiles arrive by cp.async.bulk.tensor
+// (a tensor map per operand, 128-byte swizzle -- the layout the tensor core
+// reads through umma_desc -- and zero fill outside the matrix) into a ring of
+// kTmaStages stages, so loads run up to three K tiles ahead of the MMAs:
+//   * thread 0 (producer): waits until the MMAs of the tile that last used a
+//     stage have completed (the stage's "empty" mbarrier, arrived by
+//     tcgen05.commit), announces the stage's bytes on its "full" mbarrier and
+//     issues the two tile loads, which complete the transaction;
+//   * thread 32 (MMA issuer): waits for a stage's "full" mbarrier, issues the
+//     four tcgen05.mma of the K tile and commits them to the stage's "empty"
+//     mbarrier; after the last tile, one more commit to "done";
+//   * then all four warps read the accumulator from TMEM and run the
+//     epilogue as in k_gemm_tc.
+// Three stages (96 KiB) let two CTAs share an SM, so one CTA's epilogue
+// overlaps the other's loads.  No multicast: every CTA loads its own tiles.
+// Every wait is bounded; on expiry the kernel records the error, stops
+// issuing, waits (bounded) for the loads and MMAs already issued, frees its
+// tensor memory and returns.
+constexpr int kTmaStages = 3;
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y,
+                                            uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
+__global__ void __launch_bounds__(kThreads, 2)
+k_gemm_tma(GemmArgs g, const __grid_constant__ CUtensorMap ta,
+           const __grid_constant__ CUtensorMap tb) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t bars[2 * kTmaStages + 1];
+  __shared__ uint32_t s_taddr;
+  __shared__ int s_fail, s_loaded, s_mma;
+  uint8_t *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * kTileN;
+  const int rem = g.N - n0;
+  const int nt = rem >= kTileN ? kTileN : ((rem + 15) & ~15);
+  const int kb = blockIdx.z * g.k_per_split;
+  const int ke = min(g.K, kb + g.k_per_split);
+  const int nk = ke > kb ? (ke - kb + kTileK - 1) / kTileK : 0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  auto full = [&](int st) { return smem_u32(&bars[st]); };
+  auto empty = [&](int st) { return smem_u32(&bars[kTmaStages + st]); };
+  const uint32_t done = smem_u32(&bars[2 * kTmaStages]);
+  auto stage_a = [&](int st) { return smem_u32(smem + (size_t)st * 2 * kStageBytes); };
+  auto stage_b = [&](int st) { return smem_u32(smem + (size_t)st * 2 * kStageBytes + kStageBytes); };
+
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < kTmaStages; st++) {
+      mbar_init(full(st), 1);
+      mbar_init(empty(st), 1);
+    }
+    mbar_init(done, 1);
+    s_fail = 0;
+    s_loaded = 0;
+    s_mma = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&ta)) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tb)) : "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&s_taddr)),
+                 "r"(128u));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t taddr = s_taddr;
+
+  if (threadIdx.x == 0) {  // producer
+    int kt = 0;
+    for (; kt < nk; kt++) {
+      const int st = kt % kTmaStages;
+      if (kt >= kTmaStages && !mbar_wait(empty(st), (uint32_t)((kt / kTmaStages - 1) & 1))) {
+        atomicExch(&s_fail, 1);
+        break;
+      }
+      if (*(volatile int *)&s_fail) break;
+      mbar_expect_tx(full(st), 2 * kStageBytes);
+      const int k0 = kb + kt * kTileK;
+      tma_load_2d(stage_a(st), &ta, k0, m0, full(st));
+      tma_load_2d(stage_b(st), &tb, k0, n0, full(st));
+    }
+    *(volatile int *)&s_loaded = kt;
+  } else if (threadIdx.x == 32) {  // MMA issuer
+    const uint32_t idesc = umma_idesc(nt);
+    int kt = 0;
+    for (; kt < nk; kt++) {
+      const int st = kt % kTmaStages;
+      if (!mbar_wait(full(st), (uint32_t)((kt / kTmaStages) & 1))) {
+        atomicExch(&s_fail, 1);
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a0 = stage_a(st), b0 = stage_b(st);
+#pragma unroll
+      for (int j = 0; j < kTileK / 16; j++) {
+        const uint64_t da = umma_desc(a0 + j * 32);
+        const uint64_t db = umma_desc(b0 + j * 32);
+        const uint32_t acc = (kt > 0 || j > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(taddr),
+            "l"(da), "l"(db), "r"(idesc), "r"(acc));
+      }
+      asm volatile(
+          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+              empty(st))
+          : "memory");
+    }
+    *(volatile int *)&s_mma = kt;
+    // one more commit: arrives when every MMA issued above has completed
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(done)
+        : "memory");
+  }
+  __syncthreads();
+  // every issued MMA has finished once "done" has arrived; the loads the MMA
+  // issuer did not consume (after a failure) are waited for before exit
+  if (threadIdx.x == 0) {
+    if (!mbar_wait(done, 0u)) s_fail = 1;
+    for (int kt = s_mma; kt < s_loaded; kt++)
+      if (!mbar_wait(full(kt % kTmaStages), (uint32_t)((kt / kTmaStages) & 1))) {
+        s_fail = 1;
+        break;
+      }
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (!s_fail) {
+    const int row = m0 + warp * 32 + lane;
+    for (int cc = 0; cc < nt; cc += 16) {
+      uint32_t r[16];
+      if (nk > 0) {
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+            "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+              "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+              "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)cc));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      } else {
+#pragma unroll
+        for (int i = 0; i < 16; i++) r[i] = 0u;
+      }
+      if (row < g.M) epilogue16(g, row, n0 + cc, r);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(128u));
+  if (threadIdx.x == 0 && s_fail) atomicExch(g.err, 1);
+}
+
 // the same product on the CUDA cores (FP32 accumulation), as a cross-check
 __global__ void k_gemm_simt(GemmArgs g) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x, row = blockIdx.y;
@@ -397,6 +567,44 @@ __global__ void k_gemm_simt(GemmArgs g) {
 }
 
 int *g_err_dev[16] = {};
+
+// cuTensorMapEncodeTiled, found through the runtime (the library does not
+// link the driver library itself)
+using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                 const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                 const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_tiled() {
+  static EncodeTiled fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiled>(p);
+    cudaGetLastError();
+  }
+  return fn;
+}
+
+// a K-major bf16 operand (rows x K, row stride `ld` elements) as a tensor map
+// of 64 x 128 boxes with the 128-byte swizzle; false if it cannot be encoded
+bool operand_map(CUtensorMap *m, const void *base, int rows, int K, long ld) {
+  EncodeTiled enc = encode_tiled();
+  if (!enc) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)kTileK, (cuuint32_t)kTileM};
+  const cuuint32_t estr[2] = {1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides,
+             box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
 
 }  // namespace
 }  // namespace op2b
@@ -468,6 +676,34 @@ extern "C" int op2b_gemm_bf16(int M, int N, int K, const void *A, long a_m, long
     return -1;
   }
   g.k_per_split = kps;
+  dim3 grid((M + kTileM - 1) / kTileM, (N + kTileN - 1) / kTileN, split_k);
+  // the TMA-fed kernel for k-contiguous operands (engine 2 asks for it;
+  // engine 0 takes it when the option gemm_tma is on)
+  const bool kmajor = a_k == 1 && b_k == 1;
+  if (kmajor && (engine == 2 || (engine == 0 && rt().opt_gemm_tma))) {
+    CUtensorMap ta, tb;
+    if (operand_map(&ta, A, M, K, a_m) && operand_map(&tb, B, N, K, b_n)) {
+      const size_t smem_t = (size_t)kTmaStages * 2 * kStageBytes + 1024;
+      static bool attr_t[16] = {};
+      if (!attr_t[dev]) {
+        if (!cuda_ok(cudaFuncSetAttribute(k_gemm_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem_t),
+                     "op2b_gemm_bf16: shared memory attribute"))
+          return -1;
+        attr_t[dev] = true;
+      }
+      k_gemm_tma<<<grid, kThreads, smem_t, s>>>(g, ta, tb);
+      if (rt().initialised) rt().launches++;
+      return cuda_ok(cudaGetLastError(), "op2b_gemm_bf16") ? 0 : -1;
+    }
+    if (engine == 2) {
+      set_error("op2b_gemm_bf16: the operands cannot be described as tensor maps");
+      return -1;
+    }
+  } else if (engine == 2) {
+    set_error("op2b_gemm_bf16: engine 2 (TMA) needs k-contiguous A and B");
+    return -1;
+  }
   const size_t smem = 4 * (size_t)kStageBytes + 1024;
   static bool attr[16] = {};
   if (!attr[dev]) {
@@ -477,7 +713,6 @@ extern "C" int op2b_gemm_bf16(int M, int N, int K, const void *A, long a_m, long
       return -1;
     attr[dev] = true;
   }
-  dim3 grid((M + kTileM - 1) / kTileM, (N + kTileN - 1) / kTileN, split_k);
   k_gemm_tc<<<grid, kThreads, smem, s>>>(g);
   if (rt().initialised) rt().launches++;
   return cuda_ok(cudaGetLastError(), "op2b_gemm_bf16") ? 0 : -1;

@@ -423,6 +423,7 @@ void op_exit(void) {
   r.opt_plan_mode = d.opt_plan_mode;
   r.opt_atomic_seg = d.opt_atomic_seg;
   r.ring_used = 0;
+  r.opt_gemm_tma = d.opt_gemm_tma;
   r.opt_check_plans = d.opt_check_plans;
 }
 
@@ -1021,6 +1022,8 @@ int op2b_set_option(const char *key, long value) {
     r.opt_plan_mode = (int)value;
   } else if (k == "atomic_segmented") {
     r.opt_atomic_seg = value != 0;
+  } else if (k == "gemm_tma") {
+    r.opt_gemm_tma = value != 0;
   } else if (k == "gather_kernel") {
     if (value < 1 || value > 7) {
       set_error("op2b_set_option: gather_kernel must be 1 (csr), 2 (lanes), 3 (cell4), 4 "
@@ -1090,6 +1093,7 @@ long op2b_get_option(const char *key) {
   if (k == "plan_mode") return r.opt_plan_mode;
   if (k == "atomic_segmented") return r.opt_atomic_seg;
   if (k == "ring_used") return r.ring_used;  // read-only
+  if (k == "gemm_tma") return r.opt_gemm_tma;
   if (k == "gather_kernel") return r.opt_gather_kernel;
   if (k == "pipe_block") return r.opt_pipe_block;
   if (k == "pipe_hints") return r.opt_pipe_hints;

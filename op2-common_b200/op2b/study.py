@@ -2,7 +2,8 @@
 
   python -m op2b.study mixed-error [--I 2400 --J 1200 --iters 2000]
   python -m op2b.study mixed-ttt   [--I 480 --J 240 --tol 1e-5]
-  python -m op2b.study batch       [--n 64 --tol 1e-6 --plain api|graph|none]
+  python -m op2b.study batch       [--n 64 --tol 1e-6 --plain api|graph|none
+                                    --plain-subset K --subset-seed S]
 
 Each prints one JSON object per line.
 
@@ -204,6 +205,33 @@ def batch(a):
     _emit(out)
     if a.plain == "none":
         return
+    batched_ms, batched_wall, subset = ms, run_s, list(range(len(specs)))
+    if a.plain_subset and a.plain_subset < len(specs):
+        # plain FP64 on a seeded random subset of the same instances, against
+        # the batched form on that subset alone (same tolerance)
+        rng = np.random.default_rng(a.subset_seed)
+        subset = sorted(int(i) for i in rng.choice(len(specs), a.plain_subset, replace=False))
+        sub = [specs[i] for i in subset]
+        L.op_init()
+        try:
+            b = AirfoilBatch(sub, fp32=True)
+            tune_sub = b.tune(iters=a.tune_iters)
+            b.set("tol", a.tol)
+            b.set("promote_tol", a.promote)
+            t1 = time.perf_counter()
+            active_sub, batched_ms = b.run(a.max_iter, check_every=a.check_every)
+            batched_wall = time.perf_counter() - t1
+            st_sub = b.stats()
+            b.close()
+        finally:
+            L.op_exit()
+        _emit({"study": "batch-subset", "subset": subset,
+               "cells": [int(specs[i]["I"] * specs[i]["J"]) for i in subset],
+               "batched": {"device_ms": batched_ms, "run_wall_s": batched_wall,
+                           "unconverged": int(active_sub),
+                           "iterations": st_sub["iters"].tolist(),
+                           "tuner": tune_sub.strip().splitlines()[-1]}})
+        specs = sub
     # the same instances one after another in plain FP64: through the OP2 API
     # (op_par_loop calls from the host), or on the same engine one instance at
     # a time (CUDA-graph iterations, no batching)
@@ -223,11 +251,12 @@ def batch(a):
             worst = max(worst, r["rms"] / (a.tol * probe["rms1"]))
         seq_wall += time.perf_counter() - t0
         seq_it.append(r["iterations"])
-    _emit({"study": "batch-vs-plain", "plain": a.plain, "instances": a.n, "tol": a.tol,
+    _emit({"study": "batch-vs-plain", "plain": a.plain, "instances": a.n,
+           "compared_instances": subset, "tol": a.tol,
            "plain_sequential": {"device_ms": seq_ms, "wall_s": seq_wall, "iterations": seq_it,
                                 "max_final_rms_over_tol": worst},
-           "batched_device_ms": ms, "time_ratio": ms / seq_ms,
-           "wall_ratio": run_s / seq_wall})
+           "batched_device_ms": batched_ms, "time_ratio": batched_ms / seq_ms,
+           "wall_ratio": batched_wall / seq_wall})
 
 
 def main(argv=None):
@@ -263,6 +292,10 @@ def main(argv=None):
     p.add_argument("--plain", default="api", choices=["api", "graph", "none"],
                    help="sequential plain FP64 baseline: through the OP2 API, on the engine "
                         "one instance at a time, or none")
+    p.add_argument("--plain-subset", type=int, default=0,
+                   help="compare on a seeded random subset of this many instances (the "
+                        "batched form re-run on the subset alone); 0 = all")
+    p.add_argument("--subset-seed", type=int, default=0)
     a = ap.parse_args(argv)
     from . import build
     build.build()
