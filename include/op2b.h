@@ -275,6 +275,16 @@ void *op2b_get_stream(void);
 /* Block until every launched kernel has finished; returns a CUDA error code. */
 int op2b_synchronize(void);
 
+/* Halo exchange of a partitioned mesh, device side (replaces the packing of
+ * op_exchange_halo, op2/src/mpi/op_mpi_rt_support.cpp:61-200, and its CUDA
+ * gather/scatter kernels, op2/src/mpi/op_mpi_cuda_kernels.cu:44-136).
+ * op2b_dat_pack: buf (device) receives rows rows[0..n) of dat, one row of
+ * dat->size bytes after the other.  op2b_dat_unpack: rows rows[0..n) of dat
+ * (or, rows NULL, the contiguous rows first .. first+n-1) receive the
+ * buffer's rows.  Asynchronous on the library's stream; 0 or -1. */
+int op2b_dat_pack(op_dat dat, const int *rows, int n, void *buf);
+int op2b_dat_unpack(op_dat dat, const int *rows, int first, int n, const void *buf);
+
 /* The update loop (q = qold - res/adt, res = 0, rms += sum of del^2, maxerr
  * and errloc from the largest del^2) for callers that cannot allocate device
  * memory: an application whose device memory is all held by its own pool, or

@@ -128,6 +128,9 @@ _SIGS = {
     "op2b_get_stream": (ctypes.c_void_p, []),
     "op2b_synchronize": (ctypes.c_int, []),
     "op2b_update_noalloc": (ctypes.c_int, [ctypes.c_int] + [ctypes.c_void_p] * 8),
+    "op2b_dat_pack": (ctypes.c_int, [op_dat, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "op2b_dat_unpack": (ctypes.c_int, [op_dat, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_void_p]),
     "op_profile_start": (None, [ctypes.c_char_p]),
     "op_profile_enter": (None, [ctypes.c_char_p]),
     "op_profile_enter_kernel": (None, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p]),
