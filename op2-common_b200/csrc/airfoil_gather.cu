@@ -630,13 +630,18 @@ __device__ __forceinline__ void ring_range(int c, int span, int ncell, int &rs, 
   re = min(rs + span, ncell);
 }
 
-// a slot's flux is computed by its cell unless the other cell is earlier in
-// the same range (then that cell computed it)
+// a slot's flux is read from the ring when the other cell is earlier in the
+// same range (that cell computed it), and put into the ring when the other
+// cell is later in the range; with the other cell outside the range, the
+// cell computes it for itself alone (kept in its tile's scratch, not the ring)
 __device__ __forceinline__ bool ring_consumes(int c, int nb, int rs, int re) {
   return nb >= rs && nb < re && nb < c;
 }
+__device__ __forceinline__ bool ring_produces(int c, int nb, int rs, int re) {
+  return nb >= rs && nb < re && nb > c;
+}
 
-// fluxes each cell computes
+// fluxes each cell puts into the ring
 __global__ void k_ring_count(int ncell, int span, const int4 *rec_o, const unsigned *meta,
                              int *cnt) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -648,7 +653,7 @@ __global__ void k_ring_count(int ncell, int span, const int4 *rec_o, const unsig
   const unsigned m = meta[c];
   int n = 0;
   for (int s = 0; s < 4; s++)
-    if ((m >> (8 * s)) & 1u) n += ring_consumes(c, o[s], rs, re) ? 0 : 1;
+    if ((m >> (8 * s)) & 1u) n += ring_produces(c, o[s], rs, re) ? 1 : 0;
   cnt[c] = n;
 }
 
@@ -672,9 +677,13 @@ __global__ void k_ring_fill(int ncell, int span, int nt, const int4 *rec_o, cons
   for (int s = 0; s < 4; s++) {
     if (!((m >> (8 * s)) & 1u)) continue;
     const int nb = o[s];
-    if (!ring_consumes(c, nb, rs, re)) {
+    if (ring_produces(c, nb, rs, re)) {
       const long long k = pre[c] - base + rank++;
       f[s] = (unsigned)(k & (OP2B_RING_ENTRIES - 1));
+      continue;
+    }
+    if (!ring_consumes(c, nb, rs, re)) {  // the other cell outside the range
+      f[s] = 0x4000u;
       continue;
     }
     const int4 p4 = rec_o[nb];
@@ -687,7 +696,7 @@ __global__ void k_ring_fill(int ncell, int span, int nt, const int4 *rec_o, cons
         hits++;
         found = prank;
       }
-      if (!ring_consumes(nb, po[t], rs, re)) prank++;
+      if (ring_produces(nb, po[t], rs, re)) prank++;
     }
     const long long k = pre[nb] - base + found;
     const int tile = (c - rs) / nt;

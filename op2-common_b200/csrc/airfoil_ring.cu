@@ -13,9 +13,12 @@
 // it in tiles of NT cells, one cell per thread:
 //
 //   phase A  every cell computes the flux of each of its edges whose other
-//            cell comes later in the range or lies outside it, and puts the
-//            flux (in the edge's own orientation) into a ring of
-//            OP2B_RING_ENTRIES fluxes in shared memory;
+//            cell comes later in the range, and puts the flux (in the edge's
+//            own orientation) into a ring of OP2B_RING_ENTRIES fluxes in
+//            shared memory; the flux of an edge to a cell outside the range
+//            it computes for itself into its own scratch entries (kept out of
+//            the ring, whose entries then live at most ~3000 fluxes on a
+//            renumbered mesh);
 //   phase B  every cell adds the fluxes of its edges from the ring in slot
 //            order (its edges in increasing edge order) -- its own, and those
 //            an earlier cell of the range computed -- starting from res[c]
@@ -105,9 +108,24 @@ __device__ __forceinline__ void ring_load(RingOps<T> &d, int c, const int4 *__re
   }
 }
 
-// phase A: the fluxes this cell computes, into the ring (edge orientation)
-template <typename T>
-__device__ __forceinline__ void ring_produce(const RingOps<T> &d, T ric, T pc, T *ring,
+// The tile scratch for fluxes to cells outside the range: value j of slot s
+// of thread t at local[(4 s + j) * NT + t] (consecutive threads, consecutive
+// words: no bank conflicts)
+template <typename T, int NT>
+__device__ __forceinline__ void local_st(T *local, int s, const T *f) {
+#pragma unroll
+  for (int j = 0; j < 4; j++) local[(4 * s + j) * NT + threadIdx.x] = f[j];
+}
+template <typename T, int NT>
+__device__ __forceinline__ void local_ld(const T *local, int s, T *f) {
+#pragma unroll
+  for (int j = 0; j < 4; j++) f[j] = local[(4 * s + j) * NT + threadIdx.x];
+}
+
+// phase A: the fluxes this cell computes (edge orientation): into the ring,
+// or, for an edge to a cell outside the range, into the tile scratch
+template <typename T, int NT>
+__device__ __forceinline__ void ring_produce(const RingOps<T> &d, T ric, T pc, T *ring, T *local,
                                              const AirConst<T> &k) {
 #pragma unroll
   for (int s = 0; s < 4; s++) {
@@ -123,14 +141,17 @@ __device__ __forceinline__ void ring_produce(const RingOps<T> &d, T ric, T pc, T
       air_flux_prim<T>(x1x, x1y, x2x, x2y, d.qo[s], d.qc, rio, po, ric, pc, d.ao[s], d.ac, k, f);
     else
       air_flux_prim<T>(x1x, x1y, x2x, x2y, d.qc, d.qo[s], ric, pc, rio, po, d.ac, d.ao[s], k, f);
-    Vec<T>::st4_shared(ring + 4 * (f16 & (OP2B_RING_ENTRIES - 1)), f);
+    if (f16 & 0x4000u)
+      local_st<T, NT>(local, s, f);
+    else
+      Vec<T>::st4_shared(ring + 4 * (f16 & (OP2B_RING_ENTRIES - 1)), f);
   }
 }
 
 // phase B: this cell's sums in slot order, then its boundary increments
-template <typename T, bool BRES>
+template <typename T, int NT, bool BRES>
 __device__ __forceinline__ void ring_sum(const RingOps<T> &d, int c, T ric, T pc,
-                                         const T *ring, T *__restrict__ res,
+                                         const T *ring, const T *local, T *__restrict__ res,
                                          const AirConst<T> &k) {
   T acc[4] = {d.rs[0], d.rs[1], d.rs[2], d.rs[3]};
 #pragma unroll
@@ -138,7 +159,11 @@ __device__ __forceinline__ void ring_sum(const RingOps<T> &d, int c, T ric, T pc
     const unsigned m = (d.meta >> (8 * s)) & 0xffu;
     if (!(m & 1u)) continue;
     T f[4];
-    Vec<T>::ld4_shared(ring + 4 * (ring_field(d.ring, s) & (OP2B_RING_ENTRIES - 1)), f);
+    const unsigned f16 = ring_field(d.ring, s);
+    if (f16 & 0x4000u)
+      local_ld<T, NT>(local, s, f);
+    else
+      Vec<T>::ld4_shared(ring + 4 * (f16 & (OP2B_RING_ENTRIES - 1)), f);
     if (m & 2u) {
 #pragma unroll
       for (int j = 0; j < 4; j++) acc[j] -= f[j];
@@ -179,6 +204,7 @@ k_res_ring(int ncell, int span, const int4 *__restrict__ rec_o, const int4 *__re
            T *__restrict__ res, AirConst<T> k, const int *__restrict__ bound) {
   extern __shared__ __align__(16) unsigned char ring_smem[];
   T *ring = reinterpret_cast<T *>(ring_smem);
+  T *local = ring + 4 * OP2B_RING_ENTRIES;  // the tile scratch (local_st / local_ld)
   const int rs = blockIdx.x * span;
   const int re = min(rs + span, ncell);
   if (rs >= re) return;  // the whole CTA
@@ -195,10 +221,10 @@ k_res_ring(int ncell, int span, const int4 *__restrict__ rec_o, const int4 *__re
     T ric = (T)0, pc = (T)0;
     if (valid) {
       air_prim<T>(cur.qc, k, ric, pc);
-      ring_produce<T>(cur, ric, pc, ring, k);
+      ring_produce<T, NT>(cur, ric, pc, ring, local, k);
     }
     __syncthreads();
-    if (valid) ring_sum<T, BRES>(cur, c, ric, pc, ring, res, k);
+    if (valid) ring_sum<T, NT, BRES>(cur, c, ric, pc, ring, local, res, k);
     __syncthreads();
     cur = nxt;
   }
@@ -208,7 +234,8 @@ template <typename T, bool BRES, bool ZERO>
 cudaError_t launch_ring(const LaunchCtx &ctx, const SlotRecords &s, const int *bound, const T *x,
                         const T *q, const T *adt, T *res, const AirConst<T> &k) {
   constexpr int NT = 256;
-  const size_t smem = sizeof(T) * 4 * (size_t)OP2B_RING_ENTRIES;
+  // the ring, then 4 slots of 4 values a thread for fluxes to cells outside the range
+  const size_t smem = sizeof(T) * 4 * ((size_t)OP2B_RING_ENTRIES + 4 * NT);
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(k_res_ring<T, NT, BRES, ZERO>,

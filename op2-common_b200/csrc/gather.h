@@ -43,10 +43,12 @@ struct SlotRecords {
   // res_calc + bres_calc and res_calc over corner records): cells are split
   // into ring_ctas contiguous ranges of ring_span cells, one per CTA, swept in
   // tiles of ring_nt cells.  16 bits per slot in ring[c] (slots 0-1 in .x,
-  // 2-3 in .y, low half first): bit 15 clear = the cell computes the edge's
-  // flux (its other cell comes later in the range, or lies outside it) and
-  // puts it at entry (bits 0-11) of the CTA's shared-memory ring; bit 15 set
-  // = the flux was put there by the other cell, earlier in the range.
+  // 2-3 in .y, low half first): bits 14-15 clear = the cell computes the
+  // edge's flux (its other cell comes later in the range) and puts it at
+  // entry (bits 0-11) of the CTA's shared-memory ring; bit 15 = the flux was
+  // put there by the other cell, earlier in the range; bit 14 = the other cell
+  // lies outside the range: the cell computes the flux for itself alone
+  // (kept in its tile's scratch, not the ring).
   const uint2 *ring;
   int ring_ctas, ring_span, ring_nt;
 };
