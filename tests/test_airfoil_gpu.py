@@ -175,8 +175,9 @@ def test_flux_ring_is_bit_identical_to_corner_kernel(op2, I, J, renumber):
     shared-memory ring in the same slot order: q, adt and res equal the
     corner kernel's bit for bit, fused with bres_calc and alone, in both
     precisions.  On the renumbered mesh the ring records are built and used;
-    on a randomly numbered large mesh they cannot be (neighbours too far
-    apart) and the corner kernel serves."""
+    on a randomly numbered mesh nearly every neighbour lies outside the
+    cell's range, so the cells compute nearly every flux themselves, and
+    whichever kernel serves, the results are the same."""
     m = M.channel_bump(I, J, seed=7)
     for dtype in (np.float64, np.float32):
         for fuse in (1, 0):
@@ -197,8 +198,6 @@ def test_flux_ring_is_bit_identical_to_corner_kernel(op2, I, J, renumber):
             assert used[0] == 0
             if renumber:
                 assert used[1] == 1, (I, J)
-            elif I * J >= 2400 * 1200:
-                assert used[1] == 0
 
 
 @pytest.mark.parametrize("hints", [0, 1])
