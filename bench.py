@@ -472,10 +472,12 @@ def main():
             keep.append(t)
             return arr
 
-        from op2b.mesh import Mesh
+        from op2b.mesh import Mesh, airfoil_constants
         hm = Mesh(x=pin(m.x.astype(dtype)), cell=pin(m.cell), edge=pin(m.edge),
                   ecell=pin(m.ecell), bedge=pin(m.bedge), becell=pin(m.becell),
                   bound=pin(m.bound))
+        # the initial field (freestream), a host input like the mesh
+        q0 = pin(np.tile(np.asarray(airfoil_constants()["qinf"], dtype), (m.ncell, 1)))
         L.op_init()
         L.set_option("inc_mode", args.inc_mode)
         L.set_option("part_size", args.part_size)
@@ -484,7 +486,7 @@ def main():
         barrier()
         K = max(args.e2e_iters, 1)
         t0 = time.perf_counter()
-        app2 = Airfoil(hm, dtype=dtype)
+        app2 = Airfoil(hm, dtype=dtype, q0=q0)
         ta = time.perf_counter()
         if args.numbering == "rcm":
             app2.renumber()
@@ -513,8 +515,8 @@ def main():
                "h2d_bytes_per_step": int(h2d / K),
                "d2h_bytes_per_step": int(d2h / K),
                "note": f"per iteration of a whole {K}-iteration job through the API: "
-                       "op_decl_* uploads (mesh arrays pinned), op_renumber, the iterations "
-                       "(rms read back after every update), op_fetch_data(q)"}
+                       "op_decl_* uploads (mesh arrays and the initial q pinned), op_renumber, "
+                       "the iterations (rms read back after every update), op_fetch_data(q)"}
         L.op_exit()
 
     # ---------------------------------------------------------- CPU baseline (rank 0, N=1)

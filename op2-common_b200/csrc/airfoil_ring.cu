@@ -67,18 +67,39 @@ __device__ __forceinline__ unsigned ring_field(const uint2 &r, int s) {
   return (s & 1) ? (w >> 16) : (w & 0xffffu);
 }
 
+// a cell's records, loaded a tile before its operands (two tiles ahead of
+// its arithmetic), so one level of gather latency is left in a tile
+struct RingRec {
+  int4 o, cn;
+  unsigned meta;
+  uint2 ring;
+};
+
+__device__ __forceinline__ void ring_rec(RingRec &r, int c, int re, const int4 *__restrict__ rec_o,
+                                         const int4 *__restrict__ rec_cn,
+                                         const unsigned *__restrict__ rec_meta,
+                                         const uint2 *__restrict__ rec_ring) {
+  if (c < re) {
+    r.o = __ldg(rec_o + c);
+    r.cn = __ldg(rec_cn + c);
+    r.meta = __ldg(rec_meta + c);
+    r.ring = __ldg(rec_ring + c);
+  } else {
+    r.o = r.cn = make_int4(0, 0, 0, 0);
+    r.meta = 0u;
+    r.ring = make_uint2(0u, 0u);
+  }
+}
+
 template <typename T, bool BRES, bool ZERO>
-__device__ __forceinline__ void ring_load(RingOps<T> &d, int c, const int4 *__restrict__ rec_o,
-                                          const int4 *__restrict__ rec_cn,
-                                          const unsigned *__restrict__ rec_meta,
-                                          const uint2 *__restrict__ rec_ring,
+__device__ __forceinline__ void ring_load(RingOps<T> &d, int c, const RingRec &rr,
                                           const T *__restrict__ x, const T *__restrict__ q,
                                           const T *__restrict__ adt, const T *__restrict__ res,
                                           const int *__restrict__ bound) {
-  const int4 o4 = __ldg(rec_o + c);
-  const int4 cn = __ldg(rec_cn + c);
-  d.meta = __ldg(rec_meta + c);
-  d.ring = __ldg(rec_ring + c);
+  const int4 o4 = rr.o;
+  const int4 cn = rr.cn;
+  d.meta = rr.meta;
+  d.ring = rr.ring;
   Vec<T>::ld4(q + 4 * (size_t)c, d.qc);
   if constexpr (ZERO) {
 #pragma unroll
@@ -209,15 +230,19 @@ k_res_ring(int ncell, int span, const int4 *__restrict__ rec_o, const int4 *__re
   const int re = min(rs + span, ncell);
   if (rs >= re) return;  // the whole CTA
   RingOps<T> cur, nxt;
-  if (rs + (int)threadIdx.x < re)
-    ring_load<T, BRES, ZERO>(cur, rs + threadIdx.x, rec_o, rec_cn, rec_meta, rec_ring, x, q, adt,
-                             res, bound);
+  RingRec r1, r2;
+  {
+    RingRec r0;
+    ring_rec(r0, rs + threadIdx.x, re, rec_o, rec_cn, rec_meta, rec_ring);
+    ring_rec(r1, rs + NT + threadIdx.x, re, rec_o, rec_cn, rec_meta, rec_ring);
+    if (rs + (int)threadIdx.x < re)
+      ring_load<T, BRES, ZERO>(cur, rs + threadIdx.x, r0, x, q, adt, res, bound);
+  }
   for (int t0 = rs; t0 < re; t0 += NT) {  // the same trip count for every thread
     const int c = t0 + threadIdx.x;
     const bool valid = c < re;
-    if (c + NT < re)
-      ring_load<T, BRES, ZERO>(nxt, c + NT, rec_o, rec_cn, rec_meta, rec_ring, x, q, adt, res,
-                               bound);
+    ring_rec(r2, c + 2 * NT, re, rec_o, rec_cn, rec_meta, rec_ring);
+    if (c + NT < re) ring_load<T, BRES, ZERO>(nxt, c + NT, r1, x, q, adt, res, bound);
     T ric = (T)0, pc = (T)0;
     if (valid) {
       air_prim<T>(cur.qc, k, ric, pc);
@@ -227,6 +252,7 @@ k_res_ring(int ncell, int span, const int4 *__restrict__ rec_o, const int4 *__re
     if (valid) ring_sum<T, NT, BRES>(cur, c, ric, pc, ring, local, res, k);
     __syncthreads();
     cur = nxt;
+    r1 = r2;
   }
 }
 
