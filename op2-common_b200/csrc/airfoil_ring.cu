@@ -131,41 +131,60 @@ __device__ __forceinline__ void ring_load(RingOps<T> &d, int c, const RingRec &r
 
 // The tile scratch for fluxes to cells outside the range: value j of slot s
 // of thread t at local[(4 s + j) * NT + t] (consecutive threads, consecutive
-// words: no bank conflicts)
-template <typename T, int NT>
-__device__ __forceinline__ void local_st(T *local, int s, const T *f) {
-#pragma unroll
-  for (int j = 0; j < 4; j++) local[(4 * s + j) * NT + threadIdx.x] = f[j];
-}
+// words: no bank conflicts); ring_produce writes it, ring_sum reads it
 template <typename T, int NT>
 __device__ __forceinline__ void local_ld(const T *local, int s, T *f) {
 #pragma unroll
   for (int j = 0; j < 4; j++) f[j] = local[(4 * s + j) * NT + threadIdx.x];
 }
 
+// v[s] for a slot index s known only at run time, by selects (no
+// local-memory indexing)
+template <typename V>
+__device__ __forceinline__ V sel4(unsigned s, V v0, V v1, V v2, V v3) {
+  const V lo = (s & 1u) ? v1 : v0;
+  const V hi = (s & 1u) ? v3 : v2;
+  return (s & 2u) ? hi : lo;
+}
+
 // phase A: the fluxes this cell computes (edge orientation): into the ring,
-// or, for an edge to a cell outside the range, into the tile scratch
+// or, for an edge to a cell outside the range, into the tile scratch.  The
+// loop runs over this cell's own computed slots, in slot order, their
+// operands picked by selects: a warp issues as many fluxes as its busiest
+// lane computes (two for most cells of a renumbered mesh), where a loop over
+// the four slot positions would issue four whenever the lanes' computed slots
+// sit at different positions.
 template <typename T, int NT>
 __device__ __forceinline__ void ring_produce(const RingOps<T> &d, T ric, T pc, T *ring, T *local,
                                              const AirConst<T> &k) {
+  unsigned todo = 0;
 #pragma unroll
-  for (int s = 0; s < 4; s++) {
+  for (int s = 0; s < 4; s++)
+    if (((d.meta >> (8 * s)) & 1u) && !(ring_field(d.ring, s) & 0x8000u)) todo |= 1u << s;
+  while (todo) {
+    const unsigned s = (unsigned)__ffs(todo) - 1u;
+    todo &= todo - 1u;
     const unsigned m = (d.meta >> (8 * s)) & 0xffu;
-    const unsigned f16 = ring_field(d.ring, s);
-    if (!(m & 1u) || (f16 & 0x8000u)) continue;
+    const unsigned f16 = ((s < 2u ? d.ring.x : d.ring.y) >> (16 * (s & 1u))) & 0xffffu;
     const unsigned a = (m >> 2) & 3u, b = (m >> 4) & 3u;
     const T x1x = ring_corner<T>(d.xn, a, 0), x1y = ring_corner<T>(d.xn, a, 1);
     const T x2x = ring_corner<T>(d.xn, b, 0), x2y = ring_corner<T>(d.xn, b, 1);
+    T qo[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) qo[j] = sel4<T>(s, d.qo[0][j], d.qo[1][j], d.qo[2][j], d.qo[3][j]);
+    const T ao = sel4<T>(s, d.ao[0], d.ao[1], d.ao[2], d.ao[3]);
     T f[4], rio, po;
-    air_prim<T>(d.qo[s], k, rio, po);
+    air_prim<T>(qo, k, rio, po);
     if (m & 2u)  // this cell is the edge's second cell
-      air_flux_prim<T>(x1x, x1y, x2x, x2y, d.qo[s], d.qc, rio, po, ric, pc, d.ao[s], d.ac, k, f);
+      air_flux_prim<T>(x1x, x1y, x2x, x2y, qo, d.qc, rio, po, ric, pc, ao, d.ac, k, f);
     else
-      air_flux_prim<T>(x1x, x1y, x2x, x2y, d.qc, d.qo[s], ric, pc, rio, po, d.ac, d.ao[s], k, f);
-    if (f16 & 0x4000u)
-      local_st<T, NT>(local, s, f);
-    else
+      air_flux_prim<T>(x1x, x1y, x2x, x2y, d.qc, qo, ric, pc, rio, po, d.ac, ao, k, f);
+    if (f16 & 0x4000u) {
+#pragma unroll
+      for (int j = 0; j < 4; j++) local[(4 * s + j) * NT + threadIdx.x] = f[j];
+    } else {
       Vec<T>::st4_shared(ring + 4 * (f16 & (OP2B_RING_ENTRIES - 1)), f);
+    }
   }
 }
 
