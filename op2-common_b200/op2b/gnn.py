@@ -204,6 +204,11 @@ def edge_features(mesh: Mesh, g=None):
 
 
 # ---------------------------------------------------------------- the network
+# products with k-contiguous operands (the forward MLP layers) run on the
+# TMA-fed tensor-core kernel; False keeps the register-staged one everywhere
+GEMM_TMA = True
+
+
 class GraphNet:
     """Device-resident network: FP32 master parameters, bf16 copies, AdamW
     moments, gradient; forward / backward / step through the C ABI."""
@@ -229,6 +234,7 @@ class GraphNet:
             np.asarray(norm, np.float64)
         self._ws = {}
         self.launches = 0
+        self.gemm_tma = GEMM_TMA
 
     # -- helpers ------------------------------------------------------------
     @property
@@ -242,8 +248,11 @@ class GraphNet:
 
     def _gemm(self, M, N, K, A, a_m, a_k, B, b_n, b_k, C, ldc, epi, bias=None, Z=None, R=None,
               ldr=0, split=1):
+        # k-contiguous operands go to the TMA-fed kernel (engine 2) unless
+        # gemm_tma is off; the others to the register-staged one (engine 0)
+        engine = 2 if (self.gemm_tma and a_k == 1 and b_k == 1) else 0
         _call("op2b_gemm_bf16", M, N, K, A, a_m, a_k, B, b_n, b_k, C, ldc, epi, bias, Z, R, ldr,
-              split, 0, self.stream)
+              split, engine, self.stream)
         self.launches += 1
 
     def _split_for(self, rows, ntiles):

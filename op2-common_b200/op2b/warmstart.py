@@ -309,7 +309,11 @@ def main(argv=None):
     ap.add_argument("--synthetic", action="store_true",
                     help="random targets instead of solved fields (timing/profiling of training)")
     ap.add_argument("--log-every", type=int, default=100)
+    ap.add_argument("--gemm-tma", type=int, default=1,
+                    help="1: forward products on the TMA-fed tensor-core GEMM; 0: all on the "
+                         "register-staged one")
     a = ap.parse_args(argv)
+    G.GEMM_TMA = bool(a.gemm_tma)
     log = lambda s: print(s, flush=True)
     report = dict(args=vars(a))
     if a.load:
