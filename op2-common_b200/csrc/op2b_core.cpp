@@ -22,6 +22,8 @@
 
 #include <algorithm>
 #include <chrono>
+#include <condition_variable>
+#include <mutex>
 #include <cmath>
 #include <cstdarg>
 #include <cstdint>
@@ -65,9 +67,86 @@ bool cuda_ok(cudaError_t e, const char *what) {
   return false;
 }
 
+// A pool of host threads for large memcpys, started at the first use and
+// kept for the process: copying into freshly allocated memory is bound by
+// its page faults, which the kernel serves in parallel, and a staged
+// download copies many chunks in a row (starting threads per chunk would
+// cost more than some of the copies).
+namespace {
+struct CopyPool {
+  std::mutex user;  // one job at a time (callers on several host threads wait their turn)
+  std::mutex mu;
+  std::condition_variable go, done;
+  std::vector<std::thread> workers;
+  // the current job: worker i copies part i + 1 (the caller part 0)
+  char *dst = nullptr;
+  const char *src = nullptr;
+  size_t bytes = 0, part = 0;
+  unsigned parts = 0, pending = 0;
+  unsigned long long gen = 0;
+  bool quit = false;
+
+  void start(unsigned n) {
+    for (unsigned i = (unsigned)workers.size(); i < n; i++)
+      workers.emplace_back([this, i] {
+        unsigned long long seen = 0;
+        for (;;) {
+          char *d;
+          const char *sp;
+          size_t b, e;
+          {
+            std::unique_lock<std::mutex> lk(mu);
+            go.wait(lk, [&] { return quit || gen != seen; });
+            if (quit) return;
+            seen = gen;
+            if (i + 1 >= parts) continue;  // not part of this job
+            d = dst;
+            sp = src;
+            b = (i + 1) * part;
+            e = std::min(bytes, b + part);
+          }
+          if (b < e) memcpy(d + b, sp + b, e - b);
+          std::lock_guard<std::mutex> lk(mu);
+          if (--pending == 0) done.notify_one();
+        }
+      });
+  }
+  ~CopyPool() {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      quit = true;
+    }
+    go.notify_all();
+    for (auto &t : workers) t.join();
+  }
+  void copy(void *d, const void *sp, size_t n, unsigned nt) {
+    std::lock_guard<std::mutex> one(user);
+    start(nt - 1);
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      dst = (char *)d;
+      src = (const char *)sp;
+      bytes = n;
+      parts = nt;
+      part = ((n + nt - 1) / nt + 4095) & ~(size_t)4095;
+      pending = nt - 1;
+      gen++;
+    }
+    go.notify_all();
+    memcpy(d, sp, std::min(part, n));
+    std::unique_lock<std::mutex> lk(mu);
+    done.wait(lk, [&] { return pending == 0; });
+  }
+};
+
+CopyPool &copy_pool() {
+  static CopyPool p;
+  return p;
+}
+}  // namespace
+
 // memcpy of a large host array by up to `host_threads` threads (option,
-// default 8, at most the host's): copying into freshly allocated memory is bound by its page
-// faults, which the kernel serves in parallel
+// default 8, at most the host's)
 static void host_copy(void *dst, const void *src, size_t bytes) {
   const size_t kParallel = (size_t)8 << 20;
   unsigned nt = std::min((unsigned)std::max(1, rt().opt_host_threads),
@@ -76,52 +155,61 @@ static void host_copy(void *dst, const void *src, size_t bytes) {
     memcpy(dst, src, bytes);
     return;
   }
-  const size_t chunk = ((bytes + nt - 1) / nt + 4095) & ~(size_t)4095;
-  std::vector<std::thread> th;
-  for (unsigned i = 1; i < nt; i++) {
-    const size_t b = i * chunk;
-    if (b >= bytes) break;
-    const size_t e = std::min(bytes, b + chunk);
-    th.emplace_back([=] { memcpy((char *)dst + b, (const char *)src + b, e - b); });
-  }
-  memcpy(dst, src, std::min(chunk, bytes));
-  for (auto &t : th) t.join();
+  copy_pool().copy(dst, src, bytes, nt);
 }
 
-bool download_host(void *dst, const void *src_d, size_t bytes, const char *what) {
+// Device -> host copies of several arrays, one pipeline through the pinned
+// staging buffers: chunk k of the whole list goes through buffer k % 2, its
+// DMA under way while the host threads empty the other buffer; a pinned
+// destination takes its DMA directly.  Synchronous.
+bool download_host_many(const std::vector<HostDownload> &jobs, const char *what) {
   Runtime &r = rt();
   const size_t kChunk = (size_t)16 << 20;
-  cudaPointerAttributes pa{};
-  const bool pinned = cudaPointerGetAttributes(&pa, dst) == cudaSuccess &&
-                      pa.type == cudaMemoryTypeHost;
-  cudaGetLastError();
-  if (bytes <= kChunk || pinned) {  // a pinned destination takes the DMA directly
-    return cuda_ok(cudaMemcpyAsync(dst, src_d, bytes, cudaMemcpyDeviceToHost, r.stream), what) &&
-           cuda_ok(cudaStreamSynchronize(r.stream), what);
+  struct Piece {
+    char *dst;
+    const char *src;
+    size_t len;
+  };
+  std::vector<Piece> pieces;
+  for (const auto &j : jobs) {
+    if (!j.bytes) continue;
+    cudaPointerAttributes pa{};
+    const bool pinned = cudaPointerGetAttributes(&pa, j.dst) == cudaSuccess &&
+                        pa.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    if (pinned || j.bytes <= ((size_t)1 << 20)) {  // straight DMA, on the stream in order
+      if (!cuda_ok(cudaMemcpyAsync(j.dst, j.src_d, j.bytes, cudaMemcpyDeviceToHost, r.stream),
+                   what))
+        return false;
+      continue;
+    }
+    for (size_t off = 0; off < j.bytes; off += kChunk)
+      pieces.push_back({(char *)j.dst + off, (const char *)j.src_d + off,
+                        std::min(kChunk, j.bytes - off)});
   }
+  if (pieces.empty()) return cuda_ok(cudaStreamSynchronize(r.stream), what);
   if (!r.stage) {
     if (!cuda_ok(cudaHostAlloc((void **)&r.stage, 2 * kChunk, cudaHostAllocDefault), what))
       return false;
     for (auto &e : r.stage_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   }
-  // chunk k goes through buffer k % 2: the copy of chunk i + 1 is under way
-  // while the host threads empty buffer i % 2
-  const size_t n = (bytes + kChunk - 1) / kChunk;
   auto issue = [&](size_t k) {
-    const size_t off = k * kChunk, len = std::min(kChunk, bytes - off);
-    return cuda_ok(cudaMemcpyAsync(r.stage + (k % 2) * kChunk, (const char *)src_d + off, len,
+    return cuda_ok(cudaMemcpyAsync(r.stage + (k % 2) * kChunk, pieces[k].src, pieces[k].len,
                                    cudaMemcpyDeviceToHost, r.stream),
                    what) &&
            cuda_ok(cudaEventRecord(r.stage_ev[k % 2], r.stream), what);
   };
   if (!issue(0)) return false;
-  for (size_t i = 0; i < n; i++) {
-    if (i + 1 < n && !issue(i + 1)) return false;
+  for (size_t i = 0; i < pieces.size(); i++) {
+    if (i + 1 < pieces.size() && !issue(i + 1)) return false;
     if (!cuda_ok(cudaEventSynchronize(r.stage_ev[i % 2]), what)) return false;
-    const size_t off = i * kChunk;
-    host_copy((char *)dst + off, r.stage + (i % 2) * kChunk, std::min(kChunk, bytes - off));
+    host_copy(pieces[i].dst, r.stage + (i % 2) * kChunk, pieces[i].len);
   }
-  return true;
+  return cuda_ok(cudaStreamSynchronize(r.stream), what);
+}
+
+bool download_host(void *dst, const void *src_d, size_t bytes, const char *what) {
+  return download_host_many({HostDownload{dst, src_d, bytes}}, what);
 }
 
 // Host memory for large copies: 2 MiB aligned with a transparent-huge-page

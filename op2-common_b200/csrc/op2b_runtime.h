@@ -207,6 +207,13 @@ bool cuda_ok(cudaError_t e, const char *what);
 // Device -> pageable host copy on the library stream, through pinned buffers
 // with the host-side copies spread over threads (synchronous).
 bool download_host(void *dst, const void *src_d, size_t bytes, const char *what);
+// several device -> host copies in one staged pipeline (synchronous)
+struct HostDownload {
+  void *dst;
+  const void *src_d;
+  size_t bytes;
+};
+bool download_host_many(const std::vector<HostDownload> &jobs, const char *what);
 int type_bytes(const char *type);
 bool is_real(const char *type, int bytes);
 

@@ -1003,19 +1003,19 @@ int renumber(op_map base, long stats[4]) {
   // host copies of the maps, and of the dats on reordered sets, follow the
   // device (the reference reorders dat->data and map->map on the host,
   // op_renumber.cpp:180-200)
+  std::vector<HostDownload> mirrors;
   for (auto &mp : r.maps) {
     op_map m = mp.get();
     if (m && m->map_d && m->map)
-      ok &= download_host(m->map, m->map_d, sizeof(int) * (size_t)m->from->size * m->dim,
-                          "op_renumber: host maps");
+      mirrors.push_back({m->map, m->map_d, sizeof(int) * (size_t)m->from->size * m->dim});
   }
   for (auto &dp : r.dats) {
     op_dat d = dp.get();
     // (a copy of zeros stays zeros in any order)
     if (d && d->data && d->data_d && perm[d->set->index] && !r.zero_mirror.count(d))
-      ok &= download_host(d->data, d->data_d, (size_t)d->set->size * d->size,
-                          "op_renumber: host dats");
+      mirrors.push_back({d->data, d->data_d, (size_t)d->set->size * d->size});
   }
+  ok &= download_host_many(mirrors, "op_renumber: host copies of maps and dats");
   // compose with earlier renumberings: original -> current
   for (auto &sp : r.sets) {
     op_set set = sp.get();
