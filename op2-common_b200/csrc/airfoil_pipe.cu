@@ -470,7 +470,74 @@ __device__ __forceinline__ void compute_corner(const CornerOps<T> &d, int c, T *
   Vec<T>::st4(res + 4 * (size_t)c, acc);
 }
 
-template <typename T, int NT, int MINB>
+// compute_corner with the slots' fluxes free of branches, so the four
+// (independent) flux evaluations of a cell can overlap in the FP64 pipe
+// instead of running one after another.  Each slot selects its operands in
+// the edge's order -- (q, ri, p, adt) of the edge's first cell, then of its
+// second -- and calls air_flux_prim on them, so f is the same value the
+// branchy form computes; the cell then adds f (first cell) or adds -f
+// (second cell: a - b is a + (-b) in IEEE arithmetic), and a slot that is
+// not an interior edge keeps the sum by a select.  The sums run in slot
+// order, as before.
+template <typename T, bool BRES = false>
+__device__ __forceinline__ void compute_corner_il(const CornerOps<T> &d, int c,
+                                                  T *__restrict__ res, const AirConst<T> &k) {
+  T ric, pc;
+  air_prim<T>(d.qc, k, ric, pc);
+  T f[4][4];
+#pragma unroll
+  for (int s = 0; s < 4; s++) {
+    const unsigned m = (d.meta >> (8 * s)) & 0xffu;
+    const unsigned a = (m >> 2) & 3u, b = (m >> 4) & 3u;
+    const bool second = (m & 2u) != 0;
+    T rio, po;
+    air_prim<T>(d.qo[s], k, rio, po);
+    T q1[4], q2[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      q1[j] = second ? d.qo[s][j] : d.qc[j];
+      q2[j] = second ? d.qc[j] : d.qo[s][j];
+    }
+    air_flux_prim<T>(corner<T>(d.xn, a, 0), corner<T>(d.xn, a, 1), corner<T>(d.xn, b, 0),
+                     corner<T>(d.xn, b, 1), q1, q2, second ? rio : ric, second ? po : pc,
+                     second ? ric : rio, second ? pc : po, second ? d.ao[s] : d.ac,
+                     second ? d.ac : d.ao[s], k, f[s]);
+  }
+  T acc[4] = {d.rs[0], d.rs[1], d.rs[2], d.rs[3]};
+#pragma unroll
+  for (int s = 0; s < 4; s++) {
+    const unsigned m = (d.meta >> (8 * s)) & 0xffu;
+    const bool interior = (m & 1u) != 0, second = (m & 2u) != 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const T sum = acc[j] + (second ? -f[s][j] : f[s][j]);
+      acc[j] = interior ? sum : acc[j];
+    }
+  }
+  if constexpr (BRES) {
+    if (d.meta & 0x40404040u) {
+#pragma unroll
+      for (int s = 0; s < 4; s++) {
+        const unsigned m = (d.meta >> (8 * s)) & 0xffu;
+        if (!(m & 0x40u)) continue;
+        const unsigned a = (m >> 2) & 3u, b = (m >> 4) & 3u;
+        T rr[4];
+        air_bflux_prim<T>(corner<T>(d.xn, a, 0), corner<T>(d.xn, a, 1), corner<T>(d.xn, b, 0),
+                          corner<T>(d.xn, b, 1), d.qc, ric, pc, d.ac, d.bnd[s], k, rr);
+        if (d.bnd[s] == 1) {
+          acc[1] += rr[1];
+          acc[2] += rr[2];
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; j++) acc[j] += rr[j];
+        }
+      }
+    }
+  }
+  Vec<T>::st4(res + 4 * (size_t)c, acc);
+}
+
+template <typename T, int NT, int MINB, bool IL = false>
 __global__ void __launch_bounds__(NT, MINB)
 k_res_gather_corner(int ncell, const int4 *__restrict__ rec_o, const int4 *__restrict__ rec_cn,
                     const unsigned *__restrict__ rec_meta, const T *__restrict__ x,
@@ -488,7 +555,8 @@ k_res_gather_corner(int ncell, const int4 *__restrict__ rec_o, const int4 *__res
   for (; c < ncell; c += G) {
     const CornerRec r2 = load_crec(rec_o, rec_cn, rec_meta, c + 2 * G, ncell);
     if (c + G < ncell) load_corner_cell<T>(nxt, c + G, r1, x, q, adt, res);
-    compute_corner<T>(cur, c, res, k);
+    if constexpr (IL) compute_corner_il<T>(cur, c, res, k);
+    else compute_corner<T>(cur, c, res, k);
     cur = nxt;
     r1 = r2;
   }
@@ -497,7 +565,7 @@ k_res_gather_corner(int ncell, const int4 *__restrict__ rec_o, const int4 *__res
 // res_calc and the bres_calc that follows it in one launch (the runtime
 // defers res_calc until the next loop call; when that is bres_calc on the
 // same res, q, adt and x, this kernel runs instead of both)
-template <typename T, int NT, bool ZERO = false>
+template <typename T, int NT, bool ZERO = false, bool IL = false>
 __global__ void __launch_bounds__(NT, 1)
 k_res_bres_corner(int ncell, const int4 *__restrict__ rec_o, const int4 *__restrict__ rec_cn,
                   const unsigned *__restrict__ rec_meta, const T *__restrict__ x,
@@ -515,7 +583,8 @@ k_res_bres_corner(int ncell, const int4 *__restrict__ rec_o, const int4 *__restr
   for (; c < ncell; c += G) {
     const CornerRec r2 = load_crec(rec_o, rec_cn, rec_meta, c + 2 * G, ncell);
     if (c + G < ncell) load_corner_cell<T, true, ZERO>(nxt, c + G, r1, x, q, adt, res, bl);
-    compute_corner<T, true>(cur, c, res, k);
+    if constexpr (IL) compute_corner_il<T, true>(cur, c, res, k);
+    else compute_corner<T, true>(cur, c, res, k);
     cur = nxt;
     r1 = r2;
   }
@@ -542,8 +611,13 @@ cudaError_t launch_corner(K kern, int nt, const LaunchCtx &ctx, const SlotRecord
 template <typename T>
 cudaError_t launch_res_calc_gather_corner(const LaunchCtx &ctx, const SlotRecords &s, const T *x,
                                           const T *q, const T *adt, T *res,
-                                          const AirConst<T> &k, int block, int minb) {
+                                          const AirConst<T> &k, int block, int minb,
+                                          bool interleave) {
   if (s.ncell <= 0) return cudaSuccess;
+  if (interleave)
+    return block == 128
+               ? launch_corner(k_res_gather_corner<T, 128, 1, true>, 128, ctx, s, x, q, adt, res, k)
+               : launch_corner(k_res_gather_corner<T, 256, 1, true>, 256, ctx, s, x, q, adt, res, k);
   if (block == 64)
     return minb >= 6 ? launch_corner(k_res_gather_corner<T, 64, 6>, 64, ctx, s, x, q, adt, res, k)
                      : launch_corner(k_res_gather_corner<T, 64, 5>, 64, ctx, s, x, q, adt, res, k);
@@ -557,7 +631,7 @@ template <typename T>
 cudaError_t launch_res_bres_corner(const LaunchCtx &ctx, const SlotRecords &s,
                                    const BresRecords &b, const int *bound, const T *x,
                                    const T *q, const T *adt, T *res, const AirConst<T> &k,
-                                   int block, bool zero_res) {
+                                   int block, bool zero_res, bool interleave) {
   if (s.ncell <= 0) return cudaSuccess;
   (void)b;
   const BresLink bl{bound};
@@ -574,6 +648,17 @@ cudaError_t launch_res_bres_corner(const LaunchCtx &ctx, const SlotRecords &s,
     ctx.count();
     return cudaGetLastError();
   };
+  if (interleave) {
+    if (zero_res)
+      return block == 128 ? run(k_res_bres_corner<T, 128, true, true>, 128)
+                          : run(k_res_bres_corner<T, 256, true, true>, 256);
+    return block == 128 ? run(k_res_bres_corner<T, 128, false, true>, 128)
+                        : run(k_res_bres_corner<T, 256, false, true>, 256);
+  }
+  // 384 threads: 12 warps in the SM's one CTA, three on each scheduler,
+  // whose register file caps a thread at 170 registers
+  if (block == 384)
+    return zero_res ? run(k_res_bres_corner<T, 384, true>, 384) : run(k_res_bres_corner<T, 384>, 384);
   if (zero_res)
     return block == 128 ? run(k_res_bres_corner<T, 128, true>, 128)
                         : run(k_res_bres_corner<T, 256, true>, 256);
@@ -584,20 +669,22 @@ template cudaError_t launch_res_bres_corner<double>(const LaunchCtx &, const Slo
                                                     const BresRecords &, const int *,
                                                     const double *, const double *,
                                                     const double *, double *,
-                                                    const AirConst<double> &, int, bool);
+                                                    const AirConst<double> &, int, bool, bool);
 template cudaError_t launch_res_bres_corner<float>(const LaunchCtx &, const SlotRecords &,
                                                    const BresRecords &, const int *, const float *,
                                                    const float *, const float *, float *,
-                                                   const AirConst<float> &, int, bool);
+                                                   const AirConst<float> &, int, bool, bool);
 
 template cudaError_t launch_res_calc_gather_corner<double>(const LaunchCtx &, const SlotRecords &,
                                                            const double *, const double *,
                                                            const double *, double *,
-                                                           const AirConst<double> &, int, int);
+                                                           const AirConst<double> &, int, int,
+                                                           bool);
 template cudaError_t launch_res_calc_gather_corner<float>(const LaunchCtx &, const SlotRecords &,
                                                           const float *, const float *,
                                                           const float *, float *,
-                                                          const AirConst<float> &, int, int);
+                                                          const AirConst<float> &, int, int,
+                                                          bool);
 
 template <typename T>
 cudaError_t launch_res_calc_gather_regpipe(const LaunchCtx &ctx, const SlotRecords &s,

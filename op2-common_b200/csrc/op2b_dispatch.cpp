@@ -228,7 +228,7 @@ static cudaError_t launch_fused_pair(Runtime &r, const SlotRecords &cr, const Br
   r.ring_used = r.opt_gather_kernel == OP2B_GATHER_RING && build_ring_records(&cr, r.nsm, 256);
   if (r.ring_used) return launch_res_ring<T>(r.ctx(), cr, bound, x, q, adt, res, k, zero);
   return launch_res_bres_corner<T>(r.ctx(), cr, br, bound, x, q, adt, res, k, r.opt_pipe_block,
-                                   zero);
+                                   zero, r.opt_corner_il != 0);
 }
 
 // the update's call launches the res_calc + bres_calc pair learned last
@@ -419,7 +419,8 @@ static cudaError_t res_gather_slots(Runtime &r, const SlotRecords &s, const ResC
         return launch_res_ring<T>(r.ctx(), s, nullptr, p.x, p.q, p.adt, p.res, k, false);
       if (s.corners)  // neighbours too far apart in the numbering for the ring
         return launch_res_calc_gather_corner<T>(r.ctx(), s, p.x, p.q, p.adt, p.res, k,
-                                                r.opt_pipe_block, r.opt_gather_minb);
+                                                r.opt_pipe_block, r.opt_gather_minb,
+                                                r.opt_corner_il != 0);
       return launch_res_calc_gather_regpipe<T>(r.ctx(), s, p.x, p.q, p.adt, p.res, k,
                                                r.opt_pipe_block);
     case OP2B_GATHER_LANES:
@@ -433,7 +434,8 @@ static cudaError_t res_gather_slots(Runtime &r, const SlotRecords &s, const ResC
     case OP2B_GATHER_CORNER:
       if (s.corners)
         return launch_res_calc_gather_corner<T>(r.ctx(), s, p.x, p.q, p.adt, p.res, k,
-                                                r.opt_pipe_block, r.opt_gather_minb);
+                                                r.opt_pipe_block, r.opt_gather_minb,
+                                                r.opt_corner_il != 0);
       // edges touching more than four nodes per cell: the slot-record pipeline
       return launch_res_calc_gather_regpipe<T>(r.ctx(), s, p.x, p.q, p.adt, p.res, k,
                                                r.opt_pipe_block);
@@ -922,7 +924,8 @@ bool op2b::Runtime::flush_loop() {
                                                       (const double *)pd.q->data_d,
                                                       (const double *)pd.adt->data_d,
                                                       (double *)pd.res->data_d, pd.kd,
-                                                      opt_pipe_block, opt_gather_minb);
+                                                      opt_pipe_block, opt_gather_minb,
+                                                      opt_corner_il != 0);
     else
       e = ring_used
               ? launch_res_ring<float>(ctx(), *cr, nullptr, (const float *)pd.x->data_d,
@@ -932,7 +935,8 @@ bool op2b::Runtime::flush_loop() {
                                                      (const float *)pd.q->data_d,
                                                      (const float *)pd.adt->data_d,
                                                      (float *)pd.res->data_d, pd.kf,
-                                                     opt_pipe_block, opt_gather_minb);
+                                                     opt_pipe_block, opt_gather_minb,
+                                                      opt_corner_il != 0);
     end_loop(pd.bytes);
     return finish(e, "res_calc") == 0;
   }

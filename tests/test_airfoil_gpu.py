@@ -167,6 +167,58 @@ def test_gather_mode_is_bit_exact_with_reference(op2, fixture, kernel):
     assert np.max(np.abs(np.array([h[0] for h in hist]) / gd["rms"] - 1)) < 1e-13
 
 
+@pytest.mark.parametrize("fuse", [1, 0])
+@pytest.mark.parametrize("fixture", ["airfoil_24x12_s3.npz", "airfoil_240x120_s1.npz"])
+def test_corner_interleave_is_bit_exact_with_reference(op2, fixture, fuse):
+    """corner_interleave 1: the corner kernels evaluate a cell's four fluxes
+    without branches (operands selected in each edge's order, the second
+    cell adding -f): q after 100 iterations is still the reference's bit for
+    bit, fused with bres_calc and alone."""
+    op2.set_option("inc_mode", L.OP2B_INC_GATHER)
+    op2.set_option("gather_kernel", 6)
+    op2.set_option("corner_interleave", 1)
+    op2.set_option("fuse", fuse)
+    gd = np.load(f"{GOLDEN}/{fixture}")
+    m = M.channel_bump(int(gd["I"]), int(gd["J"]), seed=int(gd["seed"]))
+    app = Airfoil(m)
+    hist = app.iterate(int(gd["niter"]))
+    g = app.fetch()
+    if "q" in gd:
+        assert np.array_equal(g["q"], gd["q"])
+        assert np.array_equal(g["adt"], gd["adt"])
+    else:
+        assert np.array_equal(g["q"][gd["q_sample_idx"]], gd["q_sample"])
+        assert np.array_equal(g["q"].sum(axis=0), gd["q_sum"])
+    assert np.array_equal(np.array([h[1] for h in hist]), gd["maxerr"])
+    assert np.array_equal(np.array([h[2] for h in hist]), gd["errloc"])
+
+
+@pytest.mark.parametrize("I,J,renumber", [(600, 300, True), (2400, 1200, True),
+                                          (2400, 1200, False)])
+def test_corner_interleave_matches_branchy_kernel(op2, I, J, renumber):
+    """The interleaved corner kernels against the default ones: q, adt and
+    res after 20 iterations equal bit for bit, fused and alone, FP64 and
+    FP32, on renumbered and randomly numbered meshes."""
+    m = M.channel_bump(I, J, seed=5)
+    for dtype in (np.float64, np.float32):
+        for fuse in (1, 0):
+            out = []
+            for il in (0, 1):
+                L.op_exit()
+                L.op_init()
+                L.set_option("inc_mode", L.OP2B_INC_GATHER)
+                L.set_option("gather_kernel", 6)
+                L.set_option("fuse", fuse)
+                L.set_option("corner_interleave", il)
+                app = Airfoil(m, dtype=dtype)
+                if renumber:
+                    app.renumber()
+                app.iterate(20)
+                out.append(app.fetch())
+            for key in ("q", "adt", "res"):
+                assert np.array_equal(out[0][key], out[1][key]), (dtype, fuse, key)
+
+
 @pytest.mark.parametrize("I,J,renumber", [(240, 120, True), (600, 300, True), (600, 300, False),
                                           (2400, 1200, True), (2400, 1200, False)])
 def test_flux_ring_is_bit_identical_to_corner_kernel(op2, I, J, renumber):
