@@ -93,17 +93,15 @@ bool build_ring_records(const SlotRecords *s, int nctas, int nt);
 #define OP2B_GATHER_REGPIPE 5  // cell4's order, register software pipeline
 #define OP2B_GATHER_CORNER 6   // the register pipeline over corner records
 #define OP2B_GATHER_RING 7     // corner records, each in-range flux computed once (flux ring)
+#define OP2B_GATHER_ASYNC 8    // corner records, next cell's operands staged by cp.async
 
 // airfoil_pipe.cu: the register pipeline over corner records (four node
 // gathers per cell instead of eight); block 64, 128 or 256 threads, minb the
-// __launch_bounds__ minimum CTAs per SM (1 = no register cap).  interleave:
-// the slots' fluxes without branches (block 128 or 256, no register cap), so
-// a cell's four flux evaluations overlap; the values are the same.
+// __launch_bounds__ minimum CTAs per SM (1 = no register cap)
 template <typename T>
 cudaError_t launch_res_calc_gather_corner(const LaunchCtx &c, const SlotRecords &s, const T *x,
                                           const T *q, const T *adt, T *res,
-                                          const AirConst<T> &k, int block, int minb,
-                                          bool interleave = false);
+                                          const AirConst<T> &k, int block, int minb);
 
 // Boundary records for bres_calc's gather, one per (cell, boundary edge) in
 // ascending (cell, edge) order: {cell, node 1, node 2, edge}; a record that
@@ -129,12 +127,17 @@ bool link_boundary_records(const SlotRecords *s, const BresRecords *b, op_map pb
 // airfoil_pipe.cu: the fused kernel (block 128 or 256).  zero_res: res is
 // known to be all zeros (the update before left it so without writing it):
 // the kernel starts each cell's sums from 0 instead of reading res.
-// interleave: the slots' fluxes without branches, as above.
 template <typename T>
 cudaError_t launch_res_bres_corner(const LaunchCtx &c, const SlotRecords &s,
                                    const BresRecords &b, const int *bound, const T *x,
                                    const T *q, const T *adt, T *res, const AirConst<T> &k,
-                                   int block, bool zero_res = false, bool interleave = false);
+                                   int block, bool zero_res = false);
+// airfoil_pipe.cu: the fused kernel with the next cell's operands staged in
+// shared memory by cp.async (block 256 or 384)
+template <typename T>
+cudaError_t launch_res_bres_async(const LaunchCtx &c, const SlotRecords &s, const int *bound,
+                                  const T *x, const T *q, const T *adt, T *res,
+                                  const AirConst<T> &k, int block, bool zero_res);
 // airfoil_ring.cu: res_calc (bound = nullptr) or the fused res_calc +
 // bres_calc over the flux-ring records (s.ring set; one CTA per range)
 template <typename T>

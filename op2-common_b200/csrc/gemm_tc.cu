@@ -21,6 +21,7 @@
 // Every mbarrier wait is bounded in time (%globaltimer): on expiry the kernel
 // records an error, stops issuing, waits (bounded) for its outstanding
 // commits, frees its tensor memory and returns.
+#include <algorithm>
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -555,6 +556,244 @@ k_gemm_tma(GemmArgs g, const __grid_constant__ CUtensorMap ta,
   if (threadIdx.x == 0 && s_fail) atomicExch(g.err, 1);
 }
 
+// ---------------------------------------------------------------------------
+// The persistent, warp-specialised form of the TMA-fed kernel (engine 2 by
+// default).  One CTA per SM walks the output tiles t = blockIdx.x,
+// blockIdx.x + gridDim.x, ... (M tiles fastest, so CTAs running together
+// share their B tile in L2), and its roles run side by side:
+//   * warp 0, lane 0: TMA producer over a kWsStages-deep operand ring that
+//     continues from one tile into the next;
+//   * warp 1, lane 0: MMA issuer.  The accumulator alternates between two
+//     128-column halves of tensor memory, so the MMAs of tile i+1 run while
+//     the epilogue drains tile i; a half is reused once the epilogue warps
+//     have read it (the "acc empty" mbarrier, one arrival per warp);
+//   * EW epilogue warps (2 .. EW + 1; EW = 8 or 16).  Warp w reads TMEM
+//     lanes 32 (w % 4) .. 32 (w % 4) + 31 (the lane quarter the hardware
+//     lets it access), columns [c0, c0 + 128 / (EW / 4)) with c0 set by
+//     (w - 2) / 4, and stores those parts of the rows as k_gemm_tma does;
+//     two or four warps per scheduler keep the epilogue's arithmetic and
+//     stores from being the bound.
+// The K order of every tile's MMAs is the same as in k_gemm_tma and
+// k_gemm_tc, so the three give identical results.  Every wait is bounded and
+// also ends when another role has recorded a failure; on failure the CTA
+// waits (bounded) for its issued loads and MMAs, frees tensor memory and
+// returns.
+constexpr int kWsStages = 4;
+
+__device__ __forceinline__ bool mbar_wait_or_fail(uint32_t bar, uint32_t parity,
+                                                  const volatile int *fail) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = globaltimer();
+  while (!mbar_try(bar, parity)) {
+    if (*fail) return false;
+    if (globaltimer() - t0 > kWaitNs) return false;
+  }
+  return true;
+}
+
+struct WsTile {
+  int m0, n0, nt, kb, nk;
+};
+
+__device__ __forceinline__ WsTile ws_tile(const GemmArgs &g, int t, int mtiles, int ntiles) {
+  WsTile w;
+  const int mb = t % mtiles, rest = t / mtiles;
+  w.m0 = mb * kTileM;
+  w.n0 = (rest % ntiles) * kTileN;
+  const int kz = rest / ntiles;
+  const int rem = g.N - w.n0;
+  w.nt = rem >= kTileN ? kTileN : ((rem + 15) & ~15);
+  w.kb = kz * g.k_per_split;
+  const int ke = min(g.K, w.kb + g.k_per_split);
+  w.nk = ke > w.kb ? (ke - w.kb + kTileK - 1) / kTileK : 0;
+  return w;
+}
+
+template <int EW>
+__global__ void __launch_bounds__(64 + 32 * EW, 1)
+k_gemm_ws(GemmArgs g, const __grid_constant__ CUtensorMap ta,
+          const __grid_constant__ CUtensorMap tb, int mtiles, int ntiles, int ntotal) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  // full[kWsStages], empty[kWsStages], acc_full[2], acc_empty[2], done
+  __shared__ __align__(8) uint64_t bars[2 * kWsStages + 5];
+  __shared__ uint32_t s_taddr;
+  __shared__ int s_fail, s_loaded, s_mma;
+  uint8_t *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  auto full = [&](int st) { return smem_u32(&bars[st]); };
+  auto empty = [&](int st) { return smem_u32(&bars[kWsStages + st]); };
+  auto acc_full = [&](int b) { return smem_u32(&bars[2 * kWsStages + b]); };
+  auto acc_empty = [&](int b) { return smem_u32(&bars[2 * kWsStages + 2 + b]); };
+  const uint32_t done = smem_u32(&bars[2 * kWsStages + 4]);
+  auto stage_a = [&](int st) { return smem_u32(smem + (size_t)st * 2 * kStageBytes); };
+  auto stage_b = [&](int st) { return smem_u32(smem + (size_t)st * 2 * kStageBytes + kStageBytes); };
+  volatile int *fail = &s_fail;
+
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < kWsStages; st++) {
+      mbar_init(full(st), 1);
+      mbar_init(empty(st), 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(acc_full(b), 1);
+      mbar_init(acc_empty(b), EW);
+    }
+    mbar_init(done, 1);
+    s_fail = 0;
+    s_loaded = 0;
+    s_mma = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&ta)) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tb)) : "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&s_taddr)),
+                 "r"(256u));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t taddr = s_taddr;
+
+  if (threadIdx.x == 0) {  // producer
+    int it = 0;
+    for (int t = blockIdx.x; t < ntotal && !*fail; t += gridDim.x) {
+      const WsTile w = ws_tile(g, t, mtiles, ntiles);
+      for (int kt = 0; kt < w.nk; kt++, it++) {
+        const int st = it % kWsStages;
+        if (it >= kWsStages &&
+            !mbar_wait_or_fail(empty(st), (uint32_t)((it / kWsStages - 1) & 1), fail)) {
+          atomicExch(&s_fail, 1);
+          break;
+        }
+        mbar_expect_tx(full(st), 2 * kStageBytes);
+        const int k0 = w.kb + kt * kTileK;
+        tma_load_2d(stage_a(st), &ta, k0, w.m0, full(st));
+        tma_load_2d(stage_b(st), &tb, k0, w.n0, full(st));
+      }
+    }
+    *(volatile int *)&s_loaded = it;
+  } else if (threadIdx.x == 32) {  // MMA issuer
+    int it = 0, i = 0;
+    for (int t = blockIdx.x; t < ntotal && !*fail; t += gridDim.x, i++) {
+      const WsTile w = ws_tile(g, t, mtiles, ntiles);
+      const int b = i & 1;
+      if (i >= 2 && !mbar_wait_or_fail(acc_empty(b), (uint32_t)(((i >> 1) - 1) & 1), fail)) {
+        atomicExch(&s_fail, 1);
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t idesc = umma_idesc(w.nt);
+      const uint32_t d = taddr + (uint32_t)(b * kTileN);
+      bool ok = true;
+      for (int kt = 0; kt < w.nk; kt++, it++) {
+        const int st = it % kWsStages;
+        if (!mbar_wait_or_fail(full(st), (uint32_t)((it / kWsStages) & 1), fail)) {
+          atomicExch(&s_fail, 1);
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t a0 = stage_a(st), b0 = stage_b(st);
+#pragma unroll
+        for (int j = 0; j < kTileK / 16; j++) {
+          const uint64_t da = umma_desc(a0 + j * 32);
+          const uint64_t db = umma_desc(b0 + j * 32);
+          const uint32_t acc = (kt > 0 || j > 0) ? 1u : 0u;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\t"
+              "setp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+              "l"(da), "l"(db), "r"(idesc), "r"(acc));
+        }
+        asm volatile(
+            "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                empty(st))
+            : "memory");
+      }
+      if (!ok) break;
+      // the tile's accumulator is complete once these MMAs have finished
+      asm volatile(
+          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+              acc_full(b))
+          : "memory");
+    }
+    *(volatile int *)&s_mma = it;
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(done)
+        : "memory");
+  } else if (warp >= 2) {  // epilogue
+    const int quarter = warp & 3;
+    constexpr int kCols = kTileN / (EW / 4);
+    const int c0 = ((warp - 2) >> 2) * kCols;
+    int i = 0;
+    for (int t = blockIdx.x; t < ntotal; t += gridDim.x, i++) {
+      const WsTile w = ws_tile(g, t, mtiles, ntiles);
+      const int b = i & 1;
+      bool ok = mbar_wait_or_fail(acc_full(b), (uint32_t)((i >> 1) & 1), fail);
+      ok = __all_sync(0xffffffffu, ok);
+      if (!ok) {
+        if (lane == 0) atomicExch(&s_fail, 1);
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int row = w.m0 + quarter * 32 + lane;
+      const uint32_t src = taddr + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * kTileN);
+      const int ce = min(w.nt, c0 + kCols);
+      if (c0 >= ce) {  // nothing of this tile in the warp's columns
+        __syncwarp();
+        if (lane == 0)
+          asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(acc_empty(b)) : "memory");
+        continue;
+      }
+      for (int cc = c0; cc < ce; cc += 16) {
+        uint32_t r[16];
+        if (w.nk > 0) {
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+              "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+              : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+                "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+              : "r"(src + (uint32_t)cc));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        } else {
+#pragma unroll
+          for (int k = 0; k < 16; k++) r[k] = 0u;
+        }
+        if (cc + 16 >= ce) {  // the warp's part has been read: the MMAs may reuse it
+          asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+          __syncwarp();
+          if (lane == 0)
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(acc_empty(b))
+                         : "memory");
+        }
+        if (row < g.M) epilogue16(g, row, w.n0 + cc, r);
+      }
+    }
+  }
+  __syncthreads();
+  // every issued MMA has finished once "done" has arrived; loads the MMA
+  // issuer did not consume (after a failure) are waited for before exit
+  if (threadIdx.x == 0) {
+    if (!mbar_wait(done, 0u)) s_fail = 1;
+    for (int it = s_mma; it < s_loaded; it++)
+      if (!mbar_wait(full(it % kWsStages), (uint32_t)((it / kWsStages) & 1))) {
+        s_fail = 1;
+        break;
+      }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 1) {
+    __syncwarp();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(256u));
+  }
+  if (threadIdx.x == 0 && s_fail) atomicExch(g.err, 1);
+}
+
 // the same product on the CUDA cores (FP32 accumulation), as a cross-check
 __global__ void k_gemm_simt(GemmArgs g) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x, row = blockIdx.y;
@@ -683,6 +922,38 @@ extern "C" int op2b_gemm_bf16(int M, int N, int K, const void *A, long a_m, long
   if (kmajor && (engine == 2 || (engine == 0 && rt().opt_gemm_tma))) {
     CUtensorMap ta, tb;
     if (operand_map(&ta, A, M, K, a_m) && operand_map(&tb, B, N, K, b_n)) {
+      if (rt().opt_gemm_ws) {  // the persistent, warp-specialised kernel
+        const size_t smem_w = (size_t)kWsStages * 2 * kStageBytes + 1024;
+        static bool attr_w[16] = {};
+        if (!attr_w[dev]) {
+          if (!cuda_ok(cudaFuncSetAttribute(k_gemm_ws<8>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem_w),
+                       "op2b_gemm_bf16: shared memory attribute") ||
+              !cuda_ok(cudaFuncSetAttribute(k_gemm_ws<16>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem_w),
+                       "op2b_gemm_bf16: shared memory attribute"))
+            return -1;
+          attr_w[dev] = true;
+        }
+        int nsm = 0;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        const long long total = (long long)grid.x * grid.y * grid.z;
+        if (total > 0x7fffffffLL) {
+          set_error("op2b_gemm_bf16: too many output tiles");
+          return -1;
+        }
+        const int ctas = (int)std::min<long long>(total, nsm > 0 ? nsm : 148);
+        if (rt().opt_gemm_ws == 2)
+          k_gemm_ws<16><<<ctas, 64 + 32 * 16, smem_w, s>>>(g, ta, tb, (int)grid.x, (int)grid.y,
+                                                           (int)total);
+        else
+          k_gemm_ws<8><<<ctas, 64 + 32 * 8, smem_w, s>>>(g, ta, tb, (int)grid.x, (int)grid.y,
+                                                         (int)total);
+        if (rt().initialised) rt().launches++;
+        return cuda_ok(cudaGetLastError(), "op2b_gemm_bf16") ? 0 : -1;
+      }
       const size_t smem_t = (size_t)kTmaStages * 2 * kStageBytes + 1024;
       static bool attr_t[16] = {};
       if (!attr_t[dev]) {

@@ -510,9 +510,9 @@ void op_exit(void) {
   r.opt_pipe_hints = d.opt_pipe_hints;
   r.opt_plan_mode = d.opt_plan_mode;
   r.opt_atomic_seg = d.opt_atomic_seg;
-  r.opt_corner_il = d.opt_corner_il;
   r.ring_used = 0;
   r.opt_gemm_tma = d.opt_gemm_tma;
+  r.opt_gemm_ws = d.opt_gemm_ws;
   r.opt_check_plans = d.opt_check_plans;
 }
 
@@ -1113,19 +1113,26 @@ int op2b_set_option(const char *key, long value) {
     r.opt_atomic_seg = value != 0;
   } else if (k == "gemm_tma") {
     r.opt_gemm_tma = value != 0;
-  } else if (k == "corner_interleave") {
-    r.opt_corner_il = value != 0;
+  } else if (k == "gemm_persistent") {
+    if (value < 0 || value > 2) {
+      set_error("op2b_set_option: gemm_persistent must be 0 (a CTA per tile), 1 (persistent, "
+                "8 epilogue warps) or 2 (persistent, 16 epilogue warps)");
+      return -1;
+    }
+    r.opt_gemm_ws = (int)value;
+
   } else if (k == "gather_kernel") {
-    if (value < 1 || value > 7) {
+    if (value < 1 || value > 8) {
       set_error("op2b_set_option: gather_kernel must be 1 (csr), 2 (lanes), 3 (cell4), 4 "
                 "(shared-memory pipeline), 5 (register pipeline), 6 (register pipeline "
-                "over corner records) or 7 (corner records, each flux computed once)");
+                "over corner records), 7 (corner records, each flux computed once) or 8 "
+                "(corner records, operands staged by cp.async)");
       return -1;
     }
     r.opt_gather_kernel = (int)value;
   } else if (k == "pipe_block") {
-    if (value != 64 && value != 96 && value != 128 && value != 256 && value != 384) {
-      set_error("op2b_set_option: pipe_block must be 64, 96, 128, 256 or 384");
+    if (value != 64 && value != 96 && value != 128 && value != 256) {
+      set_error("op2b_set_option: pipe_block must be 64, 96, 128 or 256");
       return -1;
     }
     r.opt_pipe_block = (int)value;
@@ -1185,7 +1192,7 @@ long op2b_get_option(const char *key) {
   if (k == "atomic_segmented") return r.opt_atomic_seg;
   if (k == "ring_used") return r.ring_used;  // read-only
   if (k == "gemm_tma") return r.opt_gemm_tma;
-  if (k == "corner_interleave") return r.opt_corner_il;
+  if (k == "gemm_persistent") return r.opt_gemm_ws;
   if (k == "gather_kernel") return r.opt_gather_kernel;
   if (k == "pipe_block") return r.opt_pipe_block;
   if (k == "pipe_hints") return r.opt_pipe_hints;

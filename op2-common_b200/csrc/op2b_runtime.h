@@ -129,9 +129,10 @@ struct Runtime {
                               // compiled loops' colourings; 1 = Jones-Plassmann for every
                               // plan; 2 = serial greedy for every plan
   int opt_atomic_seg = 1;     // inc_mode 0: 1 = segmented (warp-combined) atomics, 0 = per edge
-  int opt_corner_il = 0;      // corner kernels: a cell's four fluxes without branches
   int ring_used = 0;          // the last res_calc launch ran over the flux-ring records
   int opt_gemm_tma = 0;       // op2b_gemm_bf16 engine 0: TMA-fed kernel for k-major operands
+  int opt_gemm_ws = 2;        // TMA-fed products: 0 = a CTA per tile, 1 / 2 = the persistent
+                              // warp-specialised kernel with 8 / 16 epilogue warps
   bool opt_check_plans = false;
   bool quiet_errors = false;  // set_error records without printing or aborting
 

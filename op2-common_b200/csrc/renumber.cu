@@ -128,6 +128,21 @@ struct RcmWork {
                          // [4] / [5] = microseconds in Cuthill-McKee / breadth-first walks
 };
 
+__device__ __forceinline__ unsigned long long rcm_clock() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// thread 0 adds the time since prof[3] to prof[k] and restarts the lap
+__device__ __forceinline__ void rcm_lap(unsigned long long *prof, int k) {
+  if (threadIdx.x == 0) {
+    const unsigned long long now = rcm_clock();
+    prof[k] += now - prof[3];
+    prof[3] = now;
+  }
+}
+
 constexpr int kRcmThreads = 1024;
 // Positions of a level below kLevShared live in shared memory, the rest in
 // the global list: the levels of a 2-D mesh of a few million cells fit,
@@ -312,7 +327,10 @@ __device__ int rcm_bfs(RcmWork &w, Lev cur, Lev nxt, int start, int stamp, Lev *
     // kB vertices per thread per round, their first kNb neighbours unrolled:
     // every load of a round is independent of the others, so one round costs
     // a handful of memory latencies however many vertices it covers
-    for (int j0 = threadIdx.x; j0 < len; j0 += kB * blockDim.x) {
+    // (every thread runs the same rounds, so that the warp can combine its
+    // appends: one shared-memory atomic per warp instead of one per vertex)
+    for (int r0 = 0; r0 < len; r0 += kB * blockDim.x) {
+      const int j0 = r0 + threadIdx.x;
       LevelBatch b;
       b.load(w, cur, len, j0, thr, false);
       // all exchanges first (none waits on another's result), then the appends
@@ -322,11 +340,26 @@ __device__ int rcm_bfs(RcmWork &w, Lev cur, Lev nxt, int start, int stamp, Lev *
 #pragma unroll
         for (int t = 0; t < kNb; t++)
           old[k][t] = b.v[k][t] >= 0 ? atomicExch(&w.mark[b.v[k][t]], stamp) : stamp;
+      int cnt = 0;
+#pragma unroll
+      for (int k = 0; k < kB; k++)
+#pragma unroll
+        for (int t = 0; t < kNb; t++) cnt += old[k][t] != stamp ? 1 : 0;
+      const int lane = threadIdx.x & 31;
+      int incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      int wbase = 0;
+      if (lane == 31 && incl > 0) wbase = atomicAdd(&s_next, incl);
+      int pos = __shfl_sync(0xffffffffu, wbase, 31) + incl - cnt;
 #pragma unroll
       for (int k = 0; k < kB; k++)
 #pragma unroll
         for (int t = 0; t < kNb; t++)
-          if (old[k][t] != stamp) nxt.put(atomicAdd(&s_next, 1), b.v[k][t]);
+          if (old[k][t] != stamp) nxt.put(pos++, b.v[k][t]);
 #pragma unroll
       for (int k = 0; k < kB; k++)
         for (int t = kNb; t < b.d[k]; t++) {  // vertices of higher degree
@@ -429,7 +462,7 @@ __device__ __forceinline__ void rcm_emit(RcmWork &w, const ParentBatch &pb, int 
 // s_pos (shared).  Its levels are the BFS levels from `start`: returns
 // their number and leaves the last level in *last.
 __device__ int rcm_cm(RcmWork &w, Lev cur, Lev nxt, int start, int &s_pos, int &s_len, Lev *last,
-                      int *last_len) {
+                      int *last_len, unsigned long long *prof) {
   if (threadIdx.x == 0) {
     cur.put(0, start);
     w.newidx[start] = s_pos++;
@@ -447,6 +480,7 @@ __device__ int rcm_cm(RcmWork &w, Lev cur, Lev nxt, int start, int &s_pos, int &
       // a level of at most kB parents a thread: each thread loads its run of
       // parents once, claims their children, counts and places them -- the
       // steps below with the loads shared between them
+      if (threadIdx.x == 0) prof[3] = rcm_clock();
       ParentBatch pb;
       pb.load_open(w, cur, jb, je);
 #pragma unroll
@@ -462,12 +496,14 @@ __device__ int rcm_cm(RcmWork &w, Lev cur, Lev nxt, int start, int &s_pos, int &
         }
       }
       __syncthreads();
+      rcm_lap(prof, 0);
       pb.load_keys(w);
       int mine = 0;
 #pragma unroll
       for (int k = 0; k < kB; k++) mine += pb.count(w, k, jb + k);
       int nl = 0;
       int pos = rcm_block_scan(mine, &nl);
+      rcm_lap(prof, 1);
       if (nl == 0) {
         *last = cur;
         *last_len = len;
@@ -488,6 +524,7 @@ __device__ int rcm_cm(RcmWork &w, Lev cur, Lev nxt, int start, int &s_pos, int &
       cur = nxt;
       nxt = t;
       __syncthreads();
+      rcm_lap(prof, 2);
       continue;
     }
     // first parent (lowest position in this level) of every new vertex
@@ -548,12 +585,6 @@ __device__ int rcm_cm(RcmWork &w, Lev cur, Lev nxt, int start, int &s_pos, int &
   }
 }
 
-__device__ __forceinline__ unsigned long long rcm_clock() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
 __global__ void __launch_bounds__(kRcmThreads) k_rcm(RcmWork w) {
   extern __shared__ int s_lev[];  // 2 * kLevShared
   __shared__ int s_start, s_len;
@@ -563,6 +594,8 @@ __global__ void __launch_bounds__(kRcmThreads) k_rcm(RcmWork w) {
   int walks = 0;         // breadth-first and Cuthill-McKee walks (counted by every thread
   long long levels = 0;  // alike; thread 0 reports them)
   unsigned long long t_cm = 0, t_bfs = 0;
+  __shared__ unsigned long long s_prof[4];  // Cuthill-McKee level phases (small levels)
+  if (threadIdx.x == 0) s_prof[0] = s_prof[1] = s_prof[2] = 0;
   if (threadIdx.x == 0) s_pos = 0;
   __syncthreads();
   while (s_pos < w.n) {
@@ -602,7 +635,7 @@ __global__ void __launch_bounds__(kRcmThreads) k_rcm(RcmWork w) {
     Lev last;
     int last_len;
     unsigned long long t0 = rcm_clock();
-    int ecc = rcm_cm(w, la, lb, start, s_pos, s_len, &last, &last_len);
+    int ecc = rcm_cm(w, la, lb, start, s_pos, s_len, &last, &last_len, s_prof);
     unsigned long long t1 = rcm_clock();
     t_cm += t1 - t0;
     int cand = rcm_pick(w, last, last_len);
@@ -631,7 +664,7 @@ __global__ void __launch_bounds__(kRcmThreads) k_rcm(RcmWork w) {
         start = cand;
       }
       t0 = rcm_clock();
-      levels += rcm_cm(w, la, lb, start, s_pos, s_len, &last, &last_len);
+      levels += rcm_cm(w, la, lb, start, s_pos, s_len, &last, &last_len, s_prof);
       t_cm += rcm_clock() - t0;
       walks++;
     }
@@ -643,6 +676,9 @@ __global__ void __launch_bounds__(kRcmThreads) k_rcm(RcmWork w) {
     w.status[3] = (int)levels;
     w.status[4] = (int)(t_cm / 1000);
     w.status[5] = (int)(t_bfs / 1000);
+    w.status[6] = (int)(s_prof[0] / 1000);
+    w.status[7] = (int)(s_prof[1] / 1000);
+    w.status[8] = (int)(s_prof[2] / 1000);
   }
 }
 
@@ -826,14 +862,14 @@ static bool base_rcm(op_map base, int *perm_d, cudaStream_t s) {
   w.lev_a = (int *)A(sizeof(int) * n);
   w.lev_b = (int *)A(sizeof(int) * n);
   w.pkey = (int *)A(sizeof(int) * n);
-  w.status = (int *)A(sizeof(int) * 6);
+  w.status = (int *)A(sizeof(int) * 9);
   if (!ell || !w.newidx || !w.mark || !w.lev_a || !w.lev_b || !w.pkey || !w.status)
     return cleanup(), false;
   k_adj_ell<<<grid1(n), 256, 0, s>>>(n, row, deg, col, ell);
   cudaMemsetAsync(w.newidx, 0xff, sizeof(int) * n, s);
   cudaMemsetAsync(w.mark, 0, sizeof(int) * n, s);
   cudaMemsetAsync(w.pkey, 0x7f, sizeof(int) * n, s);  // 0x7f7f7f7f > any position
-  cudaMemsetAsync(w.status, 0, sizeof(int) * 6, s);
+  cudaMemsetAsync(w.status, 0, sizeof(int) * 9, s);
   // pkey must read as "none": 0x7f7f7f7f is used as the no-parent value
   if (cudaFuncSetAttribute(k_rcm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRcmSmem) !=
       cudaSuccess) {
@@ -843,13 +879,14 @@ static bool base_rcm(op_map base, int *perm_d, cudaStream_t s) {
   }
   k_rcm<<<1, kRcmThreads, kRcmSmem, s>>>(w);
   k_reverse<<<grid1(n), 256, 0, s>>>(n, w.newidx, perm_d);
-  int st[6] = {0, 0, 0, 0, 0, 0};
+  int st[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   cudaMemcpyAsync(st, w.status, sizeof(st), cudaMemcpyDeviceToHost, s);
   bool ok = cudaStreamSynchronize(s) == cudaSuccess && st[0] == n;
   if (!ok) set_error("op_renumber: reverse Cuthill-McKee ordered %d of %d elements", st[0], n);
   if (ok && rt().opt_diags > 2)
-    fprintf(stderr, "op_renumber: Cuthill-McKee %d walks, %d levels, %d us ordering, %d us "
-            "searching\n", st[2], st[3], st[4], st[5]);
+    fprintf(stderr, "op_renumber: Cuthill-McKee %d walks, %d levels, %d us ordering (small "
+            "levels: %d us claims, %d us counts, %d us placing), %d us searching\n", st[2],
+            st[3], st[4], st[6], st[7], st[8], st[5]);
   cleanup();
   return ok;
 }

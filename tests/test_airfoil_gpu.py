@@ -131,7 +131,7 @@ def test_colouring_is_deterministic_and_matches_atomics(op2, part):
 GATHER_KERNELS = [(1, 0, 0, 0), (2, 0, 0, 1), (3, 0, 0, 1), (4, 64, 0, 1), (4, 96, 0, 1),
                   (4, 128, 0, 1), (4, 256, 0, 1), (5, 64, 0, 1), (5, 96, 0, 1), (5, 128, 0, 0),
                   (5, 256, 0, 1), (6, 64, 5, 1), (6, 64, 6, 1), (6, 128, 0, 1), (6, 128, 3, 0),
-                  (6, 256, 0, 1), (7, 0, 0, 1), (7, 0, 0, 0)]
+                  (6, 256, 0, 1), (7, 0, 0, 1), (7, 0, 0, 0), (8, 0, 0, 1), (8, 256, 0, 1)]
 
 
 @pytest.mark.parametrize("kernel", GATHER_KERNELS,
@@ -167,58 +167,6 @@ def test_gather_mode_is_bit_exact_with_reference(op2, fixture, kernel):
     assert np.max(np.abs(np.array([h[0] for h in hist]) / gd["rms"] - 1)) < 1e-13
 
 
-@pytest.mark.parametrize("fuse", [1, 0])
-@pytest.mark.parametrize("fixture", ["airfoil_24x12_s3.npz", "airfoil_240x120_s1.npz"])
-def test_corner_interleave_is_bit_exact_with_reference(op2, fixture, fuse):
-    """corner_interleave 1: the corner kernels evaluate a cell's four fluxes
-    without branches (operands selected in each edge's order, the second
-    cell adding -f): q after 100 iterations is still the reference's bit for
-    bit, fused with bres_calc and alone."""
-    op2.set_option("inc_mode", L.OP2B_INC_GATHER)
-    op2.set_option("gather_kernel", 6)
-    op2.set_option("corner_interleave", 1)
-    op2.set_option("fuse", fuse)
-    gd = np.load(f"{GOLDEN}/{fixture}")
-    m = M.channel_bump(int(gd["I"]), int(gd["J"]), seed=int(gd["seed"]))
-    app = Airfoil(m)
-    hist = app.iterate(int(gd["niter"]))
-    g = app.fetch()
-    if "q" in gd:
-        assert np.array_equal(g["q"], gd["q"])
-        assert np.array_equal(g["adt"], gd["adt"])
-    else:
-        assert np.array_equal(g["q"][gd["q_sample_idx"]], gd["q_sample"])
-        assert np.array_equal(g["q"].sum(axis=0), gd["q_sum"])
-    assert np.array_equal(np.array([h[1] for h in hist]), gd["maxerr"])
-    assert np.array_equal(np.array([h[2] for h in hist]), gd["errloc"])
-
-
-@pytest.mark.parametrize("I,J,renumber", [(600, 300, True), (2400, 1200, True),
-                                          (2400, 1200, False)])
-def test_corner_interleave_matches_branchy_kernel(op2, I, J, renumber):
-    """The interleaved corner kernels against the default ones: q, adt and
-    res after 20 iterations equal bit for bit, fused and alone, FP64 and
-    FP32, on renumbered and randomly numbered meshes."""
-    m = M.channel_bump(I, J, seed=5)
-    for dtype in (np.float64, np.float32):
-        for fuse in (1, 0):
-            out = []
-            for il in (0, 1):
-                L.op_exit()
-                L.op_init()
-                L.set_option("inc_mode", L.OP2B_INC_GATHER)
-                L.set_option("gather_kernel", 6)
-                L.set_option("fuse", fuse)
-                L.set_option("corner_interleave", il)
-                app = Airfoil(m, dtype=dtype)
-                if renumber:
-                    app.renumber()
-                app.iterate(20)
-                out.append(app.fetch())
-            for key in ("q", "adt", "res"):
-                assert np.array_equal(out[0][key], out[1][key]), (dtype, fuse, key)
-
-
 @pytest.mark.parametrize("I,J,renumber", [(240, 120, True), (600, 300, True), (600, 300, False),
                                           (2400, 1200, True), (2400, 1200, False)])
 def test_flux_ring_is_bit_identical_to_corner_kernel(op2, I, J, renumber):
@@ -250,6 +198,31 @@ def test_flux_ring_is_bit_identical_to_corner_kernel(op2, I, J, renumber):
             assert used[0] == 0
             if renumber:
                 assert used[1] == 1, (I, J)
+
+
+@pytest.mark.parametrize("I,J,renumber,block", [(600, 300, True, 384), (2400, 1200, True, 384),
+                                                (2400, 1200, True, 256),
+                                                (2400, 1200, False, 384)])
+def test_async_staging_is_bit_identical_to_corner_kernel(op2, I, J, renumber, block):
+    """gather_kernel 8 stages the next cell's operands in shared memory by
+    cp.async instead of a second register set: q, adt and res after 3
+    iterations equal the register pipeline's bit for bit, in both precisions,
+    on renumbered and randomly numbered meshes."""
+    m = M.channel_bump(I, J, seed=7)
+    for dtype in (np.float64, np.float32):
+        out = []
+        for gk in (6, 8):
+            op2.set_option("gather_kernel", gk)
+            op2.set_option("pipe_block", block if gk == 8 else 256)
+            app = Airfoil(m, dtype=dtype)
+            if renumber:
+                app.renumber()
+            app.iterate(3)
+            out.append(app.fetch())
+            op2.op_exit()
+            op2.op_init()
+        for k in ("q", "adt", "res"):
+            assert np.array_equal(out[0][k], out[1][k]), (dtype, k)
 
 
 @pytest.mark.parametrize("hints", [0, 1])
@@ -586,7 +559,7 @@ def test_options_return_to_defaults_at_exit(op2):
     op2.op_init()
     assert {k: op2.get_option(k) for k in defaults} == defaults
     with pytest.raises(L.Op2Error):
-        op2.set_option("gather_kernel", 8)
+        op2.set_option("gather_kernel", 9)
 
 
 def test_large_mesh_one_iteration_against_oracle(op2):

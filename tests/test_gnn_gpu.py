@@ -176,6 +176,42 @@ def test_gemm_tma_engine_epilogues_and_split_k(op2):
     assert _rel(_np(s2), ref) < 2e-5
 
 
+@pytest.mark.parametrize("shape", [(300, 128, 384), (20000, 128, 8), (40000, 256, 136),
+                                   (300000, 128, 384)])
+def test_gemm_persistent_kernel_matches_per_tile_kernel(op2, shape):
+    """engine 2's persistent warp-specialised kernel (one CTA per SM walking
+    the tiles, TMEM accumulator double-buffered so a tile's epilogue overlaps
+    the next tile's loads and MMAs; 8 or 16 epilogue warps) against the
+    one-tile-per-CTA TMA kernel (option gemm_persistent 0): bit for bit, FP32
+    store and bias+SiLU with the pre-activation, and split-K to rounding."""
+    M_, N, K = shape
+    rng = np.random.default_rng(M_ + 7 * N + K)
+    a = _bf(rng.standard_normal((M_, K)) * 0.2)
+    b = _bf(rng.standard_normal((N, K)) * 0.2)
+    bias = torch.from_numpy(rng.standard_normal(N).astype(np.float32)).cuda()
+    A, B = a.cuda(), b.cuda()
+    outs = []
+    for persistent in (1, 2, 0):
+        op2.set_option("gemm_persistent", persistent)
+        C = torch.zeros(M_, N, device="cuda")
+        _gemm(M_, N, K, A, K, 1, B, K, 1, C, N, G.EPI_STORE_F32, engine=2)
+        H = torch.zeros(M_, N, dtype=torch.bfloat16, device="cuda")
+        Z = torch.zeros_like(H)
+        _gemm(M_, N, K, A, K, 1, B, K, 1, H, N, G.EPI_BIAS_SILU_BF16, bias=bias, Z=Z, engine=2)
+        S = torch.zeros(M_, N, device="cuda")
+        _gemm(M_, N, K, A, K, 1, B, K, 1, S, N, G.EPI_ATOMIC_F32, split=2, engine=2)
+        outs.append((C, H, Z, S))
+    op2.set_option("gemm_persistent", 1)
+    torch.cuda.synchronize()
+    assert G._lib().op2b_gemm_error(1) == 0
+    (c0, h0, z0, s0) = outs[-1]
+    for c1, h1, z1, s1 in outs[:-1]:
+        assert torch.equal(c1, c0) and torch.equal(h1, h0) and torch.equal(z1, z0)
+        assert _rel(_np(s1), _np(c1)) < 1e-6
+    if M_ <= 40000:
+        assert _rel(_np(c1), _np(a) @ _np(b).T) < 2e-5
+
+
 def test_gemm_tma_engine_refuses_transposed_operands(op2):
     A = torch.zeros(64, 128, dtype=torch.bfloat16, device="cuda")
     C = torch.zeros(128, 128, device="cuda")
