@@ -521,151 +521,6 @@ k_res_bres_corner(int ncell, const int4 *__restrict__ rec_o, const int4 *__restr
   }
 }
 
-// ---------------------------------------------------------------------------
-// The fused kernel with the next cell's operands staged in shared memory by
-// cp.async instead of held in a second register set (option gather_kernel
-// 8).  Each thread copies the operands of the cell after its current one --
-// q, res (unless known zero), adt of the cell, its four nodes, q and adt of
-// its interior neighbours -- into its own slots of one of two shared-memory
-// buffers while it computes the current cell from the other; the copies
-// need no registers, so the CTA can run 12 warps (the register pipeline runs
-// 8).  Slots are arrays over the CTA's threads (structure of arrays), so a
-// warp's accesses to one field are contiguous.  The arithmetic is
-// compute_corner's on the same values: bit-identical.
-__device__ __forceinline__ void cp_async(uint32_t dst, const void *src, int bytes) {
-  if (bytes == 16)
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
-  else if (bytes == 8)
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
-  else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;" ::: "memory");
-}
-template <int N> __device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-// byte offsets of one buffer's fields; every array has NT entries
-template <typename T, int NT, bool ZERO> struct AsyncSlots {
-  static constexpr int QCH = 4 * (int)sizeof(T) / 16;  // 16-byte chunks of a q row
-  static constexpr int XB = 2 * (int)sizeof(T), AB = (int)sizeof(T);
-  static constexpr int QC = 0;                          // [QCH][NT] x 16 B
-  static constexpr int QO = QC + QCH * NT * 16;         // [4][QCH][NT] x 16 B
-  static constexpr int RS = QO + 4 * QCH * NT * 16;     // [QCH][NT] x 16 B (unless ZERO)
-  static constexpr int XN = RS + (ZERO ? 0 : QCH * NT * 16);  // [4][NT] x XB
-  static constexpr int AO = XN + 4 * NT * XB;           // [4][NT] x AB
-  static constexpr int AC = AO + 4 * NT * AB;           // [NT] x AB
-  static constexpr int BYTES = AC + NT * AB;
-};
-
-template <typename T, int NT, bool ZERO>
-__device__ __forceinline__ void async_issue(uint32_t buf, int tid, int c, const CornerRec &r,
-                                            const T *__restrict__ x, const T *__restrict__ q,
-                                            const T *__restrict__ adt,
-                                            const T *__restrict__ res) {
-  using L = AsyncSlots<T, NT, ZERO>;
-  constexpr int CE = 16 / (int)sizeof(T);  // elements of a 16-byte chunk
-#pragma unroll
-  for (int ch = 0; ch < L::QCH; ch++) {
-    cp_async(buf + L::QC + (ch * NT + tid) * 16, q + 4 * (size_t)c + ch * CE, 16);
-    if constexpr (!ZERO)
-      cp_async(buf + L::RS + (ch * NT + tid) * 16, res + 4 * (size_t)c + ch * CE, 16);
-  }
-  cp_async(buf + L::AC + tid * L::AB, adt + c, L::AB);
-  const int nd[4] = {r.cn.x, r.cn.y, r.cn.z, r.cn.w};
-#pragma unroll
-  for (int j = 0; j < 4; j++) cp_async(buf + L::XN + (j * NT + tid) * L::XB, x + 2 * (size_t)nd[j], L::XB);
-  const int o[4] = {r.o.x, r.o.y, r.o.z, r.o.w};
-#pragma unroll
-  for (int sl = 0; sl < 4; sl++) {
-    if (!((r.meta >> (8 * sl)) & 1u)) continue;  // not an interior edge: no neighbour
-#pragma unroll
-    for (int ch = 0; ch < L::QCH; ch++)
-      cp_async(buf + L::QO + ((sl * L::QCH + ch) * NT + tid) * 16, q + 4 * (size_t)o[sl] + ch * CE,
-               16);
-    cp_async(buf + L::AO + (sl * NT + tid) * L::AB, adt + o[sl], L::AB);
-  }
-}
-
-template <typename T> __device__ __forceinline__ T lds(const uint8_t *p) {
-  return *reinterpret_cast<const T *>(p);
-}
-
-template <typename T, int NT, bool ZERO>
-__device__ __forceinline__ void async_gather(CornerOps<T> &d, const uint8_t *buf, int tid,
-                                             const CornerRec &r, const BresLink &bl) {
-  using L = AsyncSlots<T, NT, ZERO>;
-  constexpr int CE = 16 / (int)sizeof(T);
-#pragma unroll
-  for (int ch = 0; ch < L::QCH; ch++)
-#pragma unroll
-    for (int e = 0; e < CE; e++) {
-      d.qc[ch * CE + e] = lds<T>(buf + L::QC + (ch * NT + tid) * 16 + e * sizeof(T));
-      d.rs[ch * CE + e] =
-          ZERO ? (T)0 : lds<T>(buf + L::RS + (ch * NT + tid) * 16 + e * sizeof(T));
-    }
-  d.ac = lds<T>(buf + L::AC + tid * L::AB);
-#pragma unroll
-  for (int j = 0; j < 4; j++) {
-    d.xn[j][0] = lds<T>(buf + L::XN + (j * NT + tid) * L::XB);
-    d.xn[j][1] = lds<T>(buf + L::XN + (j * NT + tid) * L::XB + sizeof(T));
-  }
-#pragma unroll
-  for (int sl = 0; sl < 4; sl++) {
-    if (!((r.meta >> (8 * sl)) & 1u)) continue;
-#pragma unroll
-    for (int ch = 0; ch < L::QCH; ch++)
-#pragma unroll
-      for (int e = 0; e < CE; e++)
-        d.qo[sl][ch * CE + e] =
-            lds<T>(buf + L::QO + ((sl * L::QCH + ch) * NT + tid) * 16 + e * sizeof(T));
-    d.ao[sl] = lds<T>(buf + L::AO + (sl * NT + tid) * L::AB);
-  }
-  d.meta = r.meta;
-  if (r.meta & 0x40404040u) {  // a boundary cell: its boundary edges' flags
-    const int o[4] = {r.o.x, r.o.y, r.o.z, r.o.w};
-#pragma unroll
-    for (int sl = 0; sl < 4; sl++)
-      d.bnd[sl] = ((r.meta >> (8 * sl + 6)) & 1u) ? __ldg(bl.bound + o[sl]) : 0;
-  }
-}
-
-template <typename T, int NT, bool ZERO>
-__global__ void __launch_bounds__(NT, 1)
-k_res_bres_async(int ncell, const int4 *__restrict__ rec_o, const int4 *__restrict__ rec_cn,
-                 const unsigned *__restrict__ rec_meta, const T *__restrict__ x,
-                 const T *__restrict__ q, const T *__restrict__ adt, T *__restrict__ res,
-                 AirConst<T> k, BresLink bl) {
-  using L = AsyncSlots<T, NT, ZERO>;
-  extern __shared__ __align__(16) uint8_t smem_async[];
-  const int tid = threadIdx.x;
-  const int G = gridDim.x * NT;
-  int c = blockIdx.x * NT + tid;
-  if (c >= ncell) return;
-  const uint32_t base = (uint32_t)__cvta_generic_to_shared(smem_async);
-  CornerRec rc = load_crec(rec_o, rec_cn, rec_meta, c, ncell);
-  async_issue<T, NT, ZERO>(base, tid, c, rc, x, q, adt, res);
-  cp_async_commit();
-  CornerRec rn = load_crec(rec_o, rec_cn, rec_meta, c + G, ncell);
-  for (int it = 0; c < ncell; c += G, it++) {
-    const int b = it & 1;
-    const CornerRec rn2 = load_crec(rec_o, rec_cn, rec_meta, c + 2 * G, ncell);
-    if (c + G < ncell)
-      async_issue<T, NT, ZERO>(base + (uint32_t)((b ^ 1) * L::BYTES), tid, c + G, rn, x, q, adt,
-                               res);
-    cp_async_commit();
-    cp_async_wait<1>();  // this cell's copies have landed (the next cell's may not)
-    CornerOps<T> d;
-    async_gather<T, NT, ZERO>(d, smem_async + b * L::BYTES, tid, rc, bl);
-    compute_corner<T, true>(d, c, res, k);
-    rc = rn;
-    rn = rn2;
-  }
-  cp_async_wait<0>();
-}
-
 template <typename T, typename K>
 cudaError_t launch_corner(K kern, int nt, const LaunchCtx &ctx, const SlotRecords &s,
                           const T *x, const T *q, const T *adt, T *res, const AirConst<T> &k) {
@@ -724,45 +579,6 @@ cudaError_t launch_res_bres_corner(const LaunchCtx &ctx, const SlotRecords &s,
                         : run(k_res_bres_corner<T, 256, true>, 256);
   return block == 128 ? run(k_res_bres_corner<T, 128>, 128) : run(k_res_bres_corner<T, 256>, 256);
 }
-
-template <typename T>
-cudaError_t launch_res_bres_async(const LaunchCtx &ctx, const SlotRecords &s, const int *bound,
-                                  const T *x, const T *q, const T *adt, T *res,
-                                  const AirConst<T> &k, int block, bool zero_res) {
-  if (s.ncell <= 0) return cudaSuccess;
-  const BresLink bl{bound};
-  auto run = [&](auto kern, int nt, int bytes) -> cudaError_t {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e != cudaSuccess) return e;
-    int per_sm = 1;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nt, bytes);
-    if (e != cudaSuccess) return e;
-    long long blocks = (long long)ctx.nsm * (per_sm < 1 ? 1 : per_sm);
-    const long long need = (s.ncell + nt - 1) / nt;
-    if (blocks > need) blocks = need;
-    kern<<<(unsigned)blocks, nt, bytes, ctx.stream>>>(
-        s.ncell, reinterpret_cast<const int4 *>(s.o), reinterpret_cast<const int4 *>(s.cn),
-        s.meta, x, q, adt, res, k, bl);
-    ctx.count();
-    return cudaGetLastError();
-  };
-  // two buffers of the operand slots per thread: 384 threads (12 warps) fit
-  // 227 KB of shared memory in FP64; 256 threads leave room for more
-  if (block == 256)
-    return zero_res ? run(k_res_bres_async<T, 256, true>, 256, 2 * AsyncSlots<T, 256, true>::BYTES)
-                    : run(k_res_bres_async<T, 256, false>, 256, 2 * AsyncSlots<T, 256, false>::BYTES);
-  return zero_res ? run(k_res_bres_async<T, 384, true>, 384, 2 * AsyncSlots<T, 384, true>::BYTES)
-                  : run(k_res_bres_async<T, 384, false>, 384, 2 * AsyncSlots<T, 384, false>::BYTES);
-}
-
-template cudaError_t launch_res_bres_async<double>(const LaunchCtx &, const SlotRecords &,
-                                                   const int *, const double *, const double *,
-                                                   const double *, double *,
-                                                   const AirConst<double> &, int, bool);
-template cudaError_t launch_res_bres_async<float>(const LaunchCtx &, const SlotRecords &,
-                                                  const int *, const float *, const float *,
-                                                  const float *, float *, const AirConst<float> &,
-                                                  int, bool);
 
 template cudaError_t launch_res_bres_corner<double>(const LaunchCtx &, const SlotRecords &,
                                                     const BresRecords &, const int *,

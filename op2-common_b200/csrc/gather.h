@@ -93,7 +93,6 @@ bool build_ring_records(const SlotRecords *s, int nctas, int nt);
 #define OP2B_GATHER_REGPIPE 5  // cell4's order, register software pipeline
 #define OP2B_GATHER_CORNER 6   // the register pipeline over corner records
 #define OP2B_GATHER_RING 7     // corner records, each in-range flux computed once (flux ring)
-#define OP2B_GATHER_ASYNC 8    // corner records, next cell's operands staged by cp.async
 
 // airfoil_pipe.cu: the register pipeline over corner records (four node
 // gathers per cell instead of eight); block 64, 128 or 256 threads, minb the
@@ -132,12 +131,6 @@ cudaError_t launch_res_bres_corner(const LaunchCtx &c, const SlotRecords &s,
                                    const BresRecords &b, const int *bound, const T *x,
                                    const T *q, const T *adt, T *res, const AirConst<T> &k,
                                    int block, bool zero_res = false);
-// airfoil_pipe.cu: the fused kernel with the next cell's operands staged in
-// shared memory by cp.async (block 256 or 384)
-template <typename T>
-cudaError_t launch_res_bres_async(const LaunchCtx &c, const SlotRecords &s, const int *bound,
-                                  const T *x, const T *q, const T *adt, T *res,
-                                  const AirConst<T> &k, int block, bool zero_res);
 // airfoil_ring.cu: res_calc (bound = nullptr) or the fused res_calc +
 // bres_calc over the flux-ring records (s.ring set; one CTA per range)
 template <typename T>

@@ -164,7 +164,7 @@ static void host_copy(void *dst, const void *src, size_t bytes) {
 // destination takes its DMA directly.  Synchronous.
 bool download_host_many(const std::vector<HostDownload> &jobs, const char *what) {
   Runtime &r = rt();
-  const size_t kChunk = (size_t)16 << 20;
+  const size_t kChunk = kStageChunk;
   struct Piece {
     char *dst;
     const char *src;
@@ -188,11 +188,16 @@ bool download_host_many(const std::vector<HostDownload> &jobs, const char *what)
                         std::min(kChunk, j.bytes - off)});
   }
   if (pieces.empty()) return cuda_ok(cudaStreamSynchronize(r.stream), what);
-  if (!r.stage) {
-    if (!cuda_ok(cudaHostAlloc((void **)&r.stage, 2 * kChunk, cudaHostAllocDefault), what))
-      return false;
-    for (auto &e : r.stage_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
-  }
+  const auto t0 = std::chrono::steady_clock::now();
+  if (r.stage_alloc.joinable()) r.stage_alloc.join();
+  if (!r.stage &&
+      !cuda_ok(cudaHostAlloc((void **)&r.stage, 2 * kChunk, cudaHostAllocDefault), what))
+    return false;
+  for (auto &e : r.stage_ev)
+    if (!e && !cuda_ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), what)) return false;
+  const auto t1 = std::chrono::steady_clock::now();
+  size_t total = 0;
+  for (const auto &p : pieces) total += p.len;
   auto issue = [&](size_t k) {
     return cuda_ok(cudaMemcpyAsync(r.stage + (k % 2) * kChunk, pieces[k].src, pieces[k].len,
                                    cudaMemcpyDeviceToHost, r.stream),
@@ -205,7 +210,15 @@ bool download_host_many(const std::vector<HostDownload> &jobs, const char *what)
     if (!cuda_ok(cudaEventSynchronize(r.stage_ev[i % 2]), what)) return false;
     host_copy(pieces[i].dst, r.stage + (i % 2) * kChunk, pieces[i].len);
   }
-  return cuda_ok(cudaStreamSynchronize(r.stream), what);
+  const bool ok = cuda_ok(cudaStreamSynchronize(r.stream), what);
+  if (r.opt_diags > 2) {
+    const auto t2 = std::chrono::steady_clock::now();
+    const double a_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    const double c_ms = std::chrono::duration<double, std::milli>(t2 - t1).count();
+    fprintf(stderr, "%s: %.1f MB through staging in %.2f ms (%.1f GB/s), staging set up in "
+            "%.2f ms\n", what, total / 1e6, c_ms, total / 1e6 / c_ms, a_ms);
+  }
+  return ok;
 }
 
 bool download_host(void *dst, const void *src_d, size_t bytes, const char *what) {
@@ -407,6 +420,19 @@ void op_init(int argc, char **argv, int diags) {
     uint64_t keep = UINT64_MAX;
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
   }
+  // the pinned staging buffers of large device -> host copies: pinning takes
+  // tens of milliseconds, so a thread does it while the program declares
+  // its mesh (the first copy that needs them, or op_exit, waits for it)
+  if (r.stage_alloc.joinable()) r.stage_alloc.join();
+  if (!r.stage)
+    r.stage_alloc = std::thread([&r, dev] {
+      char *p = nullptr;
+      if (cudaSetDevice(dev) == cudaSuccess &&
+          cudaHostAlloc((void **)&p, 2 * kStageChunk, cudaHostAllocDefault) == cudaSuccess)
+        r.stage = p;
+      else
+        cudaGetLastError();
+    });
   r.initialised = true;
   if (diags > 1)
     printf(" op2b: device %d (%s, %d SMs), stream %p\n", dev, prop.name, r.nsm,
@@ -460,6 +486,7 @@ void op_exit(void) {
   cudaFree(r.check_d);
   r.check_d = nullptr;
   cudaFreeHost(r.pinned);
+  if (r.stage_alloc.joinable()) r.stage_alloc.join();
   cudaFreeHost(r.stage);
   r.stage = nullptr;
   for (auto &e : r.stage_ev) {
@@ -1122,11 +1149,10 @@ int op2b_set_option(const char *key, long value) {
     r.opt_gemm_ws = (int)value;
 
   } else if (k == "gather_kernel") {
-    if (value < 1 || value > 8) {
+    if (value < 1 || value > 7) {
       set_error("op2b_set_option: gather_kernel must be 1 (csr), 2 (lanes), 3 (cell4), 4 "
                 "(shared-memory pipeline), 5 (register pipeline), 6 (register pipeline "
-                "over corner records), 7 (corner records, each flux computed once) or 8 "
-                "(corner records, operands staged by cp.async)");
+                "over corner records) or 7 (corner records, each flux computed once)");
       return -1;
     }
     r.opt_gather_kernel = (int)value;

@@ -227,9 +227,6 @@ static cudaError_t launch_fused_pair(Runtime &r, const SlotRecords &cr, const Br
                                      T *res, const AirConst<T> &k, bool zero) {
   r.ring_used = r.opt_gather_kernel == OP2B_GATHER_RING && build_ring_records(&cr, r.nsm, 256);
   if (r.ring_used) return launch_res_ring<T>(r.ctx(), cr, bound, x, q, adt, res, k, zero);
-  if (r.opt_gather_kernel == OP2B_GATHER_ASYNC)
-    return launch_res_bres_async<T>(r.ctx(), cr, bound, x, q, adt, res, k,
-                                    r.opt_pipe_block == 256 ? 256 : 384, zero);
   return launch_res_bres_corner<T>(r.ctx(), cr, br, bound, x, q, adt, res, k, r.opt_pipe_block,
                                    zero);
 }
@@ -434,7 +431,6 @@ static cudaError_t res_gather_slots(Runtime &r, const SlotRecords &s, const ResC
       return launch_res_calc_gather_regpipe<T>(r.ctx(), s, p.x, p.q, p.adt, p.res, k,
                                                r.opt_pipe_block);
     case OP2B_GATHER_CORNER:
-    case OP2B_GATHER_ASYNC:  // (res_calc alone: the register pipeline)
       if (s.corners)
         return launch_res_calc_gather_corner<T>(r.ctx(), s, p.x, p.q, p.adt, p.res, k,
                                                 r.opt_pipe_block, r.opt_gather_minb);
@@ -480,8 +476,7 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
   int E = set->size, N = a[0].dat->set->size, C = a[2].dat->set->size;
   double bytes = 16.0 * E + (double)rb * (2.0 * N + 13.0 * C);
   if (r.opt_fuse && r.opt_inc_mode == OP2B_INC_GATHER &&
-      (r.opt_gather_kernel == OP2B_GATHER_CORNER || r.opt_gather_kernel == OP2B_GATHER_RING ||
-       r.opt_gather_kernel == OP2B_GATHER_ASYNC) &&
+      (r.opt_gather_kernel == OP2B_GATHER_CORNER || r.opt_gather_kernel == OP2B_GATHER_RING) &&
       r.opt_bres_kernel == 1) {
     const SlotRecords *cr = get_corner_records(pecell, pedge);
     if (!cr) return -1;
@@ -516,8 +511,7 @@ int loop_res_calc(const char *name, op_set set, int nargs, op_arg *a) {
   const InvMap *inv = nullptr;
   const SlotRecords *slots = nullptr;
   if (r.opt_inc_mode == OP2B_INC_GATHER) {
-    if (r.opt_gather_kernel == OP2B_GATHER_CORNER || r.opt_gather_kernel == OP2B_GATHER_RING ||
-        r.opt_gather_kernel == OP2B_GATHER_ASYNC) {
+    if (r.opt_gather_kernel == OP2B_GATHER_CORNER || r.opt_gather_kernel == OP2B_GATHER_RING) {
       slots = get_corner_records(pecell, pedge);
       if (!slots) return -1;
     } else if (r.opt_gather_kernel != OP2B_GATHER_CSR) {

@@ -7,6 +7,7 @@
 #include <memory>
 #include <set>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "loops.h"
@@ -97,6 +98,9 @@ struct ResLearn {
 };
 
 struct Runtime {
+  ~Runtime() {
+    if (stage_alloc.joinable()) stage_alloc.join();
+  }
   bool initialised = false;
   int device = 0, nsm = 148, cc_major = 0, cc_minor = 0;
   cudaStream_t stream = nullptr, own_stream = nullptr;
@@ -149,7 +153,8 @@ struct Runtime {
   void *red_base = nullptr;
   void *pinned = nullptr;      // 4 KiB mapped pinned host page for reduction read-back
   void *pinned_dev = nullptr;  // its device address
-  char *stage = nullptr;       // 2 x 16 MiB pinned buffers for large device -> host copies
+  char *stage = nullptr;       // 2 x kStageChunk pinned buffers for large device -> host copies
+  std::thread stage_alloc;     // pins them in the background from op_init on
   cudaEvent_t stage_ev[2] = {nullptr, nullptr};
   long long red_seq = 0;       // sequence number of the last update launch
   unsigned long long *check_d = nullptr;  // device word for op_decl_map's range check
@@ -209,6 +214,7 @@ bool cuda_ok(cudaError_t e, const char *what);
 // Device -> pageable host copy on the library stream, through pinned buffers
 // with the host-side copies spread over threads (synchronous).
 bool download_host(void *dst, const void *src_d, size_t bytes, const char *what);
+constexpr size_t kStageChunk = (size_t)16 << 20;
 // several device -> host copies in one staged pipeline (synchronous)
 struct HostDownload {
   void *dst;

@@ -210,13 +210,23 @@ __device__ __forceinline__ void load_vertices(const RcmWork &w, const int (&u)[k
     if (u[k] >= 0) {
       nb = w.ell[u[k]];
       d[k] = w.deg[u[k]];
-      r[k] = w.row[u[k]];
     }
     v[k][0] = nb.x;
     v[k][1] = nb.y;
     v[k][2] = nb.z;
     v[k][3] = nb.w;
   }
+  // the adjacency row only where the neighbours do not fit the table
+#pragma unroll
+  for (int k = 0; k < kB; k++)
+    if (d[k] > kNb) r[k] = w.row[u[k]];
+}
+
+// A vertex just placed in the next level: its neighbour-table entry and
+// degree, read when that level is walked, start towards L2 now.
+__device__ __forceinline__ void rcm_prefetch(const RcmWork &w, int v) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(w.ell + v));
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(w.deg + v));
 }
 
 // The first kNb unvisited neighbours of up to kB level vertices
@@ -359,7 +369,10 @@ __device__ int rcm_bfs(RcmWork &w, Lev cur, Lev nxt, int start, int stamp, Lev *
       for (int k = 0; k < kB; k++)
 #pragma unroll
         for (int t = 0; t < kNb; t++)
-          if (old[k][t] != stamp) nxt.put(pos++, b.v[k][t]);
+          if (old[k][t] != stamp) {
+            rcm_prefetch(w, b.v[k][t]);
+            nxt.put(pos++, b.v[k][t]);
+          }
 #pragma unroll
       for (int k = 0; k < kB; k++)
         for (int t = kNb; t < b.d[k]; t++) {  // vertices of higher degree
@@ -406,6 +419,7 @@ __device__ int rcm_pick(const RcmWork &w, const Lev &last, int last_len) {
 // Parent k (level position j) of a batch appends its claimed children to
 // the next level at pos, in sequential Cuthill-McKee's order, and places them.
 __device__ __forceinline__ void rcm_place(RcmWork &w, const Lev &nxt, int &pos, int base, int v) {
+  rcm_prefetch(w, v);
   nxt.put(pos, v);
   w.newidx[v] = base + pos;
   w.pkey[v] = INT_MAX;
@@ -585,44 +599,136 @@ __device__ int rcm_cm(RcmWork &w, Lev cur, Lev nxt, int start, int &s_pos, int &
   }
 }
 
+// An unvisited vertex of minimum degree, lowest id on ties (a corner of a
+// structured mesh region: usually already pseudo-peripheral); -1 when every
+// vertex is ordered.  Called by the whole CTA.
+__device__ int rcm_min_degree(const RcmWork &w) {
+  __shared__ unsigned long long s_key[kRcmThreads / 32];
+  __shared__ int s_start;
+  unsigned long long best = ~0ull;
+  for (int v = threadIdx.x; v < w.n; v += blockDim.x)
+    if (w.newidx[v] < 0) {
+      const unsigned long long key = ((unsigned long long)(unsigned)w.deg[v] << 32) | (unsigned)v;
+      best = key < best ? key : best;
+    }
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long other = __shfl_down_sync(0xffffffffu, best, o);
+    best = other < best ? other : best;
+  }
+  if ((threadIdx.x & 31) == 0) s_key[threadIdx.x >> 5] = best;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < (int)(blockDim.x >> 5); k++) best = s_key[k] < best ? s_key[k] : best;
+    s_start = best == ~0ull ? -1 : (int)(best & 0xffffffffull);
+  }
+  __syncthreads();
+  const int start = s_start;
+  __syncthreads();  // s_key and s_start are reused by the next call
+  return start;
+}
+
+// Reverse Cuthill-McKee of the first component is found by two CTAs at once
+// (two kernels on two streams), which share nothing they write:
+//   * k_rcm_search runs the plain George-Liu search: breadth-first walks
+//     (w.mark, its own level lists) from the minimum-degree vertex, then from
+//     the candidate of each last level (minimum degree, lowest id), while
+//     the eccentricity grows, at most 8 candidates;
+//   * k_rcm_first orders the component by Cuthill-McKee from the
+//     minimum-degree vertex meanwhile (w.newidx, w.pkey, w.lev_a/b).
+// When the search keeps the first vertex -- the usual case -- that order is
+// the one the sequential algorithm builds; otherwise k_rcm_redo undoes it
+// and orders from the vertex found.  k_rcm then takes the other components
+// (if any) one after another in one CTA, each by Cuthill-McKee from its
+// minimum-degree vertex followed by the breadth-first test of that order's
+// last level (and the search, when the test finds a more eccentric vertex).
+// rcm[0] = start found, [1] = first start, [2] = search walks, [3] = their
+// levels, [4] = microseconds searching.
+__global__ void __launch_bounds__(kRcmThreads) k_rcm_search(RcmWork w, int *lev_c, int *lev_d,
+                                                            int *rcm) {
+  extern __shared__ int s_lev[];  // 2 * kLevShared
+  const Lev la{s_lev, lev_c}, lb{s_lev + kLevShared, lev_d};
+  const unsigned long long t0 = rcm_clock();
+  int start = rcm_min_degree(w);
+  if (start < 0) return;
+  const int start0 = start;
+  Lev last;
+  int last_len;
+  int stamp = 1;
+  int ecc = rcm_bfs(w, la, lb, start, stamp++, &last, &last_len);
+  int walks = 1, levels = ecc;
+  for (int round = 0; round < 8; round++) {
+    const int cand = rcm_pick(w, last, last_len);
+    const int e2 = rcm_bfs(w, la, lb, cand, stamp++, &last, &last_len);
+    walks++;
+    levels += e2;
+    if (e2 <= ecc) break;
+    ecc = e2;
+    start = cand;
+  }
+  if (threadIdx.x == 0) {
+    rcm[0] = start;
+    rcm[1] = start0;
+    rcm[2] = walks;
+    rcm[3] = levels;
+    rcm[4] = (int)((rcm_clock() - t0) / 1000);
+  }
+}
+
+// Cuthill-McKee of the component of the minimum-degree vertex (start < 0) or
+// of `start` after undoing the component ordered before (start >= 0).
+// status[0] = vertices ordered, [2] = walks, [3] = levels, [4] = microseconds,
+// [6..8] = the small levels' phases.
+__global__ void __launch_bounds__(kRcmThreads) k_rcm_first(RcmWork w, int start) {
+  extern __shared__ int s_lev[];
+  __shared__ int s_len, s_pos;
+  __shared__ unsigned long long s_prof[4];
+  const Lev la{s_lev, w.lev_a}, lb{s_lev + kLevShared, w.lev_b};
+  const unsigned long long t0 = rcm_clock();
+  if (threadIdx.x == 0) {
+    s_pos = 0;
+    s_prof[0] = s_prof[1] = s_prof[2] = 0;
+  }
+  if (start >= 0) {  // undo: the search found a more eccentric start
+    for (int v = threadIdx.x; v < w.n; v += blockDim.x)
+      if (w.newidx[v] >= 0) w.newidx[v] = -1;
+  }
+  __syncthreads();
+  if (start < 0) start = rcm_min_degree(w);
+  if (start < 0) return;
+  Lev last;
+  int last_len;
+  const int lv = rcm_cm(w, la, lb, start, s_pos, s_len, &last, &last_len, s_prof);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    w.status[0] = s_pos;
+    w.status[2] += 1;
+    w.status[3] += lv;
+    w.status[4] += (int)((rcm_clock() - t0) / 1000);
+    w.status[6] += (int)(s_prof[0] / 1000);
+    w.status[7] += (int)(s_prof[1] / 1000);
+    w.status[8] += (int)(s_prof[2] / 1000);
+  }
+}
+
+// The remaining components, from position status[0] on (see above).
 __global__ void __launch_bounds__(kRcmThreads) k_rcm(RcmWork w) {
   extern __shared__ int s_lev[];  // 2 * kLevShared
-  __shared__ int s_start, s_len;
+  __shared__ int s_len;
   __shared__ int s_pos;
   const Lev la{s_lev, w.lev_a}, lb{s_lev + kLevShared, w.lev_b};
-  int stamp = 1;
+  int stamp = 1 << 20;  // above the search kernel's stamps
   int walks = 0;         // breadth-first and Cuthill-McKee walks (counted by every thread
   long long levels = 0;  // alike; thread 0 reports them)
   unsigned long long t_cm = 0, t_bfs = 0;
-  __shared__ unsigned long long s_prof[4];  // Cuthill-McKee level phases (small levels)
-  if (threadIdx.x == 0) s_prof[0] = s_prof[1] = s_prof[2] = 0;
-  if (threadIdx.x == 0) s_pos = 0;
+  __shared__ unsigned long long s_prof[4];
+  if (threadIdx.x == 0) {
+    s_prof[0] = s_prof[1] = s_prof[2] = 0;
+    s_pos = w.status[0];
+  }
   __syncthreads();
   while (s_pos < w.n) {
-    // an unvisited vertex of minimum degree, lowest id on ties (a corner of a
-    // structured mesh region: usually already pseudo-peripheral)
-    {
-      __shared__ unsigned long long s_key[kRcmThreads / 32];
-      unsigned long long best = ~0ull;
-      for (int v = threadIdx.x; v < w.n; v += blockDim.x)
-        if (w.newidx[v] < 0) {
-          const unsigned long long key =
-              ((unsigned long long)(unsigned)w.deg[v] << 32) | (unsigned)v;
-          best = key < best ? key : best;
-        }
-      for (int o = 16; o > 0; o >>= 1) {
-        const unsigned long long other = __shfl_down_sync(0xffffffffu, best, o);
-        best = other < best ? other : best;
-      }
-      if ((threadIdx.x & 31) == 0) s_key[threadIdx.x >> 5] = best;
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        for (int k = 1; k < (int)(blockDim.x >> 5); k++) best = s_key[k] < best ? s_key[k] : best;
-        s_start = (int)(best & 0xffffffffull);
-      }
-      __syncthreads();
-    }
-    int start = s_start;
+    int start = rcm_min_degree(w);
+    if (start < 0) break;
     const int comp_base = s_pos;
     // George-Liu pseudo-peripheral vertex.  Its first BFS, from `start`, has
     // the levels of Cuthill-McKee from `start`: order the component from
@@ -672,13 +778,13 @@ __global__ void __launch_bounds__(kRcmThreads) k_rcm(RcmWork w) {
   }
   if (threadIdx.x == 0) {
     w.status[0] = s_pos;
-    w.status[2] = walks;
-    w.status[3] = (int)levels;
-    w.status[4] = (int)(t_cm / 1000);
-    w.status[5] = (int)(t_bfs / 1000);
-    w.status[6] = (int)(s_prof[0] / 1000);
-    w.status[7] = (int)(s_prof[1] / 1000);
-    w.status[8] = (int)(s_prof[2] / 1000);
+    w.status[2] += walks;
+    w.status[3] += (int)levels;
+    w.status[4] += (int)(t_cm / 1000);
+    w.status[5] += (int)(t_bfs / 1000);
+    w.status[6] += (int)(s_prof[0] / 1000);
+    w.status[7] += (int)(s_prof[1] / 1000);
+    w.status[8] += (int)(s_prof[2] / 1000);
   }
 }
 
@@ -863,30 +969,66 @@ static bool base_rcm(op_map base, int *perm_d, cudaStream_t s) {
   w.lev_b = (int *)A(sizeof(int) * n);
   w.pkey = (int *)A(sizeof(int) * n);
   w.status = (int *)A(sizeof(int) * 9);
-  if (!ell || !w.newidx || !w.mark || !w.lev_a || !w.lev_b || !w.pkey || !w.status)
+  int *lev_c = (int *)A(sizeof(int) * n), *lev_d = (int *)A(sizeof(int) * n);
+  int *search = (int *)A(sizeof(int) * 5);
+  if (!ell || !w.newidx || !w.mark || !w.lev_a || !w.lev_b || !w.pkey || !w.status || !lev_c ||
+      !lev_d || !search)
     return cleanup(), false;
   k_adj_ell<<<grid1(n), 256, 0, s>>>(n, row, deg, col, ell);
   cudaMemsetAsync(w.newidx, 0xff, sizeof(int) * n, s);
   cudaMemsetAsync(w.mark, 0, sizeof(int) * n, s);
   cudaMemsetAsync(w.pkey, 0x7f, sizeof(int) * n, s);  // 0x7f7f7f7f > any position
   cudaMemsetAsync(w.status, 0, sizeof(int) * 9, s);
+  cudaMemsetAsync(search, 0xff, sizeof(int) * 5, s);
   // pkey must read as "none": 0x7f7f7f7f is used as the no-parent value
-  if (cudaFuncSetAttribute(k_rcm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRcmSmem) !=
-      cudaSuccess) {
-    cudaGetLastError();
-    set_error("op_renumber: %zu bytes of shared memory refused", kRcmSmem);
-    return cleanup(), false;
+  for (const void *kern : {(const void *)k_rcm, (const void *)k_rcm_first,
+                           (const void *)k_rcm_search})
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRcmSmem) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      set_error("op_renumber: %zu bytes of shared memory refused", kRcmSmem);
+      return cleanup(), false;
+    }
+  // the first component: the search on a second stream beside the ordering
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ready = nullptr, found = nullptr;
+  bool ok = cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&ready, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&found, cudaEventDisableTiming) == cudaSuccess;
+  int sr[5] = {-1, -1, 0, 0, 0};
+  if (ok) {
+    cudaEventRecord(ready, s);
+    cudaStreamWaitEvent(aux, ready, 0);
+    k_rcm_search<<<1, kRcmThreads, kRcmSmem, aux>>>(w, lev_c, lev_d, search);
+    cudaEventRecord(found, aux);
+    k_rcm_first<<<1, kRcmThreads, kRcmSmem, s>>>(w, -1);
+    cudaStreamWaitEvent(s, found, 0);
+    cudaMemcpyAsync(sr, search, sizeof(sr), cudaMemcpyDeviceToHost, s);
+    ok = cudaStreamSynchronize(s) == cudaSuccess;
   }
-  k_rcm<<<1, kRcmThreads, kRcmSmem, s>>>(w);
-  k_reverse<<<grid1(n), 256, 0, s>>>(n, w.newidx, perm_d);
+  if (ok && sr[0] >= 0 && sr[0] != sr[1])  // a more eccentric start: order from it
+    k_rcm_first<<<1, kRcmThreads, kRcmSmem, s>>>(w, sr[0]);
+  if (ok) k_rcm<<<1, kRcmThreads, kRcmSmem, s>>>(w);  // the other components
+  if (ok) k_reverse<<<grid1(n), 256, 0, s>>>(n, w.newidx, perm_d);
   int st[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  cudaMemcpyAsync(st, w.status, sizeof(st), cudaMemcpyDeviceToHost, s);
-  bool ok = cudaStreamSynchronize(s) == cudaSuccess && st[0] == n;
-  if (!ok) set_error("op_renumber: reverse Cuthill-McKee ordered %d of %d elements", st[0], n);
+  if (ok) cudaMemcpyAsync(st, w.status, sizeof(st), cudaMemcpyDeviceToHost, s);
+  ok = ok && cudaStreamSynchronize(s) == cudaSuccess && st[0] == n;
+  if (!ok) {
+    cudaGetLastError();
+    set_error("op_renumber: reverse Cuthill-McKee ordered %d of %d elements", st[0], n);
+  }
   if (ok && rt().opt_diags > 2)
     fprintf(stderr, "op_renumber: Cuthill-McKee %d walks, %d levels, %d us ordering (small "
-            "levels: %d us claims, %d us counts, %d us placing), %d us searching\n", st[2],
-            st[3], st[4], st[6], st[7], st[8], st[5]);
+            "levels: %d us claims, %d us counts, %d us placing), %d us searching after; first "
+            "component searched beside the ordering: %d walks, %d levels, %d us%s\n",
+            st[2], st[3], st[4], st[6], st[7], st[8], st[5], sr[2], sr[3], sr[4],
+            sr[0] != sr[1] ? " (start moved)" : "");
+  if (aux) {
+    cudaStreamSynchronize(aux);
+    cudaStreamDestroy(aux);
+  }
+  if (ready) cudaEventDestroy(ready);
+  if (found) cudaEventDestroy(found);
   cleanup();
   return ok;
 }

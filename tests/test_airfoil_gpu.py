@@ -131,7 +131,7 @@ def test_colouring_is_deterministic_and_matches_atomics(op2, part):
 GATHER_KERNELS = [(1, 0, 0, 0), (2, 0, 0, 1), (3, 0, 0, 1), (4, 64, 0, 1), (4, 96, 0, 1),
                   (4, 128, 0, 1), (4, 256, 0, 1), (5, 64, 0, 1), (5, 96, 0, 1), (5, 128, 0, 0),
                   (5, 256, 0, 1), (6, 64, 5, 1), (6, 64, 6, 1), (6, 128, 0, 1), (6, 128, 3, 0),
-                  (6, 256, 0, 1), (7, 0, 0, 1), (7, 0, 0, 0), (8, 0, 0, 1), (8, 256, 0, 1)]
+                  (6, 256, 0, 1), (7, 0, 0, 1), (7, 0, 0, 0)]
 
 
 @pytest.mark.parametrize("kernel", GATHER_KERNELS,
@@ -198,31 +198,6 @@ def test_flux_ring_is_bit_identical_to_corner_kernel(op2, I, J, renumber):
             assert used[0] == 0
             if renumber:
                 assert used[1] == 1, (I, J)
-
-
-@pytest.mark.parametrize("I,J,renumber,block", [(600, 300, True, 384), (2400, 1200, True, 384),
-                                                (2400, 1200, True, 256),
-                                                (2400, 1200, False, 384)])
-def test_async_staging_is_bit_identical_to_corner_kernel(op2, I, J, renumber, block):
-    """gather_kernel 8 stages the next cell's operands in shared memory by
-    cp.async instead of a second register set: q, adt and res after 3
-    iterations equal the register pipeline's bit for bit, in both precisions,
-    on renumbered and randomly numbered meshes."""
-    m = M.channel_bump(I, J, seed=7)
-    for dtype in (np.float64, np.float32):
-        out = []
-        for gk in (6, 8):
-            op2.set_option("gather_kernel", gk)
-            op2.set_option("pipe_block", block if gk == 8 else 256)
-            app = Airfoil(m, dtype=dtype)
-            if renumber:
-                app.renumber()
-            app.iterate(3)
-            out.append(app.fetch())
-            op2.op_exit()
-            op2.op_init()
-        for k in ("q", "adt", "res"):
-            assert np.array_equal(out[0][k], out[1][k]), (dtype, k)
 
 
 @pytest.mark.parametrize("hints", [0, 1])
@@ -559,7 +534,7 @@ def test_options_return_to_defaults_at_exit(op2):
     op2.op_init()
     assert {k: op2.get_option(k) for k in defaults} == defaults
     with pytest.raises(L.Op2Error):
-        op2.set_option("gather_kernel", 9)
+        op2.set_option("gather_kernel", 8)
 
 
 def test_large_mesh_one_iteration_against_oracle(op2):
