@@ -178,14 +178,41 @@ def traffic_from_profiles(key, loop):
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region (start before, stop after)."""
+    """SM clock and throttle reasons sampled during the timed region (start
+    before, stop after): NVML every 2 ms from a thread, or nvidia-smi every
+    200 ms where NVML cannot be loaded."""
+
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
 
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.thread = None
         self.path = os.path.join(tempfile.gettempdir(), f"op2b_clocks_{os.getpid()}.csv")
 
     def start(self):
+        try:
+            import threading
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            self.samples, self.mask = [], 0
+            self.done = threading.Event()
+
+            def poll():
+                while True:
+                    self.samples.append(float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)))
+                    self.mask |= int(pynvml.nvmlDeviceGetCurrentClocksEventReasons(h))
+                    if self.done.wait(0.002):
+                        return
+
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.thread = None
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -199,6 +226,13 @@ class Clocks:
             self.proc = None
 
     def stop(self):
+        if self.thread is not None:
+            self.done.set()
+            self.thread.join()
+            reasons = sorted(n for b, n in self.REASONS.items() if self.mask & b)
+            sm = self.samples
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                    "reasons": reasons, "samples": len(sm), "source": "nvml, every 2 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         time.sleep(0.25)
@@ -225,7 +259,7 @@ class Clocks:
                         reasons.add(n)
         os.unlink(self.path)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi, every 200 ms"}
 
 
 def run_reference(args, m_path, ncell, iters, skip, threads, numbering):

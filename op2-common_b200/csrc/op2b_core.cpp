@@ -148,7 +148,7 @@ CopyPool &copy_pool() {
 // memcpy of a large host array by up to `host_threads` threads (option,
 // default 8, at most the host's)
 static void host_copy(void *dst, const void *src, size_t bytes) {
-  const size_t kParallel = (size_t)8 << 20;
+  const size_t kParallel = (size_t)2 << 20;
   unsigned nt = std::min((unsigned)std::max(1, rt().opt_host_threads),
                          std::max(1u, std::thread::hardware_concurrency()));
   if (bytes < kParallel || nt < 2) {
@@ -162,6 +162,24 @@ static void host_copy(void *dst, const void *src, size_t bytes) {
 // staging buffers: chunk k of the whole list goes through buffer k % 2, its
 // DMA under way while the host threads empty the other buffer; a pinned
 // destination takes its DMA directly.  Synchronous.
+// The pinned staging buffers of large device -> host copies: pinning them
+// takes tens of milliseconds, so op_renumber has a thread do it while the
+// device orders the mesh (the first copy that needs them, or op_exit, waits
+// for it); without a renumbering the first large copy pins them itself.
+void stage_in_background() {
+  Runtime &r = rt();
+  if (r.stage || r.stage_alloc.joinable()) return;
+  const int dev = r.device;
+  r.stage_alloc = std::thread([&r, dev] {
+    char *p = nullptr;
+    if (cudaSetDevice(dev) == cudaSuccess &&
+        cudaHostAlloc((void **)&p, 2 * kStageChunk, cudaHostAllocDefault) == cudaSuccess)
+      r.stage = p;
+    else
+      cudaGetLastError();
+  });
+}
+
 bool download_host_many(const std::vector<HostDownload> &jobs, const char *what) {
   Runtime &r = rt();
   const size_t kChunk = kStageChunk;
@@ -420,19 +438,6 @@ void op_init(int argc, char **argv, int diags) {
     uint64_t keep = UINT64_MAX;
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
   }
-  // the pinned staging buffers of large device -> host copies: pinning takes
-  // tens of milliseconds, so a thread does it while the program declares
-  // its mesh (the first copy that needs them, or op_exit, waits for it)
-  if (r.stage_alloc.joinable()) r.stage_alloc.join();
-  if (!r.stage)
-    r.stage_alloc = std::thread([&r, dev] {
-      char *p = nullptr;
-      if (cudaSetDevice(dev) == cudaSuccess &&
-          cudaHostAlloc((void **)&p, 2 * kStageChunk, cudaHostAllocDefault) == cudaSuccess)
-        r.stage = p;
-      else
-        cudaGetLastError();
-    });
   r.initialised = true;
   if (diags > 1)
     printf(" op2b: device %d (%s, %d SMs), stream %p\n", dev, prop.name, r.nsm,
@@ -576,7 +581,7 @@ op_map op_decl_map(op_set from, op_set to, int dim, int *imap, char const *name)
     set_error("op_decl_map: NULL data for map %s", name ? name : "");
     return nullptr;
   }
-  int *h = (int *)malloc(sizeof(int) * (n ? n : 1));
+  int *h = (int *)host_alloc(sizeof(int) * (n ? n : 1));
   int *map_d = nullptr;
   auto bad_entry = [&](size_t i) {
     set_error("op_decl_map: invalid data for map %s: element %zu, dimension %zu, value %d "

@@ -215,6 +215,9 @@ bool cuda_ok(cudaError_t e, const char *what);
 // with the host-side copies spread over threads (synchronous).
 bool download_host(void *dst, const void *src_d, size_t bytes, const char *what);
 constexpr size_t kStageChunk = (size_t)16 << 20;
+// pin the staging buffers on a thread of their own (op_renumber, while the
+// device works)
+void stage_in_background();
 // several device -> host copies in one staged pipeline (synchronous)
 struct HostDownload {
   void *dst;

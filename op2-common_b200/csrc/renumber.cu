@@ -1002,6 +1002,9 @@ static bool base_rcm(op_map base, int *perm_d, cudaStream_t s) {
     k_rcm_search<<<1, kRcmThreads, kRcmSmem, aux>>>(w, lev_c, lev_d, search);
     cudaEventRecord(found, aux);
     k_rcm_first<<<1, kRcmThreads, kRcmSmem, s>>>(w, -1);
+    // the host copies of the reordered maps and dats come next: their pinned
+    // staging buffers are pinned while the device orders
+    if (rt().opt_host_mirror) stage_in_background();
     cudaStreamWaitEvent(s, found, 0);
     cudaMemcpyAsync(sr, search, sizeof(sr), cudaMemcpyDeviceToHost, s);
     ok = cudaStreamSynchronize(s) == cudaSuccess;
