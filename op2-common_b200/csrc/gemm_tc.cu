@@ -85,6 +85,23 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
   return d;
 }
 
+// The same descriptor for an MN-major operand tile (128 MN x 64 K) as TMA
+// writes it with the 128-byte swizzle: two boxes of 64 MN x 64 K, 8 KiB
+// apart, each 64 rows of 128 bytes (64 MN values of one k) in 1024-byte
+// groups of 8 rows.  In the canonical MN-major layout ((8,n),(8,k)) :
+// ((1,LBO),(8,SBO)) in 16-byte units the leading byte offset is the 8 KiB
+// between the two 64-wide MN blocks and the stride byte offset the 1024 bytes
+// between groups of 8 k; a K step of 16 starts 2048 bytes further on.
+__device__ __forceinline__ uint64_t umma_desc_mn(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)(8192 >> 4) << 16;
+  d |= (uint64_t)(1024 >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
+  return d;
+}
+
 // instruction descriptor, kind::f16: FP32 accumulator (bits 4-5 = 1), A and B
 // bf16 (bits 7-9 = 1, 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 in
 // bits 17-22, M >> 4 in bits 24-28
@@ -609,7 +626,7 @@ __device__ __forceinline__ WsTile ws_tile(const GemmArgs &g, int t, int mtiles, 
   return w;
 }
 
-template <int EW>
+template <int EW, bool AMN, bool BMN>
 __global__ void __launch_bounds__(64 + 32 * EW, 1)
 k_gemm_ws(GemmArgs g, const __grid_constant__ CUtensorMap ta,
           const __grid_constant__ CUtensorMap tb, int mtiles, int ntiles, int ntotal) {
@@ -670,8 +687,18 @@ k_gemm_ws(GemmArgs g, const __grid_constant__ CUtensorMap ta,
         }
         mbar_expect_tx(full(st), 2 * kStageBytes);
         const int k0 = w.kb + kt * kTileK;
-        tma_load_2d(stage_a(st), &ta, k0, w.m0, full(st));
-        tma_load_2d(stage_b(st), &tb, k0, w.n0, full(st));
+        if (AMN) {  // two 64 (MN) x 64 (K) boxes
+          tma_load_2d(stage_a(st), &ta, w.m0, k0, full(st));
+          tma_load_2d(stage_a(st) + kStageBytes / 2, &ta, w.m0 + 64, k0, full(st));
+        } else {
+          tma_load_2d(stage_a(st), &ta, k0, w.m0, full(st));
+        }
+        if (BMN) {
+          tma_load_2d(stage_b(st), &tb, w.n0, k0, full(st));
+          tma_load_2d(stage_b(st) + kStageBytes / 2, &tb, w.n0 + 64, k0, full(st));
+        } else {
+          tma_load_2d(stage_b(st), &tb, k0, w.n0, full(st));
+        }
       }
     }
     *(volatile int *)&s_loaded = it;
@@ -685,7 +712,8 @@ k_gemm_ws(GemmArgs g, const __grid_constant__ CUtensorMap ta,
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t idesc = umma_idesc(w.nt);
+      const uint32_t idesc =
+          umma_idesc(w.nt) | (AMN ? 1u << 15 : 0u) | (BMN ? 1u << 16 : 0u);  // MN-major
       const uint32_t d = taddr + (uint32_t)(b * kTileN);
       bool ok = true;
       for (int kt = 0; kt < w.nk; kt++, it++) {
@@ -699,8 +727,8 @@ k_gemm_ws(GemmArgs g, const __grid_constant__ CUtensorMap ta,
         const uint32_t a0 = stage_a(st), b0 = stage_b(st);
 #pragma unroll
         for (int j = 0; j < kTileK / 16; j++) {
-          const uint64_t da = umma_desc(a0 + j * 32);
-          const uint64_t db = umma_desc(b0 + j * 32);
+          const uint64_t da = AMN ? umma_desc_mn(a0 + j * 2048) : umma_desc(a0 + j * 32);
+          const uint64_t db = BMN ? umma_desc_mn(b0 + j * 2048) : umma_desc(b0 + j * 32);
           const uint32_t acc = (kt > 0 || j > 0) ? 1u : 0u;
           asm volatile(
               "{\n\t.reg .pred p;\n\t"
@@ -845,6 +873,36 @@ bool operand_map(CUtensorMap *m, const void *base, int rows, int K, long ld) {
          CUDA_SUCCESS;
 }
 
+// an MN-major bf16 operand (K rows of `mn` contiguous values, row stride `ld`
+// elements) as a tensor map of 64 (MN) x 64 (K) boxes with the 128-byte
+// swizzle; false if it cannot be encoded
+bool operand_map_mn(CUtensorMap *m, const void *base, int mn, int K, long ld) {
+  EncodeTiled enc = encode_tiled();
+  if (!enc) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)mn, (cuuint64_t)K};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  const cuuint32_t box[2] = {64, (cuuint32_t)kTileK};
+  const cuuint32_t estr[2] = {1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides,
+             box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
+template <int EW, bool AMN, bool BMN>
+cudaError_t launch_ws(const GemmArgs &g, const CUtensorMap &ta, const CUtensorMap &tb,
+                      dim3 grid, int nsm, cudaStream_t s) {
+  const size_t smem_w = (size_t)kWsStages * 2 * kStageBytes + 1024;
+  cudaError_t e = cudaFuncSetAttribute(k_gemm_ws<EW, AMN, BMN>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_w);
+  if (e != cudaSuccess) return e;
+  const long long total = (long long)grid.x * grid.y * grid.z;
+  const int ctas = (int)std::min<long long>(total, nsm > 0 ? nsm : 148);
+  k_gemm_ws<EW, AMN, BMN><<<ctas, 64 + 32 * EW, smem_w, s>>>(g, ta, tb, (int)grid.x,
+                                                             (int)grid.y, (int)total);
+  return cudaGetLastError();
+}
+
 }  // namespace
 }  // namespace op2b
 
@@ -916,64 +974,51 @@ extern "C" int op2b_gemm_bf16(int M, int N, int K, const void *A, long a_m, long
   }
   g.k_per_split = kps;
   dim3 grid((M + kTileM - 1) / kTileM, (N + kTileN - 1) / kTileN, split_k);
-  // the TMA-fed kernel for k-contiguous operands (engine 2 asks for it;
-  // engine 0 takes it when the option gemm_tma is on)
-  const bool kmajor = a_k == 1 && b_k == 1;
-  if (kmajor && (engine == 2 || (engine == 0 && rt().opt_gemm_tma))) {
+  // the TMA-fed kernels (engine 2 asks for them; engine 0 takes them when the
+  // option gemm_tma is on): the persistent kernel for any layout of A and B
+  // (k-contiguous operands as K-major tiles, the others as MN-major tiles),
+  // the one-tile-per-CTA kernel for k-contiguous operands
+  const bool a_mn = a_k != 1, b_mn = b_k != 1;
+  const bool ws = rt().opt_gemm_ws != 0;
+  if (engine == 2 || (engine == 0 && rt().opt_gemm_tma)) {
     CUtensorMap ta, tb;
-    if (operand_map(&ta, A, M, K, a_m) && operand_map(&tb, B, N, K, b_n)) {
-      if (rt().opt_gemm_ws) {  // the persistent, warp-specialised kernel
-        const size_t smem_w = (size_t)kWsStages * 2 * kStageBytes + 1024;
-        static bool attr_w[16] = {};
-        if (!attr_w[dev]) {
-          if (!cuda_ok(cudaFuncSetAttribute(k_gemm_ws<8>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)smem_w),
-                       "op2b_gemm_bf16: shared memory attribute") ||
-              !cuda_ok(cudaFuncSetAttribute(k_gemm_ws<16>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)smem_w),
-                       "op2b_gemm_bf16: shared memory attribute"))
-            return -1;
-          attr_w[dev] = true;
-        }
+    const bool mapped = (a_mn ? operand_map_mn(&ta, A, M, K, a_k) : operand_map(&ta, A, M, K, a_m)) &&
+                        (b_mn ? operand_map_mn(&tb, B, N, K, b_k) : operand_map(&tb, B, N, K, b_n));
+    if ((a_mn || b_mn) && !ws) {
+      if (engine == 2) {
+        set_error("op2b_gemm_bf16: engine 2 with gemm_persistent 0 needs k-contiguous A and B");
+        return -1;
+      }
+    } else if (mapped) {
+      const long long total = (long long)grid.x * grid.y * grid.z;
+      if (total > 0x7fffffffLL) {
+        set_error("op2b_gemm_bf16: too many output tiles");
+        return -1;
+      }
+      cudaError_t e;
+      if (ws) {
         int nsm = 0;
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        const long long total = (long long)grid.x * grid.y * grid.z;
-        if (total > 0x7fffffffLL) {
-          set_error("op2b_gemm_bf16: too many output tiles");
-          return -1;
+        if (a_mn && b_mn) e = launch_ws<16, true, true>(g, ta, tb, grid, nsm, s);
+        else if (a_mn) e = launch_ws<16, true, false>(g, ta, tb, grid, nsm, s);
+        else if (b_mn) e = launch_ws<16, false, true>(g, ta, tb, grid, nsm, s);
+        else if (rt().opt_gemm_ws == 2) e = launch_ws<16, false, false>(g, ta, tb, grid, nsm, s);
+        else e = launch_ws<8, false, false>(g, ta, tb, grid, nsm, s);
+      } else {
+        const size_t smem_t = (size_t)kTmaStages * 2 * kStageBytes + 1024;
+        e = cudaFuncSetAttribute(k_gemm_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem_t);
+        if (e == cudaSuccess) {
+          k_gemm_tma<<<grid, kThreads, smem_t, s>>>(g, ta, tb);
+          e = cudaGetLastError();
         }
-        const int ctas = (int)std::min<long long>(total, nsm > 0 ? nsm : 148);
-        if (rt().opt_gemm_ws == 2)
-          k_gemm_ws<16><<<ctas, 64 + 32 * 16, smem_w, s>>>(g, ta, tb, (int)grid.x, (int)grid.y,
-                                                           (int)total);
-        else
-          k_gemm_ws<8><<<ctas, 64 + 32 * 8, smem_w, s>>>(g, ta, tb, (int)grid.x, (int)grid.y,
-                                                         (int)total);
-        if (rt().initialised) rt().launches++;
-        return cuda_ok(cudaGetLastError(), "op2b_gemm_bf16") ? 0 : -1;
       }
-      const size_t smem_t = (size_t)kTmaStages * 2 * kStageBytes + 1024;
-      static bool attr_t[16] = {};
-      if (!attr_t[dev]) {
-        if (!cuda_ok(cudaFuncSetAttribute(k_gemm_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem_t),
-                     "op2b_gemm_bf16: shared memory attribute"))
-          return -1;
-        attr_t[dev] = true;
-      }
-      k_gemm_tma<<<grid, kThreads, smem_t, s>>>(g, ta, tb);
       if (rt().initialised) rt().launches++;
-      return cuda_ok(cudaGetLastError(), "op2b_gemm_bf16") ? 0 : -1;
-    }
-    if (engine == 2) {
+      return cuda_ok(e, "op2b_gemm_bf16") ? 0 : -1;
+    } else if (engine == 2) {
       set_error("op2b_gemm_bf16: the operands cannot be described as tensor maps");
       return -1;
     }
-  } else if (engine == 2) {
-    set_error("op2b_gemm_bf16: engine 2 (TMA) needs k-contiguous A and B");
-    return -1;
   }
   const size_t smem = 4 * (size_t)kStageBytes + 1024;
   static bool attr[16] = {};

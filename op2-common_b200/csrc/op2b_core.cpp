@@ -168,7 +168,7 @@ static void host_copy(void *dst, const void *src, size_t bytes) {
 // for it); without a renumbering the first large copy pins them itself.
 void stage_in_background() {
   Runtime &r = rt();
-  if (r.stage || r.stage_alloc.joinable()) return;
+  if (!r.opt_host_staging || r.stage || r.stage_alloc.joinable()) return;
   const int dev = r.device;
   r.stage_alloc = std::thread([&r, dev] {
     char *p = nullptr;
@@ -206,6 +206,23 @@ bool download_host_many(const std::vector<HostDownload> &jobs, const char *what)
                         std::min(kChunk, j.bytes - off)});
   }
   if (pieces.empty()) return cuda_ok(cudaStreamSynchronize(r.stream), what);
+  if (!r.opt_host_staging) {  // the driver's own copies into pageable memory
+    const auto t0 = std::chrono::steady_clock::now();
+    size_t total = 0;
+    for (const auto &p : pieces) {
+      if (!cuda_ok(cudaMemcpyAsync(p.dst, p.src, p.len, cudaMemcpyDeviceToHost, r.stream), what))
+        return false;
+      total += p.len;
+    }
+    const bool ok = cuda_ok(cudaStreamSynchronize(r.stream), what);
+    if (r.opt_diags > 2) {
+      const double ms = std::chrono::duration<double, std::milli>(
+                            std::chrono::steady_clock::now() - t0).count();
+      fprintf(stderr, "%s: %.1f MB by the driver's pageable copies in %.2f ms (%.1f GB/s)\n",
+              what, total / 1e6, ms, total / 1e6 / ms);
+    }
+    return ok;
+  }
   const auto t0 = std::chrono::steady_clock::now();
   if (r.stage_alloc.joinable()) r.stage_alloc.join();
   if (!r.stage &&
@@ -545,6 +562,7 @@ void op_exit(void) {
   r.ring_used = 0;
   r.opt_gemm_tma = d.opt_gemm_tma;
   r.opt_gemm_ws = d.opt_gemm_ws;
+  r.opt_host_staging = d.opt_host_staging;
   r.opt_check_plans = d.opt_check_plans;
 }
 
@@ -1145,6 +1163,8 @@ int op2b_set_option(const char *key, long value) {
     r.opt_atomic_seg = value != 0;
   } else if (k == "gemm_tma") {
     r.opt_gemm_tma = value != 0;
+  } else if (k == "host_staging") {
+    r.opt_host_staging = value != 0;
   } else if (k == "gemm_persistent") {
     if (value < 0 || value > 2) {
       set_error("op2b_set_option: gemm_persistent must be 0 (a CTA per tile), 1 (persistent, "
@@ -1224,6 +1244,7 @@ long op2b_get_option(const char *key) {
   if (k == "ring_used") return r.ring_used;  // read-only
   if (k == "gemm_tma") return r.opt_gemm_tma;
   if (k == "gemm_persistent") return r.opt_gemm_ws;
+  if (k == "host_staging") return r.opt_host_staging;
   if (k == "gather_kernel") return r.opt_gather_kernel;
   if (k == "pipe_block") return r.opt_pipe_block;
   if (k == "pipe_hints") return r.opt_pipe_hints;

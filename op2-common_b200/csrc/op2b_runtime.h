@@ -135,6 +135,9 @@ struct Runtime {
   int opt_atomic_seg = 1;     // inc_mode 0: 1 = segmented (warp-combined) atomics, 0 = per edge
   int ring_used = 0;          // the last res_calc launch ran over the flux-ring records
   int opt_gemm_tma = 0;       // op2b_gemm_bf16 engine 0: TMA-fed kernel for k-major operands
+  int opt_host_staging = 1;   // large device -> pageable host copies: 0 the driver's copies,
+                              // 1 through two pinned staging buffers (pinned while op_renumber
+                              // waits for the device)
   int opt_gemm_ws = 2;        // TMA-fed products: 0 = a CTA per tile, 1 / 2 = the persistent
                               // warp-specialised kernel with 8 / 16 epilogue warps
   bool opt_check_plans = false;
@@ -214,7 +217,7 @@ bool cuda_ok(cudaError_t e, const char *what);
 // Device -> pageable host copy on the library stream, through pinned buffers
 // with the host-side copies spread over threads (synchronous).
 bool download_host(void *dst, const void *src_d, size_t bytes, const char *what);
-constexpr size_t kStageChunk = (size_t)16 << 20;
+constexpr size_t kStageChunk = (size_t)4 << 20;
 // pin the staging buffers on a thread of their own (op_renumber, while the
 // device works)
 void stage_in_background();

@@ -248,9 +248,10 @@ class GraphNet:
 
     def _gemm(self, M, N, K, A, a_m, a_k, B, b_n, b_k, C, ldc, epi, bias=None, Z=None, R=None,
               ldr=0, split=1):
-        # k-contiguous operands go to the TMA-fed kernel (engine 2) unless
-        # gemm_tma is off; the others to the register-staged one (engine 0)
-        engine = 2 if (self.gemm_tma and a_k == 1 and b_k == 1) else 0
+        # every product goes to the TMA-fed persistent kernel (engine 2: k-
+        # contiguous operands as K-major tiles, the others as MN-major tiles)
+        # unless gemm_tma is off (engine 0, operands staged through registers)
+        engine = 2 if self.gemm_tma else 0
         _call("op2b_gemm_bf16", M, N, K, A, a_m, a_k, B, b_n, b_k, C, ldc, epi, bias, Z, R, ldr,
               split, engine, self.stream)
         self.launches += 1

@@ -212,13 +212,52 @@ def test_gemm_persistent_kernel_matches_per_tile_kernel(op2, shape):
         assert _rel(_np(c1), _np(a) @ _np(b).T) < 2e-5
 
 
-def test_gemm_tma_engine_refuses_transposed_operands(op2):
+def test_gemm_tma_engine_refuses_transposed_operands_one_tile_per_cta(op2):
+    op2.set_option("gemm_persistent", 0)
     A = torch.zeros(64, 128, dtype=torch.bfloat16, device="cuda")
     C = torch.zeros(128, 128, device="cuda")
     rc = G._lib().op2b_gemm_bf16(128, 128, 64, A.data_ptr(), 1, 128, A.data_ptr(), 1, 128,
                                  C.data_ptr(), 128, G.EPI_STORE_F32, None, None, None, 0, 1, 2,
                                  torch.cuda.current_stream().cuda_stream)
+    op2.set_option("gemm_persistent", 2)
     assert rc == -1 and "k-contiguous" in L.last_error()
+
+
+@pytest.mark.parametrize("layout", ["a_mn", "b_mn", "both_mn"])
+@pytest.mark.parametrize("shape", [(128, 128, 64), (304, 136, 520), (128, 384, 40000),
+                                   (8, 128, 20000), (20000, 256, 128)])
+def test_gemm_persistent_mn_major_operands(op2, shape, layout):
+    """Transposed operands on engine 2: the persistent kernel loads them by
+    TMA as MN-major tiles (two 64 x 64 boxes, 128-byte swizzle) and the MMAs
+    read them through MN-major descriptors.  Against engine 0 (which
+    transposes them in registers into K-major tiles) and float64."""
+    M_, N, K = shape
+    rng = np.random.default_rng(M_ + 3 * N + 5 * K)
+    a = _bf(rng.standard_normal((M_, K)) * 0.2)
+    b = _bf(rng.standard_normal((N, K)) * 0.2)
+    ref = _np(a) @ _np(b).T
+    if layout in ("a_mn", "both_mn"):
+        A, a_m, a_k = a.t().contiguous().cuda(), 1, M_   # stored K x M
+    else:
+        A, a_m, a_k = a.cuda(), K, 1
+    if layout in ("b_mn", "both_mn"):
+        B, b_n, b_k = b.t().contiguous().cuda(), 1, N    # stored K x N
+    else:
+        B, b_n, b_k = b.cuda(), K, 1
+    outs = []
+    for engine in (2, 0):
+        C = torch.zeros(M_, N, device="cuda")
+        _gemm(M_, N, K, A, a_m, a_k, B, b_n, b_k, C, N, G.EPI_STORE_F32, engine=engine)
+        S = torch.zeros(M_, N, device="cuda")
+        _gemm(M_, N, K, A, a_m, a_k, B, b_n, b_k, S, N, G.EPI_ATOMIC_F32, split=3, engine=engine)
+        outs.append((C, S))
+    torch.cuda.synchronize()
+    assert G._lib().op2b_gemm_error(1) == 0
+    (c2, s2), (c0, s0) = outs
+    tol = 2e-5 if K <= 1024 else 2e-4     # FP32 accumulation over K terms
+    assert _rel(_np(c2), ref) < tol
+    assert _rel(_np(s2), ref) < tol
+    assert _rel(_np(c2), _np(c0)) < 1e-6
 
 
 def test_gemm_rejects_bad_shapes(op2):
