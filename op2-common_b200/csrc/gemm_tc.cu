@@ -134,10 +134,31 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   return true;
 }
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+// SiLU and its derivative with the fast exponential and division (a few
+// ulp in FP32; the results are rounded to BF16).  Below z = -87 the
+// denominator passes 2^126 and the fast division gives 0, as the values
+// round to next to nothing anyway.
+__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 __device__ __forceinline__ float silu_grad(float z) {
-  const float s = 1.0f / (1.0f + __expf(-z));
+  const float s = __fdividef(1.0f, 1.0f + __expf(-z));
   return s * (1.0f + z * (1.0f - s));
+}
+
+// bias[col .. col + n) into v (16-byte loads when aligned)
+__device__ __forceinline__ void add_bias16(float *v, const float *bias, int col, int n) {
+  const float *b = bias + col;
+  if (n == 16 && (reinterpret_cast<uintptr_t>(b) & 15) == 0) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const float4 t = __ldg(reinterpret_cast<const float4 *>(b) + i);
+      v[4 * i] += t.x;
+      v[4 * i + 1] += t.y;
+      v[4 * i + 2] += t.z;
+      v[4 * i + 3] += t.w;
+    }
+  } else {
+    FOR_LT_N(i) v[i] += b[i];
+  }
 }
 
 // Shared-memory tile layout: K-major with the 128-byte swizzle.  Row r of the
@@ -241,7 +262,7 @@ __device__ void epilogue16(const GemmArgs &g, int row, int col, const uint32_t *
   switch (g.epi) {
     case OP2B_EPI_STORE_F32: {
       float *c = reinterpret_cast<float *>(g.C) + o;
-      if (g.bias) FOR_LT_N(i) v[i] += g.bias[col + i];
+      if (g.bias) add_bias16(v, g.bias, col, n);
       if (n == 16 && (reinterpret_cast<uintptr_t>(c) & 15) == 0) {
 #pragma unroll
         for (int i = 0; i < 4; i++)
@@ -258,8 +279,7 @@ __device__ void epilogue16(const GemmArgs &g, int row, int col, const uint32_t *
       return;
     }
     case OP2B_EPI_BIAS_BF16: {
-      if (g.bias)
-        FOR_LT_N(i) v[i] += g.bias[col + i];
+      if (g.bias) add_bias16(v, g.bias, col, n);
       if (g.R) {
         float rr[16];
         load_bf16x16(g.R + (long)row * g.ldr + col, rr, n);
@@ -269,8 +289,7 @@ __device__ void epilogue16(const GemmArgs &g, int row, int col, const uint32_t *
       return;
     }
     case OP2B_EPI_BIAS_SILU_BF16: {
-      if (g.bias)
-        FOR_LT_N(i) v[i] += g.bias[col + i];
+      if (g.bias) add_bias16(v, g.bias, col, n);
       if (g.Z) store_bf16x16(g.Z + o, v, n);
       FOR_LT_N(i) v[i] = silu(v[i]);
       store_bf16x16(reinterpret_cast<__nv_bfloat16 *>(g.C) + o, v, n);
