@@ -63,7 +63,19 @@ def _deps_mtime():
 
 
 def build(verbose: bool = False, force: bool = False) -> str:
+    """Compile what is out of date and link libop2b.so.  Processes that build
+    at once (the ranks of one job) take turns through a lock file."""
+    import fcntl
     os.makedirs(BUILD, exist_ok=True)
+    with open(os.path.join(BUILD, ".lock"), "w") as lock:
+        fcntl.flock(lock, fcntl.LOCK_EX)
+        try:
+            return _build(verbose, force)
+        finally:
+            fcntl.flock(lock, fcntl.LOCK_UN)
+
+
+def _build(verbose: bool, force: bool) -> str:
     nvcc = _nvcc()
     hdr_t = _deps_mtime()
     objs = []
@@ -91,11 +103,12 @@ def build(verbose: bool = False, force: bool = False) -> str:
         if verbose:
             print("compiled", base, file=sys.stderr)
     if changed:
-        cmd = [nvcc, *ARCH, "-shared", "-o", LIB + ".tmp", *objs, "-lcuda", "-lnvrtc"]
+        tmp = f"{LIB}.{os.getpid()}.tmp"
+        cmd = [nvcc, *ARCH, "-shared", "-o", tmp, *objs, "-lcuda", "-lnvrtc"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"linking libop2b.so failed:\n{res.stdout}{res.stderr}")
-        os.replace(LIB + ".tmp", LIB)
+        os.replace(tmp, LIB)
         if verbose:
             print("linked", LIB, file=sys.stderr)
     return LIB
