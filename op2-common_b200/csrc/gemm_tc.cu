@@ -58,6 +58,7 @@ struct GemmArgs {
   int epi;
   int k_per_split;
   int *err;
+  int staged;  // k_gemm_ws<16>: C (and Z) 16-byte aligned rows: stores through shared memory
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -645,6 +646,114 @@ __device__ __forceinline__ WsTile ws_tile(const GemmArgs &g, int t, int mtiles, 
   return w;
 }
 
+// The persistent kernel's epilogue through shared memory (16 epilogue warps,
+// 32 rows x 32 columns a warp a tile, taken in two halves of 16 columns).
+// Each lane computes its row's values with the arithmetic of epilogue16 and
+// writes them into the warp's staging rows (padded: 16-byte accesses free of
+// bank conflicts); the warp then stores whole row segments -- four lanes a
+// 64-byte BF16 row, eight a 128-byte FP32 row -- instead of each lane its own
+// row 16 bytes at a time.  Two staging areas: C, and Z for bias + SiLU.
+// Z's BF16 rows follow C's BF16 rows; FP32 rows of C (no Z) take the space of both.
+constexpr int kEpiRowF32 = 32 * 4 + 16, kEpiRowBf16 = 32 * 2 + 16;
+constexpr int kEpiAreaBytes = 32 * kEpiRowBf16;  // offset of Z's area
+constexpr int kEpiStageBytes =
+    32 * kEpiRowF32 > 2 * kEpiAreaBytes ? 32 * kEpiRowF32 : 2 * kEpiAreaBytes;  // per warp
+
+__device__ __forceinline__ void stage_bf16x16(uint8_t *area, int lane, int h, const float *v) {
+#pragma unroll
+  for (int j = 0; j < 2; j++) {
+    uint4 w;
+    __nv_bfloat162 *p = reinterpret_cast<__nv_bfloat162 *>(&w);
+#pragma unroll
+    for (int i = 0; i < 4; i++) p[i] = __floats2bfloat162_rn(v[8 * j + 2 * i], v[8 * j + 2 * i + 1]);
+    *reinterpret_cast<uint4 *>(area + lane * kEpiRowBf16 + h * 32 + j * 16) = w;
+  }
+}
+
+__device__ __forceinline__ void stage_f32x16(uint8_t *area, int lane, int h, const float *v) {
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+    *reinterpret_cast<float4 *>(area + lane * kEpiRowF32 + h * 64 + j * 16) =
+        make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+}
+
+__device__ __forceinline__ void store_rows_bf16(const uint8_t *area, int lane, int ncols,
+                                                __nv_bfloat16 *dst, long ld, int row0, int col0,
+                                                int M) {
+  const int seg = lane & 3;
+#pragma unroll
+  for (int pass = 0; pass < 4; pass++) {
+    const int r = pass * 8 + (lane >> 2);
+    if (row0 + r < M && seg * 8 < ncols)
+      *reinterpret_cast<uint4 *>(dst + (long)(row0 + r) * ld + col0 + seg * 8) =
+          *reinterpret_cast<const uint4 *>(area + r * kEpiRowBf16 + seg * 16);
+  }
+}
+
+__device__ __forceinline__ void store_rows_f32(const uint8_t *area, int lane, int ncols,
+                                               float *dst, long ld, int row0, int col0, int M) {
+  const int seg = lane & 7;
+#pragma unroll
+  for (int pass = 0; pass < 8; pass++) {
+    const int r = pass * 4 + (lane >> 3);
+    if (row0 + r < M && seg * 4 < ncols)
+      *reinterpret_cast<float4 *>(dst + (long)(row0 + r) * ld + col0 + seg * 4) =
+          *reinterpret_cast<const float4 *>(area + r * kEpiRowF32 + seg * 16);
+  }
+}
+
+// half h (columns col0 + 16h ..) of the lane's row into the staging areas
+__device__ __forceinline__ void epilogue_half(const GemmArgs &g, uint8_t *stage, int lane,
+                                              int row, int col, int n, int h, float *v) {
+  uint8_t *areaC = stage, *areaZ = stage + kEpiAreaBytes;
+  const bool live = row < g.M;
+  switch (g.epi) {
+    case OP2B_EPI_STORE_F32:
+      if (g.bias && n > 0) add_bias16(v, g.bias, col, n);
+      stage_f32x16(areaC, lane, h, v);
+      return;
+    case OP2B_EPI_BIAS_BF16:
+      if (g.bias && n > 0) add_bias16(v, g.bias, col, n);
+      if (g.R && live && n > 0) {
+        float rr[16];
+        load_bf16x16(g.R + (long)row * g.ldr + col, rr, n);
+        FOR_LT_N(i) v[i] += rr[i];
+      }
+      stage_bf16x16(areaC, lane, h, v);
+      return;
+    case OP2B_EPI_BIAS_SILU_BF16:
+      if (g.bias && n > 0) add_bias16(v, g.bias, col, n);
+      stage_bf16x16(areaZ, lane, h, v);
+#pragma unroll
+      for (int i = 0; i < 16; i++) v[i] = silu(v[i]);
+      stage_bf16x16(areaC, lane, h, v);
+      return;
+    case OP2B_EPI_SILU_GRAD_BF16:
+      if (live && n > 0) {
+        float z[16];
+        load_bf16x16(g.R + (long)row * g.ldr + col, z, n);
+        FOR_LT_N(i) v[i] *= silu_grad(z[i]);
+      }
+      stage_bf16x16(areaC, lane, h, v);
+      return;
+    default:
+      stage_bf16x16(areaC, lane, h, v);
+  }
+}
+
+// the staged rows of the warp out to C (and Z)
+__device__ __forceinline__ void epilogue_store(const GemmArgs &g, const uint8_t *stage, int lane,
+                                               int row0, int col0, int ncols) {
+  if (g.epi == OP2B_EPI_STORE_F32) {
+    store_rows_f32(stage, lane, ncols, reinterpret_cast<float *>(g.C), g.ldc, row0, col0, g.M);
+    return;
+  }
+  if (g.epi == OP2B_EPI_BIAS_SILU_BF16 && g.Z)
+    store_rows_bf16(stage + kEpiAreaBytes, lane, ncols, g.Z, g.ldc, row0, col0, g.M);
+  store_rows_bf16(stage, lane, ncols, reinterpret_cast<__nv_bfloat16 *>(g.C), g.ldc, row0, col0,
+                  g.M);
+}
+
 template <int EW, bool AMN, bool BMN>
 __global__ void __launch_bounds__(64 + 32 * EW, 1)
 k_gemm_ws(GemmArgs g, const __grid_constant__ CUtensorMap ta,
@@ -775,6 +884,8 @@ k_gemm_ws(GemmArgs g, const __grid_constant__ CUtensorMap ta,
     const int quarter = warp & 3;
     constexpr int kCols = kTileN / (EW / 4);
     const int c0 = ((warp - 2) >> 2) * kCols;
+    // the warp's staging rows, after the operand ring (EW == 16 only)
+    uint8_t *epi_stage = smem + (size_t)kWsStages * 2 * kStageBytes + (warp - 2) * kEpiStageBytes;
     int i = 0;
     for (int t = blockIdx.x; t < ntotal; t += gridDim.x, i++) {
       const WsTile w = ws_tile(g, t, mtiles, ntiles);
@@ -793,6 +904,42 @@ k_gemm_ws(GemmArgs g, const __grid_constant__ CUtensorMap ta,
         __syncwarp();
         if (lane == 0)
           asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(acc_empty(b)) : "memory");
+        continue;
+      }
+      if (EW == 16 && g.staged) {  // 32 columns: the row-coalesced epilogue
+        // the warp's columns of the matrix (nt is rounded up to 16; N is not)
+        const int nv = min(ce, g.N - w.n0) - c0;
+#pragma unroll 1
+        for (int h = 0; h < 2; h++) {
+          uint32_t r[16];
+#pragma unroll
+          for (int k = 0; k < 16; k++) r[k] = 0u;
+          if (w.nk > 0 && c0 + 16 * h < ce) {
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                  "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+                  "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                : "r"(src + (uint32_t)(c0 + 16 * h)));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          }
+          if (h == 1) {  // the warp's part has been read: the MMAs may reuse it
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0)
+              asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(acc_empty(b))
+                           : "memory");
+          }
+          float v[16];
+#pragma unroll
+          for (int k = 0; k < 16; k++) v[k] = __uint_as_float(r[k]);
+          epilogue_half(g, epi_stage, lane, row, w.n0 + c0 + 16 * h,
+                        min(16, nv - 16 * h), h, v);
+        }
+        __syncwarp();
+        epilogue_store(g, epi_stage, lane, w.m0 + quarter * 32, w.n0 + c0, nv);
+        __syncwarp();
         continue;
       }
       for (int cc = c0; cc < ce; cc += 16) {
@@ -911,7 +1058,8 @@ bool operand_map_mn(CUtensorMap *m, const void *base, int mn, int K, long ld) {
 template <int EW, bool AMN, bool BMN>
 cudaError_t launch_ws(const GemmArgs &g, const CUtensorMap &ta, const CUtensorMap &tb,
                       dim3 grid, int nsm, cudaStream_t s) {
-  const size_t smem_w = (size_t)kWsStages * 2 * kStageBytes + 1024;
+  const size_t smem_w =
+      (size_t)kWsStages * 2 * kStageBytes + (EW == 16 ? 16 * kEpiStageBytes : 0) + 1024;
   cudaError_t e = cudaFuncSetAttribute(k_gemm_ws<EW, AMN, BMN>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_w);
   if (e != cudaSuccess) return e;
@@ -971,6 +1119,12 @@ extern "C" int op2b_gemm_bf16(int M, int N, int K, const void *A, long a_m, long
   GemmArgs g{M,   N,   K,   (const __nv_bfloat16 *)A, a_m, a_k, (const __nv_bfloat16 *)B,
              b_n, b_k, C,   ldc, bias, (__nv_bfloat16 *)Z,     (const __nv_bfloat16 *)R,
              ldr, epi, 0,   g_err_dev[dev]};
+  {  // rows of C (and Z) that 16-byte stores can cover
+    const long esize = epi == OP2B_EPI_STORE_F32 ? 4 : 2;
+    g.staged = rt().opt_gemm_rows && epi != OP2B_EPI_ATOMIC_F32 &&
+               (reinterpret_cast<uintptr_t>(C) & 15) == 0 && (ldc * esize) % 16 == 0 &&
+               (reinterpret_cast<uintptr_t>(Z) & 15) == 0;
+  }
   if (engine == 1) {
     if (epi != OP2B_EPI_STORE_F32) {
       set_error("op2b_gemm_bf16: the CUDA-core path stores FP32 only");

@@ -562,6 +562,7 @@ void op_exit(void) {
   r.ring_used = 0;
   r.opt_gemm_tma = d.opt_gemm_tma;
   r.opt_gemm_ws = d.opt_gemm_ws;
+  r.opt_gemm_rows = d.opt_gemm_rows;
   r.opt_host_staging = d.opt_host_staging;
   r.opt_check_plans = d.opt_check_plans;
 }
@@ -1163,6 +1164,8 @@ int op2b_set_option(const char *key, long value) {
     r.opt_atomic_seg = value != 0;
   } else if (k == "gemm_tma") {
     r.opt_gemm_tma = value != 0;
+  } else if (k == "gemm_rows") {
+    r.opt_gemm_rows = value != 0;
   } else if (k == "host_staging") {
     r.opt_host_staging = value != 0;
   } else if (k == "gemm_persistent") {
@@ -1245,6 +1248,7 @@ long op2b_get_option(const char *key) {
   if (k == "gemm_tma") return r.opt_gemm_tma;
   if (k == "gemm_persistent") return r.opt_gemm_ws;
   if (k == "host_staging") return r.opt_host_staging;
+  if (k == "gemm_rows") return r.opt_gemm_rows;
   if (k == "gather_kernel") return r.opt_gather_kernel;
   if (k == "pipe_block") return r.opt_pipe_block;
   if (k == "pipe_hints") return r.opt_pipe_hints;

@@ -138,6 +138,7 @@ struct Runtime {
   int opt_host_staging = 1;   // large device -> pageable host copies: 0 the driver's copies,
                               // 1 through two pinned staging buffers (pinned while op_renumber
                               // waits for the device)
+  int opt_gemm_rows = 1;      // persistent GEMM: stores whole rows through shared memory
   int opt_gemm_ws = 2;        // TMA-fed products: 0 = a CTA per tile, 1 / 2 = the persistent
                               // warp-specialised kernel with 8 / 16 epilogue warps
   bool opt_check_plans = false;

@@ -4,8 +4,9 @@
 
 M = rows (messages of 8 copies of the 200x100 cell graph by default), N = 128,
 K and epilogue as the network's products use them.  Each product runs on
-engine 2 with the persistent kernel (16 and 8 epilogue warps), engine 2 one
-CTA per tile, and engine 0; one JSON line per run with the mean CUDA-event
+engine 2 with the persistent kernel (16 epilogue warps storing whole rows
+through shared memory, and each lane its own row; 8 epilogue warps), engine 2
+one CTA per tile, and engine 0; one JSON line per run with the mean CUDA-event
 time of `reps` launches after 3 untimed, and GB/s over the bytes of A, B and
 the outputs (C, and Z for bias+SiLU).
 """
@@ -37,8 +38,9 @@ def main():
         C = torch.zeros(M, N, device="cuda", dtype=torch.float32 if f32 else torch.bfloat16)
         Z = None if f32 or epi != G.EPI_BIAS_SILU_BF16 else torch.zeros_like(C)
         out_bytes = M * N * (4 if f32 else 2) * (2 if Z is not None else 1)
-        for engine, pers in ((2, 2), (2, 1), (2, 0), (0, 0)):
+        for engine, pers, rows in ((2, 2, 1), (2, 2, 0), (2, 1, 0), (2, 0, 0), (0, 0, 0)):
             L.set_option("gemm_persistent", pers)
+            L.set_option("gemm_rows", rows)
 
             def run():
                 rc = G._lib().op2b_gemm_bf16(M, N, K, A.data_ptr(), K, 1, B.data_ptr(), K, 1,
@@ -61,9 +63,10 @@ def main():
             us = e0.elapsed_time(e1) * 1e3 / a.reps
             byts = M * K * 2 + N * K * 2 + out_bytes
             print(json.dumps({"M": M, "N": N, "K": K, "epi": epi, "engine": engine,
-                              "gemm_persistent": pers, "us": round(us, 1),
+                              "gemm_persistent": pers, "gemm_rows": rows, "us": round(us, 1),
                               "gbs": round(byts / us / 1e3)}), flush=True)
     L.set_option("gemm_persistent", 2)
+    L.set_option("gemm_rows", 1)
     torch.cuda.synchronize()
     if G._lib().op2b_gemm_error(1) != 0:
         raise RuntimeError("a GEMM wait timed out")

@@ -177,13 +177,16 @@ def test_gemm_tma_engine_epilogues_and_split_k(op2):
 
 
 @pytest.mark.parametrize("shape", [(300, 128, 384), (20000, 128, 8), (40000, 256, 136),
-                                   (300000, 128, 384)])
+                                   (300000, 128, 384), (1000, 136, 64), (5000, 8, 128),
+                                   (777, 40, 72)])
 def test_gemm_persistent_kernel_matches_per_tile_kernel(op2, shape):
     """engine 2's persistent warp-specialised kernel (one CTA per SM walking
     the tiles, TMEM accumulator double-buffered so a tile's epilogue overlaps
-    the next tile's loads and MMAs; 8 or 16 epilogue warps) against the
-    one-tile-per-CTA TMA kernel (option gemm_persistent 0): bit for bit, FP32
-    store and bias+SiLU with the pre-activation, and split-K to rounding."""
+    the next tile's loads and MMAs; 8 or 16 epilogue warps, rows stored
+    through shared memory or by each lane) against the one-tile-per-CTA TMA
+    kernel (option gemm_persistent 0): bit for bit, FP32 store and bias+SiLU
+    with the pre-activation, and split-K to rounding; N not a multiple of the
+    tile or of a warp's columns included."""
     M_, N, K = shape
     rng = np.random.default_rng(M_ + 7 * N + K)
     a = _bf(rng.standard_normal((M_, K)) * 0.2)
@@ -191,8 +194,9 @@ def test_gemm_persistent_kernel_matches_per_tile_kernel(op2, shape):
     bias = torch.from_numpy(rng.standard_normal(N).astype(np.float32)).cuda()
     A, B = a.cuda(), b.cuda()
     outs = []
-    for persistent in (1, 2, 0):
+    for persistent, rows in ((1, 0), (2, 1), (2, 0), (0, 0)):
         op2.set_option("gemm_persistent", persistent)
+        op2.set_option("gemm_rows", rows)
         C = torch.zeros(M_, N, device="cuda")
         _gemm(M_, N, K, A, K, 1, B, K, 1, C, N, G.EPI_STORE_F32, engine=2)
         H = torch.zeros(M_, N, dtype=torch.bfloat16, device="cuda")
@@ -201,7 +205,8 @@ def test_gemm_persistent_kernel_matches_per_tile_kernel(op2, shape):
         S = torch.zeros(M_, N, device="cuda")
         _gemm(M_, N, K, A, K, 1, B, K, 1, S, N, G.EPI_ATOMIC_F32, split=2, engine=2)
         outs.append((C, H, Z, S))
-    op2.set_option("gemm_persistent", 1)
+    op2.set_option("gemm_persistent", 2)
+    op2.set_option("gemm_rows", 1)
     torch.cuda.synchronize()
     assert G._lib().op2b_gemm_error(1) == 0
     (c0, h0, z0, s0) = outs[-1]
