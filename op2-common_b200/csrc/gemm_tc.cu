@@ -1060,9 +1060,16 @@ cudaError_t launch_ws(const GemmArgs &g, const CUtensorMap &ta, const CUtensorMa
                       dim3 grid, int nsm, cudaStream_t s) {
   const size_t smem_w =
       (size_t)kWsStages * 2 * kStageBytes + (EW == 16 ? 16 * kEpiStageBytes : 0) + 1024;
-  cudaError_t e = cudaFuncSetAttribute(k_gemm_ws<EW, AMN, BMN>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_w);
-  if (e != cudaSuccess) return e;
+  static bool attr[16] = {};  // per device, once
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 16) return cudaErrorInvalidDevice;
+  if (!attr[dev]) {
+    cudaError_t e = cudaFuncSetAttribute(k_gemm_ws<EW, AMN, BMN>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_w);
+    if (e != cudaSuccess) return e;
+    attr[dev] = true;
+  }
   const long long total = (long long)grid.x * grid.y * grid.z;
   const int ctas = (int)std::min<long long>(total, nsm > 0 ? nsm : 148);
   k_gemm_ws<EW, AMN, BMN><<<ctas, 64 + 32 * EW, smem_w, s>>>(g, ta, tb, (int)grid.x,
@@ -1179,8 +1186,13 @@ extern "C" int op2b_gemm_bf16(int M, int N, int K, const void *A, long a_m, long
         else e = launch_ws<8, false, false>(g, ta, tb, grid, nsm, s);
       } else {
         const size_t smem_t = (size_t)kTmaStages * 2 * kStageBytes + 1024;
-        e = cudaFuncSetAttribute(k_gemm_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem_t);
+        static bool attr_t[16] = {};
+        e = cudaSuccess;
+        if (!attr_t[dev]) {
+          e = cudaFuncSetAttribute(k_gemm_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem_t);
+          attr_t[dev] = e == cudaSuccess;
+        }
         if (e == cudaSuccess) {
           k_gemm_tma<<<grid, kThreads, smem_t, s>>>(g, ta, tb);
           e = cudaGetLastError();
