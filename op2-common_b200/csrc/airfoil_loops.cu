@@ -374,6 +374,7 @@ __global__ void __launch_bounds__(THREADS)
 k_update(int ncell, const T *__restrict__ qold, T *__restrict__ q, T *__restrict__ res,
          const T *adt, RedSlot *__restrict__ parts, unsigned *__restrict__ counter,
          RedSlot *__restrict__ out, RedSlot *host_out, long long seq, AdtNext<T> an) {
+  grid_dependency_wait();
   RedTriple t{0.0, -INFINITY, LLONG_MAX};
   int stride = gridDim.x * THREADS;
   for (int n = blockIdx.x * THREADS + threadIdx.x; n < ncell; n += stride) {
@@ -448,26 +449,23 @@ cudaError_t launch_update(const LaunchCtx &c, int ncell, const T *qold, T *q, T 
   constexpr int TH = 256;
   int grid = grid_for(c, ncell, TH, 4);
   if (grid > s.capacity) grid = s.capacity;
+  cudaError_t e;
   if (adt_next) {
     const AdtNext<T> an{reinterpret_cast<const int4 *>(pcell), x, adt_next, *k};
-    if (keep_res)
-      k_update<T, TH, true, true><<<grid, TH, 0, c.stream>>>(ncell, qold, q, res, adt, s.parts,
-                                                             s.counter, s.out, s.host_out,
-                                                             s.seq, an);
-    else
-      k_update<T, TH, true><<<grid, TH, 0, c.stream>>>(ncell, qold, q, res, adt, s.parts,
-                                                       s.counter, s.out, s.host_out, s.seq, an);
-  } else if (keep_res) {
-    k_update<T, TH, false, true><<<grid, TH, 0, c.stream>>>(ncell, qold, q, res, adt, s.parts,
-                                                            s.counter, s.out, s.host_out,
-                                                            s.seq, AdtNext<T>{});
+    e = keep_res ? launch_dependent(c, k_update<T, TH, true, true>, grid, TH, 0, ncell, qold, q,
+                                    res, adt, s.parts, s.counter, s.out, s.host_out, s.seq, an)
+                 : launch_dependent(c, k_update<T, TH, true>, grid, TH, 0, ncell, qold, q, res,
+                                    adt, s.parts, s.counter, s.out, s.host_out, s.seq, an);
   } else {
-    k_update<T, TH, false><<<grid, TH, 0, c.stream>>>(ncell, qold, q, res, adt, s.parts,
-                                                      s.counter, s.out, s.host_out, s.seq,
-                                                      AdtNext<T>{});
+    e = keep_res ? launch_dependent(c, k_update<T, TH, false, true>, grid, TH, 0, ncell, qold, q,
+                                    res, adt, s.parts, s.counter, s.out, s.host_out, s.seq,
+                                    AdtNext<T>{})
+                 : launch_dependent(c, k_update<T, TH, false>, grid, TH, 0, ncell, qold, q, res,
+                                    adt, s.parts, s.counter, s.out, s.host_out, s.seq,
+                                    AdtNext<T>{});
   }
   c.count();
-  return cudaGetLastError();
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 // ---------------------------------------------------------------- instantiations

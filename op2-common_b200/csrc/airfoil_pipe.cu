@@ -505,6 +505,7 @@ k_res_bres_corner(int ncell, const int4 *__restrict__ rec_o, const int4 *__restr
                   AirConst<T> k, BresLink bl) {
   const int G = gridDim.x * NT;
   int c = blockIdx.x * NT + threadIdx.x;
+  grid_dependency_wait();
   if (c >= ncell) return;
   CornerOps<T> cur, nxt;
   CornerRec r1 = load_crec(rec_o, rec_cn, rec_meta, c + G, ncell);
@@ -568,11 +569,11 @@ cudaError_t launch_res_bres_corner(const LaunchCtx &ctx, const SlotRecords &s,
     long long blocks = (long long)ctx.nsm * (per_sm < 1 ? 1 : per_sm);
     const long long need = (s.ncell + nt - 1) / nt;
     if (blocks > need) blocks = need;
-    kern<<<(unsigned)blocks, nt, 0, ctx.stream>>>(
-        s.ncell, reinterpret_cast<const int4 *>(s.o), reinterpret_cast<const int4 *>(s.cn),
-        s.meta, x, q, adt, res, k, bl);
+    e = launch_dependent(ctx, kern, dim3((unsigned)blocks), dim3(nt), 0, s.ncell,
+                         reinterpret_cast<const int4 *>(s.o), reinterpret_cast<const int4 *>(s.cn),
+                         s.meta, x, q, adt, res, k, bl);
     ctx.count();
-    return cudaGetLastError();
+    return e != cudaSuccess ? e : cudaGetLastError();
   };
   if (zero_res)
     return block == 128 ? run(k_res_bres_corner<T, 128, true>, 128)

@@ -13,10 +13,41 @@ struct LaunchCtx {
   cudaStream_t stream;
   int nsm;                 // SMs on the device (148 on B200)
   long *launch_counter;    // incremented once per kernel launch
+  bool pdl = false;        // programmatic dependent launch for the kernels that wait for it
   void count() const {
     if (launch_counter) ++*launch_counter;
   }
 };
+
+// Launch `kern` on ctx's stream, with programmatic dependent launch when
+// ctx.pdl: the kernel's CTAs may start as the previous kernel's finish, and
+// the kernel itself waits (griddepcontrol.wait, grid_dependency_wait below)
+// for the previous grid to complete before it touches memory.  Only kernels
+// that make that wait their first step may be launched this way.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_dependent(const LaunchCtx &ctx, void (*kern)(KArgs...), dim3 grid, dim3 block,
+                             size_t smem, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = ctx.stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = ctx.pdl ? at : nullptr;
+  cfg.numAttrs = ctx.pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
+// First step of a kernel launched by launch_dependent: let the next kernel in
+// the stream be launched (its CTAs still wait for this grid to complete),
+// then wait for the previous grid's completion and memory.  Without
+// programmatic launch both are no-ops.
+__device__ __forceinline__ void grid_dependency_wait() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
 
 // One partial of the fused update reduction (32 bytes).
 struct RedSlot {

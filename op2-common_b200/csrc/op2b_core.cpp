@@ -300,7 +300,7 @@ bool is_real(const char *type, int bytes) {
   return (bytes == 8 && t == "double") || (bytes == 4 && t == "float");
 }
 
-LaunchCtx Runtime::ctx() { return LaunchCtx{stream, nsm, &launches}; }
+LaunchCtx Runtime::ctx() { return LaunchCtx{stream, nsm, &launches, opt_pdl != 0}; }
 
 // launch a deferred loop before a call that observes the library's state
 // (restore: also put adt back if an update wrote it early -- for calls that
@@ -321,9 +321,16 @@ bool Runtime::ready() {
 
 // ------------------------------------------------------------------ timing
 
+// Device time per loop by CUDA events around its launches: one call in
+// opt_timing_stride of each loop (every call inside a profiled region), so
+// that the events, which keep consecutive kernels from overlapping their
+// launch, stay off most calls.  Totals are the sampled mean times the calls.
 void Runtime::begin_loop(const char *name) {
   cur_loop = name;
+  cur_ev0 = cur_ev1 = nullptr;
   if (!opt_timing) return;
+  const long calls = stats[cur_loop].calls;
+  if (opt_timing_stride > 1 && calls % opt_timing_stride != 0 && !profile_times_loops()) return;
   if (ev_free.size() < 2) {
     for (int i = 0; i < 64; i++) {
       cudaEvent_t e;
@@ -341,7 +348,7 @@ void Runtime::end_loop(double bytes) {
   LoopStat &s = stats[cur_loop];
   s.calls++;
   s.bytes_per_call = bytes;
-  if (!opt_timing) return;
+  if (!opt_timing || !cur_ev0) return;
   cudaEventRecord(cur_ev1, stream);
   pending.push_back(PendingTime{cur_loop, cur_ev0, cur_ev1, profile_loop_node(cur_loop)});
   if (pending.size() > 4096) resolve_timing();
@@ -563,6 +570,8 @@ void op_exit(void) {
   r.opt_gemm_tma = d.opt_gemm_tma;
   r.opt_gemm_ws = d.opt_gemm_ws;
   r.opt_gemm_rows = d.opt_gemm_rows;
+  r.opt_pdl = d.opt_pdl;
+  r.opt_timing_stride = d.opt_timing_stride;
   r.opt_host_staging = d.opt_host_staging;
   r.opt_check_plans = d.opt_check_plans;
 }
@@ -1098,8 +1107,9 @@ void op_timing_output(void) {
          " -----------------------------------------------------------\n");
   for (auto &kv : v) {
     const LoopStat &s = kv.second;
-    double sec = s.total_ms * 1e-3;
-    double gbs = sec > 0 ? s.bytes_per_call * (double)s.timed / sec * 1e-9 : 0.0;
+    const double sampled = s.total_ms * 1e-3;  // over the s.timed sampled calls
+    double sec = s.timed > 0 ? sampled * (double)s.calls / (double)s.timed : 0.0;
+    double gbs = sampled > 0 ? s.bytes_per_call * (double)s.timed / sampled * 1e-9 : 0.0;
     printf(" %6ld;  %8.4f;  %12.6f;  %8.2f;   %s\n", s.calls, s.plan_ms * 1e-3, sec, gbs,
            kv.first.c_str());
   }
@@ -1164,6 +1174,14 @@ int op2b_set_option(const char *key, long value) {
     r.opt_atomic_seg = value != 0;
   } else if (k == "gemm_tma") {
     r.opt_gemm_tma = value != 0;
+  } else if (k == "timing_stride") {
+    if (value < 1) {
+      set_error("op2b_set_option: timing_stride must be at least 1");
+      return -1;
+    }
+    r.opt_timing_stride = (int)value;
+  } else if (k == "pdl") {
+    r.opt_pdl = value != 0;
   } else if (k == "gemm_rows") {
     r.opt_gemm_rows = value != 0;
   } else if (k == "host_staging") {
@@ -1249,6 +1267,8 @@ long op2b_get_option(const char *key) {
   if (k == "gemm_persistent") return r.opt_gemm_ws;
   if (k == "host_staging") return r.opt_host_staging;
   if (k == "gemm_rows") return r.opt_gemm_rows;
+  if (k == "pdl") return r.opt_pdl;
+  if (k == "timing_stride") return r.opt_timing_stride;
   if (k == "gather_kernel") return r.opt_gather_kernel;
   if (k == "pipe_block") return r.opt_pipe_block;
   if (k == "pipe_hints") return r.opt_pipe_hints;
@@ -1274,8 +1294,10 @@ int op2b_loop_stats(const char *name, double *total_ms, long *calls, double *byt
   r.resolve_timing();
   auto it = r.stats.find(name ? name : "");
   if (it == r.stats.end()) return -1;
-  if (total_ms) *total_ms = it->second.total_ms;
-  if (calls) *calls = it->second.calls;
+  const LoopStat &st = it->second;
+  if (total_ms)  // the sampled calls' mean times every call
+    *total_ms = st.timed > 0 ? st.total_ms * (double)st.calls / (double)st.timed : 0.0;
+  if (calls) *calls = st.calls;
   if (bytes_per_call) *bytes_per_call = it->second.bytes_per_call;
   if (last_ms) *last_ms = it->second.last_ms;
   return 0;

@@ -110,6 +110,7 @@ struct Runtime {
   int opt_diags = 0;
   bool opt_abort = false;
   bool opt_timing = true;
+  int opt_timing_stride = 16;  // time one call in this many of each loop (1: every call)
   int opt_block_size = 0;
   int opt_part_size = 0;
   int opt_cache_line = 128;
@@ -138,6 +139,7 @@ struct Runtime {
   int opt_host_staging = 1;   // large device -> pageable host copies: 0 the driver's copies,
                               // 1 through two pinned staging buffers (pinned while op_renumber
                               // waits for the device)
+  int opt_pdl = 1;            // the iteration's kernels by programmatic dependent launch
   int opt_gemm_rows = 1;      // persistent GEMM: stores whole rows through shared memory
   int opt_gemm_ws = 2;        // TMA-fed products: 0 = a CTA per tile, 1 / 2 = the persistent
                               // warp-specialised kernel with 8 / 16 epilogue warps
@@ -211,6 +213,7 @@ Runtime &rt();
 // node a loop starting now is timed into (-1 = none); op_exit's clean-up
 void profile_submit(int id, float ms);
 int profile_loop_node(const std::string &loop);
+bool profile_times_loops();
 void profile_on_exit();
 
 void set_error(const char *fmt, ...);

@@ -173,6 +173,12 @@ void profile_submit(int id, float ms) {
   n.total_ns += ns;
 }
 
+// whether a loop called now is timed into a region of the profile
+bool profile_times_loops() {
+  Profiler &p = prof();
+  return p.started && !p.finished && p.level >= 2 && !p.scope.empty();
+}
+
 // the kernel node a loop called now is timed into (-1: none)
 int profile_loop_node(const std::string &loop) {
   Profiler &p = prof();
