@@ -523,7 +523,7 @@ def main():
         app2 = Airfoil(hm, dtype=dtype, q0=q0)
         ta = time.perf_counter()
         if args.numbering == "rcm":
-            app2.renumber()
+            app2.renumber(stats=False)  # as airfoil.cpp's op_renumber: no bandwidth report
         tb = time.perf_counter()
         e2e_hist = app2.iterate(K)
         tc = time.perf_counter()

@@ -1185,8 +1185,11 @@ int renumber(op_map base, long stats[4]) {
     if (cudaMallocAsync(&reserve, est, s) == cudaSuccess) cudaFreeAsync(reserve, s);
     else cudaGetLastError();  // no reservation: the allocations below ask one by one
   }
-  long bmx, bavg;
-  bandwidth(base, bmx, bavg, s);
+  // the base map's bandwidth before and after: for the caller's statistics
+  // and the diagnostics only
+  const bool want_bw = stats != nullptr || r.opt_diags > 1;
+  long bmx = 0, bavg = 0;
+  if (want_bw) bandwidth(base, bmx, bavg, s);
   lap("bandwidth before");
   std::vector<int *> perm(r.sets.size(), nullptr);
   op_set to = base->to;
@@ -1288,8 +1291,8 @@ int renumber(op_map base, long stats[4]) {
   release_plans();  // plans and inverse maps refer to the old numbering
   release_inverse_maps();
   bool good = cuda_ok(cudaStreamSynchronize(s), "op_renumber") && ok;
-  long amx, aavg;
-  bandwidth(base, amx, aavg, s);
+  long amx = 0, aavg = 0;
+  if (want_bw) bandwidth(base, amx, aavg, s);
   lap("release, bandwidth after");
   if (stats) {
     stats[0] = bmx;

@@ -119,10 +119,11 @@ class Airfoil:
                 hist.append((r, float(self.maxerr[0]), int(self.errloc[0])))
         return hist
 
-    def renumber(self):
+    def renumber(self, stats: bool = True):
         """op_renumber(pecell): RCM on the cell graph, propagated to edges,
-        boundary edges and nodes (the call the reference's MPI Airfoil makes)."""
-        return L.op_renumber(self.pecell)
+        boundary edges and nodes (the call the reference's MPI Airfoil makes);
+        returns the bandwidth statistics unless stats is False."""
+        return L.op_renumber(self.pecell, stats)
 
     def fetch_original(self):
         """q in the order the cells were declared (op_fetch_data_idx)."""

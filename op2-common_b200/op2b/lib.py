@@ -12,7 +12,6 @@ The library must exist (build with op2b.build.build()); there is no fallback.
 from __future__ import annotations
 
 import ctypes
-import mmap
 import os
 
 import numpy as np
@@ -188,12 +187,15 @@ _SIGS.update({
 })
 
 
-def op_renumber(base):
+def op_renumber(base, stats: bool = True):
     """Renumber the mesh from `base` (GPU reverse Cuthill-McKee); returns the
-    base map's bandwidth (max, avg) before and after."""
-    st = (ctypes.c_long * 4)()
+    base map's bandwidth (max, avg) before and after, or None with
+    stats=False (as the C API's op_renumber, which does not measure them)."""
+    st = (ctypes.c_long * 4)() if stats else None
     if load().op2b_renumber(base, st) != 0:
         _check(False, "op_renumber")
+    if not stats:
+        return None
     return dict(before_max=st[0], before_avg=st[1], after_max=st[2], after_avg=st[3])
 
 
@@ -431,29 +433,12 @@ def op_par_loop(name: str, set_, *args):
         _check(False, f"op_par_loop({name})")
 
 
-def _host_array(shape, dtype) -> np.ndarray:
-    """An empty host array; a large one on transparent huge pages (an
-    anonymous mapping with MADV_HUGEPAGE), so that filling it takes a few
-    hundred page faults instead of tens of thousands."""
-    dtype = np.dtype(dtype)
-    count = int(np.prod(shape))
-    nbytes = count * dtype.itemsize
-    if nbytes < (8 << 20) or not hasattr(mmap, "MADV_HUGEPAGE"):
-        return np.empty(shape, dtype=dtype)
-    mm = mmap.mmap(-1, nbytes)
-    try:
-        mm.madvise(mmap.MADV_HUGEPAGE)
-    except OSError:
-        pass
-    return np.frombuffer(mm, dtype=dtype, count=count).reshape(shape)
-
-
 def op_fetch_data(dat) -> np.ndarray:
     d = dat.contents
     t = d.type.decode().split(":")[0]
     dt = {"double": np.float64, "float": np.float32, "int": np.int32}[t]
     n = d.set.contents.size
-    out = _host_array((n, d.dim), dt)
+    out = np.empty((n, d.dim), dtype=dt)
     before = load().op2b_last_error()
     load().op_fetch_data_char(dat, out.ctypes.data)
     after = load().op2b_last_error()
@@ -466,7 +451,7 @@ def op_fetch_data_idx(dat, low: int, high: int) -> np.ndarray:
     d = dat.contents
     t = d.type.decode().split(":")[0]
     dt = {"double": np.float64, "float": np.float32, "int": np.int32}[t]
-    out = _host_array((max(high - low + 1, 0), d.dim), dt)
+    out = np.empty((max(high - low + 1, 0), d.dim), dtype=dt)
     load().op_fetch_data_idx_char(dat, out.ctypes.data, int(low), int(high))
     return out
 
