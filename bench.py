@@ -527,7 +527,7 @@ def main():
         tb = time.perf_counter()
         e2e_hist = app2.iterate(K)
         tc = time.perf_counter()
-        q = L.op_fetch_data(app2.p_q)
+        q = L.op_fetch_data(app2.p_q, out=q0)  # into the pinned array the initial q came from
         t1 = time.perf_counter()
         barrier()
         ms_e2e = max_over_ranks(1e3 * (t1 - t0) / K)
@@ -550,7 +550,8 @@ def main():
                "d2h_bytes_per_step": int(d2h / K),
                "note": f"per iteration of a whole {K}-iteration job through the API: "
                        "op_decl_* uploads (mesh arrays and the initial q pinned), op_renumber, "
-                       "the iterations (rms read back after every update), op_fetch_data(q)"}
+                       "the iterations (rms read back after every update), op_fetch_data(q) "
+                       "into the pinned array the initial q came from"}
         L.op_exit()
 
     # ---------------------------------------------------------- CPU baseline (rank 0, N=1)

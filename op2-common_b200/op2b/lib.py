@@ -433,12 +433,19 @@ def op_par_loop(name: str, set_, *args):
         _check(False, f"op_par_loop({name})")
 
 
-def op_fetch_data(dat) -> np.ndarray:
+def op_fetch_data(dat, out: np.ndarray | None = None) -> np.ndarray:
+    """The dat's values (set size x dim) in a new array, or into `out` (a
+    C-contiguous array of that shape and type, e.g. page-locked memory the
+    caller keeps for its results)."""
     d = dat.contents
     t = d.type.decode().split(":")[0]
     dt = {"double": np.float64, "float": np.float32, "int": np.int32}[t]
     n = d.set.contents.size
-    out = np.empty((n, d.dim), dtype=dt)
+    if out is None:
+        out = np.empty((n, d.dim), dtype=dt)
+    elif out.shape != (n, d.dim) or out.dtype != dt or not out.flags.c_contiguous:
+        raise Op2Error(f"op_fetch_data: out must be a C-contiguous {np.dtype(dt)} array of "
+                       f"shape {(n, d.dim)}")
     before = load().op2b_last_error()
     load().op_fetch_data_char(dat, out.ctypes.data)
     after = load().op2b_last_error()
