@@ -283,14 +283,15 @@ k_res_calc_atomic_seg(int nedge, const int2 *__restrict__ pedge, const int2 *__r
 template <typename T>
 cudaError_t launch_res_calc_atomic(const LaunchCtx &c, int nedge, const int *pedge,
                                    const int *pecell, const T *x, const T *q, const T *adt,
-                                   T *res, const AirConst<T> &k, bool segmented) {
+                                   T *res, const AirConst<T> &k, bool segmented,
+                                   int blocks_per_sm) {
   if (nedge <= 0) return cudaSuccess;
   if (segmented)
-    k_res_calc_atomic_seg<T, 256><<<grid_for(c, nedge, 256, 8), 256, 0, c.stream>>>(
+    k_res_calc_atomic_seg<T, 256><<<grid_for(c, nedge, 256, blocks_per_sm), 256, 0, c.stream>>>(
         nedge, reinterpret_cast<const int2 *>(pedge), reinterpret_cast<const int2 *>(pecell), x,
         q, adt, res, k);
   else
-    k_res_calc_atomic<T><<<grid_for(c, nedge, 256, 8), 256, 0, c.stream>>>(
+    k_res_calc_atomic<T><<<grid_for(c, nedge, 256, blocks_per_sm), 256, 0, c.stream>>>(
         nedge, reinterpret_cast<const int2 *>(pedge), reinterpret_cast<const int2 *>(pecell), x,
         q, adt, res, k);
   c.count();
@@ -517,11 +518,11 @@ template cudaError_t launch_adt_save<float>(const LaunchCtx &, int, const int *,
 template cudaError_t launch_res_calc_atomic<double>(const LaunchCtx &, int, const int *,
                                                     const int *, const double *, const double *,
                                                     const double *, double *,
-                                                    const AirConst<double> &, bool);
+                                                    const AirConst<double> &, bool, int);
 template cudaError_t launch_res_calc_atomic<float>(const LaunchCtx &, int, const int *,
                                                    const int *, const float *, const float *,
                                                    const float *, float *,
-                                                   const AirConst<float> &, bool);
+                                                   const AirConst<float> &, bool, int);
 template cudaError_t launch_bres_calc_atomic<double>(const LaunchCtx &, int, const int *,
                                                      const int *, const int *, const double *,
                                                      const double *, const double *, double *,

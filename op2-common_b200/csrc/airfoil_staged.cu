@@ -229,7 +229,7 @@ cudaError_t run_res_calc(const LaunchCtx &c, const ResCalcArgs<T> &a, Plan *plan
   if (a.nedge <= 0) return cudaSuccess;
   if (mode == OP2B_INC_ATOMIC || !plan)
     return launch_res_calc_atomic<T>(c, a.nedge, a.pedge, a.pecell, a.x, a.q, a.adt, a.res, a.k,
-                                     rt().opt_atomic_seg != 0);
+                                     rt().opt_atomic_seg != 0, rt().opt_atomic_blocks);
   const Plan &pl = *plan;
   ResPlanDev d{};
   d.bsize = pl.bsize;

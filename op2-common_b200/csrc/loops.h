@@ -86,11 +86,13 @@ cudaError_t launch_adt_calc(const LaunchCtx &c, int ncell, const int *pcell, con
 template <typename T>
 cudaError_t launch_adt_save(const LaunchCtx &c, int ncell, const int *pcell, const T *x,
                             const T *q, T *adt, T *qold, const AirConst<T> &k);
-// segmented: a warp's increments to one cell are combined before the atomics
+// segmented: a warp's increments to one cell are combined before the atomics;
+// blocks_per_sm: the grid's 256-thread CTAs per SM, up to one edge a thread
 template <typename T>
 cudaError_t launch_res_calc_atomic(const LaunchCtx &c, int nedge, const int *pedge,
                                    const int *pecell, const T *x, const T *q, const T *adt,
-                                   T *res, const AirConst<T> &k, bool segmented = true);
+                                   T *res, const AirConst<T> &k, bool segmented = true,
+                                   int blocks_per_sm = 4096);
 template <typename T>
 cudaError_t launch_bres_calc_atomic(const LaunchCtx &c, int nbedge, const int *pbedge,
                                     const int *pbecell, const int *bound, const T *x,
