@@ -9,5 +9,6 @@
 #include <stdio.h>
 
 #include "op2b.h"
+#include "op_hdf5.h" /* as op2/include/op_lib_c.h:131 */
 
 #endif /* OP2B_OP_LIB_C_H */

@@ -31,6 +31,7 @@
 
 #include "op2b.h"
 #include "op2b_plan.h"
+#include "op_hdf5.h"
 
 /* op2/include/op_lib_core.h:246-249 */
 #ifndef MIN

@@ -104,7 +104,7 @@ def _build(verbose: bool, force: bool) -> str:
             print("compiled", base, file=sys.stderr)
     if changed:
         tmp = f"{LIB}.{os.getpid()}.tmp"
-        cmd = [nvcc, *ARCH, "-shared", "-o", tmp, *objs, "-lcuda", "-lnvrtc"]
+        cmd = [nvcc, *ARCH, "-shared", "-o", tmp, *objs, "-lcuda", "-lnvrtc", "-lz"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"linking libop2b.so failed:\n{res.stdout}{res.stderr}")

@@ -139,6 +139,33 @@ _SIGS = {
     "op_profile_end": (None, []),
     "op_profile_output": (None, []),
     "op_profile_output_json": (None, [ctypes.c_char_p]),
+    "op_decl_set_hdf5": (op_set, [ctypes.c_char_p, ctypes.c_char_p]),
+    "op_decl_set_hdf5_infer_size": (op_set, [ctypes.c_char_p] * 3),
+    "op_decl_map_hdf5": (op_map, [op_set, op_set, ctypes.c_int, ctypes.c_char_p,
+                                  ctypes.c_char_p]),
+    "op_decl_dat_hdf5": (op_dat, [op_set, ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p,
+                                  ctypes.c_char_p]),
+    "op_get_const_hdf5": (None, [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p,
+                                 ctypes.c_void_p, ctypes.c_char_p]),
+    "op_dump_to_hdf5": (None, [ctypes.c_char_p]),
+    "op_write_const_hdf5": (None, [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p,
+                                   ctypes.c_void_p, ctypes.c_char_p]),
+    "op_fetch_data_hdf5_file": (None, [op_dat, ctypes.c_char_p]),
+    "op_fetch_data_hdf5_file_path": (None, [op_dat, ctypes.c_char_p, ctypes.c_char_p]),
+    "op2b_h5_info": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p,
+                                    ctypes.POINTER(ctypes.c_int),
+                                    ctypes.POINTER(ctypes.c_longlong), ctypes.c_char_p,
+                                    ctypes.c_int]),
+    "op2b_h5_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                    ctypes.c_void_p, ctypes.c_longlong]),
+    "op2b_h5_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                     ctypes.c_int, ctypes.POINTER(ctypes.c_longlong),
+                                     ctypes.c_void_p]),
+    "op2b_h5_set_attr": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                        ctypes.c_char_p, ctypes.c_int, ctypes.c_void_p]),
+    "op2b_h5_get_attr": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                        ctypes.c_char_p, ctypes.c_int]),
+    "op2b_h5_list": (ctypes.c_longlong, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_longlong]),
 }
 
 
@@ -461,6 +488,130 @@ def op_fetch_data_idx(dat, low: int, high: int) -> np.ndarray:
     out = np.empty((max(high - low + 1, 0), d.dim), dtype=dt)
     load().op_fetch_data_idx_char(dat, out.ctypes.data, int(low), int(high))
     return out
+
+
+# ---- HDF5 mesh I/O (include/op_hdf5.h): the OP2 calls, then the host helpers
+
+_H5_DTYPES = {"int": np.int32, "long": np.int64, "long long": np.int64, "float": np.float32,
+              "double": np.float64}
+
+
+def _fails(call):
+    """Run `call`; raise Op2Error if it recorded a new error."""
+    before = load().op2b_last_error()
+    r = call()
+    after = load().op2b_last_error()
+    if after and after != before:
+        raise Op2Error(after.decode())
+    return r
+
+
+def op_decl_set_hdf5(file: str, name: str):
+    return _fails(lambda: load().op_decl_set_hdf5(_b(file), _b(name)))
+
+
+def op_decl_set_hdf5_infer_size(file: str, name: str, set_dataset_name: str):
+    return _fails(lambda: load().op_decl_set_hdf5_infer_size(_b(file), _b(name),
+                                                             _b(set_dataset_name)))
+
+
+def op_decl_map_hdf5(frm, to, dim: int, file: str, name: str):
+    return _fails(lambda: load().op_decl_map_hdf5(frm, to, int(dim), _b(file), _b(name)))
+
+
+def op_decl_dat_hdf5(set_, dim: int, type_: str, file: str, name: str):
+    return _fails(lambda: load().op_decl_dat_hdf5(set_, int(dim), _b(type_), _b(file),
+                                                  _b(name)))
+
+
+def op_get_const_hdf5(name: str, dim: int, type_: str, file: str) -> np.ndarray:
+    out = np.zeros(dim, dtype=_H5_DTYPES[type_])
+    _fails(lambda: load().op_get_const_hdf5(_b(name), int(dim), _b(type_), out.ctypes.data,
+                                            _b(file)))
+    return out
+
+
+def op_dump_to_hdf5(file: str):
+    _fails(lambda: load().op_dump_to_hdf5(_b(file)))
+
+
+def op_write_const_hdf5(name: str, dim: int, type_: str, value, file: str):
+    a = np.ascontiguousarray(value, dtype=_H5_DTYPES[type_]).reshape(-1)
+    _fails(lambda: load().op_write_const_hdf5(_b(name), int(dim), _b(type_), a.ctypes.data,
+                                              _b(file)))
+
+
+def op_fetch_data_hdf5_file(dat, file: str, path: str | None = None):
+    if path is None:
+        _fails(lambda: load().op_fetch_data_hdf5_file(dat, _b(file)))
+    else:
+        _fails(lambda: load().op_fetch_data_hdf5_file_path(dat, _b(file), _b(path)))
+
+
+def h5_info(file: str, path: str):
+    """(shape, OP2 type name) of a dataset, or None when there is none."""
+    rank = ctypes.c_int()
+    dims = (ctypes.c_longlong * 8)()
+    typ = ctypes.create_string_buffer(32)
+    r = load().op2b_h5_info(_b(file), _b(path), ctypes.byref(rank), dims, typ, 32)
+    if r < 0:
+        _check(False, "op2b_h5_info")
+    if r == 1:
+        return None
+    return tuple(dims[k] for k in range(rank.value)), typ.value.decode()
+
+
+def h5_read(file: str, path: str, type_: str | None = None) -> np.ndarray:
+    """A dataset's values as a numpy array of its shape (in `type_`, default
+    the file's own type)."""
+    info = h5_info(file, path)
+    if info is None:
+        raise Op2Error(f"no dataset {path} in {file}")
+    shape, t = info
+    t = type_ or t
+    out = np.empty(shape, dtype=_H5_DTYPES[t])
+    _check(load().op2b_h5_read(_b(file), _b(path), _b(t), out.ctypes.data, out.size) == 0,
+           "op2b_h5_read")
+    return out
+
+
+def h5_write(file: str, path: str, data, type_: str | None = None):
+    a = np.asarray(data, order="C")   # (ascontiguousarray would make a scalar 1-d)
+    t = type_ or {np.dtype(np.int32): "int", np.dtype(np.int64): "long",
+                  np.dtype(np.float32): "float", np.dtype(np.float64): "double"}[a.dtype]
+    a = np.asarray(a, dtype=_H5_DTYPES[t], order="C")
+    dims = (ctypes.c_longlong * max(a.ndim, 1))(*a.shape)
+    _check(load().op2b_h5_write(_b(file), _b(path), _b(t), a.ndim, dims, a.ctypes.data) == 0,
+           "op2b_h5_write")
+
+
+def h5_set_attr(file: str, path: str, name: str, value, type_: str = "int"):
+    if type_ == "string":
+        b = value.encode()
+        r = load().op2b_h5_set_attr(_b(file), _b(path), _b(name), b"string", len(b),
+                                    ctypes.c_char_p(b))
+    else:
+        a = np.ascontiguousarray(value, dtype=_H5_DTYPES[type_]).reshape(-1)
+        r = load().op2b_h5_set_attr(_b(file), _b(path), _b(name), _b(type_), a.size,
+                                    a.ctypes.data)
+    _check(r == 0, "op2b_h5_set_attr")
+
+
+def h5_get_attr(file: str, path: str, name: str) -> str | None:
+    buf = ctypes.create_string_buffer(4096)
+    r = load().op2b_h5_get_attr(_b(file), _b(path), _b(name), buf, 4096)
+    if r < 0:
+        _check(False, "op2b_h5_get_attr")
+    return None if r == 1 else buf.value.decode()
+
+
+def h5_list(file: str) -> list[str]:
+    n = load().op2b_h5_list(_b(file), None, 0)
+    if n < 0:
+        _check(False, "op2b_h5_list")
+    buf = ctypes.create_string_buffer(int(n))
+    load().op2b_h5_list(_b(file), buf, n)
+    return [ln for ln in buf.value.decode().split("\n") if ln]
 
 
 def op_get_size(set_) -> int:
