@@ -506,22 +506,30 @@ def _fails(call):
     return r
 
 
+def _declared(h, what: str):
+    if not h:
+        _check(False, what)
+    return h
+
+
 def op_decl_set_hdf5(file: str, name: str):
-    return _fails(lambda: load().op_decl_set_hdf5(_b(file), _b(name)))
+    return _declared(load().op_decl_set_hdf5(_b(file), _b(name)), "op_decl_set_hdf5")
 
 
 def op_decl_set_hdf5_infer_size(file: str, name: str, set_dataset_name: str):
-    return _fails(lambda: load().op_decl_set_hdf5_infer_size(_b(file), _b(name),
-                                                             _b(set_dataset_name)))
+    return _declared(load().op_decl_set_hdf5_infer_size(_b(file), _b(name),
+                                                        _b(set_dataset_name)),
+                     "op_decl_set_hdf5_infer_size")
 
 
 def op_decl_map_hdf5(frm, to, dim: int, file: str, name: str):
-    return _fails(lambda: load().op_decl_map_hdf5(frm, to, int(dim), _b(file), _b(name)))
+    return _declared(load().op_decl_map_hdf5(frm, to, int(dim), _b(file), _b(name)),
+                     "op_decl_map_hdf5")
 
 
 def op_decl_dat_hdf5(set_, dim: int, type_: str, file: str, name: str):
-    return _fails(lambda: load().op_decl_dat_hdf5(set_, int(dim), _b(type_), _b(file),
-                                                  _b(name)))
+    return _declared(load().op_decl_dat_hdf5(set_, int(dim), _b(type_), _b(file), _b(name)),
+                     "op_decl_dat_hdf5")
 
 
 def op_get_const_hdf5(name: str, dim: int, type_: str, file: str) -> np.ndarray:
