@@ -143,6 +143,11 @@ struct ArgPlan {
   std::string ctype;
   int dim = 1, acc = OP_READ, mdim = 0, idx = -1, bytes = 8;
   int vec = 0;  // vector map argument (idx = -vec): the kernel gets vec pointers
+  // stage 1: a direct dat moved through the warp's shared memory in whole
+  // rows (coalesced), the kernel working on registers; stage 2: an indirect
+  // OP_READ gathered by `vw`-element vector loads into registers
+  int stage = 0, vw = 0;
+  bool seg = false;  // indirect OP_INC combined per warp before the atomics
 };
 
 std::string base_type(const char *t) {
@@ -279,13 +284,52 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
       s << "  " << a.ctype << " op2b_l" << i << "[" << a.dim << "];\n  for (int k = 0; k < "
         << a.dim << "; k++) op2b_l" << i << "[k] = " << identity(a.ctype, a.acc) << ";\n";
   }
-  if (coloured)
+  // warp mode: the loop advances a warp at a time (32 consecutive elements,
+  // every lane reaching each warp-wide step) when a direct dat is staged
+  // through shared memory or an increment is combined per warp
+  bool warp = false;
+  size_t wbytes = 0;  // shared memory a lane needs: the widest staged row (+ padding)
+  for (const ArgPlan &a : ap) {
+    if (a.stage == 1) wbytes = std::max(wbytes, (size_t)(a.dim + 1) * a.bytes);
+    if (a.seg) wbytes = std::max(wbytes, (size_t)a.dim * a.bytes);
+    warp |= a.stage == 1 || a.seg;
+  }
+  wbytes = (wbytes + 15) & ~(size_t)15;
+  if (warp) {
+    s << "  __shared__ __align__(16) unsigned char op2b_sh[" << 256 * wbytes << "];\n"
+      << "  const int op2b_lane = threadIdx.x & 31;\n"
+      << "  unsigned char *op2b_w = op2b_sh + (threadIdx.x >> 5) * " << 32 * wbytes << ";\n"
+      << "  for (int op2b_b = blockIdx.x * blockDim.x + (threadIdx.x & ~31); op2b_b < op2b_n;"
+         " op2b_b += gridDim.x * blockDim.x) {\n"
+      // the element (loads of lanes past the end repeat the last element's;
+      // only lanes with op2b_ok call the kernel and store)
+      << "    const bool op2b_ok = op2b_b + op2b_lane < op2b_n;\n"
+      << "    const int op2b_e = op2b_ok ? op2b_b + op2b_lane : op2b_n - 1;\n"
+      << "    const int op2b_cnt = op2b_n - op2b_b < 32 ? op2b_n - op2b_b : 32;\n";
+    for (size_t i = 0; i < ap.size(); i++) {
+      const ArgPlan &a = ap[i];
+      if (a.stage == 1) {
+        // the warp's rows as whole words, all loads issued before any is used
+        s << "    " << a.ctype << " op2b_y" << i << "[" << a.dim << "];\n#pragma unroll\n"
+          << "    for (int k = 0; k < " << a.dim << "; k++) {\n      const int w = k * 32 + op2b_lane;\n"
+          << "      op2b_y" << i << "[k] = w < op2b_cnt * " << a.dim << " ? op2b_d" << i
+          << "[(size_t)op2b_b * " << a.dim << " + w] : (" << a.ctype << ")0;\n    }\n";
+      }
+      if (a.seg) {
+        const int nv = std::max(a.vec, 1);
+        s << "    " << a.ctype << " op2b_l" << i << "[" << nv * a.dim << "];\n    for (int k = 0; k < "
+          << nv * a.dim << "; k++) op2b_l" << i << "[k] = 0;\n    int op2b_t" << i << "[" << nv
+          << "];\n";
+      }
+    }
+  } else if (coloured) {
     s << "  for (int op2b_i = blockIdx.x * blockDim.x + threadIdx.x; op2b_i < op2b_n;"
          " op2b_i += gridDim.x * blockDim.x) {\n"
          "    const int op2b_e = op2b_perm[op2b_first + op2b_i];\n";
-  else
+  } else {
     s << "  for (int op2b_e = blockIdx.x * blockDim.x + threadIdx.x; op2b_e < op2b_n;"
          " op2b_e += gridDim.x * blockDim.x) {\n";
+  }
   // OP_WORK: every element starts from the caller's values
   for (size_t i = 0; i < ap.size(); i++)
     if (ap[i].kind == GBL && ap[i].acc == OP_WORK)
@@ -297,6 +341,7 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
     if (ap[i].kind == INFO)
       s << "    " << ap[i].ctype << " op2b_s" << i << "[" << ap[i].dim << "];\n    for (int k = 0; k < "
         << ap[i].dim << "; k++) op2b_s" << i << "[k] = op2b_l" << i << "[k];\n";
+  static const char *comp[4] = {".x", ".y", ".z", ".w"};
   std::ostringstream call;
   call << "    " << name << "(";
   for (size_t i = 0; i < ap.size(); i++) {
@@ -304,7 +349,10 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
     if (i) call << ", ";
     switch (a.kind) {
       case DIRECT:
-        call << "op2b_d" << i << " + (size_t)op2b_e * " << a.dim;
+        if (a.stage == 1)
+          call << "op2b_r" << i;
+        else
+          call << "op2b_d" << i << " + (size_t)op2b_e * " << a.dim;
         break;
       case OFF:
         if (a.vec) {
@@ -320,9 +368,12 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
           // one pointer per map entry (op_seq.h op_arg_copy_in); increments
           // into locals added atomically after the call
           s << "    " << a.ctype << " *op2b_v" << i << "[" << a.vec << "];\n";
-          if (a.acc == OP_INC)
+          if (a.acc == OP_INC && !a.seg)
             s << "    " << a.ctype << " op2b_l" << i << "[" << a.vec * a.dim << "];\n"
               << "    for (int k = 0; k < " << a.vec * a.dim << "; k++) op2b_l" << i << "[k] = 0;\n";
+          if (a.seg)
+            s << "    for (int j = 0; j < " << a.vec << "; j++) op2b_t" << i << "[j] = op2b_ok ? op2b_m"
+              << i << "[(size_t)op2b_e * " << a.mdim << " + j] : -1 - op2b_lane;\n";
           s << "    for (int j = 0; j < " << a.vec << "; j++) op2b_v" << i << "[j] = ";
           if (a.acc == OP_INC)
             s << "op2b_l" << i << " + j * " << a.dim << ";\n";
@@ -332,12 +383,32 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
           call << "op2b_vec<" << a.ctype << ">{op2b_v" << i << "}";
           break;
         }
+        if (a.seg) {
+          s << "    op2b_t" << i << "[0] = op2b_ok ? op2b_m" << i << "[(size_t)op2b_e * " << a.mdim
+            << " + " << a.idx << "] : -1 - op2b_lane;\n";
+          call << "op2b_l" << i;
+          break;
+        }
         s << "    const int op2b_t" << i << " = op2b_m" << i << "[(size_t)op2b_e * " << a.mdim
           << " + " << a.idx << "];\n";
         if (a.acc == OP_INC) {
           s << "    " << a.ctype << " op2b_l" << i << "[" << a.dim << "];\n    for (int k = 0; k < "
             << a.dim << "; k++) op2b_l" << i << "[k] = 0;\n";
           call << "op2b_l" << i;
+        } else if (a.stage == 2) {
+          // the row by vector loads into registers
+          const std::string vt = (a.ctype == "double" ? "double" : a.ctype) + std::to_string(a.vw);
+          s << "    " << a.ctype << " op2b_r" << i << "[" << a.dim << "];\n    {\n      const " << vt
+            << " *op2b_p = (const " << vt << " *)(op2b_d" << i << " + (size_t)op2b_t" << i
+            << " * " << a.dim << ");\n";
+          for (int v = 0; v < a.dim / a.vw; v++) {
+            s << "      { const " << vt << " op2b_x = op2b_p[" << v << "];";
+            for (int c = 0; c < a.vw; c++)
+              s << " op2b_r" << i << "[" << v * a.vw + c << "] = op2b_x" << comp[c] << ";";
+            s << " }\n";
+          }
+          s << "    }\n";
+          call << "op2b_r" << i;
         } else {
           call << "op2b_d" << i << " + (size_t)op2b_t" << i << " * " << a.dim;
         }
@@ -360,6 +431,23 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
     }
   }
   call << ");\n";
+  if (warp) {
+    // staged rows from the loaded words through the warp's shared memory
+    // (rows padded by one element against bank conflicts) into registers
+    for (size_t i = 0; i < ap.size(); i++) {
+      const ArgPlan &a = ap[i];
+      if (a.stage != 1) continue;
+      const int P = a.dim + 1;
+      s << "    " << a.ctype << " op2b_r" << i << "[" << a.dim << "];\n    {\n      " << a.ctype
+        << " *op2b_q = (" << a.ctype << " *)op2b_w;\n#pragma unroll\n"
+        << "      for (int k = 0; k < " << a.dim << "; k++) {\n        const int w = k * 32 + op2b_lane;\n"
+        << "        op2b_q[(w / " << a.dim << ") * " << P << " + w % " << a.dim << "] = op2b_y" << i
+        << "[k];\n      }\n      __syncwarp();\n#pragma unroll\n"
+        << "      for (int k = 0; k < " << a.dim << "; k++) op2b_r" << i << "[k] = op2b_q[op2b_lane * "
+        << P << " + k];\n      __syncwarp();\n    }\n";
+    }
+    s << "    if (op2b_ok) {\n";
+  }
   s << call.str();
   // the thread's candidate: its best value, and the element whose call last
   // wrote the payload (an improvement, or a write on a tie)
@@ -373,6 +461,7 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
     }
   for (size_t i = 0; i < ap.size(); i++) {
     const ArgPlan &a = ap[i];
+    if (a.seg) continue;
     if (a.kind == INDIRECT && a.acc == OP_INC && a.vec)
       s << "    for (int j = 0; j < " << a.vec << "; j++) {\n      const size_t t = (size_t)op2b_m"
         << i << "[(size_t)op2b_e * " << a.mdim << " + j] * " << a.dim << ";\n"
@@ -381,6 +470,40 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
     else if (a.kind == INDIRECT && a.acc == OP_INC)
       s << "    for (int k = 0; k < " << a.dim << "; k++) atomicAdd(op2b_d" << i
         << " + (size_t)op2b_t" << i << " * " << a.dim << " + k, op2b_l" << i << "[k]);\n";
+  }
+  if (warp) {
+    s << "    }\n";  // if (op2b_ok)
+    for (size_t i = 0; i < ap.size(); i++) {
+      const ArgPlan &a = ap[i];
+      if (a.stage != 1 || a.acc == OP_READ) continue;
+      // written rows back through shared memory, whole rows per store
+      const int P = a.dim + 1;
+      s << "    {\n      " << a.ctype << " *op2b_q = (" << a.ctype << " *)op2b_w;\n"
+        << "      for (int k = 0; k < " << a.dim << "; k++) op2b_q[op2b_lane * " << P
+        << " + k] = op2b_r" << i << "[k];\n      __syncwarp();\n#pragma unroll\n"
+        << "      for (int k = 0; k < " << a.dim << "; k++) {\n        const int w = k * 32 + op2b_lane;\n"
+        << "        if (w < op2b_cnt * " << a.dim << ") op2b_d" << i << "[(size_t)op2b_b * " << a.dim
+        << " + w] = op2b_q[(w / " << a.dim << ") * " << P << " + w % " << a.dim << "];\n      }\n"
+        << "      __syncwarp();\n    }\n";
+    }
+    for (size_t i = 0; i < ap.size(); i++) {
+      const ArgPlan &a = ap[i];
+      if (!a.seg) continue;
+      // lanes with the same target combine their increments (lowest lane
+      // sums them in lane order) and that lane adds the sum atomically
+      s << "    for (int j = 0; j < " << std::max(a.vec, 1) << "; j++) {\n      " << a.ctype
+        << " *op2b_q = (" << a.ctype << " *)op2b_w;\n      const int op2b_k = op2b_t" << i
+        << "[j];\n      for (int k = 0; k < " << a.dim << "; k++) op2b_q[k * 32 + op2b_lane] = op2b_l"
+        << i << "[j * " << a.dim << " + k];\n      __syncwarp();\n"
+        << "      const unsigned op2b_g = __match_any_sync(0xffffffffu, op2b_k);\n"
+        << "      if (op2b_k >= 0 && op2b_lane == __ffs(op2b_g) - 1)\n"
+        << "        for (int k = 0; k < " << a.dim << "; k++) {\n          " << a.ctype
+        << " op2b_a = op2b_q[k * 32 + op2b_lane];\n"
+        << "          for (unsigned op2b_m = op2b_g & (op2b_g - 1); op2b_m; op2b_m &= op2b_m - 1)\n"
+        << "            op2b_a += op2b_q[k * 32 + __ffs(op2b_m) - 1];\n"
+        << "          atomicAdd(op2b_d" << i << " + (size_t)op2b_k * " << a.dim << " + k, op2b_a);\n"
+        << "        }\n      __syncwarp();\n    }\n";
+    }
   }
   s << "  }\n";
   for (size_t i = 0; i < ap.size(); i++) {
@@ -642,6 +765,51 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
     key << "|" << a.kind << ":" << a.ctype << ":" << a.dim << ":" << a.acc << ":" << a.mdim
         << ":" << a.idx << ":" << a.vec;
   }
+  // option jit_warp: a direct dat that no other argument of the loop names
+  // moves through the warp's shared memory in whole rows (coalesced) and the
+  // kernel works on registers; an indirect dat the loop only reads is
+  // gathered by vector loads; indirect increments are combined per warp
+  // before the atomics.  Not for loops that run colour by colour (their
+  // elements come permuted) except the gathers; rows up to 128 bytes (32
+  // with op_arg_info, whose reduction needs shared memory as well).
+  bool has_info = false, has_red = false;
+  for (auto &a : ap) {
+    has_info |= a.kind == INFO;
+    has_red |= a.kind == INFO || (a.kind == GBL && a.acc != OP_READ && a.acc != OP_WORK);
+  }
+  if (r.opt_jit_warp) {
+    std::map<op_dat, int> uses, writes;
+    for (int i = 0; i < nargs; i++)
+      if (ap[(size_t)i].kind == DIRECT || ap[(size_t)i].kind == INDIRECT) {
+        uses[args[i].dat]++;
+        if (ap[(size_t)i].acc != OP_READ) writes[args[i].dat]++;
+      }
+    const int maxrow = has_info ? 32 : 128;
+    bool gathers = false;
+    for (auto &a : ap) gathers |= a.kind == INDIRECT && a.acc == OP_READ;
+    for (int i = 0; i < nargs; i++) {
+      ArgPlan &a = ap[(size_t)i];
+      const int row = a.dim * a.bytes;
+      // staged: rows the kernel reads (OP_READ, OP_RW, direct OP_INC), a
+      // write-only row is stored by the kernel itself (loading it first cost
+      // more than the scattered stores); read-only rows only in loops without
+      // gathers, whose latency the staging would otherwise add to
+      if (a.kind == DIRECT && !coloured && a.dim > 1 && uses[args[i].dat] == 1 &&
+          row + a.bytes <= maxrow && a.acc != OP_WRITE && (a.acc != OP_READ || !gathers))
+        a.stage = 1;
+      if (a.kind == INDIRECT && !a.vec && a.acc == OP_READ && writes[args[i].dat] == 0) {
+        const uintptr_t base = (uintptr_t)args[i].dat->data_d;
+        const int vw = (row % 16 == 0 && base % 16 == 0) ? 16 / a.bytes
+                       : (row % 8 == 0 && base % 8 == 0 && a.bytes < 8) ? 8 / a.bytes : 0;
+        if (vw >= 2) {
+          a.stage = 2;
+          a.vw = vw;
+        }
+      }
+      if (a.kind == INDIRECT && a.acc == OP_INC && !coloured && row <= maxrow) a.seg = true;
+      key << "|w" << a.stage << a.vw << a.seg;
+    }
+  }
   std::string body;
   std::vector<std::string> seen;
   for (auto &p : sources().preludes) body += expand(p, seen, 0) + "\n";
@@ -795,7 +963,10 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
       n = plan->pub.color2_offsets[c + 1] - first;
     }
     if (n <= 0) continue;
-    grid = (unsigned)std::min<long long>(((long long)n + 255) / 256, max_grid);
+    // a thread per element, unless per-block reduction partials bound the
+    // grid (op_arg_info) or the global reductions' atomics should stay few
+    grid = (unsigned)std::min<long long>(((long long)n + 255) / 256,
+                                         has_red ? max_grid : (long long)INT32_MAX);
     if (!cuda_ok(cudaLaunchKernel((const void *)j.fn, dim3(grid), dim3(256), kp.data(), 0,
                                   r.stream),
                  "op_par_loop: launch")) {

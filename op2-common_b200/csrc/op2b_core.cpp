@@ -566,6 +566,7 @@ void op_exit(void) {
   r.opt_pipe_hints = d.opt_pipe_hints;
   r.opt_plan_mode = d.opt_plan_mode;
   r.opt_atomic_seg = d.opt_atomic_seg;
+  r.opt_jit_warp = d.opt_jit_warp;
   r.opt_atomic_blocks = d.opt_atomic_blocks;
   r.ring_used = 0;
   r.opt_gemm_tma = d.opt_gemm_tma;
@@ -1173,6 +1174,8 @@ int op2b_set_option(const char *key, long value) {
     r.opt_plan_mode = (int)value;
   } else if (k == "atomic_segmented") {
     r.opt_atomic_seg = value != 0;
+  } else if (k == "jit_warp") {
+    r.opt_jit_warp = value != 0;
   } else if (k == "atomic_blocks") {
     if (value < 1 || value > 4096) {
       set_error("op2b_set_option: atomic_blocks must be between 1 and 4096");
@@ -1269,6 +1272,7 @@ long op2b_get_option(const char *key) {
   if (k == "block_size") return r.opt_block_size;
   if (k == "plan_mode") return r.opt_plan_mode;
   if (k == "atomic_segmented") return r.opt_atomic_seg;
+  if (k == "jit_warp") return r.opt_jit_warp;
   if (k == "atomic_blocks") return r.opt_atomic_blocks;
   if (k == "ring_used") return r.ring_used;  // read-only
   if (k == "gemm_tma") return r.opt_gemm_tma;

@@ -522,3 +522,80 @@ def test_temporary_and_overlay_dats(op2):
     mp = op2.op_decl_map(small, big, 1, np.arange(m, dtype=np.int32).reshape(m, 1), "pm")
     with pytest.raises(L.Op2Error, match="overlay"):
         op2.op_renumber(mp)
+
+
+ROWS = """
+inline void gen_rows(const double *a, double *b, float *c, int *d, const double *x1,
+                     const double *x2, double *acc, float **vacc) {
+  for (int k = 0; k < 3; k++) b[k] += a[k] * x1[k % 2] - x2[1];
+  c[0] = 2.0f * c[1] + (float)a[0];
+  c[1] = c[1] - 1.0f;
+  d[0] += d[1];
+  for (int k = 0; k < 4; k++) acc[k] += a[k % 3] * 0.5 + k;
+  for (int j = 0; j < 3; j++) { vacc[j][0] += 1.0f; vacc[j][1] += (float)j; }
+}
+"""
+
+
+@pytest.mark.parametrize("n", [1, 31, 33, 1000, 40963])
+def test_coalesced_rows_gathers_and_warp_combined_increments(op2, n):
+    """The generated loop's warp mode (option jit_warp, the default): direct
+    rows read through shared memory (OP_READ, OP_RW, direct OP_INC of double,
+    float and int rows), a write-only row stored by the kernel, read-only
+    gathers by vector loads, increments combined per warp -- with sets that
+    end inside a warp, every element of a warp incrementing the same target,
+    and a vector map whose entries repeat within an element.  Equal to numpy
+    (exact where no sum is reordered), and to the same loop with jit_warp 0."""
+    op2.register_kernel("gen_rows", ROWS)
+    rng = np.random.default_rng(n)
+    m = 7
+    a = rng.standard_normal((n, 3))
+    b0 = rng.standard_normal((n, 3))
+    c0 = rng.standard_normal((n, 2)).astype(np.float32)
+    d0 = rng.integers(-50, 50, size=(n, 2)).astype(np.int32)
+    x = rng.standard_normal((m, 2))
+    tgt = np.zeros((n, 2), np.int32)            # x1 by map 0; x2 by map 1
+    tgt[:, 0] = rng.integers(0, m, n)
+    tgt[:, 1] = rng.integers(0, m, n)
+    ends = np.zeros((n, 1), np.int32)           # every element increments target 0
+    vmap = np.stack([rng.integers(0, m, n)] * 2 + [rng.integers(0, m, n)], 1).astype(np.int32)
+    out = {}
+    for warp in (1, 0):
+        op2.set_option("jit_warp", warp)
+        s = op2.op_decl_set(n, f"e{warp}")
+        t = op2.op_decl_set(m, f"t{warp}")
+        pa = op2.op_decl_dat(s, 3, "double", a, f"a{warp}")
+        pb = op2.op_decl_dat(s, 3, "double", b0, f"b{warp}")
+        pc = op2.op_decl_dat(s, 2, "float", c0, f"c{warp}")
+        pd = op2.op_decl_dat(s, 2, "int", d0, f"d{warp}")
+        px = op2.op_decl_dat(t, 2, "double", x, f"x{warp}")
+        pacc = op2.op_decl_dat(t, 4, "double", None, f"acc{warp}")
+        pv = op2.op_decl_dat(t, 2, "float", None, f"v{warp}")
+        mt = op2.op_decl_map(s, t, 2, tgt, f"mt{warp}")
+        me = op2.op_decl_map(s, t, 1, ends, f"me{warp}")
+        mv = op2.op_decl_map(s, t, 3, vmap, f"mv{warp}")
+        A, R, RW, INC, W = op2.op_arg_dat, op2.OP_READ, op2.OP_RW, op2.OP_INC, op2.OP_WRITE
+        op2.op_par_loop("gen_rows", s, A(pa, -1, op2.OP_ID, 3, "double", R),
+                        A(pb, -1, op2.OP_ID, 3, "double", RW),
+                        A(pc, -1, op2.OP_ID, 2, "float", RW),
+                        A(pd, -1, op2.OP_ID, 2, "int", INC),
+                        A(px, 0, mt, 2, "double", R), A(px, 1, mt, 2, "double", R),
+                        A(pacc, 0, me, 4, "double", INC), A(pv, -3, mv, 2, "float", INC))
+        out[warp] = [op2.op_fetch_data(p) for p in (pb, pc, pd, pacc, pv)]
+    x1, x2 = x[tgt[:, 0]], x[tgt[:, 1]]
+    b = b0 + (a * x1[:, [0, 1, 0]] - x2[:, [1]])
+    c = np.stack([np.float32(2) * c0[:, 1] + a[:, 0].astype(np.float32),
+                  c0[:, 1] - np.float32(1)], 1)
+    d = d0.copy()
+    d[:, 0] += d0[:, 1]
+    acc = np.zeros((m, 4))
+    acc[0] = (a[:, [0, 1, 2, 0]] * 0.5 + np.arange(4)).sum(0)
+    v = np.zeros((m, 2), np.float32)
+    for j in range(3):
+        np.add.at(v[:, 0], vmap[:, j], 1.0)
+        np.add.at(v[:, 1], vmap[:, j], float(j))
+    for warp in (1, 0):
+        gb, gc, gd, gacc, gv = out[warp]
+        assert np.array_equal(gb, b) and np.array_equal(gc, c) and np.array_equal(gd, d)
+        np.testing.assert_allclose(gacc, acc, rtol=1e-12, atol=1e-12 * n)
+        assert np.array_equal(gv, v)             # small integers: exact in any order
