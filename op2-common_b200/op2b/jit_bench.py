@@ -3,12 +3,14 @@ loops written as OP2 user kernels (this module's own restatement, registered
 under other names, so no hand-written kernel matches them) run through
 libop2b's generated loops, beside the hand-written kernels on the same mesh.
 
-    python -m op2b.jit_bench [--mesh 2400 1200] [--iters 20] [--renumber 1]
+    python -m op2b.jit_bench [--mesh 2400 1200] [--iters 20] [--renumber 1] [--soa 1]
 
 Prints one JSON line: per loop, the mean device time per call (CUDA events,
 every call timed) and GB/s on the loop's algorithmic bytes (the same bytes as
 bench.py's), for the generated loops and for the hand-written ones run alone
-(no fusion or speculation)."""
+(no fusion or speculation); with --soa 1 also the generated loops on
+structure-of-arrays copies (one one-component dat per component of x, q, qold
+and res)."""
 import argparse
 import json
 
@@ -97,6 +99,70 @@ inline void jupdate(const double *qold, double *q, double *res, const double *ad
 }
 """
 
+# the same loops on structure-of-arrays dats: every component of x, q, qold
+# and res its own one-component dat
+KERNELS_SOA = r"""
+inline void ssave(const double *q0, const double *q1, const double *q2, const double *q3,
+                  double *o0, double *o1, double *o2, double *o3) {
+  *o0 = *q0; *o1 = *q1; *o2 = *q2; *o3 = *q3;
+}
+inline void sadt(const double *x1a, const double *x1b, const double *x2a, const double *x2b,
+                 const double *x3a, const double *x3b, const double *x4a, const double *x4b,
+                 const double *q0, const double *q1, const double *q2, const double *q3,
+                 double *adt) {
+  const double x1[2] = {*x1a, *x1b}, x2[2] = {*x2a, *x2b}, x3[2] = {*x3a, *x3b},
+               x4[2] = {*x4a, *x4b}, q[4] = {*q0, *q1, *q2, *q3};
+  jadt(x1, x2, x3, x4, q, adt);
+}
+inline void sres(const double *x1a, const double *x1b, const double *x2a, const double *x2b,
+                 const double *a0, const double *a1, const double *a2, const double *a3,
+                 const double *b0, const double *b1, const double *b2, const double *b3,
+                 const double *adt1, const double *adt2, double *r0, double *r1, double *r2,
+                 double *r3, double *s0, double *s1, double *s2, double *s3) {
+  const double x1[2] = {*x1a, *x1b}, x2[2] = {*x2a, *x2b}, q1[4] = {*a0, *a1, *a2, *a3},
+               q2[4] = {*b0, *b1, *b2, *b3};
+  double res1[4] = {0, 0, 0, 0}, res2[4] = {0, 0, 0, 0};
+  jres(x1, x2, q1, q2, adt1, adt2, res1, res2);
+  *r0 += res1[0]; *r1 += res1[1]; *r2 += res1[2]; *r3 += res1[3];
+  *s0 += res2[0]; *s1 += res2[1]; *s2 += res2[2]; *s3 += res2[3];
+}
+inline void supdate(const double *o0, const double *o1, const double *o2, const double *o3,
+                    double *q0, double *q1, double *q2, double *q3, double *r0, double *r1,
+                    double *r2, double *r3, const double *adt, double *rms) {
+  const double qold[4] = {*o0, *o1, *o2, *o3};
+  double q[4], res[4] = {*r0, *r1, *r2, *r3};
+  jupdate(qold, q, res, adt, rms);
+  *q0 = q[0]; *q1 = q[1]; *q2 = q[2]; *q3 = q[3];
+  *r0 = res[0]; *r1 = res[1]; *r2 = res[2]; *r3 = res[3];
+}
+"""
+
+
+def soa_loops(app, rms):
+    """The structure-of-arrays loops over copies of the Airfoil dats."""
+    t, R, W, RW, INC = "double", L.OP_READ, L.OP_WRITE, L.OP_RW, L.OP_INC
+    A = L.op_arg_dat
+    x = L.op_fetch_data(app.p_x)
+    q = L.op_fetch_data(app.p_q)
+    dx = [L.op_decl_dat(app.nodes, 1, t, np.ascontiguousarray(x[:, k]), f"sx{k}") for k in range(2)]
+    dq = [L.op_decl_dat(app.cells, 1, t, np.ascontiguousarray(q[:, k]), f"sq{k}") for k in range(4)]
+    do = [L.op_decl_dat(app.cells, 1, t, None, f"so{k}") for k in range(4)]
+    dr = [L.op_decl_dat(app.cells, 1, t, None, f"sr{k}") for k in range(4)]
+    xs = lambda i, m: [A(d, i, m, 1, t, R) for d in dx]
+    return [
+        ("ssave", app.cells, [A(d, -1, L.OP_ID, 1, t, R) for d in dq] +
+         [A(d, -1, L.OP_ID, 1, t, W) for d in do]),
+        ("sadt", app.cells, sum((xs(i, app.pcell) for i in range(4)), []) +
+         [A(d, -1, L.OP_ID, 1, t, R) for d in dq] + [A(app.p_adt, -1, L.OP_ID, 1, t, W)]),
+        ("sres", app.edges, xs(0, app.pedge) + xs(1, app.pedge) +
+         [A(d, 0, app.pecell, 1, t, R) for d in dq] + [A(d, 1, app.pecell, 1, t, R) for d in dq] +
+         [A(app.p_adt, 0, app.pecell, 1, t, R), A(app.p_adt, 1, app.pecell, 1, t, R)] +
+         [A(d, 0, app.pecell, 1, t, INC) for d in dr] + [A(d, 1, app.pecell, 1, t, INC) for d in dr]),
+        ("supdate", app.cells, [A(d, -1, L.OP_ID, 1, t, R) for d in do] +
+         [A(d, -1, L.OP_ID, 1, t, W) for d in dq] + [A(d, -1, L.OP_ID, 1, t, RW) for d in dr] +
+         [A(app.p_adt, -1, L.OP_ID, 1, t, R), L.op_arg_gbl(rms, 1, "double", L.OP_INC)])]
+
+
 # algorithmic bytes per call (C cells, N nodes, E edges, B boundary edges):
 # the figures bench.py's roofline uses
 def alg_bytes(m):
@@ -112,6 +178,8 @@ def main(argv=None):
     p.add_argument("--iters", type=int, default=20)
     p.add_argument("--renumber", type=int, default=1)
     p.add_argument("--option", action="append", default=[], metavar="KEY=VALUE")
+    p.add_argument("--soa", type=int, default=0,
+                   help="also time the loops on structure-of-arrays copies of the dats")
     a = p.parse_args(argv)
     m = M.channel_bump(a.mesh[0], a.mesh[1], seed=1)
     L.op_init()
@@ -186,6 +254,24 @@ def main(argv=None):
         out["hand_written"][n] = {"us": round(ms * 1000, 2),
                                   "gbs": round(bytes_[n] / (ms * 1e-3) / 1e9, 1)}
     out["last_rms_sum_generated"] = rms_gen
+    if a.soa:
+        for k in ("ssave", "sadt", "sres", "supdate"):
+            L.register_kernel(k, KERNELS + KERNELS_SOA)
+        sl = soa_loops(app, rms)
+        for _ in range(2):
+            for nm, st_, args in sl:
+                L.op_par_loop(nm, st_, *args)
+        L.load().op2b_reset_stats()
+        for _ in range(a.iters):
+            for nm, st_, args in sl:
+                L.op_par_loop(nm, st_, *args)
+        out["generated_soa"] = {}
+        for j, n in (("ssave", "save_soln"), ("sadt", "adt_calc"), ("sres", "res_calc"),
+                     ("supdate", "update")):
+            st = L.loop_stats(j)
+            ms = st["total_ms"] / st["calls"]
+            out["generated_soa"][n] = {"us": round(ms * 1000, 2),
+                                       "gbs": round(bytes_[n] / (ms * 1e-3) / 1e9, 1)}
     print(json.dumps(out))
     L.op_exit()
 
