@@ -843,11 +843,18 @@ __global__ void k_first_touch(int nfrom, int dim, const int *map, const int *per
   }
 }
 
-__global__ void k_flag_keys(int n, const int *key, int *flag, int *missing) {
+// elements of the target set no map entry reached (key still the memset
+// pattern 0x7f7f7f7f), one atomic a warp
+__global__ void k_count_unreached(int n, const int *key, int *missing) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  if (key[i] == INT_MAX) atomicAdd(missing, 1);
-  else flag[key[i]] = 1;
+  const bool miss = i < n && key[i] == 0x7f7f7f7f;
+  const unsigned b = __ballot_sync(0xffffffffu, miss);
+  if ((threadIdx.x & 31) == 0 && b) atomicAdd(missing, __popc(b));
+}
+
+__global__ void k_flag_keys(int n, const int *key, int *flag) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) flag[key[i]] = 1;
 }
 
 __global__ void k_rank_keys(int n, const int *key, const long long *pos, int *perm) {
@@ -1088,11 +1095,10 @@ static void propagate(op_set from, op_set to, std::vector<int *> &perm, cudaStre
       // 0x7f7f7f7f stands for "not reached"; map the sentinel to INT_MAX
       k_first_touch<<<grid1(from->size), 256, 0, s>>>(from->size, m->dim, m->map_d,
                                                        perm[from->index], n, key);
-      std::vector<int> hk(n);
-      cudaMemcpyAsync(hk.data(), key, sizeof(int) * n, cudaMemcpyDeviceToHost, s);
-      cudaStreamSynchronize(s);
       int nmiss = 0;
-      for (int i = 0; i < n; i++) nmiss += hk[i] == 0x7f7f7f7f;
+      k_count_unreached<<<grid1(n), 256, 0, s>>>(n, key, missing);
+      cudaMemcpyAsync(&nmiss, missing, sizeof(int), cudaMemcpyDeviceToHost, s);
+      cudaStreamSynchronize(s);
       if (nmiss) {  // not onto: try the next map (:113-117)
         cudaFreeAsync(key, s);
         cudaFreeAsync(flag, s);
@@ -1100,7 +1106,7 @@ static void propagate(op_set from, op_set to, std::vector<int *> &perm, cudaStre
         cudaFreeAsync(pos, s);
         continue;
       }
-      k_flag_keys<<<grid1(n), 256, 0, s>>>(n, key, flag, missing);
+      k_flag_keys<<<grid1(n), 256, 0, s>>>(n, key, flag);
       ok = scan_exclusive(flag, pos, nslots, s);
       cudaMallocAsync(&pd, sizeof(int) * n, s);
       k_rank_keys<<<grid1(n), 256, 0, s>>>(n, key, pos, pd);
