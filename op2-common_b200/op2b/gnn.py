@@ -448,6 +448,25 @@ class GraphNet:
               self.stream)
         self.launches += 1
 
+    def average_grad(self, group=None):
+        """Data-parallel training: the gradient of this rank's minibatch
+        replaced by the mean over the ranks of a torch.distributed group --
+        an all-reduce on the device with NCCL, through host memory with gloo
+        (ranks sharing a GPU).  Each rank's loss is a mean over its own
+        minibatch, so the result is the gradient of the mean over all ranks'
+        samples."""
+        import torch.distributed as dist
+        w = dist.get_world_size(group)
+        if w == 1:
+            return
+        if dist.get_backend(group) == "nccl":
+            dist.all_reduce(self.g, group=group)
+            self.g.div_(w)
+        else:
+            t = self.g.cpu()
+            dist.all_reduce(t, group=group)
+            self.g.copy_(t.div_(w))
+
     def zero_grad(self):
         _call("op2b_gnn_memset", self.g.data_ptr(), 0, self.n * 4, self.stream)
 

@@ -137,16 +137,51 @@ class Dataset:
                 self.target[s * N:(s + B) * N])
 
 
+def lr_at(it, steps, lr=1e-3, lr_min=1e-5, warmup=100):
+    """Linear warm-up over `warmup` steps, then cosine decay to lr_min."""
+    if it < warmup:
+        return lr * (it + 1) / warmup
+    u = (it - warmup) / max(1, steps - warmup)
+    return lr_min + 0.5 * (lr - lr_min) * (1 + math.cos(math.pi * u))
+
+
+class Schedule:
+    """Minibatch order: minibatch j of the run (j = step * ranks + rank under
+    data parallelism) is entry j % nb of a permutation of the nb minibatches,
+    drawn afresh from one seeded generator for every pass over the data, so
+    that every rank draws the same permutations."""
+
+    def __init__(self, nb, seed=0):
+        self.nb = nb
+        self.rng = np.random.default_rng(seed)
+        self.order = self.rng.permutation(nb)
+        self.epoch = 0
+
+    def start(self, j):
+        while j // self.nb > self.epoch:
+            self.order = self.rng.permutation(self.nb)
+            self.epoch += 1
+        return int(self.order[j % self.nb])
+
+
 def train(net: G.GraphNet, data: Dataset, val: Dataset | None = None, steps=3000, batch=8,
           lr=1e-3, lr_min=1e-5, warmup=100, weight_decay=1e-5, seed=0, log=print,
-          log_every=100):
+          log_every=100, group=None):
     """AdamW with linear warm-up and cosine decay over `steps` minibatches of
-    `batch` consecutive samples.  Returns the loss history."""
+    `batch` consecutive samples.  With a torch.distributed `group`, data
+    parallel: each rank takes its own minibatches (step * ranks + rank of the
+    shared schedule) and the gradients are averaged before every step, so all
+    ranks keep the same parameters.  Returns the loss history (this rank's
+    losses) and the device time."""
     torch = net.torch
     dg = net.upload_graph(G.replicate_graph(data.g, batch))
     nb = data.n // batch
-    rng = np.random.default_rng(seed)
-    order = rng.permutation(nb)
+    if group is not None:
+        import torch.distributed as dist
+        rank, world = dist.get_rank(group), dist.get_world_size(group)
+    else:
+        rank, world = 0, 1
+    sched = Schedule(nb, seed)
     hist = []
     t0 = time.time()
     ev0 = torch.cuda.Event(enable_timing=True)
@@ -154,17 +189,13 @@ def train(net: G.GraphNet, data: Dataset, val: Dataset | None = None, steps=3000
     ev0.record()
     fresh = True
     for it in range(steps):
-        if it % nb == 0 and it:
-            order = rng.permutation(nb)
-        s = int(order[it % nb]) * batch
+        s = sched.start(it * world + rank) * batch
         ni, ei, tg = data.batch(s, batch)
         acc = net.loss_grad(dg, ni, ei, tg, zero_loss=fresh)
         fresh = False
-        if it < warmup:
-            lr_it = lr * (it + 1) / warmup
-        else:
-            u = (it - warmup) / max(1, steps - warmup)
-            lr_it = lr_min + 0.5 * (lr - lr_min) * (1 + math.cos(math.pi * u))
+        if world > 1:
+            net.average_grad(group)
+        lr_it = lr_at(it, steps, lr, lr_min, warmup)
         net.step(lr_it, weight_decay=weight_decay)
         if (it + 1) % log_every == 0 or it + 1 == steps:
             l = float(acc.item()) / (it % log_every + 1)
@@ -309,6 +340,9 @@ def main(argv=None):
     ap.add_argument("--synthetic", action="store_true",
                     help="random targets instead of solved fields (timing/profiling of training)")
     ap.add_argument("--log-every", type=int, default=100)
+    ap.add_argument("--dp-backend", default="nccl", choices=["nccl", "gloo"],
+                    help="under torchrun (WORLD_SIZE > 1) training is data parallel; the "
+                         "gradient all-reduce's backend (gloo: ranks may share a GPU)")
     ap.add_argument("--gemm-tma", type=int, default=1,
                     help="1: forward products on the TMA-fed tensor-core GEMM; 0: all on the "
                          "register-staged one")
@@ -316,6 +350,20 @@ def main(argv=None):
     G.GEMM_TMA = bool(a.gemm_tma)
     log = lambda s: print(s, flush=True)
     report = dict(args=vars(a))
+    group, rank = None, 0
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")) % torch.cuda.device_count())
+        dist.init_process_group(a.dp_backend, timeout=datetime.timedelta(seconds=300))
+        group, rank = dist.group.WORLD, dist.get_rank()
+        report["ranks"] = dist.get_world_size()
+        if rank:  # rank 0 reports and writes; every rank trains
+            log = lambda s: None
+            a.out = a.report = None
+            a.eval = []
     if a.load:
         net = G.GraphNet.load(a.load)
     else:
@@ -338,7 +386,7 @@ def main(argv=None):
                      norm=tr.norm) if a.val else None
         net = G.GraphNet(steps=a.mp_steps, seed=0, norm=tr.norm)
         hist, ms = train(net, tr, va, steps=a.steps, batch=a.batch, lr=a.lr, log=log,
-                         log_every=a.log_every)
+                         log_every=a.log_every, group=group)
         report["train"] = dict(ms=ms, ms_per_step=ms / max(a.steps, 1), history=hist,
                                launches=net.launches)
         if a.out:
@@ -367,6 +415,10 @@ def main(argv=None):
     if a.report:
         with open(a.report, "w") as fh:
             json.dump(report, fh, indent=1, default=float)
+    if group is not None:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 if __name__ == "__main__":
