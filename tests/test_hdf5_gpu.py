@@ -198,3 +198,44 @@ def test_reference_airfoil_hdf5_programs_run_on_libop2b():
         for name in ("nodes", "cells", "edges", "bedges", "pedge", "pecell", "pbedge",
                      "pbecell", "pcell", "p_bound", "p_x", "gam", "qinf"):
             np.testing.assert_array_equal(L.h5_read(dump, name), L.h5_read(src, name))
+
+
+def test_full_size_mesh_round_trip(op2, tmp_path):
+    """The benchmark's 2400x1200 mesh (2.88M cells, 484 MB in the file):
+    dumped after renumbering, declared back in a new session, every map and
+    dat equal; the times are printed (host file I/O)."""
+    import time
+    m = M.channel_bump(2400, 1200, seed=1)
+    app = Airfoil(m)
+    app.renumber(stats=False)
+    app.iterate(1)
+    f = str(tmp_path / "big.h5")
+    want = {n: L.op_fetch_data(d) for n, d in (("p_q", app.p_q), ("p_x", app.p_x),
+                                                 ("p_adt", app.p_adt), ("p_bound", app.p_bound))}
+    t0 = time.perf_counter()
+    L.op_dump_to_hdf5(f)
+    t1 = time.perf_counter()
+    size = os.path.getsize(f)
+    L.op_exit()
+    L.op_init()
+    t2 = time.perf_counter()
+    nodes = L.op_decl_set_hdf5(f, "nodes")
+    cells = L.op_decl_set_hdf5(f, "cells")
+    edges = L.op_decl_set_hdf5(f, "edges")
+    bedges = L.op_decl_set_hdf5(f, "bedges")
+    maps = {n: L.op_decl_map_hdf5(fr, to, d, f, n) for n, fr, to, d in (
+        ("pedge", edges, nodes, 2), ("pecell", edges, cells, 2), ("pbedge", bedges, nodes, 2),
+        ("pbecell", bedges, cells, 1), ("pcell", cells, nodes, 4))}
+    got = {"p_q": L.op_decl_dat_hdf5(cells, 4, "double", f, "p_q"),
+           "p_x": L.op_decl_dat_hdf5(nodes, 2, "double", f, "p_x"),
+           "p_adt": L.op_decl_dat_hdf5(cells, 1, "double", f, "p_adt"),
+           "p_bound": L.op_decl_dat_hdf5(bedges, 1, "int", f, "p_bound")}
+    t3 = time.perf_counter()
+    print(f"2400x1200 mesh: {size / 1e6:.0f} MB, op_dump_to_hdf5 {1e3 * (t1 - t0):.0f} ms, "
+          f"declared back {1e3 * (t3 - t2):.0f} ms")
+    assert size > 450e6
+    for n, d in got.items():
+        assert np.array_equal(L.op_fetch_data(d), want[n]), n
+    # the maps as the library held them (renumbered), through the file
+    assert np.array_equal(_map_host(maps["pecell"], m.nedge, 2), L.h5_read(f, "pecell"))
+    assert np.array_equal(_map_host(maps["pcell"], m.ncell, 4), L.h5_read(f, "pcell"))
