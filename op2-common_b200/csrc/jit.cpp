@@ -770,8 +770,8 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
   // kernel works on registers; an indirect dat the loop only reads is
   // gathered by vector loads; indirect increments are combined per warp
   // before the atomics.  Not for loops that run colour by colour (their
-  // elements come permuted) except the gathers; rows up to 128 bytes (32
-  // with op_arg_info, whose reduction needs shared memory as well).
+  // elements come permuted) except the gathers; rows up to 128 bytes, and
+  // fewer where op_arg_info's reduction takes shared memory as well.
   bool has_info = false, has_red = false;
   for (auto &a : ap) {
     has_info |= a.kind == INFO;
@@ -784,7 +784,15 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
         uses[args[i].dat]++;
         if (ap[(size_t)i].acc != OP_READ) writes[args[i].dat]++;
       }
-    const int maxrow = has_info ? 32 : 128;
+    // the warp buffer (256 threads x the widest row, 16-byte padded) shares
+    // the 48 KB of static shared memory with op_arg_info's block reduction
+    size_t info_bytes = 0;
+    for (auto &a : ap)
+      if (a.kind == INFO) info_bytes += 256 * (16 + (size_t)a.dim * a.bytes);
+    const size_t budget = info_bytes < 46 * 1024 ? 46 * 1024 - info_bytes : 0;
+    auto fits = [&](size_t row_bytes) {
+      return row_bytes <= 128 && 256 * ((row_bytes + 15) & ~(size_t)15) <= budget;
+    };
     bool gathers = false;
     for (auto &a : ap) gathers |= a.kind == INDIRECT && a.acc == OP_READ;
     for (int i = 0; i < nargs; i++) {
@@ -795,7 +803,7 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
       // more than the scattered stores); read-only rows only in loops without
       // gathers, whose latency the staging would otherwise add to
       if (a.kind == DIRECT && !coloured && a.dim > 1 && uses[args[i].dat] == 1 &&
-          row + a.bytes <= maxrow && a.acc != OP_WRITE && (a.acc != OP_READ || !gathers))
+          fits((size_t)row + a.bytes) && a.acc != OP_WRITE && (a.acc != OP_READ || !gathers))
         a.stage = 1;
       if (a.kind == INDIRECT && !a.vec && a.acc == OP_READ && writes[args[i].dat] == 0) {
         const uintptr_t base = (uintptr_t)args[i].dat->data_d;
@@ -806,7 +814,7 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
           a.vw = vw;
         }
       }
-      if (a.kind == INDIRECT && a.acc == OP_INC && !coloured && row <= maxrow) a.seg = true;
+      if (a.kind == INDIRECT && a.acc == OP_INC && !coloured && fits((size_t)row)) a.seg = true;
       key << "|w" << a.stage << a.vw << a.seg;
     }
   }

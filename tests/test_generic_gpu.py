@@ -599,3 +599,45 @@ def test_coalesced_rows_gathers_and_warp_combined_increments(op2, n):
         assert np.array_equal(gb, b) and np.array_equal(gc, c) and np.array_equal(gd, d)
         np.testing.assert_allclose(gacc, acc, rtol=1e-12, atol=1e-12 * n)
         assert np.array_equal(gv, v)             # small integers: exact in any order
+
+
+def test_arg_info_beside_staged_rows_and_combined_increments(op2):
+    """A loop with a large op_arg_info payload (16 doubles: 36 KB of the
+    block's shared memory for its reduction) beside a read-write direct row
+    and an indirect increment: the rows staged through shared memory get only
+    what the reduction leaves, and the loop compiles and gives the numpy
+    result (argmax payload, rows, increments)."""
+    op2.register_kernel("gen_info_rows", """
+inline void gen_info_rows(double *r, const int *i, double *acc, double *best, double *pay) {
+  r[0] += 1.0; r[1] *= 2.0; r[2] -= r[0];
+  for (int k = 0; k < 4; k++) acc[k] += r[k % 3];
+  if (r[1] > *best) { *best = r[1]; for (int k = 0; k < 16; k++) pay[k] = k + *i; }
+}
+""")
+    rng = np.random.default_rng(21)
+    n, m = 50001, 9
+    r0 = rng.standard_normal((n, 3))
+    tgt = rng.integers(0, m, size=(n, 1)).astype(np.int32)
+    s = op2.op_decl_set(n, "s")
+    t = op2.op_decl_set(m, "t")
+    pr = op2.op_decl_dat(s, 3, "double", r0, "r")
+    pacc = op2.op_decl_dat(t, 4, "double", None, "acc")
+    mp = op2.op_decl_map(s, t, 1, tgt, "mp")
+    best = np.array([-1e300])
+    pay = np.full(16, -1.0)
+    op2.op_par_loop("gen_info_rows", s, op2.op_arg_dat(pr, -1, op2.OP_ID, 3, "double", op2.OP_RW),
+                    op2.op_arg_idx(-1, op2.OP_ID),
+                    op2.op_arg_dat(pacc, 0, mp, 4, "double", op2.OP_INC),
+                    op2.op_arg_gbl(best, 1, "double", op2.OP_MAX),
+                    op2.op_arg_info(pay, 16, "double", 3))
+    r = r0.copy()
+    r[:, 0] += 1.0
+    r[:, 1] *= 2.0
+    r[:, 2] -= r[:, 0]
+    assert np.array_equal(op2.op_fetch_data(pr), r)
+    acc = np.zeros((m, 4))
+    for k in range(4):
+        np.add.at(acc[:, k], tgt[:, 0], r[:, k % 3])
+    np.testing.assert_allclose(op2.op_fetch_data(pacc), acc, rtol=1e-12, atol=1e-9)
+    e = int(np.argmax(r[:, 1]))
+    assert best[0] == r[e, 1] and np.array_equal(pay, np.arange(16) + e)
