@@ -141,7 +141,7 @@ def cpu_model():
     return None
 
 
-def survey_bytes(loop, C, N, E, B, es=8):
+def algorithmic_bytes(loop, C, N, E, B, es=8):
     """Compulsory bytes of one call of `loop` (each array element moved once;
     es-byte reals, int32 maps): save_soln 64 C; adt_calc 16 C + 16 N + 40 C;
     res_calc 16 E + 16 N + 104 C; bres_calc 12 B + 120 B; update 136 C -- for
@@ -585,7 +585,7 @@ def main():
         es = np.dtype(dtype).itemsize
         sizes = (m.ncell, m.nnode, m.nedge, m.nbedge)
         for n, x in loops.items():
-            sb = survey_bytes(n, *sizes, es=es)
+            sb = algorithmic_bytes(n, *sizes, es=es)
             x["moved_bytes"] = x.pop("alg_bytes")       # what the runtime's launch must move
             x["alg_bytes"] = sb                          # the loops' compulsory bytes
             x["moved_gbs"] = x.pop("gbs")
@@ -594,7 +594,7 @@ def main():
         d = loops[dom]
         key = f"{work}_{args.precision}_{args.numbering}_mode{args.inc_mode}"
         # the iteration: save_soln + 2 x (adt_calc, res_calc, bres_calc, update)
-        it_bytes = (survey_bytes("save_soln", *sizes, es=es) + 2 * survey_bytes(
+        it_bytes = (algorithmic_bytes("save_soln", *sizes, es=es) + 2 * algorithmic_bytes(
             "adt_calc+res_calc+bres_calc+update", *sizes, es=es))
         it_gbs = it_bytes / (ms * 1e-3) / 1e9 if ms > 0 else None
         parity = None
