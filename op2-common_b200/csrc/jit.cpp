@@ -54,6 +54,7 @@
 #include <string>
 #include <vector>
 
+#include "gather.h"
 #include "op2b_plan.h"
 #include "op2b_runtime.h"
 #include "plan.h"
@@ -235,8 +236,10 @@ template <typename T> __device__ T op2b_min(T a, T b) { return b < a ? b : a; }
 template <typename T> __device__ T op2b_max(T a, T b) { return b > a ? b : a; }
 )";
 
+// own >= 0: the owner-computes loop (option jit_exact) for the increments of
+// argument own's dat; the others of its increment arguments share its map
 std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std::string &body,
-                     bool coloured) {
+                     bool coloured, int own = -1) {
   Runtime &r = rt();
   std::ostringstream s;
   s << "// libop2b: generated loop for the user kernel '" << name << "'\n";
@@ -263,6 +266,8 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
   }
   // coloured: this launch runs the elements op2b_perm[op2b_first, +op2b_n)
   if (coloured) s << ", const int *op2b_perm, int op2b_first";
+  // owner computes: op2b_n targets, each with its (element, slot) entries
+  if (own >= 0) s << ", const long long *op2b_ioff, const int *op2b_ient, const int *op2b_rows";
   s << ") {\n";
   for (size_t i = 0; i < ap.size(); i++) {
     const ArgPlan &a = ap[i];
@@ -295,7 +300,22 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
     warp |= a.stage == 1 || a.seg;
   }
   wbytes = (wbytes + 15) & ~(size_t)15;
-  if (warp) {
+  if (own >= 0) {
+    // a thread per target: the elements that increment it, in element order
+    // (each slot in slot order), the kernel adding straight into the target's
+    // own sum -- the additions of the sequential loop, in its order
+    const ArgPlan &o = ap[(size_t)own];
+    // (op2b_rows, when given, lists the targets that have entries)
+    s << "  for (int op2b_i = blockIdx.x * blockDim.x + threadIdx.x; op2b_i < op2b_n;"
+         " op2b_i += gridDim.x * blockDim.x) {\n"
+      << "  const int op2b_t = op2b_rows ? op2b_rows[op2b_i] : op2b_i;\n"
+      << "  " << o.ctype << " op2b_acc[" << o.dim << "];\n"
+      << "  for (int k = 0; k < " << o.dim << "; k++) op2b_acc[k] = op2b_d" << own
+      << "[(size_t)op2b_t * " << o.dim << " + k];\n"
+      << "  for (long long op2b_k = op2b_ioff[op2b_t]; op2b_k < op2b_ioff[op2b_t + 1]; op2b_k++) {\n"
+      << "    const int op2b_e = op2b_ient[op2b_k] / " << o.mdim << ";\n"
+      << "    const int op2b_s = op2b_ient[op2b_k] % " << o.mdim << ";\n";
+  } else if (warp) {
     s << "  __shared__ __align__(16) unsigned char op2b_sh[" << 256 * wbytes << "];\n"
       << "  const int op2b_lane = threadIdx.x & 31;\n"
       << "  unsigned char *op2b_w = op2b_sh + (threadIdx.x >> 5) * " << 32 * wbytes << ";\n"
@@ -364,6 +384,22 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
         }
         break;
       case INDIRECT:
+        if (own >= 0 && a.acc == OP_INC) {
+          // the owner's slot adds into its sum, the element's other slots
+          // into scratch
+          const int nv = std::max(a.vec, 1);
+          s << "    " << a.ctype << " op2b_l" << i << "[" << nv * a.dim << "];\n"
+            << "    for (int k = 0; k < " << nv * a.dim << "; k++) op2b_l" << i << "[k] = 0;\n";
+          if (a.vec) {
+            s << "    " << a.ctype << " *op2b_v" << i << "[" << a.vec << "];\n    for (int j = 0; j < "
+              << a.vec << "; j++) op2b_v" << i << "[j] = op2b_s == j ? op2b_acc : op2b_l" << i
+              << " + j * " << a.dim << ";\n";
+            call << "op2b_vec<" << a.ctype << ">{op2b_v" << i << "}";
+          } else {
+            call << "(op2b_s == " << a.idx << " ? op2b_acc : op2b_l" << i << ")";
+          }
+          break;
+        }
         if (a.vec) {
           // one pointer per map entry (op_seq.h op_arg_copy_in); increments
           // into locals added atomically after the call
@@ -461,7 +497,7 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
     }
   for (size_t i = 0; i < ap.size(); i++) {
     const ArgPlan &a = ap[i];
-    if (a.seg) continue;
+    if (a.seg || own >= 0) continue;
     if (a.kind == INDIRECT && a.acc == OP_INC && a.vec)
       s << "    for (int j = 0; j < " << a.vec << "; j++) {\n      const size_t t = (size_t)op2b_m"
         << i << "[(size_t)op2b_e * " << a.mdim << " + j] * " << a.dim << ";\n"
@@ -470,6 +506,11 @@ std::string generate(const char *name, const std::vector<ArgPlan> &ap, const std
     else if (a.kind == INDIRECT && a.acc == OP_INC)
       s << "    for (int k = 0; k < " << a.dim << "; k++) atomicAdd(op2b_d" << i
         << " + (size_t)op2b_t" << i << " * " << a.dim << " + k, op2b_l" << i << "[k]);\n";
+  }
+  if (own >= 0) {
+    const ArgPlan &o = ap[(size_t)own];
+    s << "  }\n  for (int k = 0; k < " << o.dim << "; k++) op2b_d" << own << "[(size_t)op2b_t * "
+      << o.dim << " + k] = op2b_acc[k];\n";
   }
   if (warp) {
     s << "    }\n";  // if (op2b_ok)
@@ -765,6 +806,40 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
     key << "|" << a.kind << ":" << a.ctype << ":" << a.dim << ":" << a.acc << ":" << a.mdim
         << ":" << a.idx << ":" << a.vec;
   }
+  // option jit_exact: a loop whose only effect is to increment one dat
+  // through one map (no other writes, no global reductions, the dat read by
+  // no other argument, each slot of the map incremented by at most one
+  // argument) runs owner-computes: a thread per target walks the inverse map
+  // and re-runs the kernel for each element that increments the target, in
+  // element order, the target's argument pointing at its own sum.  The sum
+  // then sees the sequential loop's additions in its order: bit for bit.
+  int own = -1;
+  if (r.opt_jit_exact && !coloured) {
+    bool ok = true;
+    std::vector<int> slots;
+    for (int i = 0; i < nargs && ok; i++) {
+      const ArgPlan &a = ap[(size_t)i];
+      if (a.kind == INDIRECT && a.acc == OP_INC) {
+        if (own < 0) own = i;
+        else ok = args[i].dat == args[own].dat && args[i].map == args[own].map && !a.vec &&
+                  !ap[(size_t)own].vec;
+        slots.push_back(a.vec ? -1 : a.idx);
+      } else if ((a.kind == DIRECT || a.kind == INDIRECT) && a.acc != OP_READ) {
+        ok = false;
+      } else if ((a.kind == GBL && a.acc != OP_READ && a.acc != OP_WORK) || a.kind == INFO) {
+        ok = false;
+      }
+    }
+    for (int i = 0; i < nargs && ok && own >= 0; i++)
+      if ((ap[(size_t)i].kind == DIRECT || ap[(size_t)i].kind == INDIRECT) &&
+          args[i].dat == args[own].dat && ap[(size_t)i].acc != OP_INC)
+        ok = false;
+    std::sort(slots.begin(), slots.end());
+    ok = ok && std::adjacent_find(slots.begin(), slots.end()) == slots.end();
+    if (!ok || own < 0 || (long long)args[own].map->from->size * args[own].map->dim >= INT32_MAX)
+      own = -1;
+    if (own >= 0) key << "|own" << own;
+  }
   // option jit_warp: a direct dat that no other argument of the loop names
   // moves through the warp's shared memory in whole rows (coalesced) and the
   // kernel works on registers; an indirect dat the loop only reads is
@@ -777,7 +852,7 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
     has_info |= a.kind == INFO;
     has_red |= a.kind == INFO || (a.kind == GBL && a.acc != OP_READ && a.acc != OP_WORK);
   }
-  if (r.opt_jit_warp) {
+  if (r.opt_jit_warp && own < 0) {
     std::map<op_dat, int> uses, writes;
     for (int i = 0; i < nargs; i++)
       if (ap[(size_t)i].kind == DIRECT || ap[(size_t)i].kind == INDIRECT) {
@@ -854,7 +929,7 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
   if (coloured && set->size > 0 && !(plan = colour_plan(name, set, nargs, args))) return -1;
   Jit &j = cache()[key.str()];
   if (!j.fn) {
-    const std::string src = generate(name, ap, body, coloured);
+    const std::string src = generate(name, ap, body, coloured, own);
     if (!compile(name, src, j)) {
       cache().erase(key.str());
       return -1;
@@ -955,6 +1030,21 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
       kp.push_back(&ptrs.back());
     }
   }
+  // owner computes: the targets and the inverse of the increments' map
+  const long long *ioff = nullptr;
+  const int *ient = nullptr, *irows = nullptr;
+  if (own >= 0) {
+    const InvMap *inv = get_inverse_map(args[own].map);
+    if (!inv) return -1;
+    ioff = inv->off;
+    ient = inv->ent;
+    // every target, or only those that have entries (the others keep their values)
+    irows = inv->all_rows ? nullptr : inv->rows;
+    n = inv->all_rows ? inv->nto : inv->nrows;
+    kp.push_back(&ioff);
+    kp.push_back(&ient);
+    kp.push_back(&irows);
+  }
   r.begin_loop(name);
   // one launch over the set, or one per colour over its slice of col_reord
   const int ncol = plan ? plan->pub.ncolors : 1;
@@ -965,7 +1055,7 @@ int jit_par_loop(const char *name, op_set set, int nargs, op_arg *args) {
     kp.push_back(&first);
   }
   unsigned grid = 0;  // of the last launch (a loop with op_arg_info has one)
-  for (int c = 0; c < ncol && set->size > 0; c++) {
+  for (int c = 0; c < ncol && set->size > 0 && n > 0; c++) {
     if (plan) {
       first = plan->pub.color2_offsets[c];
       n = plan->pub.color2_offsets[c + 1] - first;

@@ -417,6 +417,7 @@ void op_init(int argc, char **argv, int diags) {
   r.opt_diags = diags;
   if (const char *e = getenv("OP2B_ABORT_ON_ERROR")) r.opt_abort = atoi(e) != 0;
   if (const char *e = getenv("OP2B_INC_MODE")) r.opt_inc_mode = atoi(e);
+  if (const char *e = getenv("OP2B_JIT_EXACT")) r.opt_jit_exact = atoi(e) != 0;
   parse_args(argc, argv);
   int dev = 0;
   if (const char *e = getenv("OP2B_DEVICE")) dev = atoi(e);
@@ -567,6 +568,7 @@ void op_exit(void) {
   r.opt_plan_mode = d.opt_plan_mode;
   r.opt_atomic_seg = d.opt_atomic_seg;
   r.opt_jit_warp = d.opt_jit_warp;
+  r.opt_jit_exact = d.opt_jit_exact;
   r.opt_atomic_blocks = d.opt_atomic_blocks;
   r.ring_used = 0;
   r.opt_gemm_tma = d.opt_gemm_tma;
@@ -1176,6 +1178,8 @@ int op2b_set_option(const char *key, long value) {
     r.opt_atomic_seg = value != 0;
   } else if (k == "jit_warp") {
     r.opt_jit_warp = value != 0;
+  } else if (k == "jit_exact") {
+    r.opt_jit_exact = value != 0;
   } else if (k == "atomic_blocks") {
     if (value < 1 || value > 4096) {
       set_error("op2b_set_option: atomic_blocks must be between 1 and 4096");
@@ -1273,6 +1277,7 @@ long op2b_get_option(const char *key) {
   if (k == "plan_mode") return r.opt_plan_mode;
   if (k == "atomic_segmented") return r.opt_atomic_seg;
   if (k == "jit_warp") return r.opt_jit_warp;
+  if (k == "jit_exact") return r.opt_jit_exact;
   if (k == "atomic_blocks") return r.opt_atomic_blocks;
   if (k == "ring_used") return r.ring_used;  // read-only
   if (k == "gemm_tma") return r.opt_gemm_tma;

@@ -641,3 +641,67 @@ inline void gen_info_rows(double *r, const int *i, double *acc, double *best, do
     np.testing.assert_allclose(op2.op_fetch_data(pacc), acc, rtol=1e-12, atol=1e-9)
     e = int(np.argmax(r[:, 1]))
     assert best[0] == r[e, 1] and np.array_equal(pay, np.arange(16) + e)
+
+
+def test_exact_increments_are_the_sequential_loops(op2):
+    """Option jit_exact: a generated loop whose only effect is incrementing
+    one dat runs owner-computes (each target re-runs the kernel for the
+    elements that increment it, in element order, adding into its own sum),
+    so the result is the sequential loop's bit for bit: the scatter above
+    against numpy's in-order np.add.at, and Airfoil's res_calc and bres_calc
+    written as user kernels (op2b.jit_bench's restatement) against the C
+    restatement of the reference's sequential loops."""
+    from op2b import jit_bench as JB
+    from op2b import mesh as M
+    from op2b.airfoil import Airfoil
+    from oracle import oracle as O
+    op2.set_option("jit_exact", 1)
+    op2.register_kernel("gen_scatter", EDGES)
+    rng, pp = _rng_mesh()
+    nn, ne = 5000, pp.shape[0]
+    A = rng.standard_normal(ne)
+    u = rng.standard_normal((nn, 2))
+    du0 = rng.standard_normal((nn, 2))
+    nodes = op2.op_decl_set(nn, "nodes")
+    edges = op2.op_decl_set(ne, "edges")
+    m = op2.op_decl_map(edges, nodes, 2, pp, "ppedge")
+    pA = op2.op_decl_dat(edges, 1, "double", A, "A")
+    pu = op2.op_decl_dat(nodes, 2, "double", u, "u")
+    pdu = op2.op_decl_dat(nodes, 2, "double", du0, "du")
+    op2.op_par_loop("gen_scatter", edges,
+                    op2.op_arg_dat(pA, -1, op2.OP_ID, 1, "double", op2.OP_READ),
+                    op2.op_arg_dat(pu, 1, m, 2, "double", op2.OP_READ),
+                    op2.op_arg_dat(pdu, 0, m, 2, "double", op2.OP_INC),
+                    op2.op_arg_gbl(np.array([0.75]), 1, "double", op2.OP_READ),
+                    op2.op_arg_idx(-1, op2.OP_ID),
+                    op2.op_arg_idx(0, m))
+    ref = du0.copy()
+    e = np.arange(ne)
+    np.add.at(ref[:, 0], pp[:, 0], 0.75 * A * u[pp[:, 1], 0])
+    np.add.at(ref[:, 1], pp[:, 0], 0.75 * u[pp[:, 1], 1] - e + 0.5 * pp[:, 0])
+    assert np.array_equal(op2.op_fetch_data(pdu), ref)
+    # Airfoil's increment loops, generated
+    mesh = M.channel_bump(60, 30, seed=3)
+    app = Airfoil(mesh)
+    app.iterate(2)
+    for k in ("jres", "jbres"):
+        op2.register_kernel(k, JB.KERNELS)
+    t, R, INC = "double", op2.OP_READ, op2.OP_INC
+    Ad = op2.op_arg_dat
+    op2.op_par_loop("jres", app.edges, Ad(app.p_x, 0, app.pedge, 2, t, R),
+                    Ad(app.p_x, 1, app.pedge, 2, t, R), Ad(app.p_q, 0, app.pecell, 4, t, R),
+                    Ad(app.p_q, 1, app.pecell, 4, t, R), Ad(app.p_adt, 0, app.pecell, 1, t, R),
+                    Ad(app.p_adt, 1, app.pecell, 1, t, R), Ad(app.p_res, 0, app.pecell, 4, t, INC),
+                    Ad(app.p_res, 1, app.pecell, 4, t, INC))
+    op2.op_par_loop("jbres", app.bedges, Ad(app.p_x, 0, app.pbedge, 2, t, R),
+                    Ad(app.p_x, 1, app.pbedge, 2, t, R), Ad(app.p_q, 0, app.pbecell, 4, t, R),
+                    Ad(app.p_adt, 0, app.pbecell, 1, t, R), Ad(app.p_res, 0, app.pbecell, 4, t, INC),
+                    Ad(app.p_bound, -1, op2.OP_ID, 1, "int", R))
+    f = app.fetch()
+    st = O.State(mesh.ncell, app.c["qinf"])
+    st.q[:] = f["q"]
+    st.adt[:] = f["adt"]
+    st.res[:] = 0.0
+    O.loop("res_calc", mesh, app.c, st)
+    O.loop("bres_calc", mesh, app.c, st)
+    assert np.array_equal(f["res"], st.res)
