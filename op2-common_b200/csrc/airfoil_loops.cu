@@ -407,11 +407,12 @@ template <typename T, int THREADS, bool ADT, bool KEEP_RES = false>
 __global__ void __launch_bounds__(THREADS)
 k_update(int ncell, const T *__restrict__ qold, T *__restrict__ q, T *__restrict__ res,
          const T *adt, RedSlot *__restrict__ parts, unsigned *__restrict__ counter,
-         RedSlot *__restrict__ out, RedSlot *host_out, long long seq, AdtNext<T> an) {
+         RedSlot *__restrict__ out, RedSlot *host_out, long long seq, AdtNext<T> an, int rev) {
   grid_dependency_wait();
   RedTriple t{0.0, -INFINITY, LLONG_MAX};
   int stride = gridDim.x * THREADS;
-  for (int n = blockIdx.x * THREADS + threadIdx.x; n < ncell; n += stride) {
+  for (int i = blockIdx.x * THREADS + threadIdx.x; i < ncell; i += stride) {
+    const int n = rev ? ncell - 1 - i : i;
     T qo[4], r[4], qn[4];
     T x1x, x1y, x2x, x2y, x3x, x3y, x4x, x4y;
     if constexpr (ADT) {  // the node gathers first: they do not depend on the update
@@ -431,7 +432,7 @@ k_update(int ncell, const T *__restrict__ qold, T *__restrict__ q, T *__restrict
       qn[m] = (T)((double)qo[m] - del);
       double sq = del * del;
       t.sum += sq;
-      if (sq > t.maxv) {
+      if (sq > t.maxv || (sq == t.maxv && n < t.idx)) {  // the lowest cell on ties
         t.maxv = sq;
         t.idx = n;
       }
@@ -479,24 +480,25 @@ k_update(int ncell, const T *__restrict__ qold, T *__restrict__ q, T *__restrict
 template <typename T>
 cudaError_t launch_update(const LaunchCtx &c, int ncell, const T *qold, T *q, T *res,
                           const T *adt, const RedScratch &s, const int *pcell, const T *x,
-                          T *adt_next, const AirConst<T> *k, bool keep_res) {
+                          T *adt_next, const AirConst<T> *k, bool keep_res, bool reverse) {
   constexpr int TH = 256;
   int grid = grid_for(c, ncell, TH, 4);
   if (grid > s.capacity) grid = s.capacity;
+  const int rev = reverse ? 1 : 0;
   cudaError_t e;
   if (adt_next) {
     const AdtNext<T> an{reinterpret_cast<const int4 *>(pcell), x, adt_next, *k};
     e = keep_res ? launch_dependent(c, k_update<T, TH, true, true>, grid, TH, 0, ncell, qold, q,
-                                    res, adt, s.parts, s.counter, s.out, s.host_out, s.seq, an)
+                                    res, adt, s.parts, s.counter, s.out, s.host_out, s.seq, an, rev)
                  : launch_dependent(c, k_update<T, TH, true>, grid, TH, 0, ncell, qold, q, res,
-                                    adt, s.parts, s.counter, s.out, s.host_out, s.seq, an);
+                                    adt, s.parts, s.counter, s.out, s.host_out, s.seq, an, rev);
   } else {
     e = keep_res ? launch_dependent(c, k_update<T, TH, false, true>, grid, TH, 0, ncell, qold, q,
                                     res, adt, s.parts, s.counter, s.out, s.host_out, s.seq,
-                                    AdtNext<T>{})
+                                    AdtNext<T>{}, rev)
                  : launch_dependent(c, k_update<T, TH, false>, grid, TH, 0, ncell, qold, q, res,
                                     adt, s.parts, s.counter, s.out, s.host_out, s.seq,
-                                    AdtNext<T>{});
+                                    AdtNext<T>{}, rev);
   }
   c.count();
   return e != cudaSuccess ? e : cudaGetLastError();
@@ -534,10 +536,10 @@ template cudaError_t launch_bres_calc_atomic<float>(const LaunchCtx &, int, cons
 template cudaError_t launch_update<double>(const LaunchCtx &, int, const double *, double *,
                                            double *, const double *, const RedScratch &,
                                            const int *, const double *, double *,
-                                           const AirConst<double> *, bool);
+                                           const AirConst<double> *, bool, bool);
 template cudaError_t launch_update<float>(const LaunchCtx &, int, const float *, float *,
                                           float *, const float *, const RedScratch &,
                                           const int *, const float *, float *,
-                                          const AirConst<float> *, bool);
+                                          const AirConst<float> *, bool, bool);
 
 } // namespace op2b

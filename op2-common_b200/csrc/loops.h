@@ -101,11 +101,14 @@ cudaError_t launch_bres_calc_atomic(const LaunchCtx &c, int nbedge, const int *p
 // x with constants k, as adt_calc computes it, written into adt_next (adt is
 // only read).  keep_res: res is read but not zeroed (the
 // runtime records that it is zero and zeroes it only if something reads it
-// before a res_calc rewrites it)
+// before a res_calc rewrites it).  reverse: the cells are taken from the last
+// down (the loop before walked them upwards, so the rows it touched last are
+// the ones still in L2); the result is the same but for rms's summation order
 template <typename T>
 cudaError_t launch_update(const LaunchCtx &c, int ncell, const T *qold, T *q, T *res,
                           const T *adt, const RedScratch &s, const int *pcell = nullptr,
                           const T *x = nullptr, T *adt_next = nullptr,
-                          const AirConst<T> *k = nullptr, bool keep_res = false);
+                          const AirConst<T> *k = nullptr, bool keep_res = false,
+                          bool reverse = false);
 
 }  // namespace op2b

@@ -569,6 +569,7 @@ void op_exit(void) {
   r.opt_atomic_seg = d.opt_atomic_seg;
   r.opt_jit_warp = d.opt_jit_warp;
   r.opt_jit_exact = d.opt_jit_exact;
+  r.opt_update_rev = d.opt_update_rev;
   r.opt_atomic_blocks = d.opt_atomic_blocks;
   r.ring_used = 0;
   r.opt_gemm_tma = d.opt_gemm_tma;
@@ -1180,6 +1181,8 @@ int op2b_set_option(const char *key, long value) {
     r.opt_jit_warp = value != 0;
   } else if (k == "jit_exact") {
     r.opt_jit_exact = value != 0;
+  } else if (k == "update_reverse") {
+    r.opt_update_rev = value != 0;
   } else if (k == "atomic_blocks") {
     if (value < 1 || value > 4096) {
       set_error("op2b_set_option: atomic_blocks must be between 1 and 4096");
@@ -1278,6 +1281,7 @@ long op2b_get_option(const char *key) {
   if (k == "atomic_segmented") return r.opt_atomic_seg;
   if (k == "jit_warp") return r.opt_jit_warp;
   if (k == "jit_exact") return r.opt_jit_exact;
+  if (k == "update_reverse") return r.opt_update_rev;
   if (k == "atomic_blocks") return r.opt_atomic_blocks;
   if (k == "ring_used") return r.ring_used;  // read-only
   if (k == "gemm_tma") return r.opt_gemm_tma;

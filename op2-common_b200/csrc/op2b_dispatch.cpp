@@ -775,14 +775,16 @@ int loop_update(const char *name, op_set set, int nargs, op_arg *a) {
                               (const double *)a[3].dat->data_d, r.red,
                               spec ? sp.pcell->map_d : nullptr,
                               spec ? (const double *)sp.x->data_d : nullptr,
-                              spec ? (double *)sp.shadow : nullptr, &sp.kd, keep_res);
+                              spec ? (double *)sp.shadow : nullptr, &sp.kd, keep_res,
+                              r.opt_update_rev != 0);
   else
     e = launch_update<float>(r.ctx(), C, (const float *)qin, (float *)qout,
                              (float *)a[2].dat->data_d,
                              (const float *)a[3].dat->data_d, r.red,
                              spec ? sp.pcell->map_d : nullptr,
                              spec ? (const float *)sp.x->data_d : nullptr,
-                             spec ? (float *)sp.shadow : nullptr, &sp.kf, keep_res);
+                             spec ? (float *)sp.shadow : nullptr, &sp.kf, keep_res,
+                             r.opt_update_rev != 0);
   // with the speculation the pass also reads pcell and x and writes adt
   r.end_loop(spec ? bytes + 16.0 * C + (double)rb * (2.0 * N + C) : bytes);
   sp.inplace = spec && e == cudaSuccess;

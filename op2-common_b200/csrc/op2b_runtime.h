@@ -136,6 +136,7 @@ struct Runtime {
   int opt_atomic_seg = 1;     // inc_mode 0: 1 = segmented (warp-combined) atomics, 0 = per edge
   int opt_jit_warp = 1;       // generated loops: coalesced direct rows, vector gathers, warp-combined increments
   int opt_jit_exact = 0;      // generated loops that only increment one dat: owner computes, bit-exact
+  int opt_update_rev = 1;     // the update kernel walks the cells downwards (L2 reuse after the pair)
   int opt_atomic_blocks = 4096; // inc_mode 0: 256-thread CTAs per SM in res_calc's grid (at most)
   int ring_used = 0;          // the last res_calc launch ran over the flux-ring records
   int opt_gemm_tma = 0;       // op2b_gemm_bf16 engine 0: TMA-fed kernel for k-major operands
