@@ -370,6 +370,10 @@ struct File::Reader {
   explicit Reader(File &f_) : f(f_) {}
 
   std::vector<uint8_t> rd(uint64_t addr, size_t n) const {
+    // sizes come from the file: bounded by it before anything is allocated
+    if (n > f.fsize_ || addr > f.fsize_)
+      fail("corrupt file: " + std::to_string(n) + " bytes at address " + std::to_string(addr) +
+           " lie beyond its end");
     std::vector<uint8_t> v(n);
     if (n == 0) return v;
     if (addr == undef_of(f.sa_) || fseeko(f.fp_, (off_t)(f.base_ + addr), SEEK_SET) != 0 ||
@@ -746,6 +750,7 @@ std::unique_ptr<File> File::open(const std::string &path) {
   if (!f->fp_) fail("cannot open file '" + path + "'");
   fseeko(f->fp_, 0, SEEK_END);
   uint64_t fsize = (uint64_t)ftello(f->fp_);
+  f->fsize_ = fsize;
   // the superblock is at 0 or after a user block of 512, 1024, 2048, ... bytes
   uint64_t sb = kUndef;
   for (uint64_t off = 0; off + 8 <= fsize; off = off ? 2 * off : 512) {

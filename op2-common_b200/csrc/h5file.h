@@ -119,6 +119,7 @@ class File {
   std::unique_ptr<Object> root_;
   FILE *fp_ = nullptr;
   uint64_t base_ = 0;
+  uint64_t fsize_ = 0;  // bytes in the source file: no structure may claim more
   int sa_ = 8, sl_ = 8;  // sizes of offsets and lengths in the source file
   friend struct Reader;
 };

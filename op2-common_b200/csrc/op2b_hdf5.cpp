@@ -15,6 +15,7 @@
 #include <sys/stat.h>
 
 #include <cstdio>
+#include <exception>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -155,7 +156,7 @@ op_set op_decl_set_hdf5(char const *file, char const *name) {
     int size;
     memcpy(&size, v.data(), 4);
     return op_decl_set(size, name);
-  } catch (const H::Error &e) {
+  } catch (const std::exception &e) {
     set_error("op_decl_set_hdf5: %s: %s", file, e.what());
     return nullptr;
   }
@@ -175,7 +176,7 @@ op_set op_decl_set_hdf5_infer_size(char const *file, char const *name,
     long long size, dim;
     props(*o, size, dim);
     return op_decl_set((int)size, name);
-  } catch (const H::Error &e) {
+  } catch (const std::exception &e) {
     set_error("op_decl_set_hdf5_infer_size: %s: %s", file, e.what());
     return nullptr;
   }
@@ -223,7 +224,7 @@ op_map op_decl_map_hdf5(op_set from, op_set to, int dim, char const *file, char 
       m[i] = (int)w[i];
     }
     return op_decl_map(from, to, dim, m.empty() ? nullptr : m.data(), name);
-  } catch (const H::Error &e) {
+  } catch (const std::exception &e) {
     set_error("op_decl_map_hdf5: %s: %s", file, e.what());
     return nullptr;
   }
@@ -266,7 +267,7 @@ op_dat op_decl_dat_hdf5(op_set set, int dim, char const *type, char const *file,
     std::vector<uint8_t> v = f->read(*o, want);
     return op_decl_dat_char(set, dim, type, (int)want.size, v.empty() ? nullptr : (char *)v.data(),
                             name);
-  } catch (const H::Error &e) {
+  } catch (const std::exception &e) {
     set_error("op_decl_dat_hdf5: %s: %s", file, e.what());
     return nullptr;
   }
@@ -308,7 +309,7 @@ void op_get_const_hdf5(char const *name, int dim, char const *type, char *const_
     }
     std::vector<uint8_t> v = f->read(*o, want);
     memcpy(const_data, v.data(), (size_t)dim * want.size);
-  } catch (const H::Error &e) {
+  } catch (const std::exception &e) {
     set_error("op_get_const_hdf5: %s: %s", file_name, e.what());
   }
 }
@@ -348,7 +349,7 @@ void op_dump_to_hdf5(char const *file_name) {
       o.set_attr(str_attr("type", d->type, strlen(d->type)));
     }
     f->save(file_name);
-  } catch (const H::Error &e) {
+  } catch (const std::exception &e) {
     set_error("op_dump_to_hdf5: %s: %s", file_name, e.what());
   }
 }
@@ -372,7 +373,7 @@ void op_write_const_hdf5(char const *name, int dim, char const *type, char *cons
     o.set_attr(int_attr("dim", dim));
     o.set_attr(str_attr("type", stored_name(type), strlen(type)));
     f->save(file_name);
-  } catch (const H::Error &e) {
+  } catch (const std::exception &e) {
     set_error("op_write_const_hdf5: %s: %s", file_name, e.what());
   }
 }
@@ -448,7 +449,7 @@ void op_fetch_data_hdf5_file_path(op_dat dat, char const *file_name, char const 
       n.set_attr(str_attr("type", dat->type, strlen(dat->type)));
     }
     f->save(file_name);
-  } catch (const H::Error &e) {
+  } catch (const std::exception &e) {
     set_error("op_fetch_data_hdf5_file: %s: %s", file_name, e.what());
   }
 }
@@ -477,7 +478,7 @@ int op2b_h5_info(const char *file, const char *path, int *rank, long long dims[8
       snprintf(type, (size_t)type_len, "%s", t.c_str());
     }
     return 0;
-  } catch (const H::Error &e) {
+  } catch (const std::exception &e) {
     set_error("op2b_h5_info: %s", e.what());
     return -1;
   }
@@ -505,7 +506,7 @@ int op2b_h5_read(const char *file, const char *path, const char *type, void *out
     std::vector<uint8_t> v = f->read(*o, t);
     if (!v.empty()) memcpy(out, v.data(), v.size());
     return 0;
-  } catch (const H::Error &e) {
+  } catch (const std::exception &e) {
     set_error("op2b_h5_read: %s", e.what());
     return -1;
   }
@@ -531,7 +532,7 @@ int op2b_h5_write(const char *file, const char *path, const char *type, int rank
     f->put(path ? path : "", t, d, data);
     f->save(file);
     return 0;
-  } catch (const H::Error &e) {
+  } catch (const std::exception &e) {
     set_error("op2b_h5_write: %s", e.what());
     return -1;
   }
@@ -563,7 +564,7 @@ int op2b_h5_set_attr(const char *file, const char *path, const char *name, const
     }
     f->save(file);
     return 0;
-  } catch (const H::Error &e) {
+  } catch (const std::exception &e) {
     set_error("op2b_h5_set_attr: %s", e.what());
     return -1;
   }
@@ -591,7 +592,7 @@ int op2b_h5_get_attr(const char *file, const char *path, const char *name, char 
     }
     if (out && out_len > 0) snprintf(out, (size_t)out_len, "%s", s.c_str());
     return 0;
-  } catch (const H::Error &e) {
+  } catch (const std::exception &e) {
     set_error("op2b_h5_get_attr: %s", e.what());
     return -1;
   }
@@ -616,7 +617,7 @@ long long op2b_h5_list(const char *file, char *out, long long out_len) {
     w.go(f->root(), "");
     if (out && out_len > 0) snprintf(out, (size_t)out_len, "%s", s.c_str());
     return (long long)s.size() + 1;
-  } catch (const H::Error &e) {
+  } catch (const std::exception &e) {
     set_error("op2b_h5_list: %s", e.what());
     return -1;
   }

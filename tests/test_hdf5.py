@@ -231,3 +231,23 @@ def test_reader_paths_the_writer_does_not_produce(tmp_path):
     np.testing.assert_array_equal(L.h5_read(f, "/grid/a", "int"), a)
     assert L.h5_info(f, "/grid/a") == ((7, 5), "UNRECOGNISED")
     np.testing.assert_array_equal(L.h5_read(f, "b"), b)
+
+
+def test_corrupt_sizes_are_errors_not_allocations(tmp_path):
+    """A file whose structures claim more bytes than it holds (here the root
+    object header's size, and a truncated copy) is refused with a message;
+    the reader never allocates what the file merely claims."""
+    f = str(tmp_path / "ok.h5")
+    L.h5_write(f, "x", np.arange(10.0))
+    raw = bytearray(open(f, "rb").read())
+    root_oh = struct.unpack_from("<Q", raw, 64)[0]      # root symbol table entry
+    bad = bytearray(raw)
+    struct.pack_into("<I", bad, root_oh + 8, 0xFFFFFFF0)   # object header size
+    g = str(tmp_path / "bad.h5")
+    open(g, "wb").write(bytes(bad))
+    with pytest.raises(L.Op2Error, match="beyond its end"):
+        L.h5_list(g)
+    t = str(tmp_path / "short.h5")
+    open(t, "wb").write(bytes(raw[:len(raw) - 40]))          # the data cut short
+    with pytest.raises(L.Op2Error):
+        L.h5_read(t, "x")
