@@ -586,3 +586,28 @@ def test_errors_are_reported_not_run_on_host(op2):
         L.op_decl_map(app.edges, app.cells, 2, np.full(2 * m.nedge, m.ncell), "bad")
     launches = L.load().op2b_kernel_launches()
     assert launches >= 0
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_reversed_update_changes_only_the_rms_summation_order(op2, dtype):
+    """Option update_reverse (the default) walks the update's cells from the
+    last down, for the L2: q, res, adt, maxerr and errloc are the same bits as
+    walking upwards (errloc: the lowest cell on ties either way), and rms
+    differs only by the order of its sum."""
+    m = M.channel_bump(240, 120, seed=2)
+    out = {}
+    for rev in (1, 0):
+        L.op_exit()
+        L.op_init()
+        L.set_option("update_reverse", rev)
+        app = Airfoil(m, dtype=dtype)
+        app.renumber(stats=False)
+        hist = app.iterate(20)
+        f = app.fetch()
+        out[rev] = (hist, f)
+    (h1, f1), (h0, f0) = out[1], out[0]
+    for k in ("q", "res", "adt", "qold"):
+        assert np.array_equal(f1[k], f0[k]), k
+    for (r1, m1, e1), (r0, m0, e0) in zip(h1, h0):
+        assert m1 == m0 and e1 == e0
+        assert abs(r1 / r0 - 1) < 1e-12
