@@ -6,10 +6,12 @@ gradients per step and averages them itself.  The ranks run as two processes
 on one GPU with gloo (the all-reduce goes through host memory; no kernel
 waits for the other rank); NCCL between GPUs takes the same code path with an
 on-device all-reduce.  The backward pass's split-K products add with atomics,
-so gradients agree to rounding, not bit for bit: the data-parallel
-parameters must sit as close to the emulation as the emulation run twice sits
-to itself (2.1e-3 of the update's norm, both, on one run), and far from
-training on rank 0's minibatches alone (0.19)."""
+so gradients agree to rounding, not bit for bit, and AdamW magnifies that
+rounding on parameters whose gradients are near zero: the emulation run twice
+has differed from itself by 1.7e-5 to 2.1e-3 of the update's norm between
+runs, the data-parallel parameters from it by 5e-4 to 2.1e-3.  The test
+asks for at most 1e-2, and at least twenty times closer than training on
+rank 0's minibatches alone (0.19 away)."""
 import os
 import sys
 
@@ -80,5 +82,5 @@ def test_two_ranks_train_as_one_process_averaging_their_gradients(tmp_path):
     print(f"update {upd:.3e}; relative distance: data parallel {rel(p_dp):.3e}, the same "
           f"emulation again {rel(p_avg2):.3e}, rank 0 alone {rel(p_one):.3e}")
     assert upd > 0
-    assert rel(p_dp) <= max(5 * rel(p_avg2), 1e-3)
     assert rel(p_one) >= 0.1
+    assert rel(p_dp) <= 1e-2 and rel(p_dp) <= 0.05 * rel(p_one)
